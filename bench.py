@@ -1,0 +1,330 @@
+"""Throughput benchmark of the SPH step: particle-steps/s on B200.
+
+Workload: the fractal-channel configuration — seeded diamond-square DEM
+1024 x 1024 at 5 m (Hurst 0.8, relief 800 m, carved V-channel), elliptical
+release of ~200k particles (semi-axes 150 x 80 m, mean depth 4 m), Voellmy
+mu = 0.15, xi = 400, Hungr erosion 0.005 1/m over a 2 m layer, adaptive dt.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gfsph|reference]
+
+One JSON line on rank 0.  `value` is measured with the state resident in HBM:
+every timed step is preceded by a 256 MiB write that flushes L2, and only the
+device time of the step (CUDA events inside gfsph_step) is summed.  `e2e`
+goes through the C ABI from pinned host buffers every step: upload of the
+state, one step, download of the state.  With N > 1 every rank runs its own
+replica (a different seed) on its own GPU: there is no exchange in the path.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "deslizamientos-y-flujos_b200")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+METRIC = "SPH particle-steps/s"
+UNIT = "particle-steps/s"
+B_ALG = {"k_density": 24, "k_force_rk": 72, "k_xsph": 44, "k_hist": 28}  # bytes per particle and launch
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+_REF_CASE = None
+
+
+def cpu_reference_rate(seconds_budget, mode=0):
+    """The reference path on the host (FP32 oracle port, one thread) on a
+    bounded sample of the workload: a scaled-down release on the same DEM
+    shape; returns (particle-steps/s, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gfsph
+    import oracle
+    import workloads
+    global _REF_CASE
+    if _REF_CASE is None:
+        w = workloads.fractal_channel(n_target=20_000)
+        p = workloads.make_params(w, gfsph)
+        _REF_CASE = (w, p, oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv))
+    w, p, topol = _REF_CASE
+    ny, nx = w.z.shape
+    st = oracle.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    t0 = time.perf_counter()
+    oracle.run(mode, p, nx, ny, w.dx, w.dy, st, 1)
+    one = max(time.perf_counter() - t0, 1e-3)
+    steps = max(1, min(200, int(seconds_budget / one)))
+    t0 = time.perf_counter()
+    oracle.run(mode, p, nx, ny, w.dx, w.dy, st, steps)
+    el = time.perf_counter() - t0
+    desc = (f"{steps} steps of the fractal-channel workload with a {w.n}-particle release (same DEM, "
+            f"same physics) on 1 host thread, oracle mode FP32")
+    return w.n * steps / el, steps, w.n, el, desc
+
+
+def run_reference_arm(args, rank, world):
+    """The reference's CPU path (the FP32 oracle port; the Fortran reference
+    cannot be built here) on the host, one thread, each bench step a bounded
+    sample of oracle steps so the whole run stays within a few minutes."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gfsph
+    import oracle
+    import workloads
+    w = workloads.fractal_channel(n_target=20_000)
+    p = workloads.make_params(w, gfsph)
+    topol = oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv)
+    ny, nx = w.z.shape
+    st = oracle.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    t0 = time.perf_counter()
+    oracle.run(0, p, nx, ny, w.dx, w.dy, st, 1)
+    one = max(time.perf_counter() - t0, 1e-4)
+    per = max(1, int(150.0 / max(args.steps + args.warmup, 1) / one))
+    for _ in range(args.warmup):
+        oracle.run(0, p, nx, ny, w.dx, w.dy, st, per)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.run(0, p, nx, ny, w.dx, w.dy, st, per)
+    el = time.perf_counter() - t0
+    value = w.n * per * args.steps / el
+    desc = (f"{per} oracle steps per bench step of the fractal-channel workload with a {w.n}-particle "
+            f"release (same DEM and physics), FP32, 1 host thread")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / (args.steps * per),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "fractal_channel: 1024^2 DEM at 5 m, elliptical release (bounded sample)",
+                   "parallelism": "single host thread (the reference is single-threaded)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="gfsph", choices=["gfsph", "reference"])
+    ap.add_argument("--n", type=int, default=200_000, help="particles per replica")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+
+    import build as pkg_build
+    pkg_build.build()
+    import gfsph
+    import workloads
+
+    w = workloads.fractal_channel(n_target=args.n, seed=2 + rank)
+    p = workloads.make_params(w, gfsph)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)  # the flush, the events and the library share one stream
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    n = w.n
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (graph capture, capacity growth)
+    for _ in range(args.warmup):
+        sim.step(1)
+
+    # ---- timed: device-resident state, L2 flushed before every step
+    sim.profile(2)
+    l0 = sim.launch_count()
+    barrier()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            sim.step(1)
+        barrier()
+    launches = sim.launch_count() - l0
+    ms_total, nsteps = sim.profile_read().get("step_batches", (0.0, 0))
+    t_dev = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
+    ms_total = float(t_dev.item())
+    value = world * n * args.steps / (ms_total / 1000.0)
+    clocks = clk.summary()
+
+    # ---- steady state: K steps in one call, L2 warm (for reference only)
+    sim.profile(2)
+    barrier()
+    sim.step(args.steps)
+    ms_steady = sim.profile_read().get("step_batches", (0.0, 0))[0]
+    steady = n * args.steps / (ms_steady / 1000.0)
+
+    # ---- per-kernel device times (events around every launch)
+    sim.profile(1)
+    kprof_steps = min(args.steps, 50)
+    for _ in range(kprof_steps):
+        flush.zero_()
+        sim.step(1)
+    kprof = sim.profile_read()
+    sim.profile(0)
+    tot = sum(ms for ms, _ in kprof.values())
+    dom = max(kprof, key=lambda k: kprof[k][0])
+    dom_ms = kprof[dom][0] / kprof[dom][1]
+    peak, peak_kind = load_peaks()
+    st_now = sim.download()
+    nact = int((st_now["flag"] == 0).sum())
+    b_launch = B_ALG.get(dom, 0) * nact
+    achieved = b_launch / (dom_ms / 1000.0) / 1e9
+    shares = {k: round(ms / tot, 4) for k, (ms, _) in sorted(kprof.items(), key=lambda kv: -kv[1][0])}
+
+    # ---- e2e through the C ABI with pinned host buffers
+    pin = {k: torch.empty(a.shape, dtype=torch.float32 if a.dtype == np.float32 else torch.int32,
+                          pin_memory=True).numpy() for k, a in st_now.items()}
+    for k in pin:
+        pin[k][...] = st_now[k]
+    h2d = n * (8 + 8 + 4 + 4 + 4 + 4)
+    d2h = n * (8 + 8 + 4 + 4 + 4 + 4)
+    for _ in range(3):
+        sim.upload(pin["x"], pin["v"], pin["rho"], pin["mass"], pin["hsml"], pin["flag"])
+        sim.step(1)
+        sim.download(pin)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = min(args.steps, 100)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        sim.upload(pin["x"], pin["v"], pin["rho"], pin["mass"], pin["hsml"], pin["flag"])
+        sim.step(1)
+        sim.download(pin)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t_e2e = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * e2e_steps / (float(t_e2e.item()) / 1000.0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, steps, nc, el, desc = cpu_reference_rate(args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "fractal_channel: 1024^2 DEM at 5 m, ~200k-particle elliptical release, "
+                                   "Voellmy + Hungr erosion, adaptive dt",
+                       "n_particles": n, "dem": w.meta["dem"], "lattice_m": round(w.meta["lattice"], 4),
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "alg_bytes_per_launch": b_launch, "avg_launch_ms": dom_ms,
+                         "step_achieved_gbs": 168 * n * args.steps / (ms_total / 1000.0) / 1e9 / world},
+            "kernel_shares": shares,
+            "steady_state": {"value": steady, "unit": UNIT, "note": "K steps in one call, L2 not flushed"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,814 @@
+// C ABI of the SPH step (include/gfsph.h): handle, device memory, the
+// per-step launch sequence, CUDA-graph replay and capacity growth.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/gfsph.h"
+#include "gfsph_kernels.cuh"
+
+using namespace gfsph;
+
+namespace {
+
+enum KernelId {
+    K_PREP, K_BOUNDS, K_GRID, K_CLEAR, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
+    K_REORDER, K_DENSITY, K_FORCE_RK, K_XSPH, K_DEM_ERODE, K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD,
+    K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
+    K_COUNT
+};
+const char* kKernelNames[K_COUNT] = {
+    "k_prep", "k_bounds", "k_grid", "k_clear_cells", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
+    "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_force_rk", "k_xsph", "k_dem_erode", "k_step_end",
+    "k_copy_state", "k_unsort", "k_raster_idw", "k_hazard", "step_batches"};
+
+constexpr int kThreads = 128;
+constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
+constexpr int kChunkSteps = 256;     // steps between host checks of the error word
+constexpr int kMaxCells = kScanTile * 8192;
+
+__global__ void k_copy_state(PState A, PState B, int n) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        B.pos[s] = A.pos[s]; B.vel[s] = A.vel[s]; B.rho[s] = A.rho[s]; B.mass[s] = A.mass[s];
+        B.hsml[s] = A.hsml[s]; B.flag[s] = A.flag[s]; B.id[s] = A.id[s];
+    }
+}
+
+// Scatters the sorted state back to the original particle order.
+__global__ void k_unsort(PState B, int n, PState U) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        int o = B.id[s];
+        U.pos[o] = B.pos[s]; U.vel[o] = B.vel[s]; U.rho[o] = B.rho[s]; U.mass[o] = B.mass[s];
+        U.hsml[o] = B.hsml[s]; U.flag[o] = B.flag[s];
+    }
+}
+
+__global__ void k_unsort_f2(const float2* src, const int* id, int n, float2* dst) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) dst[id[s]] = src[s];
+}
+
+__global__ void k_iota(int* id, int n) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) id[s] = s;
+}
+
+__global__ void k_hazard_finish(const unsigned int* mo, float* out, int np) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+        unsigned int o = mo[k];
+        out[k] = (o == 0u) ? 0.f : o2f(o);
+    }
+}
+
+__global__ void k_d2f(const double* src, float* out, int np) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) out[k] = (float)src[k];
+}
+
+__global__ void k_i2f(const int* src, float* out, int np) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) out[k] = (float)src[k];
+}
+
+template <class T>
+int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)p, count * sizeof(T)) == cudaSuccess ? 0 : GFSPH_ERR_CUDA;
+}
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+int blocks_for(long long work, int threads = kThreads) {
+    long long b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148LL * 64) b = 148LL * 64;
+    return (int)b;
+}
+
+}  // namespace
+
+struct gfsph_handle {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    gfsph_params P;
+    Rheo rheo;
+    // DEM
+    int nx = 0, ny = 0;
+    DemView dem;
+    float2* d_grad = nullptr;
+    float4* d_curvA = nullptr;
+    float2* d_curvB = nullptr;
+    float* d_z = nullptr;
+    float* d_eroded = nullptr;
+    float* d_avail = nullptr;
+    double2* d_auxv = nullptr;
+    // particles
+    int n = 0;
+    PState A{}, B{}, U{};
+    int* cellA = nullptr;
+    float2* velfin = nullptr;
+    float* pterm = nullptr;
+    int2* keyrank = nullptr;
+    int* perm = nullptr;
+    float2* f2tmp = nullptr;
+    int* nbr = nullptr;
+    int* ncount = nullptr;
+    int kcap = 0;
+    // cells
+    int* count = nullptr;
+    int* start = nullptr;
+    int* tile_sum = nullptr;
+    int cap_cells = 0;
+    // scalars
+    StepScalars* S = nullptr;
+    StepScalars* hS = nullptr;  // pinned mirror
+    // graphs
+    cudaGraphExec_t g1 = nullptr, gK = nullptr;
+    // profiling: level 1 = per-kernel events (no graphs), 2 = events around
+    // each gfsph_step's device work (graphs kept)
+    bool profile = false;
+    int profile_level = 0;
+    cudaEvent_t ev0[K_COUNT]{}, ev1[K_COUNT]{};
+    bool pending[K_COUNT]{};
+    double prof_ms[K_COUNT]{};
+    long long prof_cnt[K_COUNT]{};
+    long long launches = 0;
+    bool has_state = false, searched = false;
+    // outputs
+    double2* d_racc = nullptr;
+    float* d_rout = nullptr;
+    double *haz_sum_h = nullptr, *haz_sum_v = nullptr;
+    unsigned int *haz_max_h = nullptr, *haz_max_v = nullptr;
+    int* haz_cnt = nullptr;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return GFSPH_OK;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return GFSPH_ERR_NO_DEVICE;
+    return GFSPH_ERR_CUDA;
+}
+
+#define CK(x)                                   \
+    do {                                        \
+        cudaError_t e_ = (x);                   \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+void drop_graphs(gfsph_handle* h) {
+    if (h->g1) cudaGraphExecDestroy(h->g1);
+    if (h->gK) cudaGraphExecDestroy(h->gK);
+    h->g1 = h->gK = nullptr;
+}
+
+template <class F>
+void launch(gfsph_handle* h, int kid, F&& f) {
+    if (h->profile) cudaEventRecord(h->ev0[kid], h->stream);
+    f();
+    if (h->profile) {
+        cudaEventRecord(h->ev1[kid], h->stream);
+        h->pending[kid] = true;
+    }
+    h->launches++;
+}
+
+int profile_collect(gfsph_handle* h) {
+    if (!h->profile) return 0;
+    CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < K_COUNT; k++)
+        if (h->pending[k]) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, h->ev0[k], h->ev1[k]);
+            h->prof_ms[k] += ms;
+            h->prof_cnt[k] += 1;
+            h->pending[k] = false;
+        }
+    return 0;
+}
+
+// The cell search: bounds, grid, counting sort, reorder, neighbours+density.
+// Returns the number of kernels enqueued.
+int enqueue_search(gfsph_handle* h, int advance) {
+    const int n = h->n;
+    cudaStream_t st = h->stream;
+    StepScalars* S = h->S;
+    int nk = 0;
+    int pb = blocks_for(n);
+    int nscan = (h->cap_cells + kScanTile - 1) / kScanTile;
+    launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++;
+    launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, S); }); nk++;
+    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_cells); }); nk++;
+    launch(h, K_CLEAR, [&] { k_clear_cells<<<148 * 4, 256, 0, st>>>(h->count, S); }); nk++;
+    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, S, h->count, h->keyrank); }); nk++;
+    launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, S); }); nk++;
+    launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, S); }); nk++;
+    launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, S); }); nk++;
+    launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, S, h->perm); }); nk++;
+    launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, S); }); nk++;
+    launch(h, K_REORDER, [&] { k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, S); }); nk++;
+    launch(h, K_DENSITY, [&] {
+        k_density<<<pb, kThreads, 0, st>>>(h->A, h->cellA, h->start, S, h->rheo, n, h->kcap, h->nbr, h->ncount, h->pterm);
+    }); nk++;
+    return nk;
+}
+
+int enqueue_step(gfsph_handle* h) {
+    const int n = h->n;
+    cudaStream_t st = h->stream;
+    StepScalars* S = h->S;
+    int pb = blocks_for(n);
+    int nk = enqueue_search(h, 1);
+    launch(h, K_FORCE_RK, [&] {
+        k_force_rk<<<pb, kThreads, 0, st>>>(h->A, h->pterm, h->nbr, h->ncount, S, h->rheo, h->dem, n, h->B, h->velfin,
+                                            h->d_auxv, 0, nullptr);
+    }); nk++;
+    if (h->rheo.av_vel) {
+        launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(h->A, h->nbr, h->ncount, S, h->rheo, n, h->B, h->velfin); });
+        nk++;
+    }
+    if (h->rheo.erosion) {
+        launch(h, K_DEM_ERODE, [&] { k_dem_erode<<<148 * 2, 256, 0, st>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S); });
+        nk++;
+    }
+    launch(h, K_STEP_END, [&] { k_step_end<<<1, 32, 0, st>>>(S); }); nk++;
+    return nk;
+}
+
+int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    long long before = h->launches;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < steps; s++) enqueue_step(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->launches = before;  // capture launches nothing
+    if (e != cudaSuccess) return cuda_status(e);
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    return cuda_status(e);
+}
+
+int kernels_per_step(const gfsph_handle* h) {
+    return 12 + 1 + (h->rheo.av_vel ? 1 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+}
+
+int alloc_cells(gfsph_handle* h, int cap) {
+    if (cap > kMaxCells) return GFSPH_ERR_CAPACITY;
+    dfree(h->count); dfree(h->start); dfree(h->tile_sum);
+    int st = 0;
+    st |= dalloc(&h->count, (size_t)cap + 1);
+    st |= dalloc(&h->start, (size_t)cap + 1);
+    st |= dalloc(&h->tile_sum, 8192);
+    if (st) return GFSPH_ERR_CUDA;
+    CK(cudaMemsetAsync(h->count, 0, ((size_t)cap + 1) * sizeof(int), h->stream));
+    h->cap_cells = cap;
+    drop_graphs(h);
+    return 0;
+}
+
+int alloc_nbr(gfsph_handle* h, int kcap) {
+    dfree(h->nbr);
+    if (dalloc(&h->nbr, (size_t)kcap * (size_t)std::max(h->n, 1))) return GFSPH_ERR_CUDA;
+    h->kcap = kcap;
+    drop_graphs(h);
+    return 0;
+}
+
+void free_particles(gfsph_handle* h) {
+    PState* sets[3] = {&h->A, &h->B, &h->U};
+    for (PState* p : sets) {
+        dfree(p->pos); dfree(p->vel); dfree(p->rho); dfree(p->mass); dfree(p->hsml); dfree(p->flag); dfree(p->id);
+    }
+    dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
+    dfree(h->nbr); dfree(h->f2tmp);
+    h->kcap = 0;
+}
+
+int alloc_pstate(PState* p, int n) {
+    int st = 0;
+    st |= dalloc(&p->pos, n); st |= dalloc(&p->vel, n); st |= dalloc(&p->rho, n); st |= dalloc(&p->mass, n);
+    st |= dalloc(&p->hsml, n); st |= dalloc(&p->flag, n); st |= dalloc(&p->id, n);
+    return st;
+}
+
+// Reads the scalars back (synchronises the stream).
+int read_scalars(gfsph_handle* h) {
+    CK(cudaMemcpyAsync(h->hS, h->S, sizeof(StepScalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+template <class T>
+int set_field(gfsph_handle* h, size_t off, T value) {
+    T* host = reinterpret_cast<T*>(reinterpret_cast<char*>(h->hS) + off);
+    *host = value;
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(h->S) + off, host, sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+
+// After a step batch stopped on a capacity error: grow and clear the error.
+int grow_after_error(gfsph_handle* h) {
+    StepScalars* s = h->hS;
+    int e = s->err;
+    if (e & kErrNonFinite) return GFSPH_ERR_NONFINITE;
+    if (e & kErrEmpty) return GFSPH_ERR_DOMAIN;
+    if (e & kErrCells) {
+        long long want = std::max<long long>((long long)s->need_cells * 2, (long long)h->cap_cells * 2);
+        if (want > kMaxCells) want = kMaxCells;
+        if (want < s->need_cells) return GFSPH_ERR_CAPACITY;
+        int st = alloc_cells(h, (int)want);
+        if (st) return st;
+        // the previous grid's cell range is gone with the old buffer
+        set_field<int>(h, offsetof(StepScalars, ncells), 0);
+        set_field<int>(h, offsetof(StepScalars, ncells_prev), 0);
+    }
+    if (e & kErrNbr) {
+        int want = std::max(s->need_nbr + 16, h->kcap * 3 / 2);
+        int st = alloc_nbr(h, want);
+        if (st) return st;
+    }
+    set_field<int>(h, offsetof(StepScalars, err), 0);
+    set_field<int>(h, offsetof(StepScalars, need_nbr), 0);
+    return 0;
+}
+
+int validate(const gfsph_params* p) {
+    int nfric = (int)(p->cst[4] + 0.01f);
+    bool erosion = p->cst[20] > 1.e-9f;
+    if (!(nfric == 4 || (nfric >= 5 && nfric <= 7))) return GFSPH_ERR_UNSUPPORTED;
+    if (nfric == 4 && !(p->cst[5] >= 1.e-32f)) return GFSPH_ERR_ARG;  // SPH_SW_2019.f90:9547-9550
+    if (erosion && (int)(p->cst[20] + 0.1f) != 1) return GFSPH_ERR_UNSUPPORTED;
+    if (p->skf != 1 && p->skf != 4) return GFSPH_ERR_UNSUPPORTED;
+    if (p->pa_sph != 1 && p->pa_sph != 2) return GFSPH_ERR_UNSUPPORTED;
+    if (p->nnps != 2 && p->nnps != 4) return GFSPH_ERR_UNSUPPORTED;
+    if (p->sle != 0 && p->sle != 1) return GFSPH_ERR_UNSUPPORTED;
+    if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
+    if (p->ic_adapt < 0 || p->ic_adapt > 2) return GFSPH_ERR_UNSUPPORTED;
+    if ((int)(p->cst[15] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;  // ic_cosTheta
+    if ((int)(p->cst[19] + 0.1f) != 0) return GFSPH_ERR_UNSUPPORTED;   // ic_fct_dens
+    if (p->cst[0] < 0.f) return GFSPH_ERR_UNSUPPORTED;                 // inclined-plane gravity input
+    if (p->cst[14] <= 1.e-8f || p->cst[9] <= 1.e-8f) return GFSPH_ERR_ARG;  // comp, hfrict0 (:1357-1365)
+    if (!(p->dt > 0.f)) return GFSPH_ERR_ARG;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol);
+
+extern "C" {
+
+int gfsph_version(void) { return 1; }
+
+const char* gfsph_strerror(int s) {
+    switch (s) {
+    case GFSPH_OK: return "ok";
+    case GFSPH_T_END_REACHED: return "t_end reached";
+    case GFSPH_ERR_ARG: return "invalid argument";
+    case GFSPH_ERR_CUDA: return "CUDA runtime error";
+    case GFSPH_ERR_CAPACITY: return "capacity exceeded";
+    case GFSPH_ERR_UNSUPPORTED: return "unsupported option";
+    case GFSPH_ERR_STATE: return "call out of order";
+    case GFSPH_ERR_NO_DEVICE: return "no usable CUDA device";
+    case GFSPH_ERR_NONFINITE: return "non-finite value in the particle state";
+    case GFSPH_ERR_DOMAIN: return "no particle inside the DEM box";
+    default: return "unknown status";
+    }
+}
+
+int gfsph_num_kernels(void) { return K_COUNT; }
+const char* gfsph_kernel_name(int k) { return (k >= 0 && k < K_COUNT) ? kKernelNames[k] : nullptr; }
+
+int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out) {
+    if (!p || !dem || !out) return GFSPH_ERR_ARG;
+    *out = nullptr;
+    int st = validate(p);
+    if (st) return st;
+    if (dem->nx < 3 || dem->ny < 3 || !(dem->dx > 0.f) || !(dem->dy > 0.f)) return GFSPH_ERR_ARG;
+    if (!dem->topol && !dem->z) return GFSPH_ERR_ARG;
+    if (dem->topol && dem->ntopo < 15) return GFSPH_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return GFSPH_ERR_NO_DEVICE;
+
+    gfsph_handle* h = new (std::nothrow) gfsph_handle();
+    if (!h) return GFSPH_ERR_ARG;
+    cudaGetDevice(&h->dev);
+    if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return GFSPH_ERR_CUDA;
+    }
+    h->stream = h->own_stream;
+    h->P = *p;
+    Rheo& c = h->rheo;
+    const float* k = p->cst;  // k[i-1] = const(i)
+    c.g = k[0]; c.dens = k[1]; c.xi = k[2]; c.tauy0 = k[5]; c.constK = k[6]; c.tanfi = k[8];
+    c.hfrict0 = k[9]; c.comp = k[14]; c.keros = k[21];
+    c.slip = (k[46] > 1.e-6f) ? (2.f * k[46]) / (1.f + k[46]) : 1.f;
+    c.h_inf = p->h_inf;
+    c.cgra05 = k[0] * 0.5f;
+    c.nfric = (int)(k[4] + 0.01f);
+    c.erosion = (k[20] > 1.e-9f) ? 1 : 0;
+    c.skf = p->skf; c.pa_sph = p->pa_sph; c.sle = p->sle; c.av_vel = p->average_velocity ? 1 : 0;
+    c.ic_adapt = p->ic_adapt;
+
+    // DEM rows on the host, as Topo_main leaves them before the time loop
+    int nx = dem->nx, ny = dem->ny;
+    size_t np = (size_t)nx * ny;
+    std::vector<float> topol(np * GFSPH_NTOPO, 0.f);
+    if (dem->topol) {
+        for (size_t ip = 0; ip < np; ip++)
+            for (int r = 0; r < 15; r++) topol[ip * GFSPH_NTOPO + r] = dem->topol[ip * (size_t)dem->ntopo + r];
+    } else {
+        for (size_t ip = 0; ip < np; ip++) topol[ip * GFSPH_NTOPO] = dem->z[ip];
+        st = gfsph_dem_topol(p->dem_deriv, nx, ny, dem->dx, dem->dy, topol.data());
+        if (st) { gfsph_destroy(h); return st; }
+        // erodible depth, Input_SW SPH_SW_2019.f90:1288-1307
+        float avail = 0.f;
+        if (k[20] > 1.e-9f) avail = (k[47] > 1.e-6f) ? k[47] : 999.f;
+        for (size_t ip = 0; ip < np; ip++) topol[ip * GFSPH_NTOPO + 14] = avail;
+    }
+    std::vector<float2> grad(np), curvB(np);
+    std::vector<float4> curvA(np);
+    std::vector<float> z(np), er(np), av(np);
+    for (size_t ip = 0; ip < np; ip++) {
+        const float* t = &topol[ip * GFSPH_NTOPO];
+        z[ip] = t[0];
+        grad[ip] = make_float2(t[1], t[2]);
+        curvA[ip] = make_float4(t[3], t[4], t[5], t[6]);
+        curvB[ip] = make_float2(t[7], t[8]);
+        er[ip] = t[13];
+        av[ip] = t[14];
+    }
+    h->nx = nx; h->ny = ny;
+    st = 0;
+    st |= dalloc(&h->d_grad, np); st |= dalloc(&h->d_curvA, np); st |= dalloc(&h->d_curvB, np);
+    st |= dalloc(&h->d_z, np); st |= dalloc(&h->d_eroded, np); st |= dalloc(&h->d_avail, np);
+    st |= dalloc(&h->d_auxv, np);
+    st |= dalloc(&h->S, 1);
+    if (st) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
+    if (cudaMallocHost((void**)&h->hS, sizeof(StepScalars)) != cudaSuccess) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
+    cudaMemcpy(h->d_grad, grad.data(), np * sizeof(float2), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_curvA, curvA.data(), np * sizeof(float4), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_curvB, curvB.data(), np * sizeof(float2), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_z, z.data(), np * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_eroded, er.data(), np * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_avail, av.data(), np * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(h->d_auxv, 0, np * sizeof(double2));
+    DemView& d = h->dem;
+    d.nx = nx; d.ny = ny; d.xmin = dem->xmin; d.ymin = dem->ymin; d.dx = dem->dx; d.dy = dem->dy;
+    d.xmax = d.xmin + (float)(nx - 1) * d.dx;
+    d.ymax = d.ymin + (float)(ny - 1) * d.dy;
+    d.grad = h->d_grad; d.curvA = h->d_curvA; d.curvB = h->d_curvB;
+    std::memset(h->hS, 0, sizeof(StepScalars));
+    h->hS->dt = p->dt;
+    h->hS->time = 0.0;
+    h->hS->t_end = 1e300;
+    cudaMemcpy(h->S, h->hS, sizeof(StepScalars), cudaMemcpyHostToDevice);
+    for (int kk = 0; kk < K_COUNT; kk++) {
+        cudaEventCreate(&h->ev0[kk]);
+        cudaEventCreate(&h->ev1[kk]);
+    }
+    if (cudaGetLastError() != cudaSuccess) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
+    *out = h;
+    return GFSPH_OK;
+}
+
+int gfsph_destroy(gfsph_handle* h) {
+    if (!h) return GFSPH_ERR_ARG;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
+    free_particles(h);
+    dfree(h->count); dfree(h->start); dfree(h->tile_sum);
+    dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
+    dfree(h->d_auxv); dfree(h->S); dfree(h->d_racc); dfree(h->d_rout);
+    dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
+    if (h->hS) cudaFreeHost(h->hS);
+    for (int k = 0; k < K_COUNT; k++) {
+        if (h->ev0[k]) cudaEventDestroy(h->ev0[k]);
+        if (h->ev1[k]) cudaEventDestroy(h->ev1[k]);
+    }
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return GFSPH_OK;
+}
+
+int gfsph_set_stream(gfsph_handle* h, void* stream) {
+    if (!h) return GFSPH_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return GFSPH_OK;
+}
+
+int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const float* rho, const float* mass,
+                 const float* hsml, const int* itype, const int* out_flag) {
+    if (!h || n < 1 || !x || !v || !rho || !mass || !hsml) return GFSPH_ERR_ARG;
+    if (itype)
+        for (int i = 0; i < n; i++)
+            if (itype[i] != 1) return GFSPH_ERR_UNSUPPORTED;  // only soil particles (ic_ws_Interact = 0)
+    if (n != h->n) {
+        CK(cudaStreamSynchronize(h->stream));
+        free_particles(h);
+        h->n = n;
+        int st = 0;
+        st |= alloc_pstate(&h->A, n); st |= alloc_pstate(&h->B, n); st |= alloc_pstate(&h->U, n);
+        st |= dalloc(&h->cellA, n); st |= dalloc(&h->velfin, n); st |= dalloc(&h->pterm, n);
+        st |= dalloc(&h->keyrank, n); st |= dalloc(&h->perm, n); st |= dalloc(&h->ncount, n);
+        st |= dalloc(&h->f2tmp, n);
+        if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
+        st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
+        if (st) return st;
+        drop_graphs(h);
+    }
+    if (h->cap_cells == 0) {
+        int st = alloc_cells(h, 1 << 18);
+        if (st) return st;
+    }
+    cudaStream_t st = h->stream;
+    CK(cudaMemcpyAsync(h->B.pos, x, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->B.vel, v, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->B.rho, rho, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->B.mass, mass, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(h->B.hsml, hsml, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (out_flag) CK(cudaMemcpyAsync(h->B.flag, out_flag, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
+    else CK(cudaMemsetAsync(h->B.flag, 0, (size_t)n * sizeof(int), st));
+    launch(h, K_UNSORT, [&] { k_iota<<<blocks_for(n), kThreads, 0, st>>>(h->B.id, n); });
+    CK(cudaGetLastError());
+    h->has_state = true;
+    h->searched = false;
+    return GFSPH_OK;
+}
+
+int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass, float* hsml, int* out_flag) {
+    if (!h) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    int n = h->n;
+    cudaStream_t st = h->stream;
+    launch(h, K_UNSORT, [&] { k_unsort<<<blocks_for(n), kThreads, 0, st>>>(h->B, n, h->U); });
+    if (x) CK(cudaMemcpyAsync(x, h->U.pos, (size_t)n * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    if (v) CK(cudaMemcpyAsync(v, h->U.vel, (size_t)n * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    if (rho) CK(cudaMemcpyAsync(rho, h->U.rho, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (mass) CK(cudaMemcpyAsync(mass, h->U.mass, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (hsml) CK(cudaMemcpyAsync(hsml, h->U.hsml, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (out_flag) CK(cudaMemcpyAsync(out_flag, h->U.flag, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return GFSPH_OK;
+}
+
+int gfsph_get_time(gfsph_handle* h, double* t, float* dt) {
+    if (!h) return GFSPH_ERR_ARG;
+    int st = read_scalars(h);
+    if (st) return st;
+    if (t) *t = h->hS->time;
+    if (dt) *dt = h->hS->dt;
+    return GFSPH_OK;
+}
+
+int gfsph_set_time(gfsph_handle* h, double t, float dt) {
+    if (!h || !(dt > 0.f)) return GFSPH_ERR_ARG;
+    set_field<double>(h, offsetof(StepScalars, time), t);
+    set_field<float>(h, offsetof(StepScalars, dt), dt);
+    CK(cudaStreamSynchronize(h->stream));
+    return GFSPH_OK;
+}
+
+int gfsph_step(gfsph_handle* h, int nsteps, double t_end, double* t_out, int* steps_done) {
+    if (!h || nsteps < 0) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    int done = 0;
+    int status = GFSPH_OK;
+    int guard = 0;
+    while (done < nsteps) {
+        int chunk = std::min(kChunkSteps, nsteps - done);
+        set_field<double>(h, offsetof(StepScalars, t_end), t_end);
+        set_field<int>(h, offsetof(StepScalars, steps_done), 0);
+        if (h->profile) {
+            for (int s = 0; s < chunk; s++) {
+                enqueue_step(h);
+                int st = profile_collect(h);
+                if (st) return st;
+            }
+        } else {
+            if (!h->g1) { int st = build_graph(h, 1, &h->g1); if (st) return st; }
+            if (!h->gK) { int st = build_graph(h, kGraphSteps, &h->gK); if (st) return st; }
+            int per = kernels_per_step(h);
+            int s = 0;
+            if (h->profile_level == 2) CK(cudaEventRecord(h->ev0[K_STEPS], h->stream));
+            for (; s + kGraphSteps <= chunk; s += kGraphSteps) {
+                CK(cudaGraphLaunch(h->gK, h->stream));
+                h->launches += (long long)per * kGraphSteps;
+            }
+            for (; s < chunk; s++) {
+                CK(cudaGraphLaunch(h->g1, h->stream));
+                h->launches += per;
+            }
+            if (h->profile_level == 2) {
+                CK(cudaEventRecord(h->ev1[K_STEPS], h->stream));
+                CK(cudaEventSynchronize(h->ev1[K_STEPS]));
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, h->ev0[K_STEPS], h->ev1[K_STEPS]);
+                h->prof_ms[K_STEPS] += ms;
+                h->prof_cnt[K_STEPS] += chunk;
+            }
+        }
+        CK(cudaGetLastError());
+        int st = read_scalars(h);
+        if (st) return st;
+        done += h->hS->steps_done;
+        h->searched = true;
+        if (h->hS->err) {
+            if (++guard > 16) return GFSPH_ERR_CAPACITY;
+            st = grow_after_error(h);
+            if (st) { status = st; break; }
+            continue;
+        }
+        if (h->hS->time >= t_end) {
+            if (done < nsteps) status = GFSPH_T_END_REACHED;
+            break;
+        }
+    }
+    if (t_out) *t_out = h->hS->time;
+    if (steps_done) *steps_done = done;
+    return status;
+}
+
+// search + density on the current state (no advance); the state in B is
+// replaced by the cell-sorted copy with the new densities.
+static int search_only(gfsph_handle* h) {
+    for (int tries = 0; tries < 16; tries++) {
+        enqueue_search(h, 0);
+        CK(cudaGetLastError());
+        int st = profile_collect(h);
+        if (st) return st;
+        st = read_scalars(h);
+        if (st) return st;
+        if (h->hS->err) {
+            st = grow_after_error(h);
+            if (st) return st;
+            continue;
+        }
+        h->searched = true;
+        return 0;
+    }
+    return GFSPH_ERR_CAPACITY;
+}
+
+int gfsph_density(gfsph_handle* h, float* rho_out) {
+    if (!h) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    int st = search_only(h);
+    if (st) return st;
+    int n = h->n;
+    launch(h, K_COPY, [&] { k_copy_state<<<blocks_for(n), kThreads, 0, h->stream>>>(h->A, h->B, n); });
+    if (rho_out) return gfsph_download(h, nullptr, nullptr, rho_out, nullptr, nullptr, nullptr);
+    CK(cudaStreamSynchronize(h->stream));
+    return GFSPH_OK;
+}
+
+int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
+    if (!h || !indvxdt) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    int st = search_only(h);
+    if (st) return st;
+    int n = h->n;
+    cudaStream_t s = h->stream;
+    launch(h, K_FORCE_RK, [&] {
+        k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, h->pterm, h->nbr, h->ncount, h->S, h->rheo, h->dem, n, h->B,
+                                                     h->velfin, h->d_auxv, 1, h->velfin);
+    });
+    launch(h, K_UNSORT, [&] { k_unsort_f2<<<blocks_for(n), kThreads, 0, s>>>(h->velfin, h->A.id, n, h->f2tmp); });
+    launch(h, K_COPY, [&] { k_copy_state<<<blocks_for(n), kThreads, 0, s>>>(h->A, h->B, n); });
+    CK(cudaMemcpyAsync(indvxdt, h->f2tmp, (size_t)n * sizeof(float2), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return GFSPH_OK;
+}
+
+int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
+    if (!h || !offsets) return GFSPH_ERR_ARG;
+    if (!h->searched) return GFSPH_ERR_STATE;
+    int n = h->n;
+    int st = read_scalars(h);
+    if (st) return st;
+    int nact = h->hS->nactive;
+    std::vector<int> cnt(n), id(n), tab((size_t)h->kcap * n);
+    CK(cudaMemcpy(cnt.data(), h->ncount, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(id.data(), h->A.id, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tab.data(), h->nbr, tab.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<std::vector<int>> lists(n);
+    for (int s = 0; s < nact; s++) {
+        auto& L = lists[id[s]];
+        for (int k = 0; k < cnt[s] && k < h->kcap; k++) L.push_back(id[tab[(size_t)k * n + s]]);
+        std::sort(L.begin(), L.end());
+    }
+    int tot = 0;
+    for (int i = 0; i < n; i++) {
+        offsets[i] = tot;
+        for (int j : lists[i]) {
+            if (idx && tot < cap) idx[tot] = j;
+            tot++;
+        }
+    }
+    offsets[n] = tot;
+    return (tot > cap) ? GFSPH_ERR_CAPACITY : GFSPH_OK;
+}
+
+int gfsph_raster(gfsph_handle* h, int kind, float* out) {
+    if (!h || !out) return GFSPH_ERR_ARG;
+    int np = h->nx * h->ny;
+    cudaStream_t s = h->stream;
+    int gb = blocks_for(np, 256);
+    if (!h->d_rout && dalloc(&h->d_rout, np)) return GFSPH_ERR_CUDA;
+    switch (kind) {
+    case GFSPH_RASTER_DEPTH_IDW: {
+        if (!h->has_state) return GFSPH_ERR_STATE;
+        if (!h->d_racc && dalloc(&h->d_racc, np)) return GFSPH_ERR_CUDA;
+        CK(cudaMemsetAsync(h->d_racc, 0, (size_t)np * sizeof(double2), s));
+        launch(h, K_RASTER, [&] { k_raster_idw<<<blocks_for(h->n), kThreads, 0, s>>>(h->B, h->n, h->dem, h->d_racc); });
+        launch(h, K_RASTER, [&] { k_raster_idw_finish<<<gb, 256, 0, s>>>(h->d_racc, h->d_rout, np); });
+        break;
+    }
+    case GFSPH_RASTER_MAX_DEPTH:
+    case GFSPH_RASTER_MAX_VEL:
+    case GFSPH_RASTER_SUM_DEPTH:
+    case GFSPH_RASTER_SUM_VEL:
+    case GFSPH_RASTER_COUNT: {
+        if (!h->haz_cnt) {
+            CK(cudaMemsetAsync(h->d_rout, 0, (size_t)np * sizeof(float), s));
+            break;
+        }
+        if (kind == GFSPH_RASTER_MAX_DEPTH) launch(h, K_HAZARD, [&] { k_hazard_finish<<<gb, 256, 0, s>>>(h->haz_max_h, h->d_rout, np); });
+        if (kind == GFSPH_RASTER_MAX_VEL) launch(h, K_HAZARD, [&] { k_hazard_finish<<<gb, 256, 0, s>>>(h->haz_max_v, h->d_rout, np); });
+        if (kind == GFSPH_RASTER_SUM_DEPTH) launch(h, K_HAZARD, [&] { k_d2f<<<gb, 256, 0, s>>>(h->haz_sum_h, h->d_rout, np); });
+        if (kind == GFSPH_RASTER_SUM_VEL) launch(h, K_HAZARD, [&] { k_d2f<<<gb, 256, 0, s>>>(h->haz_sum_v, h->d_rout, np); });
+        if (kind == GFSPH_RASTER_COUNT) launch(h, K_HAZARD, [&] { k_i2f<<<gb, 256, 0, s>>>(h->haz_cnt, h->d_rout, np); });
+        break;
+    }
+    case GFSPH_RASTER_Z: CK(cudaMemcpyAsync(out, h->d_z, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
+    case GFSPH_RASTER_ERODED: CK(cudaMemcpyAsync(out, h->d_eroded, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
+    case GFSPH_RASTER_AVAILABLE: CK(cudaMemcpyAsync(out, h->d_avail, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
+    default: return GFSPH_ERR_ARG;
+    }
+    if (kind <= GFSPH_RASTER_COUNT) CK(cudaMemcpyAsync(out, h->d_rout, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return GFSPH_OK;
+}
+
+int gfsph_hazard_reset(gfsph_handle* h) {
+    if (!h) return GFSPH_ERR_ARG;
+    int np = h->nx * h->ny;
+    if (!h->haz_cnt) {
+        int st = 0;
+        st |= dalloc(&h->haz_sum_h, np); st |= dalloc(&h->haz_sum_v, np);
+        st |= dalloc(&h->haz_max_h, np); st |= dalloc(&h->haz_max_v, np); st |= dalloc(&h->haz_cnt, np);
+        if (st) return GFSPH_ERR_CUDA;
+    }
+    cudaStream_t s = h->stream;
+    CK(cudaMemsetAsync(h->haz_sum_h, 0, (size_t)np * sizeof(double), s));
+    CK(cudaMemsetAsync(h->haz_sum_v, 0, (size_t)np * sizeof(double), s));
+    CK(cudaMemsetAsync(h->haz_max_h, 0, (size_t)np * sizeof(unsigned int), s));
+    CK(cudaMemsetAsync(h->haz_max_v, 0, (size_t)np * sizeof(unsigned int), s));
+    CK(cudaMemsetAsync(h->haz_cnt, 0, (size_t)np * sizeof(int), s));
+    CK(cudaStreamSynchronize(s));
+    return GFSPH_OK;
+}
+
+int gfsph_hazard_sample(gfsph_handle* h) {
+    if (!h) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    if (!h->haz_cnt) {
+        int st = gfsph_hazard_reset(h);
+        if (st) return st;
+    }
+    cudaStream_t s = h->stream;
+    launch(h, K_HAZARD, [&] {
+        k_hazard<<<blocks_for(h->n), kThreads, 0, s>>>(h->B, h->n, h->dem, h->haz_sum_h, h->haz_sum_v, h->haz_max_h,
+                                                      h->haz_max_v, h->haz_cnt);
+    });
+    CK(cudaGetLastError());
+    return GFSPH_OK;
+}
+
+int gfsph_profile(gfsph_handle* h, int enable) {
+    if (!h) return GFSPH_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    h->profile = enable == 1;
+    h->profile_level = enable;
+    for (int k = 0; k < K_COUNT; k++) { h->prof_ms[k] = 0; h->prof_cnt[k] = 0; h->pending[k] = false; }
+    return GFSPH_OK;
+}
+
+int gfsph_profile_read(gfsph_handle* h, int kernel, double* total_ms, long long* launches) {
+    if (!h || kernel < 0 || kernel >= K_COUNT) return GFSPH_ERR_ARG;
+    if (total_ms) *total_ms = h->prof_ms[kernel];
+    if (launches) *launches = h->prof_cnt[kernel];
+    return GFSPH_OK;
+}
+
+long long gfsph_launch_count(gfsph_handle* h) { return h ? h->launches : -1; }
+
+}  // extern "C"

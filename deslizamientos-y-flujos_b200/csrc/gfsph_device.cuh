@@ -1,0 +1,296 @@
+// Device-side arithmetic of the SPH step: the SPH kernel, the bilinear DEM
+// lookup and the basal rheology.  Every expression keeps the evaluation order
+// of the Fortran source it restates (cited per function) and the library is
+// compiled with --fmad=false, so each FP32 operation rounds exactly as the
+// reference's FP32 build does; only the neighbour sums differ (FP64 here).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace gfsph {
+
+constexpr float kPi = 3.14159274101257324f;  // pi = 4.*atan(1.0) in default real
+constexpr float kTwoThirds = (float)(2.0 / 3.0);
+
+// kernel_TOOLS, My_SPH_Tools_2019.f90:2062-2180 (2-D; skf 1 cubic spline,
+// skf 4 Wendland C2).  Returns w and dW/dx for the offset (dx0, dx1) at
+// distance r with smoothing length hs.
+__device__ __forceinline__ void sph_kernel(int skf, float r, float dx0, float dx1, float hs, float& w,
+                                           float& d0, float& d1) {
+    float q = r / hs;
+    w = 0.f; d0 = 0.f; d1 = 0.f;
+    if (skf == 1) {
+        float factor = 15.f / (((7.f * kPi) * hs) * hs);
+        if (q >= 0.f && q <= 1.f) {
+            w = factor * ((kTwoThirds - q * q) + ((q * q) * q) / 2.f);
+            float t = (factor * (-2.f + 1.5f * q)) / (hs * hs);
+            d0 = t * dx0;
+            d1 = t * dx1;
+        } else if (q > 1.f && q <= 2.f) {
+            float u = 2.f - q;
+            w = ((factor * 1.f) / 6.f) * ((u * u) * u);
+            float t = ((((factor * 1.f) / 6.f) * 3.f) * (u * u)) / hs;
+            d0 = -(t * (dx0 / r));
+            d1 = -(t * (dx1 / r));
+        }
+    } else {  // skf == 4
+        float factor = 7.f / (((4.f * kPi) * hs) * hs);
+        if (q >= 0.f && q <= 2.f) {
+            float a = 1.f - q / 2.f;
+            w = factor * (((a * a) * (a * a)) * (2.f * q + 1.f));
+            float t = factor * (-(5.f * ((a * a) * a)));
+            float s = (1.f / hs) / hs;
+            d0 = t * (s * dx0);
+            d1 = t * (s * dx1);
+        }
+    }
+}
+
+__device__ __forceinline__ float sph_kernel_w(int skf, float r, float hs) {
+    float w, a, b;
+    sph_kernel(skf, r, 0.f, 0.f, hs, w, a, b);
+    return w;
+}
+
+// Neighbour test of grid_find (My_SPH_Tools_2019.f90:1010-1019):
+// dr = dx*dx + dy*dy, mh = (hi+hj)/2, r = sqrt(dr), neighbour iff r < 2*mh.
+struct PairGeom {
+    float dx0, dx1, r, mh;
+};
+
+__device__ __forceinline__ bool pair_test(float2 xi, float2 xj, float hi, float hj, PairGeom& g) {
+    g.dx0 = xi.x - xj.x;
+    float dr = g.dx0 * g.dx0;
+    g.dx1 = xi.y - xj.y;
+    dr = dr + g.dx1 * g.dx1;
+    g.mh = (hi + hj) / 2.f;
+    g.r = sqrtf(dr);
+    return g.r < 2.f * g.mh;
+}
+
+// Float <-> order-preserving uint, for atomicMin/atomicMax reductions.
+__device__ __forceinline__ unsigned int f2o(float f) {
+    unsigned int b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float o2f(unsigned int o) {
+#ifdef __CUDA_ARCH__
+    unsigned int b = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+    return __uint_as_float(b);
+#else
+    unsigned int b = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+#endif
+}
+
+// DEM on the device: node (ix, iy) at (xmin + ix*dx, ymin + iy*dy), x fastest.
+struct DemView {
+    int nx, ny;
+    float xmin, ymin, dx, dy, xmax, ymax;
+    const float2* __restrict__ grad;  // topol(2:3,:)
+    const float4* __restrict__ curvA; // topol(4:7,:)  (nfric 7 only)
+    const float2* __restrict__ curvB; // topol(8:9,:)
+};
+
+// Get_Z_Topo, SPH_FEM_topo_2019.f90:2395-2491: bilinear shape functions on
+// the DEM cell containing (xx, yy).  Returns Zx, Zy and, when want_curv, the
+// six curvature terms topol(4..9).
+__device__ __forceinline__ void dem_lookup(const DemView& d, float xx, float yy, float& zpx, float& zpy,
+                                           bool want_curv, float top[6]) {
+    int ipx = (int)((xx - d.xmin) / d.dx + 1.f);
+    int ipy = (int)((yy - d.ymin) / d.dy + 1.f);
+    ipx = min(max(ipx, 1), d.nx - 1);
+    ipy = min(max(ipy, 1), d.ny - 1);
+    int ip = (ipy - 1) * d.nx + (ipx - 1);
+    int n1 = ip, n2 = ip + 1, n3 = ip + 1 + d.nx, n4 = n3 - 1;
+    float xref = d.xmin + (float)(ipx - 1) * d.dx;
+    float yref = d.ymin + (float)(ipy - 1) * d.dy;
+    float xi = (xx - xref) / d.dx;
+    float eta = (yy - yref) / d.dy;
+    float sh1 = (1.f - xi) * (1.f - eta);
+    float sh2 = xi * (1.f - eta);
+    float sh3 = xi * eta;
+    float sh4 = (1.f - xi) * eta;
+    float2 g1 = __ldg(&d.grad[n1]), g2 = __ldg(&d.grad[n2]), g3 = __ldg(&d.grad[n3]), g4 = __ldg(&d.grad[n4]);
+    zpx = ((sh1 * g1.x + sh2 * g2.x) + sh3 * g3.x) + sh4 * g4.x;
+    zpy = ((sh1 * g1.y + sh2 * g2.y) + sh3 * g3.y) + sh4 * g4.y;
+    if (want_curv) {
+        float4 a1 = __ldg(&d.curvA[n1]), a2 = __ldg(&d.curvA[n2]), a3 = __ldg(&d.curvA[n3]), a4 = __ldg(&d.curvA[n4]);
+        float2 b1 = __ldg(&d.curvB[n1]), b2 = __ldg(&d.curvB[n2]), b3 = __ldg(&d.curvB[n3]), b4 = __ldg(&d.curvB[n4]);
+        top[0] = ((sh1 * a1.x + sh2 * a2.x) + sh3 * a3.x) + sh4 * a4.x;
+        top[1] = ((sh1 * a1.y + sh2 * a2.y) + sh3 * a3.y) + sh4 * a4.y;
+        top[2] = ((sh1 * a1.z + sh2 * a2.z) + sh3 * a3.z) + sh4 * a4.z;
+        top[3] = ((sh1 * a1.w + sh2 * a2.w) + sh3 * a3.w) + sh4 * a4.w;
+        top[4] = ((sh1 * b1.x + sh2 * b2.x) + sh3 * b3.x) + sh4 * b4.x;
+        top[5] = ((sh1 * b1.y + sh2 * b2.y) + sh3 * b3.y) + sh4 * b4.y;
+    }
+}
+
+// Constants of the basal rheology, read from const(1..110).
+struct Rheo {
+    float g, dens, xi, tauy0, constK, tanfi, hfrict0, comp, keros, slip, h_inf, cgra05;
+    int nfric, erosion, skf, pa_sph, sle, av_vel, ic_adapt;
+};
+
+// Locals of ExtForces_SW shared with its contained routines.
+struct ExtLocal {
+    float h, hu, hv, hinv, vmod, hvmod, hvmodinv, frictx, fricty, totfrict, cf5, gravx, gravy;
+};
+
+// Start of the ExtForces_SW particle loop, SPH_SW_2019.f90:8564-8596.
+__device__ __forceinline__ void ext_locals(const Rheo& c, float hdepth, float vx, float vy, ExtLocal& L) {
+    L.h = hdepth;
+    L.hu = L.h * vx;
+    L.hv = L.h * vy;
+    if (L.h < c.comp) {
+        L.h = c.comp;
+        L.hu = 0.f; L.hv = 0.f; L.hinv = 0.f; L.vmod = 0.f; L.hvmod = 0.f; L.hvmodinv = 0.f;
+    } else {
+        L.hinv = 1.f / L.h;
+        L.hvmod = sqrtf(L.hu * L.hu + L.hv * L.hv);
+        L.vmod = L.hvmod * L.hinv;
+        L.hvmodinv = (L.hvmod >= 1.e-5f) ? 1.f / L.hvmod : 0.f;
+    }
+}
+
+// Get_Grav_Ext_SW (SPH_SW_2019.f90:9241-9349, ic_cosTheta = 0) and
+// basal_friction_Ext_SW (:9355-9828) before its reversal filter.
+__device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& d, float xx, float yy, float vx,
+                                                  float vy, ExtLocal& L) {
+    const bool frictional = (c.nfric >= 5 && c.nfric <= 7);
+    const bool v2byr = (c.nfric == 7);
+    float zpx, zpy, top[6];
+    dem_lookup(d, xx, yy, zpx, zpy, v2byr, top);
+    L.gravx = -(c.g * zpx);
+    L.gravy = -(c.g * zpy);
+    float hfrict = (L.h > c.hfrict0) ? L.h : c.hfrict0;
+    L.frictx = 0.f; L.fricty = 0.f; L.totfrict = 0.f; L.cf5 = 0.f;
+    if (c.nfric == 4) {  // Bingham regimes, :9552-9572
+        float a_hat = ((6.f * c.constK) * L.hvmod) / (c.tauy0 * (hfrict * hfrict));
+        if (a_hat > 50.f) {
+            float cf4b = (3.f * c.constK) / c.dens;
+            L.frictx = (cf4b * L.hu) / (hfrict * hfrict);
+            L.fricty = (cf4b * L.hv) / (hfrict * hfrict);
+        } else if (a_hat < 0.01f) {
+            float cf4b = c.tauy0 / c.dens;
+            L.frictx = (cf4b * L.hu) * L.hvmodinv;
+            L.fricty = (cf4b * L.hv) * L.hvmodinv;
+        } else {
+            float a2 = 48.f, b2 = -(32.f * a_hat) - 114.f, c2 = 65.f;
+            float xh = (-b2 - sqrtf(b2 * b2 - (4.f * a2) * c2)) / (2.f * a2);
+            float tau0 = c.tauy0 / xh;
+            float cf4b = tau0 / c.dens;
+            L.frictx = (cf4b * L.hu) * L.hvmodinv;
+            L.fricty = (cf4b * L.hv) * L.hvmodinv;
+        }
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+    } else if (frictional) {  // :9660-9750
+        float cv2byr = 0.f;
+        if (v2byr) {
+            float vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
+            L.vmod = sqrtf(vxx * vxx + vyy * vyy);
+            if (L.vmod >= 1e-5f) {
+                float cosa = vxx / L.vmod, sina = vyy / L.vmod;
+                float cos2 = cosa * cosa, sin2 = sina * sina, cbs = sina * cosa;
+                float xnum = (top[3] * cos2 + top[4] * cbs) + top[5] * sin2;
+                float xden = (top[0] * cos2 + top[1] * cbs) + top[2] * sin2;
+                float rinv = xnum / xden;
+                cv2byr = (L.vmod * L.vmod) * rinv;
+            }
+        }
+        float gtanfi = ((c.g + cv2byr) * c.tanfi) * 1.f;
+        if (gtanfi < 0.f) gtanfi = 0.f;
+        L.cf5 = gtanfi;
+        L.frictx = ((L.cf5 * L.hu) * L.hvmodinv) * L.h;
+        L.fricty = ((L.cf5 * L.hv) * L.hvmodinv) * L.h;
+        if (c.xi != 0.f) {
+            float vm = vx * vx + vy * vy;
+            vm = (vm > 0.f) ? sqrtf(vm) : 0.f;
+            L.vmod = vm;
+            if (c.xi > 0.f) {
+                L.frictx = L.frictx + ((c.g * L.vmod) * vx) / c.xi;
+                L.fricty = L.fricty + ((c.g * L.vmod) * vy) / c.xi;
+            } else {
+                float constMu = -((25.f * c.xi) / 4.f);
+                L.frictx = L.frictx + ((constMu * L.vmod) * vx) / (hfrict * hfrict);
+                L.fricty = L.fricty + ((constMu * L.vmod) * vy) / (hfrict * hfrict);
+            }
+        }
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+    }
+}
+
+// Reversal filter of basal_friction_Ext_SW, SPH_SW_2019.f90:9829-9895.
+__device__ __forceinline__ void reversal_filter(const Rheo& c, float dt, float vx, float vy, float acc0, float acc1,
+                                                ExtLocal& L) {
+    const bool frictional = (c.nfric >= 5 && c.nfric <= 7);
+    float dc0 = -(L.frictx * L.hinv), dc1 = -(L.fricty * L.hinv);
+    if (L.vmod > 1.e-5f) {
+        float vs0 = vx + dt * (acc0 + dc0), vs1 = vy + dt * (acc1 + dc1);
+        float vdot = vs0 * vx + vs1 * vy;
+        if (vdot < 0.f) {
+            float vt0 = vx / L.vmod, vt1 = vy / L.vmod;
+            float accT = acc0 * vt0 + acc1 * vt1;
+            float decT = dc0 * vt0 + dc1 * vt1;
+            if (accT * decT < 0.f) {
+                dc0 = -vx / dt - acc0;
+                dc1 = -vy / dt - acc1;
+                L.frictx = -dc0 * L.h;
+                L.fricty = -dc1 * L.h;
+            }
+        }
+    } else {
+        float accT = sqrtf(acc0 * acc0 + acc1 * acc1);
+        if (accT > 1.e-5f) {
+            float ctf = frictional ? L.cf5 : L.totfrict;
+            L.frictx = (ctf * acc0) / accT;
+            L.fricty = (ctf * acc1) / accT;
+            float fricT = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+            if (accT <= fricT) { L.frictx = acc0; L.fricty = acc1; }
+        } else {
+            L.frictx = 0.f; L.fricty = 0.f;
+        }
+        L.frictx = L.frictx * L.h;
+        L.fricty = L.fricty * L.h;
+    }
+}
+
+// External acceleration of one particle in one RK stage: ExtForces_SW(0)
+// particle loop, SPH_SW_2019.f90:8532-8716 (gravity, basal friction with the
+// reversal filter, Hungr erosion momentum :8664-8697).
+__device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float dt, float xx, float yy, float vx,
+                                          float vy, float hdepth, float in0, float in1, float& ex0, float& ex1) {
+    ExtLocal L;
+    ext_locals(c, hdepth, vx, vy, L);
+    grav_and_friction(c, d, xx, yy, vx, vy, L);
+    ex0 = 0.f + L.gravx;
+    ex1 = 0.f + L.gravy;
+    reversal_filter(c, dt, vx, vy, ex0 + in0, ex1 + in1, L);
+    ex0 = ex0 - L.frictx / L.h;
+    ex1 = ex1 - L.fricty / L.h;
+    if (c.erosion) {
+        float er = (c.keros * L.h) * L.vmod;
+        ex0 = ex0 - ((er * vx) * L.hinv) * c.slip;
+        ex1 = ex1 - ((er * vy) * L.hinv) * c.slip;
+    }
+}
+
+// Hungr erosion rate after the RK update (ExtForces_SW(1), :8717-8760):
+// E = C22 * h * vmod with the ExtForces locals after basal friction.
+__device__ __forceinline__ float erosion_rate_final(const Rheo& c, const DemView& d, float xx, float yy, float vx,
+                                                    float vy, float hdepth) {
+    ExtLocal L;
+    ext_locals(c, hdepth, vx, vy, L);
+    grav_and_friction(c, d, xx, yy, vx, vy, L);
+    return (c.keros * L.h) * L.vmod;
+}
+
+__device__ __forceinline__ bool out_of_box(const DemView& d, float xx, float yy) {
+    float a = (xx - d.xmin) * (xx - d.xmax);
+    float b = (yy - d.ymin) * (yy - d.ymax);
+    return (a > 0.f) || (b > 0.f);
+}
+
+}  // namespace gfsph

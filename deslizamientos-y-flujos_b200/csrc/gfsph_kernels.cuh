@@ -1,0 +1,643 @@
+// Kernels of one SPH time step (Geoflow-SPH RK45, SPH_MAIN_2019.f90:746-1005)
+// on sm_100a.  Particles live in HBM as structure-of-arrays, re-sorted by cell
+// every step (counting sort); the neighbour table is built once per step and
+// reused by the density, force and XSPH passes, as the reference reuses its
+// pair list (w and dW frozen at the start of the step).
+#pragma once
+#include "gfsph_device.cuh"
+
+namespace gfsph {
+
+constexpr int kScanTile = 2048;  // cells per scan tile (256 threads x 8)
+constexpr int kScanThreads = 256;
+
+// error bits in StepScalars::err
+constexpr int kErrCells = 1;
+constexpr int kErrNbr = 2;
+constexpr int kErrNonFinite = 4;
+constexpr int kErrEmpty = 8;
+
+// Device-resident scalars of the step (one per handle).
+struct StepScalars {
+    double time;      // time_sph
+    double t_end;
+    float dt;         // dt_sph
+    int skip;         // this step does nothing (time >= t_end or an error)
+    int err;          // sticky error bits
+    int steps_done;
+    unsigned int xmin_o, xmax_o, ymin_o, ymax_o, hmax_o, dtmin_o;  // reductions (ordered uint)
+    int bad;          // non-finite state seen by k_bounds
+    float gx0, gy0, gd;  // cell grid origin and cell size
+    int ndx, ndy, ncells, ncells_prev;
+    int nactive, nout;
+    int need_cells, need_nbr;
+    int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
+    int advance;      // 1 inside gfsph_step, 0 for search-only passes
+};
+
+// Particle state, structure of arrays, one buffer set per ordering.
+struct PState {
+    float2* pos;
+    float2* vel;
+    float* rho;
+    float* mass;
+    float* hsml;
+    int* flag;
+    int* id;
+};
+
+__device__ __forceinline__ bool step_skipped(const StepScalars* S) { return S->skip != 0; }
+
+// ---------------------------------------------------------------- prologue
+__global__ void k_prep(StepScalars* S, int advance) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    S->advance = advance;
+    S->skip = (S->err != 0) || (advance && S->time >= S->t_end);
+    S->xmin_o = 0xffffffffu; S->ymin_o = 0xffffffffu;
+    S->xmax_o = 0u; S->ymax_o = 0u; S->hmax_o = 0u;
+    S->dtmin_o = 0xffffffffu;
+    S->bad = 0;
+    S->nout = 0;
+    S->ex0 = 0x7fffffff; S->ey0 = 0x7fffffff; S->ex1 = -1; S->ey1 = -1;
+}
+
+__device__ __forceinline__ float warp_min(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Bounds of the active particles and max(hsml) (grid_find :906-919 /
+// :1150-1165) and the stability time step of Adaptive_dt_sph_SW
+// (SPH_SW_2019.f90:6537-6567): min hsml/(3 max(1e-6, sqrt(g h))) [+|v|].
+__global__ void k_bounds(const PState B, int n, Rheo c, StepScalars* S) {
+    if (step_skipped(S)) return;
+    float xmn = 3.4e38f, xmx = -3.4e38f, ymn = 3.4e38f, ymx = -3.4e38f, hmx = 0.f, dtm = 1.e10f;
+    int bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (B.flag[i]) continue;
+        float2 p = B.pos[i];
+        float hs = B.hsml[i];
+        float h = B.rho[i];
+        float2 v = B.vel[i];
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(hs) && isfinite(h) && isfinite(v.x) && isfinite(v.y))) bad = 1;
+        xmn = fminf(xmn, p.x); xmx = fmaxf(xmx, p.x);
+        ymn = fminf(ymn, p.y); ymx = fmaxf(ymx, p.y);
+        hmx = fmaxf(hmx, hs);
+        if (c.ic_adapt == 1 || c.ic_adapt == 2) {
+            float hh = (h < c.h_inf) ? c.h_inf : h;
+            float cs = sqrtf(c.g * hh);
+            float cc = (1.e-6f > cs) ? 1.e-6f : cs;
+            if (c.ic_adapt == 2) {
+                float vv = v.x * v.x + v.y * v.y;
+                vv = sqrtf(vv);
+                cc = cc + vv;
+            }
+            cc = hs / (3.f * cc);
+            dtm = fminf(dtm, cc);
+        }
+    }
+    xmn = warp_min(xmn); xmx = warp_max(xmx); ymn = warp_min(ymn); ymx = warp_max(ymx);
+    hmx = warp_max(hmx); dtm = warp_min(dtm);
+    bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&S->xmin_o, f2o(xmn)); atomicMax(&S->xmax_o, f2o(xmx));
+        atomicMin(&S->ymin_o, f2o(ymn)); atomicMax(&S->ymax_o, f2o(ymx));
+        atomicMax(&S->hmax_o, f2o(hmx)); atomicMin(&S->dtmin_o, f2o(dtm));
+        if (bad) atomicOr(&S->bad, 1);
+    }
+}
+
+// dt update (Adaptive_dt_sph_SW :6658-6662) and the cell grid of
+// grid_find_NEW_tools (:1150-1165): cell = 2*max(hsml), ndivx = length/cell+1,
+// origin shifted by half the slack and 0.1% of the length.
+__global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (S->skip) return;
+    if (S->bad) { S->err |= kErrNonFinite; S->skip = 1; return; }
+    float xmn = o2f(S->xmin_o), xmx = o2f(S->xmax_o), ymn = o2f(S->ymin_o), ymx = o2f(S->ymax_o);
+    float hmx = o2f(S->hmax_o);
+    if (S->xmin_o == 0xffffffffu || !(hmx > 0.f)) { S->err |= kErrEmpty; S->skip = 1; return; }
+    if (S->advance) {
+        float dtmin = (c.ic_adapt == 1 || c.ic_adapt == 2) ? o2f(S->dtmin_o) : 1.e10f;
+        float dt = S->dt;
+        if (dtmin < dt) dt = dtmin;
+        else if (c.ic_adapt != 0) dt = fminf(1.1f * dt, dtmin);
+        S->dt = dt;
+    }
+    float deltx = hmx * 2.f;
+    float lx = xmx - xmn, ly = ymx - ymn;
+    int ndx = (int)(lx / deltx + 1.f);
+    int ndy = (int)(ly / deltx + 1.f);
+    float lxn = (float)ndx * deltx, lyn = (float)ndy * deltx;
+    S->gx0 = (xmn - (lxn - lx) / 2.f) - 0.001f * lx;
+    S->gy0 = (ymn - (lyn - ly) / 2.f) - 0.001f * ly;
+    S->gd = deltx;
+    S->ndx = ndx;
+    S->ndy = ndy;
+    long long nc = (long long)ndx * (long long)ndy;
+    if (nc + 1 > (long long)cap_cells) {
+        S->err |= kErrCells;
+        S->need_cells = (nc + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(nc + 1);
+        S->skip = 1;
+        return;
+    }
+    S->ncells_prev = S->ncells;
+    S->ncells = (int)nc;
+}
+
+// Clears the cell histogram over [0, max(ncells, ncells_prev)] (+1 for the
+// scan's total slot).
+__global__ void k_clear_cells(int* count, const StepScalars* S) {
+    if (S->skip) return;
+    int m = max(S->ncells, S->ncells_prev) + 1;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) count[k] = 0;
+}
+
+// Cell key and within-cell arrival rank of each particle (counting sort
+// histogram, grid_find :938-948).  Out-of-domain particles get key -1.
+__global__ void k_hist(const PState B, int n, StepScalars* S, int* count, int2* keyrank) {
+    if (S->skip) return;
+    float gx0 = S->gx0, gy0 = S->gy0, gd = S->gd;
+    int ndx = S->ndx, ndy = S->ndy;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int2 kr = make_int2(-1, 0);
+        if (!B.flag[i]) {
+            float2 p = B.pos[i];
+            int ix = (int)((p.x - gx0) / gd + 1.f);
+            int iy = (int)((p.y - gy0) / gd + 1.f);
+            ix = min(max(ix, 1), ndx);
+            iy = min(max(iy, 1), ndy);
+            int key = (iy - 1) * ndx + (ix - 1);
+            kr.x = key;
+            kr.y = atomicAdd(&count[key], 1);
+        }
+        keyrank[i] = kr;
+    }
+}
+
+// Exclusive scan of the histogram, tile pass: each block scans kScanTile
+// cells and writes its tile total.
+__global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const StepScalars* S) {
+    if (S->skip) return;
+    int m = S->ncells + 1;
+    int base = blockIdx.x * kScanTile;
+    if (base >= m) return;
+    __shared__ int sh[kScanTile];
+    __shared__ int wsum[kScanThreads / 32];
+    for (int k = threadIdx.x; k < kScanTile; k += kScanThreads) {
+        int g = base + k;
+        sh[k] = (g < m) ? count[g] : 0;
+    }
+    __syncthreads();
+    const int per = kScanTile / kScanThreads;
+    int loc[per];
+    int s = 0;
+    for (int k = 0; k < per; k++) { loc[k] = s; s += sh[threadIdx.x * per + k]; }
+    // block-wide exclusive scan of the per-thread sums
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int w = (lane < kScanThreads / 32) ? wsum[lane] : 0;
+        int wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < kScanThreads / 32) wsum[lane] = wi - w;
+        if (lane == kScanThreads / 32 - 1) tile_sum[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    int off = wsum[wid] + incl - s;
+    for (int k = 0; k < per; k++) sh[threadIdx.x * per + k] = off + loc[k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < kScanTile; k += kScanThreads) {
+        int g = base + k;
+        if (g < m) start[g] = sh[k];
+    }
+}
+
+// Scan of the tile totals (one block of 1024 threads, up to 8192 tiles).
+__global__ void k_scan_top(int* tile_sum, const StepScalars* S) {
+    if (S->skip) return;
+    int ntiles = (S->ncells + 1 + kScanTile - 1) / kScanTile;
+    __shared__ int wsum[32];
+    const int per = 8;
+    int loc[per];
+    int s = 0;
+    for (int k = 0; k < per; k++) {
+        int g = threadIdx.x * per + k;
+        int v = (g < ntiles) ? tile_sum[g] : 0;
+        loc[k] = s;
+        s += v;
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int w = wsum[lane];
+        int wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        wsum[lane] = wi - w;
+    }
+    __syncthreads();
+    int off = wsum[wid] + incl - s;
+    for (int k = 0; k < per; k++) {
+        int g = threadIdx.x * per + k;
+        if (g < ntiles) tile_sum[g] = off + loc[k];
+    }
+}
+
+__global__ void k_scan_add(int* start, const int* tile_sum, StepScalars* S) {
+    if (S->skip) return;
+    int m = S->ncells + 1;
+    int base = blockIdx.x * kScanTile;
+    if (base >= m) return;
+    int add = tile_sum[blockIdx.x];
+    for (int k = threadIdx.x; k < kScanTile; k += blockDim.x) {
+        int g = base + k;
+        if (g < m) start[g] += add;
+    }
+}
+
+// Scatter (grid_find :952-958): slot = start[cell] + rank; out-of-domain
+// particles go behind the active ones.
+__global__ void k_scatter(const int2* keyrank, int n, const int* start, StepScalars* S, int* perm) {
+    if (S->skip) return;
+    int nact = start[S->ncells];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int2 kr = keyrank[i];
+        int slot = (kr.x >= 0) ? start[kr.x] + kr.y : nact + atomicAdd(&S->nout, 1);
+        perm[slot] = i;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->nactive = nact;
+}
+
+// Orders each cell's particles by original index, so the within-cell order
+// (hence every neighbour-sum order) is independent of atomic arrival order.
+__global__ void k_cell_sort(int* perm, const int* id_old, const int* start, const StepScalars* S) {
+    if (S->skip) return;
+    int nc = S->ncells;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        int a = start[c], b = start[c + 1];
+        for (int k = a + 1; k < b; k++) {
+            int pk = perm[k];
+            int key = id_old[pk];
+            int m = k - 1;
+            while (m >= a && id_old[perm[m]] > key) { perm[m + 1] = perm[m]; m--; }
+            perm[m + 1] = pk;
+        }
+    }
+}
+
+// Gathers the state into the new (cell-sorted) order.
+__global__ void k_reorder(const PState B, int n, const int* perm, const int2* keyrank, PState A, int* cellA,
+                          const StepScalars* S) {
+    if (S->skip) return;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        int o = perm[s];
+        A.pos[s] = B.pos[o];
+        A.vel[s] = B.vel[o];
+        A.rho[s] = B.rho[o];
+        A.mass[s] = B.mass[o];
+        A.hsml[s] = B.hsml[o];
+        A.flag[s] = B.flag[o];
+        A.id[s] = B.id[o];
+        cellA[s] = keyrank[o].x;
+    }
+}
+
+// Neighbour search and summation density, fused: for every active particle
+// scan the 3x3 cells around its cell, keep j when r < 2*(hi+hj)/2 (the pair
+// set of grid_find, :987-1060), append j to the neighbour table (k-major,
+// nbr[k*n + i]) and accumulate m_j W_ij in FP64 (sum_density_Tools
+// :1796-1836, h_i = W(0,h_i) m_i + sum_j m_j W_ij).  Also stores the
+// per-particle pressure term of IntForces_SW: p/h^2 (pa_sph 2) or p (pa_sph 1)
+// with h clamped to h_inf (:6769, :6797).
+__global__ void __launch_bounds__(128) k_density(PState A, const int* cellA, const int* start, StepScalars* S,
+                                                  Rheo c, int n, int kcap, int* nbr, int* ncount, float* pterm) {
+    if (S->skip) return;
+    const int nact = S->nactive;
+    const int ndx = S->ndx, ndy = S->ndy;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
+        float2 xi = A.pos[i];
+        float hi = A.hsml[i];
+        int cell = cellA[i];
+        int cx = cell % ndx, cy = cell / ndx;
+        double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * A.mass[i]);
+        int cnt = 0;
+        for (int jy = max(cy - 1, 0); jy <= min(cy + 1, ndy - 1); jy++) {
+            int row = jy * ndx;
+            int c0 = row + max(cx - 1, 0), c1 = row + min(cx + 1, ndx - 1);
+            int ja = start[c0], jb = start[c1 + 1];
+            for (int j = ja; j < jb; j++) {
+                if (j == i) continue;
+                PairGeom g;
+                if (pair_test(xi, A.pos[j], hi, A.hsml[j], g)) {
+                    if (cnt < kcap) nbr[(size_t)cnt * n + i] = j;
+                    cnt++;
+                    float w = sph_kernel_w(c.skf, g.r, g.mh);
+                    acc += (double)(A.mass[j] * w);
+                }
+            }
+        }
+        ncount[i] = cnt;
+        if (cnt > kcap) {  // table too small: stop this step before any state is written
+            atomicOr(&S->err, kErrNbr);
+            atomicMax(&S->need_nbr, cnt);
+            atomicExch(&S->skip, 1);
+        }
+        float h = (float)acc;
+        A.rho[i] = h;
+        float hc = (h < c.h_inf) ? c.h_inf : h;
+        float p = (c.cgra05 * hc) * hc;
+        pterm[i] = (c.pa_sph == 1) ? p : p / (hc * hc);
+    }
+}
+
+// Internal acceleration of IntForces_SW (SPH_SW_2019.f90:6905-6920) for
+// particle i, gathered over its neighbour table in FP64.
+__device__ __forceinline__ void internal_force(const PState& A, const float* pterm, const Rheo& c, int i, int n,
+                                               int cnt, const int* nbr, float& in0, float& in1) {
+    float2 xi = A.pos[i];
+    float hi = A.hsml[i];
+    float pi_ = pterm[i];
+    float rhoi = A.rho[i];
+    rhoi = (rhoi < c.h_inf) ? c.h_inf : rhoi;
+    double a0 = 0.0, a1 = 0.0;
+    for (int k = 0; k < cnt; k++) {
+        int j = nbr[(size_t)k * n + i];
+        PairGeom g;
+        pair_test(xi, A.pos[j], hi, A.hsml[j], g);
+        float w, d0, d1;
+        sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+        float mj = A.mass[j];
+        float pj = pterm[j];
+        float h0, h1;
+        if (c.pa_sph == 1) {
+            float rhoj = A.rho[j];
+            rhoj = (rhoj < c.h_inf) ? c.h_inf : rhoj;
+            float rij = 1.f / (rhoi * rhoj);
+            h0 = (-(pi_ + pj) * d0) * rij;
+            h1 = (-(pi_ + pj) * d1) * rij;
+        } else {
+            h0 = -(pi_ + pj) * d0;
+            h1 = -(pi_ + pj) * d1;
+        }
+        a0 += (double)(mj * h0);
+        a1 += (double)(mj * h1);
+    }
+    in0 = (float)a0;
+    in1 = (float)a1;
+}
+
+// The RK45 body for each active particle, entirely in registers: internal
+// acceleration (stage-invariant, see below), four stages of
+// x = x0 + c_i dt v, v = v0 + c_i dt (ex + in) with ExtForces_SW(0) at each
+// stage (SPH_MAIN_2019.f90:808-906), the final update (:908-922), the
+// out-of-domain freeze (Check_Out_Domain), Hungr erosion of mass and the DEM
+// scatter of ExtForces_SW(1) (:8717-8760), and h_upgrade (:2925-2931).
+//
+// Why the internal force is computed once: with summation density the stage
+// density depends only on masses, hsml and the frozen W_ij, none of which
+// change inside the step, so IntForces_SW returns the same value in all four
+// stages.  (A particle that leaves the DEM box mid-step is frozen; the
+// reference then keeps scattering its stale pressure into its neighbours for
+// the remaining stages, which is not reproduced.)
+__global__ void __launch_bounds__(128) k_force_rk(PState A, const float* pterm, const int* nbr, const int* ncount,
+                                                   StepScalars* S, Rheo c, DemView dem, int n, PState B,
+                                                   float2* velfin, double2* auxv, int forces_only,
+                                                   float2* indv_out) {
+    if (S->skip) return;
+    const int nact = S->nactive;
+    const float dt = S->dt;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (i >= nact) {  // carried particles (out of the domain at step start)
+            if (!forces_only) {
+                B.pos[i] = A.pos[i]; B.vel[i] = A.vel[i]; velfin[i] = A.vel[i];
+                B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
+                B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
+            }
+            continue;
+        }
+        int cnt = min(ncount[i], 0x7fffffff);
+        float in0, in1;
+        internal_force(A, pterm, c, i, n, cnt, nbr, in0, in1);
+        if (forces_only) { indv_out[i] = make_float2(in0, in1); continue; }
+
+        const float h = A.rho[i];
+        const float hc = (h < c.h_inf) ? c.h_inf : h;  // IntForces_SW clamp, seen by ExtForces_SW(0)
+        const float2 x0 = A.pos[i], v0 = A.vel[i];
+        float xx = x0.x, xy = x0.y, vx = v0.x, vy = v0.y;
+        float ex0 = 0.f, ex1 = 0.f;
+        float Dx0 = 0.f, Dx1 = 0.f, Dv0 = 0.f, Dv1 = 0.f;
+        bool out = false;
+        const float f1[4] = {0.f, 0.5f, 0.5f, 1.f};
+        const float f2[4] = {1.f, 2.f, 2.f, 1.f};
+#pragma unroll 1
+        for (int s = 0; s < 4; s++) {
+            float fdt = f1[s] * dt;
+            xx = x0.x + fdt * vx;
+            xy = x0.y + fdt * vy;
+            vx = v0.x + fdt * (ex0 + in0);
+            vy = v0.y + fdt * (ex1 + in1);
+            if (out_of_box(dem, xx, xy)) { out = true; break; }
+            ext_accel(c, dem, dt, xx, xy, vx, vy, hc, in0, in1, ex0, ex1);
+            Dv0 = Dv0 + f2[s] * (ex0 + in0);
+            Dv1 = Dv1 + f2[s] * (ex1 + in1);
+            Dx0 = Dx0 + f2[s] * vx;
+            Dx1 = Dx1 + f2[s] * vy;
+        }
+        float m = A.mass[i];
+        float hs = A.hsml[i];
+        if (!out) {
+            float dt6 = dt / 6.f;
+            xx = x0.x + dt6 * Dx0;
+            xy = x0.y + dt6 * Dx1;
+            vx = v0.x + dt6 * Dv0;
+            vy = v0.y + dt6 * Dv1;
+            out = out_of_box(dem, xx, xy);
+        }
+        if (!out) {
+            if (c.erosion) {
+                float er = erosion_rate_final(c, dem, xx, xy, vx, vy, h);
+                float base = dt * er;
+                int ipx = (int)((xx - dem.xmin) / dem.dx + 1.f);
+                int ipy = (int)((xy - dem.ymin) / dem.dy + 1.f);
+                int ix0 = max(1, ipx - 1), iy0 = max(1, ipy - 1);
+                int ix1 = min(dem.nx, ipx + 2), iy1 = min(dem.ny, ipy + 2);
+                for (int ix = ix0; ix <= ix1; ix++)
+                    for (int iy = iy0; iy <= iy1; iy++) {
+                        int ip = (iy - 1) * dem.nx + (ix - 1);
+                        float ddx = xx - (dem.xmin + (float)(ix - 1) * dem.dx);
+                        ddx = ddx * ddx;
+                        float ddy = xy - (dem.ymin + (float)(iy - 1) * dem.dy);
+                        ddy = ddy * ddy;
+                        float dist = sqrtf(ddx + ddy);
+                        dist = (1.e-6f > dist) ? 1.e-6f : dist;
+                        atomicAdd(&auxv[ip].x, (double)(base / dist));
+                        atomicAdd(&auxv[ip].y, (double)(1.f / dist));
+                    }
+                atomicMin(&S->ex0, ix0); atomicMax(&S->ex1, ix1);
+                atomicMin(&S->ey0, iy0); atomicMax(&S->ey1, iy1);
+                m = m + ((dt * er) * m) / h;
+            }
+            if (c.sle == 1) hs = 2.f * sqrtf(m / h);
+        }
+        B.pos[i] = make_float2(xx, xy);
+        velfin[i] = make_float2(vx, vy);
+        B.vel[i] = make_float2(vx, vy);
+        B.rho[i] = h;
+        B.mass[i] = m;
+        B.hsml[i] = hs;
+        B.flag[i] = out ? 1 : 0;
+        B.id[i] = A.id[i];
+    }
+}
+
+// av_vel (SPH_MAIN_2019.f90:3042-3099) with the start-of-step W_ij, then
+// v += 0.3*av for particles still inside the domain (:987-993).
+__global__ void __launch_bounds__(128) k_xsph(PState A, const int* nbr, const int* ncount, StepScalars* S, Rheo c,
+                                               int n, PState B, const float2* velfin) {
+    if (S->skip || !c.av_vel) return;
+    const int nact = S->nactive;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
+        if (B.flag[i]) continue;
+        float2 xi = A.pos[i];
+        float hi = A.hsml[i];
+        float2 vi = velfin[i];
+        float rhoi = A.rho[i];
+        int cnt = ncount[i];
+        double a0 = 0.0, a1 = 0.0;
+        for (int k = 0; k < cnt; k++) {
+            int j = nbr[(size_t)k * n + i];
+            PairGeom g;
+            pair_test(xi, A.pos[j], hi, A.hsml[j], g);
+            float w = sph_kernel_w(c.skf, g.r, g.mh);
+            float2 vj = velfin[j];
+            float mj = B.mass[j];
+            float den = rhoi + A.rho[j];
+            float t0 = (((2.f * mj) * (vi.x - vj.x)) / den) * w;
+            float t1 = (((2.f * mj) * (vi.y - vj.y)) / den) * w;
+            a0 -= (double)t0;
+            a1 -= (double)t1;
+        }
+        float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
+        B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
+    }
+}
+
+// DEM update of ExtForces_SW(1) (SPH_SW_2019.f90:8795-8807) over the node box
+// touched this step; resets the scatter accumulators.
+__global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail, int nx, StepScalars* S) {
+    if (S->skip) return;
+    int x0 = S->ex0, x1 = S->ex1, y0 = S->ey0, y1 = S->ey1;
+    if (x1 < x0 || y1 < y0) return;
+    int w = x1 - x0 + 1, hgt = y1 - y0 + 1;
+    long long tot = (long long)w * hgt;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
+        int ix = x0 + (int)(k % w), iy = y0 + (int)(k / w);
+        int ip = (iy - 1) * nx + (ix - 1);
+        double2 a = auxv[ip];
+        if ((float)a.y > 1.e-6f) {
+            float xnum = (float)(a.x / a.y);
+            float av = avail[ip];
+            if (xnum > av) xnum = av;
+            if (av > 0.f) {
+                eroded[ip] = eroded[ip] + xnum;
+                z[ip] = z[ip] - xnum;
+                avail[ip] = av - xnum;
+            }
+        }
+        auxv[ip] = make_double2(0.0, 0.0);
+    }
+}
+
+__global__ void k_step_end(StepScalars* S) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (S->skip || !S->advance) return;
+    S->time += (double)S->dt;
+    S->steps_done += 1;
+}
+
+// ---------------------------------------------------------------- outputs
+
+// Depth raster: IDW of h onto the 4x4 DEM nodes around each particle
+// (SPH_SW_2019.f90:14310-14400, auxv(1)/auxv(5)).
+__global__ void k_raster_idw(const PState B, int n, DemView dem, double2* acc) {
+    float distg = sqrtf(dem.dx * dem.dx + dem.dy * dem.dy);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (B.flag[i]) continue;
+        float2 p = B.pos[i];
+        float h = B.rho[i];
+        int ipx = (int)((p.x - dem.xmin) / dem.dx + 1.f);
+        int ipy = (int)((p.y - dem.ymin) / dem.dy + 1.f);
+        int ix0 = max(1, ipx - 1), iy0 = max(1, ipy - 1), ix1 = min(dem.nx, ipx + 2), iy1 = min(dem.ny, ipy + 2);
+        for (int ix = ix0; ix <= ix1; ix++)
+            for (int iy = iy0; iy <= iy1; iy++) {
+                int ip = (iy - 1) * dem.nx + (ix - 1);
+                float ddx = p.x - (dem.xmin + (float)(ix - 1) * dem.dx);
+                ddx = ddx * ddx;
+                float ddy = p.y - (dem.ymin + (float)(iy - 1) * dem.dy);
+                ddy = ddy * ddy;
+                float dist = sqrtf(ddx + ddy);
+                dist = (1.e-6f > dist) ? 1.e-6f : dist;
+                dist = dist / distg;
+                atomicAdd(&acc[ip].x, (double)(h / dist));
+                atomicAdd(&acc[ip].y, (double)(1.f / dist));
+            }
+    }
+}
+
+__global__ void k_raster_idw_finish(const double2* acc, float* out, int np) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+        double2 a = acc[k];
+        out[k] = ((float)a.y >= 1.e-6f) ? (float)(a.x / a.y) : (float)a.x;
+    }
+}
+
+// Per-node hazard statistics of Get_MC_pixel_Vars_SW (SPH_SW_2019.f90:20739-20812):
+// each particle adds h and |v| to the 4 nodes of its DEM cell.
+__global__ void k_hazard(const PState B, int n, DemView dem, double* sum_h, double* sum_v, unsigned int* max_h,
+                         unsigned int* max_v, int* cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (B.flag[i]) continue;
+        float2 p = B.pos[i];
+        int ipx = (int)((p.x - dem.xmin) / dem.dx + 1.f);
+        int ipy = (int)((p.y - dem.ymin) / dem.dy + 1.f);
+        ipx = min(max(ipx, 1), dem.nx - 1);
+        ipy = min(max(ipy, 1), dem.ny - 1);
+        int ip = (ipy - 1) * dem.nx + (ipx - 1);
+        int nodes[4] = {ip, ip + 1, ip + 1 + dem.nx, ip + dem.nx};
+        float hh = B.rho[i];
+        float2 v = B.vel[i];
+        float vv = sqrtf(v.x * v.x + v.y * v.y);
+        for (int k = 0; k < 4; k++) {
+            int q = nodes[k];
+            atomicAdd(&cnt[q], 1);
+            atomicAdd(&sum_h[q], (double)hh);
+            atomicAdd(&sum_v[q], (double)vv);
+            atomicMax(&max_h[q], f2o(hh));
+            atomicMax(&max_v[q], f2o(vv));
+        }
+    }
+}
+
+}  // namespace gfsph

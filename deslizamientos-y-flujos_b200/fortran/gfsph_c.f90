@@ -1,0 +1,150 @@
+! gfsph_c.f90 — ISO_C_BINDING interface of libgfsph (include/gfsph.h) for the
+! Geoflow-SPH Fortran host.  Source only: the image that builds the library has
+! no Fortran compiler.  A maintainer adds this module to the reference's build
+! and, in Driver_Flow (SPH_FEM_Driver_2019.f90:1580-1697), replaces the calls
+! to adaptive_dt_sph and time_integration_sph with one gfsph_step per output
+! interval, uploading x, vx, rho, mass, hsml once after Init_sph and
+! downloading them before each Out_PLOT / Out_Save.
+module gfsph_c
+  use, intrinsic :: iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: GFSPH_NCONST = 110, GFSPH_NTOPO = 16
+  integer(c_int), parameter :: GFSPH_OK = 0, GFSPH_T_END_REACHED = 1
+  integer(c_int), parameter :: GFSPH_RASTER_DEPTH_IDW = 0, GFSPH_RASTER_MAX_DEPTH = 1, &
+                               GFSPH_RASTER_MAX_VEL = 2, GFSPH_RASTER_SUM_DEPTH = 3, &
+                               GFSPH_RASTER_SUM_VEL = 4, GFSPH_RASTER_COUNT = 5, &
+                               GFSPH_RASTER_Z = 6, GFSPH_RASTER_ERODED = 7, GFSPH_RASTER_AVAILABLE = 8
+
+  type, bind(c) :: gfsph_params
+     real(c_float)  :: cst(GFSPH_NCONST)        ! const(1..110)
+     integer(c_int) :: pa_sph, nnps, sle, skf
+     integer(c_int) :: summation_density, average_velocity, nor_density
+     integer(c_int) :: ic_adapt
+     real(c_float)  :: h_inf, dt
+     integer(c_int) :: dem_deriv, max_neighbours
+     integer(c_int) :: reserved(8)
+  end type gfsph_params
+
+  type, bind(c) :: gfsph_dem
+     integer(c_int) :: nx, ny                  ! npoigx, npoigy
+     real(c_float)  :: xmin, ymin, dx, dy      ! xming, yming, deltxg, deltyg
+     type(c_ptr)    :: topol                   ! c_loc(topol) of topol(ntopo, npoig)
+     integer(c_int) :: ntopo
+     type(c_ptr)    :: z
+  end type gfsph_dem
+
+  interface
+     integer(c_int) function gfsph_create(params, dem, handle) bind(c, name="gfsph_create")
+       import :: c_int, c_ptr, gfsph_params, gfsph_dem
+       type(gfsph_params), intent(in) :: params
+       type(gfsph_dem), intent(in) :: dem
+       type(c_ptr), intent(out) :: handle
+     end function
+     integer(c_int) function gfsph_destroy(handle) bind(c, name="gfsph_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+     end function
+     integer(c_int) function gfsph_upload(handle, n, x, vx, rho, mass, hsml, itype, out_flag) &
+          bind(c, name="gfsph_upload")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: handle
+       integer(c_int), value :: n
+       real(c_float), intent(in) :: x(2, n), vx(2, n), rho(n), mass(n), hsml(n)
+       integer(c_int), intent(in) :: itype(n), out_flag(n)
+     end function
+     integer(c_int) function gfsph_download(handle, x, vx, rho, mass, hsml, out_flag) &
+          bind(c, name="gfsph_download")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: handle
+       real(c_float), intent(out) :: x(2, *), vx(2, *), rho(*), mass(*), hsml(*)
+       integer(c_int), intent(out) :: out_flag(*)
+     end function
+     integer(c_int) function gfsph_step(handle, nsteps, t_end, t_out, steps_done) bind(c, name="gfsph_step")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: handle
+       integer(c_int), value :: nsteps
+       real(c_double), value :: t_end
+       real(c_double), intent(out) :: t_out
+       integer(c_int), intent(out) :: steps_done
+     end function
+     integer(c_int) function gfsph_get_time(handle, t, dt) bind(c, name="gfsph_get_time")
+       import :: c_int, c_ptr, c_double, c_float
+       type(c_ptr), value :: handle
+       real(c_double), intent(out) :: t
+       real(c_float), intent(out) :: dt
+     end function
+     integer(c_int) function gfsph_set_time(handle, t, dt) bind(c, name="gfsph_set_time")
+       import :: c_int, c_ptr, c_double, c_float
+       type(c_ptr), value :: handle
+       real(c_double), value :: t
+       real(c_float), value :: dt
+     end function
+     integer(c_int) function gfsph_density(handle, rho) bind(c, name="gfsph_density")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: handle
+       real(c_float), intent(out) :: rho(*)
+     end function
+     integer(c_int) function gfsph_neighbours(handle, cap, offsets, idx) bind(c, name="gfsph_neighbours")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+       integer(c_int), value :: cap
+       integer(c_int), intent(out) :: offsets(*), idx(*)
+     end function
+     integer(c_int) function gfsph_internal_forces(handle, indvxdt) bind(c, name="gfsph_internal_forces")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: handle
+       real(c_float), intent(out) :: indvxdt(2, *)
+     end function
+     integer(c_int) function gfsph_raster(handle, kind, out) bind(c, name="gfsph_raster")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: handle
+       integer(c_int), value :: kind
+       real(c_float), intent(out) :: out(*)
+     end function
+     integer(c_int) function gfsph_hazard_sample(handle) bind(c, name="gfsph_hazard_sample")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+     end function
+     integer(c_int) function gfsph_hazard_reset(handle) bind(c, name="gfsph_hazard_reset")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+     end function
+     integer(c_int) function gfsph_profile(handle, enable) bind(c, name="gfsph_profile")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+       integer(c_int), value :: enable
+     end function
+     integer(c_int) function gfsph_profile_read(handle, kernel, total_ms, launches) bind(c, name="gfsph_profile_read")
+       import :: c_int, c_ptr, c_double, c_long_long
+       type(c_ptr), value :: handle
+       integer(c_int), value :: kernel
+       real(c_double), intent(out) :: total_ms
+       integer(c_long_long), intent(out) :: launches
+     end function
+     integer(c_int) function gfsph_num_kernels() bind(c, name="gfsph_num_kernels")
+       import :: c_int
+     end function
+     type(c_ptr) function gfsph_kernel_name(kernel) bind(c, name="gfsph_kernel_name")
+       import :: c_int, c_ptr
+       integer(c_int), value :: kernel
+     end function
+     integer(c_long_long) function gfsph_launch_count(handle) bind(c, name="gfsph_launch_count")
+       import :: c_long_long, c_ptr
+       type(c_ptr), value :: handle
+     end function
+     integer(c_int) function gfsph_dem_topol(mode, nx, ny, dx, dy, topol) bind(c, name="gfsph_dem_topol")
+       import :: c_int, c_float
+       integer(c_int), value :: mode, nx, ny
+       real(c_float), value :: dx, dy
+       real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
+     end function
+     type(c_ptr) function gfsph_strerror(status) bind(c, name="gfsph_strerror")
+       import :: c_int, c_ptr
+       integer(c_int), value :: status
+     end function
+     integer(c_int) function gfsph_version() bind(c, name="gfsph_version")
+       import :: c_int
+     end function
+  end interface
+end module gfsph_c

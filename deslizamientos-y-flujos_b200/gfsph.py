@@ -1,0 +1,269 @@
+"""Python binding of the gfsph C ABI (include/gfsph.h) over ctypes.
+
+This is the host-side mirror of the reference's step interface for tests and
+benchmarks: the Fortran host of the reference would bind the same symbols
+through ISO_C_BINDING (fortran/gfsph_c.f90).  Arrays follow the Fortran
+layout: particle vectors are (n, 2) float32 in C order, which is the (2, n)
+column-major layout of the reference.
+
+There is no CPU fallback: without libgfsph.so, or without a CUDA device, the
+calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgfsph.so")
+
+NCONST = 110
+NTOPO = 16
+
+OK = 0
+T_END_REACHED = 1
+
+RASTER_DEPTH_IDW = 0
+RASTER_MAX_DEPTH = 1
+RASTER_MAX_VEL = 2
+RASTER_SUM_DEPTH = 3
+RASTER_SUM_VEL = 4
+RASTER_COUNT = 5
+RASTER_Z = 6
+RASTER_ERODED = 7
+RASTER_AVAILABLE = 8
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("cst", C.c_float * NCONST),
+        ("pa_sph", C.c_int), ("nnps", C.c_int), ("sle", C.c_int), ("skf", C.c_int),
+        ("summation_density", C.c_int), ("average_velocity", C.c_int), ("nor_density", C.c_int),
+        ("ic_adapt", C.c_int), ("h_inf", C.c_float), ("dt", C.c_float), ("dem_deriv", C.c_int),
+        ("max_neighbours", C.c_int), ("reserved", C.c_int * 8),
+    ]
+
+
+class Dem(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("xmin", C.c_float), ("ymin", C.c_float),
+        ("dx", C.c_float), ("dy", C.c_float), ("topol", C.POINTER(C.c_float)), ("ntopo", C.c_int),
+        ("z", C.POINTER(C.c_float)),
+    ]
+
+
+_FP = C.POINTER(C.c_float)
+_IP = C.POINTER(C.c_int)
+_lib = None
+
+# every symbol include/gfsph.h declares, with its ctypes signature
+SIGNATURES = {
+    "gfsph_create": (C.c_int, [C.POINTER(Params), C.POINTER(Dem), C.POINTER(C.c_void_p)]),
+    "gfsph_destroy": (C.c_int, [C.c_void_p]),
+    "gfsph_upload": (C.c_int, [C.c_void_p, C.c_int, _FP, _FP, _FP, _FP, _FP, _IP, _IP]),
+    "gfsph_download": (C.c_int, [C.c_void_p, _FP, _FP, _FP, _FP, _FP, _IP]),
+    "gfsph_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_double), _IP]),
+    "gfsph_get_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), _FP]),
+    "gfsph_set_time": (C.c_int, [C.c_void_p, C.c_double, C.c_float]),
+    "gfsph_density": (C.c_int, [C.c_void_p, _FP]),
+    "gfsph_neighbours": (C.c_int, [C.c_void_p, C.c_int, _IP, _IP]),
+    "gfsph_internal_forces": (C.c_int, [C.c_void_p, _FP]),
+    "gfsph_raster": (C.c_int, [C.c_void_p, C.c_int, _FP]),
+    "gfsph_hazard_sample": (C.c_int, [C.c_void_p]),
+    "gfsph_hazard_reset": (C.c_int, [C.c_void_p]),
+    "gfsph_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gfsph_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "gfsph_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    "gfsph_num_kernels": (C.c_int, []),
+    "gfsph_kernel_name": (C.c_char_p, [C.c_int]),
+    "gfsph_launch_count": (C.c_longlong, [C.c_void_p]),
+    "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
+    "gfsph_strerror": (C.c_char_p, [C.c_int]),
+    "gfsph_version": (C.c_int, []),
+}
+
+
+class GfsphError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__(f"{what}: {status} ({strerror(status)})")
+
+
+def lib():
+    """Loads libgfsph.so (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run build.py (the CUDA library is required)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def strerror(status):
+    return lib().gfsph_strerror(status).decode()
+
+
+def _check(st, what):
+    if st < 0:
+        raise GfsphError(st, what)
+    return st
+
+
+def _fp(a):
+    return a.ctypes.data_as(_FP) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(_IP) if a is not None else None
+
+
+def make_params(const=None, *, pa_sph=2, nnps=2, sle=1, skf=1, summation_density=1, average_velocity=1,
+                nor_density=0, ic_adapt=0, h_inf=0.01, dt=0.01, dem_deriv=1, max_neighbours=0):
+    """Params from a {k: value} map of the reference's const(k) (1-based)."""
+    p = Params()
+    for k, val in (const or {}).items():
+        p.cst[k - 1] = float(val)
+    p.pa_sph, p.nnps, p.sle, p.skf = pa_sph, nnps, sle, skf
+    p.summation_density, p.average_velocity, p.nor_density = summation_density, average_velocity, nor_density
+    p.ic_adapt, p.h_inf, p.dt, p.dem_deriv, p.max_neighbours = ic_adapt, h_inf, dt, dem_deriv, max_neighbours
+    return p
+
+
+def dem_topol(z, dx, dy, mode=1):
+    """Slope/curvature rows topol(2..13) from Z with the library's host set-up."""
+    ny, nx = z.shape
+    t = np.zeros((ny * nx, NTOPO), dtype=np.float32)
+    t[:, 0] = z.reshape(-1)
+    _check(lib().gfsph_dem_topol(mode, nx, ny, dx, dy, _fp(t)), "gfsph_dem_topol")
+    return t
+
+
+class Sim:
+    """One gfsph handle: a DEM, a particle set and the step state."""
+
+    def __init__(self, params, z=None, *, xmin=0.0, ymin=0.0, dx=1.0, dy=1.0, topol=None):
+        L = lib()
+        if topol is not None:
+            topol = np.ascontiguousarray(topol, dtype=np.float32)
+            ny, nx = (z.shape if z is not None else (None, None))
+            if nx is None:
+                raise ValueError("pass z (for the grid shape) together with topol")
+        else:
+            z = np.ascontiguousarray(z, dtype=np.float32)
+            ny, nx = z.shape
+        self.nx, self.ny = nx, ny
+        self.params = params
+        self._z = np.ascontiguousarray(z, dtype=np.float32)
+        self._topol = topol
+        d = Dem()
+        d.nx, d.ny, d.xmin, d.ymin, d.dx, d.dy = nx, ny, xmin, ymin, dx, dy
+        d.topol = _fp(topol) if topol is not None else None
+        d.ntopo = topol.shape[1] if topol is not None else 0
+        d.z = _fp(self._z)
+        self.dem = d
+        h = C.c_void_p()
+        _check(L.gfsph_create(C.byref(params), C.byref(d), C.byref(h)), "gfsph_create")
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            lib().gfsph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, x, v, rho, mass, hsml, flag=None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n = x.shape[0]
+        self._up = [x, np.ascontiguousarray(v, dtype=np.float32), np.ascontiguousarray(rho, dtype=np.float32),
+                    np.ascontiguousarray(mass, dtype=np.float32), np.ascontiguousarray(hsml, dtype=np.float32),
+                    None if flag is None else np.ascontiguousarray(flag, dtype=np.int32)]
+        a = self._up
+        _check(lib().gfsph_upload(self.h, n, _fp(a[0]), _fp(a[1]), _fp(a[2]), _fp(a[3]), _fp(a[4]), None, _ip(a[5])),
+               "gfsph_upload")
+        self.n = n
+
+    def download(self, out=None):
+        n = self.n
+        if out is None:
+            out = dict(x=np.empty((n, 2), np.float32), v=np.empty((n, 2), np.float32), rho=np.empty(n, np.float32),
+                       mass=np.empty(n, np.float32), hsml=np.empty(n, np.float32), flag=np.empty(n, np.int32))
+        _check(lib().gfsph_download(self.h, _fp(out["x"]), _fp(out["v"]), _fp(out["rho"]), _fp(out["mass"]),
+                                    _fp(out["hsml"]), _ip(out["flag"])), "gfsph_download")
+        return out
+
+    def step(self, nsteps, t_end=1e300):
+        t = C.c_double()
+        done = C.c_int()
+        st = _check(lib().gfsph_step(self.h, nsteps, t_end, C.byref(t), C.byref(done)), "gfsph_step")
+        return st, t.value, done.value
+
+    def time(self):
+        t = C.c_double()
+        dt = C.c_float()
+        _check(lib().gfsph_get_time(self.h, C.byref(t), C.byref(dt)), "gfsph_get_time")
+        return t.value, dt.value
+
+    def set_time(self, t, dt):
+        _check(lib().gfsph_set_time(self.h, t, dt), "gfsph_set_time")
+
+    def density(self):
+        rho = np.empty(self.n, np.float32)
+        _check(lib().gfsph_density(self.h, _fp(rho)), "gfsph_density")
+        return rho
+
+    def internal_forces(self):
+        a = np.empty((self.n, 2), np.float32)
+        _check(lib().gfsph_internal_forces(self.h, _fp(a)), "gfsph_internal_forces")
+        return a
+
+    def neighbours(self):
+        off = np.empty(self.n + 1, np.int32)
+        st = lib().gfsph_neighbours(self.h, 0, _ip(off), None)
+        if st < 0 and st != -3:
+            _check(st, "gfsph_neighbours")
+        cap = int(off[-1])
+        idx = np.empty(max(cap, 1), np.int32)
+        _check(lib().gfsph_neighbours(self.h, cap, _ip(off), _ip(idx)), "gfsph_neighbours")
+        return off, idx[:cap]
+
+    def raster(self, kind):
+        out = np.empty((self.ny, self.nx), np.float32)
+        _check(lib().gfsph_raster(self.h, kind, _fp(out)), "gfsph_raster")
+        return out
+
+    def hazard_sample(self):
+        _check(lib().gfsph_hazard_sample(self.h), "gfsph_hazard_sample")
+
+    def hazard_reset(self):
+        _check(lib().gfsph_hazard_reset(self.h), "gfsph_hazard_reset")
+
+    def set_stream(self, stream_ptr):
+        _check(lib().gfsph_set_stream(self.h, C.c_void_p(stream_ptr)), "gfsph_set_stream")
+
+    def profile(self, on):
+        _check(lib().gfsph_profile(self.h, 1 if on else 0), "gfsph_profile")
+
+    def profile_read(self):
+        L = lib()
+        res = {}
+        for k in range(L.gfsph_num_kernels()):
+            ms = C.c_double()
+            cnt = C.c_longlong()
+            _check(L.gfsph_profile_read(self.h, k, C.byref(ms), C.byref(cnt)), "gfsph_profile_read")
+            if cnt.value:
+                res[L.gfsph_kernel_name(k).decode()] = (ms.value, cnt.value)
+        return res
+
+    def launch_count(self):
+        return int(lib().gfsph_launch_count(self.h))

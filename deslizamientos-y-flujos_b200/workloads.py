@@ -1,0 +1,180 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+No public dataset is involved: every input (DEM, release area, depth field)
+is generated here from a seed.  Particles are placed the way
+Read_Source_plus_New does it (SPH_SW_2019.f90:4999-5272): one particle per
+lattice node of spacing delt2D, volume mass = dA * h * fct_area with
+dA = dx*dy/4 and fct_area the number of the node's four lattice cells whose
+corners all carry material, smoothing length hsml = delt2D * facthsml, depth
+clamped to h_inf.
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Workload:
+    name: str
+    const: dict                  # {k: const(k)} of the reference, 1-based
+    options: dict                # pa_sph, nnps, sle, skf, ... for gfsph.make_params
+    z: np.ndarray                # (ny, nx) float32 elevations
+    dx: float
+    dy: float
+    x: np.ndarray                # (n, 2) float32
+    v: np.ndarray                # (n, 2) float32
+    rho: np.ndarray              # (n,) float32 depth
+    mass: np.ndarray             # (n,) float32 volume
+    hsml: np.ndarray             # (n,) float32
+    steps: int = 0
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self):
+        return self.x.shape[0]
+
+
+def lattice_particles(mask, depth, x0, y0, spacing, facthsml, h_inf):
+    """Particles on the nodes of a lattice (mask True) as Read_Source_plus_New builds them."""
+    ny, nx = mask.shape
+    full = mask[:-1, :-1] & mask[1:, :-1] & mask[:-1, 1:] & mask[1:, 1:]
+    fct = np.zeros(mask.shape, np.int32)
+    fct[:-1, :-1] += full
+    fct[1:, :-1] += full
+    fct[:-1, 1:] += full
+    fct[1:, 1:] += full
+    keep = mask & (fct > 0)            # nodes with no complete cell would get zero volume
+    iy, ix = np.nonzero(keep)
+    xs = (np.float32(x0) + ix.astype(np.float32) * np.float32(spacing)).astype(np.float32)
+    ys = (np.float32(y0) + iy.astype(np.float32) * np.float32(spacing)).astype(np.float32)
+    h = depth[iy, ix].astype(np.float32)
+    h = np.maximum(h, np.float32(h_inf)).astype(np.float32)
+    d_area = np.float32(spacing) * np.float32(spacing) / np.float32(4.0)
+    mass = (d_area * h * fct[iy, ix].astype(np.float32)).astype(np.float32)
+    n = xs.size
+    hsml = np.full(n, np.float32(spacing) * np.float32(facthsml), np.float32)
+    x = np.stack([xs, ys], axis=1).astype(np.float32)
+    return x, np.zeros((n, 2), np.float32), h, mass, hsml
+
+
+def diamond_square(k, hurst, rng):
+    """Fractional-Brownian surface on a (2^k+1)^2 grid by midpoint displacement."""
+    n = 2 ** k + 1
+    a = np.zeros((n, n), np.float64)
+    a[0, 0], a[0, -1], a[-1, 0], a[-1, -1] = rng.standard_normal(4)
+    step = n - 1
+    scale = 1.0
+    while step > 1:
+        half = step // 2
+        # diamond step: square centres
+        c = (a[0:-1:step, 0:-1:step] + a[step::step, 0:-1:step] + a[0:-1:step, step::step] + a[step::step, step::step]) / 4.0
+        a[half::step, half::step] = c + scale * rng.standard_normal(c.shape)
+        # square step: edge midpoints, averaging the available neighbours
+        p = np.pad(a, half, mode="constant", constant_values=np.nan)
+        for (r0, c0) in ((0, half), (half, 0)):
+            rows = np.arange(r0, n, step)
+            cols = np.arange(c0, n, step)
+            R, Cc = np.meshgrid(rows + half, cols + half, indexing="ij")
+            nb = np.stack([p[R - half, Cc], p[R + half, Cc], p[R, Cc - half], p[R, Cc + half]])
+            m = np.nanmean(nb, axis=0)
+            a[np.ix_(rows, cols)] = m + scale * rng.standard_normal(m.shape)
+        scale *= 2.0 ** (-hurst)
+        step = half
+    return a
+
+
+def smooth_field(x, y, rng, nmodes=6, lmin=30.0, lmax=100.0):
+    """Sum of seeded plane waves, normalised to zero mean and unit max."""
+    f = np.zeros_like(x, dtype=np.float64)
+    for _ in range(nmodes):
+        lam = rng.uniform(lmin, lmax)
+        th = rng.uniform(0, 2 * math.pi)
+        ph = rng.uniform(0, 2 * math.pi)
+        f += np.cos(2 * math.pi * (x * math.cos(th) + y * math.sin(th)) / lam + ph)
+    f -= f.mean()
+    m = np.abs(f).max()
+    return f / m if m > 0 else f
+
+
+def voellmy_const(mu, xi, dens=2000.0, g=9.8, erosion=None):
+    """const(k) map of a frictional (nfric 5) + Voellmy run; erosion = (C22, C48) for Hungr."""
+    c = {1: g, 2: dens, 3: xi, 5: 5, 9: mu, 10: 0.01, 15: 0.01}
+    if erosion:
+        c.update({21: 1, 22: erosion[0], 48: erosion[1]})
+    return c
+
+
+def inclined_plane(seed=1, spacing=2.0, facthsml=2.0, nx=200, ny=400, cell=5.0):
+    """Granular collapse on an analytic DEM: 30 deg plane over the first 250
+    rows then flat; paraboloid cap (10 m, radius 50 m) centred 200 m upslope
+    of the toe on a 2 m lattice with seeded +-1% depth jitter; Voellmy
+    mu = 0.2, xi = 500, density 2000, fixed dt = 0.01 s, 2000 steps."""
+    rows = np.arange(ny, dtype=np.float64)[:, None] * np.ones((1, nx))
+    z = np.where(rows < 250, (250 - rows) * cell * math.tan(math.radians(30.0)), 0.0).astype(np.float32)
+    xc, yc, r0 = nx * cell / 2.0, 250 * cell - 200.0, 50.0
+    m = int(math.ceil(r0 / spacing)) + 1
+    gx0, gy0 = xc - m * spacing, yc - m * spacing
+    ii = np.arange(2 * m + 1)
+    X, Y = np.meshgrid(gx0 + ii * spacing, gy0 + ii * spacing)
+    r2 = (X - xc) ** 2 + (Y - yc) ** 2
+    mask = r2 < r0 * r0
+    rng = np.random.default_rng(seed)
+    depth = 10.0 * (1.0 - r2 / (r0 * r0)) * (1.0 + rng.uniform(-0.01, 0.01, size=X.shape))
+    x, v, h, mass, hsml = lattice_particles(mask, depth, gx0, gy0, spacing, facthsml, 0.01)
+    return Workload(
+        name="inclined_plane_2k", const=voellmy_const(0.2, 500.0),
+        options=dict(pa_sph=2, nnps=2, sle=1, skf=1, average_velocity=1, ic_adapt=0, h_inf=0.01, dt=0.01,
+                     dem_deriv=1),
+        z=z, dx=cell, dy=cell, x=x, v=v, rho=h, mass=mass, hsml=hsml, steps=2000,
+        meta=dict(dem=f"{nx}x{ny} at {cell} m", lattice=spacing))
+
+
+def fractal_channel(n_target=200_000, dem_k=10, cell=5.0, seed=2, facthsml=2.0, mean_depth=4.0,
+                    semi_along=150.0, semi_across=80.0, erosion=(0.005, 2.0), mu=0.15, xi=400.0,
+                    relief=800.0):
+    """Seeded diamond-square fBm DEM (Hurst 0.8) of 2^dem_k nodes a side at
+    `cell` m with a carved V-channel, relief `relief` m; an elliptical release
+    (semi-axes 150 m along the channel, 80 m across) on the lattice spacing
+    that gives ~n_target particles; smooth seeded depth field of mean 4 m;
+    Voellmy mu = 0.15, xi = 400 with Hungr erosion 0.005 1/m over a 2 m
+    erodible layer; adaptive dt (ic_adapt_dt_sph = 1)."""
+    rng = np.random.default_rng(seed)
+    f = diamond_square(dem_k, 0.8, rng)[: 2 ** dem_k, : 2 ** dem_k]
+    f = (f - f.min()) / (f.max() - f.min())
+    nx = ny = 2 ** dem_k
+    L = nx * cell
+    ys = np.arange(ny)[:, None] * cell
+    xs = np.arange(nx)[None, :] * cell
+    xc = L / 2.0
+    decay = 0.3125 * L
+    base = (relief - 100.0) * np.exp(-ys / decay)
+    rough = 100.0 * f * np.exp(-ys / (2 * decay))
+    half_w = 0.04 * L
+    carve = 40.0 * np.clip(1.0 - np.abs(xs - xc) / half_w, 0.0, None)
+    z = (base + rough - carve).astype(np.float32)
+    yc = 0.137 * L
+    area = math.pi * semi_along * semi_across
+    spacing = math.sqrt(area / n_target)
+    mx = int(math.ceil(semi_across / spacing)) + 1
+    my = int(math.ceil(semi_along / spacing)) + 1
+    gx0, gy0 = xc - mx * spacing, yc - my * spacing
+    X, Y = np.meshgrid(gx0 + np.arange(2 * mx + 1) * spacing, gy0 + np.arange(2 * my + 1) * spacing)
+    mask = ((X - xc) / semi_across) ** 2 + ((Y - yc) / semi_along) ** 2 < 1.0
+    fld = smooth_field(X, Y, np.random.default_rng(seed + 1000))
+    depth = mean_depth * (1.0 + 0.25 * fld)
+    depth *= mean_depth / depth[mask].mean()
+    x, v, h, mass, hsml = lattice_particles(mask, depth, gx0, gy0, spacing, facthsml, 0.01)
+    return Workload(
+        name=f"fractal_channel_{x.shape[0] // 1000}k",
+        const=voellmy_const(mu, xi, erosion=erosion),
+        options=dict(pa_sph=2, nnps=2, sle=1, skf=1, average_velocity=1, ic_adapt=1, h_inf=0.01, dt=0.01,
+                     dem_deriv=1),
+        z=z, dx=cell, dy=cell, x=x, v=v, rho=h, mass=mass, hsml=hsml, steps=10_000,
+        meta=dict(dem=f"{nx}x{ny} at {cell} m", lattice=spacing, relief=relief))
+
+
+def make_params(w, gfsph_module, **over):
+    opts = dict(w.options)
+    opts.update(over)
+    return gfsph_module.make_params(w.const, **opts)

@@ -1,0 +1,196 @@
+/*
+ * gfsph.h — C ABI of the B200 (sm_100a) implementation of Geoflow-SPH's
+ * per-time-step depth-integrated SPH hot path.
+ *
+ * Reference program: EL-BID/Deslizamientos-y-flujos, the Fortran sources in "Codes Geoflow_SPH"
+ * (files are cited by base name without their numeric prefix).
+ *
+ * In the reference the step is a set of argument-less Fortran module procedures
+ * working on module globals:
+ *   - adaptive_dt_sph        SPH_MAIN_2019.f90:289 -> Adaptive_dt_sph_SW SPH_SW_2019.f90:6521-6664
+ *   - time_integration_sph   SPH_MAIN_2019.f90:220-283 -> RK45 SPH_MAIN_2019.f90:746-1005
+ *   - called from Driver_Flow's DTGT loop SPH_FEM_Driver_2019.f90:1580-1697
+ *     (adaptive_dt_sph at :1590, time_integration_sph at :1617)
+ * The globals it reads and writes are x, vx, rho (= flow depth h), mass
+ * (= volume), hsml, itype, If_Out_Domain (SPH_Main_Vars_2019.f90), dt_sph and
+ * time_sph (SPH_FEM_Driver_time_vars_2019.f90), const(1..110)
+ * (SPH_SW_Vars_2019.f90:27) and topol/coorg/xming/deltxg/npoigx
+ * (SPH_FEM_topo_2019.f90:94-110).
+ *
+ * This ABI replaces those procedures with explicit calls on an opaque handle
+ * that owns all device memory.  Host arrays are caller-owned and only copied.
+ * Particle arrays use the reference's Fortran layout: vectors are (2,n)
+ * column-major FP32, i.e. x[2*i+0] = x(1,i+1), x[2*i+1] = x(2,i+1).
+ * Every call returns an int status: 0 ok, > 0 warning, < 0 error.
+ * Calls on one handle must not run concurrently.  Nothing here falls back to
+ * the CPU: without a usable CUDA device every compute call fails with
+ * GFSPH_ERR_NO_DEVICE.
+ */
+#ifndef GFSPH_H
+#define GFSPH_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GFSPH_NCONST 110
+#define GFSPH_NTOPO 16
+
+/* status codes */
+#define GFSPH_OK 0
+#define GFSPH_T_END_REACHED 1        /* warning: stopped early because time >= t_end */
+#define GFSPH_ERR_ARG (-1)           /* bad argument (null pointer, bad size) */
+#define GFSPH_ERR_CUDA (-2)          /* CUDA runtime error */
+#define GFSPH_ERR_CAPACITY (-3)      /* cell grid / neighbour table could not be grown */
+#define GFSPH_ERR_UNSUPPORTED (-4)   /* option outside the implemented path */
+#define GFSPH_ERR_STATE (-5)         /* call out of order (e.g. step before upload) */
+#define GFSPH_ERR_NO_DEVICE (-6)     /* no usable CUDA device */
+#define GFSPH_ERR_NONFINITE (-7)     /* a non-finite value appeared in the state */
+#define GFSPH_ERR_DOMAIN (-8)        /* all particles left the DEM box */
+
+/*
+ * Control parameters.  cst[k-1] holds the reference's const(k)
+ * (read in blocks of 15 by Input_SW, SPH_SW_2019.f90:1151-1204).  The ones the
+ * step uses: const(1) g, const(2) density, const(3) Voellmy xi (or Manning),
+ * const(5) nfric, const(6) Bingham yield stress, const(7) Bingham viscosity,
+ * const(9) tan(phi), const(10) hfrict0, const(15) comp, const(16) cos-theta
+ * switch (must be 0), const(20) density-factor switch (must be 0), const(21)
+ * erosion law (1 = Hungr), const(22) Hungr constant, const(47) slip factor
+ * alpha, const(48) maximum erodible depth.
+ */
+typedef struct gfsph_params {
+    float cst[GFSPH_NCONST];
+    int pa_sph;            /* 1 or 2, SPH_SW_2019.f90:6905-6920 */
+    int nnps;              /* 2 or 4 (grid_find_NEW_tools / _tools3); neighbour sets are the same */
+    int sle;               /* 0 keep hsml, 1 hsml = 2 sqrt(m/h) (h_upgrade SPH_MAIN_2019.f90:2925-2931) */
+    int skf;               /* 1 cubic spline, 4 Wendland C2 (kernel_TOOLS My_SPH_Tools_2019.f90:2062) */
+    int summation_density; /* must be 1 (sum_density_Tools) */
+    int average_velocity;  /* 1 applies av_vel (XSPH, SPH_MAIN_2019.f90:3042-3099) */
+    int nor_density;       /* must be 0 */
+    int ic_adapt;          /* ic_adapt_dt_sph: 0 fixed, 1 hsml/(3c), 2 hsml/(3(c+|v|)) */
+    float h_inf;           /* h_inf_SW */
+    float dt;              /* initial dt_sph */
+    int dem_deriv;         /* slopes when not supplied: 0 FEM projection (Get_Topol), 1 finite differences */
+    int max_neighbours;    /* initial neighbour-table capacity per particle; 0 = 96 (grows on demand) */
+    int reserved[8];
+} gfsph_params;
+
+/*
+ * The DEM ("topo grid"): npoigx x npoigy nodes, x fastest, node (ix,iy) at
+ * (xmin + ix*dx, ymin + iy*dy).  Either pass the reference's topol(ntopo,npoig)
+ * array as-is (topol != NULL, column-major, ntopo >= 15: Z, Zx, Zy, the six
+ * curvature terms, ..., eroded depth (14), erodible depth (15)), or pass only
+ * z (topol == NULL) and the slopes are derived with params->dem_deriv and the
+ * erodible depth is initialised as Input_SW does (SPH_SW_2019.f90:1290-1310).
+ */
+typedef struct gfsph_dem {
+    int nx, ny;            /* npoigx, npoigy */
+    float xmin, ymin;      /* xming, yming */
+    float dx, dy;          /* deltxg, deltyg */
+    const float* topol;    /* optional, topol(ntopo, nx*ny) */
+    int ntopo;
+    const float* z;        /* used when topol == NULL: Z(nx*ny) */
+} gfsph_dem;
+
+typedef struct gfsph_handle gfsph_handle;
+
+/* raster kinds for gfsph_raster (one value per DEM node, nx*ny) */
+#define GFSPH_RASTER_DEPTH_IDW 0  /* IDW of h over the 4x4 node stencil, SPH_SW_2019.f90:14310-14400 */
+#define GFSPH_RASTER_MAX_DEPTH 1  /* per-node max h over hazard samples, Get_MC_pixel_Vars_SW :20800-20812 */
+#define GFSPH_RASTER_MAX_VEL 2    /* per-node max |v| over hazard samples */
+#define GFSPH_RASTER_SUM_DEPTH 3  /* per-node sum of h over hazard samples */
+#define GFSPH_RASTER_SUM_VEL 4    /* per-node sum of |v| over hazard samples */
+#define GFSPH_RASTER_COUNT 5      /* per-node count of particle visits over hazard samples */
+#define GFSPH_RASTER_Z 6          /* current terrain elevation topol(1,:) (lowered by erosion) */
+#define GFSPH_RASTER_ERODED 7     /* accumulated eroded depth topol(14,:) */
+#define GFSPH_RASTER_AVAILABLE 8  /* remaining erodible depth topol(15,:) */
+
+/* Replaces Init_sph's SPH setup (SPH_MAIN_2019.f90:74) for the step: validates
+ * the options, copies the DEM to the device, derives slopes if needed. */
+int gfsph_create(const gfsph_params* params, const gfsph_dem* dem, gfsph_handle** out);
+
+/* Frees all device memory of the handle. */
+int gfsph_destroy(gfsph_handle* h);
+
+/* Replaces the particle arrays filled by Setup_Global_Arrays_SW
+ * (SPH_SW_2019.f90:6223-6246).  x, v: (2,n); rho, mass, hsml: (n); itype (n)
+ * must be 1 (soil) for every particle; out_flag (n) is If_Out_Domain (may be
+ * NULL = all inside). */
+int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const float* rho,
+                 const float* mass, const float* hsml, const int* itype, const int* out_flag);
+
+/* Copies the particle state back in the original particle order.  Any
+ * pointer may be NULL to skip that array. */
+int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass, float* hsml,
+                   int* out_flag);
+
+/* Replaces up to nsteps iterations of the DTGT loop body
+ * (SPH_FEM_Driver_2019.f90:1580-1617): adaptive_dt_sph, time_integration_sph
+ * (RK45 with summation density, internal and external forces, erosion,
+ * h_upgrade, av_vel) and time += dt.  Stops early, returning
+ * GFSPH_T_END_REACHED, once time >= t_end.  All steps run on the device
+ * without host synchronisation.  t_out / steps_done may be NULL. */
+int gfsph_step(gfsph_handle* h, int nsteps, double t_end, double* t_out, int* steps_done);
+
+/* time_sph and dt_sph of the handle. */
+int gfsph_get_time(gfsph_handle* h, double* t, float* dt);
+int gfsph_set_time(gfsph_handle* h, double t, float dt);
+
+/* Summation density on the current state without advancing it: the
+ * neighbour search of grid_find_NEW_tools (My_SPH_Tools_2019.f90:1109-1370)
+ * followed by sum_density_Tools (My_SPH_Tools_2019.f90:1763-1859).  Writes h
+ * per particle (original order) and keeps the neighbour table for
+ * gfsph_neighbours. */
+int gfsph_density(gfsph_handle* h, float* rho_out);
+
+/* Neighbour sets of the last search (start of the last step, or
+ * gfsph_density), original particle indices, CSR: offsets[n+1], idx[cap].
+ * Each list is sorted ascending.  Returns GFSPH_ERR_CAPACITY when cap is too
+ * small (offsets[n] then holds the needed size). */
+int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx);
+
+/* Per-particle internal (pressure) acceleration of IntForces_SW
+ * (SPH_SW_2019.f90:6669-6941) on the current state, (2,n), original order.
+ * Runs the search and density first. */
+int gfsph_internal_forces(gfsph_handle* h, float* indvxdt);
+
+/* One raster per DEM node, nx*ny values, x fastest. */
+int gfsph_raster(gfsph_handle* h, int kind, float* out);
+
+/* Adds the current particles to the per-node hazard statistics
+ * (Get_MC_pixel_Vars_SW, SPH_SW_2019.f90:20717-20833: sum/max of h and |v|
+ * over the particles in each node's cell).  Called at plot times. */
+int gfsph_hazard_sample(gfsph_handle* h);
+int gfsph_hazard_reset(gfsph_handle* h);
+
+/* Runs the handle's kernels on this cudaStream_t (NULL = the handle's own). */
+int gfsph_set_stream(gfsph_handle* h, void* cuda_stream);
+
+/* Device timing with CUDA events on the handle's stream.  enable = 1: one
+ * event pair around every kernel launch (graph replay off while on);
+ * enable = 2: one event pair around the device work of each gfsph_step
+ * call (graphs kept), read back as the last "kernel" slot ("step_batches",
+ * launches = steps).  enable = 0: off.  Enabling resets the counters. */
+int gfsph_profile(gfsph_handle* h, int enable);
+int gfsph_profile_read(gfsph_handle* h, int kernel, double* total_ms, long long* launches);
+int gfsph_num_kernels(void);
+const char* gfsph_kernel_name(int kernel);
+
+/* Number of kernels this handle has launched so far (graph replays count
+ * each kernel node). */
+long long gfsph_launch_count(gfsph_handle* h);
+
+/* Derives the DEM slope/curvature rows topol(2..13,:) from topol(1,:) on the
+ * host, once, as Topo_main does before the time loop: mode 0 = lumped-mass
+ * FEM projection with 5 Jacobi sweeps (Get_Topol, SPH_FEM_topo_2019.f90:1723-1939),
+ * mode 1 = central differences (Fdiff_derivs, :2812-2877).  topol is
+ * (GFSPH_NTOPO, nx*ny) column-major; row 1 is read, rows 2..13 written. */
+int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol);
+
+const char* gfsph_strerror(int status);
+int gfsph_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFSPH_H */

@@ -1,0 +1,989 @@
+/*
+ * TEST INFRASTRUCTURE ONLY — CPU oracle for the gfsph GPU step.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py (its CPU-baseline leg and
+ * its reference arm) may load this library, and only as the checker or as the
+ * timed CPU baseline.  The product (libgfsph.so) never links or calls it.
+ *
+ * What it is: a literal restatement, in C++, of the per-time-step path of
+ * Geoflow-SPH (EL-BID/Deslizamientos-y-flujos, Fortran, "Codes Geoflow_SPH"),
+ * following the reference's own control flow: the pair list is built once per
+ * step (grid_find_NEW_tools / _tools3), then RK45 re-evaluates summation
+ * density, IntForces_SW and ExtForces_SW(0) in each of its four stages,
+ * recomputes the density after the final update, applies ExtForces_SW(1)
+ * erosion, h_upgrade and av_vel.  Every floating-point expression keeps the
+ * Fortran left-to-right evaluation order, without FMA contraction
+ * (build with -ffp-contract=off).
+ *
+ * Precision modes (template <R, A>: R = state and arithmetic, A = accumulators
+ * of the pair sums and of the erosion scatter):
+ *   mode 0  R=float,  A=float  : the reference as shipped (irk = k_real,
+ *                                SPH_FEM_variable_types_2019.f90:14), pair sums
+ *                                in pair-list order.
+ *   mode 1  R=float,  A=double : the precision scheme of the GPU path
+ *                                (FP32 state and per-pair terms, FP64 sums).
+ *   mode 2  R=double, A=double : the reference rebuilt with irk = k_double
+ *                                (:13).  Fortran literals without a kind
+ *                                suffix stay default-real (single precision)
+ *                                in such a build, so every such literal is
+ *                                taken as its float value here (lit()).
+ *
+ * Parity status: UNPINNED.  The reference ships no tests, no golden vectors
+ * and no expected outputs, and it cannot be compiled here (Fortran; no
+ * gfortran/ifort/flang in the image).  This oracle is pinned instead by
+ * known-answer tests derived from the mathematics (kernel normalisation and
+ * gradient consistency, still layer on flat ground, infinite-slope Voellmy
+ * terminal velocity, mass conservation, brute-force neighbour sets) in
+ * tests/test_oracle_kat.py.
+ *
+ * Deviations from the literal Fortran, each one a place where the literal
+ * code reads undefined or out-of-range data:
+ *   - Bingham (nfric = 4): SPH_SW_2019.f90:9616-9618 overwrite the regime
+ *     friction of :9552-9572 with Tau0/dens*hu/|hu|, where Tau0 is only set
+ *     in the intermediate regime and is otherwise stale from a previous
+ *     particle (or undefined).  The regime value of :9552-9572 is kept.
+ *   - Get_Z_Topo (SPH_FEM_topo_2019.f90:2420-2432) only warns when a point
+ *     maps to the last node column/row and then reads the next row; the cell
+ *     index is clamped to the last cell instead.
+ *   - hsml = 2*(m/h)**(1./2) is evaluated with a correctly rounded sqrt.
+ *   - Pair traversal order: generation order of grid_find (the linked list's
+ *     order depends on the node-reuse history of earlier steps).
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "../include/gfsph.h"
+
+namespace {
+
+/* default-real literal: the value a Fortran constant like 0.3 or 2./3. has */
+template <class R> inline R lit(double v) { return (R)(float)v; }
+
+template <class R> inline R fpi() { return (R)(4.0f * atanf(1.0f)); } /* pi = 4.*atan(1.0) */
+
+template <class R> inline R rmax(R a, R b) { return (a > b) ? a : b; } /* MAX(a,b) */
+template <class R> inline R rmin(R a, R b) { return (a < b) ? a : b; }
+
+/* kernel_TOOLS, My_SPH_Tools_2019.f90:2062-2180, 2-D, skf 1 and 4 */
+template <class R>
+inline void kernel_tools(int skf, R r, R dx0, R dx1, R hs, R& w, R& d0, R& d1) {
+    const R pi = fpi<R>();
+    R q = r / hs;
+    w = 0; d0 = 0; d1 = 0;
+    if (skf == 1) {
+        R factor = (R)15 / ((((R)7 * pi) * hs) * hs);                 /* :2089 */
+        if (q >= 0 && q <= 1) {                                           /* :2095-2099 */
+            w = factor * (((lit<R>(2.0 / 3.0) - q * q) + ((q * q) * q) / (R)2));
+            R t = (factor * ((R)-2 + (R)1.5 * q)) / (hs * hs);
+            d0 = t * dx0;
+            d1 = t * dx1;
+        } else if (q > 1 && q <= 2) {                                     /* :2100-2104 */
+            R u = (R)2 - q;
+            w = ((factor * (R)1) / (R)6) * ((u * u) * u);
+            R t = ((((factor * (R)1) / (R)6) * (R)3) * (u * u)) / hs;
+            d0 = -(t * (dx0 / r));
+            d1 = -(t * (dx1 / r));
+        }
+    } else if (skf == 4) {
+        R factor = (R)7 / ((((R)4 * pi) * hs) * hs);                    /* :2164 */
+        if (q >= 0 && q <= 2) {                                           /* :2169-2174 */
+            R a = (R)1 - q / (R)2;
+            w = factor * (((a * a) * (a * a)) * ((R)2 * q + (R)1));
+            R t = factor * (-((R)5 * ((a * a) * a)));
+            R s = ((R)1 / hs) / hs;
+            d0 = t * (s * dx0);
+            d1 = t * (s * dx1);
+        }
+    }
+}
+
+template <class R> inline R self_density_w(int skf, R hs) {
+    R w, a, b;
+    kernel_tools<R>(skf, (R)0, (R)0, (R)0, hs, w, a, b);
+    return w;
+}
+
+struct Pair { int i, j; };
+
+template <class R, class A>
+struct Oracle {
+    /* options */
+    const gfsph_params* P;
+    R cst[GFSPH_NCONST + 1]; /* 1-based like const(k) */
+    int nfric, ic_erosion;
+    /* DEM */
+    int nx, ny, npoig;
+    R xming, yming, dxg, dyg, xmaxg, ymaxg;
+    std::vector<R> topol; /* (16, npoig) column-major, like topol(16,npoig) */
+    /* particles */
+    int n;
+    std::vector<R> x, v, rho, mass, hsml, x0, v0, p;
+    std::vector<R> ex, in, Dx, Dv, av;
+    std::vector<int> flag;
+    /* pairs */
+    std::vector<Pair> pairs;
+    std::vector<R> pw, pd0, pd1;
+    R dt;
+    double time;
+    std::vector<A> auxv1, auxv2; /* erosion scatter, ExtForces_SW(1) */
+
+    R& T(int k, int ip) { return topol[(size_t)ip * GFSPH_NTOPO + (k - 1)]; }
+    R coorgx(int ix) { return xming + (R)ix * dxg; } /* 0-based ix */
+    R coorgy(int iy) { return yming + (R)iy * dyg; }
+
+    /* Check_Out_Domain, SPH_MAIN_2019.f90:1764-1788 */
+    void check_out_domain() {
+        for (int i = 0; i < n; i++) {
+            R d0 = (x[2 * i] - xming) * (x[2 * i] - xmaxg);
+            if (d0 > 0) flag[i] = 1;
+            R d1 = (x[2 * i + 1] - yming) * (x[2 * i + 1] - ymaxg);
+            if (d1 > 0) flag[i] = 1;
+        }
+    }
+
+    /* Adaptive_dt_sph_SW, SPH_SW_2019.f90:6521-6664 (modes 0, 1, 2) */
+    void adaptive_dt() {
+        R dtmin = lit<R>(1.e10);
+        R cgra = cst[1];
+        if (P->ic_adapt == 1 || P->ic_adapt == 2) {
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                if (rho[i] < (R)P->h_inf) rho[i] = (R)P->h_inf;
+                R c = std::sqrt(cgra * rho[i]);
+                R cc = rmax<R>(lit<R>(1.e-6), c);
+                if (P->ic_adapt == 2) {
+                    R vv = v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1];
+                    vv = std::sqrt(vv);
+                    cc = cc + vv;
+                }
+                cc = hsml[i] / ((R)3 * cc);
+                dtmin = rmin<R>(cc, dtmin);
+            }
+        }
+        if (dtmin < dt) dt = dtmin;
+        else if (P->ic_adapt != 0) dt = rmin<R>(lit<R>(1.1) * dt, dtmin);
+    }
+
+    /* grid_find_NEW_tools (nnps=2, My_SPH_Tools_2019.f90:1109-1370) and
+     * grid_find_NEW_tools3 (nnps=4, :802-1104): counting sort into cells of
+     * size 2*max(hsml), half-stencil pair enumeration, r < 2*(hi+hj)/2. */
+    void grid_find() {
+        pairs.clear(); pw.clear(); pd0.clear(); pd1.clear();
+        std::vector<R> xr(2 * (size_t)n);
+        if (P->nnps == 4) {
+            R xg0 = 0, xg1 = 0; int cnt = 0;
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                cnt++; xg0 = xg0 + x[2 * i]; xg1 = xg1 + x[2 * i + 1];
+            }
+            if (cnt == 0) return;
+            xg0 = xg0 / (R)cnt; xg1 = xg1 / (R)cnt;
+            R ixx = 0, ixy = 0, iyy = 0;
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                R a = x[2 * i] - xg0, b = x[2 * i + 1] - xg1;
+                ixx = ixx + b * b; ixy = ixy + a * b; iyy = iyy + a * a;
+            }
+            R th = -(lit<R>(0.5) * std::atan2((R)2 * ixy, iyy - ixx));
+            R c = std::cos(th), s = std::sin(th);
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                R a = x[2 * i] - xg0, b = x[2 * i + 1] - xg1;
+                xr[2 * i] = c * a + s * b;
+                xr[2 * i + 1] = -s * a + c * b;
+            }
+        } else {
+            xr = x;
+        }
+        R xmin[2] = {lit<R>(1.e10), lit<R>(1.e10)}, xmax[2] = {-lit<R>(1.e10), -lit<R>(1.e10)};
+        R deltx[2] = {0, 0};
+        int ndiv[2] = {1, 1};
+        for (int d = 0; d < 2; d++) {
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                if (xr[2 * i + d] < xmin[d]) xmin[d] = xr[2 * i + d];
+                if (xr[2 * i + d] > xmax[d]) xmax[d] = xr[2 * i + d];
+                if (deltx[d] < hsml[i]) deltx[d] = hsml[i];
+            }
+            deltx[d] = deltx[d] * (R)2;
+            R length = xmax[d] - xmin[d];
+            ndiv[d] = (int)(length / deltx[d] + (R)1);
+            R length_new = (R)ndiv[d] * deltx[d];
+            xmin[d] = (xmin[d] - (length_new - length) / (R)2) - lit<R>(0.001) * length;
+        }
+        long ndivt = (long)ndiv[0] * ndiv[1];
+        std::vector<int> cell(n, -1), cnt(ndivt + 1, 0), start(ndivt + 1, 0), list(n);
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            int id[2];
+            for (int d = 0; d < 2; d++) {
+                id[d] = (int)((xr[2 * i + d] - xmin[d]) / deltx[d] + (R)1);
+                if (id[d] > ndiv[d]) id[d] = ndiv[d];
+            }
+            long c = (long)ndiv[0] * (id[1] - 1) + (id[0] - 1);
+            cell[i] = (int)c;
+            cnt[c]++;
+        }
+        for (long c = 0, s = 0; c < ndivt; c++) { start[c] = (int)s; s += cnt[c]; }
+        std::vector<int> fill(ndivt, 0);
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            list[start[cell[i]] + fill[cell[i]]++] = i;
+        }
+        const int scale_k = 2; /* skf 1 and 4 */
+        for (int idy = 1; idy <= ndiv[1]; idy++)
+            for (int idx = 1; idx <= ndiv[0]; idx++) {
+                long ic = (long)ndiv[0] * (idy - 1) + (idx - 1);
+                for (int a = 0; a < cnt[ic]; a++) {
+                    int it = list[start[ic] + a];
+                    int jx0 = std::max(1, idx - 1), jx1 = std::min(ndiv[0], idx + 1);
+                    int jy1 = std::min(ndiv[1], idy + 1);
+                    for (int jdy = idy; jdy <= jy1; jdy++)
+                        for (int jdx = jx0; jdx <= jx1; jdx++) {
+                            long jc = (long)ndiv[0] * (jdy - 1) + (jdx - 1);
+                            if (jc < ic) continue;
+                            int b0 = (jc == ic) ? a + 1 : 0;
+                            for (int b = b0; b < cnt[jc]; b++) {
+                                int jt = list[start[jc] + b];
+                                R d0 = x[2 * it] - x[2 * jt];
+                                R dr = d0 * d0;
+                                R d1 = x[2 * it + 1] - x[2 * jt + 1];
+                                dr = dr + d1 * d1;
+                                R mh = (hsml[it] + hsml[jt]) / (R)2;
+                                R r = std::sqrt(dr);
+                                if (r < (R)scale_k * mh) {
+                                    R w, g0, g1;
+                                    kernel_tools<R>(P->skf, r, d0, d1, mh, w, g0, g1);
+                                    pairs.push_back({it, jt});
+                                    pw.push_back(w); pd0.push_back(g0); pd1.push_back(g1);
+                                }
+                            }
+                        }
+                }
+            }
+        /* Pint_Update_SW_tools (My_SPH_Tools_2019.f90:1652-1758): all particles
+         * are soil (itype 1), every pair is type 0 and keeps its order. */
+    }
+
+    /* sum_density_Tools, My_SPH_Tools_2019.f90:1763-1859 (nor_density = F) */
+    void sum_density() {
+        std::vector<A> acc(n);
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) { acc[i] = (A)rho[i]; continue; }
+            R sd = self_density_w<R>(P->skf, hsml[i]);
+            acc[i] = (A)(sd * mass[i]);
+        }
+        for (size_t k = 0; k < pairs.size(); k++) {
+            int i = pairs[k].i, j = pairs[k].j;
+            acc[i] = acc[i] + (A)(mass[j] * pw[k]);
+            acc[j] = acc[j] + (A)(mass[i] * pw[k]);
+        }
+        for (int i = 0; i < n; i++) rho[i] = (R)acc[i];
+    }
+
+    /* IntForces_SW, SPH_SW_2019.f90:6669-6941 (ic_ws_Interact = 0, ic_SWalg = 0,
+     * ic_cosTheta = 0, no K0, no end-solid law) */
+    void int_forces() {
+        R cgra05 = cst[1] * lit<R>(0.5); /* gravz*0.5, gravz = const(1) */
+        for (int i = 0; i < n; i++)
+            if (rho[i] < (R)P->h_inf) rho[i] = (R)P->h_inf; /* :6769 */
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            p[i] = (cgra05 * rho[i]) * rho[i]; /* :6797 */
+        }
+        std::vector<A> a0(n, (A)0), a1(n, (A)0);
+        for (size_t k = 0; k < pairs.size(); k++) {
+            int i = pairs[k].i, j = pairs[k].j;
+            R mi = mass[i], mj = mass[j];
+            R g[2] = {pd0[k], pd1[k]};
+            for (int d = 0; d < 2; d++) {
+                R h;
+                if (P->pa_sph == 1) { /* :6905-6912 */
+                    R rij = (R)1 / (rho[i] * rho[j]);
+                    h = -(p[i] + p[j]) * g[d];
+                    h = h * rij;
+                } else { /* :6914-6920 */
+                    h = -(p[i] / (rho[i] * rho[i]) + p[j] / (rho[j] * rho[j])) * g[d];
+                }
+                A* ai = d ? &a1[0] : &a0[0];
+                ai[i] = ai[i] + (A)(mj * h);
+                ai[j] = ai[j] - (A)(mi * h);
+            }
+        }
+        for (int i = 0; i < n; i++) { in[2 * i] = (R)a0[i]; in[2 * i + 1] = (R)a1[i]; }
+    }
+
+    /* Get_Z_Topo, SPH_FEM_topo_2019.f90:2395-2491: bilinear shape functions
+     * on the DEM cell; all nodes inside the model (kpoin = 4). */
+    void get_z_topo(R xx, R yy, R& zp, R& zpx, R& zpy, R top[6], bool want_top) {
+        int ipx = (int)((xx - xming) / dxg + (R)1);
+        int ipy = (int)((yy - yming) / dyg + (R)1);
+        if (ipx >= nx) ipx = nx - 1;
+        if (ipy >= ny) ipy = ny - 1;
+        if (ipx < 1) ipx = 1;
+        if (ipy < 1) ipy = 1;
+        int ip = (ipy - 1) * nx + (ipx - 1);
+        int n1 = ip, n2 = ip + 1, n3 = ip + 1 + nx, n4 = n3 - 1;
+        R xref = xming + (R)(ipx - 1) * dxg;
+        R yref = yming + (R)(ipy - 1) * dyg;
+        R xi = (xx - xref) / dxg;
+        R eta = (yy - yref) / dyg;
+        R sh1 = ((R)1 - xi) * ((R)1 - eta);
+        R sh2 = xi * ((R)1 - eta);
+        R sh3 = xi * eta;
+        R sh4 = ((R)1 - xi) * eta;
+        auto interp = [&](int k) {
+            return ((sh1 * T(k, n1) + sh2 * T(k, n2)) + sh3 * T(k, n3)) + sh4 * T(k, n4);
+        };
+        zp = interp(1);
+        zpx = interp(2);
+        zpy = interp(3);
+        if (want_top)
+            for (int k = 0; k < 6; k++) top[k] = interp(4 + k);
+    }
+
+    struct Local { /* ExtForces_SW locals shared with its contained routines */
+        R h, hu, hv, hinv, vmod, hvmod, hvmodinv, frictx, fricty, totfrict, cf5, gravx, gravy, gravz;
+    };
+
+    /* the start of the ExtForces_SW particle loop, SPH_SW_2019.f90:8564-8596 */
+    void ext_locals(int i, R hdepth, Local& L) {
+        L.h = hdepth;
+        L.hu = L.h * v[2 * i];
+        L.hv = L.h * v[2 * i + 1];
+        if (L.h < cst[15]) {
+            L.h = cst[15];
+            L.hu = 0; L.hv = 0; L.hinv = 0; L.vmod = 0; L.hvmod = 0; L.hvmodinv = 0;
+        } else {
+            L.hinv = (R)1 / L.h;
+            L.hvmod = std::sqrt(L.hu * L.hu + L.hv * L.hv);
+            L.vmod = L.hvmod * L.hinv;
+            L.hvmodinv = (L.hvmod >= lit<R>(1.e-5)) ? (R)1 / L.hvmod : (R)0;
+        }
+    }
+
+    /* Get_Grav_Ext_SW (SPH_SW_2019.f90:9241-9349, ic_cosTheta = 0) followed by
+     * basal_friction_Ext_SW (:9355-9901) up to, not including, its reversal
+     * filter.  Returns via L the friction and the (possibly recomputed) vmod. */
+    void grav_and_friction(int i, Local& L, R top[6]) {
+        R cgra = cst[1];
+        bool frictional = (nfric >= 5 && nfric <= 7);
+        bool v2byr = (nfric == 7);
+        R zp, zpx, zpy;
+        get_z_topo(x[2 * i], x[2 * i + 1], zp, zpx, zpy, top, v2byr);
+        L.gravz = cgra;
+        L.gravx = -(cgra * zpx);
+        L.gravy = -(cgra * zpy);
+        R hfrict = rmax<R>(L.h, cst[10]);
+        L.frictx = 0; L.fricty = 0; L.totfrict = 0; L.cf5 = 0;
+        R dens = cst[2];
+        if (nfric == 4) { /* Bingham, :9538-9572 (regime value kept, see header) */
+            R tauy0 = cst[6], constK = cst[7];
+            R a_hat = (((R)6 * constK) * L.hvmod) / (tauy0 * (hfrict * hfrict));
+            if (a_hat > (R)50) {
+                R cf4b = ((R)3 * constK) / dens;
+                L.frictx = (cf4b * L.hu) / (hfrict * hfrict);
+                L.fricty = (cf4b * L.hv) / (hfrict * hfrict);
+            } else if (a_hat < lit<R>(0.01)) {
+                R cf4b = tauy0 / dens;
+                L.frictx = (cf4b * L.hu) * L.hvmodinv;
+                L.fricty = (cf4b * L.hv) * L.hvmodinv;
+            } else {
+                R a2 = (R)48, b2 = -((R)32 * a_hat) - (R)114, c2 = (R)65;
+                R xh = (-b2 - std::sqrt(b2 * b2 - ((R)4 * a2) * c2)) / ((R)2 * a2);
+                R tau0 = tauy0 / xh;
+                R cf4b = tau0 / dens;
+                L.frictx = (cf4b * L.hu) * L.hvmodinv;
+                L.fricty = (cf4b * L.hv) * L.hvmodinv;
+            }
+            L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+        } else if (frictional) { /* :9660-9750 */
+            R cv2byr = 0;
+            if (v2byr) {
+                R vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
+                L.vmod = std::sqrt(vxx * vxx + vyy * vyy);
+                if (L.vmod >= lit<R>(1e-5)) {
+                    R cosa = vxx / L.vmod, sina = vyy / L.vmod;
+                    R cos2 = cosa * cosa, sin2 = sina * sina, cbs = sina * cosa;
+                    R xnum = (top[3] * cos2 + top[4] * cbs) + top[5] * sin2;
+                    R xden = (top[0] * cos2 + top[1] * cbs) + top[2] * sin2;
+                    R rinv = xnum / xden;
+                    cv2byr = (L.vmod * L.vmod) * rinv;
+                }
+            }
+            R tanfi = cst[9];
+            R gtanfi = ((L.gravz + cv2byr) * tanfi) * (R)1; /* fact_dens = 1 */
+            if (gtanfi < 0) gtanfi = 0;
+            L.cf5 = gtanfi;
+            L.frictx = ((L.cf5 * L.hu) * L.hvmodinv) * L.h;
+            L.fricty = ((L.cf5 * L.hv) * L.hvmodinv) * L.h;
+            R xi = cst[3];
+            if (xi != 0) {
+                R vxx = v[2 * i], vyy = v[2 * i + 1];
+                R vm = vxx * vxx + vyy * vyy;
+                vm = (vm > 0) ? std::sqrt(vm) : (R)0;
+                L.vmod = vm;
+                if (xi > 0) {
+                    L.frictx = L.frictx + ((cgra * L.vmod) * vxx) / xi;
+                    L.fricty = L.fricty + ((cgra * L.vmod) * vyy) / xi;
+                } else {
+                    R constMu = -(((R)25 * cst[3]) / (R)4);
+                    L.frictx = L.frictx + ((constMu * L.vmod) * vxx) / (hfrict * hfrict);
+                    L.fricty = L.fricty + ((constMu * L.vmod) * vyy) / (hfrict * hfrict);
+                }
+            }
+            L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+        }
+    }
+
+    /* the reversal filter of basal_friction_Ext_SW, SPH_SW_2019.f90:9829-9895 */
+    void reversal_filter(int i, Local& L, R acc0, R acc1) {
+        bool frictional = (nfric >= 5 && nfric <= 7);
+        R dc0 = -(L.frictx * L.hinv), dc1 = -(L.fricty * L.hinv);
+        if (L.vmod > lit<R>(1.e-5)) {
+            R vc0 = v[2 * i], vc1 = v[2 * i + 1];
+            R vs0 = vc0 + dt * (acc0 + dc0), vs1 = vc1 + dt * (acc1 + dc1);
+            R vdot = vs0 * vc0 + vs1 * vc1;
+            if (vdot < 0) {
+                R vt0 = vc0 / L.vmod, vt1 = vc1 / L.vmod;
+                R accT = acc0 * vt0 + acc1 * vt1;
+                R decT = dc0 * vt0 + dc1 * vt1;
+                if (accT * decT < 0) {
+                    dc0 = -vc0 / dt - acc0;
+                    dc1 = -vc1 / dt - acc1;
+                    L.frictx = -dc0 * L.h;
+                    L.fricty = -dc1 * L.h;
+                }
+            }
+        } else {
+            R accT = std::sqrt(acc0 * acc0 + acc1 * acc1);
+            if (accT > lit<R>(1.e-5)) {
+                R ctf = frictional ? L.cf5 : L.totfrict;
+                L.frictx = (ctf * acc0) / accT;
+                L.fricty = (ctf * acc1) / accT;
+                R fricT = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+                if (accT <= fricT) { L.frictx = acc0; L.fricty = acc1; }
+            } else {
+                L.frictx = 0; L.fricty = 0;
+            }
+            L.frictx = L.frictx * L.h;
+            L.fricty = L.fricty * L.h;
+        }
+    }
+
+    R slip_fact() {
+        R s = 1;
+        if (cst[47] > lit<R>(1.e-6)) s = ((R)2 * cst[47]) / ((R)1 + cst[47]);
+        return s;
+    }
+
+    /* ExtForces_SW(0): SPH_SW_2019.f90:8483 and the particle loop :8532-8716 */
+    void ext_forces0() {
+        std::fill(ex.begin(), ex.end(), (R)0);
+        R top[6];
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            Local L;
+            ext_locals(i, rho[i], L);
+            grav_and_friction(i, L, top);
+            ex[2 * i] = ex[2 * i] + L.gravx;
+            ex[2 * i + 1] = ex[2 * i + 1] + L.gravy;
+            reversal_filter(i, L, ex[2 * i] + in[2 * i], ex[2 * i + 1] + in[2 * i + 1]);
+            ex[2 * i] = ex[2 * i] - L.frictx / L.h;
+            ex[2 * i + 1] = ex[2 * i + 1] - L.fricty / L.h;
+            if (ic_erosion) { /* Hungr, Get_Erosion_Rate_SW :10329-10331; momentum :8664-8697 */
+                R er = (cst[22] * L.h) * L.vmod;
+                R sf = slip_fact();
+                ex[2 * i] = ex[2 * i] - ((er * v[2 * i]) * L.hinv) * sf;
+                ex[2 * i + 1] = ex[2 * i + 1] - ((er * v[2 * i + 1]) * L.hinv) * sf;
+            }
+        }
+    }
+
+    /* ExtForces_SW(1): erosion after the RK update, SPH_SW_2019.f90:8717-8807 */
+    void ext_forces1() {
+        if (!ic_erosion) return;
+        std::fill(auxv1.begin(), auxv1.end(), (A)0);
+        std::fill(auxv2.begin(), auxv2.end(), (A)0);
+        R top[6];
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            Local L;
+            ext_locals(i, rho[i], L);
+            grav_and_friction(i, L, top);
+            R er = (cst[22] * L.h) * L.vmod;
+            R base = dt * er;
+            R xx = x[2 * i], yy = x[2 * i + 1];
+            int ipx = (int)((xx - xming) / dxg + (R)1);
+            int ipy = (int)((yy - yming) / dyg + (R)1);
+            int x0_ = std::max(1, ipx - 1), y0_ = std::max(1, ipy - 1);
+            int x1_ = std::min(nx, ipx + 2), y1_ = std::min(ny, ipy + 2);
+            for (int ix = x0_; ix <= x1_; ix++)
+                for (int iy = y0_; iy <= y1_; iy++) {
+                    int ip = (iy - 1) * nx + (ix - 1);
+                    R dx2 = xx - coorgx(ix - 1); dx2 = dx2 * dx2;
+                    R dy2 = yy - coorgy(iy - 1); dy2 = dy2 * dy2;
+                    R dist = rmax<R>(lit<R>(1.e-6), std::sqrt(dx2 + dy2));
+                    auxv1[ip] = auxv1[ip] + (A)(base / dist);
+                    auxv2[ip] = auxv2[ip] + (A)((R)1 / dist);
+                }
+            mass[i] = mass[i] + ((dt * er) * mass[i]) / rho[i];
+        }
+        for (int ip = 0; ip < npoig; ip++) {
+            if ((R)auxv2[ip] > lit<R>(1.e-6)) {
+                R xnum = (R)(auxv1[ip] / auxv2[ip]);
+                if (xnum > T(15, ip)) xnum = T(15, ip);
+                if (T(15, ip) > 0) {
+                    T(14, ip) = T(14, ip) + xnum;
+                    T(1, ip) = T(1, ip) - xnum;
+                    T(15, ip) = T(15, ip) - xnum;
+                }
+            }
+        }
+    }
+
+    /* h_upgrade sle = 1, SPH_MAIN_2019.f90:2925-2931 */
+    void h_upgrade() {
+        if (P->sle != 1) return;
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            hsml[i] = (R)2 * std::sqrt(mass[i] / rho[i]);
+        }
+    }
+
+    /* av_vel, SPH_MAIN_2019.f90:3042-3099, and v += av (:987-993) */
+    void av_vel() {
+        std::vector<A> a0(n, (A)0), a1(n, (A)0);
+        for (size_t k = 0; k < pairs.size(); k++) {
+            int i = pairs[k].i, j = pairs[k].j;
+            for (int d = 0; d < 2; d++) {
+                R dvx = v[2 * i + d] - v[2 * j + d];
+                R den = rho[i] + rho[j];
+                R ti = ((((R)2 * mass[j]) * dvx) / den) * pw[k];
+                R tj = ((((R)2 * mass[i]) * dvx) / den) * pw[k];
+                A* a = d ? &a1[0] : &a0[0];
+                a[i] = a[i] - (A)ti;
+                a[j] = a[j] + (A)tj;
+            }
+        }
+        const R eps = lit<R>(0.3);
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            av[2 * i] = eps * (R)a0[i];
+            av[2 * i + 1] = eps * (R)a1[i];
+            v[2 * i] = v[2 * i] + av[2 * i];
+            v[2 * i + 1] = v[2 * i + 1] + av[2 * i + 1];
+        }
+    }
+
+    /* RK45, SPH_MAIN_2019.f90:746-1005 */
+    void rk45() {
+        std::fill(in.begin(), in.end(), (R)0);
+        std::fill(ex.begin(), ex.end(), (R)0);
+        std::fill(Dx.begin(), Dx.end(), (R)0);
+        std::fill(Dv.begin(), Dv.end(), (R)0);
+        grid_find();
+        x0 = x; v0 = v;
+        const R f1[4] = {0, lit<R>(0.5), lit<R>(0.5), 1};
+        const R f2[4] = {1, 2, 2, 1};
+        for (int s = 0; s < 4; s++) {
+            R fdt = f1[s] * dt;
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                for (int d = 0; d < 2; d++) {
+                    x[2 * i + d] = x0[2 * i + d] + fdt * v[2 * i + d];
+                    v[2 * i + d] = v0[2 * i + d] + fdt * (ex[2 * i + d] + in[2 * i + d]);
+                }
+            }
+            check_out_domain();
+            sum_density();
+            int_forces();
+            ext_forces0();
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                for (int d = 0; d < 2; d++) {
+                    Dv[2 * i + d] = Dv[2 * i + d] + f2[s] * (ex[2 * i + d] + in[2 * i + d]);
+                    Dx[2 * i + d] = Dx[2 * i + d] + f2[s] * v[2 * i + d];
+                }
+            }
+        }
+        R dt6 = dt / (R)6;
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) continue;
+            for (int d = 0; d < 2; d++) {
+                x[2 * i + d] = x0[2 * i + d] + dt6 * Dx[2 * i + d];
+                v[2 * i + d] = v0[2 * i + d] + dt6 * Dv[2 * i + d];
+            }
+        }
+        sum_density();
+        check_out_domain();
+        ext_forces1();
+        h_upgrade();
+        if (P->average_velocity) av_vel();
+    }
+
+    /* one iteration of the DTGT loop, SPH_FEM_Driver_2019.f90:1580-1630 */
+    void step() {
+        adaptive_dt();
+        check_out_domain();           /* time_integration_sph :232 */
+        rk45();
+        check_out_domain();           /* :266 */
+        time += (double)dt;
+    }
+
+    int setup(const gfsph_params* p_, int nx_, int ny_, double xmin, double ymin, double dx, double dy,
+              const double* topol_in) {
+        P = p_;
+        cst[0] = 0;
+        for (int k = 1; k <= GFSPH_NCONST; k++) cst[k] = (R)P->cst[k - 1];
+        nfric = (int)(cst[5] + lit<R>(0.01));
+        ic_erosion = (cst[21] > lit<R>(1.e-9)) ? 1 : 0;
+        if (!(nfric == 4 || (nfric >= 5 && nfric <= 7))) return GFSPH_ERR_UNSUPPORTED;
+        if (ic_erosion && (int)(cst[21] + lit<R>(0.1)) != 1) return GFSPH_ERR_UNSUPPORTED;
+        if (P->skf != 1 && P->skf != 4) return GFSPH_ERR_UNSUPPORTED;
+        nx = nx_; ny = ny_; npoig = nx * ny;
+        xming = (R)(float)xmin; yming = (R)(float)ymin; dxg = (R)(float)dx; dyg = (R)(float)dy;
+        xmaxg = xming + (R)(nx - 1) * dxg;
+        ymaxg = yming + (R)(ny - 1) * dyg;
+        topol.assign((size_t)npoig * GFSPH_NTOPO, (R)0);
+        for (size_t k = 0; k < topol.size(); k++) topol[k] = (R)topol_in[k];
+        auxv1.assign(npoig, (A)0);
+        auxv2.assign(npoig, (A)0);
+        return 0;
+    }
+};
+
+template <class R, class A>
+int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+             double* topol, int n, double* x, double* v, double* rho, double* mass, double* hsml, int* flag,
+             int nsteps, double* dt, double* t, double t_end, int* steps_done) {
+    Oracle<R, A> o;
+    int st = o.setup(p, nx, ny, xmin, ymin, dx, dy, topol);
+    if (st) return st;
+    o.n = n;
+    auto cp = [&](std::vector<R>& dst, const double* src, size_t m) {
+        dst.resize(m);
+        for (size_t k = 0; k < m; k++) dst[k] = (R)src[k];
+    };
+    cp(o.x, x, 2 * (size_t)n); cp(o.v, v, 2 * (size_t)n);
+    cp(o.rho, rho, n); cp(o.mass, mass, n); cp(o.hsml, hsml, n);
+    o.flag.assign(flag, flag + n);
+    o.p.assign(n, (R)0);
+    o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
+    o.dt = (R)*dt;
+    o.time = *t;
+    int done = 0;
+    for (int s = 0; s < nsteps; s++) {
+        if (o.time >= t_end) break;
+        o.step();
+        done++;
+    }
+    for (size_t k = 0; k < 2 * (size_t)n; k++) { x[k] = (double)o.x[k]; v[k] = (double)o.v[k]; }
+    for (int k = 0; k < n; k++) {
+        rho[k] = (double)o.rho[k]; mass[k] = (double)o.mass[k]; hsml[k] = (double)o.hsml[k]; flag[k] = o.flag[k];
+    }
+    for (size_t k = 0; k < o.topol.size(); k++) topol[k] = (double)o.topol[k];
+    *dt = (double)o.dt;
+    *t = o.time;
+    if (steps_done) *steps_done = done;
+    return 0;
+}
+
+template <class R, class A>
+int pairs_mode(const gfsph_params* p, int n, const double* x, const double* hsml, const double* mass,
+               const double* rho_in, const int* flag, int cap, int* offsets, int* idx, double* rho_out,
+               double* indvxdt) {
+    Oracle<R, A> o;
+    o.P = p;
+    o.n = n;
+    o.x.resize(2 * (size_t)n); o.hsml.resize(n); o.mass.resize(n); o.rho.resize(n);
+    for (size_t k = 0; k < 2 * (size_t)n; k++) o.x[k] = (R)x[k];
+    for (int k = 0; k < n; k++) {
+        o.hsml[k] = (R)hsml[k];
+        o.mass[k] = mass ? (R)mass[k] : (R)0;
+        o.rho[k] = rho_in ? (R)rho_in[k] : (R)0;
+    }
+    o.flag.assign(flag, flag + n);
+    for (int k = 1; k <= GFSPH_NCONST; k++) o.cst[k] = (R)p->cst[k - 1];
+    o.grid_find();
+    if (offsets) {
+        std::vector<std::vector<int>> nb(n);
+        for (auto& pr : o.pairs) { nb[pr.i].push_back(pr.j); nb[pr.j].push_back(pr.i); }
+        int tot = 0;
+        for (int i = 0; i < n; i++) {
+            std::sort(nb[i].begin(), nb[i].end());
+            offsets[i] = tot;
+            for (int j : nb[i]) { if (tot < cap && idx) idx[tot] = j; tot++; }
+        }
+        offsets[n] = tot;
+        if (tot > cap) return GFSPH_ERR_CAPACITY;
+    }
+    if (rho_out || indvxdt) {
+        o.sum_density();
+        if (rho_out) for (int k = 0; k < n; k++) rho_out[k] = (double)o.rho[k];
+        if (indvxdt) {
+            o.p.assign(n, (R)0);
+            o.in.assign(2 * (size_t)n, (R)0);
+            o.int_forces();
+            for (size_t k = 0; k < 2 * (size_t)n; k++) indvxdt[k] = (double)o.in[k];
+        }
+    }
+    return 0;
+}
+
+/* getgeom2D + Get_Topol (SPH_FEM_topo_2019.f90:1660-1939) on the regular
+ * background triangulation of :583-604, and Fdiff_derivs (:2812-2877). */
+template <class R>
+int dem_topol_mode(int mode, int nx, int ny, double dx, double dy, double* topol_io) {
+    int np = nx * ny;
+    std::vector<R> t((size_t)np * GFSPH_NTOPO);
+    for (size_t k = 0; k < t.size(); k++) t[k] = (R)topol_io[k];
+    auto T = [&](int k, int ip) -> R& { return t[(size_t)ip * GFSPH_NTOPO + (k - 1)]; };
+    R dxg = (R)(float)dx, dyg = (R)(float)dy;
+    if (mode == 1) {
+        R del2x = (R)2 * dxg, del2y = (R)2 * dyg, delx2 = dxg * dxg, dely2 = dyg * dyg, delxy = dxg * dyg;
+        for (int iy = 1; iy < ny - 1; iy++)
+            for (int ix = 1; ix < nx - 1; ix++) {
+                int a = iy * nx + ix;
+                int al = a - 1, ar = a + 1, at = a + nx, atl = at - 1, atr = at + 1, ab = a - nx, abl = ab - 1,
+                    abr = ab + 1;
+                R zx = (T(1, ar) - T(1, al)) / del2x;
+                R zy = (T(1, at) - T(1, ab)) / del2y;
+                R rt = std::sqrt(((R)1 + zx * zx) + zy * zy);
+                R zxx = ((T(1, al) - (R)2 * T(1, a)) + T(1, ar)) / delx2;
+                R zyy = ((T(1, ab) - (R)2 * T(1, a)) + T(1, at)) / dely2;
+                R zxy = (((T(1, atr) - T(1, abr)) - T(1, atl)) + T(1, abl)) / ((R)4 * delxy);
+                T(2, a) = zx; T(3, a) = zy;
+                T(4, a) = (R)1 + zx * zx; T(5, a) = zx * zy; T(6, a) = (R)1 + zy * zy;
+                T(7, a) = zxx / rt; T(8, a) = zxy / rt; T(9, a) = zyy / rt;
+                T(10, a) = rt; T(11, a) = zxx; T(12, a) = zxy; T(13, a) = zyy;
+            }
+    } else {
+        int ne = 2 * (nx - 1) * (ny - 1);
+        std::vector<int> im(3 * (size_t)ne);
+        for (int iy = 0; iy < ny - 1; iy++)
+            for (int ix = 0; ix < nx - 1; ix++) {
+                int e = iy * (nx - 1) + ix;
+                int ip = iy * nx + ix;
+                int e1 = 2 * e, e2 = 2 * e + 1;
+                im[3 * e1 + 0] = ip; im[3 * e1 + 1] = ip + 1; im[3 * e1 + 2] = ip + 1 + nx;
+                im[3 * e2 + 0] = ip; im[3 * e2 + 1] = ip + 1 + nx; im[3 * e2 + 2] = ip + nx;
+            }
+        std::vector<R> geo(7 * (size_t)ne);
+        const R nxi[3] = {-1, 1, 0}, net[3] = {-1, 0, 1};
+        for (int e = 0; e < ne; e++) {
+            R xx[3], yy[3];
+            for (int k = 0; k < 3; k++) {
+                int ip = im[3 * e + k];
+                /* node coordinates relative to the DEM origin (xming, yming) */
+                xx[k] = (R)(ip % nx) * dxg;
+                yy[k] = (R)(ip / nx) * dyg;
+            }
+            R x21 = xx[1] - xx[0], x31 = xx[2] - xx[0], y21 = yy[1] - yy[0], y31 = yy[2] - yy[0];
+            R rj = x21 * y31 - x31 * y21;
+            R rj1 = (R)1 / rj;
+            R xix = y31 * rj1, xiy = -(x31 * rj1), etx = -(y21 * rj1), ety = x21 * rj1;
+            for (int k = 0; k < 3; k++) {
+                geo[7 * e + k] = xix * nxi[k] + etx * net[k];
+                geo[7 * e + k + 3] = xiy * nxi[k] + ety * net[k];
+            }
+            geo[7 * e + 6] = rj;
+        }
+        std::vector<R> ml(np, (R)0);
+        for (int e = 0; e < ne; e++) {
+            R a3 = geo[7 * e + 6] / (R)6;
+            for (int k = 0; k < 3; k++) ml[im[3 * e + k]] = ml[im[3 * e + k]] + a3;
+        }
+        std::vector<R> tel2(ne), tel3(ne);
+        for (int e = 0; e < ne; e++) {
+            R ddx = 0, ddy = 0;
+            for (int k = 0; k < 3; k++) {
+                int ip = im[3 * e + k];
+                ddx = ddx + T(1, ip) * geo[7 * e + k];
+                ddy = ddy + T(1, ip) * geo[7 * e + k + 3];
+            }
+            tel2[e] = ddx; tel3[e] = ddy;
+        }
+        const R mm[3][3] = {{2, 1, 1}, {1, 2, 1}, {1, 1, 2}};
+        auto project = [&](int nf, std::vector<R>* tel, int* rows) {
+            std::vector<R> rhs((size_t)np * nf, (R)0), rh((size_t)np * nf);
+            for (int e = 0; e < ne; e++) {
+                R coe = geo[7 * e + 6] / (R)6;
+                for (int k = 0; k < 3; k++) {
+                    int ip = im[3 * e + k];
+                    for (int f = 0; f < nf; f++) rhs[(size_t)ip * nf + f] = rhs[(size_t)ip * nf + f] + tel[f][e] * coe;
+                }
+            }
+            for (int ip = 0; ip < np; ip++)
+                for (int f = 0; f < nf; f++) T(rows[f], ip) = rhs[(size_t)ip * nf + f] / ml[ip];
+            for (int it = 2; it <= 5; it++) {
+                std::fill(rh.begin(), rh.end(), (R)0);
+                for (int e = 0; e < ne; e++) {
+                    R coe = geo[7 * e + 6] / (R)24;
+                    for (int a = 0; a < 3; a++) {
+                        int ip = im[3 * e + a];
+                        for (int b = 0; b < 3; b++) {
+                            int jp = im[3 * e + b];
+                            R cm = mm[a][b];
+                            for (int f = 0; f < nf; f++)
+                                rh[(size_t)ip * nf + f] = rh[(size_t)ip * nf + f] + (cm * coe) * T(rows[f], jp);
+                        }
+                    }
+                }
+                for (int ip = 0; ip < np; ip++)
+                    for (int f = 0; f < nf; f++)
+                        T(rows[f], ip) = T(rows[f], ip) + (rhs[(size_t)ip * nf + f] - rh[(size_t)ip * nf + f]) / ml[ip];
+            }
+        };
+        std::vector<R> tl1[2] = {tel2, tel3};
+        int rows1[2] = {2, 3};
+        project(2, tl1, rows1);
+        std::vector<R> t4(ne), t5(ne), t6(ne);
+        for (int e = 0; e < ne; e++) {
+            R dxx = 0, dxy = 0, dyx = 0, dyy = 0;
+            for (int k = 0; k < 3; k++) {
+                int ip = im[3 * e + k];
+                dxx = dxx + T(2, ip) * geo[7 * e + k];
+                dxy = dxy + T(2, ip) * geo[7 * e + k + 3];
+                dyx = dyx + T(3, ip) * geo[7 * e + k];
+                dyy = dyy + T(3, ip) * geo[7 * e + k + 3];
+            }
+            t4[e] = dxx; t5[e] = (dxy + dyx) / (R)2; t6[e] = dyy;
+        }
+        std::vector<R> tl2[3] = {t4, t5, t6};
+        int rows2[3] = {4, 5, 6};
+        project(3, tl2, rows2);
+        for (int ip = 0; ip < np; ip++) {
+            R zx = T(2, ip), zy = T(3, ip), zxx = T(4, ip), zxy = T(5, ip), zyy = T(6, ip);
+            R rt = std::sqrt(((R)1 + zx * zx) + zy * zy);
+            T(4, ip) = (R)1 + zx * zx; T(5, ip) = zx * zy; T(6, ip) = (R)1 + zy * zy;
+            T(7, ip) = zxx / rt; T(8, ip) = zxy / rt; T(9, ip) = zyy / rt;
+            T(10, ip) = rt; T(11, ip) = zxx; T(12, ip) = zxy; T(13, ip) = zyy;
+        }
+    }
+    for (size_t k = 0; k < t.size(); k++) topol_io[k] = (double)t[k];
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+/* Runs nsteps steps of the reference path on the given state (in/out).
+ * topol: (16, nx*ny) in/out (erosion lowers Z).  mode: 0, 1, 2 as above. */
+int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+               double* topol, int n, double* x, double* v, double* rho, double* mass, double* hsml, int* flag,
+               int nsteps, double* dt, double* t, double t_end, int* steps_done) {
+    if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || !dt || !t || n < 0 || nx < 2 || ny < 2)
+        return GFSPH_ERR_ARG;
+    if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
+    switch (mode) {
+    case 0: return run_mode<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, t_end, steps_done);
+    case 1: return run_mode<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, t_end, steps_done);
+    case 2: return run_mode<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, t_end, steps_done);
+    default: return GFSPH_ERR_ARG;
+    }
+}
+
+/* Neighbour sets (CSR, sorted), summation density and internal forces of the
+ * reference on one state. Any of offsets/rho_out/indvxdt may be NULL. */
+int oracle_pairs(int mode, const gfsph_params* p, int n, const double* x, const double* hsml, const double* mass,
+                 const double* rho_in, const int* flag, int cap, int* offsets, int* idx, double* rho_out,
+                 double* indvxdt) {
+    if (!p || !x || !hsml || !flag || n < 0) return GFSPH_ERR_ARG;
+    switch (mode) {
+    case 0: return pairs_mode<float, float>(p, n, x, hsml, mass, rho_in, flag, cap, offsets, idx, rho_out, indvxdt);
+    case 1: return pairs_mode<float, double>(p, n, x, hsml, mass, rho_in, flag, cap, offsets, idx, rho_out, indvxdt);
+    case 2: return pairs_mode<double, double>(p, n, x, hsml, mass, rho_in, flag, cap, offsets, idx, rho_out, indvxdt);
+    default: return GFSPH_ERR_ARG;
+    }
+}
+
+/* SPH kernel values, for known-answer tests. */
+int oracle_kernel(int mode, int skf, int m, const double* r, const double* dx, const double* dy, const double* hs,
+                  double* w, double* d0, double* d1) {
+    for (int k = 0; k < m; k++) {
+        if (mode == 2) {
+            double a, b, c;
+            kernel_tools<double>(skf, r[k], dx[k], dy[k], hs[k], a, b, c);
+            w[k] = a; d0[k] = b; d1[k] = c;
+        } else {
+            float a, b, c;
+            kernel_tools<float>(skf, (float)r[k], (float)dx[k], (float)dy[k], (float)hs[k], a, b, c);
+            w[k] = a; d0[k] = b; d1[k] = c;
+        }
+    }
+    return 0;
+}
+
+/* DEM slope/curvature rows from Z (row 1 of topol). */
+int oracle_dem_topol(int mode, int deriv, int nx, int ny, double dx, double dy, double* topol) {
+    if (!topol || nx < 3 || ny < 3) return GFSPH_ERR_ARG;
+    return mode == 2 ? dem_topol_mode<double>(deriv, nx, ny, dx, dy, topol)
+                     : dem_topol_mode<float>(deriv, nx, ny, dx, dy, topol);
+}
+
+/* Depth raster: IDW of h over the 4x4 node stencil (SPH_SW_2019.f90:14310-14400,
+ * auxv(1)/auxv(5)); zero where no particle contributes. */
+int oracle_raster_idw(int nx, int ny, double xmin, double ymin, double dx, double dy, int n, const double* x,
+                      const double* rho, const int* flag, double* out) {
+    float xm = (float)xmin, ym = (float)ymin, dxg = (float)dx, dyg = (float)dy;
+    float distg = std::sqrt(dxg * dxg + dyg * dyg);
+    std::vector<float> a1((size_t)nx * ny, 0.f), a5((size_t)nx * ny, 0.f);
+    for (int i = 0; i < n; i++) {
+        if (flag[i]) continue;
+        float xx = (float)x[2 * i], yy = (float)x[2 * i + 1];
+        int ipx = (int)((xx - xm) / dxg + 1.f), ipy = (int)((yy - ym) / dyg + 1.f);
+        int x0 = std::max(1, ipx - 1), y0 = std::max(1, ipy - 1), x1 = std::min(nx, ipx + 2), y1 = std::min(ny, ipy + 2);
+        for (int ix = x0; ix <= x1; ix++)
+            for (int iy = y0; iy <= y1; iy++) {
+                int ip = (iy - 1) * nx + (ix - 1);
+                float ddx = xx - (xm + (float)(ix - 1) * dxg); ddx = ddx * ddx;
+                float ddy = yy - (ym + (float)(iy - 1) * dyg); ddy = ddy * ddy;
+                float dist = std::max(1.e-6f, std::sqrt(ddx + ddy));
+                dist = dist / distg;
+                a1[ip] = a1[ip] + (float)rho[i] / dist;
+                a5[ip] = a5[ip] + 1.f / dist;
+            }
+    }
+    for (size_t ip = 0; ip < a1.size(); ip++) out[ip] = (a5[ip] >= 1.e-6f) ? (double)(a1[ip] / a5[ip]) : (double)a1[ip];
+    return 0;
+}
+
+/* Per-node hazard sample (Get_MC_pixel_Vars_SW, SPH_SW_2019.f90:20739-20812):
+ * each in-domain particle visits the 4 nodes of its DEM cell and adds h and
+ * |v| to the sums, the count, and the maxima.  acc: (4, nx*ny) in/out:
+ * sum h, max h, sum |v|, max |v|; cnt (nx*ny) in/out. */
+int oracle_hazard_sample(int nx, int ny, double xmin, double ymin, double dx, double dy, int n, const double* x,
+                         const double* v, const double* rho, const int* flag, double* acc, int* cnt) {
+    float xm = (float)xmin, ym = (float)ymin, dxg = (float)dx, dyg = (float)dy;
+    for (int i = 0; i < n; i++) {
+        if (flag[i]) continue;
+        float xx = (float)x[2 * i], yy = (float)x[2 * i + 1];
+        int ipx = (int)((xx - xm) / dxg + 1.f), ipy = (int)((yy - ym) / dyg + 1.f);
+        if (ipx >= nx) ipx = nx - 1;
+        if (ipy >= ny) ipy = ny - 1;
+        int ip = (ipy - 1) * nx + (ipx - 1);
+        int nodes[4] = {ip, ip + 1, ip + 1 + nx, ip + nx};
+        float hh = (float)rho[i];
+        float vx = (float)v[2 * i], vy = (float)v[2 * i + 1];
+        float vv = std::sqrt(vx * vx + vy * vy);
+        for (int k = 0; k < 4; k++) {
+            int q = nodes[k];
+            cnt[q]++;
+            double* o = acc + 4 * (size_t)q;
+            o[0] = (double)((float)o[0] + hh);
+            o[2] = (double)((float)o[2] + vv);
+            if (hh > (float)o[1]) o[1] = hh;
+            if (vv > (float)o[3]) o[3] = vv;
+        }
+    }
+    return 0;
+}
+
+int oracle_version(void) { return 1; }
+
+} /* extern "C" */

@@ -1,0 +1,177 @@
+"""TEST INFRASTRUCTURE ONLY — Python binding of the CPU oracle (gfsph_oracle.cpp).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg and
+reference arm use this, as the checker or as the timed CPU baseline.
+Parity status: unpinned (the reference ships no tests or golden outputs and
+cannot be compiled here); see the header of gfsph_oracle.cpp.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libgfsph_oracle.so")
+NTOPO = 16
+
+MODE_FP32 = 0        # reference FP32 build
+MODE_FP32_DACC = 1   # FP32 state, FP64 sums (the GPU scheme)
+MODE_FP64 = 2        # reference FP64 build
+
+_lib = None
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+
+
+def build():
+    src = os.path.join(HERE, "gfsph_oracle.cpp")
+    hdr = os.path.join(HERE, "..", "include", "gfsph.h")
+    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(src), os.path.getmtime(hdr)):
+        return LIB
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.oracle_run.restype = C.c_int
+        L.oracle_run.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_int, _DP, _DP,
+                                 C.c_double, _IP]
+        L.oracle_pairs.restype = C.c_int
+        L.oracle_pairs.argtypes = [C.c_int, C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, _IP, C.c_int, _IP, _IP, _DP,
+                                   _DP]
+        L.oracle_kernel.restype = C.c_int
+        L.oracle_kernel.argtypes = [C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
+        L.oracle_dem_topol.restype = C.c_int
+        L.oracle_dem_topol.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _DP]
+        L.oracle_raster_idw.restype = C.c_int
+        L.oracle_raster_idw.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                        _DP, _DP, _IP, _DP]
+        L.oracle_hazard_sample.restype = C.c_int
+        L.oracle_hazard_sample.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                           C.c_int, _DP, _DP, _DP, _IP, _DP, _IP]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(_IP) if a is not None else None
+
+
+def dem_topol(z, dx, dy, deriv=1, mode=MODE_FP32):
+    """topol (npoig, 16) with rows 2..13 derived from Z (Get_Topol / Fdiff_derivs)."""
+    ny, nx = z.shape
+    t = np.zeros((ny * nx, NTOPO), np.float64)
+    t[:, 0] = z.reshape(-1)
+    st = lib().oracle_dem_topol(mode, deriv, nx, ny, dx, dy, _dp(t))
+    if st:
+        raise RuntimeError(f"oracle_dem_topol: {st}")
+    return t
+
+
+def initial_topol(z, dx, dy, const, deriv=1, mode=MODE_FP32):
+    """DEM rows as the reference has them before the time loop (slopes + erodible depth)."""
+    t = dem_topol(z, dx, dy, deriv, mode)
+    avail = 0.0
+    if const.get(21, 0.0) > 1e-9:
+        avail = const[48] if const.get(48, 0.0) > 1e-6 else 999.0
+    t[:, 14] = np.float32(avail)
+    return t
+
+
+class State:
+    """Particle state and DEM of an oracle run (float64 arrays)."""
+
+    def __init__(self, x, v, rho, mass, hsml, topol, flag=None, dt=0.01, t=0.0):
+        self.x, self.v = _d(x).copy(), _d(v).copy()
+        self.rho, self.mass, self.hsml = _d(rho).copy(), _d(mass).copy(), _d(hsml).copy()
+        n = self.x.shape[0]
+        self.flag = np.zeros(n, np.int32) if flag is None else np.ascontiguousarray(flag, np.int32).copy()
+        self.topol = _d(topol).copy()
+        self.dt, self.t = float(dt), float(t)
+
+    def copy(self):
+        s = State(self.x, self.v, self.rho, self.mass, self.hsml, self.topol, self.flag, self.dt, self.t)
+        return s
+
+
+def run(mode, params, nx, ny, dx, dy, state, nsteps, xmin=0.0, ymin=0.0, t_end=1e300):
+    """Advances `state` in place by nsteps reference steps; returns steps done."""
+    dt = C.c_double(state.dt)
+    t = C.c_double(state.t)
+    done = C.c_int(0)
+    st = lib().oracle_run(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol),
+                          state.x.shape[0], _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass),
+                          _dp(state.hsml), _ip(state.flag), nsteps, C.byref(dt), C.byref(t), t_end, C.byref(done))
+    if st:
+        raise RuntimeError(f"oracle_run: {st}")
+    state.dt, state.t = dt.value, t.value
+    return done.value
+
+
+def pairs(mode, params, x, hsml, mass=None, rho=None, flag=None, want_sets=True, want_rho=False,
+          want_force=False):
+    """Neighbour sets (CSR), summation density, internal forces of one state."""
+    x, hsml = _d(x), _d(hsml)
+    n = x.shape[0]
+    mass = _d(mass) if mass is not None else None
+    rho = _d(rho) if rho is not None else None
+    flag = np.zeros(n, np.int32) if flag is None else np.ascontiguousarray(flag, np.int32)
+    L = lib()
+    off = np.zeros(n + 1, np.int32) if want_sets else None
+    rho_out = np.zeros(n) if want_rho or want_force else None
+    force = np.zeros((n, 2)) if want_force else None
+    idx = None
+    if want_sets:
+        st = L.oracle_pairs(mode, C.addressof(params), n, _dp(x), _dp(hsml), _dp(mass), _dp(rho), _ip(flag), 0,
+                            _ip(off), None, None, None)
+        cap = int(off[-1])
+        idx = np.zeros(max(cap, 1), np.int32)
+    else:
+        cap = 0
+    st = L.oracle_pairs(mode, C.addressof(params), n, _dp(x), _dp(hsml), _dp(mass), _dp(rho), _ip(flag), cap,
+                        _ip(off), _ip(idx), _dp(rho_out), _dp(force))
+    if st:
+        raise RuntimeError(f"oracle_pairs: {st}")
+    return dict(offsets=off, idx=None if idx is None else idx[:cap], rho=rho_out, force=force)
+
+
+def kernel(skf, r, dx, dy, hs, mode=MODE_FP32):
+    r, dx, dy, hs = (_d(np.atleast_1d(a)) for a in (r, dx, dy, hs))
+    m = r.size
+    w, d0, d1 = np.zeros(m), np.zeros(m), np.zeros(m)
+    lib().oracle_kernel(mode, skf, m, _dp(r), _dp(dx), _dp(dy), _dp(hs), _dp(w), _dp(d0), _dp(d1))
+    return w, d0, d1
+
+
+def raster_idw(nx, ny, dx, dy, x, rho, flag, xmin=0.0, ymin=0.0):
+    out = np.zeros(nx * ny)
+    lib().oracle_raster_idw(nx, ny, xmin, ymin, dx, dy, x.shape[0], _dp(_d(x)), _dp(_d(rho)),
+                            _ip(np.ascontiguousarray(flag, np.int32)), _dp(out))
+    return out.reshape(ny, nx)
+
+
+class Hazard:
+    def __init__(self, nx, ny, dx, dy, xmin=0.0, ymin=0.0):
+        self.geom = (nx, ny, xmin, ymin, dx, dy)
+        self.acc = np.zeros((nx * ny, 4))
+        self.cnt = np.zeros(nx * ny, np.int32)
+
+    def sample(self, x, v, rho, flag):
+        nx, ny, xmin, ymin, dx, dy = self.geom
+        lib().oracle_hazard_sample(nx, ny, xmin, ymin, dx, dy, x.shape[0], _dp(_d(x)), _dp(_d(v)), _dp(_d(rho)),
+                                   _ip(np.ascontiguousarray(flag, np.int32)), _dp(self.acc), _ip(self.cnt))

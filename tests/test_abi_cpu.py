@@ -1,0 +1,73 @@
+"""The C-ABI library without a GPU: it builds, loads, exports every symbol the
+header declares, and its compute entry points refuse to run without a CUDA
+device (no CPU fallback)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "gfsph.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gfsph_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_declares_the_step_interface():
+    syms = declared_symbols()
+    for s in ("gfsph_create", "gfsph_upload", "gfsph_step", "gfsph_download", "gfsph_destroy",
+              "gfsph_raster", "gfsph_neighbours", "gfsph_density"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol(gfsph_lib):
+    L = gfsph_lib.lib()
+    for s in declared_symbols():
+        assert hasattr(L, s), s
+    assert set(declared_symbols()) <= set(gfsph_lib.SIGNATURES)
+
+
+def test_library_is_built_for_sm100a(gfsph_lib):
+    import subprocess
+    out = subprocess.run(["cuobjdump", "--list-elf", gfsph_lib.LIB_PATH], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+def test_status_strings(gfsph_lib):
+    assert gfsph_lib.strerror(0) == "ok"
+    assert "CUDA device" in gfsph_lib.strerror(-6)
+    assert gfsph_lib.lib().gfsph_version() >= 1
+
+
+def test_rejects_unsupported_options_before_touching_the_device(gfsph_lib):
+    z = np.zeros((8, 8), np.float32)
+    for bad in (dict(skf=2), dict(nor_density=1), dict(pa_sph=3)):
+        p = gfsph_lib.make_params({1: 9.8, 2: 2000, 3: 500, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01}, **bad)
+        with pytest.raises(gfsph_lib.GfsphError) as e:
+            gfsph_lib.Sim(p, z, dx=1.0, dy=1.0)
+        assert e.value.status == -4
+    p = gfsph_lib.make_params({1: 9.8, 2: 2000, 3: 500, 5: 1, 9: 0.2, 10: 0.01, 15: 0.01})  # Manning
+    with pytest.raises(gfsph_lib.GfsphError):
+        gfsph_lib.Sim(p, z, dx=1.0, dy=1.0)
+
+
+def test_no_cpu_fallback_without_device(gfsph_lib):
+    if os.path.exists("/dev/nvidia0"):
+        pytest.skip("a GPU is present")
+    p = gfsph_lib.make_params({1: 9.8, 2: 2000, 3: 500, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01})
+    with pytest.raises(gfsph_lib.GfsphError) as e:
+        gfsph_lib.Sim(p, np.zeros((8, 8), np.float32), dx=1.0, dy=1.0)
+    assert e.value.status == -6
+
+
+def test_fortran_interface_names_every_symbol():
+    src = open(os.path.join(ROOT, "deslizamientos-y-flujos_b200", "fortran", "gfsph_c.f90")).read().lower()
+    for s in declared_symbols():
+        if s in ("gfsph_set_stream",):
+            continue
+        assert f'bind(c, name="{s}")' in src, s

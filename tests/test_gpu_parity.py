@@ -1,0 +1,254 @@
+"""Parity of the CUDA step (through the C ABI) with the CPU oracle.
+
+Tolerances:
+  - neighbour sets: bit-exact as sets, against the FP32 oracle;
+  - one step, density, internal force: against the oracle in the GPU's own
+    precision scheme (FP32 state and terms, FP64 sums; oracle mode 1), where
+    the only freedom left is the order of the FP64 sums — relative error
+    <= 1e-6 (in practice 0 or 1 ulp);
+  - many steps: relative L2 of the depth field <= 1e-5 against oracle mode 1,
+    and <= 2e-4 against the FP64 oracle (the reference's own FP32 build sits
+    at ~2e-5..6e-5 from FP64 on these cases).
+"""
+import numpy as np
+import pytest
+
+import gfsph
+import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def max_rel(a, b, floor=1e-6):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
+
+
+def setup_pair(w, oracle_mod, **opts):
+    """A GPU handle and an oracle state on identical inputs (same FP32 DEM rows)."""
+    p = workloads.make_params(w, gfsph, **opts)
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv, mode=oracle_mod.MODE_FP32)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy, topol=topol.astype(np.float32))
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    st = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    return sim, st, p
+
+
+def small_channel(n=6000, k=8):
+    return workloads.fractal_channel(n_target=n, dem_k=k, cell=5.0)
+
+
+def test_neighbour_sets_bit_exact(gfsph_lib, oracle_mod):
+    rng = np.random.default_rng(11)
+    clouds = []
+    n = 4000
+    x = rng.uniform(0, 60, size=(n, 2)).astype(np.float32) + np.float32(100.0)
+    h = rng.uniform(0.5, 2.0, size=n).astype(np.float32)
+    clouds.append((x, h))
+    w = workloads.inclined_plane()
+    clouds.append((w.x, w.hsml))
+    wc = small_channel()
+    clouds.append((wc.x, wc.hsml))
+    for x, h in clouds:
+        z = np.zeros((64, 64), np.float32)
+        cell = float(np.ceil((x.max() + 10) / 63.0))
+        p = gfsph.make_params({1: 9.8, 2: 2000, 3: 500, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01})
+        sim = gfsph.Sim(p, z, dx=cell, dy=cell)
+        m = np.ones(x.shape[0], np.float32)
+        sim.upload(x, np.zeros_like(x), m, m, h)
+        sim.density()
+        off, idx = sim.neighbours()
+        ref = oracle_mod.pairs(oracle_mod.MODE_FP32, p, x, h)
+        assert np.array_equal(off, ref["offsets"])
+        assert np.array_equal(idx, ref["idx"])
+        sim.close()
+
+
+def test_density_and_internal_force_match_oracle(gfsph_lib, oracle_mod):
+    for w in (workloads.inclined_plane(), small_channel()):
+        sim, st, p = setup_pair(w, oracle_mod)
+        rho_g = sim.density()
+        ref = oracle_mod.pairs(oracle_mod.MODE_FP32_DACC, p, w.x, w.hsml, mass=w.mass, rho=w.rho,
+                               want_sets=False, want_rho=True, want_force=True)
+        assert max_rel(rho_g, ref["rho"]) <= 1e-6
+        sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+        f_g = sim.internal_forces()
+        scale = np.abs(ref["force"]).max()
+        assert np.abs(f_g - ref["force"]).max() <= 1e-6 * scale
+        sim.close()
+
+
+@pytest.mark.parametrize("case", ["plane", "channel_erosion"])
+def test_one_step_matches_oracle(gfsph_lib, oracle_mod, case):
+    w = workloads.inclined_plane() if case == "plane" else small_channel()
+    sim, st, p = setup_pair(w, oracle_mod)
+    sim.step(1)
+    g = sim.download()
+    ny, nx = w.z.shape
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, 1)
+    assert np.array_equal(g["flag"], st.flag)
+    for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass), ("hsml", st.hsml)):
+        err = max_rel(g[key], ref, floor=1e-3)
+        assert err <= 1e-6, (key, err)
+    t, dt = sim.time()
+    assert abs(dt - st.dt) <= 1e-7 * st.dt
+    sim.close()
+
+
+def test_many_steps_inclined_plane(gfsph_lib, oracle_mod):
+    w = workloads.inclined_plane()
+    sim, st1, p = setup_pair(w, oracle_mod)
+    st2 = st1.copy()
+    nsteps = 200
+    sim.step(nsteps)
+    g = sim.download()
+    ny, nx = w.z.shape
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st1, nsteps)
+    oracle_mod.run(oracle_mod.MODE_FP64, p, nx, ny, w.dx, w.dy, st2, nsteps)
+    assert rel_l2(g["rho"], st1.rho) <= 1e-5
+    assert rel_l2(g["x"], st1.x) <= 1e-6
+    assert rel_l2(g["rho"], st2.rho) <= 2e-4
+    assert np.array_equal(g["mass"], w.mass)  # no erosion: volume exactly conserved
+    sim.close()
+
+
+def test_erosion_and_dem_rows_match_oracle(gfsph_lib, oracle_mod):
+    w = small_channel()
+    sim, st, p = setup_pair(w, oracle_mod)
+    nsteps = 20
+    sim.step(nsteps)
+    g = sim.download()
+    ny, nx = w.z.shape
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+    t = st.topol.reshape(ny, nx, 16)
+    assert rel_l2(g["mass"], st.mass) <= 1e-6
+    assert rel_l2(g["rho"], st.rho) <= 1e-5
+    eroded = sim.raster(gfsph.RASTER_ERODED)
+    assert eroded.max() > 0
+    assert np.abs(eroded - t[..., 13]).max() <= 1e-6 + 1e-5 * t[..., 13].max()
+    assert np.abs(sim.raster(gfsph.RASTER_Z) - t[..., 0]).max() <= 1e-3
+    assert np.abs(sim.raster(gfsph.RASTER_AVAILABLE) - t[..., 14]).max() <= 1e-5
+    sim.close()
+
+
+def test_rasters_match_oracle(gfsph_lib, oracle_mod):
+    w = small_channel()
+    sim, st, p = setup_pair(w, oracle_mod)
+    ny, nx = w.z.shape
+    sim.hazard_reset()
+    haz = oracle_mod.Hazard(nx, ny, w.dx, w.dy)
+    for _ in range(3):
+        sim.step(5)
+        g = sim.download()
+        sim.hazard_sample()
+        haz.sample(g["x"], g["v"], g["rho"], g["flag"])
+    idw = sim.raster(gfsph.RASTER_DEPTH_IDW)
+    ref = oracle_mod.raster_idw(nx, ny, w.dx, w.dy, g["x"], g["rho"], g["flag"])
+    assert np.abs(idw - ref).max() <= 1e-5 * max(ref.max(), 1.0)
+    cnt = sim.raster(gfsph.RASTER_COUNT).reshape(-1)
+    assert np.array_equal(cnt.astype(np.int64), haz.cnt)
+    assert np.array_equal(sim.raster(gfsph.RASTER_MAX_DEPTH).reshape(-1), haz.acc[:, 1].astype(np.float32))
+    assert np.array_equal(sim.raster(gfsph.RASTER_MAX_VEL).reshape(-1), haz.acc[:, 3].astype(np.float32))
+    sh = sim.raster(gfsph.RASTER_SUM_DEPTH).reshape(-1)
+    assert np.abs(sh - haz.acc[:, 0]).max() <= 1e-5 * haz.acc[:, 0].max()
+    sim.close()
+
+
+def test_capacity_growth_gives_identical_results(gfsph_lib, oracle_mod):
+    w = small_channel()
+    sim_a, _, _ = setup_pair(w, oracle_mod)
+    sim_b, _, _ = setup_pair(w, oracle_mod, max_neighbours=4)
+    sim_a.step(6)
+    sim_b.step(6)
+    a, b = sim_a.download(), sim_b.download()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    sim_a.close()
+    sim_b.close()
+
+
+def test_runs_are_deterministic(gfsph_lib, oracle_mod):
+    w = small_channel()
+    outs = []
+    for _ in range(2):
+        sim, _, _ = setup_pair(w, oracle_mod)
+        sim.step(12)
+        outs.append(sim.download())
+        sim.close()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_t_end_stops_the_loop(gfsph_lib, oracle_mod):
+    w = workloads.inclined_plane()
+    sim, _, _ = setup_pair(w, oracle_mod)
+    st, t, done = sim.step(100, t_end=0.0499)
+    assert st == gfsph.T_END_REACHED
+    assert done == 5 and abs(t - 0.05) < 1e-6
+    sim.close()
+
+
+def test_particles_leaving_the_dem_are_frozen(gfsph_lib, oracle_mod):
+    w = workloads.inclined_plane()
+    x = w.x.copy()
+    v = w.v.copy()
+    x[0] = (0.2, 1000.0)        # next to the west edge, moving out
+    v[0] = (-30.0, 0.0)
+    sim, st, p = setup_pair(w, oracle_mod)
+    sim.upload(x, v, w.rho, w.mass, w.hsml)
+    sim.step(3)
+    g = sim.download()
+    assert g["flag"][0] == 1 and g["flag"][1:].sum() == 0
+    frozen = g["x"][0].copy()
+    sim.step(3)
+    assert np.array_equal(sim.download()["x"][0], frozen)
+    sim.close()
+
+
+def test_full_size_channel_properties(gfsph_lib, oracle_mod):
+    """The benchmark workload at full size (~200k particles, 1024^2 DEM)."""
+    w = workloads.fractal_channel()
+    sim, st, p = setup_pair(w, oracle_mod)
+    sim.step(5)
+    g = sim.download()
+    assert all(np.all(np.isfinite(g[k])) for k in ("x", "v", "rho", "mass", "hsml"))
+    assert g["mass"].sum() >= w.mass.sum()
+    off, idx = sim.neighbours()
+    counts = np.diff(off)
+    assert counts.min() > 0
+    # symmetry: j in N(i) <=> i in N(j)
+    src = np.repeat(np.arange(w.n), counts)
+    a = np.sort(src.astype(np.int64) * w.n + idx)
+    b = np.sort(idx.astype(np.int64) * w.n + src)
+    assert np.array_equal(a, b)
+    # sets equal to the FP32 oracle's at this size (positions of the 5th step)
+    sim2, _, _ = setup_pair(w, oracle_mod)
+    sim2.upload(g["x"], g["v"], g["rho"], g["mass"], g["hsml"])
+    sim2.density()
+    off2, idx2 = sim2.neighbours()
+    ref = oracle_mod.pairs(oracle_mod.MODE_FP32, p, g["x"], g["hsml"])
+    assert np.array_equal(off2, ref["offsets"]) and np.array_equal(idx2, ref["idx"])
+    sim.close()
+    sim2.close()
+
+
+def test_profile_counts_launches(gfsph_lib, oracle_mod):
+    w = small_channel()
+    sim, _, _ = setup_pair(w, oracle_mod)
+    n0 = sim.launch_count()
+    sim.step(16)
+    per_step = (sim.launch_count() - n0) / 16
+    assert per_step >= 14
+    sim.profile(True)
+    sim.step(4)
+    prof = sim.profile_read()
+    assert prof["k_force_rk"][1] == 4 and prof["k_density"][1] == 4
+    assert all(ms >= 0 for ms, _ in prof.values())
+    sim.close()

@@ -1,0 +1,211 @@
+"""Known-answer tests that pin the CPU oracle (no GPU).
+
+The reference ships no tests, fixtures or golden outputs, so the oracle is
+pinned by answers that follow from the mathematics the reference implements:
+kernel normalisation and gradient consistency, exact slopes of a plane,
+neighbour sets against a brute-force search, zero interior force on a still
+layer, the infinite-slope Voellmy and Bingham terminal velocities, and volume
+conservation without erosion.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import gfsph
+import workloads
+
+
+def params(const=None, **kw):
+    c = {1: 9.8, 2: 2000.0, 3: 500.0, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01}
+    if const:
+        c.update(const)
+    return gfsph.make_params(c, **kw)
+
+
+@pytest.mark.parametrize("skf", [1, 4])
+def test_kernel_normalisation_and_gradient(oracle_mod, skf):
+    hs = 1.3
+    g = np.linspace(-2.7, 2.7, 541)
+    X, Y = np.meshgrid(g, g)
+    r = np.hypot(X, Y).ravel()
+    w, d0, d1 = oracle_mod.kernel(skf, r, X.ravel(), Y.ravel(), np.full(r.size, hs), mode=oracle_mod.MODE_FP64)
+    cell = (g[1] - g[0]) ** 2
+    assert abs(w.sum() * cell - 1.0) < 2e-3
+    # gradient = derivative of W along the offset (central differences in r)
+    rr = np.linspace(0.05, 2 * hs - 0.05, 200)
+    e = 1e-6
+    wp, _, _ = oracle_mod.kernel(skf, rr + e, rr + e, 0 * rr, hs + 0 * rr, mode=oracle_mod.MODE_FP64)
+    wm, _, _ = oracle_mod.kernel(skf, rr - e, rr - e, 0 * rr, hs + 0 * rr, mode=oracle_mod.MODE_FP64)
+    _, gx, gy = oracle_mod.kernel(skf, rr, rr, 0 * rr, hs + 0 * rr, mode=oracle_mod.MODE_FP64)
+    fd = (wp - wm) / (2 * e)
+    assert np.allclose(gx, fd, rtol=1e-5, atol=1e-7)
+    assert np.all(gy == 0)
+    # compact support 2h
+    w2, a, b = oracle_mod.kernel(skf, np.array([2 * hs * 1.0001]), np.array([2 * hs * 1.0001]), np.zeros(1),
+                                 np.array([hs]))
+    assert w2[0] == 0 and a[0] == 0
+
+
+def test_dem_slopes_exact_on_a_plane(oracle_mod):
+    ny, nx, d = 40, 50, 5.0
+    yy, xx = np.mgrid[0:ny, 0:nx] * d
+    z = 0.3 * xx - 0.7 * yy + 100.0
+    for deriv in (0, 1):
+        t = oracle_mod.dem_topol(z, d, d, deriv=deriv, mode=oracle_mod.MODE_FP64).reshape(ny, nx, 16)
+        inner = t[1:-1, 1:-1] if deriv == 1 else t
+        assert np.allclose(inner[..., 1], 0.3, atol=1e-9)
+        assert np.allclose(inner[..., 2], -0.7, atol=1e-9)
+        assert np.allclose(inner[..., 6:9], 0.0, atol=1e-9)
+
+
+def test_dem_topol_library_matches_oracle(oracle_mod):
+    """The library's host DEM set-up (no GPU needed) against the oracle's."""
+    rng = np.random.default_rng(7)
+    z = rng.normal(size=(33, 41)).cumsum(axis=0).astype(np.float32)
+    for deriv in (0, 1):
+        a = gfsph.dem_topol(z, 5.0, 5.0, mode=deriv).astype(np.float64)
+        b = oracle_mod.dem_topol(z, 5.0, 5.0, deriv=deriv, mode=oracle_mod.MODE_FP32)
+        assert np.allclose(a[:, :13], b[:, :13], rtol=2e-5, atol=2e-5)
+
+
+def brute_force_sets(x, h):
+    """O(N^2) neighbour sets with the reference's FP32 operations."""
+    x = x.astype(np.float32)
+    h = h.astype(np.float32)
+    n = x.shape[0]
+    sets = []
+    for i in range(n):
+        d0 = (x[i, 0] - x[:, 0]).astype(np.float32)
+        d1 = (x[i, 1] - x[:, 1]).astype(np.float32)
+        dr = (d0 * d0).astype(np.float32)
+        dr = (dr + (d1 * d1).astype(np.float32)).astype(np.float32)
+        mh = ((h[i] + h) / np.float32(2)).astype(np.float32)
+        r = np.sqrt(dr).astype(np.float32)
+        m = r < (np.float32(2) * mh)
+        m[i] = False
+        sets.append(np.nonzero(m)[0])
+    return sets
+
+
+@pytest.mark.parametrize("nnps", [2, 4])
+def test_neighbour_sets_match_brute_force(oracle_mod, nnps):
+    rng = np.random.default_rng(3)
+    n = 700
+    x = rng.uniform(0, 40, size=(n, 2)).astype(np.float32)
+    x[:, 1] = x[:, 1] * 0.4 + 0.3 * x[:, 0]          # elongated, rotated cloud
+    h = rng.uniform(0.6, 1.6, size=n).astype(np.float32)
+    p = params(nnps=nnps)
+    res = oracle_mod.pairs(0, p, x, h)
+    ref = brute_force_sets(x, h)
+    off, idx = res["offsets"], res["idx"]
+    for i in range(n):
+        assert np.array_equal(np.sort(idx[off[i]:off[i + 1]]), ref[i]), i
+
+
+def test_still_layer_interior_force_is_zero(oracle_mod):
+    s = 1.0
+    n = 30
+    g = np.arange(n) * s
+    X, Y = np.meshgrid(g, g)
+    x = np.stack([X.ravel(), Y.ravel()], 1)
+    h0 = 2.0
+    mass = np.full(n * n, s * s * h0)
+    hsml = np.full(n * n, 2 * s)
+    p = params()
+    res = oracle_mod.pairs(oracle_mod.MODE_FP64, p, x, hsml, mass=mass, rho=np.full(n * n, h0), want_force=True)
+    f = res["force"].reshape(n, n, 2)
+    inner = f[6:-6, 6:-6]
+    assert np.abs(inner).max() < 1e-9
+    edge = np.abs(f[0, n // 2]).max()
+    assert edge > 1e-3  # the free edge is pushed outwards
+
+
+def single_particle_run(oracle_mod, const, tan_theta, steps, dt, sle=0, mode=2):
+    nx, ny, d = 20, 1200, 5.0
+    yy = np.arange(ny)[:, None] * d * np.ones((1, nx))
+    z = (ny * d - yy) * tan_theta
+    p = params(const, sle=sle, dt=dt, ic_adapt=0, average_velocity=0)
+    topol = oracle_mod.initial_topol(z, d, d, {}, deriv=1, mode=mode)
+    hs = 2.0
+    m = 4.0
+    st = oracle_mod.State(np.array([[50.0, 100.0]]), np.zeros((1, 2)), np.array([1.0]), np.array([m]),
+                          np.array([hs]), topol, dt=dt)
+    oracle_mod.run(mode, p, nx, ny, d, d, st, steps)
+    w0 = 15.0 / (7.0 * math.pi * hs * hs) * (2.0 / 3.0)
+    return st, w0 * m
+
+
+def test_voellmy_terminal_velocity_on_infinite_slope(oracle_mod):
+    tan_t, mu, xi = 0.5, 0.2, 500.0
+    st, h = single_particle_run(oracle_mod, {3: xi, 9: mu}, tan_t, 1500, 0.02)
+    vt = math.sqrt(xi * h * (tan_t - mu))
+    v = np.hypot(*st.v[0])
+    assert abs(v - vt) / vt < 2e-3, (v, vt)
+    assert abs(st.v[0, 0]) < 1e-9  # moves straight down the fall line
+
+
+def test_bingham_viscous_terminal_velocity(oracle_mod):
+    tan_t, K, tau = 0.5, 1000.0, 1e-3
+    st, h = single_particle_run(oracle_mod, {5: 4, 6: tau, 7: K, 3: 0.0, 9: 0.0}, tan_t, 1500, 0.02)
+    vt = 9.8 * tan_t * 2000.0 * h * h / (3.0 * K)
+    v = np.hypot(*st.v[0])
+    assert abs(v - vt) / vt < 2e-3, (v, vt)
+
+
+def test_volume_conserved_without_erosion(oracle_mod):
+    w = workloads.inclined_plane()
+    p = workloads.make_params(w, gfsph)
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const)
+    st = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=0.01)
+    oracle_mod.run(1, p, nx, ny, w.dx, w.dy, st, 20)
+    assert np.array_equal(st.mass, w.mass.astype(np.float64))
+    assert np.all(np.isfinite(st.x)) and st.flag.sum() == 0
+    # the cap has started to slide down the 30 degree plane (+y)
+    assert st.v[:, 1].mean() > 0.5
+
+
+def test_erosion_moves_volume_from_dem_to_flow(oracle_mod):
+    w = workloads.fractal_channel(n_target=3000, dem_k=7, cell=5.0)
+    p = workloads.make_params(w, gfsph)
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const)
+    st = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=0.01)
+    oracle_mod.run(1, p, nx, ny, w.dx, w.dy, st, 30)
+    t = st.topol.reshape(ny, nx, 16)
+    assert st.mass.sum() > w.mass.sum()
+    assert t[..., 13].max() > 0                       # eroded depth recorded
+    assert np.all(t[..., 14] >= 0) and np.all(t[..., 14] <= 2.0)
+    assert np.allclose(t[..., 0] + t[..., 13], w.z, atol=1e-3)  # Z lowered by exactly the eroded depth
+
+
+def test_fp32_and_fp64_oracles_agree_closely(oracle_mod):
+    w = workloads.inclined_plane()
+    p = workloads.make_params(w, gfsph)
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const)
+    out = {}
+    for mode in (0, 1, 2):
+        st = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=0.01)
+        oracle_mod.run(mode, p, nx, ny, w.dx, w.dy, st, 40)
+        out[mode] = st
+    # The reference's own FP32 arithmetic sits ~2e-5 (relative L2 of depth)
+    # away from its FP64 rebuild after 40 steps on this case; FP64 sums alone
+    # do not close that gap (it comes from FP32 positions and kernel values).
+    for mode in (0, 1):
+        rel = np.linalg.norm(out[mode].rho - out[2].rho) / np.linalg.norm(out[2].rho)
+        assert rel < 1e-4, (mode, rel)
+
+
+def test_workload_generators():
+    w = workloads.fractal_channel()
+    assert 190_000 < w.n < 210_000
+    assert w.z.shape == (1024, 1024)
+    assert abs(w.rho.mean() - 4.0) < 0.05
+    assert np.all(w.mass > 0) and np.all(w.hsml > 0)
+    # release inside the DEM box and on the downhill side of the channel head
+    assert w.x[:, 0].min() > 0 and w.x[:, 0].max() < 1023 * w.dx
+    w1 = workloads.inclined_plane()
+    assert 1800 < w1.n < 2100
+    assert abs(w1.rho.max() - 10.0) < 0.2
