@@ -99,68 +99,75 @@ def dist_setup(n_gpus):
     return rank, world, local
 
 
-_REF_CASE = None
-
-
-def cpu_reference_rate(seconds_budget, mode=0):
-    """The reference path on the host (FP32 oracle port, one thread) on a
-    bounded sample of the workload: a scaled-down release on the same DEM
-    shape; returns (particle-steps/s, description)."""
+def _oracle_case(n_target=20_000):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import gfsph
     import oracle
     import workloads
-    global _REF_CASE
-    if _REF_CASE is None:
-        w = workloads.fractal_channel(n_target=20_000)
-        p = workloads.make_params(w, gfsph)
-        _REF_CASE = (w, p, oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv))
-    w, p, topol = _REF_CASE
-    ny, nx = w.z.shape
-    st = oracle.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
-    t0 = time.perf_counter()
-    oracle.run(mode, p, nx, ny, w.dx, w.dy, st, 1)
-    one = max(time.perf_counter() - t0, 1e-3)
-    steps = max(1, min(200, int(seconds_budget / one)))
-    t0 = time.perf_counter()
-    oracle.run(mode, p, nx, ny, w.dx, w.dy, st, steps)
-    el = time.perf_counter() - t0
-    desc = (f"{steps} steps of the fractal-channel workload with a {w.n}-particle release (same DEM, "
-            f"same physics) on 1 host thread, oracle mode FP32")
-    return w.n * steps / el, steps, w.n, el, desc
-
-
-def run_reference_arm(args, rank, world):
-    """The reference's CPU path (the FP32 oracle port; the Fortran reference
-    cannot be built here) on the host, one thread, each bench step a bounded
-    sample of oracle steps so the whole run stays within a few minutes."""
-    if rank != 0:
-        return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import gfsph
-    import oracle
-    import workloads
-    w = workloads.fractal_channel(n_target=20_000)
+    w = workloads.fractal_channel(n_target=n_target)
     p = workloads.make_params(w, gfsph)
     topol = oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv)
     ny, nx = w.z.shape
     st = oracle.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    return oracle, w, p, nx, ny, st
+
+
+def cpu_reference_rate(seconds_budget, warm_steps=20):
+    """The reference path on the host (the FP32 oracle port, one thread) on a
+    bounded sample of the workload: the same DEM and physics with a
+    20k-particle release, timed over the same early phase of the flow as the
+    GPU measurement.  Returns (particle-steps/s, steps, n, seconds, sample)."""
+    oracle, w, p, nx, ny, st = _oracle_case()
+    run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st)
+    run.advance(warm_steps)
     t0 = time.perf_counter()
-    oracle.run(0, p, nx, ny, w.dx, w.dy, st, 1)
+    run.advance(1)
     one = max(time.perf_counter() - t0, 1e-4)
-    per = max(1, int(150.0 / max(args.steps + args.warmup, 1) / one))
-    for _ in range(args.warmup):
-        oracle.run(0, p, nx, ny, w.dx, w.dy, st, per)
+    steps = max(1, min(400, int(seconds_budget / one)))
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        oracle.run(0, p, nx, ny, w.dx, w.dy, st, per)
+    run.advance(steps)
     el = time.perf_counter() - t0
-    value = w.n * per * args.steps / el
-    desc = (f"{per} oracle steps per bench step of the fractal-channel workload with a {w.n}-particle "
-            f"release (same DEM and physics), FP32, 1 host thread")
+    run.close()
+    desc = (f"steps {warm_steps + 2}..{warm_steps + 1 + steps} of the fractal-channel workload with a "
+            f"{w.n}-particle release (same DEM and physics), FP32 oracle port, 1 host thread")
+    return w.n * steps / el, steps, w.n, el, desc
+
+
+def run_reference_arm(args, rank, world):
+    """The reference's CPU path (the FP32 oracle port: the Fortran reference
+    cannot be built here), one host thread.  Each bench step is a bounded
+    sample of oracle steps, restarted from the same early-flow state, so the
+    whole run stays within a few minutes."""
+    if rank != 0:
+        return 0
+    oracle, w, p, nx, ny, st = _oracle_case()
+    warm = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st)
+    warm.advance(20)
+    snap = warm.state(with_topol=True)
+    warm.close()
+    run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, snap)
+    t0 = time.perf_counter()
+    run.advance(1)
+    one = max(time.perf_counter() - t0, 1e-4)
+    run.close()
+    per = max(1, min(100, int(120.0 / max(args.steps + args.warmup, 1) / one)))
+    total_steps = 0
+    el = 0.0
+    for k in range(args.warmup + args.steps):
+        run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, snap)
+        t0 = time.perf_counter()
+        run.advance(per)
+        dt_ = time.perf_counter() - t0
+        run.close()
+        if k >= args.warmup:
+            el += dt_
+            total_steps += per
+    value = w.n * total_steps / el
+    desc = (f"{per} oracle steps per bench step from the state after 20 steps of the fractal-channel workload "
+            f"with a {w.n}-particle release (same DEM and physics), FP32, 1 host thread")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / (args.steps * per),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "fractal_channel: 1024^2 DEM at 5 m, elliptical release (bounded sample)",
                    "parallelism": "single host thread (the reference is single-threaded)"},

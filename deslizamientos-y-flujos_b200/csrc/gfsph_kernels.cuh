@@ -130,8 +130,15 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
     }
     float deltx = hmx * 2.f;
     float lx = xmx - xmn, ly = ymx - ymn;
-    int ndx = (int)(lx / deltx + 1.f);
-    int ndy = (int)(ly / deltx + 1.f);
+    float fx = lx / deltx + 1.f, fy = ly / deltx + 1.f;
+    if (!(fx < 1.0e8f) || !(fy < 1.0e8f) || !(fx * fy < 2.0e9f)) {  // far beyond any capacity
+        S->err |= kErrCells;
+        S->need_cells = 0x3fffffff;
+        S->skip = 1;
+        return;
+    }
+    int ndx = (int)fx;
+    int ndy = (int)fy;
     float lxn = (float)ndx * deltx, lyn = (float)ndy * deltx;
     S->gx0 = (xmn - (lxn - lx) / 2.f) - 0.001f * lx;
     S->gy0 = (ymn - (lyn - ly) / 2.f) - 0.001f * ly;

@@ -656,6 +656,71 @@ struct Oracle {
     }
 };
 
+struct OracleBase {
+    virtual ~OracleBase() {}
+    virtual int advance(int nsteps, double t_end) = 0;
+    virtual void get(double* x, double* v, double* rho, double* mass, double* hsml, int* flag, double* dt,
+                     double* t, double* topol) = 0;
+};
+
+template <class R, class A>
+struct OracleObj : OracleBase {
+    Oracle<R, A> o;
+    gfsph_params params;
+    int advance(int nsteps, double t_end) override {
+        int done = 0;
+        for (int s = 0; s < nsteps; s++) {
+            if (o.time >= t_end) break;
+            o.step();
+            done++;
+        }
+        return done;
+    }
+    void get(double* x, double* v, double* rho, double* mass, double* hsml, int* flag, double* dt, double* t,
+             double* topol) override {
+        int n = o.n;
+        for (size_t k = 0; k < 2 * (size_t)n; k++) {
+            if (x) x[k] = (double)o.x[k];
+            if (v) v[k] = (double)o.v[k];
+        }
+        for (int k = 0; k < n; k++) {
+            if (rho) rho[k] = (double)o.rho[k];
+            if (mass) mass[k] = (double)o.mass[k];
+            if (hsml) hsml[k] = (double)o.hsml[k];
+            if (flag) flag[k] = o.flag[k];
+        }
+        if (topol)
+            for (size_t k = 0; k < o.topol.size(); k++) topol[k] = (double)o.topol[k];
+        if (dt) *dt = (double)o.dt;
+        if (t) *t = o.time;
+    }
+};
+
+template <class R, class A>
+OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+                     const double* topol, int n, const double* x, const double* v, const double* rho,
+                     const double* mass, const double* hsml, const int* flag, double dt, double t, int* status) {
+    OracleObj<R, A>* ob = new OracleObj<R, A>();
+    ob->params = *p;
+    Oracle<R, A>& o = ob->o;
+    int st = o.setup(&ob->params, nx, ny, xmin, ymin, dx, dy, topol);
+    if (st) { delete ob; *status = st; return nullptr; }
+    o.n = n;
+    auto cp = [&](std::vector<R>& dst, const double* src, size_t m) {
+        dst.resize(m);
+        for (size_t k = 0; k < m; k++) dst[k] = (R)src[k];
+    };
+    cp(o.x, x, 2 * (size_t)n); cp(o.v, v, 2 * (size_t)n);
+    cp(o.rho, rho, n); cp(o.mass, mass, n); cp(o.hsml, hsml, n);
+    o.flag.assign(flag, flag + n);
+    o.p.assign(n, (R)0);
+    o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
+    o.dt = (R)dt;
+    o.time = t;
+    *status = 0;
+    return ob;
+}
+
 template <class R, class A>
 int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
              double* topol, int n, double* x, double* v, double* rho, double* mass, double* hsml, int* flag,
@@ -887,6 +952,34 @@ int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, dou
     default: return GFSPH_ERR_ARG;
     }
 }
+
+/* Persistent oracle run: create on a state, advance, read back, free. */
+void* oracle_new(int mode, const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+                 const double* topol, int n, const double* x, const double* v, const double* rho,
+                 const double* mass, const double* hsml, const int* flag, double dt, double t, int* status) {
+    *status = GFSPH_ERR_ARG;
+    if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || n < 0 || nx < 2 || ny < 2) return nullptr;
+    if (p->summation_density != 1 || p->nor_density != 0) { *status = GFSPH_ERR_UNSUPPORTED; return nullptr; }
+    switch (mode) {
+    case 0: return make_obj<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, dt, t, status);
+    case 1: return make_obj<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, dt, t, status);
+    case 2: return make_obj<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, dt, t, status);
+    default: return nullptr;
+    }
+}
+
+int oracle_advance(void* h, int nsteps, double t_end) {
+    return h ? static_cast<OracleBase*>(h)->advance(nsteps, t_end) : GFSPH_ERR_ARG;
+}
+
+int oracle_get(void* h, double* x, double* v, double* rho, double* mass, double* hsml, int* flag, double* dt,
+               double* t, double* topol) {
+    if (!h) return GFSPH_ERR_ARG;
+    static_cast<OracleBase*>(h)->get(x, v, rho, mass, hsml, flag, dt, t, topol);
+    return 0;
+}
+
+void oracle_free(void* h) { delete static_cast<OracleBase*>(h); }
 
 /* Neighbour sets (CSR, sorted), summation density and internal forces of the
  * reference on one state. Any of offsets/rho_out/indvxdt may be NULL. */

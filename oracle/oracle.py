@@ -56,6 +56,16 @@ def lib():
         L.oracle_hazard_sample.restype = C.c_int
         L.oracle_hazard_sample.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                            C.c_int, _DP, _DP, _DP, _IP, _DP, _IP]
+        L.oracle_new.restype = C.c_void_p
+        L.oracle_new.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_double, C.c_double,
+                                 _IP]
+        L.oracle_advance.restype = C.c_int
+        L.oracle_advance.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.oracle_get.restype = C.c_int
+        L.oracle_get.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP, _DP, _IP, _DP, _DP, _DP]
+        L.oracle_free.restype = None
+        L.oracle_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -175,3 +185,44 @@ class Hazard:
         nx, ny, xmin, ymin, dx, dy = self.geom
         lib().oracle_hazard_sample(nx, ny, xmin, ymin, dx, dy, x.shape[0], _dp(_d(x)), _dp(_d(v)), _dp(_d(rho)),
                                    _ip(np.ascontiguousarray(flag, np.int32)), _dp(self.acc), _ip(self.cnt))
+
+
+class Run:
+    """A persistent oracle run: the state stays inside the oracle between
+    advance() calls, so timing advance() measures only the steps."""
+
+    def __init__(self, mode, params, nx, ny, dx, dy, state, xmin=0.0, ymin=0.0):
+        self.params = params
+        self.n = state.x.shape[0]
+        self.topol_shape = state.topol.shape
+        stv = C.c_int(0)
+        self.h = lib().oracle_new(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), self.n,
+                                  _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.hsml),
+                                  _ip(state.flag), state.dt, state.t, C.byref(stv))
+        if not self.h:
+            raise RuntimeError(f"oracle_new: {stv.value}")
+
+    def advance(self, nsteps, t_end=1e300):
+        return lib().oracle_advance(self.h, nsteps, t_end)
+
+    def state(self, with_topol=False):
+        n = self.n
+        x, v = np.zeros((n, 2)), np.zeros((n, 2))
+        rho, mass, hsml = np.zeros(n), np.zeros(n), np.zeros(n)
+        flag = np.zeros(n, np.int32)
+        dt, t = C.c_double(), C.c_double()
+        topol = np.zeros(self.topol_shape) if with_topol else None
+        lib().oracle_get(self.h, _dp(x), _dp(v), _dp(rho), _dp(mass), _dp(hsml), _ip(flag), C.byref(dt), C.byref(t),
+                         _dp(topol))
+        return State(x, v, rho, mass, hsml, topol if with_topol else np.zeros(1), flag, dt.value, t.value)
+
+    def close(self):
+        if self.h:
+            lib().oracle_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
