@@ -203,10 +203,10 @@ int enqueue_search(gfsph_handle* h, int advance) {
     int pb = blocks_for(n);
     int nscan = (h->cap_cells + kScanTile - 1) / kScanTile;
     launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++;
-    launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, S); }); nk++;
+    launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
     launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_cells); }); nk++;
     launch(h, K_CLEAR, [&] { k_clear_cells<<<148 * 4, 256, 0, st>>>(h->count, S); }); nk++;
-    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, S, h->count, h->keyrank); }); nk++;
+    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->count, h->keyrank); }); nk++;
     launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, S); }); nk++;

@@ -21,7 +21,8 @@ constexpr int kErrEmpty = 8;
 struct StepScalars {
     double time;      // time_sph
     double t_end;
-    float dt;         // dt_sph
+    float dt;         // dt_sph, committed at the end of a completed step
+    float dt_step;    // dt of the step in flight (a step stopped by a capacity error leaves dt unchanged)
     int skip;         // this step does nothing (time >= t_end or an error)
     int err;          // sticky error bits
     int steps_done;
@@ -70,10 +71,12 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
-// Bounds of the active particles and max(hsml) (grid_find :906-919 /
-// :1150-1165) and the stability time step of Adaptive_dt_sph_SW
-// (SPH_SW_2019.f90:6537-6567): min hsml/(3 max(1e-6, sqrt(g h))) [+|v|].
-__global__ void k_bounds(const PState B, int n, Rheo c, StepScalars* S) {
+// The stability time step of Adaptive_dt_sph_SW (SPH_SW_2019.f90:6537-6567,
+// min hsml/(3 max(1e-6, sqrt(g h))) [+|v|]) over the particles not yet
+// flagged; then the Check_Out_Domain at the start of time_integration_sph
+// (SPH_MAIN_2019.f90:232, :1764-1788) and, over the particles still inside,
+// the bounds and max(hsml) of the cell grid (grid_find :906-919 / :1150-1165).
+__global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
     if (step_skipped(S)) return;
     float xmn = 3.4e38f, xmx = -3.4e38f, ymn = 3.4e38f, ymx = -3.4e38f, hmx = 0.f, dtm = 1.e10f;
     int bad = 0;
@@ -84,9 +87,13 @@ __global__ void k_bounds(const PState B, int n, Rheo c, StepScalars* S) {
         float h = B.rho[i];
         float2 v = B.vel[i];
         if (!(isfinite(p.x) && isfinite(p.y) && isfinite(hs) && isfinite(h) && isfinite(v.x) && isfinite(v.y))) bad = 1;
-        xmn = fminf(xmn, p.x); xmx = fmaxf(xmx, p.x);
-        ymn = fminf(ymn, p.y); ymx = fmaxf(ymx, p.y);
-        hmx = fmaxf(hmx, hs);
+        bool out = out_of_box(dem, p.x, p.y);
+        if (out && S->advance) B.flag[i] = 1;
+        if (!out) {
+            xmn = fminf(xmn, p.x); xmx = fmaxf(xmx, p.x);
+            ymn = fminf(ymn, p.y); ymx = fmaxf(ymx, p.y);
+            hmx = fmaxf(hmx, hs);
+        }
         if (c.ic_adapt == 1 || c.ic_adapt == 2) {
             float hh = (h < c.h_inf) ? c.h_inf : h;
             float cs = sqrtf(c.g * hh);
@@ -121,13 +128,13 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
     float xmn = o2f(S->xmin_o), xmx = o2f(S->xmax_o), ymn = o2f(S->ymin_o), ymx = o2f(S->ymax_o);
     float hmx = o2f(S->hmax_o);
     if (S->xmin_o == 0xffffffffu || !(hmx > 0.f)) { S->err |= kErrEmpty; S->skip = 1; return; }
+    float dt = S->dt;
     if (S->advance) {
         float dtmin = (c.ic_adapt == 1 || c.ic_adapt == 2) ? o2f(S->dtmin_o) : 1.e10f;
-        float dt = S->dt;
         if (dtmin < dt) dt = dtmin;
         else if (c.ic_adapt != 0) dt = fminf(1.1f * dt, dtmin);
-        S->dt = dt;
     }
+    S->dt_step = dt;
     float deltx = hmx * 2.f;
     float lx = xmx - xmn, ly = ymx - ymn;
     float fx = lx / deltx + 1.f, fy = ly / deltx + 1.f;
@@ -166,14 +173,14 @@ __global__ void k_clear_cells(int* count, const StepScalars* S) {
 
 // Cell key and within-cell arrival rank of each particle (counting sort
 // histogram, grid_find :938-948).  Out-of-domain particles get key -1.
-__global__ void k_hist(const PState B, int n, StepScalars* S, int* count, int2* keyrank) {
+__global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* count, int2* keyrank) {
     if (S->skip) return;
     float gx0 = S->gx0, gy0 = S->gy0, gd = S->gd;
     int ndx = S->ndx, ndy = S->ndy;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int2 kr = make_int2(-1, 0);
-        if (!B.flag[i]) {
-            float2 p = B.pos[i];
+        float2 p = B.pos[i];
+        if (!B.flag[i] && !out_of_box(dem, p.x, p.y)) {
             int ix = (int)((p.x - gx0) / gd + 1.f);
             int iy = (int)((p.y - gy0) / gd + 1.f);
             ix = min(max(ix, 1), ndx);
@@ -434,7 +441,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, const float* pterm, 
                                                    float2* indv_out) {
     if (S->skip) return;
     const int nact = S->nactive;
-    const float dt = S->dt;
+    const float dt = S->dt_step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (i >= nact) {  // carried particles (out of the domain at step start)
             if (!forces_only) {
@@ -580,6 +587,7 @@ __global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail
 __global__ void k_step_end(StepScalars* S) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (S->skip || !S->advance) return;
+    S->dt = S->dt_step;
     S->time += (double)S->dt;
     S->steps_done += 1;
 }

@@ -251,8 +251,9 @@ class Sim:
     def set_stream(self, stream_ptr):
         _check(lib().gfsph_set_stream(self.h, C.c_void_p(stream_ptr)), "gfsph_set_stream")
 
-    def profile(self, on):
-        _check(lib().gfsph_profile(self.h, 1 if on else 0), "gfsph_profile")
+    def profile(self, level):
+        """0 off, 1 per-kernel events, 2 events around each step call."""
+        _check(lib().gfsph_profile(self.h, int(level)), "gfsph_profile")
 
     def profile_read(self):
         L = lib()

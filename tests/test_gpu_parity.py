@@ -252,3 +252,21 @@ def test_profile_counts_launches(gfsph_lib, oracle_mod):
     assert prof["k_force_rk"][1] == 4 and prof["k_density"][1] == 4
     assert all(ms >= 0 for ms, _ in prof.values())
     sim.close()
+
+
+def test_release_outside_the_dem_box_is_flagged_at_the_first_step(gfsph_lib, oracle_mod):
+    """Check_Out_Domain at the start of time_integration_sph: a release that
+    overhangs the DEM box loses the overhanging particles before the search."""
+    w = workloads.fractal_channel(n_target=4000, dem_k=7, cell=5.0)
+    assert (w.x[:, 1] < 0).any()
+    sim, st, p = setup_pair(w, oracle_mod)
+    sim.step(2)
+    g = sim.download()
+    ny, nx = w.z.shape
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, 2)
+    assert np.array_equal(g["flag"], st.flag)
+    out = w.x[:, 1] < 0
+    assert g["flag"][out].all()
+    assert np.array_equal(g["x"][out], w.x[out])
+    assert max_rel(g["x"], st.x, floor=1e-3) <= 1e-6
+    sim.close()
