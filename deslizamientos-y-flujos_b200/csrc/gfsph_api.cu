@@ -18,14 +18,16 @@ namespace {
 
 enum KernelId {
     K_PREP, K_BOUNDS, K_GRID, K_CLEAR, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
-    K_REORDER, K_DENSITY, K_FORCE_RK, K_XSPH, K_DEM_ERODE, K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD,
+    K_BIG_SORT, K_REORDER, K_DENSITY, K_DENSITY_BIG, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
+    K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
 const char* kKernelNames[K_COUNT] = {
     "k_prep", "k_bounds", "k_grid", "k_clear_cells", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
-    "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_force_rk", "k_xsph", "k_dem_erode", "k_step_end",
-    "k_copy_state", "k_unsort", "k_raster_idw", "k_hazard", "step_batches"};
+    "k_scatter", "k_cell_sort", "k_big_sort", "k_reorder", "k_density", "k_density_big", "k_force_big",
+    "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
+    "k_raster_idw", "k_hazard", "k_export_big", "step_batches"};
 
 constexpr int kThreads = 128;
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
@@ -117,9 +119,14 @@ struct gfsph_handle {
     int2* keyrank = nullptr;
     int* perm = nullptr;
     float2* f2tmp = nullptr;
+    float4* xhm = nullptr;
     int* nbr = nullptr;
     int* ncount = nullptr;
     int kcap = 0;
+    // big list
+    float2* indv_big = nullptr;
+    int* bigtmp = nullptr;
+    int big_cap = 0;
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -193,12 +200,28 @@ int profile_collect(gfsph_handle* h) {
     return 0;
 }
 
+Search make_search(gfsph_handle* h) {
+    Search q;
+    q.start = h->start;
+    q.cellA = h->cellA;
+    q.xhm = h->xhm;
+    q.nbr = h->nbr;
+    q.ncount = h->ncount;
+    q.pterm = h->pterm;
+    q.indv_big = h->indv_big;
+    q.kcap = h->kcap;
+    return q;
+}
+
+int big_blocks(const gfsph_handle* h) { return std::max(1, std::min(h->big_cap, 148 * 2)); }
+
 // The cell search: bounds, grid, counting sort, reorder, neighbours+density.
 // Returns the number of kernels enqueued.
 int enqueue_search(gfsph_handle* h, int advance) {
     const int n = h->n;
     cudaStream_t st = h->stream;
     StepScalars* S = h->S;
+    Search q = make_search(h);
     int nk = 0;
     int pb = blocks_for(n);
     int nscan = (h->cap_cells + kScanTile - 1) / kScanTile;
@@ -206,16 +229,18 @@ int enqueue_search(gfsph_handle* h, int advance) {
     launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
     launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_cells); }); nk++;
     launch(h, K_CLEAR, [&] { k_clear_cells<<<148 * 4, 256, 0, st>>>(h->count, S); }); nk++;
-    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->count, h->keyrank); }); nk++;
+    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->count, h->keyrank, h->big_cap); }); nk++;
     launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, S); }); nk++;
     launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, S, h->perm); }); nk++;
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, S); }); nk++;
-    launch(h, K_REORDER, [&] { k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, S); }); nk++;
-    launch(h, K_DENSITY, [&] {
-        k_density<<<pb, kThreads, 0, st>>>(h->A, h->cellA, h->start, S, h->rheo, n, h->kcap, h->nbr, h->ncount, h->pterm);
+    launch(h, K_BIG_SORT, [&] { k_big_sort<<<1, 1024, 0, st>>>(h->perm, h->B.id, h->bigtmp, S); }); nk++;
+    launch(h, K_REORDER, [&] {
+        k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S);
     }); nk++;
+    launch(h, K_DENSITY, [&] { k_density<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
+    launch(h, K_DENSITY_BIG, [&] { k_density_big<<<big_blocks(h), 256, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
     return nk;
 }
 
@@ -223,15 +248,16 @@ int enqueue_step(gfsph_handle* h) {
     const int n = h->n;
     cudaStream_t st = h->stream;
     StepScalars* S = h->S;
+    Search q = make_search(h);
     int pb = blocks_for(n);
     int nk = enqueue_search(h, 1);
+    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 256, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
     launch(h, K_FORCE_RK, [&] {
-        k_force_rk<<<pb, kThreads, 0, st>>>(h->A, h->pterm, h->nbr, h->ncount, S, h->rheo, h->dem, n, h->B, h->velfin,
-                                            h->d_auxv, 0, nullptr);
+        k_force_rk<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
     }); nk++;
     if (h->rheo.av_vel) {
-        launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(h->A, h->nbr, h->ncount, S, h->rheo, n, h->B, h->velfin); });
-        nk++;
+        launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B, h->velfin); }); nk++;
+        launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 256, 0, st>>>(h->A, q, S, h->rheo, h->B, h->velfin); }); nk++;
     }
     if (h->rheo.erosion) {
         launch(h, K_DEM_ERODE, [&] { k_dem_erode<<<148 * 2, 256, 0, st>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S); });
@@ -255,7 +281,7 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 12 + 1 + (h->rheo.av_vel ? 1 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 14 + 2 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
 }
 
 int alloc_cells(gfsph_handle* h, int cap) {
@@ -268,6 +294,14 @@ int alloc_cells(gfsph_handle* h, int cap) {
     if (st) return GFSPH_ERR_CUDA;
     CK(cudaMemsetAsync(h->count, 0, ((size_t)cap + 1) * sizeof(int), h->stream));
     h->cap_cells = cap;
+    drop_graphs(h);
+    return 0;
+}
+
+int alloc_big(gfsph_handle* h, int cap) {
+    dfree(h->indv_big); dfree(h->bigtmp);
+    if (dalloc(&h->indv_big, cap) || dalloc(&h->bigtmp, cap)) return GFSPH_ERR_CUDA;
+    h->big_cap = cap;
     drop_graphs(h);
     return 0;
 }
@@ -286,8 +320,9 @@ void free_particles(gfsph_handle* h) {
         dfree(p->pos); dfree(p->vel); dfree(p->rho); dfree(p->mass); dfree(p->hsml); dfree(p->flag); dfree(p->id);
     }
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
-    dfree(h->nbr); dfree(h->f2tmp);
+    dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv_big); dfree(h->bigtmp);
     h->kcap = 0;
+    h->big_cap = 0;
 }
 
 int alloc_pstate(PState* p, int n) {
@@ -333,8 +368,15 @@ int grow_after_error(gfsph_handle* h) {
         int st = alloc_nbr(h, want);
         if (st) return st;
     }
+    if (e & kErrBig) {
+        int want = std::max(s->need_big * 2, h->big_cap * 2);
+        if (want > (1 << 24)) return GFSPH_ERR_CAPACITY;
+        int st = alloc_big(h, want);
+        if (st) return st;
+    }
     set_field<int>(h, offsetof(StepScalars, err), 0);
     set_field<int>(h, offsetof(StepScalars, need_nbr), 0);
+    set_field<int>(h, offsetof(StepScalars, need_big), 0);
     return 0;
 }
 
@@ -519,9 +561,11 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
         st |= alloc_pstate(&h->A, n); st |= alloc_pstate(&h->B, n); st |= alloc_pstate(&h->U, n);
         st |= dalloc(&h->cellA, n); st |= dalloc(&h->velfin, n); st |= dalloc(&h->pterm, n);
         st |= dalloc(&h->keyrank, n); st |= dalloc(&h->perm, n); st |= dalloc(&h->ncount, n);
-        st |= dalloc(&h->f2tmp, n);
+        st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n);
         if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
+        if (st) return st;
+        st = alloc_big(h, 1024);
         if (st) return st;
         drop_graphs(h);
     }
@@ -677,9 +721,11 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
     if (st) return st;
     int n = h->n;
     cudaStream_t s = h->stream;
+    Search q = make_search(h);
+    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 256, 0, s>>>(h->A, q, h->S, h->rheo); });
     launch(h, K_FORCE_RK, [&] {
-        k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, h->pterm, h->nbr, h->ncount, h->S, h->rheo, h->dem, n, h->B,
-                                                     h->velfin, h->d_auxv, 1, h->velfin);
+        k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 1,
+                                                     h->velfin);
     });
     launch(h, K_UNSORT, [&] { k_unsort_f2<<<blocks_for(n), kThreads, 0, s>>>(h->velfin, h->A.id, n, h->f2tmp); });
     launch(h, K_COPY, [&] { k_copy_state<<<blocks_for(n), kThreads, 0, s>>>(h->A, h->B, n); });
@@ -694,26 +740,51 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
     int n = h->n;
     int st = read_scalars(h);
     if (st) return st;
-    int nact = h->hS->nactive;
+    int nreg = h->hS->nreg, nbig = h->hS->nbig;
     std::vector<int> cnt(n), id(n), tab((size_t)h->kcap * n);
     CK(cudaMemcpy(cnt.data(), h->ncount, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(id.data(), h->A.id, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(tab.data(), h->nbr, tab.size() * sizeof(int), cudaMemcpyDeviceToHost));
     std::vector<std::vector<int>> lists(n);
-    for (int s = 0; s < nact; s++) {
+    for (int s = 0; s < nreg; s++) {
         auto& L = lists[id[s]];
         for (int k = 0; k < cnt[s] && k < h->kcap; k++) L.push_back(id[tab[(size_t)k * n + s]]);
-        std::sort(L.begin(), L.end());
+    }
+    if (nbig > 0) {  // pairs of the big particles, found on the device
+        int pcap = 1 << 20;
+        for (int tries = 0; tries < 8; tries++) {
+            int2* dpairs = nullptr;
+            int* dcount = nullptr;
+            if (dalloc(&dpairs, pcap) || dalloc(&dcount, 1)) { dfree(dpairs); dfree(dcount); return GFSPH_ERR_CUDA; }
+            cudaMemset(dcount, 0, sizeof(int));
+            Search q = make_search(h);
+            launch(h, K_EXPORT, [&] { k_export_big<<<big_blocks(h), 256, 0, h->stream>>>(q, h->S, dpairs, dcount, pcap); });
+            cudaStreamSynchronize(h->stream);
+            int np = 0;
+            cudaMemcpy(&np, dcount, sizeof(int), cudaMemcpyDeviceToHost);
+            if (np > pcap) { dfree(dpairs); dfree(dcount); pcap = np; continue; }
+            std::vector<int2> pr(np);
+            cudaMemcpy(pr.data(), dpairs, (size_t)np * sizeof(int2), cudaMemcpyDeviceToHost);
+            dfree(dpairs); dfree(dcount);
+            for (const int2& q2 : pr) {
+                lists[id[q2.x]].push_back(id[q2.y]);
+                if (q2.y < nreg) lists[id[q2.y]].push_back(id[q2.x]);  // a big j reports its own pairs
+            }
+            break;
+        }
     }
     int tot = 0;
     for (int i = 0; i < n; i++) {
+        auto& L = lists[i];
+        std::sort(L.begin(), L.end());
         offsets[i] = tot;
-        for (int j : lists[i]) {
+        for (int j : L) {
             if (idx && tot < cap) idx[tot] = j;
             tot++;
         }
     }
     offsets[n] = tot;
+    CK(cudaGetLastError());
     return (tot > cap) ? GFSPH_ERR_CAPACITY : GFSPH_OK;
 }
 

@@ -10,28 +10,33 @@ namespace gfsph {
 
 constexpr int kScanTile = 2048;  // cells per scan tile (256 threads x 8)
 constexpr int kScanThreads = 256;
+constexpr float kBigFactor = 2.5f;  // hsml above kBigFactor * mean(hsml) goes to the big list
+constexpr float kCellPerHc = 2.f;   // cells per regular-hsml bound Hc: cell size = Hc / 2
 
 // error bits in StepScalars::err
 constexpr int kErrCells = 1;
 constexpr int kErrNbr = 2;
 constexpr int kErrNonFinite = 4;
 constexpr int kErrEmpty = 8;
+constexpr int kErrBig = 16;
 
 // Device-resident scalars of the step (one per handle).
 struct StepScalars {
     double time;      // time_sph
     double t_end;
+    double hsum;      // sum of hsml over the particles inside the DEM box
     float dt;         // dt_sph, committed at the end of a completed step
     float dt_step;    // dt of the step in flight (a step stopped by a capacity error leaves dt unchanged)
     int skip;         // this step does nothing (time >= t_end or an error)
     int err;          // sticky error bits
     int steps_done;
     unsigned int xmin_o, xmax_o, ymin_o, ymax_o, hmax_o, dtmin_o;  // reductions (ordered uint)
+    int hcount;
     int bad;          // non-finite state seen by k_bounds
-    float gx0, gy0, gd;  // cell grid origin and cell size
+    float gx0, gy0, gd, hc;  // cell grid origin, cell size, regular-hsml bound
     int ndx, ndy, ncells, ncells_prev;
-    int nactive, nout;
-    int need_cells, need_nbr;
+    int nreg, nbig, nactive, nout;
+    int need_cells, need_nbr, need_big;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
     int advance;      // 1 inside gfsph_step, 0 for search-only passes
 };
@@ -47,6 +52,18 @@ struct PState {
     int* id;
 };
 
+// Scratch of the neighbour search (sorted order).
+struct Search {
+    const int* start;    // cell -> first slot (exclusive scan), ncells+1
+    const int* cellA;    // slot -> cell key (regular), -2 big, -1 out
+    const float4* xhm;   // slot -> (x, y, hsml, mass) at the start of the step
+    int* nbr;            // k-major neighbour table of the regular particles
+    int* ncount;
+    float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
+    float2* indv_big;    // internal force of the big particles
+    int kcap;
+};
+
 __device__ __forceinline__ bool step_skipped(const StepScalars* S) { return S->skip != 0; }
 
 // ---------------------------------------------------------------- prologue
@@ -57,8 +74,11 @@ __global__ void k_prep(StepScalars* S, int advance) {
     S->xmin_o = 0xffffffffu; S->ymin_o = 0xffffffffu;
     S->xmax_o = 0u; S->ymax_o = 0u; S->hmax_o = 0u;
     S->dtmin_o = 0xffffffffu;
+    S->hsum = 0.0;
+    S->hcount = 0;
     S->bad = 0;
     S->nout = 0;
+    S->nbig = 0;
     S->ex0 = 0x7fffffff; S->ey0 = 0x7fffffff; S->ex1 = -1; S->ey1 = -1;
 }
 
@@ -70,15 +90,25 @@ __device__ __forceinline__ float warp_max(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ int warp_sum(int v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 
 // The stability time step of Adaptive_dt_sph_SW (SPH_SW_2019.f90:6537-6567,
 // min hsml/(3 max(1e-6, sqrt(g h))) [+|v|]) over the particles not yet
 // flagged; then the Check_Out_Domain at the start of time_integration_sph
 // (SPH_MAIN_2019.f90:232, :1764-1788) and, over the particles still inside,
-// the bounds and max(hsml) of the cell grid (grid_find :906-919 / :1150-1165).
+// the bounds, max and mean of hsml for the cell grid.
 __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
     if (step_skipped(S)) return;
     float xmn = 3.4e38f, xmx = -3.4e38f, ymn = 3.4e38f, ymx = -3.4e38f, hmx = 0.f, dtm = 1.e10f;
+    double hs_sum = 0.0;
+    int hs_cnt = 0;
     int bad = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (B.flag[i]) continue;
@@ -93,6 +123,8 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
             xmn = fminf(xmn, p.x); xmx = fmaxf(xmx, p.x);
             ymn = fminf(ymn, p.y); ymx = fmaxf(ymx, p.y);
             hmx = fmaxf(hmx, hs);
+            hs_sum += (double)hs;
+            hs_cnt += 1;
         }
         if (c.ic_adapt == 1 || c.ic_adapt == 2) {
             float hh = (h < c.h_inf) ? c.h_inf : h;
@@ -109,25 +141,32 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
     }
     xmn = warp_min(xmn); xmx = warp_max(xmx); ymn = warp_min(ymn); ymx = warp_max(ymx);
     hmx = warp_max(hmx); dtm = warp_min(dtm);
+    hs_sum = warp_sum(hs_sum);
+    hs_cnt = warp_sum(hs_cnt);
     bad = __any_sync(0xffffffffu, bad);
     if ((threadIdx.x & 31) == 0) {
         atomicMin(&S->xmin_o, f2o(xmn)); atomicMax(&S->xmax_o, f2o(xmx));
         atomicMin(&S->ymin_o, f2o(ymn)); atomicMax(&S->ymax_o, f2o(ymx));
         atomicMax(&S->hmax_o, f2o(hmx)); atomicMin(&S->dtmin_o, f2o(dtm));
+        if (hs_cnt) { atomicAdd(&S->hsum, hs_sum); atomicAdd(&S->hcount, hs_cnt); }
         if (bad) atomicOr(&S->bad, 1);
     }
 }
 
-// dt update (Adaptive_dt_sph_SW :6658-6662) and the cell grid of
-// grid_find_NEW_tools (:1150-1165): cell = 2*max(hsml), ndivx = length/cell+1,
-// origin shifted by half the slack and 0.1% of the length.
+// dt update (Adaptive_dt_sph_SW :6658-6662) and the cell grid.  The
+// reference sizes its cells by 2*max(hsml) (grid_find :906-919); here the
+// regular particles are those with hsml <= Hc = min(max, 2.5*mean) and the
+// cell size is Hc/2, each particle scanning the cells within hsml_i + Hc.
+// Particles above Hc (a handful of thin-front particles whose hsml keeps
+// growing) are searched separately.  The neighbour set is the reference's,
+// {j : r_ij < 2*(h_i+h_j)/2}, whatever the grid.
 __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (S->skip) return;
     if (S->bad) { S->err |= kErrNonFinite; S->skip = 1; return; }
     float xmn = o2f(S->xmin_o), xmx = o2f(S->xmax_o), ymn = o2f(S->ymin_o), ymx = o2f(S->ymax_o);
     float hmx = o2f(S->hmax_o);
-    if (S->xmin_o == 0xffffffffu || !(hmx > 0.f)) { S->err |= kErrEmpty; S->skip = 1; return; }
+    if (S->xmin_o == 0xffffffffu || !(hmx > 0.f) || S->hcount == 0) { S->err |= kErrEmpty; S->skip = 1; return; }
     float dt = S->dt;
     if (S->advance) {
         float dtmin = (c.ic_adapt == 1 || c.ic_adapt == 2) ? o2f(S->dtmin_o) : 1.e10f;
@@ -135,9 +174,11 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
         else if (c.ic_adapt != 0) dt = fminf(1.1f * dt, dtmin);
     }
     S->dt_step = dt;
-    float deltx = hmx * 2.f;
+    float mean = (float)(S->hsum / (double)S->hcount);
+    float hc = fminf(hmx, kBigFactor * mean);
+    float cell = hc / kCellPerHc;
     float lx = xmx - xmn, ly = ymx - ymn;
-    float fx = lx / deltx + 1.f, fy = ly / deltx + 1.f;
+    float fx = lx / cell + 1.f, fy = ly / cell + 1.f;
     if (!(fx < 1.0e8f) || !(fy < 1.0e8f) || !(fx * fy < 2.0e9f)) {  // far beyond any capacity
         S->err |= kErrCells;
         S->need_cells = 0x3fffffff;
@@ -146,10 +187,11 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
     }
     int ndx = (int)fx;
     int ndy = (int)fy;
-    float lxn = (float)ndx * deltx, lyn = (float)ndy * deltx;
+    float lxn = (float)ndx * cell, lyn = (float)ndy * cell;
     S->gx0 = (xmn - (lxn - lx) / 2.f) - 0.001f * lx;
     S->gy0 = (ymn - (lyn - ly) / 2.f) - 0.001f * ly;
-    S->gd = deltx;
+    S->gd = cell;
+    S->hc = hc;
     S->ndx = ndx;
     S->ndy = ndy;
     long long nc = (long long)ndx * (long long)ndy;
@@ -171,23 +213,40 @@ __global__ void k_clear_cells(int* count, const StepScalars* S) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) count[k] = 0;
 }
 
-// Cell key and within-cell arrival rank of each particle (counting sort
-// histogram, grid_find :938-948).  Out-of-domain particles get key -1.
-__global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* count, int2* keyrank) {
+__device__ __forceinline__ void cell_of(float2 p, float gx0, float gy0, float gd, int ndx, int ndy, int& cx,
+                                        int& cy) {
+    int ix = (int)((p.x - gx0) / gd + 1.f);
+    int iy = (int)((p.y - gy0) / gd + 1.f);
+    cx = min(max(ix, 1), ndx) - 1;
+    cy = min(max(iy, 1), ndy) - 1;
+}
+
+// Cell key and within-cell arrival rank of each regular particle (counting
+// sort histogram, grid_find :938-948); big particles get key -2 and a rank in
+// the big list; out-of-domain particles key -1.
+__global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* count, int2* keyrank, int big_cap) {
     if (S->skip) return;
-    float gx0 = S->gx0, gy0 = S->gy0, gd = S->gd;
+    float gx0 = S->gx0, gy0 = S->gy0, gd = S->gd, hc = S->hc;
     int ndx = S->ndx, ndy = S->ndy;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int2 kr = make_int2(-1, 0);
         float2 p = B.pos[i];
         if (!B.flag[i] && !out_of_box(dem, p.x, p.y)) {
-            int ix = (int)((p.x - gx0) / gd + 1.f);
-            int iy = (int)((p.y - gy0) / gd + 1.f);
-            ix = min(max(ix, 1), ndx);
-            iy = min(max(iy, 1), ndy);
-            int key = (iy - 1) * ndx + (ix - 1);
-            kr.x = key;
-            kr.y = atomicAdd(&count[key], 1);
+            if (B.hsml[i] > hc) {
+                kr.x = -2;
+                kr.y = atomicAdd(&S->nbig, 1);
+                if (kr.y >= big_cap) {
+                    atomicOr(&S->err, kErrBig);
+                    atomicMax(&S->need_big, kr.y + 1);
+                    atomicExch(&S->skip, 1);
+                }
+            } else {
+                int cx, cy;
+                cell_of(p, gx0, gy0, gd, ndx, ndy, cx, cy);
+                int key = cy * ndx + cx;
+                kr.x = key;
+                kr.y = atomicAdd(&count[key], 1);
+            }
         }
         keyrank[i] = kr;
     }
@@ -211,7 +270,6 @@ __global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const 
     int loc[per];
     int s = 0;
     for (int k = 0; k < per; k++) { loc[k] = s; s += sh[threadIdx.x * per + k]; }
-    // block-wide exclusive scan of the per-thread sums
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int incl = s;
     for (int o = 1; o < 32; o <<= 1) {
@@ -291,89 +349,131 @@ __global__ void k_scan_add(int* start, const int* tile_sum, StepScalars* S) {
     }
 }
 
-// Scatter (grid_find :952-958): slot = start[cell] + rank; out-of-domain
-// particles go behind the active ones.
+// Scatter (grid_find :952-958): regular particles to start[cell] + rank,
+// then the big list, then the out-of-domain particles.
 __global__ void k_scatter(const int2* keyrank, int n, const int* start, StepScalars* S, int* perm) {
     if (S->skip) return;
-    int nact = start[S->ncells];
+    int nreg = start[S->ncells];
+    int nbig = S->nbig;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int2 kr = keyrank[i];
-        int slot = (kr.x >= 0) ? start[kr.x] + kr.y : nact + atomicAdd(&S->nout, 1);
+        int slot;
+        if (kr.x >= 0) slot = start[kr.x] + kr.y;
+        else if (kr.x == -2) slot = nreg + kr.y;
+        else slot = nreg + nbig + atomicAdd(&S->nout, 1);
         perm[slot] = i;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->nactive = nact;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->nreg = nreg;
+        S->nactive = nreg + nbig;
+    }
 }
 
-// Orders each cell's particles by original index, so the within-cell order
-// (hence every neighbour-sum order) is independent of atomic arrival order.
+// Orders each cell's particles (and the big list) by original index, so the
+// within-cell order, hence every neighbour-sum order, is independent of
+// atomic arrival order.
+__device__ __forceinline__ void insertion_sort_by_id(int* perm, const int* id_old, int a, int b) {
+    for (int k = a + 1; k < b; k++) {
+        int pk = perm[k];
+        int key = id_old[pk];
+        int m = k - 1;
+        while (m >= a && id_old[perm[m]] > key) { perm[m + 1] = perm[m]; m--; }
+        perm[m + 1] = pk;
+    }
+}
+
 __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, const StepScalars* S) {
     if (S->skip) return;
     int nc = S->ncells;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-        int a = start[c], b = start[c + 1];
-        for (int k = a + 1; k < b; k++) {
-            int pk = perm[k];
-            int key = id_old[pk];
-            int m = k - 1;
-            while (m >= a && id_old[perm[m]] > key) { perm[m + 1] = perm[m]; m--; }
-            perm[m + 1] = pk;
-        }
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+        insertion_sort_by_id(perm, id_old, start[c], start[c + 1]);
+}
+
+// The big list sorted by original index: rank of each entry = number of
+// entries with a smaller id (one block).
+__global__ void k_big_sort(int* perm, const int* id_old, int* tmp, const StepScalars* S) {
+    if (S->skip) return;
+    int a = S->nreg, nb = S->nbig;
+    if (nb < 2) return;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) tmp[k] = perm[a + k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        int me = id_old[tmp[k]];
+        int r = 0;
+        for (int m = 0; m < nb; m++) r += (id_old[tmp[m]] < me);
+        perm[a + r] = tmp[k];
     }
 }
 
 // Gathers the state into the new (cell-sorted) order.
 __global__ void k_reorder(const PState B, int n, const int* perm, const int2* keyrank, PState A, int* cellA,
-                          const StepScalars* S) {
+                          float4* xhm, const StepScalars* S) {
     if (S->skip) return;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = perm[s];
-        A.pos[s] = B.pos[o];
+        float2 p = B.pos[o];
+        float hs = B.hsml[o], m = B.mass[o];
+        A.pos[s] = p;
         A.vel[s] = B.vel[o];
         A.rho[s] = B.rho[o];
-        A.mass[s] = B.mass[o];
-        A.hsml[s] = B.hsml[o];
+        A.mass[s] = m;
+        A.hsml[s] = hs;
         A.flag[s] = B.flag[o];
         A.id[s] = B.id[o];
         cellA[s] = keyrank[o].x;
+        xhm[s] = make_float4(p.x, p.y, hs, m);
     }
 }
 
-// Neighbour search and summation density, fused: for every active particle
-// scan the 3x3 cells around its cell, keep j when r < 2*(hi+hj)/2 (the pair
-// set of grid_find, :987-1060), append j to the neighbour table (k-major,
-// nbr[k*n + i]) and accumulate m_j W_ij in FP64 (sum_density_Tools
-// :1796-1836, h_i = W(0,h_i) m_i + sum_j m_j W_ij).  Also stores the
-// per-particle pressure term of IntForces_SW: p/h^2 (pa_sph 2) or p (pa_sph 1)
-// with h clamped to h_inf (:6769, :6797).
-__global__ void __launch_bounds__(128) k_density(PState A, const int* cellA, const int* start, StepScalars* S,
-                                                  Rheo c, int n, int kcap, int* nbr, int* ncount, float* pterm) {
+// Stencil radius in cells of a particle with smoothing length hi: every
+// regular neighbour j (hsml_j <= Hc, r < hi + hj) lies within
+// floor((hi + Hc)/cell + 0.01) + 1 cells of i's cell, whatever the rounding
+// of the cell coordinates.
+__device__ __forceinline__ int stencil_radius(float hi, const StepScalars* S) {
+    return (int)((hi + S->hc) / S->gd + 0.01f) + 1;
+}
+
+// Neighbour search and summation density of the regular particles, fused:
+// every j with r < 2*(hi+hj)/2 (the pair set of grid_find, :987-1060) among
+// the regular particles of the stencil is appended to the neighbour table
+// (k-major, nbr[k*n + i]); big neighbours come from the big list.
+// h_i = W(0,h_i) m_i + sum_j m_j W_ij (sum_density_Tools :1796-1836) in FP64.
+// Also stores the pressure term of IntForces_SW with h clamped to h_inf
+// (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
+__global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip) return;
-    const int nact = S->nactive;
+    const int nreg = S->nreg, nbig = S->nbig;
     const int ndx = S->ndx, ndy = S->ndy;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
-        float2 xi = A.pos[i];
-        float hi = A.hsml[i];
-        int cell = cellA[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
+        float4 me = Q.xhm[i];
+        float2 xi = make_float2(me.x, me.y);
+        float hi = me.z;
+        int cell = Q.cellA[i];
         int cx = cell % ndx, cy = cell / ndx;
-        double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * A.mass[i]);
+        int R = stencil_radius(hi, S);
+        double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * me.w);
         int cnt = 0;
-        for (int jy = max(cy - 1, 0); jy <= min(cy + 1, ndy - 1); jy++) {
-            int row = jy * ndx;
-            int c0 = row + max(cx - 1, 0), c1 = row + min(cx + 1, ndx - 1);
-            int ja = start[c0], jb = start[c1 + 1];
+        int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
+        for (int jy = max(cy - R, 0); jy <= min(cy + R, ndy - 1); jy++) {
+            int ja = Q.start[jy * ndx + x0], jb = Q.start[jy * ndx + x1 + 1];
             for (int j = ja; j < jb; j++) {
                 if (j == i) continue;
+                float4 o = Q.xhm[j];
                 PairGeom g;
-                if (pair_test(xi, A.pos[j], hi, A.hsml[j], g)) {
-                    if (cnt < kcap) nbr[(size_t)cnt * n + i] = j;
+                if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) {
+                    if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
                     cnt++;
-                    float w = sph_kernel_w(c.skf, g.r, g.mh);
-                    acc += (double)(A.mass[j] * w);
+                    acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
                 }
             }
         }
-        ncount[i] = cnt;
-        if (cnt > kcap) {  // table too small: stop this step before any state is written
+        for (int j = nreg; j < nreg + nbig; j++) {
+            float4 o = Q.xhm[j];
+            PairGeom g;
+            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
+        }
+        Q.ncount[i] = cnt;
+        if (cnt > Q.kcap) {  // table too small: stop this step before any state is written
             atomicOr(&S->err, kErrNbr);
             atomicMax(&S->need_nbr, cnt);
             atomicExch(&S->skip, 1);
@@ -382,41 +482,137 @@ __global__ void __launch_bounds__(128) k_density(PState A, const int* cellA, con
         A.rho[i] = h;
         float hc = (h < c.h_inf) ? c.h_inf : h;
         float p = (c.cgra05 * hc) * hc;
-        pterm[i] = (c.pa_sph == 1) ? p : p / (hc * hc);
+        Q.pterm[i] = (c.pa_sph == 1) ? p : p / (hc * hc);
     }
 }
 
-// Internal acceleration of IntForces_SW (SPH_SW_2019.f90:6905-6920) for
-// particle i, gathered over its neighbour table in FP64.
-__device__ __forceinline__ void internal_force(const PState& A, const float* pterm, const Rheo& c, int i, int n,
-                                               int cnt, const int* nbr, float& in0, float& in1) {
-    float2 xi = A.pos[i];
-    float hi = A.hsml[i];
-    float pi_ = pterm[i];
-    float rhoi = A.rho[i];
-    rhoi = (rhoi < c.h_inf) ? c.h_inf : rhoi;
-    double a0 = 0.0, a1 = 0.0;
-    for (int k = 0; k < cnt; k++) {
-        int j = nbr[(size_t)k * n + i];
-        PairGeom g;
-        pair_test(xi, A.pos[j], hi, A.hsml[j], g);
-        float w, d0, d1;
-        sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
-        float mj = A.mass[j];
-        float pj = pterm[j];
-        float h0, h1;
-        if (c.pa_sph == 1) {
-            float rhoj = A.rho[j];
-            rhoj = (rhoj < c.h_inf) ? c.h_inf : rhoj;
-            float rij = 1.f / (rhoi * rhoj);
-            h0 = (-(pi_ + pj) * d0) * rij;
-            h1 = (-(pi_ + pj) * d1) * rij;
-        } else {
-            h0 = -(pi_ + pj) * d0;
-            h1 = -(pi_ + pj) * d1;
+// Visits every neighbour j of particle i cooperatively over the block: the
+// regular particles of the (wide) stencil and the big list.
+template <class F>
+__device__ __forceinline__ void block_neighbours(const Search& Q, const StepScalars* S, int i, F&& f) {
+    float4 me = Q.xhm[i];
+    float2 xi = make_float2(me.x, me.y);
+    float hi = me.z;
+    const int ndx = S->ndx, ndy = S->ndy, nreg = S->nreg, nbig = S->nbig;
+    int cx, cy;
+    cell_of(xi, S->gx0, S->gy0, S->gd, ndx, ndy, cx, cy);
+    float rr = (hi + S->hc) / S->gd + 0.01f;
+    int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
+    int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
+    int y0 = max(cy - R, 0), y1 = min(cy + R, ndy - 1);
+    for (int jy = y0; jy <= y1; jy++) {
+        int ja = Q.start[jy * ndx + x0], jb = Q.start[jy * ndx + x1 + 1];
+        for (int j = ja + threadIdx.x; j < jb; j += blockDim.x) {
+            float4 o = Q.xhm[j];
+            PairGeom g;
+            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
         }
-        a0 += (double)(mj * h0);
-        a1 += (double)(mj * h1);
+    }
+    for (int j = nreg + threadIdx.x; j < nreg + nbig; j += blockDim.x) {
+        if (j == i) continue;
+        float4 o = Q.xhm[j];
+        PairGeom g;
+        if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+    }
+}
+
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    T t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+    return t;  // valid in thread 0
+}
+
+// Summation density of the big particles, one block per particle.
+__global__ void __launch_bounds__(256) k_density_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    if (S->skip) return;
+    __shared__ double sh[8];
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+        int i = nreg + b;
+        double acc = 0.0;
+        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+            acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
+        });
+        double tot = block_sum(acc, sh);
+        if (threadIdx.x == 0) {
+            float4 me = Q.xhm[i];
+            float h = (float)((double)(sph_kernel_w(c.skf, 0.f, me.z) * me.w) + tot);
+            A.rho[i] = h;
+            float hc = (h < c.h_inf) ? c.h_inf : h;
+            float p = (c.cgra05 * hc) * hc;
+            Q.pterm[i] = (c.pa_sph == 1) ? p : p / (hc * hc);
+        }
+    }
+}
+
+// One pair term of IntForces_SW (SPH_SW_2019.f90:6905-6920) for particle i.
+__device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rhoi, float pj, float rhoj, float mj,
+                                              const PairGeom& g, double& a0, double& a1) {
+    float w, d0, d1;
+    sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+    float h0, h1;
+    if (c.pa_sph == 1) {
+        rhoi = (rhoi < c.h_inf) ? c.h_inf : rhoi;
+        rhoj = (rhoj < c.h_inf) ? c.h_inf : rhoj;
+        float rij = 1.f / (rhoi * rhoj);
+        h0 = (-(pi_ + pj) * d0) * rij;
+        h1 = (-(pi_ + pj) * d1) * rij;
+    } else {
+        h0 = -(pi_ + pj) * d0;
+        h1 = -(pi_ + pj) * d1;
+    }
+    a0 += (double)(mj * h0);
+    a1 += (double)(mj * h1);
+}
+
+// Internal acceleration of the big particles, one block per particle.
+__global__ void __launch_bounds__(256) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    if (S->skip) return;
+    __shared__ double sh[8];
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+        int i = nreg + b;
+        float pi_ = Q.pterm[i], rhoi = A.rho[i];
+        double a0 = 0.0, a1 = 0.0;
+        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+            pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
+        });
+        double t0 = block_sum(a0, sh);
+        double t1 = block_sum(a1, sh);
+        if (threadIdx.x == 0) Q.indv_big[b] = make_float2((float)t0, (float)t1);
+    }
+}
+
+// Internal acceleration of a regular particle: its neighbour table, then the
+// big list.
+__device__ __forceinline__ void internal_force(const PState& A, const Search& Q, const Rheo& c, const StepScalars* S,
+                                               int i, int n, float& in0, float& in1) {
+    float4 me = Q.xhm[i];
+    float2 xi = make_float2(me.x, me.y);
+    float hi = me.z;
+    float pi_ = Q.pterm[i];
+    float rhoi = A.rho[i];
+    double a0 = 0.0, a1 = 0.0;
+    int cnt = Q.ncount[i];
+    for (int k = 0; k < cnt; k++) {
+        int j = Q.nbr[(size_t)k * n + i];
+        float4 o = Q.xhm[j];
+        PairGeom g;
+        pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
+        pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
+    }
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int j = nreg; j < nreg + nbig; j++) {
+        float4 o = Q.xhm[j];
+        PairGeom g;
+        if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
     }
     in0 = (float)a0;
     in1 = (float)a1;
@@ -435,12 +631,11 @@ __device__ __forceinline__ void internal_force(const PState& A, const float* pte
 // stages.  (A particle that leaves the DEM box mid-step is frozen; the
 // reference then keeps scattering its stale pressure into its neighbours for
 // the remaining stages, which is not reproduced.)
-__global__ void __launch_bounds__(128) k_force_rk(PState A, const float* pterm, const int* nbr, const int* ncount,
-                                                   StepScalars* S, Rheo c, DemView dem, int n, PState B,
-                                                   float2* velfin, double2* auxv, int forces_only,
+__global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
+                                                   PState B, float2* velfin, double2* auxv, int forces_only,
                                                    float2* indv_out) {
     if (S->skip) return;
-    const int nact = S->nactive;
+    const int nact = S->nactive, nreg = S->nreg;
     const float dt = S->dt_step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (i >= nact) {  // carried particles (out of the domain at step start)
@@ -451,9 +646,14 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, const float* pterm, 
             }
             continue;
         }
-        int cnt = min(ncount[i], 0x7fffffff);
         float in0, in1;
-        internal_force(A, pterm, c, i, n, cnt, nbr, in0, in1);
+        if (i < nreg) {
+            internal_force(A, Q, c, S, i, n, in0, in1);
+        } else {
+            float2 f = Q.indv_big[i - nreg];
+            in0 = f.x;
+            in1 = f.y;
+        }
         if (forces_only) { indv_out[i] = make_float2(in0, in1); continue; }
 
         const float h = A.rho[i];
@@ -463,21 +663,27 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, const float* pterm, 
         float ex0 = 0.f, ex1 = 0.f;
         float Dx0 = 0.f, Dx1 = 0.f, Dv0 = 0.f, Dv1 = 0.f;
         bool out = false;
-        const float f1[4] = {0.f, 0.5f, 0.5f, 1.f};
-        const float f2[4] = {1.f, 2.f, 2.f, 1.f};
-#pragma unroll 1
+#pragma unroll
         for (int s = 0; s < 4; s++) {
-            float fdt = f1[s] * dt;
-            xx = x0.x + fdt * vx;
-            xy = x0.y + fdt * vy;
-            vx = v0.x + fdt * (ex0 + in0);
-            vy = v0.y + fdt * (ex1 + in1);
-            if (out_of_box(dem, xx, xy)) { out = true; break; }
-            ext_accel(c, dem, dt, xx, xy, vx, vy, hc, in0, in1, ex0, ex1);
-            Dv0 = Dv0 + f2[s] * (ex0 + in0);
-            Dv1 = Dv1 + f2[s] * (ex1 + in1);
-            Dx0 = Dx0 + f2[s] * vx;
-            Dx1 = Dx1 + f2[s] * vy;
+            const float f1 = (s == 0) ? 0.f : (s == 3 ? 1.f : 0.5f);
+            const float f2 = (s == 0 || s == 3) ? 1.f : 2.f;
+            if (!out) {
+                float fdt = f1 * dt;
+                float nxx = x0.x + fdt * vx;
+                float nxy = x0.y + fdt * vy;
+                float nvx = v0.x + fdt * (ex0 + in0);
+                float nvy = v0.y + fdt * (ex1 + in1);
+                xx = nxx; xy = nxy; vx = nvx; vy = nvy;
+                if (out_of_box(dem, xx, xy)) {
+                    out = true;
+                } else {
+                    ext_accel(c, dem, dt, xx, xy, vx, vy, hc, in0, in1, ex0, ex1);
+                    Dv0 = Dv0 + f2 * (ex0 + in0);
+                    Dv1 = Dv1 + f2 * (ex1 + in1);
+                    Dx0 = Dx0 + f2 * vx;
+                    Dx1 = Dx1 + f2 * vy;
+                }
+            }
         }
         float m = A.mass[i];
         float hs = A.hsml[i];
@@ -526,35 +732,70 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, const float* pterm, 
     }
 }
 
+// One pair term of av_vel (SPH_MAIN_2019.f90:3072-3080) for particle i.
+__device__ __forceinline__ void xsph_pair(const Rheo& c, float2 vi, float rhoi, float2 vj, float rhoj, float mj,
+                                          const PairGeom& g, double& a0, double& a1) {
+    float w = sph_kernel_w(c.skf, g.r, g.mh);
+    float den = rhoi + rhoj;
+    float t0 = (((2.f * mj) * (vi.x - vj.x)) / den) * w;
+    float t1 = (((2.f * mj) * (vi.y - vj.y)) / den) * w;
+    a0 -= (double)t0;
+    a1 -= (double)t1;
+}
+
 // av_vel (SPH_MAIN_2019.f90:3042-3099) with the start-of-step W_ij, then
 // v += 0.3*av for particles still inside the domain (:987-993).
-__global__ void __launch_bounds__(128) k_xsph(PState A, const int* nbr, const int* ncount, StepScalars* S, Rheo c,
-                                               int n, PState B, const float2* velfin) {
+__global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S, Rheo c, int n, PState B,
+                                               const float2* velfin) {
     if (S->skip || !c.av_vel) return;
-    const int nact = S->nactive;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         if (B.flag[i]) continue;
-        float2 xi = A.pos[i];
-        float hi = A.hsml[i];
+        float4 me = Q.xhm[i];
+        float2 xi = make_float2(me.x, me.y);
+        float hi = me.z;
         float2 vi = velfin[i];
         float rhoi = A.rho[i];
-        int cnt = ncount[i];
+        int cnt = Q.ncount[i];
         double a0 = 0.0, a1 = 0.0;
         for (int k = 0; k < cnt; k++) {
-            int j = nbr[(size_t)k * n + i];
+            int j = Q.nbr[(size_t)k * n + i];
+            float4 o = Q.xhm[j];
             PairGeom g;
-            pair_test(xi, A.pos[j], hi, A.hsml[j], g);
-            float w = sph_kernel_w(c.skf, g.r, g.mh);
-            float2 vj = velfin[j];
-            float mj = B.mass[j];
-            float den = rhoi + A.rho[j];
-            float t0 = (((2.f * mj) * (vi.x - vj.x)) / den) * w;
-            float t1 = (((2.f * mj) * (vi.y - vj.y)) / den) * w;
-            a0 -= (double)t0;
-            a1 -= (double)t1;
+            pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
+            xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
+        }
+        for (int j = nreg; j < nreg + nbig; j++) {
+            float4 o = Q.xhm[j];
+            PairGeom g;
+            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g))
+                xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B,
+                                                   const float2* velfin) {
+    if (S->skip || !c.av_vel) return;
+    __shared__ double sh[8];
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+        int i = nreg + b;
+        if (B.flag[i]) continue;  // uniform over the block
+        float2 vi = velfin[i];
+        float rhoi = A.rho[i];
+        double a0 = 0.0, a1 = 0.0;
+        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+            xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
+        });
+        double t0 = block_sum(a0, sh);
+        double t1 = block_sum(a1, sh);
+        if (threadIdx.x == 0) {
+            float av0 = 0.3f * (float)t0, av1 = 0.3f * (float)t1;
+            B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
+        }
     }
 }
 
@@ -590,6 +831,19 @@ __global__ void k_step_end(StepScalars* S) {
     S->dt = S->dt_step;
     S->time += (double)S->dt;
     S->steps_done += 1;
+}
+
+// Neighbour pairs of the big particles, for the parity export: every
+// (big i, j) pair with r < hi + hj, written as slot pairs.
+__global__ void k_export_big(Search Q, StepScalars* S, int2* pairs, int* npairs, int cap) {
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+        int i = nreg + b;
+        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+            int k = atomicAdd(npairs, 1);
+            if (k < cap) pairs[k] = make_int2(i, j);
+        });
+    }
 }
 
 // ---------------------------------------------------------------- outputs

@@ -270,3 +270,63 @@ def test_release_outside_the_dem_box_is_flagged_at_the_first_step(gfsph_lib, ora
     assert np.array_equal(g["x"][out], w.x[out])
     assert max_rel(g["x"], st.x, floor=1e-3) <= 1e-6
     sim.close()
+
+
+def test_big_smoothing_lengths_sets_and_density(gfsph_lib, oracle_mod):
+    """Particles whose hsml is far above the rest (the thin-front stragglers)
+    are searched on a separate list; their sets and sums must not change."""
+    rng = np.random.default_rng(5)
+    n = 6000
+    x = (rng.uniform(0, 80, size=(n, 2)) + 50.0).astype(np.float32)
+    h = rng.uniform(0.8, 1.2, size=n).astype(np.float32)
+    big = rng.choice(n, 40, replace=False)
+    h[big] = rng.uniform(4.0, 40.0, size=40).astype(np.float32)
+    m = rng.uniform(0.5, 1.5, size=n).astype(np.float32)
+    p = gfsph.make_params({1: 9.8, 2: 2000, 3: 500, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01})
+    sim = gfsph.Sim(p, np.zeros((64, 64), np.float32), dx=4.0, dy=4.0)
+    sim.upload(x, np.zeros_like(x), np.ones(n, np.float32), m, h)
+    rho = sim.density()
+    off, idx = sim.neighbours()
+    ref = oracle_mod.pairs(oracle_mod.MODE_FP32, p, x, h)
+    assert np.array_equal(off, ref["offsets"]) and np.array_equal(idx, ref["idx"])
+    ref1 = oracle_mod.pairs(oracle_mod.MODE_FP32_DACC, p, x, h, mass=m, rho=np.ones(n), want_sets=False,
+                            want_rho=True, want_force=True)
+    assert max_rel(rho, ref1["rho"]) <= 1e-6
+    sim.upload(x, np.zeros_like(x), np.ones(n, np.float32), m, h)
+    f = sim.internal_forces()
+    assert np.abs(f - ref1["force"]).max() <= 1e-6 * np.abs(ref1["force"]).max()
+    sim.close()
+
+
+def test_big_smoothing_lengths_one_step(gfsph_lib, oracle_mod):
+    w = small_channel()
+    rng = np.random.default_rng(9)
+    big = rng.choice(w.n, 25, replace=False)
+    w.hsml = w.hsml.copy()
+    w.hsml[big] *= np.float32(6.0)
+    sim, st, p = setup_pair(w, oracle_mod)
+    sim.step(1)
+    g = sim.download()
+    ny, nx = w.z.shape
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, 1)
+    assert np.array_equal(g["flag"], st.flag)
+    for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass), ("hsml", st.hsml)):
+        assert max_rel(g[key], ref, floor=1e-3) <= 1e-6, key
+    sim.close()
+
+
+def test_long_run_with_growing_front(gfsph_lib, oracle_mod):
+    """400 steps of a small channel release: the front spreads, some hsml grow
+    far above the mean and move to the big list; the run stays on the oracle."""
+    w = workloads.fractal_channel(n_target=3000, dem_k=8, cell=5.0)
+    sim, st, p = setup_pair(w, oracle_mod)
+    nsteps = 400
+    sim.step(nsteps)
+    g = sim.download()
+    ny, nx = w.z.shape
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+    assert g["hsml"].max() > 2.5 * g["hsml"].mean()
+    assert rel_l2(g["rho"], st.rho) <= 1e-4
+    assert rel_l2(g["x"], st.x) <= 1e-5
+    assert rel_l2(g["mass"], st.mass) <= 1e-5
+    sim.close()
