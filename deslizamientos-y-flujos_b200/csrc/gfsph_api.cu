@@ -18,14 +18,14 @@ namespace {
 
 enum KernelId {
     K_PREP, K_BOUNDS, K_GRID, K_CLEAR, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
-    K_BIG_SORT, K_REORDER, K_DENSITY, K_DENSITY_BIG, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
+    K_REORDER, K_DENSITY, K_DENSITY_BIG, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
 const char* kKernelNames[K_COUNT] = {
     "k_prep", "k_bounds", "k_grid", "k_clear_cells", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
-    "k_scatter", "k_cell_sort", "k_big_sort", "k_reorder", "k_density", "k_density_big", "k_force_big",
+    "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "step_batches"};
 
@@ -123,10 +123,7 @@ struct gfsph_handle {
     int* nbr = nullptr;
     int* ncount = nullptr;
     int kcap = 0;
-    // big list
-    float2* indv_big = nullptr;
-    int* bigtmp = nullptr;
-    int big_cap = 0;
+    float2* indv_big = nullptr;  // internal force of the level >= 1 particles
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -213,7 +210,7 @@ Search make_search(gfsph_handle* h) {
     return q;
 }
 
-int big_blocks(const gfsph_handle* h) { return std::max(1, std::min(h->big_cap, 148 * 2)); }
+int big_blocks(const gfsph_handle*) { return 148 * 2; }
 
 // The cell search: bounds, grid, counting sort, reorder, neighbours+density.
 // Returns the number of kernels enqueued.
@@ -229,13 +226,12 @@ int enqueue_search(gfsph_handle* h, int advance) {
     launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
     launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_cells); }); nk++;
     launch(h, K_CLEAR, [&] { k_clear_cells<<<148 * 4, 256, 0, st>>>(h->count, S); }); nk++;
-    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->count, h->keyrank, h->big_cap); }); nk++;
+    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->count, h->keyrank); }); nk++;
     launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, S); }); nk++;
     launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, S, h->perm); }); nk++;
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, S); }); nk++;
-    launch(h, K_BIG_SORT, [&] { k_big_sort<<<1, 1024, 0, st>>>(h->perm, h->B.id, h->bigtmp, S); }); nk++;
     launch(h, K_REORDER, [&] {
         k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S);
     }); nk++;
@@ -281,7 +277,7 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 14 + 2 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 13 + 2 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
 }
 
 int alloc_cells(gfsph_handle* h, int cap) {
@@ -294,14 +290,6 @@ int alloc_cells(gfsph_handle* h, int cap) {
     if (st) return GFSPH_ERR_CUDA;
     CK(cudaMemsetAsync(h->count, 0, ((size_t)cap + 1) * sizeof(int), h->stream));
     h->cap_cells = cap;
-    drop_graphs(h);
-    return 0;
-}
-
-int alloc_big(gfsph_handle* h, int cap) {
-    dfree(h->indv_big); dfree(h->bigtmp);
-    if (dalloc(&h->indv_big, cap) || dalloc(&h->bigtmp, cap)) return GFSPH_ERR_CUDA;
-    h->big_cap = cap;
     drop_graphs(h);
     return 0;
 }
@@ -320,9 +308,8 @@ void free_particles(gfsph_handle* h) {
         dfree(p->pos); dfree(p->vel); dfree(p->rho); dfree(p->mass); dfree(p->hsml); dfree(p->flag); dfree(p->id);
     }
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
-    dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv_big); dfree(h->bigtmp);
+    dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv_big);
     h->kcap = 0;
-    h->big_cap = 0;
 }
 
 int alloc_pstate(PState* p, int n) {
@@ -366,12 +353,6 @@ int grow_after_error(gfsph_handle* h) {
     if (e & kErrNbr) {
         int want = std::max(s->need_nbr + 16, h->kcap * 3 / 2);
         int st = alloc_nbr(h, want);
-        if (st) return st;
-    }
-    if (e & kErrBig) {
-        int want = std::max(s->need_big * 2, h->big_cap * 2);
-        if (want > (1 << 24)) return GFSPH_ERR_CAPACITY;
-        int st = alloc_big(h, want);
         if (st) return st;
     }
     set_field<int>(h, offsetof(StepScalars, err), 0);
@@ -561,11 +542,9 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
         st |= alloc_pstate(&h->A, n); st |= alloc_pstate(&h->B, n); st |= alloc_pstate(&h->U, n);
         st |= dalloc(&h->cellA, n); st |= dalloc(&h->velfin, n); st |= dalloc(&h->pterm, n);
         st |= dalloc(&h->keyrank, n); st |= dalloc(&h->perm, n); st |= dalloc(&h->ncount, n);
-        st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n);
+        st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n); st |= dalloc(&h->indv_big, n);
         if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
-        if (st) return st;
-        st = alloc_big(h, 1024);
         if (st) return st;
         drop_graphs(h);
     }
@@ -766,10 +745,7 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
             std::vector<int2> pr(np);
             cudaMemcpy(pr.data(), dpairs, (size_t)np * sizeof(int2), cudaMemcpyDeviceToHost);
             dfree(dpairs); dfree(dcount);
-            for (const int2& q2 : pr) {
-                lists[id[q2.x]].push_back(id[q2.y]);
-                if (q2.y < nreg) lists[id[q2.y]].push_back(id[q2.x]);  // a big j reports its own pairs
-            }
+            for (const int2& q2 : pr) lists[id[q2.x]].push_back(id[q2.y]);
             break;
         }
     }

@@ -11,14 +11,13 @@ namespace gfsph {
 constexpr int kScanTile = 2048;  // cells per scan tile (256 threads x 8)
 constexpr int kScanThreads = 256;
 constexpr float kBigFactor = 2.5f;  // hsml above kBigFactor * mean(hsml) goes to the big list
-constexpr float kCellPerHc = 2.f;   // cells per regular-hsml bound Hc: cell size = Hc / 2
+constexpr int kMaxLevels = 24;      // level k cell size Hc * 2^(k-1)
 
 // error bits in StepScalars::err
 constexpr int kErrCells = 1;
 constexpr int kErrNbr = 2;
 constexpr int kErrNonFinite = 4;
 constexpr int kErrEmpty = 8;
-constexpr int kErrBig = 16;
 
 // Device-resident scalars of the step (one per handle).
 struct StepScalars {
@@ -33,8 +32,11 @@ struct StepScalars {
     unsigned int xmin_o, xmax_o, ymin_o, ymax_o, hmax_o, dtmin_o;  // reductions (ordered uint)
     int hcount;
     int bad;          // non-finite state seen by k_bounds
-    float gx0, gy0, gd, hc;  // cell grid origin, cell size, regular-hsml bound
-    int ndx, ndy, ncells, ncells_prev;
+    float hc;         // regular-hsml bound Hc: level k holds hsml in (Hc*2^(k-1), Hc*2^k], level 0 hsml <= Hc
+    int nlev;         // number of grid levels
+    float lev_gx0[kMaxLevels], lev_gy0[kMaxLevels], lev_c[kMaxLevels];  // origin and cell size per level
+    int lev_ndx[kMaxLevels], lev_ndy[kMaxLevels], lev_off[kMaxLevels + 1];  // cells per level, first cell key
+    int ncells, ncells_prev;
     int nreg, nbig, nactive, nout;
     int need_cells, need_nbr, need_big;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
@@ -55,12 +57,12 @@ struct PState {
 // Scratch of the neighbour search (sorted order).
 struct Search {
     const int* start;    // cell -> first slot (exclusive scan), ncells+1
-    const int* cellA;    // slot -> cell key (regular), -2 big, -1 out
+    const int* cellA;    // slot -> cell key (all levels), -1 out of the domain
     const float4* xhm;   // slot -> (x, y, hsml, mass) at the start of the step
     int* nbr;            // k-major neighbour table of the regular particles
     int* ncount;
     float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
-    float2* indv_big;    // internal force of the big particles
+    float2* indv_big;    // internal force of the level >= 1 particles (slot - nreg)
     int kcap;
 };
 
@@ -153,13 +155,15 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
     }
 }
 
-// dt update (Adaptive_dt_sph_SW :6658-6662) and the cell grid.  The
-// reference sizes its cells by 2*max(hsml) (grid_find :906-919); here the
-// regular particles are those with hsml <= Hc = min(max, 2.5*mean) and the
-// cell size is Hc/2, each particle scanning the cells within hsml_i + Hc.
-// Particles above Hc (a handful of thin-front particles whose hsml keeps
-// growing) are searched separately.  The neighbour set is the reference's,
-// {j : r_ij < 2*(h_i+h_j)/2}, whatever the grid.
+// dt update (Adaptive_dt_sph_SW :6658-6662) and the cell grids.  The
+// reference sizes its single grid by 2*max(hsml) (grid_find :906-919), so one
+// thin-front particle whose hsml keeps growing inflates every cell.  Here
+// particles are split by smoothing length into levels: level 0 holds
+// hsml <= Hc = min(max, 2.5*mean), level k >= 1 holds hsml in
+// (Hc*2^(k-1), Hc*2^k]; level k has its own grid of cell size Hc*2^(k-1)
+// over the same box, and one cell-key space covers all levels.  A particle
+// searches each level within hsml_i + (that level's hsml bound), so the
+// neighbour set is the reference's {j : r_ij < 2*(h_i+h_j)/2} exactly.
 __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (S->skip) return;
@@ -176,33 +180,41 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
     S->dt_step = dt;
     float mean = (float)(S->hsum / (double)S->hcount);
     float hc = fminf(hmx, kBigFactor * mean);
-    float cell = hc / kCellPerHc;
+    int nlev = 1;
+    while (nlev < kMaxLevels && ldexpf(hc, nlev - 1) < hmx) nlev++;
+    if (ldexpf(hc, nlev - 1) < hmx) { S->err |= kErrCells; S->need_cells = 0x3fffffff; S->skip = 1; return; }
     float lx = xmx - xmn, ly = ymx - ymn;
-    float fx = lx / cell + 1.f, fy = ly / cell + 1.f;
-    if (!(fx < 1.0e8f) || !(fy < 1.0e8f) || !(fx * fy < 2.0e9f)) {  // far beyond any capacity
-        S->err |= kErrCells;
-        S->need_cells = 0x3fffffff;
-        S->skip = 1;
-        return;
+    long long off = 0;
+    for (int k = 0; k < nlev; k++) {
+        float cell = ldexpf(hc, k - 1);
+        float fx = lx / cell + 1.f, fy = ly / cell + 1.f;
+        if (!(fx < 1.0e8f) || !(fy < 1.0e8f) || !(fx * fy < 2.0e9f)) {  // far beyond any capacity
+            S->err |= kErrCells;
+            S->need_cells = 0x3fffffff;
+            S->skip = 1;
+            return;
+        }
+        int ndx = (int)fx, ndy = (int)fy;
+        float lxn = (float)ndx * cell, lyn = (float)ndy * cell;
+        S->lev_gx0[k] = (xmn - (lxn - lx) / 2.f) - 0.001f * lx;
+        S->lev_gy0[k] = (ymn - (lyn - ly) / 2.f) - 0.001f * ly;
+        S->lev_c[k] = cell;
+        S->lev_ndx[k] = ndx;
+        S->lev_ndy[k] = ndy;
+        S->lev_off[k] = (int)min(off, 0x7fffffffLL);
+        off += (long long)ndx * (long long)ndy;
     }
-    int ndx = (int)fx;
-    int ndy = (int)fy;
-    float lxn = (float)ndx * cell, lyn = (float)ndy * cell;
-    S->gx0 = (xmn - (lxn - lx) / 2.f) - 0.001f * lx;
-    S->gy0 = (ymn - (lyn - ly) / 2.f) - 0.001f * ly;
-    S->gd = cell;
+    S->lev_off[nlev] = (int)min(off, 0x7fffffffLL);
     S->hc = hc;
-    S->ndx = ndx;
-    S->ndy = ndy;
-    long long nc = (long long)ndx * (long long)ndy;
-    if (nc + 1 > (long long)cap_cells) {
+    S->nlev = nlev;
+    if (off + 1 > (long long)cap_cells) {
         S->err |= kErrCells;
-        S->need_cells = (nc + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(nc + 1);
+        S->need_cells = (off + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(off + 1);
         S->skip = 1;
         return;
     }
     S->ncells_prev = S->ncells;
-    S->ncells = (int)nc;
+    S->ncells = (int)off;
 }
 
 // Clears the cell histogram over [0, max(ncells, ncells_prev)] (+1 for the
@@ -213,40 +225,35 @@ __global__ void k_clear_cells(int* count, const StepScalars* S) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) count[k] = 0;
 }
 
-__device__ __forceinline__ void cell_of(float2 p, float gx0, float gy0, float gd, int ndx, int ndy, int& cx,
-                                        int& cy) {
-    int ix = (int)((p.x - gx0) / gd + 1.f);
-    int iy = (int)((p.y - gy0) / gd + 1.f);
-    cx = min(max(ix, 1), ndx) - 1;
-    cy = min(max(iy, 1), ndy) - 1;
+__device__ __forceinline__ void cell_of(float2 p, const StepScalars* S, int k, int& cx, int& cy) {
+    float gd = S->lev_c[k];
+    int ix = (int)((p.x - S->lev_gx0[k]) / gd + 1.f);
+    int iy = (int)((p.y - S->lev_gy0[k]) / gd + 1.f);
+    cx = min(max(ix, 1), S->lev_ndx[k]) - 1;
+    cy = min(max(iy, 1), S->lev_ndy[k]) - 1;
 }
 
-// Cell key and within-cell arrival rank of each regular particle (counting
-// sort histogram, grid_find :938-948); big particles get key -2 and a rank in
-// the big list; out-of-domain particles key -1.
-__global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* count, int2* keyrank, int big_cap) {
+__device__ __forceinline__ int level_of(float hs, const StepScalars* S) {
+    int k = 0;
+    while (k + 1 < S->nlev && hs > ldexpf(S->hc, k)) k++;
+    return k;
+}
+
+// Cell key (level offset + cell of that level's grid) and within-cell
+// arrival rank of each particle (counting sort histogram, grid_find
+// :938-948); out-of-domain particles get key -1.
+__global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* count, int2* keyrank) {
     if (S->skip) return;
-    float gx0 = S->gx0, gy0 = S->gy0, gd = S->gd, hc = S->hc;
-    int ndx = S->ndx, ndy = S->ndy;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int2 kr = make_int2(-1, 0);
         float2 p = B.pos[i];
         if (!B.flag[i] && !out_of_box(dem, p.x, p.y)) {
-            if (B.hsml[i] > hc) {
-                kr.x = -2;
-                kr.y = atomicAdd(&S->nbig, 1);
-                if (kr.y >= big_cap) {
-                    atomicOr(&S->err, kErrBig);
-                    atomicMax(&S->need_big, kr.y + 1);
-                    atomicExch(&S->skip, 1);
-                }
-            } else {
-                int cx, cy;
-                cell_of(p, gx0, gy0, gd, ndx, ndy, cx, cy);
-                int key = cy * ndx + cx;
-                kr.x = key;
-                kr.y = atomicAdd(&count[key], 1);
-            }
+            int k = level_of(B.hsml[i], S);
+            int cx, cy;
+            cell_of(p, S, k, cx, cy);
+            int key = S->lev_off[k] + cy * S->lev_ndx[k] + cx;
+            kr.x = key;
+            kr.y = atomicAdd(&count[key], 1);
         }
         keyrank[i] = kr;
     }
@@ -349,29 +356,26 @@ __global__ void k_scan_add(int* start, const int* tile_sum, StepScalars* S) {
     }
 }
 
-// Scatter (grid_find :952-958): regular particles to start[cell] + rank,
-// then the big list, then the out-of-domain particles.
+// Scatter (grid_find :952-958): particles to start[cell] + rank (level 0
+// first, then the higher levels), out-of-domain particles behind them.
 __global__ void k_scatter(const int2* keyrank, int n, const int* start, StepScalars* S, int* perm) {
     if (S->skip) return;
-    int nreg = start[S->ncells];
-    int nbig = S->nbig;
+    int nact = start[S->ncells];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int2 kr = keyrank[i];
-        int slot;
-        if (kr.x >= 0) slot = start[kr.x] + kr.y;
-        else if (kr.x == -2) slot = nreg + kr.y;
-        else slot = nreg + nbig + atomicAdd(&S->nout, 1);
+        int slot = (kr.x >= 0) ? start[kr.x] + kr.y : nact + atomicAdd(&S->nout, 1);
         perm[slot] = i;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int nreg = (S->nlev > 1) ? start[S->lev_off[1]] : nact;
         S->nreg = nreg;
-        S->nactive = nreg + nbig;
+        S->nbig = nact - nreg;
+        S->nactive = nact;
     }
 }
 
-// Orders each cell's particles (and the big list) by original index, so the
-// within-cell order, hence every neighbour-sum order, is independent of
-// atomic arrival order.
+// Orders each cell's particles by original index, so the within-cell order,
+// hence every neighbour-sum order, is independent of atomic arrival order.
 __device__ __forceinline__ void insertion_sort_by_id(int* perm, const int* id_old, int a, int b) {
     for (int k = a + 1; k < b; k++) {
         int pk = perm[k];
@@ -387,22 +391,6 @@ __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, cons
     int nc = S->ncells;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
         insertion_sort_by_id(perm, id_old, start[c], start[c + 1]);
-}
-
-// The big list sorted by original index: rank of each entry = number of
-// entries with a smaller id (one block).
-__global__ void k_big_sort(int* perm, const int* id_old, int* tmp, const StepScalars* S) {
-    if (S->skip) return;
-    int a = S->nreg, nb = S->nbig;
-    if (nb < 2) return;
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) tmp[k] = perm[a + k];
-    __syncthreads();
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-        int me = id_old[tmp[k]];
-        int r = 0;
-        for (int m = 0; m < nb; m++) r += (id_old[tmp[m]] < me);
-        perm[a + r] = tmp[k];
-    }
 }
 
 // Gathers the state into the new (cell-sorted) order.
@@ -425,53 +413,54 @@ __global__ void k_reorder(const PState B, int n, const int* perm, const int2* ke
     }
 }
 
-// Stencil radius in cells of a particle with smoothing length hi: every
-// regular neighbour j (hsml_j <= Hc, r < hi + hj) lies within
-// floor((hi + Hc)/cell + 0.01) + 1 cells of i's cell, whatever the rounding
-// of the cell coordinates.
-__device__ __forceinline__ int stencil_radius(float hi, const StepScalars* S) {
-    return (int)((hi + S->hc) / S->gd + 0.01f) + 1;
+// Visits the particles j != i of level k that are neighbours of particle i
+// (position xi, smoothing length hi): every j of level k has hsml_j <= Hk =
+// Hc*2^k, so with r < hi + hj it lies within floor((hi + Hk)/cell + 0.01) + 1
+// cells of i's cell in that level's grid, whatever the rounding of the cell
+// coordinates.  Threads t0, t0+ts, ... of the caller share the candidates.
+template <class F>
+__device__ __forceinline__ void level_neighbours(const Search& Q, const StepScalars* S, int k, int i, float2 xi, float hi,
+                                                 int t0, int ts, F&& f) {
+    const int ndx = S->lev_ndx[k], ndy = S->lev_ndy[k], off = S->lev_off[k];
+    float rr = (hi + ldexpf(S->hc, k)) / S->lev_c[k] + 0.01f;
+    int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
+    int cx, cy;
+    cell_of(xi, S, k, cx, cy);
+    int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
+    int y0 = max(cy - R, 0), y1 = min(cy + R, ndy - 1);
+    for (int jy = y0; jy <= y1; jy++) {
+        int row = off + jy * ndx;
+        int ja = Q.start[row + x0], jb = Q.start[row + x1 + 1];
+        for (int j = ja + t0; j < jb; j += ts) {
+            if (j == i) continue;
+            float4 o = Q.xhm[j];
+            PairGeom g;
+            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+        }
+    }
 }
 
-// Neighbour search and summation density of the regular particles, fused:
-// every j with r < 2*(hi+hj)/2 (the pair set of grid_find, :987-1060) among
-// the regular particles of the stencil is appended to the neighbour table
-// (k-major, nbr[k*n + i]); big neighbours come from the big list.
-// h_i = W(0,h_i) m_i + sum_j m_j W_ij (sum_density_Tools :1796-1836) in FP64.
-// Also stores the pressure term of IntForces_SW with h clamped to h_inf
-// (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
+// Neighbour search and summation density of the level-0 particles, fused:
+// every j with r < 2*(hi+hj)/2 (the pair set of grid_find, :987-1060), on
+// every level, is appended to the neighbour table (k-major, nbr[k*n + i]),
+// and h_i = W(0,h_i) m_i + sum_j m_j W_ij (sum_density_Tools :1796-1836) is
+// accumulated in FP64.  Also stores the pressure term of IntForces_SW with h
+// clamped to h_inf (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
 __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip) return;
-    const int nreg = S->nreg, nbig = S->nbig;
-    const int ndx = S->ndx, ndy = S->ndy;
+    const int nreg = S->nreg, nlev = S->nlev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         float4 me = Q.xhm[i];
         float2 xi = make_float2(me.x, me.y);
         float hi = me.z;
-        int cell = Q.cellA[i];
-        int cx = cell % ndx, cy = cell / ndx;
-        int R = stencil_radius(hi, S);
         double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * me.w);
         int cnt = 0;
-        int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
-        for (int jy = max(cy - R, 0); jy <= min(cy + R, ndy - 1); jy++) {
-            int ja = Q.start[jy * ndx + x0], jb = Q.start[jy * ndx + x1 + 1];
-            for (int j = ja; j < jb; j++) {
-                if (j == i) continue;
-                float4 o = Q.xhm[j];
-                PairGeom g;
-                if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) {
-                    if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
-                    cnt++;
-                    acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
-                }
-            }
-        }
-        for (int j = nreg; j < nreg + nbig; j++) {
-            float4 o = Q.xhm[j];
-            PairGeom g;
-            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
-        }
+        for (int k = 0; k < nlev; k++)
+            level_neighbours(Q, S, k, i, xi, hi, 0, 1, [&](int j, float4 o, const PairGeom& g) {
+                if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
+                cnt++;
+                acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
+            });
         Q.ncount[i] = cnt;
         if (cnt > Q.kcap) {  // table too small: stop this step before any state is written
             atomicOr(&S->err, kErrNbr);
@@ -486,34 +475,12 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
     }
 }
 
-// Visits every neighbour j of particle i cooperatively over the block: the
-// regular particles of the (wide) stencil and the big list.
+// Visits every neighbour j of particle i cooperatively over the block.
 template <class F>
 __device__ __forceinline__ void block_neighbours(const Search& Q, const StepScalars* S, int i, F&& f) {
     float4 me = Q.xhm[i];
     float2 xi = make_float2(me.x, me.y);
-    float hi = me.z;
-    const int ndx = S->ndx, ndy = S->ndy, nreg = S->nreg, nbig = S->nbig;
-    int cx, cy;
-    cell_of(xi, S->gx0, S->gy0, S->gd, ndx, ndy, cx, cy);
-    float rr = (hi + S->hc) / S->gd + 0.01f;
-    int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
-    int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
-    int y0 = max(cy - R, 0), y1 = min(cy + R, ndy - 1);
-    for (int jy = y0; jy <= y1; jy++) {
-        int ja = Q.start[jy * ndx + x0], jb = Q.start[jy * ndx + x1 + 1];
-        for (int j = ja + threadIdx.x; j < jb; j += blockDim.x) {
-            float4 o = Q.xhm[j];
-            PairGeom g;
-            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
-        }
-    }
-    for (int j = nreg + threadIdx.x; j < nreg + nbig; j += blockDim.x) {
-        if (j == i) continue;
-        float4 o = Q.xhm[j];
-        PairGeom g;
-        if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
-    }
+    for (int k = 0; k < S->nlev; k++) level_neighbours(Q, S, k, i, xi, me.z, threadIdx.x, blockDim.x, f);
 }
 
 template <class T>
@@ -590,10 +557,9 @@ __global__ void __launch_bounds__(256) k_force_big(PState A, Search Q, StepScala
     }
 }
 
-// Internal acceleration of a regular particle: its neighbour table, then the
-// big list.
-__device__ __forceinline__ void internal_force(const PState& A, const Search& Q, const Rheo& c, const StepScalars* S,
-                                               int i, int n, float& in0, float& in1) {
+// Internal acceleration of a level-0 particle over its neighbour table.
+__device__ __forceinline__ void internal_force(const PState& A, const Search& Q, const Rheo& c, int i, int n,
+                                               float& in0, float& in1) {
     float4 me = Q.xhm[i];
     float2 xi = make_float2(me.x, me.y);
     float hi = me.z;
@@ -607,12 +573,6 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
         PairGeom g;
         pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
         pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
-    }
-    const int nreg = S->nreg, nbig = S->nbig;
-    for (int j = nreg; j < nreg + nbig; j++) {
-        float4 o = Q.xhm[j];
-        PairGeom g;
-        if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
     }
     in0 = (float)a0;
     in1 = (float)a1;
@@ -648,7 +608,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
         }
         float in0, in1;
         if (i < nreg) {
-            internal_force(A, Q, c, S, i, n, in0, in1);
+            internal_force(A, Q, c, i, n, in0, in1);
         } else {
             float2 f = Q.indv_big[i - nreg];
             in0 = f.x;
@@ -748,7 +708,7 @@ __device__ __forceinline__ void xsph_pair(const Rheo& c, float2 vi, float rhoi, 
 __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S, Rheo c, int n, PState B,
                                                const float2* velfin) {
     if (S->skip || !c.av_vel) return;
-    const int nreg = S->nreg, nbig = S->nbig;
+    const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         if (B.flag[i]) continue;
         float4 me = Q.xhm[i];
@@ -764,12 +724,6 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
             PairGeom g;
             pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
             xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
-        }
-        for (int j = nreg; j < nreg + nbig; j++) {
-            float4 o = Q.xhm[j];
-            PairGeom g;
-            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g))
-                xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
