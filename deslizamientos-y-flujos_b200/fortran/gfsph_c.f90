@@ -139,6 +139,14 @@ module gfsph_c
        real(c_float), value :: dx, dy
        real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
      end function
+     ! allocation-free depth raster: device pointers in and out (c_devptr from CUDA Fortran or c_loc)
+     integer(c_int) function gfsph_raster_idw_noalloc(n, d_x, d_rho, d_flag, nx, ny, xmin, ymin, dx, dy, d_out, &
+          stream) bind(c, name="gfsph_raster_idw_noalloc")
+       import :: c_int, c_ptr, c_float
+       integer(c_int), value :: n, nx, ny
+       type(c_ptr), value :: d_x, d_rho, d_flag, d_out, stream
+       real(c_float), value :: xmin, ymin, dx, dy
+     end function
      type(c_ptr) function gfsph_strerror(status) bind(c, name="gfsph_strerror")
        import :: c_int, c_ptr
        integer(c_int), value :: status

@@ -78,6 +78,8 @@ SIGNATURES = {
     "gfsph_kernel_name": (C.c_char_p, [C.c_int]),
     "gfsph_launch_count": (C.c_longlong, [C.c_void_p]),
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
+    "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
+                                           C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
     "gfsph_strerror": (C.c_char_p, [C.c_int]),
     "gfsph_version": (C.c_int, []),
 }

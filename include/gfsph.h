@@ -187,6 +187,23 @@ long long gfsph_launch_count(gfsph_handle* h);
  * (GFSPH_NTOPO, nx*ny) column-major; row 1 is read, rows 2..13 written. */
 int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol);
 
+/* Allocation-free variant of the depth raster (GFSPH_RASTER_DEPTH_IDW), for
+ * callers that cannot allocate device memory once their run has started (a
+ * host that reserves all device memory up front, or one embedded in a
+ * framework that owns the allocator).  It has no counterpart in the
+ * reference.  Inputs and output are device pointers owned by the caller:
+ * d_x (2,n), d_rho (n), d_flag (n, may be NULL = all inside), d_out (nx*ny).
+ * The per-node accumulators live in a fixed device array of
+ * GFSPH_NOALLOC_MAX_NODES nodes (16 MiB, held by every GPU that loads the
+ * library until exit); larger grids are rejected with GFSPH_ERR_CAPACITY.
+ * The first call on a device looks up that array's device address (make it
+ * before any stream capture).  Every call shares the array: calls that
+ * overlap on the GPU race.  The work is enqueued on `stream`
+ * (cudaStream_t, NULL = default stream) and nothing is allocated or freed. */
+#define GFSPH_NOALLOC_MAX_NODES (1 << 20)
+int gfsph_raster_idw_noalloc(int n, const float* d_x, const float* d_rho, const int* d_flag, int nx, int ny,
+                             float xmin, float ymin, float dx, float dy, float* d_out, void* stream);
+
 const char* gfsph_strerror(int status);
 int gfsph_version(void);
 
