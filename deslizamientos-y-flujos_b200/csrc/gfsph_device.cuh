@@ -68,6 +68,25 @@ __device__ __forceinline__ bool pair_test(float2 xi, float2 xj, float hi, float 
     return g.r < 2.f * g.mh;
 }
 
+// The same test for a search over candidates, with a cheap early reject:
+// sqrt_rn(dr) < t implies dr < t*t in exact arithmetic, and
+// dr > fl(fl(t*t) * (1 + 1e-5)) implies dr >= t*t (the two roundings move
+// t*t by at most 2^-23 relative), so the reject never drops a pair that the
+// exact test keeps.
+__device__ __forceinline__ bool pair_search(float2 xi, float2 xj, float hi, float hj, PairGeom& g) {
+    float d0 = xi.x - xj.x;
+    float d1 = xi.y - xj.y;
+    float dr = d0 * d0;
+    dr = dr + d1 * d1;
+    float t = 2.f * ((hi + hj) / 2.f);
+    if (dr > (t * t) * 1.00001f) return false;
+    g.dx0 = d0;
+    g.dx1 = d1;
+    g.mh = (hi + hj) / 2.f;
+    g.r = sqrtf(dr);
+    return g.r < 2.f * g.mh;
+}
+
 // Float <-> order-preserving uint, for atomicMin/atomicMax reductions.
 __device__ __forceinline__ unsigned int f2o(float f) {
     unsigned int b = __float_as_uint(f);

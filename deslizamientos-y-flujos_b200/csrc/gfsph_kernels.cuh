@@ -435,7 +435,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
             if (j == i) continue;
             float4 o = Q.xhm[j];
             PairGeom g;
-            if (pair_test(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+            if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
         }
     }
 }
@@ -557,7 +557,9 @@ __global__ void __launch_bounds__(256) k_force_big(PState A, Search Q, StepScala
     }
 }
 
-// Internal acceleration of a level-0 particle over its neighbour table.
+// Internal acceleration of a level-0 particle over its neighbour table.  The
+// table is read four entries at a time so that four independent gather
+// chains are in flight per thread; the FP64 sum keeps the table order.
 __device__ __forceinline__ void internal_force(const PState& A, const Search& Q, const Rheo& c, int i, int n,
                                                float& in0, float& in1) {
     float4 me = Q.xhm[i];
@@ -566,13 +568,34 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
     float pi_ = Q.pterm[i];
     float rhoi = A.rho[i];
     double a0 = 0.0, a1 = 0.0;
-    int cnt = Q.ncount[i];
-    for (int k = 0; k < cnt; k++) {
-        int j = Q.nbr[(size_t)k * n + i];
-        float4 o = Q.xhm[j];
+    const int cnt = Q.ncount[i];
+    const int* tab = Q.nbr + i;
+    int k = 0;
+    for (; k + 4 <= cnt; k += 4) {
+        int j[4];
+        float4 o[4];
+        float pj[4], rj[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * n);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            o[u] = __ldg(&Q.xhm[j[u]]);
+            pj[u] = __ldg(&Q.pterm[j[u]]);
+            rj[u] = __ldg(&A.rho[j[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            PairGeom g;
+            pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
+            pressure_pair(c, pi_, rhoi, pj[u], rj[u], o[u].w, g, a0, a1);
+        }
+    }
+    for (; k < cnt; k++) {
+        int j = __ldg(tab + (size_t)k * n);
+        float4 o = __ldg(&Q.xhm[j]);
         PairGeom g;
         pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-        pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
+        pressure_pair(c, pi_, rhoi, __ldg(&Q.pterm[j]), __ldg(&A.rho[j]), o.w, g, a0, a1);
     }
     in0 = (float)a0;
     in1 = (float)a1;
@@ -716,14 +739,37 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
         float hi = me.z;
         float2 vi = velfin[i];
         float rhoi = A.rho[i];
-        int cnt = Q.ncount[i];
+        const int cnt = Q.ncount[i];
+        const int* tab = Q.nbr + i;
         double a0 = 0.0, a1 = 0.0;
-        for (int k = 0; k < cnt; k++) {
-            int j = Q.nbr[(size_t)k * n + i];
-            float4 o = Q.xhm[j];
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+            int j[4];
+            float4 o[4];
+            float2 vj[4];
+            float rj[4], mj[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * n);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                o[u] = __ldg(&Q.xhm[j[u]]);
+                vj[u] = velfin[j[u]];
+                rj[u] = __ldg(&A.rho[j[u]]);
+                mj[u] = B.mass[j[u]];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                PairGeom g;
+                pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
+                xsph_pair(c, vi, rhoi, vj[u], rj[u], mj[u], g, a0, a1);
+            }
+        }
+        for (; k < cnt; k++) {
+            int j = __ldg(tab + (size_t)k * n);
+            float4 o = __ldg(&Q.xhm[j]);
             PairGeom g;
             pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-            xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
+            xsph_pair(c, vi, rhoi, velfin[j], __ldg(&A.rho[j]), B.mass[j], g, a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
