@@ -18,14 +18,14 @@ namespace {
 
 enum KernelId {
     K_PREP, K_BOUNDS, K_GRID, K_CLEAR, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
-    K_REORDER, K_DENSITY, K_DENSITY_BIG, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
+    K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
 const char* kKernelNames[K_COUNT] = {
     "k_prep", "k_bounds", "k_grid", "k_clear_cells", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
-    "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_force_big",
+    "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "step_batches"};
 
@@ -123,7 +123,7 @@ struct gfsph_handle {
     int* nbr = nullptr;
     int* ncount = nullptr;
     int kcap = 0;
-    float2* indv_big = nullptr;  // internal force of the level >= 1 particles
+    float2* indv = nullptr;  // internal acceleration of every active particle
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -205,12 +205,12 @@ Search make_search(gfsph_handle* h) {
     q.nbr = h->nbr;
     q.ncount = h->ncount;
     q.pterm = h->pterm;
-    q.indv_big = h->indv_big;
+    q.indv = h->indv;
     q.kcap = h->kcap;
     return q;
 }
 
-int big_blocks(const gfsph_handle*) { return 148 * 2; }
+int big_blocks(const gfsph_handle*) { return 148 * 16; }  // 128 threads: one warp per level >= 1 particle
 
 // The cell search: bounds, grid, counting sort, reorder, neighbours+density.
 // Returns the number of kernels enqueued.
@@ -236,7 +236,7 @@ int enqueue_search(gfsph_handle* h, int advance) {
         k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S);
     }); nk++;
     launch(h, K_DENSITY, [&] { k_density<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
-    launch(h, K_DENSITY_BIG, [&] { k_density_big<<<big_blocks(h), 256, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
+    launch(h, K_DENSITY_BIG, [&] { k_density_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
     return nk;
 }
 
@@ -247,13 +247,14 @@ int enqueue_step(gfsph_handle* h) {
     Search q = make_search(h);
     int pb = blocks_for(n);
     int nk = enqueue_search(h, 1);
-    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 256, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
+    launch(h, K_IFORCE, [&] { k_iforce<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
+    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
     launch(h, K_FORCE_RK, [&] {
         k_force_rk<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
     }); nk++;
     if (h->rheo.av_vel) {
         launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B, h->velfin); }); nk++;
-        launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 256, 0, st>>>(h->A, q, S, h->rheo, h->B, h->velfin); }); nk++;
+        launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, S, h->rheo, h->B, h->velfin); }); nk++;
     }
     if (h->rheo.erosion) {
         launch(h, K_DEM_ERODE, [&] { k_dem_erode<<<148 * 2, 256, 0, st>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S); });
@@ -277,7 +278,7 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 13 + 2 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 13 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
 }
 
 int alloc_cells(gfsph_handle* h, int cap) {
@@ -308,7 +309,7 @@ void free_particles(gfsph_handle* h) {
         dfree(p->pos); dfree(p->vel); dfree(p->rho); dfree(p->mass); dfree(p->hsml); dfree(p->flag); dfree(p->id);
     }
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
-    dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv_big);
+    dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv);
     h->kcap = 0;
 }
 
@@ -542,7 +543,7 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
         st |= alloc_pstate(&h->A, n); st |= alloc_pstate(&h->B, n); st |= alloc_pstate(&h->U, n);
         st |= dalloc(&h->cellA, n); st |= dalloc(&h->velfin, n); st |= dalloc(&h->pterm, n);
         st |= dalloc(&h->keyrank, n); st |= dalloc(&h->perm, n); st |= dalloc(&h->ncount, n);
-        st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n); st |= dalloc(&h->indv_big, n);
+        st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n); st |= dalloc(&h->indv, n);
         if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
         if (st) return st;
@@ -701,7 +702,8 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
     int n = h->n;
     cudaStream_t s = h->stream;
     Search q = make_search(h);
-    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 256, 0, s>>>(h->A, q, h->S, h->rheo); });
+    launch(h, K_IFORCE, [&] { k_iforce<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, n); });
+    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, s>>>(h->A, q, h->S, h->rheo); });
     launch(h, K_FORCE_RK, [&] {
         k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 1,
                                                      h->velfin);
@@ -737,7 +739,7 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
             if (dalloc(&dpairs, pcap) || dalloc(&dcount, 1)) { dfree(dpairs); dfree(dcount); return GFSPH_ERR_CUDA; }
             cudaMemset(dcount, 0, sizeof(int));
             Search q = make_search(h);
-            launch(h, K_EXPORT, [&] { k_export_big<<<big_blocks(h), 256, 0, h->stream>>>(q, h->S, dpairs, dcount, pcap); });
+            launch(h, K_EXPORT, [&] { k_export_big<<<big_blocks(h), 128, 0, h->stream>>>(q, h->S, dpairs, dcount, pcap); });
             cudaStreamSynchronize(h->stream);
             int np = 0;
             cudaMemcpy(&np, dcount, sizeof(int), cudaMemcpyDeviceToHost);
@@ -857,5 +859,15 @@ int gfsph_profile_read(gfsph_handle* h, int kernel, double* total_ms, long long*
 }
 
 long long gfsph_launch_count(gfsph_handle* h) { return h ? h->launches : -1; }
+
+int gfsph_stats(gfsph_handle* h, int* out, int nout) {
+    if (!h || !out || nout < 1) return GFSPH_ERR_ARG;
+    int st = read_scalars(h);
+    if (st) return st;
+    const StepScalars* s = h->hS;
+    const int v[8] = {s->nactive, s->nreg, s->nbig, s->nlev, s->ncells, h->kcap, h->cap_cells, s->nout};
+    for (int k = 0; k < nout && k < 8; k++) out[k] = v[k];
+    return GFSPH_OK;
+}
 
 }  // extern "C"

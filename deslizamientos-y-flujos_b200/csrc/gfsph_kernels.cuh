@@ -62,7 +62,7 @@ struct Search {
     int* nbr;            // k-major neighbour table of the regular particles
     int* ncount;
     float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
-    float2* indv_big;    // internal force of the level >= 1 particles (slot - nreg)
+    float2* indv;        // internal acceleration of every active particle (slot order)
     int kcap;
 };
 
@@ -475,42 +475,59 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
     }
 }
 
-// Visits every neighbour j of particle i cooperatively over the block.
+// Visits every neighbour j of particle i cooperatively over one warp: the
+// lanes fetch the slot ranges of up to 32 stencil rows at once, then share
+// each row's candidates.
 template <class F>
-__device__ __forceinline__ void block_neighbours(const Search& Q, const StepScalars* S, int i, F&& f) {
-    float4 me = Q.xhm[i];
-    float2 xi = make_float2(me.x, me.y);
-    for (int k = 0; k < S->nlev; k++) level_neighbours(Q, S, k, i, xi, me.z, threadIdx.x, blockDim.x, f);
+__device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScalars* S, int i, int lane, F&& f) {
+    const float4 me = Q.xhm[i];
+    const float2 xi = make_float2(me.x, me.y);
+    const float hi = me.z;
+    for (int k = 0; k < S->nlev; k++) {
+        const int ndx = S->lev_ndx[k], ndy = S->lev_ndy[k], off = S->lev_off[k];
+        float rr = (hi + ldexpf(S->hc, k)) / S->lev_c[k] + 0.01f;
+        int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
+        int cx, cy;
+        cell_of(xi, S, k, cx, cy);
+        int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
+        int y0 = max(cy - R, 0), y1 = min(cy + R, ndy - 1);
+        for (int yb = y0; yb <= y1; yb += 32) {
+            int jy = yb + lane, ja = 0, jb = 0;
+            if (jy <= y1) {
+                int row = off + jy * ndx;
+                ja = Q.start[row + x0];
+                jb = Q.start[row + x1 + 1];
+            }
+            int nrows = min(32, y1 - yb + 1);
+            for (int r = 0; r < nrows; r++) {
+                int a = __shfl_sync(0xffffffffu, ja, r), e = __shfl_sync(0xffffffffu, jb, r);
+                for (int j = a + lane; j < e; j += 32) {
+                    if (j == i) continue;
+                    float4 o = Q.xhm[j];
+                    PairGeom g;
+                    if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+                }
+            }
+        }
+    }
 }
 
-template <class T>
-__device__ __forceinline__ T block_sum(T v, T* sh) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) sh[wid] = v;
-    __syncthreads();
-    T t = 0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
-    return t;  // valid in thread 0
-}
-
-// Summation density of the big particles, one block per particle.
-__global__ void __launch_bounds__(256) k_density_big(PState A, Search Q, StepScalars* S, Rheo c) {
+// Summation density of the level >= 1 particles, one warp per particle.
+__global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepScalars* S, Rheo c) {
     if (S->skip) return;
-    __shared__ double sh[8];
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nreg = S->nreg, nbig = S->nbig;
-    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+    for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
         double acc = 0.0;
-        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
         });
-        double tot = block_sum(acc, sh);
-        if (threadIdx.x == 0) {
+        acc = warp_sum(acc);
+        if (lane == 0) {
             float4 me = Q.xhm[i];
-            float h = (float)((double)(sph_kernel_w(c.skf, 0.f, me.z) * me.w) + tot);
+            float h = (float)((double)(sph_kernel_w(c.skf, 0.f, me.z) * me.w) + acc);
             A.rho[i] = h;
             float hc = (h < c.h_inf) ? c.h_inf : h;
             float p = (c.cgra05 * hc) * hc;
@@ -539,21 +556,22 @@ __device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rh
     a1 += (double)(mj * h1);
 }
 
-// Internal acceleration of the big particles, one block per particle.
-__global__ void __launch_bounds__(256) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
+// Internal acceleration of the level >= 1 particles, one warp per particle.
+__global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
     if (S->skip) return;
-    __shared__ double sh[8];
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nreg = S->nreg, nbig = S->nbig;
-    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+    for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
         float pi_ = Q.pterm[i], rhoi = A.rho[i];
         double a0 = 0.0, a1 = 0.0;
-        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
         });
-        double t0 = block_sum(a0, sh);
-        double t1 = block_sum(a1, sh);
-        if (threadIdx.x == 0) Q.indv_big[b] = make_float2((float)t0, (float)t1);
+        a0 = warp_sum(a0);
+        a1 = warp_sum(a1);
+        if (lane == 0) Q.indv[i] = make_float2((float)a0, (float)a1);
     }
 }
 
@@ -601,8 +619,20 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
     in1 = (float)a1;
 }
 
-// The RK45 body for each active particle, entirely in registers: internal
-// acceleration (stage-invariant, see below), four stages of
+// Internal acceleration of the level-0 particles, one thread each.
+__global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+    if (S->skip) return;
+    const int nreg = S->nreg;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
+        float in0, in1;
+        internal_force(A, Q, c, i, n, in0, in1);
+        Q.indv[i] = make_float2(in0, in1);
+    }
+}
+
+// The RK45 body for each active particle, entirely in registers: the
+// internal acceleration (stage-invariant, see below; from k_iforce or
+// k_force_big), four stages of
 // x = x0 + c_i dt v, v = v0 + c_i dt (ex + in) with ExtForces_SW(0) at each
 // stage (SPH_MAIN_2019.f90:808-906), the final update (:908-922), the
 // out-of-domain freeze (Check_Out_Domain), Hungr erosion of mass and the DEM
@@ -618,7 +648,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
                                                    PState B, float2* velfin, double2* auxv, int forces_only,
                                                    float2* indv_out) {
     if (S->skip) return;
-    const int nact = S->nactive, nreg = S->nreg;
+    const int nact = S->nactive;
     const float dt = S->dt_step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (i >= nact) {  // carried particles (out of the domain at step start)
@@ -629,15 +659,9 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
             }
             continue;
         }
-        float in0, in1;
-        if (i < nreg) {
-            internal_force(A, Q, c, i, n, in0, in1);
-        } else {
-            float2 f = Q.indv_big[i - nreg];
-            in0 = f.x;
-            in1 = f.y;
-        }
-        if (forces_only) { indv_out[i] = make_float2(in0, in1); continue; }
+        const float2 fin = Q.indv[i];
+        const float in0 = fin.x, in1 = fin.y;
+        if (forces_only) { indv_out[i] = fin; continue; }
 
         const float h = A.rho[i];
         const float hc = (h < c.h_inf) ? c.h_inf : h;  // IntForces_SW clamp, seen by ExtForces_SW(0)
@@ -776,24 +800,25 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
     }
 }
 
-__global__ void __launch_bounds__(256) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B,
+__global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B,
                                                    const float2* velfin) {
     if (S->skip || !c.av_vel) return;
-    __shared__ double sh[8];
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nreg = S->nreg, nbig = S->nbig;
-    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+    for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
-        if (B.flag[i]) continue;  // uniform over the block
+        if (B.flag[i]) continue;  // uniform over the warp
         float2 vi = velfin[i];
         float rhoi = A.rho[i];
         double a0 = 0.0, a1 = 0.0;
-        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
         });
-        double t0 = block_sum(a0, sh);
-        double t1 = block_sum(a1, sh);
-        if (threadIdx.x == 0) {
-            float av0 = 0.3f * (float)t0, av1 = 0.3f * (float)t1;
+        a0 = warp_sum(a0);
+        a1 = warp_sum(a1);
+        if (lane == 0) {
+            float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
             B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
         }
     }
@@ -833,13 +858,15 @@ __global__ void k_step_end(StepScalars* S) {
     S->steps_done += 1;
 }
 
-// Neighbour pairs of the big particles, for the parity export: every
+// Neighbour pairs of the level >= 1 particles, for the parity export: every
 // (big i, j) pair with r < hi + hj, written as slot pairs.
 __global__ void k_export_big(Search Q, StepScalars* S, int2* pairs, int* npairs, int cap) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nreg = S->nreg, nbig = S->nbig;
-    for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+    for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
-        block_neighbours(Q, S, i, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             int k = atomicAdd(npairs, 1);
             if (k < cap) pairs[k] = make_int2(i, j);
         });

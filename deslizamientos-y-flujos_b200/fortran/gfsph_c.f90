@@ -133,6 +133,12 @@ module gfsph_c
        import :: c_long_long, c_ptr
        type(c_ptr), value :: handle
      end function
+     integer(c_int) function gfsph_stats(handle, out, nout) bind(c, name="gfsph_stats")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle
+       integer(c_int), intent(out) :: out(*)
+       integer(c_int), value :: nout
+     end function
      integer(c_int) function gfsph_dem_topol(mode, nx, ny, dx, dy, topol) bind(c, name="gfsph_dem_topol")
        import :: c_int, c_float
        integer(c_int), value :: mode, nx, ny

@@ -77,6 +77,7 @@ SIGNATURES = {
     "gfsph_num_kernels": (C.c_int, []),
     "gfsph_kernel_name": (C.c_char_p, [C.c_int]),
     "gfsph_launch_count": (C.c_longlong, [C.c_void_p]),
+    "gfsph_stats": (C.c_int, [C.c_void_p, _IP, C.c_int]),
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
     "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
@@ -270,3 +271,9 @@ class Sim:
 
     def launch_count(self):
         return int(lib().gfsph_launch_count(self.h))
+
+    def stats(self):
+        v = np.zeros(8, np.int32)
+        _check(lib().gfsph_stats(self.h, _ip(v), 8), "gfsph_stats")
+        keys = ("active", "level0", "coarse", "levels", "cells", "table_capacity", "cell_capacity", "outside")
+        return dict(zip(keys, (int(a) for a in v)))

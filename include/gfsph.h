@@ -180,6 +180,12 @@ const char* gfsph_kernel_name(int kernel);
  * each kernel node). */
 long long gfsph_launch_count(gfsph_handle* h);
 
+/* Search statistics of the last step: out[0] active particles, [1] level-0
+ * particles, [2] particles on the coarser levels, [3] levels, [4] cells,
+ * [5] neighbour-table capacity per particle, [6] cell capacity, [7] particles
+ * outside the DEM box.  Up to nout values are written. */
+int gfsph_stats(gfsph_handle* h, int* out, int nout);
+
 /* Derives the DEM slope/curvature rows topol(2..13,:) from topol(1,:) on the
  * host, once, as Topo_main does before the time loop: mode 0 = lumped-mass
  * FEM projection with 5 Jacobi sweeps (Get_Topol, SPH_FEM_topo_2019.f90:1723-1939),
