@@ -619,6 +619,62 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
     in1 = (float)a1;
 }
 
+// DEM scatter of ExtForces_SW(1) (SPH_SW_2019.f90:8731-8750): the particle
+// adds base/dist and 1/dist to the 4x4 DEM nodes around its DEM cell.
+// Particles sorted by cell mostly share a DEM cell, so the lanes of a warp
+// that share one are summed with shuffles first and one lane issues the
+// atomics (sums stay FP64).  Lanes with part == false take no part; every
+// lane of the warp must call this.
+__device__ __forceinline__ void erosion_scatter(const DemView& dem, StepScalars* S, float xx, float xy, float base,
+                                                bool part, double2* auxv) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int ipx = 0, ipy = 0, key = -1;
+    if (part) {
+        ipx = (int)((xx - dem.xmin) / dem.dx + 1.f);
+        ipy = (int)((xy - dem.ymin) / dem.dy + 1.f);
+        key = ipy * (dem.nx + 2) + ipx;
+    }
+    unsigned todo = __ballot_sync(full, key >= 0);
+    while (todo) {
+        const int leader = __ffs(todo) - 1;
+        const int lkey = __shfl_sync(full, key, leader);
+        const unsigned grp = __ballot_sync(full, key == lkey) & todo;
+        const bool mine = (grp >> lane) & 1u;
+        const int gpx = __shfl_sync(full, ipx, leader), gpy = __shfl_sync(full, ipy, leader);
+        const int ix0 = max(1, gpx - 1), iy0 = max(1, gpy - 1);
+        const int ix1 = min(dem.nx, gpx + 2), iy1 = min(dem.ny, gpy + 2);
+        for (int ix = ix0; ix <= ix1; ix++)
+            for (int iy = iy0; iy <= iy1; iy++) {
+                double a = 0.0, b = 0.0;
+                if (mine) {
+                    float ddx = xx - (dem.xmin + (float)(ix - 1) * dem.dx);
+                    ddx = ddx * ddx;
+                    float ddy = xy - (dem.ymin + (float)(iy - 1) * dem.dy);
+                    ddy = ddy * ddy;
+                    float dist = sqrtf(ddx + ddy);
+                    dist = (1.e-6f > dist) ? 1.e-6f : dist;
+                    a = (double)(base / dist);
+                    b = (double)(1.f / dist);
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    a += __shfl_xor_sync(full, a, o);
+                    b += __shfl_xor_sync(full, b, o);
+                }
+                if (lane == leader) {
+                    int ip = (iy - 1) * dem.nx + (ix - 1);
+                    atomicAdd(&auxv[ip].x, a);
+                    atomicAdd(&auxv[ip].y, b);
+                }
+            }
+        if (lane == leader) {
+            atomicMin(&S->ex0, ix0); atomicMax(&S->ex1, ix1);
+            atomicMin(&S->ey0, iy0); atomicMax(&S->ey1, iy1);
+        }
+        todo &= ~grp;
+    }
+}
+
 // Internal acceleration of the level-0 particles, one thread each.
 __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip) return;
@@ -650,19 +706,27 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
     if (S->skip) return;
     const int nact = S->nactive;
     const float dt = S->dt_step;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (forces_only) {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x)
+            indv_out[i] = Q.indv[i];
+        return;
+    }
+    // block-uniform trip count: every lane of a warp reaches erosion_scatter
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        if (i >= n) {
+            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
+            continue;
+        }
         if (i >= nact) {  // carried particles (out of the domain at step start)
-            if (!forces_only) {
-                B.pos[i] = A.pos[i]; B.vel[i] = A.vel[i]; velfin[i] = A.vel[i];
-                B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
-                B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
-            }
+            B.pos[i] = A.pos[i]; B.vel[i] = A.vel[i]; velfin[i] = A.vel[i];
+            B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
+            B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
+            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
             continue;
         }
         const float2 fin = Q.indv[i];
         const float in0 = fin.x, in1 = fin.y;
-        if (forces_only) { indv_out[i] = fin; continue; }
-
         const float h = A.rho[i];
         const float hc = (h < c.h_inf) ? c.h_inf : h;  // IntForces_SW clamp, seen by ExtForces_SW(0)
         const float2 x0 = A.pos[i], v0 = A.vel[i];
@@ -702,30 +766,11 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
             vy = v0.y + dt6 * Dv1;
             out = out_of_box(dem, xx, xy);
         }
+        float er = 0.f;
+        if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h);
+        if (c.erosion) erosion_scatter(dem, S, xx, xy, dt * er, !out, auxv);
         if (!out) {
-            if (c.erosion) {
-                float er = erosion_rate_final(c, dem, xx, xy, vx, vy, h);
-                float base = dt * er;
-                int ipx = (int)((xx - dem.xmin) / dem.dx + 1.f);
-                int ipy = (int)((xy - dem.ymin) / dem.dy + 1.f);
-                int ix0 = max(1, ipx - 1), iy0 = max(1, ipy - 1);
-                int ix1 = min(dem.nx, ipx + 2), iy1 = min(dem.ny, ipy + 2);
-                for (int ix = ix0; ix <= ix1; ix++)
-                    for (int iy = iy0; iy <= iy1; iy++) {
-                        int ip = (iy - 1) * dem.nx + (ix - 1);
-                        float ddx = xx - (dem.xmin + (float)(ix - 1) * dem.dx);
-                        ddx = ddx * ddx;
-                        float ddy = xy - (dem.ymin + (float)(iy - 1) * dem.dy);
-                        ddy = ddy * ddy;
-                        float dist = sqrtf(ddx + ddy);
-                        dist = (1.e-6f > dist) ? 1.e-6f : dist;
-                        atomicAdd(&auxv[ip].x, (double)(base / dist));
-                        atomicAdd(&auxv[ip].y, (double)(1.f / dist));
-                    }
-                atomicMin(&S->ex0, ix0); atomicMax(&S->ex1, ix1);
-                atomicMin(&S->ey0, iy0); atomicMax(&S->ey1, iy1);
-                m = m + ((dt * er) * m) / h;
-            }
+            if (c.erosion) m = m + ((dt * er) * m) / h;
             if (c.sle == 1) hs = 2.f * sqrtf(m / h);
         }
         B.pos[i] = make_float2(xx, xy);
