@@ -621,57 +621,60 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
 
 // DEM scatter of ExtForces_SW(1) (SPH_SW_2019.f90:8731-8750): the particle
 // adds base/dist and 1/dist to the 4x4 DEM nodes around its DEM cell.
-// Particles sorted by cell mostly share a DEM cell, so the lanes of a warp
-// that share one are summed with shuffles first and one lane issues the
-// atomics (sums stay FP64).  Lanes with part == false take no part; every
-// lane of the warp must call this.
+// Consecutive particles of the cell-sorted order mostly share a DEM cell, so
+// within a warp the lanes form runs of equal DEM cell; a segmented FP64 scan
+// (five shuffle steps) sums every run at once and only the last lane of each
+// run issues the atomics.  Lanes with part == false take no part; every lane
+// of the warp must call this.
 __device__ __forceinline__ void erosion_scatter(const DemView& dem, StepScalars* S, float xx, float xy, float base,
                                                 bool part, double2* auxv) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    int ipx = 0, ipy = 0, key = -1;
+    int ipx = 0, ipy = 0, key = -1 - lane;  // non-participants: singleton runs with zero values
     if (part) {
         ipx = (int)((xx - dem.xmin) / dem.dx + 1.f);
         ipy = (int)((xy - dem.ymin) / dem.dy + 1.f);
         key = ipy * (dem.nx + 2) + ipx;
     }
-    unsigned todo = __ballot_sync(full, key >= 0);
-    while (todo) {
-        const int leader = __ffs(todo) - 1;
-        const int lkey = __shfl_sync(full, key, leader);
-        const unsigned grp = __ballot_sync(full, key == lkey) & todo;
-        const bool mine = (grp >> lane) & 1u;
-        const int gpx = __shfl_sync(full, ipx, leader), gpy = __shfl_sync(full, ipy, leader);
-        const int ix0 = max(1, gpx - 1), iy0 = max(1, gpy - 1);
-        const int ix1 = min(dem.nx, gpx + 2), iy1 = min(dem.ny, gpy + 2);
-        for (int ix = ix0; ix <= ix1; ix++)
-            for (int iy = iy0; iy <= iy1; iy++) {
-                double a = 0.0, b = 0.0;
-                if (mine) {
-                    float ddx = xx - (dem.xmin + (float)(ix - 1) * dem.dx);
-                    ddx = ddx * ddx;
-                    float ddy = xy - (dem.ymin + (float)(iy - 1) * dem.dy);
-                    ddy = ddy * ddy;
-                    float dist = sqrtf(ddx + ddy);
-                    dist = (1.e-6f > dist) ? 1.e-6f : dist;
-                    a = (double)(base / dist);
-                    b = (double)(1.f / dist);
-                }
-                for (int o = 16; o > 0; o >>= 1) {
-                    a += __shfl_xor_sync(full, a, o);
-                    b += __shfl_xor_sync(full, b, o);
-                }
-                if (lane == leader) {
-                    int ip = (iy - 1) * dem.nx + (ix - 1);
-                    atomicAdd(&auxv[ip].x, a);
-                    atomicAdd(&auxv[ip].y, b);
-                }
+    if (!__any_sync(full, part)) return;
+    const int prev = __shfl_up_sync(full, key, 1);
+    const bool head = (lane == 0) || (prev != key);
+    const unsigned heads = __ballot_sync(full, head);
+    const int first = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));  // head of my run
+    const int next = __shfl_down_sync(full, key, 1);
+    const bool tail = (lane == 31) || (next != key);
+    const int ix0 = max(1, ipx - 1), iy0 = max(1, ipy - 1);
+    const int ix1 = min(dem.nx, ipx + 2), iy1 = min(dem.ny, ipy + 2);
+    // every lane walks the same 4x4 offsets; nodes outside the DEM add zero
+    for (int ox = -1; ox <= 2; ox++)
+        for (int oy = -1; oy <= 2; oy++) {
+            const int ix = ipx + ox, iy = ipy + oy;
+            const bool inside = part && ix >= ix0 && ix <= ix1 && iy >= iy0 && iy <= iy1;
+            double a = 0.0, b = 0.0;
+            if (inside) {
+                float ddx = xx - (dem.xmin + (float)(ix - 1) * dem.dx);
+                ddx = ddx * ddx;
+                float ddy = xy - (dem.ymin + (float)(iy - 1) * dem.dy);
+                ddy = ddy * ddy;
+                float dist = sqrtf(ddx + ddy);
+                dist = (1.e-6f > dist) ? 1.e-6f : dist;
+                a = (double)(base / dist);
+                b = (double)(1.f / dist);
             }
-        if (lane == leader) {
-            atomicMin(&S->ex0, ix0); atomicMax(&S->ex1, ix1);
-            atomicMin(&S->ey0, iy0); atomicMax(&S->ey1, iy1);
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                double ua = __shfl_up_sync(full, a, o), ub = __shfl_up_sync(full, b, o);
+                if (lane - o >= first) { a += ua; b += ub; }
+            }
+            if (tail && inside) {
+                int ip = (iy - 1) * dem.nx + (ix - 1);
+                atomicAdd(&auxv[ip].x, a);
+                atomicAdd(&auxv[ip].y, b);
+            }
         }
-        todo &= ~grp;
+    if (tail && part) {
+        atomicMin(&S->ex0, ix0); atomicMax(&S->ex1, ix1);
+        atomicMin(&S->ey0, iy0); atomicMax(&S->ey1, iy1);
     }
 }
 
