@@ -92,6 +92,22 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def combine_ranks(ms_local, n_local, steps, dist=None, device="cpu"):
+    """Whole-job throughput of N replicas: the slowest rank's device time
+    (max over ranks) and the particle-steps of all ranks.  Returns
+    (ms_max, total particles, particle-steps/s)."""
+    import torch
+    t = torch.tensor([float(ms_local), float(n_local)], dtype=torch.float64, device=device)
+    if dist is not None:
+        ms = t[:1].clone()
+        nn = t[1:].clone()
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        dist.all_reduce(nn, op=dist.ReduceOp.SUM)
+        t = torch.cat([ms, nn])
+    ms_max, n_total = float(t[0].item()), float(t[1].item())
+    return ms_max, n_total, n_total * steps / (ms_max / 1000.0)
+
+
 def dist_setup(n_gpus):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -237,12 +253,8 @@ def main():
             sim.step(1)
         barrier()
     launches = sim.launch_count() - l0
-    ms_total, nsteps = sim.profile_read().get("step_batches", (0.0, 0))
-    t_dev = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
-    ms_total = float(t_dev.item())
-    value = world * n * args.steps / (ms_total / 1000.0)
+    ms_local, nsteps = sim.profile_read().get("step_batches", (0.0, 0))
+    ms_total, n_job, value = combine_ranks(ms_local, n, args.steps, dist, "cuda")
     clocks = clk.summary()
 
     # ---- steady state: K steps in one call, L2 warm (for reference only)
@@ -294,10 +306,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    t_e2e = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * e2e_steps / (float(t_e2e.item()) / 1000.0)
+    _, _, e2e_value = combine_ranks(e2e_ms, n, e2e_steps, dist, "cuda")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

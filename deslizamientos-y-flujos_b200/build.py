@@ -12,6 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libgfsph.so")
+RUN_EXE = os.path.join(HERE, "gfsph_run")
 BUILD_DIR = os.path.join(HERE, "_build")
 
 NVCC_FLAGS = [
@@ -39,8 +40,9 @@ def _run(cmd, log):
 def build(verbose=False, force=False):
     """Compiles csrc/ into libgfsph.so; returns the library path."""
     srcs = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))]
+    srcs += [os.path.join(HERE, "host", f) for f in sorted(os.listdir(os.path.join(HERE, "host")))]
     srcs += [os.path.join(HERE, "..", "include", "gfsph.h")]
-    if not force and os.path.exists(OUT):
+    if not force and os.path.exists(OUT) and os.path.exists(RUN_EXE):
         newest = max(os.path.getmtime(s) for s in srcs)
         if os.path.getmtime(OUT) >= newest:
             return OUT
@@ -49,15 +51,23 @@ def build(verbose=False, force=False):
     log = []
     api_o = os.path.join(BUILD_DIR, "gfsph_api.o")
     noalloc_o = os.path.join(BUILD_DIR, "gfsph_noalloc.o")
+    cg_o = os.path.join(BUILD_DIR, "gfsph_cg.o")
     dem_o = os.path.join(BUILD_DIR, "gfsph_dem.o")
     _run([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "gfsph_api.cu"), "-o", api_o], log)
     _run([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "gfsph_noalloc.cu"), "-o", noalloc_o], log)
+    _run([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "gfsph_cg.cu"), "-o", cg_o], log)
     _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-c",
           os.path.join(CSRC, "gfsph_dem.cpp"), "-o", dem_o], log)
     tmp = OUT + ".tmp"
-    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", api_o, noalloc_o, dem_o,
+    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", api_o, noalloc_o, cg_o, dem_o,
           "-o", tmp, "-lcudart"], log)
     os.replace(tmp, OUT)
+    # the C++ host driver (reads the reference's input files, drives the ABI)
+    host = os.path.join(HERE, "host")
+    run_tmp = RUN_EXE + ".tmp"
+    _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", os.path.join(host, "gfsph_inputs.cpp"),
+          os.path.join(host, "gfsph_run.cpp"), "-L" + HERE, "-lgfsph", "-Wl,-rpath,$ORIGIN", "-o", run_tmp], log)
+    os.replace(run_tmp, RUN_EXE)
     with open(os.path.join(BUILD_DIR, "build.log"), "w") as f:
         f.write("\n".join(log))
     if verbose:

@@ -17,14 +17,14 @@ using namespace gfsph;
 namespace {
 
 enum KernelId {
-    K_PREP, K_BOUNDS, K_GRID, K_CLEAR, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
+    K_PREP, K_BOUNDS, K_GRID, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
 const char* kKernelNames[K_COUNT] = {
-    "k_prep", "k_bounds", "k_grid", "k_clear_cells", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
+    "k_prep", "k_bounds", "k_grid", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "step_batches"};
@@ -98,6 +98,9 @@ struct gfsph_handle {
     int dev = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    cudaStream_t stream2 = nullptr;       // side stream used only inside graph captures
+    cudaEvent_t ev_fork[3]{}, ev_join[3]{};
+    bool capturing = false;
     gfsph_params P;
     Rheo rheo;
     // DEM
@@ -197,6 +200,21 @@ int profile_collect(gfsph_handle* h) {
     return 0;
 }
 
+// Side stream for the coarse-level kernels while a graph is captured.
+cudaStream_t side_stream(gfsph_handle* h) { return h->capturing ? h->stream2 : h->stream; }
+
+void fork(gfsph_handle* h, int k) {
+    if (!h->capturing) return;
+    cudaEventRecord(h->ev_fork[k], h->stream);
+    cudaStreamWaitEvent(h->stream2, h->ev_fork[k], 0);
+}
+
+void join(gfsph_handle* h, int k) {
+    if (!h->capturing) return;
+    cudaEventRecord(h->ev_join[k], h->stream2);
+    cudaStreamWaitEvent(h->stream, h->ev_join[k], 0);
+}
+
 Search make_search(gfsph_handle* h) {
     Search q;
     q.start = h->start;
@@ -222,21 +240,25 @@ int enqueue_search(gfsph_handle* h, int advance) {
     int nk = 0;
     int pb = blocks_for(n);
     int nscan = (h->cap_cells + kScanTile - 1) / kScanTile;
-    launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++;
+    if (!advance) { launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++; }
     launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
     launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_cells); }); nk++;
-    launch(h, K_CLEAR, [&] { k_clear_cells<<<148 * 4, 256, 0, st>>>(h->count, S); }); nk++;
     launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->count, h->keyrank); }); nk++;
     launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, S); }); nk++;
     launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, S); }); nk++;
     launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, S, h->perm); }); nk++;
-    launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, S); }); nk++;
+    launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
     launch(h, K_REORDER, [&] {
         k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S);
     }); nk++;
+    // the coarse-level kernels run beside the level-0 ones when graphs are
+    // captured (side stream); serially otherwise
+    cudaStream_t sb = side_stream(h);
+    fork(h, 0);
+    launch(h, K_DENSITY_BIG, [&] { k_density_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); }); nk++;
     launch(h, K_DENSITY, [&] { k_density<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
-    launch(h, K_DENSITY_BIG, [&] { k_density_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
+    join(h, 0);
     return nk;
 }
 
@@ -247,14 +269,19 @@ int enqueue_step(gfsph_handle* h) {
     Search q = make_search(h);
     int pb = blocks_for(n);
     int nk = enqueue_search(h, 1);
+    cudaStream_t sb = side_stream(h);
+    fork(h, 1);
+    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); }); nk++;
     launch(h, K_IFORCE, [&] { k_iforce<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
-    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, S, h->rheo); }); nk++;
+    join(h, 1);
     launch(h, K_FORCE_RK, [&] {
         k_force_rk<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
     }); nk++;
     if (h->rheo.av_vel) {
+        fork(h, 2);
+        launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo, h->B, h->velfin); }); nk++;
         launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B, h->velfin); }); nk++;
-        launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, S, h->rheo, h->B, h->velfin); }); nk++;
+        join(h, 2);
     }
     if (h->rheo.erosion) {
         launch(h, K_DEM_ERODE, [&] { k_dem_erode<<<148 * 2, 256, 0, st>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S); });
@@ -268,7 +295,9 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     long long before = h->launches;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->capturing = true;
     for (int s = 0; s < steps; s++) enqueue_step(h);
+    h->capturing = false;
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->launches = before;  // capture launches nothing
     if (e != cudaSuccess) return cuda_status(e);
@@ -278,7 +307,7 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 13 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 11 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
 }
 
 int alloc_cells(gfsph_handle* h, int cap) {
@@ -347,9 +376,7 @@ int grow_after_error(gfsph_handle* h) {
         if (want < s->need_cells) return GFSPH_ERR_CAPACITY;
         int st = alloc_cells(h, (int)want);
         if (st) return st;
-        // the previous grid's cell range is gone with the old buffer
         set_field<int>(h, offsetof(StepScalars, ncells), 0);
-        set_field<int>(h, offsetof(StepScalars, ncells_prev), 0);
     }
     if (e & kErrNbr) {
         int want = std::max(s->need_nbr + 16, h->kcap * 3 / 2);
@@ -428,6 +455,15 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
         return GFSPH_ERR_CUDA;
     }
     h->stream = h->own_stream;
+    if (cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(h->own_stream);
+        delete h;
+        return GFSPH_ERR_CUDA;
+    }
+    for (int k = 0; k < 3; k++) {
+        cudaEventCreateWithFlags(&h->ev_fork[k], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming);
+    }
     h->P = *p;
     Rheo& c = h->rheo;
     const float* k = p->cst;  // k[i-1] = const(i)
@@ -517,6 +553,11 @@ int gfsph_destroy(gfsph_handle* h) {
         if (h->ev0[k]) cudaEventDestroy(h->ev0[k]);
         if (h->ev1[k]) cudaEventDestroy(h->ev1[k]);
     }
+    for (int k = 0; k < 3; k++) {
+        if (h->ev_fork[k]) cudaEventDestroy(h->ev_fork[k]);
+        if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
+    }
+    if (h->stream2) cudaStreamDestroy(h->stream2);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return GFSPH_OK;
@@ -611,6 +652,7 @@ int gfsph_step(gfsph_handle* h, int nsteps, double t_end, double* t_out, int* st
         int chunk = std::min(kChunkSteps, nsteps - done);
         set_field<double>(h, offsetof(StepScalars, t_end), t_end);
         set_field<int>(h, offsetof(StepScalars, steps_done), 0);
+        launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, h->stream>>>(h->S, 1); });
         if (h->profile) {
             for (int s = 0; s < chunk; s++) {
                 enqueue_step(h);

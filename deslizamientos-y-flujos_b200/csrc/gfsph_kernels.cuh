@@ -36,7 +36,7 @@ struct StepScalars {
     int nlev;         // number of grid levels
     float lev_gx0[kMaxLevels], lev_gy0[kMaxLevels], lev_c[kMaxLevels];  // origin and cell size per level
     int lev_ndx[kMaxLevels], lev_ndy[kMaxLevels], lev_off[kMaxLevels + 1];  // cells per level, first cell key
-    int ncells, ncells_prev;
+    int ncells;
     int nreg, nbig, nactive, nout;
     int need_cells, need_nbr, need_big;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
@@ -69,8 +69,10 @@ struct Search {
 __device__ __forceinline__ bool step_skipped(const StepScalars* S) { return S->skip != 0; }
 
 // ---------------------------------------------------------------- prologue
-__global__ void k_prep(StepScalars* S, int advance) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Decides whether the coming step runs and resets its reductions; run at the
+// start of a batch (k_prep) and at the end of every step for the next one
+// (k_step_end).
+__device__ __forceinline__ void prepare_step(StepScalars* S, int advance) {
     S->advance = advance;
     S->skip = (S->err != 0) || (advance && S->time >= S->t_end);
     S->xmin_o = 0xffffffffu; S->ymin_o = 0xffffffffu;
@@ -82,6 +84,11 @@ __global__ void k_prep(StepScalars* S, int advance) {
     S->nout = 0;
     S->nbig = 0;
     S->ex0 = 0x7fffffff; S->ey0 = 0x7fffffff; S->ex1 = -1; S->ey1 = -1;
+}
+
+__global__ void k_prep(StepScalars* S, int advance) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    prepare_step(S, advance);
 }
 
 __device__ __forceinline__ float warp_min(float v) {
@@ -213,16 +220,7 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
         S->skip = 1;
         return;
     }
-    S->ncells_prev = S->ncells;
     S->ncells = (int)off;
-}
-
-// Clears the cell histogram over [0, max(ncells, ncells_prev)] (+1 for the
-// scan's total slot).
-__global__ void k_clear_cells(int* count, const StepScalars* S) {
-    if (S->skip) return;
-    int m = max(S->ncells, S->ncells_prev) + 1;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) count[k] = 0;
 }
 
 __device__ __forceinline__ void cell_of(float2 p, const StepScalars* S, int k, int& cx, int& cy) {
@@ -386,11 +384,15 @@ __device__ __forceinline__ void insertion_sort_by_id(int* perm, const int* id_ol
     }
 }
 
-__global__ void k_cell_sort(int* perm, const int* id_old, const int* start, const StepScalars* S) {
+// Also zeroes the histogram it no longer needs, so the counts start at zero
+// in the next step without a clearing pass.
+__global__ void k_cell_sort(int* perm, const int* id_old, const int* start, int* count, const StepScalars* S) {
     if (S->skip) return;
     int nc = S->ncells;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         insertion_sort_by_id(perm, id_old, start[c], start[c + 1]);
+        count[c] = 0;
+    }
 }
 
 // Gathers the state into the new (cell-sorted) order.
@@ -900,10 +902,12 @@ __global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail
 
 __global__ void k_step_end(StepScalars* S) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (S->skip || !S->advance) return;
-    S->dt = S->dt_step;
-    S->time += (double)S->dt;
-    S->steps_done += 1;
+    if (!S->skip && S->advance) {
+        S->dt = S->dt_step;
+        S->time += (double)S->dt;
+        S->steps_done += 1;
+    }
+    prepare_step(S, 1);
 }
 
 // Neighbour pairs of the level >= 1 particles, for the parity export: every

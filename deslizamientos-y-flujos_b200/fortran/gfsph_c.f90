@@ -145,6 +145,44 @@ module gfsph_c
        real(c_float), value :: dx, dy
        real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
      end function
+     integer(c_int) function gfsph_cg_create(npoin, nelem, nnode, ndofn, intmat, gstif, cg) bind(c, name="gfsph_cg_create")
+       import :: c_int, c_ptr, c_float
+       integer(c_int), value :: npoin, nelem, nnode, ndofn
+       integer(c_int), intent(in) :: intmat(nnode, nelem)
+       real(c_float), intent(in) :: gstif(nnode*ndofn, nnode*ndofn, nelem)
+       type(c_ptr), intent(out) :: cg
+     end function
+     integer(c_int) function gfsph_cg_solve(cg, iffix, fixed, rcg, ficg, tol, iterations) bind(c, name="gfsph_cg_solve")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: cg
+       integer(c_int), intent(inout) :: iffix(*)
+       real(c_float), intent(in) :: fixed(*)
+       real(c_float), intent(inout) :: rcg(*)
+       real(c_float), intent(out) :: ficg(*)
+       real(c_float), value :: tol
+       integer(c_int), intent(out) :: iterations
+     end function
+     integer(c_int) function gfsph_cg_destroy(cg) bind(c, name="gfsph_cg_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: cg
+     end function
+     integer(c_long_long) function gfsph_cg_launch_count(cg) bind(c, name="gfsph_cg_launch_count")
+       import :: c_long_long, c_ptr
+       type(c_ptr), value :: cg
+     end function
+     ! drop-in for: call solvegc2(npoin, nelem, nnode, ndofn, ntotv, nevab, intmat, iffix, fixed, gstif, rcg, ficg, tolCG)
+     integer(c_int) function gfsph_solvegc2(npoin, nelem, nnode, ndofn, intmat, iffix, fixed, gstif, rcg, ficg, &
+          tol, iterations) bind(c, name="gfsph_solvegc2")
+       import :: c_int, c_float
+       integer(c_int), value :: npoin, nelem, nnode, ndofn
+       integer(c_int), intent(in) :: intmat(nnode, nelem)
+       integer(c_int), intent(inout) :: iffix(*)
+       real(c_float), intent(in) :: fixed(*), gstif(nnode*ndofn, nnode*ndofn, nelem)
+       real(c_float), intent(inout) :: rcg(*)
+       real(c_float), intent(out) :: ficg(*)
+       real(c_float), value :: tol
+       integer(c_int), intent(out) :: iterations
+     end function
      ! allocation-free depth raster: device pointers in and out (c_devptr from CUDA Fortran or c_loc)
      integer(c_int) function gfsph_raster_idw_noalloc(n, d_x, d_rho, d_flag, nx, ny, xmin, ymin, dx, dy, d_out, &
           stream) bind(c, name="gfsph_raster_idw_noalloc")

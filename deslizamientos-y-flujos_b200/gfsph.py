@@ -81,6 +81,11 @@ SIGNATURES = {
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
     "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "gfsph_cg_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _IP, _FP, C.POINTER(C.c_void_p)]),
+    "gfsph_cg_solve": (C.c_int, [C.c_void_p, _IP, _FP, _FP, _FP, C.c_float, _IP]),
+    "gfsph_cg_destroy": (C.c_int, [C.c_void_p]),
+    "gfsph_cg_launch_count": (C.c_longlong, [C.c_void_p]),
+    "gfsph_solvegc2": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _FP, _FP, _FP, _FP, C.c_float, _IP]),
     "gfsph_strerror": (C.c_char_p, [C.c_int]),
     "gfsph_version": (C.c_int, []),
 }
@@ -277,3 +282,46 @@ class Sim:
         _check(lib().gfsph_stats(self.h, _ip(v), 8), "gfsph_stats")
         keys = ("active", "level0", "coarse", "levels", "cells", "table_capacity", "cell_capacity", "outside")
         return dict(zip(keys, (int(a) for a in v)))
+
+
+class CG:
+    """solvegc2 on the device for a fixed element system (gfsph_cg_*).
+
+    intmat: (nelem, nnode) 1-based; gstif: (nelem, nevab, nevab) with
+    [e, row, col]."""
+
+    def __init__(self, intmat, gstif, ndofn=1):
+        intmat = np.ascontiguousarray(intmat, np.int32)
+        self.nelem, self.nnode = intmat.shape
+        self.npoin = int(intmat.max())
+        self.n = self.npoin * ndofn
+        g = np.ascontiguousarray(np.transpose(gstif, (0, 2, 1)), np.float32)  # Fortran gstif(nevab, nevab, nelem)
+        self._keep = (intmat, g)
+        h = C.c_void_p()
+        _check(lib().gfsph_cg_create(self.npoin, self.nelem, self.nnode, ndofn, _ip(intmat), _fp(g), C.byref(h)),
+               "gfsph_cg_create")
+        self.h = h
+
+    def solve(self, rhs, iffix=None, fixed=None, tol=1e-10):
+        n = self.n
+        fix = np.zeros(n, np.int32) if iffix is None else np.ascontiguousarray(iffix, np.int32).copy()
+        fx = np.zeros(n, np.float32) if fixed is None else np.ascontiguousarray(fixed, np.float32)
+        r = np.ascontiguousarray(rhs, np.float32).copy()
+        x = np.zeros(n, np.float32)
+        it = C.c_int(0)
+        _check(lib().gfsph_cg_solve(self.h, _ip(fix), _fp(fx), _fp(r), _fp(x), tol, C.byref(it)), "gfsph_cg_solve")
+        return x, r, fix, it.value
+
+    def launch_count(self):
+        return int(lib().gfsph_cg_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            lib().gfsph_cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

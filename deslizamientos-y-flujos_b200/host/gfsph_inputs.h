@@ -1,0 +1,80 @@
+// Readers of the Geoflow-SPH input files, for a C++ host that stands in for
+// the reference's Fortran driver: <name>.MASTER.dat (Driver_Input,
+// SPH_FEM_Driver_2019.f90:218-409), <name>.dat (Input_SW, SPH_SW_2019.f90:668-1573),
+// <topo>.top (Topo_main, SPH_FEM_topo_2019.f90:133-637) and <pts>.pts
+// (Read_Source_plus_New, SPH_SW_2019.f90:4999-5272).  Only the subset of
+// options on the implemented step is read; anything else is reported.
+#pragma once
+#include <string>
+#include <vector>
+
+namespace gfsph_host {
+
+struct MasterDat {
+    std::string title;
+    int if_sph = 0, if_gfl = 0, ic_cases_mat = 0;
+    int problem_type = 0, integ_alg = 0;
+    std::string sph_name;
+    float dt = 0.f, time_end = 0.f;
+    int maxtimesteps = 0;
+    int print_step = 0, save_step = 0, plot_step = 0;
+    float dt_sph = 0.f;
+    int ic_adapt = 0;
+};
+
+struct TopoData {
+    int ictop = 0;
+    bool fdiff = false;         // ictop >= 100: slopes by finite differences
+    int nx = 0, ny = 0;
+    float xmin = 0.f, ymin = 0.f, dx = 0.f, dy = 0.f;
+    float xshift = 0.f, yshift = 0.f;
+    std::vector<float> z;       // nx*ny, x fastest
+    std::vector<int> in_model;  // poig_in_model
+};
+
+struct SwDat {
+    int ic_swalg = 0, n_hist = 0, ndimn = 2;
+    int ic_soil = 1, ic_water = 0, ic_vps = 0, ic_abs = 0;
+    int icunk_s = 7;
+    float h_inf = 0.01f;
+    std::string pts_name;
+    int pa_sph = 2, nnps = 2, sle = 1, skf = 1;
+    bool sum_den = true, av_vel = true, virt_part = false, nor_dens = false;
+    float cst[110] = {};        // const(1..110)
+    int ic_k0 = 0;
+    int icpwp = 0;
+};
+
+struct Particles {
+    std::vector<float> x;       // (2, n)
+    std::vector<float> h, mass, hsml;
+    float delt2d = 0.f, facthsml = 0.f;
+    int np_src = 0;
+    double total_volume = 0.0;
+    int n() const { return (int)h.size(); }
+};
+
+// Each reader throws std::runtime_error with the file and the item on failure.
+MasterDat read_master(const std::string& path);
+TopoData read_top(const std::string& path);
+SwDat read_dat(const std::string& path);
+Particles read_pts(const std::string& path, float h_inf, int icunk_s, float xshift, float yshift);
+
+// Fortran list-directed and a60-label reading over a text file.
+class FortranReader {
+  public:
+    explicit FortranReader(const std::string& path);
+    std::string label();                    // one whole line (format a60)
+    std::vector<std::string> values(int n); // n list-directed items, over as many lines as needed
+    int read_int();
+    float read_real();
+    bool read_logical();
+    const std::string& path() const { return path_; }
+
+  private:
+    std::vector<std::string> lines_;
+    size_t line_ = 0;
+    std::string path_;
+};
+
+}  // namespace gfsph_host

@@ -178,3 +178,93 @@ def make_params(w, gfsph_module, **over):
     opts = dict(w.options)
     opts.update(over)
     return gfsph_module.make_params(w.const, **opts)
+
+
+def p1_mesh(nx, ny, d):
+    """The DEM background triangulation (SPH_FEM_topo_2019.f90:583-604): two
+    triangles per grid cell, (n, n+1, n+1+nx) and (n, n+1+nx, n+nx), 1-based
+    node numbers; returns intmat (nelem, 3), coords (npoin, 2)."""
+    iy, ix = np.mgrid[0:ny - 1, 0:nx - 1]
+    node = (iy * nx + ix).reshape(-1) + 1
+    t1 = np.stack([node, node + 1, node + 1 + nx], 1)
+    t2 = np.stack([node, node + 1 + nx, node + nx], 1)
+    intmat = np.empty((2 * node.size, 3), np.int32)
+    intmat[0::2] = t1
+    intmat[1::2] = t2
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    coords = np.stack([xx.reshape(-1) * d, yy.reshape(-1) * d], 1).astype(np.float64)
+    return intmat, coords
+
+
+def p1_mass_matrices(intmat, coords):
+    """Consistent P1 mass matrices (2A/24)*[[2,1,1],[1,2,1],[1,1,2]] per
+    triangle, the system of get_gradhs_w (SPH_GFL_SW_Interactions_2019.f90:483-540)."""
+    p = coords[intmat - 1]
+    a2 = np.abs((p[:, 1, 0] - p[:, 0, 0]) * (p[:, 2, 1] - p[:, 0, 1]) - (p[:, 2, 0] - p[:, 0, 0]) * (p[:, 1, 1] - p[:, 0, 1]))
+    m = np.array([[2.0, 1.0, 1.0], [1.0, 2.0, 1.0], [1.0, 1.0, 2.0]])
+    return (a2 / 24.0)[:, None, None] * m[None, :, :]
+
+
+def write_reference_inputs(w, directory, name):
+    """Writes a workload in the reference's own input formats, so that the
+    Fortran program (or gfsph_run) can read it: <name>.MASTER.dat,
+    <name>.dat, <name>.top (ictop = 100: a grid file with finite-difference
+    slopes) and <name>.pts (the particles as source points on their
+    lattice)."""
+    import os
+    os.makedirs(directory, exist_ok=True)
+    o = w.options
+    c = [0.0] * 60
+    for k, v in w.const.items():
+        if k <= 60:
+            c[k - 1] = float(v)
+    blocks = 1
+    if any(c[15:30]) or any(c[30:45]) or any(c[45:60]):
+        c[10] = -1.0
+        blocks = 2
+    if any(c[30:45]) or any(c[45:60]):
+        c[29] = -1.0
+        blocks = 3
+    if any(c[45:60]):
+        c[44] = -1.0
+        blocks = 4
+    dt = float(o["dt"])
+    with open(os.path.join(directory, name + ".MASTER.dat"), "w") as f:
+        f.write("1\n" + name + " written by gfsph workloads\n")
+        f.write("if_sph if_gfl ic_cases\n  1 0 0\n")
+        f.write("SPH_problem_type SPH_t_integ_Alg\n  1 4\n")
+        f.write("sph problem name\n" + name + "\n")
+        f.write("dt time_end maxtimesteps\n  %g %g 1000000\n" % (dt, dt * w.steps))
+        f.write("print_step save_step plot_step\n  100 100 100\n")
+        f.write("dt_sph ic_adapt\n  %g %d\n" % (dt, o["ic_adapt"]))
+        f.write("Ntime curves max pts\n  0 6\nwin\n0\n")
+    with open(os.path.join(directory, name + ".dat"), "w") as f:
+        f.write("1\n " + name + "\n ic_SW_Alg\n  0\nnhist\n  0\nndimn\n  2\n")
+        f.write("ic_soil ic_water ic_vps ic_abs\n  1 0 0 0\n")
+        f.write("Soil unkno h_inf_SW\n  7 %g\n" % o["h_inf"])
+        f.write("pts file name\n  " + name + "\n")
+        f.write("pa_sph nnps sle skf\n  %d %d %d %d\n" % (o["pa_sph"], o["nnps"], o["sle"], o["skf"]))
+        f.write("sum_den av_vel virt_part nor_dens\n  T %s F F\n" % ("T" if o["average_velocity"] else "F"))
+        for b in range(blocks):
+            f.write("constants %d-%d\n  " % (15 * b + 1, 15 * b + 15) + " ".join("%.9g" % v for v in c[15 * b:15 * b + 15]) + "\n")
+        nfric = int(c[4] + 0.01)
+        if 5 <= nfric <= 10:
+            f.write("K0 activated?\n  0\n")
+        f.write("icpwp\n  0\ncoarse mesh saving utility?\n  0\ncontrol points?\n  0\n")
+        f.write("GID filter\n  1 1 1 1 0 1 0 0 0 1 0 0\nT_change_to_W\n  1.e+12\n")
+    ny, nx = w.z.shape
+    with open(os.path.join(directory, name + ".top"), "w") as f:
+        f.write("ictop\n100\nnpoigx npoigy\n%d %d\nnode x y z\n" % (nx, ny))
+        k = 1
+        for iy in range(ny):
+            for ix in range(nx):
+                f.write("%d %.9g %.9g %.9g\n" % (k, float(np.float32(ix * w.dx)), float(np.float32(iy * w.dy)), float(w.z[iy, ix])))
+                k += 1
+    lattice = float(w.meta["lattice"])
+    facthsml = float(w.hsml[0]) / lattice
+    with open(os.path.join(directory, name + ".pts"), "w") as f:
+        f.write("npoin source  grid spacing  facthsml\n")
+        f.write("%d %.9g %.9g %.9g %.9g\n" % (w.n, lattice, lattice, lattice, facthsml))
+        f.write("X Y h\n")
+        for (xx, yy), hh in zip(w.x.astype(np.float64), w.rho.astype(np.float64)):
+            f.write("%.9g %.9g %.9g\n" % (float(xx), float(yy), float(hh)))

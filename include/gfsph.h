@@ -193,6 +193,33 @@ int gfsph_stats(gfsph_handle* h, int* out, int nout);
  * (GFSPH_NTOPO, nx*ny) column-major; row 1 is read, rows 2..13 written. */
 int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol);
 
+/*
+ * Conjugate gradients of solvegc2 (SPH_GCsolver_2019.f90:16-316) on the device:
+ * Jacobi-preconditioned CG on the element-by-element system sum_e gstif_e,
+ * prescribed dofs (iffix != 0) held at their `fixed` values and masked out
+ * of the products (kbyp, :273-313), stop when r.r / r0.r0 <= tol (squared
+ * norms, :112), at most 10*ntotv iterations.  Vectors and dot products are
+ * FP64 on the device.  Layouts are the reference's: intmat(nnode, nelem)
+ * with 1-based node numbers, gstif(nevab, nevab, nelem) with
+ * nevab = nnode*ndofn, dof index (node-1)*ndofn + idofn; iffix, fixed, rcg,
+ * ficg have ntotv = npoin*ndofn entries.  As in the reference, rcg returns
+ * the last residual and free dofs with a zero diagonal are held (marked -999
+ * during the solve).
+ */
+typedef struct gfsph_cg gfsph_cg;
+
+/* Assembles the element matrices once (CSR on the device). */
+int gfsph_cg_create(int npoin, int nelem, int nnode, int ndofn, const int* intmat, const float* gstif,
+                    gfsph_cg** out);
+/* One solve; replaces a call of solvegc2 on the system made by gfsph_cg_create. */
+int gfsph_cg_solve(gfsph_cg* cg, int* iffix, const float* fixed, float* rcg, float* ficg, float tol,
+                   int* iterations);
+int gfsph_cg_destroy(gfsph_cg* cg);
+long long gfsph_cg_launch_count(gfsph_cg* cg);
+/* solvegc2 with the reference's argument list (create + solve + destroy). */
+int gfsph_solvegc2(int npoin, int nelem, int nnode, int ndofn, const int* intmat, int* iffix, const float* fixed,
+                   const float* gstif, float* rcg, float* ficg, float tol, int* iterations);
+
 /* Allocation-free variant of the depth raster (GFSPH_RASTER_DEPTH_IDW), for
  * callers that cannot allocate device memory once their run has started (a
  * host that reserves all device memory up front, or one embedded in a

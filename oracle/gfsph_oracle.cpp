@@ -933,9 +933,112 @@ int dem_topol_mode(int mode, int nx, int ny, double dx, double dy, double* topol
     return 0;
 }
 
+/* solvegc2, SPH_GCsolver_2019.f90:16-316, literally: element-by-element K.p,
+ * Jacobi preconditioner from the assembled diagonal, prescribed dofs masked,
+ * stop when r.r / r0.r0 <= tol. intmat (nnode, nelem) column-major, 1-based. */
+template <class R>
+int solvegc2_mode(int npoin, int nelem, int nnode, int ndofn, const int* intmat, int* iffix, const double* fixed,
+                  const double* gstif, double* rcg_io, double* ficg_out, double tol_in, int* iters_out) {
+    const int ntotv = npoin * ndofn, nevab = nnode * ndofn;
+    const R tol = (R)tol_in;
+    std::vector<R> r1(ntotv, 0), s(ntotv, 0), p(ntotv, 0), q(ntotv, 0), ap(ntotv, 0), fi(ntotv, 0), rcg(ntotv),
+        fx(ntotv), gs((size_t)nevab * nevab * nelem);
+    for (int i = 0; i < ntotv; i++) { rcg[i] = (R)rcg_io[i]; fx[i] = (R)fixed[i]; }
+    for (size_t k = 0; k < gs.size(); k++) gs[k] = (R)gstif[k];
+    auto G = [&](int a, int b, int e) { return gs[(size_t)e * nevab * nevab + (size_t)b * nevab + a]; };
+    auto pos = [&](int node, int idofn) { return (node - 1) * ndofn + idofn; };
+    /* getqmat */
+    for (int e = 0; e < nelem; e++)
+        for (int in = 0; in < nnode; in++)
+            for (int id = 0; id < ndofn; id++) {
+                int ie = in * ndofn + id;
+                q[pos(intmat[(size_t)e * nnode + in], id)] += G(ie, ie, e);
+            }
+    for (int i = 0; i < ntotv; i++) {
+        if (std::fabs(q[i]) <= lit<R>(1.e-35)) {
+            if (iffix[i] == 0) iffix[i] = -999;
+        } else {
+            q[i] = (R)1 / q[i];
+        }
+    }
+    auto kbyp = [&](int iflag) {
+        std::fill(ap.begin(), ap.end(), (R)0);
+        for (int e = 0; e < nelem; e++)
+            for (int in = 0; in < nnode; in++)
+                for (int id = 0; id < ndofn; id++) {
+                    int ie = in * ndofn + id;
+                    int np_ = pos(intmat[(size_t)e * nnode + in], id);
+                    for (int jn = 0; jn < nnode; jn++)
+                        for (int jd = 0; jd < ndofn; jd++) {
+                            int je = jn * ndofn + jd;
+                            int mp = pos(intmat[(size_t)e * nnode + jn], jd);
+                            R sum = G(ie, je, e) * p[mp];
+                            if (iflag == 1 && iffix[np_] + iffix[mp] != 0) sum = 0;
+                            ap[np_] = ap[np_] + sum;
+                        }
+                }
+    };
+    /* initcg */
+    for (int i = 0; i < ntotv; i++) { fi[i] = fx[i]; p[i] = fi[i]; }
+    kbyp(0);
+    R rnorm0 = 0;
+    for (int i = 0; i < ntotv; i++) {
+        rcg[i] = rcg[i] - ap[i];
+        s[i] = q[i] * rcg[i];
+        p[i] = s[i];
+        rnorm0 = rnorm0 + rcg[i] * rcg[i];
+    }
+    for (int i = 0; i < ntotv; i++)
+        if (iffix[i] != 0) { p[i] = 0; rcg[i] = 0; s[i] = 0; }
+    R rnx = 0;
+    for (int i = 0; i < ntotv; i++) rnx = rnx + fx[i] * fx[i];
+    rnx = std::sqrt(rnx + rnorm0);
+    int it = 0;
+    if (rnx < tol) {
+        std::fill(fi.begin(), fi.end(), (R)0);
+    } else {
+        const long miter = 10L * ntotv;
+        for (long iter = 1; iter <= miter; iter++) {
+            /* jcg */
+            kbyp(1);
+            R prod1 = 0, prod2 = 0;
+            for (int i = 0; i < ntotv; i++)
+                if (iffix[i] == 0) { prod1 = prod1 + rcg[i] * s[i]; prod2 = prod2 + p[i] * ap[i]; }
+            R alfa = prod1 / prod2;
+            R prod3 = 0, rnorm1 = 0;
+            for (int i = 0; i < ntotv; i++) {
+                fi[i] = fi[i] + alfa * p[i];
+                r1[i] = rcg[i] - alfa * ap[i];
+                rnorm1 = rnorm1 + r1[i] * r1[i];
+                s[i] = q[i] * r1[i];
+                prod3 = prod3 + r1[i] * s[i];
+            }
+            it++;
+            if (rnorm1 / rnorm0 > tol) {
+                R beta = prod3 / prod1;
+                for (int i = 0; i < ntotv; i++) { p[i] = s[i] + beta * p[i]; rcg[i] = r1[i]; }
+            } else {
+                break;
+            }
+        }
+        for (int i = 0; i < ntotv; i++)
+            if (iffix[i] == -999) iffix[i] = 0;
+    }
+    for (int i = 0; i < ntotv; i++) { ficg_out[i] = (double)fi[i]; rcg_io[i] = (double)rcg[i]; }
+    if (iters_out) *iters_out = it;
+    return 0;
+}
+
 } // namespace
 
 extern "C" {
+
+int oracle_solvegc2(int mode, int npoin, int nelem, int nnode, int ndofn, const int* intmat, int* iffix,
+                    const double* fixed, const double* gstif, double* rcg, double* ficg, double tol, int* iters) {
+    if (npoin < 1 || nelem < 1 || !intmat || !iffix || !fixed || !gstif || !rcg || !ficg) return GFSPH_ERR_ARG;
+    return mode == 2 ? solvegc2_mode<double>(npoin, nelem, nnode, ndofn, intmat, iffix, fixed, gstif, rcg, ficg, tol, iters)
+                     : solvegc2_mode<float>(npoin, nelem, nnode, ndofn, intmat, iffix, fixed, gstif, rcg, ficg, tol, iters);
+}
 
 /* Runs nsteps steps of the reference path on the given state (in/out).
  * topol: (16, nx*ny) in/out (erosion lowers Z).  mode: 0, 1, 2 as above. */

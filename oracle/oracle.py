@@ -66,6 +66,9 @@ def lib():
         L.oracle_get.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP, _DP, _IP, _DP, _DP, _DP]
         L.oracle_free.restype = None
         L.oracle_free.argtypes = [C.c_void_p]
+        L.oracle_solvegc2.restype = C.c_int
+        L.oracle_solvegc2.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP, _DP, _DP, _DP,
+                                      C.c_double, _IP]
         _lib = L
     return _lib
 
@@ -226,3 +229,23 @@ class Run:
             self.close()
         except Exception:
             pass
+
+
+def solvegc2(mode, intmat, gstif, rhs, iffix=None, fixed=None, tol=1e-10, ndofn=1):
+    """solvegc2 on the element matrices gstif (nelem, nevab, nevab) with
+    intmat (nelem, nnode) 1-based; returns (x, final residual, iffix, iters)."""
+    intmat = np.ascontiguousarray(intmat, np.int32)
+    nelem, nnode = intmat.shape
+    npoin = int(intmat.max())
+    n = npoin * ndofn
+    g = np.ascontiguousarray(np.transpose(gstif, (0, 2, 1)), np.float64)  # element-major, column-major within
+    fix = np.zeros(n, np.int32) if iffix is None else np.ascontiguousarray(iffix, np.int32).copy()
+    fx = np.zeros(n) if fixed is None else _d(fixed).copy()
+    r = _d(rhs).copy()
+    x = np.zeros(n)
+    it = C.c_int(0)
+    st = lib().oracle_solvegc2(mode, npoin, nelem, nnode, ndofn, _ip(intmat), _ip(fix), _dp(fx), _dp(g), _dp(r),
+                               _dp(x), tol, C.byref(it))
+    if st:
+        raise RuntimeError(f"oracle_solvegc2: {st}")
+    return x, r, fix, it.value

@@ -1,0 +1,41 @@
+"""gfsph_run, the C++ host that reads the reference's input files, on the
+GPU: it runs the step loop with the reference's plot cadence and writes
+depth rasters."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import workloads
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+RUN = os.path.join(ROOT, "deslizamientos-y-flujos_b200", "gfsph_run")
+
+
+def read_asc(path):
+    with open(path) as f:
+        head = [next(f) for _ in range(6)]
+        data = np.loadtxt(f)
+    return head, data[::-1]
+
+
+def test_gfsph_run_on_written_inputs(gfsph_lib, tmp_path):
+    w = workloads.inclined_plane()
+    d = str(tmp_path)
+    workloads.write_reference_inputs(w, d, "plane")
+    meta = json.loads(subprocess.run([RUN, "plane", "--dir", d, "--parse-only"], capture_output=True,
+                                     text=True).stdout)
+    out = subprocess.run([RUN, "plane", "--dir", d, "--out", d, "--max-steps", "300"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    log = np.loadtxt(os.path.join(d, "plane.gfsph.log"))
+    assert log.shape[0] == 3                         # plot every 100 steps (plot_step * dt)
+    assert np.allclose(log[:, 3], meta["volume"], rtol=1e-6)   # no erosion: volume conserved
+    assert log[-1, 2] == 300 and log[-1, 6] == meta["n"]
+    head, depth = read_asc(os.path.join(d, "plane.depth_0002.asc"))
+    assert depth.shape == (400, 200) and np.isfinite(depth).all() and depth.max() > 1.0
+    _, hmax = read_asc(os.path.join(d, "plane.max_depth.asc"))
+    assert hmax.max() >= log[:, 4].max() - 1e-4

@@ -1,0 +1,56 @@
+"""The C++ host driver's readers of the reference input files (no GPU):
+MASTER.dat, the SW .dat, the .top DEM and the .pts source."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import workloads
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+RUN = os.path.join(ROOT, "deslizamientos-y-flujos_b200", "gfsph_run")
+PICACHO = "/root/reference/EJEMPLOS/Picacho Landslide/Input files"
+
+
+def parse(name, directory):
+    out = subprocess.run([RUN, name, "--dir", directory, "--parse-only"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    return json.loads(out.stdout)
+
+
+def test_written_inputs_read_back(gfsph_lib, tmp_path):
+    w = workloads.inclined_plane()
+    workloads.write_reference_inputs(w, str(tmp_path), "plane")
+    r = parse("plane", str(tmp_path))
+    assert (r["nx"], r["ny"]) == (200, 400) and r["dx"] == 5.0 and r["fdiff"] == 1 and r["ictop"] == 0
+    assert r["dt_sph"] == pytest.approx(0.01) and r["ic_adapt"] == 0
+    assert (r["pa_sph"], r["nnps"], r["sle"], r["skf"], r["nfric"], r["icpwp"]) == (2, 2, 1, 1, 5, 0)
+    assert r["const"][0] == pytest.approx(9.8) and r["const"][2] == 500 and r["const"][8] == pytest.approx(0.2)
+    assert r["hsml"] == pytest.approx(4.0)
+    # the lattice resample of Read_Source_plus_New reproduces the source nodes
+    # and adds a halo of IDW-averaged nodes around them, at most 2 nodes deep
+    assert r["n"] >= w.n and r["n"] < w.n * 1.5
+    assert r["z_mean"] == pytest.approx(float(w.z.astype(np.float64).mean()), rel=1e-5)
+
+
+@pytest.mark.skipif(not os.path.isdir(PICACHO), reason="reference example not available")
+def test_picacho_example_reads(gfsph_lib):
+    r = parse("Picacho", PICACHO)
+    assert (r["nx"], r["ny"], r["dx"]) == (442, 291, 10.0)
+    assert r["ictop"] == 10 and r["fdiff"] == 0
+    assert (r["nnps"], r["skf"], r["nfric"], r["icpwp"]) == (4, 1, 7, 3)
+    assert r["dt_sph"] == pytest.approx(0.1) and r["ic_adapt"] == 1 and r["plot_step"] == 50
+    assert 800 < r["n"] < 900 and r["hsml"] == 20.0
+    assert r["const"][2] == 300 and r["const"][8] == pytest.approx(0.6)
+
+
+def test_reader_reports_unsupported_options(gfsph_lib, tmp_path):
+    w = workloads.inclined_plane()
+    workloads.write_reference_inputs(w, str(tmp_path), "bad")
+    top = os.path.join(str(tmp_path), "bad.top")
+    txt = open(top).read().replace("ictop\n100\n", "ictop\n3\n", 1)
+    open(top, "w").write(txt)
+    out = subprocess.run([RUN, "bad", "--dir", str(tmp_path), "--parse-only"], capture_output=True, text=True)
+    assert out.returncode == 2 and "ictop 3" in out.stderr

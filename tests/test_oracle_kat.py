@@ -209,3 +209,32 @@ def test_workload_generators():
     w1 = workloads.inclined_plane()
     assert 1800 < w1.n < 2100
     assert abs(w1.rho.max() - 10.0) < 0.2
+
+
+def test_solvegc2_restatement_solves_the_p1_mass_system(oracle_mod):
+    """solvegc2 (FP64 build) on the consistent P1 mass matrix of the DEM
+    background triangulation equals a dense solve; prescribed dofs keep their
+    values; the FP32 build converges to its own precision."""
+    intmat, coords = workloads.p1_mesh(13, 11, 5.0)
+    g = workloads.p1_mass_matrices(intmat, coords)
+    n = coords.shape[0]
+    K = np.zeros((n, n))
+    for e in range(intmat.shape[0]):
+        idx = intmat[e] - 1
+        K[np.ix_(idx, idx)] += g[e]
+    rng = np.random.default_rng(4)
+    b = rng.normal(size=n)
+    x, r, fix, it = oracle_mod.solvegc2(2, intmat, g, b, tol=1e-24)
+    assert np.allclose(x, np.linalg.solve(K, b), rtol=1e-9, atol=1e-9)
+    assert 3 < it < 60
+    # Dirichlet dofs on the boundary
+    iffix = np.zeros(n, np.int32)
+    bnd = (coords[:, 0] == 0) | (coords[:, 1] == 0)
+    iffix[bnd] = 1
+    fixed = np.where(bnd, 2.5, 0.0)
+    x2, _, _, _ = oracle_mod.solvegc2(2, intmat, g, b, iffix=iffix, fixed=fixed, tol=1e-24)
+    free = ~bnd
+    ref = np.linalg.solve(K[np.ix_(free, free)], b[free] - K[np.ix_(free, bnd)] @ fixed[bnd])
+    assert np.allclose(x2[free], ref, rtol=1e-9, atol=1e-9) and np.all(x2[bnd] == 2.5)
+    x3, _, _, it3 = oracle_mod.solvegc2(0, intmat, g, b, tol=1e-10)
+    assert np.allclose(x3, x, rtol=1e-4, atol=1e-4)
