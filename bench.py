@@ -194,6 +194,61 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+def ensemble_bench(args, torch, gfsph, workloads):
+    """Monte-Carlo ensemble: R realizations (mu, xi, release volume drawn as
+    in workloads.mc_ensemble, ragged particle counts) advanced S steps by
+    gfsph_ensemble_step, against looping gfsph_step over the same members.
+    Times are device-synchronised host clocks around each phase (the members
+    run on their own streams).  Realizations/s extrapolates realization-steps/s
+    to the 5,000-step realization length."""
+    R, S = args.ensemble, args.ensemble_steps
+    ws = workloads.mc_ensemble(R, n_base=args.n)
+    params = [workloads.make_params(w, gfsph) for w in ws]
+    w0 = ws[0]
+    ens = gfsph.Ensemble(params, w0.z, dx=w0.dx, dy=w0.dy)
+
+    def upload():
+        for m, w in zip(ens.members, ws):
+            m.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+
+    upload()
+    ens.step(3)  # graph capture and capacity growth
+    upload()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m in ens.members:
+        m.step(S)
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter() - t0
+    looped = [m.download() for m in ens.members]
+    upload()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, done = ens.step(S)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    err = 0.0
+    for m, a in zip(ens.members, looped):
+        b = m.download()
+        d = np.linalg.norm((b["rho"] - a["rho"]).astype(np.float64)) / max(np.linalg.norm(a["rho"]), 1e-30)
+        err = max(err, float(d))
+    ens.close()
+    npart = [w.n for w in ws]
+    ps = sum(npart) * S
+    return {
+        "metric": "MC realizations/s", "realizations": R, "steps_per_realization_timed": S,
+        "particles_min": min(npart), "particles_max": max(npart), "particles_total": sum(npart),
+        "batched": {"realizations_per_s": R * S / t_batch / 5000.0, "seconds": t_batch,
+                    "particle_steps_per_s": ps / t_batch},
+        "looped": {"realizations_per_s": R * S / t_loop / 5000.0, "seconds": t_loop,
+                   "particle_steps_per_s": ps / t_loop},
+        "speedup_vs_looped": t_loop / t_batch,
+        "max_rel_l2_depth_vs_looped": err,
+        "note": "realizations/s = realization-steps/s / 5000 (extrapolated from the timed steps); "
+                "device-synchronised host clock; member states bit-compared with the looped run",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,6 +258,8 @@ def main():
     ap.add_argument("--n", type=int, default=200_000, help="particles per replica")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ensemble", type=int, default=16, help="realizations of the ensemble line (0: none)")
+    ap.add_argument("--ensemble-steps", type=int, default=40)
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
@@ -308,6 +365,11 @@ def main():
     e2e_ms = e0.elapsed_time(e1)
     _, _, e2e_value = combine_ranks(e2e_ms, n, e2e_steps, dist, "cuda")
 
+    sim.close()
+    ens_line = None
+    if world == 1 and args.ensemble > 0:
+        ens_line = ensemble_bench(args, torch, gfsph, workloads)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, steps, nc, el, desc = cpu_reference_rate(args.cpu_seconds)
@@ -336,8 +398,12 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if ens_line:
+            if cpu:
+                mean_n = ens_line["particles_total"] / ens_line["realizations"]
+                ens_line["cpu_sequential_realizations_per_s"] = cpu["value"] / mean_n / 5000.0
+            line["ensemble"] = ens_line
         print(json.dumps(line), flush=True)
-    sim.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

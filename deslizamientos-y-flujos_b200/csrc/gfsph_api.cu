@@ -642,58 +642,78 @@ int gfsph_set_time(gfsph_handle* h, double t, float dt) {
     return GFSPH_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Enqueues one chunk of steps (no host synchronisation).
+int enqueue_chunk(gfsph_handle* h, int chunk, double t_end) {
+    set_field<double>(h, offsetof(StepScalars, t_end), t_end);
+    set_field<int>(h, offsetof(StepScalars, steps_done), 0);
+    launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, h->stream>>>(h->S, 1); });
+    if (h->profile) {
+        for (int s = 0; s < chunk; s++) {
+            enqueue_step(h);
+            int st = profile_collect(h);
+            if (st) return st;
+        }
+        return 0;
+    }
+    if (!h->g1) { int st = build_graph(h, 1, &h->g1); if (st) return st; }
+    if (!h->gK) { int st = build_graph(h, kGraphSteps, &h->gK); if (st) return st; }
+    int per = kernels_per_step(h);
+    int s = 0;
+    if (h->profile_level == 2) CK(cudaEventRecord(h->ev0[K_STEPS], h->stream));
+    for (; s + kGraphSteps <= chunk; s += kGraphSteps) {
+        CK(cudaGraphLaunch(h->gK, h->stream));
+        h->launches += (long long)per * kGraphSteps;
+    }
+    for (; s < chunk; s++) {
+        CK(cudaGraphLaunch(h->g1, h->stream));
+        h->launches += per;
+    }
+    if (h->profile_level == 2) CK(cudaEventRecord(h->ev1[K_STEPS], h->stream));
+    return 0;
+}
+
+// Waits for a chunk and handles its outcome: returns 1 to go on, 0 when
+// t_end is reached, < 0 on error; `done` accumulates the completed steps.
+int finish_chunk(gfsph_handle* h, int chunk, double t_end, int& done, int& guard) {
+    if (h->profile_level == 2 && !h->profile) {
+        CK(cudaEventSynchronize(h->ev1[K_STEPS]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev0[K_STEPS], h->ev1[K_STEPS]);
+        h->prof_ms[K_STEPS] += ms;
+        h->prof_cnt[K_STEPS] += chunk;
+    }
+    CK(cudaGetLastError());
+    int st = read_scalars(h);
+    if (st) return st;
+    done += h->hS->steps_done;
+    h->searched = true;
+    if (h->hS->err) {
+        if (++guard > 16) return GFSPH_ERR_CAPACITY;
+        st = grow_after_error(h);
+        return st ? st : 1;
+    }
+    return (h->hS->time >= t_end) ? 0 : 1;
+}
+
+}  // namespace
+
+extern "C" {
+
 int gfsph_step(gfsph_handle* h, int nsteps, double t_end, double* t_out, int* steps_done) {
     if (!h || nsteps < 0) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
-    int done = 0;
-    int status = GFSPH_OK;
-    int guard = 0;
+    int done = 0, guard = 0, status = GFSPH_OK;
     while (done < nsteps) {
         int chunk = std::min(kChunkSteps, nsteps - done);
-        set_field<double>(h, offsetof(StepScalars, t_end), t_end);
-        set_field<int>(h, offsetof(StepScalars, steps_done), 0);
-        launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, h->stream>>>(h->S, 1); });
-        if (h->profile) {
-            for (int s = 0; s < chunk; s++) {
-                enqueue_step(h);
-                int st = profile_collect(h);
-                if (st) return st;
-            }
-        } else {
-            if (!h->g1) { int st = build_graph(h, 1, &h->g1); if (st) return st; }
-            if (!h->gK) { int st = build_graph(h, kGraphSteps, &h->gK); if (st) return st; }
-            int per = kernels_per_step(h);
-            int s = 0;
-            if (h->profile_level == 2) CK(cudaEventRecord(h->ev0[K_STEPS], h->stream));
-            for (; s + kGraphSteps <= chunk; s += kGraphSteps) {
-                CK(cudaGraphLaunch(h->gK, h->stream));
-                h->launches += (long long)per * kGraphSteps;
-            }
-            for (; s < chunk; s++) {
-                CK(cudaGraphLaunch(h->g1, h->stream));
-                h->launches += per;
-            }
-            if (h->profile_level == 2) {
-                CK(cudaEventRecord(h->ev1[K_STEPS], h->stream));
-                CK(cudaEventSynchronize(h->ev1[K_STEPS]));
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, h->ev0[K_STEPS], h->ev1[K_STEPS]);
-                h->prof_ms[K_STEPS] += ms;
-                h->prof_cnt[K_STEPS] += chunk;
-            }
-        }
-        CK(cudaGetLastError());
-        int st = read_scalars(h);
+        int st = enqueue_chunk(h, chunk, t_end);
         if (st) return st;
-        done += h->hS->steps_done;
-        h->searched = true;
-        if (h->hS->err) {
-            if (++guard > 16) return GFSPH_ERR_CAPACITY;
-            st = grow_after_error(h);
-            if (st) { status = st; break; }
-            continue;
-        }
-        if (h->hS->time >= t_end) {
+        st = finish_chunk(h, chunk, t_end, done, guard);
+        if (st < 0) { status = st; break; }
+        if (st == 0) {
             if (done < nsteps) status = GFSPH_T_END_REACHED;
             break;
         }
@@ -901,6 +921,148 @@ int gfsph_profile_read(gfsph_handle* h, int kernel, double* total_ms, long long*
 }
 
 long long gfsph_launch_count(gfsph_handle* h) { return h ? h->launches : -1; }
+
+// ---------------------------------------------------------------- ensembles
+
+}  // extern "C"
+
+struct gfsph_ensemble {
+    std::vector<gfsph_handle*> members;
+    int nx = 0, ny = 0;
+    unsigned int** d_maxptr = nullptr;  // device array of the members' per-node max-depth buffers
+    float* d_prob = nullptr;
+};
+
+namespace {
+
+__global__ void k_exceedance(unsigned int* const* maxh, int nreal, int np, float threshold, float* prob) {
+    unsigned int thr = f2o(threshold);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+        int c = 0;
+        for (int r = 0; r < nreal; r++) c += (maxh[r][k] > thr) ? 1 : 0;  // max depth > threshold
+        prob[k] = (float)c / (float)nreal;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfsph_ensemble_create(const gfsph_params* params, const gfsph_dem* dem, int nreal, gfsph_ensemble** out) {
+    if (!params || !dem || !out || nreal < 1) return GFSPH_ERR_ARG;
+    *out = nullptr;
+    for (int r = 0; r < nreal; r++) {
+        int st = validate(&params[r]);
+        if (st) return st;
+        if (params[r].dem_deriv != params[0].dem_deriv) return GFSPH_ERR_ARG;  // one set of DEM rows
+    }
+    // the DEM rows once on the host, shared by every member's copy
+    std::vector<float> topol;
+    gfsph_dem d = *dem;
+    if (!dem->topol) {
+        if (!dem->z || dem->nx < 3 || dem->ny < 3) return GFSPH_ERR_ARG;
+        size_t np = (size_t)dem->nx * dem->ny;
+        topol.assign(np * GFSPH_NTOPO, 0.f);
+        for (size_t ip = 0; ip < np; ip++) topol[ip * GFSPH_NTOPO] = dem->z[ip];
+        int st = gfsph_dem_topol(params[0].dem_deriv, dem->nx, dem->ny, dem->dx, dem->dy, topol.data());
+        if (st) return st;
+    }
+    gfsph_ensemble* e = new (std::nothrow) gfsph_ensemble();
+    if (!e) return GFSPH_ERR_ARG;
+    e->nx = dem->nx; e->ny = dem->ny;
+    for (int r = 0; r < nreal; r++) {
+        gfsph_dem dm = d;
+        if (!dem->topol) {  // erodible depth per member (Input_SW SPH_SW_2019.f90:1288-1307)
+            const float* k = params[r].cst;
+            float avail = 0.f;
+            if (k[20] > 1.e-9f) avail = (k[47] > 1.e-6f) ? k[47] : 999.f;
+            size_t np = (size_t)dem->nx * dem->ny;
+            for (size_t ip = 0; ip < np; ip++) topol[ip * GFSPH_NTOPO + 14] = avail;
+            dm.topol = topol.data();
+            dm.ntopo = GFSPH_NTOPO;
+        }
+        gfsph_handle* h = nullptr;
+        int st = gfsph_create(&params[r], &dm, &h);
+        if (st) { gfsph_ensemble_destroy(e); return st; }
+        e->members.push_back(h);
+    }
+    *out = e;
+    return GFSPH_OK;
+}
+
+int gfsph_ensemble_destroy(gfsph_ensemble* e) {
+    if (!e) return GFSPH_ERR_ARG;
+    for (gfsph_handle* h : e->members) gfsph_destroy(h);
+    dfree(e->d_maxptr);
+    dfree(e->d_prob);
+    delete e;
+    return GFSPH_OK;
+}
+
+int gfsph_ensemble_member(gfsph_ensemble* e, int r, gfsph_handle** out) {
+    if (!e || !out || r < 0 || r >= (int)e->members.size()) return GFSPH_ERR_ARG;
+    *out = e->members[r];
+    return GFSPH_OK;
+}
+
+int gfsph_ensemble_step(gfsph_ensemble* e, int nsteps, double t_end, int* min_steps_done) {
+    if (!e || nsteps < 0) return GFSPH_ERR_ARG;
+    const int R = (int)e->members.size();
+    for (gfsph_handle* h : e->members)
+        if (!h->has_state) return GFSPH_ERR_STATE;
+    std::vector<int> done(R, 0), guard(R, 0), active(R, 1);
+    int status = GFSPH_OK;
+    for (;;) {
+        bool any = false;
+        std::vector<int> chunk(R, 0);
+        for (int r = 0; r < R; r++) {  // every member's chunk goes out before any wait
+            if (!active[r] || done[r] >= nsteps) { active[r] = 0; continue; }
+            chunk[r] = std::min(kChunkSteps, nsteps - done[r]);
+            int st = enqueue_chunk(e->members[r], chunk[r], t_end);
+            if (st) return st;
+            any = true;
+        }
+        if (!any) break;
+        for (int r = 0; r < R; r++) {
+            if (!chunk[r]) continue;
+            int st = finish_chunk(e->members[r], chunk[r], t_end, done[r], guard[r]);
+            if (st < 0) return st;
+            if (st == 0) { active[r] = 0; status = GFSPH_T_END_REACHED; }
+        }
+    }
+    if (min_steps_done) *min_steps_done = *std::min_element(done.begin(), done.end());
+    return status;
+}
+
+int gfsph_ensemble_sample(gfsph_ensemble* e) {
+    if (!e) return GFSPH_ERR_ARG;
+    for (gfsph_handle* h : e->members) {
+        int st = gfsph_hazard_sample(h);
+        if (st) return st;
+    }
+    return GFSPH_OK;
+}
+
+int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob) {
+    if (!e || !prob) return GFSPH_ERR_ARG;
+    const int R = (int)e->members.size();
+    const int np = e->nx * e->ny;
+    std::vector<unsigned int*> ptrs(R);
+    for (int r = 0; r < R; r++) {
+        gfsph_handle* h = e->members[r];
+        if (!h->haz_cnt) { int st = gfsph_hazard_reset(h); if (st) return st; }
+        CK(cudaStreamSynchronize(h->stream));
+        ptrs[r] = h->haz_max_h;
+    }
+    if (!e->d_maxptr && dalloc(&e->d_maxptr, R)) return GFSPH_ERR_CUDA;
+    if (!e->d_prob && dalloc(&e->d_prob, np)) return GFSPH_ERR_CUDA;
+    cudaStream_t s = e->members[0]->stream;
+    CK(cudaMemcpyAsync(e->d_maxptr, ptrs.data(), R * sizeof(unsigned int*), cudaMemcpyHostToDevice, s));
+    k_exceedance<<<blocks_for(np, 256), 256, 0, s>>>(e->d_maxptr, R, np, threshold, e->d_prob);
+    CK(cudaMemcpyAsync(prob, e->d_prob, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return GFSPH_OK;
+}
 
 int gfsph_stats(gfsph_handle* h, int* out, int nout) {
     if (!h || !out || nout < 1) return GFSPH_ERR_ARG;

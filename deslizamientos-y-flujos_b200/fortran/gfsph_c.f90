@@ -145,6 +145,40 @@ module gfsph_c
        real(c_float), value :: dx, dy
        real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
      end function
+     integer(c_int) function gfsph_ensemble_create(params, dem, nreal, ens) bind(c, name="gfsph_ensemble_create")
+       import :: c_int, c_ptr, gfsph_params, gfsph_dem
+       type(gfsph_params), intent(in) :: params(*)
+       type(gfsph_dem), intent(in) :: dem
+       integer(c_int), value :: nreal
+       type(c_ptr), intent(out) :: ens
+     end function
+     integer(c_int) function gfsph_ensemble_destroy(ens) bind(c, name="gfsph_ensemble_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ens
+     end function
+     integer(c_int) function gfsph_ensemble_member(ens, r, member) bind(c, name="gfsph_ensemble_member")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ens
+       integer(c_int), value :: r
+       type(c_ptr), intent(out) :: member
+     end function
+     integer(c_int) function gfsph_ensemble_step(ens, nsteps, t_end, min_steps_done) bind(c, name="gfsph_ensemble_step")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ens
+       integer(c_int), value :: nsteps
+       real(c_double), value :: t_end
+       integer(c_int), intent(out) :: min_steps_done
+     end function
+     integer(c_int) function gfsph_ensemble_sample(ens) bind(c, name="gfsph_ensemble_sample")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ens
+     end function
+     integer(c_int) function gfsph_ensemble_exceedance(ens, threshold, prob) bind(c, name="gfsph_ensemble_exceedance")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: ens
+       real(c_float), value :: threshold
+       real(c_float), intent(out) :: prob(*)
+     end function
      integer(c_int) function gfsph_cg_create(npoin, nelem, nnode, ndofn, intmat, gstif, cg) bind(c, name="gfsph_cg_create")
        import :: c_int, c_ptr, c_float
        integer(c_int), value :: npoin, nelem, nnode, ndofn

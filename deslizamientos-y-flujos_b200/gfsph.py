@@ -22,6 +22,12 @@ NTOPO = 16
 
 OK = 0
 T_END_REACHED = 1
+ERR_ARG = -1
+ERR_CUDA = -2
+ERR_CAPACITY = -3
+ERR_UNSUPPORTED = -4
+ERR_STATE = -5
+ERR_NO_DEVICE = -6
 
 RASTER_DEPTH_IDW = 0
 RASTER_MAX_DEPTH = 1
@@ -81,6 +87,12 @@ SIGNATURES = {
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
     "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "gfsph_ensemble_create": (C.c_int, [C.POINTER(Params), C.POINTER(Dem), C.c_int, C.POINTER(C.c_void_p)]),
+    "gfsph_ensemble_destroy": (C.c_int, [C.c_void_p]),
+    "gfsph_ensemble_member": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "gfsph_ensemble_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _IP]),
+    "gfsph_ensemble_sample": (C.c_int, [C.c_void_p]),
+    "gfsph_ensemble_exceedance": (C.c_int, [C.c_void_p, C.c_float, _FP]),
     "gfsph_cg_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _IP, _FP, C.POINTER(C.c_void_p)]),
     "gfsph_cg_solve": (C.c_int, [C.c_void_p, _IP, _FP, _FP, _FP, C.c_float, _IP]),
     "gfsph_cg_destroy": (C.c_int, [C.c_void_p]),
@@ -318,6 +330,71 @@ class CG:
     def close(self):
         if self.h:
             lib().gfsph_cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Member(Sim):
+    """A member handle of an ensemble (owned by the ensemble)."""
+
+    def __init__(self, handle, nx, ny, params):
+        self.h = handle
+        self.nx, self.ny = nx, ny
+        self.params = params
+        self.n = 0
+
+    def close(self):
+        self.h = None
+
+
+class Ensemble:
+    """gfsph_ensemble: realizations with their own parameters on one DEM."""
+
+    def __init__(self, params_list, z, *, xmin=0.0, ymin=0.0, dx=1.0, dy=1.0):
+        L = lib()
+        self._z = np.ascontiguousarray(z, dtype=np.float32)
+        ny, nx = self._z.shape
+        arr = (Params * len(params_list))(*params_list)
+        self._params = arr
+        d = Dem()
+        d.nx, d.ny, d.xmin, d.ymin, d.dx, d.dy = nx, ny, xmin, ymin, dx, dy
+        d.topol = None
+        d.ntopo = 0
+        d.z = _fp(self._z)
+        self.dem = d
+        h = C.c_void_p()
+        _check(L.gfsph_ensemble_create(arr, C.byref(d), len(params_list), C.byref(h)), "gfsph_ensemble_create")
+        self.h = h
+        self.nx, self.ny = nx, ny
+        self.members = []
+        for r in range(len(params_list)):
+            m = C.c_void_p()
+            _check(L.gfsph_ensemble_member(h, r, C.byref(m)), "gfsph_ensemble_member")
+            self.members.append(_Member(m, nx, ny, params_list[r]))
+
+    def step(self, nsteps, t_end=1e300):
+        done = C.c_int()
+        st = _check(lib().gfsph_ensemble_step(self.h, nsteps, t_end, C.byref(done)), "gfsph_ensemble_step")
+        return st, done.value
+
+    def sample(self):
+        _check(lib().gfsph_ensemble_sample(self.h), "gfsph_ensemble_sample")
+
+    def exceedance(self, threshold):
+        out = np.empty((self.ny, self.nx), np.float32)
+        _check(lib().gfsph_ensemble_exceedance(self.h, threshold, _fp(out)), "gfsph_ensemble_exceedance")
+        return out
+
+    def close(self):
+        if self.h:
+            for m in self.members:
+                m.close()
+            lib().gfsph_ensemble_destroy(self.h)
             self.h = None
 
     def __del__(self):

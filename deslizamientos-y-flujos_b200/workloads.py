@@ -132,27 +132,29 @@ def inclined_plane(seed=1, spacing=2.0, facthsml=2.0, nx=200, ny=400, cell=5.0):
 
 def fractal_channel(n_target=200_000, dem_k=10, cell=5.0, seed=2, facthsml=2.0, mean_depth=4.0,
                     semi_along=150.0, semi_across=80.0, erosion=(0.005, 2.0), mu=0.15, xi=400.0,
-                    relief=800.0):
+                    relief=800.0, z=None):
     """Seeded diamond-square fBm DEM (Hurst 0.8) of 2^dem_k nodes a side at
     `cell` m with a carved V-channel, relief `relief` m; an elliptical release
     (semi-axes 150 m along the channel, 80 m across) on the lattice spacing
     that gives ~n_target particles; smooth seeded depth field of mean 4 m;
     Voellmy mu = 0.15, xi = 400 with Hungr erosion 0.005 1/m over a 2 m
-    erodible layer; adaptive dt (ic_adapt_dt_sph = 1)."""
-    rng = np.random.default_rng(seed)
-    f = diamond_square(dem_k, 0.8, rng)[: 2 ** dem_k, : 2 ** dem_k]
-    f = (f - f.min()) / (f.max() - f.min())
+    erodible layer; adaptive dt (ic_adapt_dt_sph = 1).  `z` reuses a DEM
+    made by an earlier call with the same dem_k, cell, seed and relief."""
     nx = ny = 2 ** dem_k
     L = nx * cell
-    ys = np.arange(ny)[:, None] * cell
-    xs = np.arange(nx)[None, :] * cell
     xc = L / 2.0
-    decay = 0.3125 * L
-    base = (relief - 100.0) * np.exp(-ys / decay)
-    rough = 100.0 * f * np.exp(-ys / (2 * decay))
-    half_w = 0.04 * L
-    carve = 40.0 * np.clip(1.0 - np.abs(xs - xc) / half_w, 0.0, None)
-    z = (base + rough - carve).astype(np.float32)
+    if z is None:
+        rng = np.random.default_rng(seed)
+        f = diamond_square(dem_k, 0.8, rng)[: 2 ** dem_k, : 2 ** dem_k]
+        f = (f - f.min()) / (f.max() - f.min())
+        ys = np.arange(ny)[:, None] * cell
+        xs = np.arange(nx)[None, :] * cell
+        decay = 0.3125 * L
+        base = (relief - 100.0) * np.exp(-ys / decay)
+        rough = 100.0 * f * np.exp(-ys / (2 * decay))
+        half_w = 0.04 * L
+        carve = 40.0 * np.clip(1.0 - np.abs(xs - xc) / half_w, 0.0, None)
+        z = (base + rough - carve).astype(np.float32)
     yc = 0.137 * L
     area = math.pi * semi_along * semi_across
     spacing = math.sqrt(area / n_target)
@@ -172,6 +174,28 @@ def fractal_channel(n_target=200_000, dem_k=10, cell=5.0, seed=2, facthsml=2.0, 
                      dem_deriv=1),
         z=z, dx=cell, dy=cell, x=x, v=v, rho=h, mass=mass, hsml=hsml, steps=10_000,
         meta=dict(dem=f"{nx}x{ny} at {cell} m", lattice=spacing, relief=relief))
+
+
+def mc_ensemble(nreal, n_base=200_000, dem_k=10, cell=5.0, seed=2024, mu=(0.08, 0.30), xi=(400.0, 0.3),
+                scale=(0.2, 2.0)):
+    """Realizations of the Monte-Carlo hazard ensemble on the fractal channel
+    DEM: mu ~ U(mu), xi ~ LogNormal(ln xi[0], xi[1]), release volume scaled by
+    s ~ U(scale) — the release keeps its ellipse, its depth field is scaled by
+    s and its lattice is refined so that the particle count is ~n_base * s
+    (ragged counts).  Returns a list of Workloads sharing one DEM array."""
+    rng = np.random.default_rng(seed)
+    z = None
+    out = []
+    for _ in range(nreal):
+        m = float(rng.uniform(*mu))
+        x = float(np.exp(rng.normal(math.log(xi[0]), xi[1])))
+        s = float(rng.uniform(*scale))
+        w = fractal_channel(n_target=max(int(n_base * s), 100), dem_k=dem_k, cell=cell, mu=m, xi=x,
+                            mean_depth=4.0 * s, z=z)
+        z = w.z
+        w.meta.update(mu=m, xi=x, volume_scale=s)
+        out.append(w)
+    return out
 
 
 def make_params(w, gfsph_module, **over):

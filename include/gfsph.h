@@ -194,6 +194,29 @@ int gfsph_stats(gfsph_handle* h, int* out, int nout);
 int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol);
 
 /*
+ * Monte-Carlo ensembles (the realization loop of SPH_FEM_Driver_2019.f90:88-139
+ * with Get_MC_pixel_Vars_SW at plot times): nreal independent runs on one
+ * DEM, each with its own parameters (params[r], e.g. sampled mu = const(9)
+ * and xi = const(3)) and particles, advanced together: every member's graph
+ * launches go out on its own stream before any wait, so small realizations
+ * share the GPU.  Each member is an ordinary handle (gfsph_ensemble_member)
+ * for upload, download and rasters; its DEM copy erodes independently.
+ */
+typedef struct gfsph_ensemble gfsph_ensemble;
+int gfsph_ensemble_create(const gfsph_params* params /* nreal entries */, const gfsph_dem* dem, int nreal,
+                          gfsph_ensemble** out);
+int gfsph_ensemble_destroy(gfsph_ensemble* e);
+int gfsph_ensemble_member(gfsph_ensemble* e, int r, gfsph_handle** member);
+/* Up to nsteps steps of every member (each stops at t_end); min_steps_done
+ * receives the fewest steps any member completed. */
+int gfsph_ensemble_step(gfsph_ensemble* e, int nsteps, double t_end, int* min_steps_done);
+/* Hazard sample of every member (call at plot times). */
+int gfsph_ensemble_sample(gfsph_ensemble* e);
+/* Per DEM node, the fraction of members whose sampled maximum depth
+ * exceeds `threshold` (nx*ny values). */
+int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob);
+
+/*
  * Conjugate gradients of solvegc2 (SPH_GCsolver_2019.f90:16-316) on the device:
  * Jacobi-preconditioned CG on the element-by-element system sum_e gstif_e,
  * prescribed dofs (iffix != 0) held at their `fixed` values and masked out
