@@ -31,6 +31,17 @@ import numpy as np  # noqa: E402
 METRIC = "SPH particle-steps/s"
 UNIT = "particle-steps/s"
 B_ALG = {"k_density": 24, "k_force_rk": 72, "k_xsph": 44, "k_hist": 28}  # bytes per particle and launch
+# From one ncu --set full capture of the fractal-channel workload (200,011
+# particles, step 11; profiles/neighbour_kernels_fractal_channel_200k.md):
+# DRAM read + write bytes and warp instructions per launch, per particle.
+NCU_PER_PARTICLE = {
+    "k_density": {"dram_bytes": (5.256960e6 + 1.702400e6) / 200011, "warp_inst": 59987700 / 200011},
+    "k_iforce": {"dram_bytes": (43.446528e6 + 0.020224e6) / 200011, "warp_inst": 41244668 / 200011},
+    "k_force_rk": {"dram_bytes": 8.216832e6 / 200011, "warp_inst": 24964335 / 200011},
+    "k_xsph": {"dram_bytes": (45.841664e6 + 0.216064e6) / 200011, "warp_inst": 35318840 / 200011},
+}
+NCU_SOURCE = "profiles/neighbour_kernels_fractal_channel_200k.md (ncu, cold caches), scaled by active particles"
+ISSUE_PEAK = 148 * 4 * 1.965e9  # warp instructions/s: SMs x schedulers x max SM clock
 
 
 def load_peaks():
@@ -205,15 +216,17 @@ def ensemble_bench(args, torch, gfsph, workloads):
     ws = workloads.mc_ensemble(R, n_base=args.n)
     params = [workloads.make_params(w, gfsph) for w in ws]
     w0 = ws[0]
-    ens = gfsph.Ensemble(params, w0.z, dx=w0.dx, dy=w0.dy)
 
-    def upload():
-        for m, w in zip(ens.members, ws):
+    def fresh():
+        """A new ensemble at the initial state, warmed by 3 steps (graph
+        capture, capacity growth) — bit-identical however it is stepped."""
+        e = gfsph.Ensemble(params, w0.z, dx=w0.dx, dy=w0.dy)
+        for m, w in zip(e.members, ws):
             m.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+        e.step(3)
+        return e
 
-    upload()
-    ens.step(3)  # graph capture and capacity growth
-    upload()
+    ens = fresh()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for m in ens.members:
@@ -221,15 +234,18 @@ def ensemble_bench(args, torch, gfsph, workloads):
     torch.cuda.synchronize()
     t_loop = time.perf_counter() - t0
     looped = [m.download() for m in ens.members]
-    upload()
+    ens.close()
+    ens = fresh()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     _, done = ens.step(S)
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
     err = 0.0
+    identical = True
     for m, a in zip(ens.members, looped):
         b = m.download()
+        identical &= all(np.array_equal(a[k], b[k]) for k in a)
         d = np.linalg.norm((b["rho"] - a["rho"]).astype(np.float64)) / max(np.linalg.norm(a["rho"]), 1e-30)
         err = max(err, float(d))
     ens.close()
@@ -243,7 +259,7 @@ def ensemble_bench(args, torch, gfsph, workloads):
         "looped": {"realizations_per_s": R * S / t_loop / 5000.0, "seconds": t_loop,
                    "particle_steps_per_s": ps / t_loop},
         "speedup_vs_looped": t_loop / t_batch,
-        "max_rel_l2_depth_vs_looped": err,
+        "max_rel_l2_depth_vs_looped": err, "bit_identical_to_looped": bool(identical),
         "note": "realizations/s = realization-steps/s / 5000 (extrapolated from the timed steps); "
                 "device-synchronised host clock; member states bit-compared with the looped run",
     }
@@ -386,7 +402,16 @@ def main():
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": (NCU_PER_PARTICLE[dom]["dram_bytes"] * nact) if dom in NCU_PER_PARTICLE else None,
+                         "traffic_source": NCU_SOURCE,
+                         "issue_bound": ({"warp_inst_per_launch": NCU_PER_PARTICLE[dom]["warp_inst"] * nact,
+                                          "achieved_warp_inst_per_s":
+                                              NCU_PER_PARTICLE[dom]["warp_inst"] * nact / (dom_ms / 1000.0),
+                                          "peak_warp_inst_per_s": ISSUE_PEAK,
+                                          "frac": NCU_PER_PARTICLE[dom]["warp_inst"] * nact / (dom_ms / 1000.0)
+                                          / ISSUE_PEAK}
+                                         if dom in NCU_PER_PARTICLE else None),
                          "alg_bytes_per_launch": b_launch, "avg_launch_ms": dom_ms,
                          "step_achieved_gbs": 168 * n * args.steps / (ms_total / 1000.0) / 1e9 / world},
             "kernel_shares": shares,

@@ -19,7 +19,7 @@ namespace {
 enum KernelId {
     K_PREP, K_BOUNDS, K_GRID, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
-    K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT,
+    K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_TOP, K_BSCAN_ADD,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
@@ -27,7 +27,8 @@ const char* kKernelNames[K_COUNT] = {
     "k_prep", "k_bounds", "k_grid", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
-    "k_raster_idw", "k_hazard", "k_export_big", "step_batches"};
+    "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)", "k_scan_top(blocks)",
+    "k_scan_add(blocks)", "step_batches"};
 
 constexpr int kThreads = 128;
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
@@ -132,6 +133,9 @@ struct gfsph_handle {
     int* start = nullptr;
     int* tile_sum = nullptr;
     int cap_cells = 0;
+    int* bmark = nullptr;   // block map: 1 where a block holds particles (cleared by k_hist)
+    int* bstart = nullptr;  // its exclusive scan: slot of each occupied block
+    int cap_blocks = 0;
     // scalars
     StepScalars* S = nullptr;
     StepScalars* hS = nullptr;  // pinned mirror
@@ -217,6 +221,7 @@ void join(gfsph_handle* h, int k) {
 
 Search make_search(gfsph_handle* h) {
     Search q;
+    q.bstart = h->bstart;
     q.start = h->start;
     q.cellA = h->cellA;
     q.xhm = h->xhm;
@@ -240,14 +245,25 @@ int enqueue_search(gfsph_handle* h, int advance) {
     int nk = 0;
     int pb = blocks_for(n);
     int nscan = (h->cap_cells + kScanTile - 1) / kScanTile;
+    int nbscan = (h->cap_blocks + kScanTile - 1) / kScanTile;
+    const int* nblk = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, nblocks));
+    const int* ncel = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, ncells));
     if (!advance) { launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++; }
     launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
-    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_cells); }); nk++;
-    launch(h, K_HIST, [&] { k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->count, h->keyrank); }); nk++;
-    launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, S); }); nk++;
-    launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, S); }); nk++;
-    launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, S); }); nk++;
-    launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, S, h->perm); }); nk++;
+    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_blocks); }); nk++;
+    launch(h, K_MARK, [&] { k_mark<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark); }); nk++;
+    launch(h, K_BSCAN_TILES, [&] {
+        k_scan_tiles<<<nbscan, kScanThreads, 0, st>>>(h->bmark, h->bstart, h->tile_sum, nblk, S);
+    }); nk++;
+    launch(h, K_BSCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, nblk, S); }); nk++;
+    launch(h, K_BSCAN_ADD, [&] { k_scan_add<<<nbscan, kScanThreads, 0, st>>>(h->bstart, h->tile_sum, nblk, S); }); nk++;
+    launch(h, K_HIST, [&] {
+        k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark, h->bstart, h->count, h->keyrank, h->cap_cells);
+    }); nk++;
+    launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, ncel, S); }); nk++;
+    launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, ncel, S); }); nk++;
+    launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, ncel, S); }); nk++;
+    launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, h->bstart, S, h->perm); }); nk++;
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
     launch(h, K_REORDER, [&] {
         k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S);
@@ -307,7 +323,20 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 11 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 15 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+}
+
+int alloc_blocks(gfsph_handle* h, int cap) {
+    if (cap > kMaxCells) return GFSPH_ERR_CAPACITY;
+    dfree(h->bmark); dfree(h->bstart);
+    int st = 0;
+    st |= dalloc(&h->bmark, (size_t)cap + 1);
+    st |= dalloc(&h->bstart, (size_t)cap + 1);
+    if (st) return GFSPH_ERR_CUDA;
+    CK(cudaMemsetAsync(h->bmark, 0, ((size_t)cap + 1) * sizeof(int), h->stream));
+    h->cap_blocks = cap;
+    drop_graphs(h);
+    return 0;
 }
 
 int alloc_cells(gfsph_handle* h, int cap) {
@@ -377,6 +406,13 @@ int grow_after_error(gfsph_handle* h) {
         int st = alloc_cells(h, (int)want);
         if (st) return st;
         set_field<int>(h, offsetof(StepScalars, ncells), 0);
+    }
+    if (e & kErrBlocks) {
+        long long want = std::max<long long>((long long)s->need_blocks * 2, (long long)h->cap_blocks * 2);
+        if (want > kMaxCells) want = kMaxCells;
+        if (want < s->need_blocks) return GFSPH_ERR_CAPACITY;
+        int st = alloc_blocks(h, (int)want);
+        if (st) return st;
     }
     if (e & kErrNbr) {
         int want = std::max(s->need_nbr + 16, h->kcap * 3 / 2);
@@ -544,7 +580,7 @@ int gfsph_destroy(gfsph_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
     free_particles(h);
-    dfree(h->count); dfree(h->start); dfree(h->tile_sum);
+    dfree(h->count); dfree(h->start); dfree(h->tile_sum); dfree(h->bmark); dfree(h->bstart);
     dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
     dfree(h->d_auxv); dfree(h->S); dfree(h->d_racc); dfree(h->d_rout);
     dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
@@ -592,6 +628,10 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
     }
     if (h->cap_cells == 0) {
         int st = alloc_cells(h, 1 << 18);
+        if (st) return st;
+    }
+    if (h->cap_blocks == 0) {
+        int st = alloc_blocks(h, 1 << 16);
         if (st) return st;
     }
     cudaStream_t st = h->stream;

@@ -3,6 +3,13 @@
 // every step (counting sort); the neighbour table is built once per step and
 // reused by the density, force and XSPH passes, as the reference reuses its
 // pair list (w and dW frozen at the start of the step).
+//
+// Cell grids are block-sparse: each level's grid over the bounding box is cut
+// into blocks of 32 x 8 cells, a dense block map over the box marks the
+// blocks that hold particles, and only those blocks get cells (slot-major
+// keys: slot * 256 + row * 32 + column).  The cell count follows the area the
+// flow covers, not its bounding box, so separated releases on a large DEM
+// with small smoothing lengths stay within memory.
 #pragma once
 #include "gfsph_device.cuh"
 
@@ -12,12 +19,16 @@ constexpr int kScanTile = 2048;  // cells per scan tile (256 threads x 8)
 constexpr int kScanThreads = 256;
 constexpr float kBigFactor = 2.5f;  // hsml above kBigFactor * mean(hsml) goes to the big list
 constexpr int kMaxLevels = 24;      // level k cell size Hc * 2^(k-1)
+constexpr int kBlkX = 32;           // cells per block along x
+constexpr int kBlkY = 8;            // cells per block along y
+constexpr int kBlockCells = kBlkX * kBlkY;
 
 // error bits in StepScalars::err
 constexpr int kErrCells = 1;
 constexpr int kErrNbr = 2;
 constexpr int kErrNonFinite = 4;
 constexpr int kErrEmpty = 8;
+constexpr int kErrBlocks = 16;
 
 // Device-resident scalars of the step (one per handle).
 struct StepScalars {
@@ -35,10 +46,13 @@ struct StepScalars {
     float hc;         // regular-hsml bound Hc: level k holds hsml in (Hc*2^(k-1), Hc*2^k], level 0 hsml <= Hc
     int nlev;         // number of grid levels
     float lev_gx0[kMaxLevels], lev_gy0[kMaxLevels], lev_c[kMaxLevels];  // origin and cell size per level
-    int lev_ndx[kMaxLevels], lev_ndy[kMaxLevels], lev_off[kMaxLevels + 1];  // cells per level, first cell key
-    int ncells;
+    int lev_ndx[kMaxLevels], lev_ndy[kMaxLevels];  // cells per level along x and y
+    int lev_nbx[kMaxLevels], lev_boff[kMaxLevels + 1];  // blocks per level along x, first block-map entry
+    unsigned int lev_hmax_o[kMaxLevels];  // max hsml of the particles of each level (ordered uint, 0 = empty)
+    int nblocks;      // block-map entries (all levels)
+    int ncells;       // cells of the occupied blocks
     int nreg, nbig, nactive, nout;
-    int need_cells, need_nbr, need_big;
+    int need_cells, need_nbr, need_big, need_blocks;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
     int advance;      // 1 inside gfsph_step, 0 for search-only passes
 };
@@ -56,7 +70,8 @@ struct PState {
 
 // Scratch of the neighbour search (sorted order).
 struct Search {
-    const int* start;    // cell -> first slot (exclusive scan), ncells+1
+    const int* bstart;   // block-map entry -> slot of its block (exclusive scan of the marks), nblocks+1
+    const int* start;    // cell key -> first particle slot (exclusive scan), ncells+1
     const int* cellA;    // slot -> cell key (all levels), -1 out of the domain
     const float4* xhm;   // slot -> (x, y, hsml, mass) at the start of the step
     int* nbr;            // k-major neighbour table of the regular particles
@@ -84,6 +99,7 @@ __device__ __forceinline__ void prepare_step(StepScalars* S, int advance) {
     S->nout = 0;
     S->nbig = 0;
     S->ex0 = 0x7fffffff; S->ey0 = 0x7fffffff; S->ex1 = -1; S->ey1 = -1;
+    for (int k = 0; k < kMaxLevels; k++) S->lev_hmax_o[k] = 0u;
 }
 
 __global__ void k_prep(StepScalars* S, int advance) {
@@ -171,7 +187,7 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
 // over the same box, and one cell-key space covers all levels.  A particle
 // searches each level within hsml_i + (that level's hsml bound), so the
 // neighbour set is the reference's {j : r_ij < 2*(h_i+h_j)/2} exactly.
-__global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
+__global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (S->skip) return;
     if (S->bad) { S->err |= kErrNonFinite; S->skip = 1; return; }
@@ -208,19 +224,21 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_cells) {
         S->lev_c[k] = cell;
         S->lev_ndx[k] = ndx;
         S->lev_ndy[k] = ndy;
-        S->lev_off[k] = (int)min(off, 0x7fffffffLL);
-        off += (long long)ndx * (long long)ndy;
+        int nbx = (ndx + kBlkX - 1) / kBlkX, nby = (ndy + kBlkY - 1) / kBlkY;
+        S->lev_nbx[k] = nbx;
+        S->lev_boff[k] = (int)min(off, 0x7fffffffLL);
+        off += (long long)nbx * (long long)nby;
     }
-    S->lev_off[nlev] = (int)min(off, 0x7fffffffLL);
+    S->lev_boff[nlev] = (int)min(off, 0x7fffffffLL);
     S->hc = hc;
     S->nlev = nlev;
-    if (off + 1 > (long long)cap_cells) {
-        S->err |= kErrCells;
-        S->need_cells = (off + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(off + 1);
+    if (off + 1 > (long long)cap_blocks) {
+        S->err |= kErrBlocks;
+        S->need_blocks = (off + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(off + 1);
         S->skip = 1;
         return;
     }
-    S->ncells = (int)off;
+    S->nblocks = (int)off;
 }
 
 __device__ __forceinline__ void cell_of(float2 p, const StepScalars* S, int k, int& cx, int& cy) {
@@ -237,11 +255,54 @@ __device__ __forceinline__ int level_of(float hs, const StepScalars* S) {
     return k;
 }
 
-// Cell key (level offset + cell of that level's grid) and within-cell
-// arrival rank of each particle (counting sort histogram, grid_find
-// :938-948); out-of-domain particles get key -1.
-__global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* count, int2* keyrank) {
+// Cell coordinates are never negative: unsigned division and remainder by
+// the block sides compile to shifts and masks.
+__device__ __forceinline__ int block_of(const StepScalars* S, int k, int cx, int cy) {
+    return S->lev_boff[k] + (int)((unsigned)cy / kBlkY) * S->lev_nbx[k] + (int)((unsigned)cx / kBlkX);
+}
+
+// Marks the blocks that hold particles (block map, all levels) and takes the
+// largest smoothing length of every level, which bounds the stencils of the
+// neighbour search more tightly than the level's upper limit.
+__global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* bmark) {
     if (S->skip) return;
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {  // warp-uniform trips
+        int i = base + threadIdx.x;
+        unsigned int h0 = 0u;
+        if (i < n && !B.flag[i]) {
+            float2 p = B.pos[i];
+            if (!out_of_box(dem, p.x, p.y)) {
+                float hs = B.hsml[i];
+                int k = level_of(hs, S);
+                int cx, cy;
+                cell_of(p, S, k, cx, cy);
+                int b = block_of(S, k, cx, cy);
+                if (bmark[b] == 0) bmark[b] = 1;
+                if (k == 0) h0 = f2o(hs);
+                else atomicMax(&S->lev_hmax_o[k], f2o(hs));
+            }
+        }
+        h0 = __reduce_max_sync(0xffffffffu, h0);
+        if (lane == 0 && h0) atomicMax(&S->lev_hmax_o[0], h0);
+    }
+}
+
+// Cell key (slot of the particle's block * 256 + cell within the block) and
+// within-cell arrival rank of each particle (counting sort histogram,
+// grid_find :938-948); out-of-domain particles get key -1.  Clears the block
+// marks for the next step.  If the occupied blocks need more cells than the
+// histogram holds, nothing is counted and the step stops with kErrCells.
+__global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* bmark, const int* bstart, int* count,
+                       int2* keyrank, int cap_cells) {
+    if (S->skip) return;
+    const long long ncells = (long long)bstart[S->nblocks] * kBlockCells;
+    const bool over = ncells + 1 > (long long)cap_cells;
+    if (over && blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicOr(&S->err, kErrCells);
+        S->need_cells = (ncells + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(ncells + 1);
+    }
+    if (!over && blockIdx.x == 0 && threadIdx.x == 0) S->ncells = (int)ncells;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int2 kr = make_int2(-1, 0);
         float2 p = B.pos[i];
@@ -249,9 +310,13 @@ __global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* 
             int k = level_of(B.hsml[i], S);
             int cx, cy;
             cell_of(p, S, k, cx, cy);
-            int key = S->lev_off[k] + cy * S->lev_ndx[k] + cx;
-            kr.x = key;
-            kr.y = atomicAdd(&count[key], 1);
+            int b = block_of(S, k, cx, cy);
+            bmark[b] = 0;
+            if (!over) {
+                int key = bstart[b] * kBlockCells + (int)((unsigned)cy % kBlkY) * kBlkX + (int)((unsigned)cx % kBlkX);
+                kr.x = key;
+                kr.y = atomicAdd(&count[key], 1);
+            }
         }
         keyrank[i] = kr;
     }
@@ -259,9 +324,9 @@ __global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* 
 
 // Exclusive scan of the histogram, tile pass: each block scans kScanTile
 // cells and writes its tile total.
-__global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const StepScalars* S) {
-    if (S->skip) return;
-    int m = S->ncells + 1;
+__global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const int* nptr, const StepScalars* S) {
+    if (S->skip || S->err) return;
+    int m = *nptr + 1;
     int base = blockIdx.x * kScanTile;
     if (base >= m) return;
     __shared__ int sh[kScanTile];
@@ -304,9 +369,14 @@ __global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const 
 }
 
 // Scan of the tile totals (one block of 1024 threads, up to 8192 tiles).
-__global__ void k_scan_top(int* tile_sum, const StepScalars* S) {
+// Also turns an error raised since the step began (k_hist) into a skip.
+__global__ void k_scan_top(int* tile_sum, const int* nptr, StepScalars* S) {
     if (S->skip) return;
-    int ntiles = (S->ncells + 1 + kScanTile - 1) / kScanTile;
+    if (S->err) {
+        if (threadIdx.x == 0) S->skip = 1;
+        return;
+    }
+    int ntiles = (*nptr + 1 + kScanTile - 1) / kScanTile;
     __shared__ int wsum[32];
     const int per = 8;
     int loc[per];
@@ -342,9 +412,9 @@ __global__ void k_scan_top(int* tile_sum, const StepScalars* S) {
     }
 }
 
-__global__ void k_scan_add(int* start, const int* tile_sum, StepScalars* S) {
-    if (S->skip) return;
-    int m = S->ncells + 1;
+__global__ void k_scan_add(int* start, const int* tile_sum, const int* nptr, const StepScalars* S) {
+    if (S->skip || S->err) return;
+    int m = *nptr + 1;
     int base = blockIdx.x * kScanTile;
     if (base >= m) return;
     int add = tile_sum[blockIdx.x];
@@ -356,7 +426,7 @@ __global__ void k_scan_add(int* start, const int* tile_sum, StepScalars* S) {
 
 // Scatter (grid_find :952-958): particles to start[cell] + rank (level 0
 // first, then the higher levels), out-of-domain particles behind them.
-__global__ void k_scatter(const int2* keyrank, int n, const int* start, StepScalars* S, int* perm) {
+__global__ void k_scatter(const int2* keyrank, int n, const int* start, const int* bstart, StepScalars* S, int* perm) {
     if (S->skip) return;
     int nact = start[S->ncells];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -365,7 +435,7 @@ __global__ void k_scatter(const int2* keyrank, int n, const int* start, StepScal
         perm[slot] = i;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int nreg = (S->nlev > 1) ? start[S->lev_off[1]] : nact;
+        int nreg = (S->nlev > 1) ? start[bstart[S->lev_boff[1]] * kBlockCells] : nact;
         S->nreg = nreg;
         S->nbig = nact - nreg;
         S->nactive = nact;
@@ -415,29 +485,56 @@ __global__ void k_reorder(const PState B, int n, const int* perm, const int2* ke
     }
 }
 
-// Visits the particles j != i of level k that are neighbours of particle i
-// (position xi, smoothing length hi): every j of level k has hsml_j <= Hk =
-// Hc*2^k, so with r < hi + hj it lies within floor((hi + Hk)/cell + 0.01) + 1
-// cells of i's cell in that level's grid, whatever the rounding of the cell
-// coordinates.  Threads t0, t0+ts, ... of the caller share the candidates.
-template <class F>
-__device__ __forceinline__ void level_neighbours(const Search& Q, const StepScalars* S, int k, int i, float2 xi, float hi,
-                                                 int t0, int ts, F&& f) {
-    const int ndx = S->lev_ndx[k], ndy = S->lev_ndy[k], off = S->lev_off[k];
-    float rr = (hi + ldexpf(S->hc, k)) / S->lev_c[k] + 0.01f;
+// Stencil of level k around particle i: every j of level k has hsml_j <= Hk
+// (the level's largest smoothing length), so with r < hi + hj it lies within
+// floor((hi + Hk)/cell + 0.01) + 1 cells of i's cell in that level's grid,
+// whatever the rounding of the cell coordinates.  Returns false for an empty
+// level.
+__device__ __forceinline__ bool level_stencil(const StepScalars* S, int k, float2 xi, float hi, int& x0, int& x1,
+                                              int& y0, int& y1) {
+    unsigned int hk = S->lev_hmax_o[k];
+    if (hk == 0u) return false;
+    float rr = (hi + o2f(hk)) / S->lev_c[k] + 0.01f;
     int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
     int cx, cy;
     cell_of(xi, S, k, cx, cy);
-    int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
-    int y0 = max(cy - R, 0), y1 = min(cy + R, ndy - 1);
+    x0 = max(cx - R, 0); x1 = min(cx + R, S->lev_ndx[k] - 1);
+    y0 = max(cy - R, 0); y1 = min(cy + R, S->lev_ndy[k] - 1);
+    return true;
+}
+
+// Slot range of the cells x0..x1 of row jy inside block column bx (empty if
+// the block holds no particles).
+__device__ __forceinline__ void block_row_range(const Search& Q, const StepScalars* S, int k, int jy, int bx, int x0,
+                                                int x1, int& ja, int& jb) {
+    int b = S->lev_boff[k] + (int)((unsigned)jy / kBlkY) * S->lev_nbx[k] + bx;
+    int s0 = Q.bstart[b];
+    if (Q.bstart[b + 1] == s0) { ja = jb = 0; return; }
+    int lo = max(x0, bx * kBlkX) - bx * kBlkX, hi = min(x1, bx * kBlkX + kBlkX - 1) - bx * kBlkX;
+    int key = s0 * kBlockCells + (int)((unsigned)jy % kBlkY) * kBlkX;
+    ja = Q.start[key + lo];
+    jb = Q.start[key + hi + 1];
+}
+
+// Visits the particles j != i of level k that are neighbours of particle i
+// (position xi, smoothing length hi), row by row of the stencil and block
+// column by block column, each range in cell order.
+template <class F>
+__device__ __forceinline__ void level_neighbours(const Search& Q, const StepScalars* S, int k, int i, float2 xi, float hi,
+                                                 F&& f) {
+    int x0, x1, y0, y1;
+    if (!level_stencil(S, k, xi, hi, x0, x1, y0, y1)) return;
+    const int bx0 = (int)((unsigned)x0 / kBlkX), bx1 = (int)((unsigned)x1 / kBlkX);
     for (int jy = y0; jy <= y1; jy++) {
-        int row = off + jy * ndx;
-        int ja = Q.start[row + x0], jb = Q.start[row + x1 + 1];
-        for (int j = ja + t0; j < jb; j += ts) {
-            if (j == i) continue;
-            float4 o = Q.xhm[j];
-            PairGeom g;
-            if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+        for (int bx = bx0; bx <= bx1; bx++) {
+            int ja, jb;
+            block_row_range(Q, S, k, jy, bx, x0, x1, ja, jb);
+            for (int j = ja; j < jb; j++) {
+                if (j == i) continue;
+                float4 o = Q.xhm[j];
+                PairGeom g;
+                if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+            }
         }
     }
 }
@@ -458,7 +555,7 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
         double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * me.w);
         int cnt = 0;
         for (int k = 0; k < nlev; k++)
-            level_neighbours(Q, S, k, i, xi, hi, 0, 1, [&](int j, float4 o, const PairGeom& g) {
+            level_neighbours(Q, S, k, i, xi, hi, [&](int j, float4 o, const PairGeom& g) {
                 if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
                 cnt++;
                 acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
@@ -478,30 +575,27 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
 }
 
 // Visits every neighbour j of particle i cooperatively over one warp: the
-// lanes fetch the slot ranges of up to 32 stencil rows at once, then share
-// each row's candidates.
+// lanes fetch the slot ranges of up to 32 (row, block column) segments of the
+// stencil at once, then share each segment's candidates.
 template <class F>
 __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScalars* S, int i, int lane, F&& f) {
     const float4 me = Q.xhm[i];
     const float2 xi = make_float2(me.x, me.y);
     const float hi = me.z;
     for (int k = 0; k < S->nlev; k++) {
-        const int ndx = S->lev_ndx[k], ndy = S->lev_ndy[k], off = S->lev_off[k];
-        float rr = (hi + ldexpf(S->hc, k)) / S->lev_c[k] + 0.01f;
-        int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
-        int cx, cy;
-        cell_of(xi, S, k, cx, cy);
-        int x0 = max(cx - R, 0), x1 = min(cx + R, ndx - 1);
-        int y0 = max(cy - R, 0), y1 = min(cy + R, ndy - 1);
-        for (int yb = y0; yb <= y1; yb += 32) {
-            int jy = yb + lane, ja = 0, jb = 0;
-            if (jy <= y1) {
-                int row = off + jy * ndx;
-                ja = Q.start[row + x0];
-                jb = Q.start[row + x1 + 1];
+        int x0, x1, y0, y1;
+        if (!level_stencil(S, k, xi, hi, x0, x1, y0, y1)) continue;
+        const int bx0 = (int)((unsigned)x0 / kBlkX), ncol = (int)((unsigned)x1 / kBlkX) - bx0 + 1;
+        const long long nseg = (long long)(y1 - y0 + 1) * ncol;
+        for (long long sb = 0; sb < nseg; sb += 32) {
+            long long sg = sb + lane;
+            int ja = 0, jb = 0;
+            if (sg < nseg) {
+                int jy = y0 + (int)(sg / ncol), bx = bx0 + (int)(sg % ncol);
+                block_row_range(Q, S, k, jy, bx, x0, x1, ja, jb);
             }
-            int nrows = min(32, y1 - yb + 1);
-            for (int r = 0; r < nrows; r++) {
+            int nr = (int)min(32LL, nseg - sb);
+            for (int r = 0; r < nr; r++) {
                 int a = __shfl_sync(0xffffffffu, ja, r), e = __shfl_sync(0xffffffffu, jb, r);
                 for (int j = a + lane; j < e; j += 32) {
                     if (j == i) continue;

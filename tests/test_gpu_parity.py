@@ -330,3 +330,39 @@ def test_long_run_with_growing_front(gfsph_lib, oracle_mod):
     assert rel_l2(g["x"], st.x) <= 1e-5
     assert rel_l2(g["mass"], st.mass) <= 1e-5
     sim.close()
+
+
+def test_far_apart_releases_on_a_large_dem(gfsph_lib, oracle_mod):
+    """Two small releases 6 km apart on a 5 km x 5 km DEM with 0.5 m smoothing
+    lengths: the bounding box holds ~2.6e8 cells of the finest level, but only
+    the occupied 32 x 8-cell blocks get cells.  Sets stay exact and one step
+    matches the oracle."""
+    rng = np.random.default_rng(21)
+    nc = 1500
+    parts = []
+    for cx, cy in ((300.0, 300.0), (4700.0, 4700.0)):
+        parts.append(np.stack([rng.uniform(cx, cx + 20.0, nc), rng.uniform(cy, cy + 20.0, nc)], 1))
+    x = np.concatenate(parts).astype(np.float32)
+    n = x.shape[0]
+    h = rng.uniform(0.4, 0.6, n).astype(np.float32)
+    h[rng.choice(n, 6, replace=False)] = np.float32(3.0)  # a coarse level as well
+    rho = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    mass = (rho * np.float32(0.25)).astype(np.float32)
+    z = np.zeros((1024, 1024), np.float32)
+    w = workloads.Workload(name="far_apart", const=workloads.voellmy_const(0.2, 500.0), options=dict(
+        pa_sph=2, nnps=2, sle=1, skf=1, average_velocity=1, ic_adapt=0, h_inf=0.01, dt=0.01, dem_deriv=1),
+        z=z, dx=5.0, dy=5.0, x=x, v=np.zeros_like(x), rho=rho, mass=mass, hsml=h)
+    sim, st, p = setup_pair(w, oracle_mod)
+    sim.density()
+    off, idx = sim.neighbours()
+    ref = oracle_mod.pairs(oracle_mod.MODE_FP32, p, x, h)
+    assert np.array_equal(off, ref["offsets"]) and np.array_equal(idx, ref["idx"])
+    s = sim.stats()
+    assert s["levels"] >= 2 and s["cells"] < 2_000_000
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    sim.step(1)
+    g = sim.download()
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, 1024, 1024, w.dx, w.dy, st, 1)
+    for key, r in (("x", st.x), ("v", st.v), ("rho", st.rho), ("hsml", st.hsml)):
+        assert max_rel(g[key], r, floor=1e-3) <= 1e-6, key
+    sim.close()
