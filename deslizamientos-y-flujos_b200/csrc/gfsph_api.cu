@@ -38,7 +38,7 @@ constexpr int kMaxCells = kScanTile * 8192;
 __global__ void k_copy_state(PState A, PState B, int n) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         B.pos[s] = A.pos[s]; B.vel[s] = A.vel[s]; B.rho[s] = A.rho[s]; B.mass[s] = A.mass[s];
-        B.hsml[s] = A.hsml[s]; B.flag[s] = A.flag[s]; B.id[s] = A.id[s];
+        B.hsml[s] = A.hsml[s]; B.flag[s] = A.flag[s]; B.id[s] = A.id[s]; B.pwp[s] = A.pwp[s];
     }
 }
 
@@ -47,8 +47,19 @@ __global__ void k_unsort(PState B, int n, PState U) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = B.id[s];
         U.pos[o] = B.pos[s]; U.vel[o] = B.vel[s]; U.rho[o] = B.rho[s]; U.mass[o] = B.mass[s];
-        U.hsml[o] = B.hsml[s]; U.flag[o] = B.flag[s];
+        U.hsml[o] = B.hsml[s]; U.flag[o] = B.flag[s]; U.pwp[o] = B.pwp[s];
     }
+}
+
+// Uaux(1,:) = pwp0rel * rho * alphas at input (Input_SW, SPH_SW_2019.f90:1829-1852).
+__global__ void k_pwp_init(float* pwp, const float* rho, int n, float pwp0rel, float alfs) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+        pwp[s] = pwp0rel * (rho[s] * alfs);
+}
+
+// dst[s] = src[id[s]]: a caller array in the original order into slot order.
+__global__ void k_gather_by_id(const float* src, const int* id, int n, float* dst) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) dst[s] = src[id[s]];
 }
 
 __global__ void k_unsort_f2(const float2* src, const int* id, int n, float2* dst) {
@@ -128,6 +139,7 @@ struct gfsph_handle {
     int* ncount = nullptr;
     int kcap = 0;
     float2* indv = nullptr;  // internal acceleration of every active particle
+    float* rho0 = nullptr;   // start-of-step depth (pore-water pressure update)
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -229,6 +241,7 @@ Search make_search(gfsph_handle* h) {
     q.ncount = h->ncount;
     q.pterm = h->pterm;
     q.indv = h->indv;
+    q.rho0 = h->rho0;
     q.kcap = h->kcap;
     return q;
 }
@@ -266,7 +279,7 @@ int enqueue_search(gfsph_handle* h, int advance) {
     launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, h->bstart, S, h->perm); }); nk++;
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
     launch(h, K_REORDER, [&] {
-        k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S);
+        k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S, h->rheo, h->rho0);
     }); nk++;
     // the coarse-level kernels run beside the level-0 ones when graphs are
     // captured (side stream); serially otherwise
@@ -365,16 +378,17 @@ void free_particles(gfsph_handle* h) {
     PState* sets[3] = {&h->A, &h->B, &h->U};
     for (PState* p : sets) {
         dfree(p->pos); dfree(p->vel); dfree(p->rho); dfree(p->mass); dfree(p->hsml); dfree(p->flag); dfree(p->id);
+        dfree(p->pwp);
     }
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
-    dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv);
+    dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv); dfree(h->rho0);
     h->kcap = 0;
 }
 
 int alloc_pstate(PState* p, int n) {
     int st = 0;
     st |= dalloc(&p->pos, n); st |= dalloc(&p->vel, n); st |= dalloc(&p->rho, n); st |= dalloc(&p->mass, n);
-    st |= dalloc(&p->hsml, n); st |= dalloc(&p->flag, n); st |= dalloc(&p->id, n);
+    st |= dalloc(&p->hsml, n); st |= dalloc(&p->flag, n); st |= dalloc(&p->id, n); st |= dalloc(&p->pwp, n);
     return st;
 }
 
@@ -425,6 +439,38 @@ int grow_after_error(gfsph_handle* h) {
     return 0;
 }
 
+// The tanfi density factor and the pore-water-pressure bounds:
+// DFs_FSs_dens_and_pwp_factors (SPH_SW_2019.f90:8959-9060) for the friction,
+// mini_DFs_dens_and_pwp_factors (:11502-11580) for Get_Pwp_SW's lower bound;
+// ic_hrelSat = 0.
+void pwp_factors(const gfsph_params* p, Rheo& c) {
+    const float* k = p->cst;  // k[i-1] = const(i)
+    const int fct = (int)(k[19] + 0.1f);
+    const float dens = k[1], denss = k[16], densw = k[17], sr = k[18], alphas = k[13];
+    c.icpwp = p->icpwp;
+    c.fact_dens = 1.f; c.fact_pwp_max = 1.f; c.fact_pwp_min = 0.f; c.fpwp_max = 1.f; c.fpwp_min = 0.f;
+    c.fpwp_min_g = 0.f;
+    if (fct == 1) {
+        float porosity = (denss - dens) / (denss - densw);
+        float dens2 = (1.f - porosity) * denss;
+        float dens1 = (1.f - porosity) * denss + porosity * densw;
+        float dens_bar = (1.f - alphas) * dens2 + alphas * dens1;
+        float dens_bar_eff = dens_bar - densw * alphas;
+        c.fact_dens = dens_bar_eff / dens_bar;
+        if (p->icpwp > 0) {
+            c.fact_pwp_max = 1.f + (alphas * densw) / dens_bar_eff;
+            c.fpwp_min = -(alphas * densw) / dens_bar_eff;
+            float g2 = (1.f - porosity) * denss + (porosity * densw) * sr;
+            float gbar = (1.f - alphas) * g2 + alphas * dens1;
+            float geff = gbar - densw * alphas;
+            c.fpwp_min_g = -(alphas * densw) / geff;
+        }
+    }
+    c.bfact = k[12];
+    c.alphas = alphas;
+    c.alphas2 = k[13] * k[13];
+}
+
 int validate(const gfsph_params* p) {
     int nfric = (int)(p->cst[4] + 0.01f);
     bool erosion = p->cst[20] > 1.e-9f;
@@ -438,7 +484,13 @@ int validate(const gfsph_params* p) {
     if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
     if (p->ic_adapt < 0 || p->ic_adapt > 2) return GFSPH_ERR_UNSUPPORTED;
     if ((int)(p->cst[15] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;  // ic_cosTheta
-    if ((int)(p->cst[19] + 0.1f) != 0) return GFSPH_ERR_UNSUPPORTED;   // ic_fct_dens
+    const int fct = (int)(p->cst[19] + 0.1f);                          // ic_fct_dens
+    if (fct != 0 && fct != 1) return GFSPH_ERR_UNSUPPORTED;
+    if (p->icpwp != 0 && p->icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
+    if ((fct != 0 || p->icpwp != 0) && (int)(p->cst[33] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;  // ic_hrelSat
+    if (p->icpwp == 3 && p->cst[25] > 0.f) return GFSPH_ERR_UNSUPPORTED;  // drag laws rescale Bfact
+    if (fct == 1 && (p->cst[16] < 1.e-3f || p->cst[17] < 1.e-3f)) return GFSPH_ERR_ARG;  // denss, densw
+    if (fct == 1 && p->icpwp != 0 && !(p->cst[13] > 0.01f)) return GFSPH_ERR_UNSUPPORTED;
     if (p->cst[0] < 0.f) return GFSPH_ERR_UNSUPPORTED;                 // inclined-plane gravity input
     if (p->cst[14] <= 1.e-8f || p->cst[9] <= 1.e-8f) return GFSPH_ERR_ARG;  // comp, hfrict0 (:1357-1365)
     if (!(p->dt > 0.f)) return GFSPH_ERR_ARG;
@@ -512,6 +564,7 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     c.erosion = (k[20] > 1.e-9f) ? 1 : 0;
     c.skf = p->skf; c.pa_sph = p->pa_sph; c.sle = p->sle; c.av_vel = p->average_velocity ? 1 : 0;
     c.ic_adapt = p->ic_adapt;
+    pwp_factors(p, c);
 
     // DEM rows on the host, as Topo_main leaves them before the time loop
     int nx = dem->nx, ny = dem->ny;
@@ -620,7 +673,7 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
         st |= alloc_pstate(&h->A, n); st |= alloc_pstate(&h->B, n); st |= alloc_pstate(&h->U, n);
         st |= dalloc(&h->cellA, n); st |= dalloc(&h->velfin, n); st |= dalloc(&h->pterm, n);
         st |= dalloc(&h->keyrank, n); st |= dalloc(&h->perm, n); st |= dalloc(&h->ncount, n);
-        st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n); st |= dalloc(&h->indv, n);
+        st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n); st |= dalloc(&h->indv, n); st |= dalloc(&h->rho0, n);
         if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
         if (st) return st;
@@ -643,6 +696,12 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
     if (out_flag) CK(cudaMemcpyAsync(h->B.flag, out_flag, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
     else CK(cudaMemsetAsync(h->B.flag, 0, (size_t)n * sizeof(int), st));
     launch(h, K_UNSORT, [&] { k_iota<<<blocks_for(n), kThreads, 0, st>>>(h->B.id, n); });
+    if (h->rheo.icpwp == 3)
+        launch(h, K_UNSORT, [&] {
+            k_pwp_init<<<blocks_for(n), kThreads, 0, st>>>(h->B.pwp, h->B.rho, n, h->P.pwp0rel, h->P.cst[13]);
+        });
+    else
+        CK(cudaMemsetAsync(h->B.pwp, 0, (size_t)n * sizeof(float), st));
     CK(cudaGetLastError());
     h->has_state = true;
     h->searched = false;
@@ -661,6 +720,28 @@ int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass,
     if (mass) CK(cudaMemcpyAsync(mass, h->U.mass, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st));
     if (hsml) CK(cudaMemcpyAsync(hsml, h->U.hsml, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st));
     if (out_flag) CK(cudaMemcpyAsync(out_flag, h->U.flag, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return GFSPH_OK;
+}
+
+int gfsph_set_pwp(gfsph_handle* h, const float* pwp) {
+    if (!h || !pwp) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    int n = h->n;
+    cudaStream_t st = h->stream;
+    CK(cudaMemcpyAsync(h->U.pwp, pwp, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
+    launch(h, K_UNSORT, [&] { k_gather_by_id<<<blocks_for(n), kThreads, 0, st>>>(h->U.pwp, h->B.id, n, h->B.pwp); });
+    CK(cudaStreamSynchronize(st));
+    return GFSPH_OK;
+}
+
+int gfsph_get_pwp(gfsph_handle* h, float* pwp) {
+    if (!h || !pwp) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    int n = h->n;
+    cudaStream_t st = h->stream;
+    launch(h, K_UNSORT, [&] { k_unsort<<<blocks_for(n), kThreads, 0, st>>>(h->B, n, h->U); });
+    CK(cudaMemcpyAsync(pwp, h->U.pwp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return GFSPH_OK;
 }

@@ -151,15 +151,22 @@ __device__ __forceinline__ void dem_lookup(const DemView& d, float xx, float yy,
 struct Rheo {
     float g, dens, xi, tauy0, constK, tanfi, hfrict0, comp, keros, slip, h_inf, cgra05;
     int nfric, erosion, skf, pa_sph, sle, av_vel, ic_adapt;
+    // basal pore-water pressure (icpwp = 3) and the density factor of tanfi:
+    // DFs_FSs_dens_and_pwp_factors (SPH_SW_2019.f90:8959-9060) for the
+    // friction, mini_DFs_dens_and_pwp_factors (:11502-11580) for the update
+    int icpwp;
+    float fact_dens, fact_pwp_max, fact_pwp_min, fpwp_max, fpwp_min, fpwp_min_g, bfact, alphas, alphas2;
 };
 
 // Locals of ExtForces_SW shared with its contained routines.
 struct ExtLocal {
     float h, hu, hv, hinv, vmod, hvmod, hvmodinv, frictx, fricty, totfrict, cf5, gravx, gravy;
+    float hrho;  // rho(ipoin) as ExtForces_SW reads it, before the comp clamp
 };
 
 // Start of the ExtForces_SW particle loop, SPH_SW_2019.f90:8564-8596.
 __device__ __forceinline__ void ext_locals(const Rheo& c, float hdepth, float vx, float vy, ExtLocal& L) {
+    L.hrho = hdepth;
     L.h = hdepth;
     L.hu = L.h * vx;
     L.hv = L.h * vy;
@@ -177,7 +184,7 @@ __device__ __forceinline__ void ext_locals(const Rheo& c, float hdepth, float vx
 // Get_Grav_Ext_SW (SPH_SW_2019.f90:9241-9349, ic_cosTheta = 0) and
 // basal_friction_Ext_SW (:9355-9828) before its reversal filter.
 __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& d, float xx, float yy, float vx,
-                                                  float vy, ExtLocal& L) {
+                                                  float vy, float pwp, ExtLocal& L) {
     const bool frictional = (c.nfric >= 5 && c.nfric <= 7);
     const bool v2byr = (c.nfric == 7);
     float zpx, zpy, top[6];
@@ -219,7 +226,17 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
                 cv2byr = (L.vmod * L.vmod) * rinv;
             }
         }
-        float gtanfi = ((c.g + cv2byr) * c.tanfi) * 1.f;
+        float tanfi = c.tanfi;
+        if (c.icpwp == 3) {  // :9670-9688: pwp = Uaux(1,ipoin), filtered, then tanfi*factpw
+            float hhh = L.hrho;
+            if (pwp > c.fpwp_max * hhh) pwp = c.fpwp_max * hhh;
+            if (pwp < c.fpwp_min * hhh) pwp = c.fpwp_min * hhh;
+            float factpw = 1.f - pwp * L.hinv;
+            if (factpw < c.fact_pwp_min) factpw = c.fact_pwp_min;
+            if (factpw > c.fact_pwp_max) factpw = c.fact_pwp_max;
+            tanfi = tanfi * factpw;
+        }
+        float gtanfi = ((c.g + cv2byr) * tanfi) * c.fact_dens;  // :9706
         if (gtanfi < 0.f) gtanfi = 0.f;
         L.cf5 = gtanfi;
         L.frictx = ((L.cf5 * L.hu) * L.hvmodinv) * L.h;
@@ -280,10 +297,11 @@ __device__ __forceinline__ void reversal_filter(const Rheo& c, float dt, float v
 // particle loop, SPH_SW_2019.f90:8532-8716 (gravity, basal friction with the
 // reversal filter, Hungr erosion momentum :8664-8697).
 __device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float dt, float xx, float yy, float vx,
-                                          float vy, float hdepth, float in0, float in1, float& ex0, float& ex1) {
+                                          float vy, float hdepth, float pwp, float in0, float in1, float& ex0,
+                                          float& ex1) {
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
-    grav_and_friction(c, d, xx, yy, vx, vy, L);
+    grav_and_friction(c, d, xx, yy, vx, vy, pwp, L);
     ex0 = 0.f + L.gravx;
     ex1 = 0.f + L.gravy;
     reversal_filter(c, dt, vx, vy, ex0 + in0, ex1 + in1, L);
@@ -299,11 +317,35 @@ __device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float
 // Hungr erosion rate after the RK update (ExtForces_SW(1), :8717-8760):
 // E = C22 * h * vmod with the ExtForces locals after basal friction.
 __device__ __forceinline__ float erosion_rate_final(const Rheo& c, const DemView& d, float xx, float yy, float vx,
-                                                    float vy, float hdepth) {
+                                                    float vy, float hdepth, float pwp) {
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
-    grav_and_friction(c, d, xx, yy, vx, vy, L);
+    grav_and_friction(c, d, xx, yy, vx, vy, pwp, L);
     return (c.keros * L.h) * L.vmod;
+}
+
+// Get_Pwp_SW with one pwp point (icpwp = 3), SPH_SW_2019.f90:11176-11371 (no
+// basal flux, no DF terms): the basal pressure head relaxes exponentially
+// towards the depth change of the step, dhh = Drho_RK (RK45 :918-919), then
+// is bounded by the depth and by hh * alphas * fpwp_min.
+__device__ __forceinline__ float pwp_update(const Rheo& c, float u, float hh, float dhh, float dt) {
+    float hinv;
+    if (hh < c.comp) {
+        hh = c.comp;
+        hinv = 1.f / c.comp;
+    } else {
+        hinv = 1.f / hh;
+    }
+    float betaw = ((c.bfact * hinv) * hinv) / c.alphas2;
+    // exp in FP64 rounded once to FP32 (a correctly rounded FP32 exp in all
+    // but vanishing cases): (1 - e) below cancels to a few bits when
+    // betaw*dt is small, so an FP32 exp that is off by an ulp would change the
+    // update by ~1e-3 relative
+    float e = (float)exp((double)(-(betaw * dt)));
+    u = u * e + ((dhh / dt) * (1.f - e)) / betaw;
+    if (u > hh) u = hh;
+    if (u < (hh * c.alphas) * c.fpwp_min_g) u = (hh * c.alphas) * c.fpwp_min_g;
+    return u;
 }
 
 __device__ __forceinline__ bool out_of_box(const DemView& d, float xx, float yy) {

@@ -66,6 +66,7 @@ struct PState {
     float* hsml;
     int* flag;
     int* id;
+    float* pwp;  // basal pore-water pressure Uaux(1,:) (icpwp = 3)
 };
 
 // Scratch of the neighbour search (sorted order).
@@ -78,6 +79,7 @@ struct Search {
     int* ncount;
     float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
     float2* indv;        // internal acceleration of every active particle (slot order)
+    float* rho0;         // depth at the start of the step, after Adaptive_dt's h_inf clamp (icpwp = 3)
     int kcap;
 };
 
@@ -466,16 +468,23 @@ __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, int*
 }
 
 // Gathers the state into the new (cell-sorted) order.
+// With icpwp = 3 also the pore-water pressure and rho0, the depth RK45 keeps
+// at its start (after the h_inf clamp of Adaptive_dt_sph_SW :6540, modes 1-2).
 __global__ void k_reorder(const PState B, int n, const int* perm, const int2* keyrank, PState A, int* cellA,
-                          float4* xhm, const StepScalars* S) {
+                          float4* xhm, const StepScalars* S, Rheo c, float* rho0) {
     if (S->skip) return;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = perm[s];
         float2 p = B.pos[o];
         float hs = B.hsml[o], m = B.mass[o];
+        float r = B.rho[o];
         A.pos[s] = p;
         A.vel[s] = B.vel[o];
-        A.rho[s] = B.rho[o];
+        A.rho[s] = r;
+        if (c.icpwp == 3) {
+            A.pwp[s] = B.pwp[o];
+            rho0[s] = ((c.ic_adapt == 1 || c.ic_adapt == 2) && r < c.h_inf) ? c.h_inf : r;
+        }
         A.mass[s] = m;
         A.hsml[s] = hs;
         A.flag[s] = B.flag[o];
@@ -516,25 +525,87 @@ __device__ __forceinline__ void block_row_range(const Search& Q, const StepScala
     jb = Q.start[key + hi + 1];
 }
 
+// Pair test of particle i against the slots ja..jb-1.
+template <class F>
+__device__ __forceinline__ void visit_range(const Search& Q, int i, float2 xi, float hi, int ja, int jb, F& f) {
+    for (int j = ja; j < jb; j++) {
+        if (j == i) continue;
+        float4 o = Q.xhm[j];
+        PairGeom g;
+        if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+    }
+}
+
 // Visits the particles j != i of level k that are neighbours of particle i
-// (position xi, smoothing length hi), row by row of the stencil and block
-// column by block column, each range in cell order.
+// (position xi, smoothing length hi), row by row of the stencil, each row in
+// cell order.  Rows further than one cell from i's row are trimmed to the
+// circle: a particle of row jy, d = |jy - cy| >= 2 rows away, is more than
+// (d - 1) cells away in y, so with r < hi + Hk it lies within
+// sqrt(rr^2 - (d - 1)^2) + 1 cells in x (rr and d - 1 carry 0.01-cell
+// margins for the rounding of the cell coordinates).  Along a row, the end of
+// one block's slots is the start of the next block's.
 template <class F>
 __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScalars* S, int k, int i, float2 xi, float hi,
                                                  F&& f) {
-    int x0, x1, y0, y1;
-    if (!level_stencil(S, k, xi, hi, x0, x1, y0, y1)) return;
-    const int bx0 = (int)((unsigned)x0 / kBlkX), bx1 = (int)((unsigned)x1 / kBlkX);
+    const unsigned int hk = S->lev_hmax_o[k];
+    if (hk == 0u) return;
+    const float rr = (hi + o2f(hk)) / S->lev_c[k] + 0.01f;
+    const int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
+    const float rr2 = rr * rr;
+    int cx, cy;
+    cell_of(xi, S, k, cx, cy);
+    const int ndx = S->lev_ndx[k], nbx = S->lev_nbx[k], boff = S->lev_boff[k];
+    const int y0 = max(cy - R, 0), y1 = min(cy + R, S->lev_ndy[k] - 1);
     for (int jy = y0; jy <= y1; jy++) {
-        for (int bx = bx0; bx <= bx1; bx++) {
-            int ja, jb;
-            block_row_range(Q, S, k, jy, bx, x0, x1, ja, jb);
-            for (int j = ja; j < jb; j++) {
+        const int d = abs(jy - cy);
+        int rx = R;
+        if (d >= 2) {
+            const float dd = (float)d - 1.01f;
+            const float q = rr2 - dd * dd;
+            if (!(q > 0.f)) continue;
+            rx = min(R, (int)sqrtf(q) + 1);
+        }
+        const int x0 = max(cx - rx, 0), x1 = min(cx + rx, ndx - 1);
+        const int c0 = (int)((unsigned)x0 / kBlkX), c1 = (int)((unsigned)x1 / kBlkX);
+        const int brow = boff + (int)((unsigned)jy / kBlkY) * nbx;
+        const int row = (int)((unsigned)jy % kBlkY) * kBlkX;
+        if (c1 - c0 <= 1) {
+            // one or two block columns: the two slot ranges are walked as one
+            // sequence, so lanes whose rows straddle a block edge and lanes
+            // whose rows do not run the same loop (no divergent second pass)
+            const int s0 = Q.bstart[brow + c0], s1 = Q.bstart[brow + c0 + 1];
+            const int e0 = min(x1, c0 * kBlkX + kBlkX - 1);
+            int ja = 0, na = 0, jb = 0, nb = 0;
+            if (s1 != s0) {
+                const int key = s0 * kBlockCells + row - c0 * kBlkX;
+                ja = Q.start[key + x0];
+                na = Q.start[key + e0 + 1] - ja;
+            }
+            if (c1 > c0) {
+                const int s2 = Q.bstart[brow + c1 + 1];
+                if (s2 != s1) {
+                    const int key = s1 * kBlockCells + row - c1 * kBlkX;
+                    jb = Q.start[key + c1 * kBlkX];
+                    nb = Q.start[key + x1 + 1] - jb;
+                }
+            }
+            for (int t = 0; t < na + nb; t++) {
+                const int j = (t < na) ? ja + t : jb + (t - na);
                 if (j == i) continue;
                 float4 o = Q.xhm[j];
                 PairGeom g;
                 if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
             }
+            continue;
+        }
+        int s1 = Q.bstart[brow + c0];
+        for (int bx = c0; bx <= c1; bx++) {
+            const int s0 = s1;
+            s1 = Q.bstart[brow + bx + 1];  // end of this block = start of the next
+            if (s1 == s0) continue;
+            const int key = s0 * kBlockCells + row - bx * kBlkX;
+            visit_range(Q, i, xi, hi, Q.start[key + max(x0, bx * kBlkX)],
+                        Q.start[key + min(x1, bx * kBlkX + kBlkX - 1) + 1], f);
         }
     }
 }
@@ -821,6 +892,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
             B.pos[i] = A.pos[i]; B.vel[i] = A.vel[i]; velfin[i] = A.vel[i];
             B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
             B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
+            if (c.icpwp == 3) B.pwp[i] = 0.f;  // Get_Pwp_SW zeroes out-of-domain particles
             if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
             continue;
         }
@@ -829,6 +901,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
         const float h = A.rho[i];
         const float hc = (h < c.h_inf) ? c.h_inf : h;  // IntForces_SW clamp, seen by ExtForces_SW(0)
         const float2 x0 = A.pos[i], v0 = A.vel[i];
+        const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
         float xx = x0.x, xy = x0.y, vx = v0.x, vy = v0.y;
         float ex0 = 0.f, ex1 = 0.f;
         float Dx0 = 0.f, Dx1 = 0.f, Dv0 = 0.f, Dv1 = 0.f;
@@ -847,7 +920,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
                 if (out_of_box(dem, xx, xy)) {
                     out = true;
                 } else {
-                    ext_accel(c, dem, dt, xx, xy, vx, vy, hc, in0, in1, ex0, ex1);
+                    ext_accel(c, dem, dt, xx, xy, vx, vy, hc, pwp, in0, in1, ex0, ex1);
                     Dv0 = Dv0 + f2 * (ex0 + in0);
                     Dv1 = Dv1 + f2 * (ex1 + in1);
                     Dx0 = Dx0 + f2 * vx;
@@ -866,7 +939,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
             out = out_of_box(dem, xx, xy);
         }
         float er = 0.f;
-        if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h);
+        if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h, pwp);
         if (c.erosion) erosion_scatter(dem, S, xx, xy, dt * er, !out, auxv);
         if (!out) {
             if (c.erosion) m = m + ((dt * er) * m) / h;
@@ -880,6 +953,7 @@ __global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalar
         B.hsml[i] = hs;
         B.flag[i] = out ? 1 : 0;
         B.id[i] = A.id[i];
+        if (c.icpwp == 3) B.pwp[i] = out ? 0.f : pwp_update(c, pwp, h, h - Q.rho0[i], dt);
     }
 }
 

@@ -23,7 +23,9 @@ module gfsph_c
      integer(c_int) :: ic_adapt
      real(c_float)  :: h_inf, dt
      integer(c_int) :: dem_deriv, max_neighbours
-     integer(c_int) :: reserved(8)
+     integer(c_int) :: icpwp                   ! 0 or 3 (Get_Pwp_SW, nUaux = 1)
+     real(c_float)  :: pwp0rel                 ! initial Uaux = pwp0rel * rho * const(14)
+     integer(c_int) :: reserved(6)
   end type gfsph_params
 
   type, bind(c) :: gfsph_dem
@@ -144,6 +146,16 @@ module gfsph_c
        integer(c_int), value :: mode, nx, ny
        real(c_float), value :: dx, dy
        real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
+     end function
+     integer(c_int) function gfsph_set_pwp(h, pwp) bind(c, name="gfsph_set_pwp")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: h
+       real(c_float), intent(in) :: pwp(*)
+     end function
+     integer(c_int) function gfsph_get_pwp(h, pwp) bind(c, name="gfsph_get_pwp")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: h
+       real(c_float), intent(out) :: pwp(*)
      end function
      integer(c_int) function gfsph_ensemble_create(params, dem, nreal, ens) bind(c, name="gfsph_ensemble_create")
        import :: c_int, c_ptr, gfsph_params, gfsph_dem

@@ -46,7 +46,7 @@ class Params(C.Structure):
         ("pa_sph", C.c_int), ("nnps", C.c_int), ("sle", C.c_int), ("skf", C.c_int),
         ("summation_density", C.c_int), ("average_velocity", C.c_int), ("nor_density", C.c_int),
         ("ic_adapt", C.c_int), ("h_inf", C.c_float), ("dt", C.c_float), ("dem_deriv", C.c_int),
-        ("max_neighbours", C.c_int), ("reserved", C.c_int * 8),
+        ("max_neighbours", C.c_int), ("icpwp", C.c_int), ("pwp0rel", C.c_float), ("reserved", C.c_int * 6),
     ]
 
 
@@ -87,6 +87,8 @@ SIGNATURES = {
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
     "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "gfsph_set_pwp": (C.c_int, [C.c_void_p, _FP]),
+    "gfsph_get_pwp": (C.c_int, [C.c_void_p, _FP]),
     "gfsph_ensemble_create": (C.c_int, [C.POINTER(Params), C.POINTER(Dem), C.c_int, C.POINTER(C.c_void_p)]),
     "gfsph_ensemble_destroy": (C.c_int, [C.c_void_p]),
     "gfsph_ensemble_member": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
@@ -143,7 +145,7 @@ def _ip(a):
 
 
 def make_params(const=None, *, pa_sph=2, nnps=2, sle=1, skf=1, summation_density=1, average_velocity=1,
-                nor_density=0, ic_adapt=0, h_inf=0.01, dt=0.01, dem_deriv=1, max_neighbours=0):
+                nor_density=0, ic_adapt=0, h_inf=0.01, dt=0.01, dem_deriv=1, max_neighbours=0, icpwp=0, pwp0rel=0.0):
     """Params from a {k: value} map of the reference's const(k) (1-based)."""
     p = Params()
     for k, val in (const or {}).items():
@@ -151,6 +153,7 @@ def make_params(const=None, *, pa_sph=2, nnps=2, sle=1, skf=1, summation_density
     p.pa_sph, p.nnps, p.sle, p.skf = pa_sph, nnps, sle, skf
     p.summation_density, p.average_velocity, p.nor_density = summation_density, average_velocity, nor_density
     p.ic_adapt, p.h_inf, p.dt, p.dem_deriv, p.max_neighbours = ic_adapt, h_inf, dt, dem_deriv, max_neighbours
+    p.icpwp, p.pwp0rel = icpwp, pwp0rel
     return p
 
 
@@ -221,6 +224,16 @@ class Sim:
         _check(lib().gfsph_download(self.h, _fp(out["x"]), _fp(out["v"]), _fp(out["rho"]), _fp(out["mass"]),
                                     _fp(out["hsml"]), _ip(out["flag"])), "gfsph_download")
         return out
+
+    def pwp(self):
+        """Uaux(1,:), the basal pore-water pressure (icpwp = 3)."""
+        out = np.empty(self.n, np.float32)
+        _check(lib().gfsph_get_pwp(self.h, _fp(out)), "gfsph_get_pwp")
+        return out
+
+    def set_pwp(self, pwp):
+        a = np.ascontiguousarray(pwp, dtype=np.float32)
+        _check(lib().gfsph_set_pwp(self.h, _fp(a)), "gfsph_set_pwp")
 
     def step(self, nsteps, t_end=1e300):
         t = C.c_double()

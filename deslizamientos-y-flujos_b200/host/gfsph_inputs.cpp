@@ -278,6 +278,10 @@ SwDat read_dat(const std::string& path) {
     }
     r.label();
     d.icpwp = r.read_int();
+    if (d.icpwp == 3) {  // Input_SW SPH_SW_2019.f90:1829-1835
+        r.label();
+        d.pwp0rel = r.read_real();
+    }
     return d;
 }
 

@@ -43,6 +43,7 @@ struct SwDat {
     float cst[110] = {};        // const(1..110)
     int ic_k0 = 0;
     int icpwp = 0;
+    float pwp0rel = 0.f;        // icpwp = 3
 };
 
 struct Particles {

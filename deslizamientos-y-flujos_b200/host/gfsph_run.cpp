@@ -102,20 +102,19 @@ int main(int argc, char** argv) {
             std::printf("{\"title\": \"%s\", \"dt\": %g, \"time_end\": %g, \"plot_step\": %d, \"dt_sph\": %g, "
                         "\"ic_adapt\": %d, \"nx\": %d, \"ny\": %d, \"xmin\": %.6f, \"ymin\": %.6f, \"dx\": %g, \"dy\": %g, "
                         "\"ictop\": %d, \"fdiff\": %d, \"n\": %d, \"dropped\": %d, \"volume\": %.6f, \"hsml\": %g, "
-                        "\"pa_sph\": %d, \"nnps\": %d, \"sle\": %d, \"skf\": %d, \"nfric\": %d, \"icpwp\": %d, \"h_inf\": %g, "
+                        "\"pa_sph\": %d, \"nnps\": %d, \"sle\": %d, \"skf\": %d, \"nfric\": %d, \"icpwp\": %d, \"pwp0rel\": %g, \"h_inf\": %g, "
                         "\"const\": [",
                         "", m.dt, m.time_end, m.plot_step, m.dt_sph, m.ic_adapt, t.nx, t.ny, (double)t.xmin,
                         (double)t.ymin, t.dx, t.dy, t.ictop, t.fdiff ? 1 : 0, n, dropped, P.total_volume,
-                        n ? hsml[0] : 0.f, d.pa_sph, d.nnps, d.sle, d.skf, (int)(d.cst[4] + 0.01f), d.icpwp, d.h_inf);
+                        n ? hsml[0] : 0.f, d.pa_sph, d.nnps, d.sle, d.skf, (int)(d.cst[4] + 0.01f), d.icpwp, d.pwp0rel, d.h_inf);
             for (int k = 0; k < 60; k++) std::printf("%s%g", k ? ", " : "", d.cst[k]);
             double zsum = 0.0;
             for (float z : t.z) zsum += z;
             std::printf("], \"z_mean\": %.6f}\n", zsum / (double)t.z.size());
             return 0;
         }
-        if (d.icpwp != 0)
-            std::fprintf(stderr, "warning: icpwp = %d (pore-water pressure) is not implemented; running with icpwp = 0\n",
-                         d.icpwp);
+        if (d.icpwp != 0 && d.icpwp != 3)
+            throw std::runtime_error("icpwp = " + std::to_string(d.icpwp) + " is not implemented (0 and 3 are)");
         gfsph_params p;
         std::memset(&p, 0, sizeof(p));
         for (int k = 0; k < GFSPH_NCONST; k++) p.cst[k] = d.cst[k];
@@ -123,6 +122,8 @@ int main(int argc, char** argv) {
         p.summation_density = d.sum_den ? 1 : 0; p.average_velocity = d.av_vel ? 1 : 0;
         p.nor_density = d.nor_dens ? 1 : 0; p.ic_adapt = m.ic_adapt; p.h_inf = d.h_inf; p.dt = m.dt_sph;
         p.dem_deriv = t.fdiff ? 1 : 0;
+        p.icpwp = d.icpwp;
+        p.pwp0rel = d.pwp0rel;
         gfsph_dem dem;
         std::memset(&dem, 0, sizeof(dem));
         dem.nx = t.nx; dem.ny = t.ny; dem.xmin = t.xmin; dem.ymin = t.ymin; dem.dx = t.dx; dem.dy = t.dy;

@@ -234,7 +234,7 @@ def write_reference_inputs(w, directory, name):
     Fortran program (or gfsph_run) can read it: <name>.MASTER.dat,
     <name>.dat, <name>.top (ictop = 100: a grid file with finite-difference
     slopes) and <name>.pts (the particles as source points on their
-    lattice)."""
+    lattice).  w.options may carry icpwp (0 or 3) and pwp0rel."""
     import os
     os.makedirs(directory, exist_ok=True)
     o = w.options
@@ -274,7 +274,11 @@ def write_reference_inputs(w, directory, name):
         nfric = int(c[4] + 0.01)
         if 5 <= nfric <= 10:
             f.write("K0 activated?\n  0\n")
-        f.write("icpwp\n  0\ncoarse mesh saving utility?\n  0\ncontrol points?\n  0\n")
+        icpwp = int(o.get("icpwp", 0))
+        f.write("icpwp\n  %d\n" % icpwp)
+        if icpwp == 3:
+            f.write(" pwp0rel\n  %.9g\n" % float(o.get("pwp0rel", 0.0)))
+        f.write("coarse mesh saving utility?\n  0\ncontrol points?\n  0\n")
         f.write("GID filter\n  1 1 1 1 0 1 0 0 0 1 0 0\nT_change_to_W\n  1.e+12\n")
     ny, nx = w.z.shape
     with open(os.path.join(directory, name + ".top"), "w") as f:

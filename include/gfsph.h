@@ -72,7 +72,9 @@ typedef struct gfsph_params {
     float dt;              /* initial dt_sph */
     int dem_deriv;         /* slopes when not supplied: 0 FEM projection (Get_Topol), 1 finite differences */
     int max_neighbours;    /* initial neighbour-table capacity per particle; 0 = 96 (grows on demand) */
-    int reserved[8];
+    int icpwp;             /* 0 none, 3 basal pore-water pressure with one point (Get_Pwp_SW, nUaux = 1) */
+    float pwp0rel;         /* icpwp = 3: initial Uaux = pwp0rel * rho * const(14) (Input_SW SPH_SW_2019.f90:1829-1852) */
+    int reserved[6];
 } gfsph_params;
 
 /*
@@ -123,6 +125,14 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
  * pointer may be NULL to skip that array. */
 int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass, float* hsml,
                    int* out_flag);
+
+/* Basal pore-water pressure Uaux(1,:) (icpwp = 3), n values in the original
+ * particle order: gfsph_upload starts it as Input_SW does
+ * (pwp0rel * rho * const(14), SPH_SW_2019.f90:1829-1852); these replace or
+ * read it (the reference's Uaux global, updated by Get_Pwp_SW
+ * SPH_SW_2019.f90:11176-11371 at the end of every step). */
+int gfsph_set_pwp(gfsph_handle* h, const float* pwp);
+int gfsph_get_pwp(gfsph_handle* h, float* pwp);
 
 /* Replaces up to nsteps iterations of the DTGT loop body
  * (SPH_FEM_Driver_2019.f90:1580-1617): adaptive_dt_sph, time_integration_sph

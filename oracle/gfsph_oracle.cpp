@@ -11,7 +11,8 @@
  * step (grid_find_NEW_tools / _tools3), then RK45 re-evaluates summation
  * density, IntForces_SW and ExtForces_SW(0) in each of its four stages,
  * recomputes the density after the final update, applies ExtForces_SW(1)
- * erosion, h_upgrade and av_vel.  Every floating-point expression keeps the
+ * erosion, the basal pore-water pressure of Get_Pwp_SW (icpwp = 3),
+ * h_upgrade and av_vel.  Every floating-point expression keeps the
  * Fortran left-to-right evaluation order, without FMA contraction
  * (build with -ffp-contract=off).
  *
@@ -121,6 +122,12 @@ struct Oracle {
     /* particles */
     int n;
     std::vector<R> x, v, rho, mass, hsml, x0, v0, p;
+    std::vector<R> uaux, rho0; /* basal pore-water pressure Uaux(1,:) (icpwp = 3) and rho at the RK45 start */
+    /* pore-water-pressure and density factors: DFs_FSs_dens_and_pwp_factors
+     * (ExtForces_SW, SPH_SW_2019.f90:8959-9109) for the friction, and
+     * mini_DFs_dens_and_pwp_factors (Get_Pwp_SW, :11502-11632) for the update */
+    int icpwp;
+    R fact_dens, fact_pwp_max, fact_pwp_min, fpwp_max, fpwp_min, fpwp_min_g, bfact, alphas, alphas2;
     std::vector<R> ex, in, Dx, Dv, av;
     std::vector<int> flag;
     /* pairs */
@@ -347,10 +354,12 @@ struct Oracle {
 
     struct Local { /* ExtForces_SW locals shared with its contained routines */
         R h, hu, hv, hinv, vmod, hvmod, hvmodinv, frictx, fricty, totfrict, cf5, gravx, gravy, gravz;
+        R hrho; /* rho(ipoin) as ExtForces_SW reads it, before the comp clamp */
     };
 
     /* the start of the ExtForces_SW particle loop, SPH_SW_2019.f90:8564-8596 */
     void ext_locals(int i, R hdepth, Local& L) {
+        L.hrho = hdepth;
         L.h = hdepth;
         L.hu = L.h * v[2 * i];
         L.hv = L.h * v[2 * i + 1];
@@ -415,7 +424,17 @@ struct Oracle {
                 }
             }
             R tanfi = cst[9];
-            R gtanfi = ((L.gravz + cv2byr) * tanfi) * (R)1; /* fact_dens = 1 */
+            if (icpwp == 3) { /* :9670-9688: pwp = Uaux(1,ipoin), filtered, then tanfi*factpw */
+                R pwp = uaux[i];
+                R hhh = L.hrho;
+                if (pwp > fpwp_max * hhh) pwp = fpwp_max * hhh;
+                if (pwp < fpwp_min * hhh) pwp = fpwp_min * hhh;
+                R factpw = (R)1 - pwp * L.hinv;
+                if (factpw < fact_pwp_min) factpw = fact_pwp_min;
+                if (factpw > fact_pwp_max) factpw = fact_pwp_max;
+                tanfi = tanfi * factpw;
+            }
+            R gtanfi = ((L.gravz + cv2byr) * tanfi) * fact_dens; /* :9706 */
             if (gtanfi < 0) gtanfi = 0;
             L.cf5 = gtanfi;
             L.frictx = ((L.cf5 * L.hu) * L.hvmodinv) * L.h;
@@ -545,6 +564,31 @@ struct Oracle {
         }
     }
 
+    /* Get_Pwp_SW with one pwp point (icpwp = 3), SPH_SW_2019.f90:11176-11371
+     * (no basal flux, no DF terms): exponential dissipation of Uaux towards
+     * the depth change of the step, Drho_RK = rho - rho0 (RK45 :918-919). */
+    void get_pwp() {
+        if (icpwp != 3) return;
+        R comp = cst[15];
+        for (int i = 0; i < n; i++) {
+            if (flag[i]) { uaux[i] = 0; continue; }
+            R hh = rho[i];
+            R dhh = rho[i] - rho0[i];
+            R hinv;
+            if (hh < comp) {
+                hh = comp;
+                hinv = (R)1 / comp;
+            } else {
+                hinv = (R)1 / hh;
+            }
+            R betaw = ((bfact * hinv) * hinv) / alphas2;
+            R e = (R)std::exp((double)(-(betaw * dt))); /* exp rounded once to R */
+            uaux[i] = uaux[i] * e + ((dhh / dt) * ((R)1 - e)) / betaw;
+            if (uaux[i] > hh) uaux[i] = hh;
+            if (uaux[i] < (hh * alphas) * fpwp_min_g) uaux[i] = (hh * alphas) * fpwp_min_g;
+        }
+    }
+
     /* h_upgrade sle = 1, SPH_MAIN_2019.f90:2925-2931 */
     void h_upgrade() {
         if (P->sle != 1) return;
@@ -587,6 +631,7 @@ struct Oracle {
         std::fill(Dv.begin(), Dv.end(), (R)0);
         grid_find();
         x0 = x; v0 = v;
+        rho0 = rho;
         const R f1[4] = {0, lit<R>(0.5), lit<R>(0.5), 1};
         const R f2[4] = {1, 2, 2, 1};
         for (int s = 0; s < 4; s++) {
@@ -621,6 +666,7 @@ struct Oracle {
         sum_density();
         check_out_domain();
         ext_forces1();
+        get_pwp();
         h_upgrade();
         if (P->average_velocity) av_vel();
     }
@@ -652,7 +698,55 @@ struct Oracle {
         for (size_t k = 0; k < topol.size(); k++) topol[k] = (R)topol_in[k];
         auxv1.assign(npoig, (A)0);
         auxv2.assign(npoig, (A)0);
+        return pwp_factors();
+    }
+
+    /* the factors of DFs_FSs_dens_and_pwp_factors (:8959-9060) and
+     * mini_DFs_dens_and_pwp_factors (:11502-11580), ic_hrelSat = 0 */
+    int pwp_factors() {
+        icpwp = P->icpwp;
+        int ic_fct_dens = (int)(cst[20] + lit<R>(0.1));
+        R dens = cst[2], denss = cst[17], densw = cst[18], sr = cst[19];
+        alphas = cst[14];
+        fact_pwp_max = 1; fact_pwp_min = 0; fpwp_max = 1; fpwp_min = 0; fpwp_min_g = 0;
+        fact_dens = 1;
+        if (ic_fct_dens == 1) {
+            if (denss < lit<R>(1.e-3) || densw < lit<R>(1.e-3)) return GFSPH_ERR_ARG;
+            R porosity = (denss - dens) / (denss - densw);
+            R dens2 = ((R)1 - porosity) * denss;
+            R dens1 = ((R)1 - porosity) * denss + porosity * densw;
+            R dens_bar = ((R)1 - alphas) * dens2 + alphas * dens1;
+            R dens_bar_eff = dens_bar - densw * alphas;
+            fact_dens = dens_bar_eff / dens_bar;
+            if (icpwp > 0) {
+                fact_pwp_max = (R)1 + (alphas * densw) / dens_bar_eff;
+                fact_pwp_min = 0;
+                fpwp_max = 1;
+                fpwp_min = -(alphas * densw) / dens_bar_eff;
+                /* Get_Pwp_SW's own factors keep the unsaturated-layer water (Sr) */
+                R g2 = ((R)1 - porosity) * denss + (porosity * densw) * sr;
+                R gbar = ((R)1 - alphas) * g2 + alphas * dens1;
+                R geff = gbar - densw * alphas;
+                fpwp_min_g = -(alphas * densw) / geff;
+            }
+        } else if (ic_fct_dens != 0) {
+            return GFSPH_ERR_UNSUPPORTED;
+        }
+        if (icpwp != 0 && icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
+        if ((ic_fct_dens != 0 || icpwp != 0) && (int)(cst[34] + lit<R>(0.01)) != 0) return GFSPH_ERR_UNSUPPORTED;
+        if (icpwp == 3 && cst[26] > 0) return GFSPH_ERR_UNSUPPORTED; /* drag laws rescale Bfact */
+        if (ic_fct_dens == 1 && icpwp != 0 && !(alphas > lit<R>(0.01))) return GFSPH_ERR_UNSUPPORTED;
+        bfact = cst[13];
+        alphas2 = cst[14] * cst[14];
         return 0;
+    }
+
+    /* Uaux(1,:) = pwp0rel * rho * alphas at input (Input_SW, SPH_SW_2019.f90:1829-1852) */
+    void init_pwp(const double* pwp_in) {
+        uaux.assign(n, (R)0);
+        if (icpwp != 3) return;
+        for (int i = 0; i < n; i++)
+            uaux[i] = pwp_in ? (R)pwp_in[i] : (R)P->pwp0rel * (rho[i] * cst[14]);
     }
 };
 
@@ -661,6 +755,7 @@ struct OracleBase {
     virtual int advance(int nsteps, double t_end) = 0;
     virtual void get(double* x, double* v, double* rho, double* mass, double* hsml, int* flag, double* dt,
                      double* t, double* topol) = 0;
+    virtual void get_pwp(double* pwp) = 0;
 };
 
 template <class R, class A>
@@ -694,12 +789,16 @@ struct OracleObj : OracleBase {
         if (dt) *dt = (double)o.dt;
         if (t) *t = o.time;
     }
+    void get_pwp(double* pwp) override {
+        for (int k = 0; k < o.n; k++) pwp[k] = (double)o.uaux[k];
+    }
 };
 
 template <class R, class A>
 OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
                      const double* topol, int n, const double* x, const double* v, const double* rho,
-                     const double* mass, const double* hsml, const int* flag, double dt, double t, int* status) {
+                     const double* mass, const double* hsml, const int* flag, const double* pwp, double dt, double t,
+                     int* status) {
     OracleObj<R, A>* ob = new OracleObj<R, A>();
     ob->params = *p;
     Oracle<R, A>& o = ob->o;
@@ -717,6 +816,7 @@ OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double 
     o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
     o.dt = (R)dt;
     o.time = t;
+    o.init_pwp(pwp);
     *status = 0;
     return ob;
 }
@@ -724,7 +824,7 @@ OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double 
 template <class R, class A>
 int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
              double* topol, int n, double* x, double* v, double* rho, double* mass, double* hsml, int* flag,
-             int nsteps, double* dt, double* t, double t_end, int* steps_done) {
+             double* pwp, int pwp_init, int nsteps, double* dt, double* t, double t_end, int* steps_done) {
     Oracle<R, A> o;
     int st = o.setup(p, nx, ny, xmin, ymin, dx, dy, topol);
     if (st) return st;
@@ -740,6 +840,7 @@ int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, do
     o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
     o.dt = (R)*dt;
     o.time = *t;
+    o.init_pwp(pwp_init ? nullptr : pwp);
     int done = 0;
     for (int s = 0; s < nsteps; s++) {
         if (o.time >= t_end) break;
@@ -751,6 +852,8 @@ int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, do
         rho[k] = (double)o.rho[k]; mass[k] = (double)o.mass[k]; hsml[k] = (double)o.hsml[k]; flag[k] = o.flag[k];
     }
     for (size_t k = 0; k < o.topol.size(); k++) topol[k] = (double)o.topol[k];
+    if (pwp)
+        for (int k = 0; k < n; k++) pwp[k] = (double)o.uaux[k];
     *dt = (double)o.dt;
     *t = o.time;
     if (steps_done) *steps_done = done;
@@ -1041,17 +1144,19 @@ int oracle_solvegc2(int mode, int npoin, int nelem, int nnode, int ndofn, const 
 }
 
 /* Runs nsteps steps of the reference path on the given state (in/out).
- * topol: (16, nx*ny) in/out (erosion lowers Z).  mode: 0, 1, 2 as above. */
+ * topol: (16, nx*ny) in/out (erosion lowers Z).  mode: 0, 1, 2 as above.
+ * pwp: Uaux(1,:) in/out when icpwp = 3 (may be NULL); pwp_init = 1 starts
+ * it from pwp0rel*rho*const(14) as Input_SW does instead of reading it. */
 int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
                double* topol, int n, double* x, double* v, double* rho, double* mass, double* hsml, int* flag,
-               int nsteps, double* dt, double* t, double t_end, int* steps_done) {
+               double* pwp, int pwp_init, int nsteps, double* dt, double* t, double t_end, int* steps_done) {
     if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || !dt || !t || n < 0 || nx < 2 || ny < 2)
         return GFSPH_ERR_ARG;
     if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
     switch (mode) {
-    case 0: return run_mode<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, t_end, steps_done);
-    case 1: return run_mode<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, t_end, steps_done);
-    case 2: return run_mode<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, t_end, steps_done);
+    case 0: return run_mode<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
+    case 1: return run_mode<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
+    case 2: return run_mode<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
     default: return GFSPH_ERR_ARG;
     }
 }
@@ -1059,14 +1164,15 @@ int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, dou
 /* Persistent oracle run: create on a state, advance, read back, free. */
 void* oracle_new(int mode, const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
                  const double* topol, int n, const double* x, const double* v, const double* rho,
-                 const double* mass, const double* hsml, const int* flag, double dt, double t, int* status) {
+                 const double* mass, const double* hsml, const int* flag, const double* pwp, double dt, double t,
+                 int* status) {
     *status = GFSPH_ERR_ARG;
     if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || n < 0 || nx < 2 || ny < 2) return nullptr;
     if (p->summation_density != 1 || p->nor_density != 0) { *status = GFSPH_ERR_UNSUPPORTED; return nullptr; }
     switch (mode) {
-    case 0: return make_obj<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, dt, t, status);
-    case 1: return make_obj<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, dt, t, status);
-    case 2: return make_obj<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, dt, t, status);
+    case 0: return make_obj<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);
+    case 1: return make_obj<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);
+    case 2: return make_obj<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);
     default: return nullptr;
     }
 }
@@ -1079,6 +1185,12 @@ int oracle_get(void* h, double* x, double* v, double* rho, double* mass, double*
                double* t, double* topol) {
     if (!h) return GFSPH_ERR_ARG;
     static_cast<OracleBase*>(h)->get(x, v, rho, mass, hsml, flag, dt, t, topol);
+    return 0;
+}
+
+int oracle_get_pwp(void* h, double* pwp) {
+    if (!h || !pwp) return GFSPH_ERR_ARG;
+    static_cast<OracleBase*>(h)->get_pwp(pwp);
     return 0;
 }
 

@@ -41,8 +41,8 @@ def lib():
         L = C.CDLL(LIB)
         L.oracle_run.restype = C.c_int
         L.oracle_run.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_int, _DP, _DP,
-                                 C.c_double, _IP]
+                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, _DP, C.c_int, C.c_int, _DP,
+                                 _DP, C.c_double, _IP]
         L.oracle_pairs.restype = C.c_int
         L.oracle_pairs.argtypes = [C.c_int, C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, _IP, C.c_int, _IP, _IP, _DP,
                                    _DP]
@@ -58,12 +58,14 @@ def lib():
                                            C.c_int, _DP, _DP, _DP, _IP, _DP, _IP]
         L.oracle_new.restype = C.c_void_p
         L.oracle_new.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_double, C.c_double,
-                                 _IP]
+                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, _DP, C.c_double,
+                                 C.c_double, _IP]
         L.oracle_advance.restype = C.c_int
         L.oracle_advance.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.oracle_get.restype = C.c_int
         L.oracle_get.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP, _DP, _IP, _DP, _DP, _DP]
+        L.oracle_get_pwp.restype = C.c_int
+        L.oracle_get_pwp.argtypes = [C.c_void_p, _DP]
         L.oracle_free.restype = None
         L.oracle_free.argtypes = [C.c_void_p]
         L.oracle_solvegc2.restype = C.c_int
@@ -109,16 +111,18 @@ def initial_topol(z, dx, dy, const, deriv=1, mode=MODE_FP32):
 class State:
     """Particle state and DEM of an oracle run (float64 arrays)."""
 
-    def __init__(self, x, v, rho, mass, hsml, topol, flag=None, dt=0.01, t=0.0):
+    def __init__(self, x, v, rho, mass, hsml, topol, flag=None, dt=0.01, t=0.0, pwp=None):
+        """pwp: Uaux(1,:) for icpwp = 3; None starts it as Input_SW does."""
         self.x, self.v = _d(x).copy(), _d(v).copy()
         self.rho, self.mass, self.hsml = _d(rho).copy(), _d(mass).copy(), _d(hsml).copy()
         n = self.x.shape[0]
         self.flag = np.zeros(n, np.int32) if flag is None else np.ascontiguousarray(flag, np.int32).copy()
         self.topol = _d(topol).copy()
         self.dt, self.t = float(dt), float(t)
+        self.pwp = None if pwp is None else _d(pwp).copy()
 
     def copy(self):
-        s = State(self.x, self.v, self.rho, self.mass, self.hsml, self.topol, self.flag, self.dt, self.t)
+        s = State(self.x, self.v, self.rho, self.mass, self.hsml, self.topol, self.flag, self.dt, self.t, self.pwp)
         return s
 
 
@@ -127,9 +131,14 @@ def run(mode, params, nx, ny, dx, dy, state, nsteps, xmin=0.0, ymin=0.0, t_end=1
     dt = C.c_double(state.dt)
     t = C.c_double(state.t)
     done = C.c_int(0)
+    n = state.x.shape[0]
+    init = 0
+    if params.icpwp == 3 and state.pwp is None:
+        state.pwp, init = np.zeros(n), 1
     st = lib().oracle_run(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol),
-                          state.x.shape[0], _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass),
-                          _dp(state.hsml), _ip(state.flag), nsteps, C.byref(dt), C.byref(t), t_end, C.byref(done))
+                          n, _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass),
+                          _dp(state.hsml), _ip(state.flag), _dp(state.pwp), init,
+                          nsteps, C.byref(dt), C.byref(t), t_end, C.byref(done))
     if st:
         raise RuntimeError(f"oracle_run: {st}")
     state.dt, state.t = dt.value, t.value
@@ -201,7 +210,7 @@ class Run:
         stv = C.c_int(0)
         self.h = lib().oracle_new(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), self.n,
                                   _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.hsml),
-                                  _ip(state.flag), state.dt, state.t, C.byref(stv))
+                                  _ip(state.flag), _dp(state.pwp), state.dt, state.t, C.byref(stv))
         if not self.h:
             raise RuntimeError(f"oracle_new: {stv.value}")
 
@@ -217,7 +226,11 @@ class Run:
         topol = np.zeros(self.topol_shape) if with_topol else None
         lib().oracle_get(self.h, _dp(x), _dp(v), _dp(rho), _dp(mass), _dp(hsml), _ip(flag), C.byref(dt), C.byref(t),
                          _dp(topol))
-        return State(x, v, rho, mass, hsml, topol if with_topol else np.zeros(1), flag, dt.value, t.value)
+        pwp = None
+        if self.params.icpwp == 3:
+            pwp = np.zeros(n)
+            lib().oracle_get_pwp(self.h, _dp(pwp))
+        return State(x, v, rho, mass, hsml, topol if with_topol else np.zeros(1), flag, dt.value, t.value, pwp)
 
     def close(self):
         if self.h:

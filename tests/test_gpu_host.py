@@ -39,3 +39,24 @@ def test_gfsph_run_on_written_inputs(gfsph_lib, tmp_path):
     assert depth.shape == (400, 200) and np.isfinite(depth).all() and depth.max() > 1.0
     _, hmax = read_asc(os.path.join(d, "plane.max_depth.asc"))
     assert hmax.max() >= log[:, 4].max() - 1e-4
+
+
+def test_gfsph_run_with_basal_pore_pressure(gfsph_lib, tmp_path):
+    """icpwp = 3 read from the .dat (with its pwp0rel line) reaches the step:
+    a liquefied release (pwp0rel = 1, slow dissipation) runs out faster than
+    the same release without pore pressure."""
+    speeds = {}
+    for icpwp in (0, 3):
+        w = workloads.inclined_plane()
+        w.const = {**w.const, 9: 0.55, 13: 0.001, 14: 1.0}
+        w.options = {**w.options, "icpwp": icpwp, "pwp0rel": 1.0}
+        d = os.path.join(str(tmp_path), "p%d" % icpwp)
+        workloads.write_reference_inputs(w, d, "plane")
+        meta = json.loads(subprocess.run([RUN, "plane", "--dir", d, "--parse-only"], capture_output=True,
+                                         text=True).stdout)
+        assert meta["icpwp"] == icpwp and (icpwp == 0 or meta["pwp0rel"] == 1.0)
+        out = subprocess.run([RUN, "plane", "--dir", d, "--out", d, "--max-steps", "200"], capture_output=True,
+                             text=True)
+        assert out.returncode == 0, out.stderr
+        speeds[icpwp] = np.loadtxt(os.path.join(d, "plane.gfsph.log"))[-1, 5]
+    assert speeds[3] > 1.2 * speeds[0]

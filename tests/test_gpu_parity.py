@@ -366,3 +366,35 @@ def test_far_apart_releases_on_a_large_dem(gfsph_lib, oracle_mod):
     for key, r in (("x", st.x), ("v", st.v), ("rho", st.rho), ("hsml", st.hsml)):
         assert max_rel(g[key], r, floor=1e-3) <= 1e-6, key
     sim.close()
+
+
+@pytest.mark.parametrize("fct", [0, 1])
+def test_pore_water_pressure_matches_oracle(gfsph_lib, oracle_mod, fct):
+    """icpwp = 3 (Get_Pwp_SW with one point): Uaux starts at pwp0rel * h,
+    lowers the basal friction by 1 - pwp/h, and relaxes towards the depth
+    change of every step.  ic_fct_dens = 1 adds the buoyancy factor of tanfi
+    and the negative pwp bounds."""
+    w = small_channel()
+    extra = {13: 0.02, 14: 1.0}
+    if fct:
+        extra.update({17: 2650.0, 18: 1000.0, 19: 0.5, 20: 1})
+    w.const = {**w.const, **extra}
+    sim, st, p = setup_pair(w, oracle_mod, icpwp=3, pwp0rel=0.8)
+    assert np.array_equal(sim.pwp(), (np.float32(0.8) * (w.rho * np.float32(1.0))).astype(np.float32))
+    ny, nx = w.z.shape
+    for nsteps in (1, 29):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        tol = 1e-6 if nsteps == 1 else 1e-5
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
+            assert rel_l2(g[key], ref) <= tol, (key, nsteps)
+        assert rel_l2(sim.pwp(), st.pwp) <= tol
+    # the friction really is lowered: without pore pressure the flow is slower
+    sim0, st0, _ = setup_pair(w, oracle_mod)
+    sim0.step(30)
+    v0 = np.hypot(*sim0.download()["v"].T).mean()
+    assert np.hypot(*g["v"].T).mean() > v0
+    sim.close()
+    sim0.close()

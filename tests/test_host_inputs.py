@@ -54,3 +54,11 @@ def test_reader_reports_unsupported_options(gfsph_lib, tmp_path):
     open(top, "w").write(txt)
     out = subprocess.run([RUN, "bad", "--dir", str(tmp_path), "--parse-only"], capture_output=True, text=True)
     assert out.returncode == 2 and "ictop 3" in out.stderr
+
+
+def test_written_inputs_with_pore_pressure_parse(gfsph_lib, tmp_path):
+    w = workloads.inclined_plane()
+    w.options = {**w.options, "icpwp": 3, "pwp0rel": 0.75}
+    workloads.write_reference_inputs(w, str(tmp_path), "pw")
+    meta = parse("pw", str(tmp_path))
+    assert meta["icpwp"] == 3 and abs(meta["pwp0rel"] - 0.75) < 1e-7

@@ -4,8 +4,9 @@ The reference ships no tests, fixtures or golden outputs, so the oracle is
 pinned by answers that follow from the mathematics the reference implements:
 kernel normalisation and gradient consistency, exact slopes of a plane,
 neighbour sets against a brute-force search, zero interior force on a still
-layer, the infinite-slope Voellmy and Bingham terminal velocities, and volume
-conservation without erosion.
+layer, the infinite-slope Voellmy and Bingham terminal velocities, volume
+conservation without erosion, and the basal pore-water pressure of icpwp = 3
+(exponential dissipation, liquefied sliding).
 """
 import math
 
@@ -121,15 +122,15 @@ def test_still_layer_interior_force_is_zero(oracle_mod):
     assert edge > 1e-3  # the free edge is pushed outwards
 
 
-def single_particle_run(oracle_mod, const, tan_theta, steps, dt, sle=0, mode=2):
+def single_particle_run(oracle_mod, const, tan_theta, steps, dt, sle=0, mode=2, rho=1.0, **kw):
     nx, ny, d = 20, 1200, 5.0
     yy = np.arange(ny)[:, None] * d * np.ones((1, nx))
     z = (ny * d - yy) * tan_theta
-    p = params(const, sle=sle, dt=dt, ic_adapt=0, average_velocity=0)
+    p = params(const, sle=sle, dt=dt, ic_adapt=0, average_velocity=0, **kw)
     topol = oracle_mod.initial_topol(z, d, d, {}, deriv=1, mode=mode)
     hs = 2.0
     m = 4.0
-    st = oracle_mod.State(np.array([[50.0, 100.0]]), np.zeros((1, 2)), np.array([1.0]), np.array([m]),
+    st = oracle_mod.State(np.array([[50.0, 100.0]]), np.zeros((1, 2)), np.array([rho]), np.array([m]),
                           np.array([hs]), topol, dt=dt)
     oracle_mod.run(mode, p, nx, ny, d, d, st, steps)
     w0 = 15.0 / (7.0 * math.pi * hs * hs) * (2.0 / 3.0)
@@ -238,3 +239,44 @@ def test_solvegc2_restatement_solves_the_p1_mass_system(oracle_mod):
     assert np.allclose(x2[free], ref, rtol=1e-9, atol=1e-9) and np.all(x2[bnd] == 2.5)
     x3, _, _, it3 = oracle_mod.solvegc2(0, intmat, g, b, tol=1e-10)
     assert np.allclose(x3, x, rtol=1e-4, atol=1e-4)
+
+
+def lone_particle_depth(oracle_mod):
+    """The summation depth W(0, 2) * 4 of the lone particle of single_particle_run."""
+    res = oracle_mod.pairs(oracle_mod.MODE_FP64, params(), np.array([[0.0, 0.0]]), np.array([2.0]),
+                           mass=np.array([4.0]), rho=np.array([1.0]), want_sets=False, want_rho=True)
+    return float(res["rho"][0])
+
+
+def test_pwp_liquefied_layer_slides_without_friction(oracle_mod):
+    """icpwp = 3 with pwp0rel = 1 and no dissipation: Uaux = h, the friction
+    factor 1 - pwp/h is 0, and a particle on a slope steeper than nothing
+    accelerates at g tan(theta) although tan(phi) = 0.6 > tan(theta) = 0.5
+    holds it still without pore pressure."""
+    tan_t, mu, dt, steps = 0.5, 0.6, 0.02, 100
+    st0, _ = single_particle_run(oracle_mod, {3: 0.0, 9: mu}, tan_t, steps, dt)
+    assert np.hypot(*st0.v[0]) < 1e-6
+    h = lone_particle_depth(oracle_mod)
+    st, _ = single_particle_run(oracle_mod, {3: 0.0, 9: mu, 13: 1e-12, 14: 1.0}, tan_t, steps, dt, rho=h,
+                                icpwp=3, pwp0rel=1.0)
+    v = np.hypot(*st.v[0])
+    assert abs(v - 9.8 * tan_t * steps * dt) < 1e-6 * v
+    assert abs(st.pwp[0] - h) < 1e-6 * h
+
+
+def test_pwp_dissipates_exponentially(oracle_mod):
+    """A lone particle keeps its depth (dh = 0), so Get_Pwp_SW reduces to
+    Uaux(t) = h exp(-beta t), beta = Bfact / (h alphas)^2, and the velocity
+    gains g (tan(theta) - tan(phi) (1 - Uaux/h)) dt per step."""
+    tan_t, mu, dt, steps, bfact = 0.5, 0.6, 0.02, 100, 0.05
+    h = lone_particle_depth(oracle_mod)
+    st, _ = single_particle_run(oracle_mod, {3: 0.0, 9: mu, 13: bfact, 14: 1.0}, tan_t, steps, dt, rho=h,
+                                icpwp=3, pwp0rel=1.0)
+    t = steps * dt
+    beta = bfact / (h * h)
+    assert abs(st.pwp[0] - h * math.exp(-beta * t)) < 1e-6 * h
+    # the friction factor of step k uses Uaux from the start of that step
+    q = math.exp(-beta * dt)
+    v_exact = 9.8 * ((tan_t - mu) * t + mu * dt * (1.0 - q ** steps) / (1.0 - q))
+    v = np.hypot(*st.v[0])
+    assert abs(v - v_exact) < 1e-5 * v_exact, (v, v_exact)
