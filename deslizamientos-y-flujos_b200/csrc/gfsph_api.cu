@@ -20,6 +20,7 @@ enum KernelId {
     K_PREP, K_BOUNDS, K_GRID, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_TOP, K_BSCAN_ADD,
+    K_DENSITY_SPARSE,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
@@ -28,7 +29,7 @@ const char* kKernelNames[K_COUNT] = {
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)", "k_scan_top(blocks)",
-    "k_scan_add(blocks)", "step_batches"};
+    "k_scan_add(blocks)", "k_density(sparse)", "step_batches"};
 
 constexpr int kThreads = 128;
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
@@ -263,19 +264,21 @@ int enqueue_search(gfsph_handle* h, int advance) {
     const int* ncel = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, ncells));
     if (!advance) { launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++; }
     launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
-    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_blocks); }); nk++;
+    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_blocks, h->cap_cells, kMaxCells); }); nk++;
     launch(h, K_MARK, [&] { k_mark<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark); }); nk++;
     launch(h, K_BSCAN_TILES, [&] {
-        k_scan_tiles<<<nbscan, kScanThreads, 0, st>>>(h->bmark, h->bstart, h->tile_sum, nblk, S);
+        k_scan_tiles<<<nbscan, kScanThreads, 0, st>>>(h->bmark, h->bstart, h->tile_sum, nblk, S, 1);
     }); nk++;
-    launch(h, K_BSCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, nblk, S); }); nk++;
-    launch(h, K_BSCAN_ADD, [&] { k_scan_add<<<nbscan, kScanThreads, 0, st>>>(h->bstart, h->tile_sum, nblk, S); }); nk++;
+    launch(h, K_BSCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, nblk, S, 1); }); nk++;
+    launch(h, K_BSCAN_ADD, [&] { k_scan_add<<<nbscan, kScanThreads, 0, st>>>(h->bstart, h->tile_sum, nblk, S, 1); }); nk++;
     launch(h, K_HIST, [&] {
         k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark, h->bstart, h->count, h->keyrank, h->cap_cells);
     }); nk++;
-    launch(h, K_SCAN_TILES, [&] { k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, ncel, S); }); nk++;
-    launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, ncel, S); }); nk++;
-    launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, ncel, S); }); nk++;
+    launch(h, K_SCAN_TILES, [&] {
+        k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, ncel, S, 0);
+    }); nk++;
+    launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, ncel, S, 0); }); nk++;
+    launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, ncel, S, 0); }); nk++;
     launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, h->bstart, S, h->perm); }); nk++;
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
     launch(h, K_REORDER, [&] {
@@ -286,7 +289,8 @@ int enqueue_search(gfsph_handle* h, int advance) {
     cudaStream_t sb = side_stream(h);
     fork(h, 0);
     launch(h, K_DENSITY_BIG, [&] { k_density_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); }); nk++;
-    launch(h, K_DENSITY, [&] { k_density<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
+    launch(h, K_DENSITY, [&] { k_density<false><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
+    launch(h, K_DENSITY_SPARSE, [&] { k_density<true><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
     join(h, 0);
     return nk;
 }
@@ -336,7 +340,7 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 15 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 16 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
 }
 
 int alloc_blocks(gfsph_handle* h, int cap) {
@@ -474,7 +478,7 @@ void pwp_factors(const gfsph_params* p, Rheo& c) {
 int validate(const gfsph_params* p) {
     int nfric = (int)(p->cst[4] + 0.01f);
     bool erosion = p->cst[20] > 1.e-9f;
-    if (!(nfric == 4 || (nfric >= 5 && nfric <= 7))) return GFSPH_ERR_UNSUPPORTED;
+    if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
     if (nfric == 4 && !(p->cst[5] >= 1.e-32f)) return GFSPH_ERR_ARG;  // SPH_SW_2019.f90:9547-9550
     if (erosion && (int)(p->cst[20] + 0.1f) != 1) return GFSPH_ERR_UNSUPPORTED;
     if (p->skf != 1 && p->skf != 4) return GFSPH_ERR_UNSUPPORTED;
@@ -565,6 +569,9 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     c.skf = p->skf; c.pa_sph = p->pa_sph; c.sle = p->sle; c.av_vel = p->average_velocity ? 1 : 0;
     c.ic_adapt = p->ic_adapt;
     pwp_factors(p, c);
+    c.muI = (c.nfric == 8 || c.nfric == 26) ? 1 : (c.nfric == 27 ? 2 : 0);
+    c.mu_a = k[2]; c.mu_r = k[5]; c.mu_b = k[6];
+    if (c.muI) c.xi = 0.f;  // const(3) is a mu(I) parameter, not xi (:9653)
 
     // DEM rows on the host, as Topo_main leaves them before the time loop
     int nx = dem->nx, ny = dem->ny;

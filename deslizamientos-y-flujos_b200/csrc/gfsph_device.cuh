@@ -156,7 +156,14 @@ struct Rheo {
     // friction, mini_DFs_dens_and_pwp_factors (:11502-11580) for the update
     int icpwp;
     float fact_dens, fact_pwp_max, fact_pwp_min, fpwp_max, fpwp_min, fpwp_min_g, bfact, alphas, alphas2;
+    // mu(I) rheologies (nfric 8 and 26: b, r, n = const(3), (6), (7); nfric 27:
+    // Mu2, r, I0 = const(3), (6), (7)), basal_friction_Ext_SW :9651-9668
+    int muI;
+    float mu_a, mu_r, mu_b;
 };
+
+// x**y for a real exponent, evaluated in FP64 and rounded once.
+__device__ __forceinline__ float powr(float x, float y) { return (float)pow((double)x, (double)y); }
 
 // Locals of ExtForces_SW shared with its contained routines.
 struct ExtLocal {
@@ -185,8 +192,8 @@ __device__ __forceinline__ void ext_locals(const Rheo& c, float hdepth, float vx
 // basal_friction_Ext_SW (:9355-9828) before its reversal filter.
 __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& d, float xx, float yy, float vx,
                                                   float vy, float pwp, ExtLocal& L) {
-    const bool frictional = (c.nfric >= 5 && c.nfric <= 7);
-    const bool v2byr = (c.nfric == 7);
+    const bool frictional = (c.nfric >= 5 && c.nfric <= 8) || c.nfric == 26 || c.nfric == 27;
+    const bool v2byr = (c.nfric == 7 || c.nfric == 8 || c.nfric == 26 || c.nfric == 27);
     float zpx, zpy, top[6];
     dem_lookup(d, xx, yy, zpx, zpy, v2byr, top);
     L.gravx = -(c.g * zpx);
@@ -227,6 +234,15 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
             }
         }
         float tanfi = c.tanfi;
+        if (c.muI == 1) {  // nfric 8, 26
+            float froude = L.vmod / sqrtf(c.g * L.h);
+            float ff = 1.f + c.mu_a * powr((froude * c.mu_r) / L.h, c.mu_b);
+            tanfi = tanfi * ff;
+        } else if (c.muI == 2) {  // nfric 27
+            float froude = L.vmod / sqrtf(c.g * L.h);
+            float inert = (froude * c.mu_r) / L.h;
+            tanfi = tanfi + (c.mu_a - tanfi) / (1.f + c.mu_b / inert);
+        }
         if (c.icpwp == 3) {  // :9670-9688: pwp = Uaux(1,ipoin), filtered, then tanfi*factpw
             float hhh = L.hrho;
             if (pwp > c.fpwp_max * hhh) pwp = c.fpwp_max * hhh;
@@ -261,7 +277,7 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
 // Reversal filter of basal_friction_Ext_SW, SPH_SW_2019.f90:9829-9895.
 __device__ __forceinline__ void reversal_filter(const Rheo& c, float dt, float vx, float vy, float acc0, float acc1,
                                                 ExtLocal& L) {
-    const bool frictional = (c.nfric >= 5 && c.nfric <= 7);
+    const bool frictional = (c.nfric >= 5 && c.nfric <= 8) || c.nfric == 26 || c.nfric == 27;
     float dc0 = -(L.frictx * L.hinv), dc1 = -(L.fricty * L.hinv);
     if (L.vmod > 1.e-5f) {
         float vs0 = vx + dt * (acc0 + dc0), vs1 = vy + dt * (acc1 + dc1);

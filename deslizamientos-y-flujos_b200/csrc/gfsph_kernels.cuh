@@ -4,12 +4,13 @@
 // reused by the density, force and XSPH passes, as the reference reuses its
 // pair list (w and dW frozen at the start of the step).
 //
-// Cell grids are block-sparse: each level's grid over the bounding box is cut
-// into blocks of 32 x 8 cells, a dense block map over the box marks the
-// blocks that hold particles, and only those blocks get cells (slot-major
-// keys: slot * 256 + row * 32 + column).  The cell count follows the area the
-// flow covers, not its bounding box, so separated releases on a large DEM
-// with small smoothing lengths stay within memory.
+// Cell grids: while every level's grid over the bounding box fits the dense
+// budget (4M cells, or 8 per particle), the cell keys are row-major over each
+// level (dense mode).  Beyond it (separated releases on a large DEM with
+// small smoothing lengths) the grids are block-sparse: cut into blocks of
+// 32 x 8 cells, a dense block map over the box marks the blocks that hold
+// particles, and only those blocks get cells (slot-major keys: slot * 256 +
+// row * 32 + column), so the cell count follows the area the flow covers.
 #pragma once
 #include "gfsph_device.cuh"
 
@@ -22,6 +23,7 @@ constexpr int kMaxLevels = 24;      // level k cell size Hc * 2^(k-1)
 constexpr int kBlkX = 32;           // cells per block along x
 constexpr int kBlkY = 8;            // cells per block along y
 constexpr int kBlockCells = kBlkX * kBlkY;
+constexpr long long kDenseCells = 1LL << 22;  // dense-mode budget (or 8 cells per particle)
 
 // error bits in StepScalars::err
 constexpr int kErrCells = 1;
@@ -47,7 +49,9 @@ struct StepScalars {
     int nlev;         // number of grid levels
     float lev_gx0[kMaxLevels], lev_gy0[kMaxLevels], lev_c[kMaxLevels];  // origin and cell size per level
     int lev_ndx[kMaxLevels], lev_ndy[kMaxLevels];  // cells per level along x and y
-    int lev_nbx[kMaxLevels], lev_boff[kMaxLevels + 1];  // blocks per level along x, first block-map entry
+    int lev_off[kMaxLevels + 1];  // dense mode: first cell key of each level
+    int lev_nbx[kMaxLevels], lev_boff[kMaxLevels + 1];  // sparse mode: blocks per level along x, first block-map entry
+    int sparse;       // 1: block-sparse cell keys this step
     unsigned int lev_hmax_o[kMaxLevels];  // max hsml of the particles of each level (ordered uint, 0 = empty)
     int nblocks;      // block-map entries (all levels)
     int ncells;       // cells of the occupied blocks
@@ -189,7 +193,7 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
 // over the same box, and one cell-key space covers all levels.  A particle
 // searches each level within hsml_i + (that level's hsml bound), so the
 // neighbour set is the reference's {j : r_ij < 2*(h_i+h_j)/2} exactly.
-__global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks) {
+__global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks, int cap_cells, int max_cells) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (S->skip) return;
     if (S->bad) { S->err |= kErrNonFinite; S->skip = 1; return; }
@@ -209,7 +213,7 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks) {
     while (nlev < kMaxLevels && ldexpf(hc, nlev - 1) < hmx) nlev++;
     if (ldexpf(hc, nlev - 1) < hmx) { S->err |= kErrCells; S->need_cells = 0x3fffffff; S->skip = 1; return; }
     float lx = xmx - xmn, ly = ymx - ymn;
-    long long off = 0;
+    long long off = 0, doff = 0;
     for (int k = 0; k < nlev; k++) {
         float cell = ldexpf(hc, k - 1);
         float fx = lx / cell + 1.f, fy = ly / cell + 1.f;
@@ -229,11 +233,26 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks) {
         int nbx = (ndx + kBlkX - 1) / kBlkX, nby = (ndy + kBlkY - 1) / kBlkY;
         S->lev_nbx[k] = nbx;
         S->lev_boff[k] = (int)min(off, 0x7fffffffLL);
+        S->lev_off[k] = (int)min(doff, 0x7fffffffLL);
         off += (long long)nbx * (long long)nby;
+        doff += (long long)ndx * (long long)ndy;
     }
     S->lev_boff[nlev] = (int)min(off, 0x7fffffffLL);
+    S->lev_off[nlev] = (int)min(doff, 0x7fffffffLL);
     S->hc = hc;
     S->nlev = nlev;
+    const long long budget = min((long long)max_cells, max(kDenseCells, 8LL * S->hcount));
+    S->sparse = (doff + 1 > budget) ? 1 : 0;
+    if (!S->sparse) {
+        if (doff + 1 > (long long)cap_cells) {
+            S->err |= kErrCells;
+            S->need_cells = (int)(doff + 1);
+            S->skip = 1;
+            return;
+        }
+        S->ncells = (int)doff;
+        return;
+    }
     if (off + 1 > (long long)cap_blocks) {
         S->err |= kErrBlocks;
         S->need_blocks = (off + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(off + 1);
@@ -279,8 +298,10 @@ __global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* 
                 int k = level_of(hs, S);
                 int cx, cy;
                 cell_of(p, S, k, cx, cy);
-                int b = block_of(S, k, cx, cy);
-                if (bmark[b] == 0) bmark[b] = 1;
+                if (S->sparse) {
+                    int b = block_of(S, k, cx, cy);
+                    if (bmark[b] == 0) bmark[b] = 1;
+                }
                 if (k == 0) h0 = f2o(hs);
                 else atomicMax(&S->lev_hmax_o[k], f2o(hs));
             }
@@ -298,13 +319,14 @@ __global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* 
 __global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* bmark, const int* bstart, int* count,
                        int2* keyrank, int cap_cells) {
     if (S->skip) return;
-    const long long ncells = (long long)bstart[S->nblocks] * kBlockCells;
+    const bool sparse = S->sparse != 0;
+    const long long ncells = sparse ? (long long)bstart[S->nblocks] * kBlockCells : (long long)S->ncells;
     const bool over = ncells + 1 > (long long)cap_cells;
     if (over && blockIdx.x == 0 && threadIdx.x == 0) {
         atomicOr(&S->err, kErrCells);
         S->need_cells = (ncells + 1 > 0x3fffffffLL) ? 0x3fffffff : (int)(ncells + 1);
     }
-    if (!over && blockIdx.x == 0 && threadIdx.x == 0) S->ncells = (int)ncells;
+    if (sparse && !over && blockIdx.x == 0 && threadIdx.x == 0) S->ncells = (int)ncells;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int2 kr = make_int2(-1, 0);
         float2 p = B.pos[i];
@@ -312,10 +334,15 @@ __global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* 
             int k = level_of(B.hsml[i], S);
             int cx, cy;
             cell_of(p, S, k, cx, cy);
-            int b = block_of(S, k, cx, cy);
-            bmark[b] = 0;
+            int key;
+            if (sparse) {
+                int b = block_of(S, k, cx, cy);
+                bmark[b] = 0;
+                key = bstart[b] * kBlockCells + (int)((unsigned)cy % kBlkY) * kBlkX + (int)((unsigned)cx % kBlkX);
+            } else {
+                key = S->lev_off[k] + cy * S->lev_ndx[k] + cx;
+            }
             if (!over) {
-                int key = bstart[b] * kBlockCells + (int)((unsigned)cy % kBlkY) * kBlkX + (int)((unsigned)cx % kBlkX);
                 kr.x = key;
                 kr.y = atomicAdd(&count[key], 1);
             }
@@ -326,8 +353,10 @@ __global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* 
 
 // Exclusive scan of the histogram, tile pass: each block scans kScanTile
 // cells and writes its tile total.
-__global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const int* nptr, const StepScalars* S) {
-    if (S->skip || S->err) return;
+// only_sparse: the block-map scan, which dense steps skip.
+__global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const int* nptr, const StepScalars* S,
+                             int only_sparse) {
+    if (S->skip || S->err || (only_sparse && !S->sparse)) return;
     int m = *nptr + 1;
     int base = blockIdx.x * kScanTile;
     if (base >= m) return;
@@ -372,8 +401,8 @@ __global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const 
 
 // Scan of the tile totals (one block of 1024 threads, up to 8192 tiles).
 // Also turns an error raised since the step began (k_hist) into a skip.
-__global__ void k_scan_top(int* tile_sum, const int* nptr, StepScalars* S) {
-    if (S->skip) return;
+__global__ void k_scan_top(int* tile_sum, const int* nptr, StepScalars* S, int only_sparse) {
+    if (S->skip || (only_sparse && !S->sparse)) return;
     if (S->err) {
         if (threadIdx.x == 0) S->skip = 1;
         return;
@@ -414,8 +443,8 @@ __global__ void k_scan_top(int* tile_sum, const int* nptr, StepScalars* S) {
     }
 }
 
-__global__ void k_scan_add(int* start, const int* tile_sum, const int* nptr, const StepScalars* S) {
-    if (S->skip || S->err) return;
+__global__ void k_scan_add(int* start, const int* tile_sum, const int* nptr, const StepScalars* S, int only_sparse) {
+    if (S->skip || S->err || (only_sparse && !S->sparse)) return;
     int m = *nptr + 1;
     int base = blockIdx.x * kScanTile;
     if (base >= m) return;
@@ -437,7 +466,8 @@ __global__ void k_scatter(const int2* keyrank, int n, const int* start, const in
         perm[slot] = i;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int nreg = (S->nlev > 1) ? start[bstart[S->lev_boff[1]] * kBlockCells] : nact;
+        int first1 = S->sparse ? bstart[S->lev_boff[1]] * kBlockCells : S->lev_off[1];
+        int nreg = (S->nlev > 1) ? start[first1] : nact;
         S->nreg = nreg;
         S->nbig = nact - nreg;
         S->nactive = nact;
@@ -516,6 +546,12 @@ __device__ __forceinline__ bool level_stencil(const StepScalars* S, int k, float
 // the block holds no particles).
 __device__ __forceinline__ void block_row_range(const Search& Q, const StepScalars* S, int k, int jy, int bx, int x0,
                                                 int x1, int& ja, int& jb) {
+    if (!S->sparse) {  // dense: the row is one key range (bx is 0)
+        int row = S->lev_off[k] + jy * S->lev_ndx[k];
+        ja = Q.start[row + x0];
+        jb = Q.start[row + x1 + 1];
+        return;
+    }
     int b = S->lev_boff[k] + (int)((unsigned)jy / kBlkY) * S->lev_nbx[k] + bx;
     int s0 = Q.bstart[b];
     if (Q.bstart[b + 1] == s0) { ja = jb = 0; return; }
@@ -542,9 +578,9 @@ __device__ __forceinline__ void visit_range(const Search& Q, int i, float2 xi, f
 // circle: a particle of row jy, d = |jy - cy| >= 2 rows away, is more than
 // (d - 1) cells away in y, so with r < hi + Hk it lies within
 // sqrt(rr^2 - (d - 1)^2) + 1 cells in x (rr and d - 1 carry 0.01-cell
-// margins for the rounding of the cell coordinates).  Along a row, the end of
-// one block's slots is the start of the next block's.
-template <class F>
+// margins for the rounding of the cell coordinates).  A dense row is one key
+// range; a sparse row is one range per block column it crosses.
+template <bool SPARSE, class F>
 __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScalars* S, int k, int i, float2 xi, float hi,
                                                  F&& f) {
     const unsigned int hk = S->lev_hmax_o[k];
@@ -566,6 +602,11 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
             rx = min(R, (int)sqrtf(q) + 1);
         }
         const int x0 = max(cx - rx, 0), x1 = min(cx + rx, ndx - 1);
+        if (!SPARSE) {
+            const int rowoff = S->lev_off[k] + jy * ndx;
+            visit_range(Q, i, xi, hi, Q.start[rowoff + x0], Q.start[rowoff + x1 + 1], f);
+            continue;
+        }
         const int c0 = (int)((unsigned)x0 / kBlkX), c1 = (int)((unsigned)x1 / kBlkX);
         const int brow = boff + (int)((unsigned)jy / kBlkY) * nbx;
         const int row = (int)((unsigned)jy % kBlkY) * kBlkX;
@@ -616,8 +657,11 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
 // and h_i = W(0,h_i) m_i + sum_j m_j W_ij (sum_density_Tools :1796-1836) is
 // accumulated in FP64.  Also stores the pressure term of IntForces_SW with h
 // clamped to h_inf (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
+// Instantiated for both cell layouts; the launch whose layout this step does
+// not use returns at once.
+template <bool SPARSE>
 __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
-    if (S->skip) return;
+    if (S->skip || (S->sparse != 0) != SPARSE) return;
     const int nreg = S->nreg, nlev = S->nlev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         float4 me = Q.xhm[i];
@@ -626,7 +670,7 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
         double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * me.w);
         int cnt = 0;
         for (int k = 0; k < nlev; k++)
-            level_neighbours(Q, S, k, i, xi, hi, [&](int j, float4 o, const PairGeom& g) {
+            level_neighbours<SPARSE>(Q, S, k, i, xi, hi, [&](int j, float4 o, const PairGeom& g) {
                 if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
                 cnt++;
                 acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
@@ -656,7 +700,8 @@ __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScala
     for (int k = 0; k < S->nlev; k++) {
         int x0, x1, y0, y1;
         if (!level_stencil(S, k, xi, hi, x0, x1, y0, y1)) continue;
-        const int bx0 = (int)((unsigned)x0 / kBlkX), ncol = (int)((unsigned)x1 / kBlkX) - bx0 + 1;
+        const int bx0 = S->sparse ? (int)((unsigned)x0 / kBlkX) : 0;
+        const int ncol = S->sparse ? (int)((unsigned)x1 / kBlkX) - bx0 + 1 : 1;
         const long long nseg = (long long)(y1 - y0 + 1) * ncol;
         for (long long sb = 0; sb < nseg; sb += 32) {
             long long sg = sb + lane;
@@ -870,7 +915,7 @@ __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars*
 // stages.  (A particle that leaves the DEM box mid-step is frozen; the
 // reference then keeps scattering its stale pressure into its neighbours for
 // the remaining stages, which is not reproduced.)
-__global__ void __launch_bounds__(128) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
+__global__ void __launch_bounds__(128, 7) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
                                                    PState B, float2* velfin, double2* auxv, int forces_only,
                                                    float2* indv_out) {
     if (S->skip) return;

@@ -379,8 +379,8 @@ struct Oracle {
      * filter.  Returns via L the friction and the (possibly recomputed) vmod. */
     void grav_and_friction(int i, Local& L, R top[6]) {
         R cgra = cst[1];
-        bool frictional = (nfric >= 5 && nfric <= 7);
-        bool v2byr = (nfric == 7);
+        bool frictional = (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27;
+        bool v2byr = (nfric == 7 || nfric == 8 || nfric == 26 || nfric == 27);
         R zp, zpx, zpy;
         get_z_topo(x[2 * i], x[2 * i + 1], zp, zpx, zpy, top, v2byr);
         L.gravz = cgra;
@@ -424,6 +424,18 @@ struct Oracle {
                 }
             }
             R tanfi = cst[9];
+            R xi = cst[3];
+            if (nfric == 8 || nfric == 26 || nfric == 27) { /* mu(I), :9651-9668 */
+                xi = 0; /* const(3) is a mu(I) parameter here */
+                R froude = L.vmod / std::sqrt(L.gravz * L.h);
+                if (nfric == 27) {
+                    R inert = (froude * cst[6]) / L.h;
+                    tanfi = tanfi + (cst[3] - tanfi) / ((R)1 + cst[7] / inert);
+                } else {
+                    R ff = (R)1 + cst[3] * (R)std::pow((double)((froude * cst[6]) / L.h), (double)cst[7]);
+                    tanfi = tanfi * ff;
+                }
+            }
             if (icpwp == 3) { /* :9670-9688: pwp = Uaux(1,ipoin), filtered, then tanfi*factpw */
                 R pwp = uaux[i];
                 R hhh = L.hrho;
@@ -439,7 +451,6 @@ struct Oracle {
             L.cf5 = gtanfi;
             L.frictx = ((L.cf5 * L.hu) * L.hvmodinv) * L.h;
             L.fricty = ((L.cf5 * L.hv) * L.hvmodinv) * L.h;
-            R xi = cst[3];
             if (xi != 0) {
                 R vxx = v[2 * i], vyy = v[2 * i + 1];
                 R vm = vxx * vxx + vyy * vyy;
@@ -460,7 +471,7 @@ struct Oracle {
 
     /* the reversal filter of basal_friction_Ext_SW, SPH_SW_2019.f90:9829-9895 */
     void reversal_filter(int i, Local& L, R acc0, R acc1) {
-        bool frictional = (nfric >= 5 && nfric <= 7);
+        bool frictional = (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27;
         R dc0 = -(L.frictx * L.hinv), dc1 = -(L.fricty * L.hinv);
         if (L.vmod > lit<R>(1.e-5)) {
             R vc0 = v[2 * i], vc1 = v[2 * i + 1];
@@ -687,7 +698,7 @@ struct Oracle {
         for (int k = 1; k <= GFSPH_NCONST; k++) cst[k] = (R)P->cst[k - 1];
         nfric = (int)(cst[5] + lit<R>(0.01));
         ic_erosion = (cst[21] > lit<R>(1.e-9)) ? 1 : 0;
-        if (!(nfric == 4 || (nfric >= 5 && nfric <= 7))) return GFSPH_ERR_UNSUPPORTED;
+        if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
         if (ic_erosion && (int)(cst[21] + lit<R>(0.1)) != 1) return GFSPH_ERR_UNSUPPORTED;
         if (P->skf != 1 && P->skf != 4) return GFSPH_ERR_UNSUPPORTED;
         nx = nx_; ny = ny_; npoig = nx * ny;

@@ -398,3 +398,33 @@ def test_pore_water_pressure_matches_oracle(gfsph_lib, oracle_mod, fct):
     assert np.hypot(*g["v"].T).mean() > v0
     sim.close()
     sim0.close()
+
+
+RHEOLOGIES = {
+    "bingham": {5: 4, 6: 500.0, 7: 50.0, 3: 0.0, 9: 0.0},
+    "frictional_voellmy": {5: 5},
+    "coulomb_cf": {5: 6, 3: -200.0},
+    "curvature": {5: 7},
+    "mu_I_8": {5: 8, 3: 1.0, 6: 0.5, 7: 2.0, 9: 0.25},
+    "mu_I_26": {5: 26, 3: 0.5, 6: 0.5, 7: 1.0, 9: 0.25},
+    "mu_I_27": {5: 27, 3: 0.6, 6: 0.5, 7: 0.3, 9: 0.2},
+}
+
+
+@pytest.mark.parametrize("rheo", sorted(RHEOLOGIES))
+def test_rheologies_match_oracle(gfsph_lib, oracle_mod, rheo):
+    """Every basal friction law on the path, 1 and 20 steps of the channel
+    release against the oracle in the GPU's precision scheme."""
+    w = small_channel()
+    w.const = {**w.const, **RHEOLOGIES[rheo]}
+    sim, st, p = setup_pair(w, oracle_mod)
+    ny, nx = w.z.shape
+    for nsteps in (1, 19):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        tol = 1e-6 if nsteps == 1 else 1e-5
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
+            assert rel_l2(g[key], ref) <= tol, (key, nsteps)
+    sim.close()

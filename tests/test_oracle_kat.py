@@ -280,3 +280,26 @@ def test_pwp_dissipates_exponentially(oracle_mod):
     v_exact = 9.8 * ((tan_t - mu) * t + mu * dt * (1.0 - q ** steps) / (1.0 - q))
     v = np.hypot(*st.v[0])
     assert abs(v - v_exact) < 1e-5 * v_exact, (v, v_exact)
+
+
+@pytest.mark.parametrize("nfric", [8, 27])
+def test_mu_of_I_steady_velocity_on_infinite_slope(oracle_mod, nfric):
+    """mu(I) basal friction (nfric 8: tanfi (1 + b I^n); nfric 27: tanfi +
+    (mu2 - tanfi) / (1 + I0/I)), I = Fr r / h, Fr = |v| / sqrt(g h): on a
+    plane (no curvature term) the lone particle settles where the friction
+    equals g tan(theta)."""
+    tan_t, tanfi, r = 0.5, 0.3, 0.5
+    h = lone_particle_depth(oracle_mod)
+    if nfric == 8:
+        b, n = 1.0, 2.0
+        const = {5: 8, 3: b, 6: r, 7: n, 9: tanfi}
+        inert = ((tan_t / tanfi - 1.0) / b) ** (1.0 / n)
+    else:
+        mu2, i0 = 0.8, 0.3
+        const = {5: 27, 3: mu2, 6: r, 7: i0, 9: tanfi}
+        a = (tan_t - tanfi) / (mu2 - tanfi)
+        inert = i0 * a / (1.0 - a)
+    st, _ = single_particle_run(oracle_mod, const, tan_t, 1500, 0.02, rho=h)
+    v_exact = inert * h / r * math.sqrt(9.8 * h)
+    v = np.hypot(*st.v[0])
+    assert abs(v - v_exact) < 2e-3 * v_exact, (v, v_exact)
