@@ -5,7 +5,13 @@
 // writes, at every plot time, a summary line and the depth raster (ESRI ASCII
 // grid), and at the end the per-node maximum depth and velocity.
 //
-//   gfsph_run <problem> [--dir D] [--topo NAME] [--out D] [--max-steps N] [--parse-only]
+//   gfsph_run <problem> [--dir D] [--topo NAME] [--out D] [--max-steps N] [--parse-only] [--dump FILE]
+//
+// --dump writes the parsed run (params struct, DEM grid and elevations, the
+// particles) to a binary file and exits: little-endian, "GFSPHDMP", int32
+// version 1, int32 sizeof(gfsph_params), the params bytes, int32 nx, ny,
+// float32 xmin, ymin, dx, dy, float32 z[nx*ny], int32 n, float32 x[2n],
+// v[2n], rho[n], mass[n], hsml[n].
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -61,13 +67,15 @@ int check(int st, const char* what) {
 
 int main(int argc, char** argv) {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: %s <problem> [--dir D] [--topo NAME] [--out D] [--max-steps N] [--parse-only]\n",
+        std::fprintf(stderr,
+                     "usage: %s <problem> [--dir D] [--topo NAME] [--out D] [--max-steps N] [--parse-only] [--dump FILE]\n",
                      argv[0]);
         return 1;
     }
     std::string problem = argv[1], dir, topo, out = ".";
     long long max_steps = -1;
     bool parse_only = false;
+    std::string dump;
     for (int k = 2; k < argc; k++) {
         std::string a = argv[k];
         if (a == "--dir" && k + 1 < argc) dir = argv[++k];
@@ -75,6 +83,7 @@ int main(int argc, char** argv) {
         else if (a == "--out" && k + 1 < argc) out = argv[++k];
         else if (a == "--max-steps" && k + 1 < argc) max_steps = std::atoll(argv[++k]);
         else if (a == "--parse-only") parse_only = true;
+        else if (a == "--dump" && k + 1 < argc) dump = argv[++k];
         else { std::fprintf(stderr, "unknown argument %s\n", a.c_str()); return 1; }
     }
     if (topo.empty()) topo = problem;  // the reference asks for it on stdin (SPH_FEM_topo_2019.f90:181)
@@ -128,6 +137,24 @@ int main(int argc, char** argv) {
         std::memset(&dem, 0, sizeof(dem));
         dem.nx = t.nx; dem.ny = t.ny; dem.xmin = t.xmin; dem.ymin = t.ymin; dem.dx = t.dx; dem.dy = t.dy;
         dem.z = t.z.data();
+        if (!dump.empty()) {
+            FILE* f = std::fopen(dump.c_str(), "wb");
+            if (!f) throw std::runtime_error("cannot write " + dump);
+            const int ver = 1, psz = (int)sizeof(p);
+            std::fwrite("GFSPHDMP", 1, 8, f);
+            std::fwrite(&ver, 4, 1, f); std::fwrite(&psz, 4, 1, f); std::fwrite(&p, sizeof(p), 1, f);
+            std::fwrite(&t.nx, 4, 1, f); std::fwrite(&t.ny, 4, 1, f);
+            std::fwrite(&t.xmin, 4, 1, f); std::fwrite(&t.ymin, 4, 1, f);
+            std::fwrite(&t.dx, 4, 1, f); std::fwrite(&t.dy, 4, 1, f);
+            std::fwrite(t.z.data(), 4, t.z.size(), f);
+            std::vector<float> vz(2 * (size_t)n, 0.f);
+            std::fwrite(&n, 4, 1, f);
+            std::fwrite(x.data(), 4, x.size(), f); std::fwrite(vz.data(), 4, vz.size(), f);
+            std::fwrite(h.data(), 4, h.size(), f); std::fwrite(mass.data(), 4, mass.size(), f);
+            std::fwrite(hsml.data(), 4, hsml.size(), f);
+            std::fclose(f);
+            return 0;
+        }
         gfsph_handle* hd = nullptr;
         check(gfsph_create(&p, &dem, &hd), "gfsph_create");
         std::vector<float> v(2 * (size_t)n, 0.f);

@@ -9,6 +9,7 @@ corners all carry material, smoothing length hsml = delt2D * facthsml, depth
 clamped to h_inf.
 """
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -296,3 +297,41 @@ def write_reference_inputs(w, directory, name):
         f.write("X Y h\n")
         for (xx, yy), hh in zip(w.x.astype(np.float64), w.rho.astype(np.float64)):
             f.write("%.9g %.9g %.9g\n" % (float(xx), float(yy), float(hh)))
+
+
+def from_driver_dump(path, gfsph_module):
+    """A Workload and its params from `gfsph_run <problem> --dump FILE`: the
+    run as the C++ driver parsed it from the reference's input files."""
+    import ctypes as C
+    with open(path, "rb") as f:
+        b = f.read()
+    if b[:8] != b"GFSPHDMP":
+        raise ValueError(path + ": not a gfsph_run dump")
+    ver, psz = np.frombuffer(b, np.int32, 2, 8)
+    if ver != 1 or psz != C.sizeof(gfsph_module.Params):
+        raise ValueError(path + ": dump version or params size mismatch")
+    off = 16
+    p = gfsph_module.Params.from_buffer_copy(b[off:off + psz])
+    off += psz
+    nx, ny = (int(v) for v in np.frombuffer(b, np.int32, 2, off))
+    off += 8
+    xmin, ymin, dx, dy = (float(v) for v in np.frombuffer(b, np.float32, 4, off))
+    off += 16
+    z = np.frombuffer(b, np.float32, nx * ny, off).reshape(ny, nx).copy()
+    off += 4 * nx * ny
+    n = int(np.frombuffer(b, np.int32, 1, off)[0])
+    off += 4
+
+    def take(count, shape):
+        nonlocal off
+        a = np.frombuffer(b, np.float32, count, off).reshape(shape).copy()
+        off += 4 * count
+        return a
+
+    x = take(2 * n, (n, 2))
+    v = take(2 * n, (n, 2))
+    rho, mass, hsml = take(n, (n,)), take(n, (n,)), take(n, (n,))
+    const = {k + 1: float(p.cst[k]) for k in range(len(p.cst)) if p.cst[k] != 0.0}
+    w = Workload(name=os.path.basename(path), const=const, options={}, z=z, dx=dx, dy=dy, x=x, v=v, rho=rho,
+                 mass=mass, hsml=hsml, meta=dict(xmin=xmin, ymin=ymin))
+    return w, p
