@@ -265,6 +265,71 @@ def ensemble_bench(args, torch, gfsph, workloads):
     }
 
 
+def cg_bench(args, gfsph, workloads, peak):
+    """The CG of the coupled large case: the P1 mass system of a 500 x 500-node
+    window of the DEM background triangulation at 2 m (498,002 triangles,
+    250,000 dofs), M x = b to r.r/r0.r0 <= 1e-10 (solvegc2's test), FP64 on the
+    device.  Bytes per iteration: CSR values and column indices, row pointers
+    and 6 FP64 vectors.  Host clock around each (synchronous) solve, which
+    includes copying b in and x out (2 MB)."""
+    nw = 500
+    intmat, coords = workloads.p1_mesh(nw, nw, 2.0)
+    g = workloads.p1_mass_matrices(intmat, coords)
+    b = np.random.default_rng(3).normal(size=coords.shape[0]).astype(np.float32)
+    cg = gfsph.CG(intmat, g)
+    cg.solve(b, tol=1e-10)
+    times, its = [], 0
+    for _ in range(5):
+        t0 = time.perf_counter()
+        _, _, _, its = cg.solve(b, tol=1e-10)
+        times.append(time.perf_counter() - t0)
+    cg.close()
+    n = coords.shape[0]
+    nnz = 7 * n  # a structured P1 mesh: every node couples to itself and 6 neighbours (fewer on the edge)
+    bytes_it = nnz * 12 + (n + 1) * 4 + 6 * 8 * n
+    t = statistics.median(times)
+    per_it = t / max(its, 1)
+    out = {"system": f"P1 mass matrix, {intmat.shape[0]} triangles, {n} dofs", "tol": 1e-10,
+           "iterations": its, "ms_per_solve": t * 1e3, "us_per_iteration": per_it * 1e6,
+           "bytes_per_iteration": bytes_it, "achieved_gbs": bytes_it / per_it / 1e9,
+           "frac_of_hbm": bytes_it / per_it / 1e9 / peak,
+           "note": "host clock around the synchronous solve; the working set (~35 MB) is L2-resident, "
+                   "so an iteration (3 kernels) is launch-latency bound"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        gs = g.astype(np.float32).astype(np.float64)
+        t0 = time.perf_counter()
+        _, _, _, it_cpu = oracle.solvegc2(0, intmat, gs, b.astype(np.float64), tol=1e-10)
+        out["cpu_port"] = {"ms_per_solve": (time.perf_counter() - t0) * 1e3, "iterations": it_cpu, "cores": 1,
+                           "kind": "port", "sample": "the same solve, FP32 restatement of solvegc2"}
+    return out
+
+
+def couple_bench(sim, w, gfsph):
+    """The coupling pass get_gradhs_w on the 500 x 500-node window of the DEM
+    around the flow: node depths from the particles, element gradients,
+    5 sweeps (the reference's) and, separately, the CG projection."""
+    st = sim.download()
+    act = st["flag"] == 0
+    c = np.floor(st["x"][act].mean(axis=0) / w.dx).astype(int)
+    ny, nx = w.z.shape
+    nw = min(500, nx, ny)
+    ix0 = int(min(max(c[0] - nw // 2, 0), nx - nw))
+    iy0 = int(min(max(c[1] - nw // 2, 0), ny - nw))
+    out = {"window": f"{nw}x{nw} nodes, {2 * (nw - 1) ** 2} triangles", "particles": int(act.sum())}
+    for niter, key in ((5, "sweeps_5"), (0, "cg")):
+        sim.gradhs(ix0, iy0, nw, nw, niter=niter)
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            sim.gradhs(ix0, iy0, nw, nw, niter=niter)
+            ts.append(time.perf_counter() - t0)
+        out[key + "_ms"] = statistics.median(ts) * 1e3
+    out["note"] = "host clock, outputs copied to the host (3 MB)"
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -381,7 +446,9 @@ def main():
     e2e_ms = e0.elapsed_time(e1)
     _, _, e2e_value = combine_ranks(e2e_ms, n, e2e_steps, dist, "cuda")
 
+    couple_line = couple_bench(sim, w, gfsph) if world == 1 else None
     sim.close()
+    cg_line = cg_bench(args, gfsph, workloads, peak) if world == 1 else None
     ens_line = None
     if world == 1 and args.ensemble > 0:
         ens_line = ensemble_bench(args, torch, gfsph, workloads)
@@ -423,6 +490,10 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if cg_line:
+            line["cg"] = cg_line
+        if couple_line:
+            line["couple"] = couple_line
         if ens_line:
             if cpu:
                 mean_n = ens_line["particles_total"] / ens_line["realizations"]

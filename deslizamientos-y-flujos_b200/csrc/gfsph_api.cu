@@ -11,6 +11,7 @@
 
 #include "../../include/gfsph.h"
 #include "gfsph_kernels.cuh"
+#include "gfsph_couple.cuh"
 
 using namespace gfsph;
 
@@ -20,7 +21,7 @@ enum KernelId {
     K_PREP, K_BOUNDS, K_GRID, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_TOP, K_BSCAN_ADD,
-    K_DENSITY_SPARSE,
+    K_DENSITY_SPARSE, K_COUPLE,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
@@ -29,7 +30,7 @@ const char* kKernelNames[K_COUNT] = {
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)", "k_scan_top(blocks)",
-    "k_scan_add(blocks)", "k_density(sparse)", "step_batches"};
+    "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "step_batches"};
 
 constexpr int kThreads = 128;
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
@@ -170,6 +171,13 @@ struct gfsph_handle {
     double *haz_sum_h = nullptr, *haz_sum_v = nullptr;
     unsigned int *haz_max_h = nullptr, *haz_max_v = nullptr;
     int* haz_cnt = nullptr;
+    // coupling pass (get_gradhs_w) buffers, sized for the largest window so far
+    int cw_nodes = 0;
+    double *cw_a1 = nullptr, *cw_a2 = nullptr;
+    float *cw_hs = nullptr, *cw_ml = nullptr;
+    float2 *cw_rhs = nullptr, *cw_g0 = nullptr, *cw_g1 = nullptr;
+    gfsph_cg* cw_cg = nullptr;  // mass-matrix CG of the last window (niter = 0)
+    int cw_key[4] = {-1, -1, -1, -1};
 };
 
 namespace {
@@ -644,6 +652,9 @@ int gfsph_destroy(gfsph_handle* h) {
     dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
     dfree(h->d_auxv); dfree(h->S); dfree(h->d_racc); dfree(h->d_rout);
     dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
+    dfree(h->cw_a1); dfree(h->cw_a2); dfree(h->cw_hs); dfree(h->cw_ml); dfree(h->cw_rhs); dfree(h->cw_g0);
+    dfree(h->cw_g1);
+    if (h->cw_cg) gfsph_cg_destroy(h->cw_cg);
     if (h->hS) cudaFreeHost(h->hS);
     for (int k = 0; k < K_COUNT; k++) {
         if (h->ev0[k]) cudaEventDestroy(h->ev0[k]);
@@ -1189,6 +1200,90 @@ int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob) {
     k_exceedance<<<blocks_for(np, 256), 256, 0, s>>>(e->d_maxptr, R, np, threshold, e->d_prob);
     CK(cudaMemcpyAsync(prob, e->d_prob, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return GFSPH_OK;
+}
+
+int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter, float tol, float* hs_w,
+                 float* gradhs_w) {
+    if (!h || nwx < 2 || nwy < 2 || ix0 < 0 || iy0 < 0 || ix0 + nwx > h->nx || iy0 + nwy > h->ny || niter < 0)
+        return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    const int nn = nwx * nwy;
+    if (nn > h->cw_nodes) {
+        dfree(h->cw_a1); dfree(h->cw_a2); dfree(h->cw_hs); dfree(h->cw_ml); dfree(h->cw_rhs); dfree(h->cw_g0);
+        dfree(h->cw_g1);
+        int st = 0;
+        st |= dalloc(&h->cw_a1, nn); st |= dalloc(&h->cw_a2, nn); st |= dalloc(&h->cw_hs, nn);
+        st |= dalloc(&h->cw_ml, nn); st |= dalloc(&h->cw_rhs, nn); st |= dalloc(&h->cw_g0, nn);
+        st |= dalloc(&h->cw_g1, nn);
+        if (st) { h->cw_nodes = 0; return GFSPH_ERR_CUDA; }
+        h->cw_nodes = nn;
+    }
+    Window w{ix0, iy0, nwx, nwy, h->dem.xmin, h->dem.ymin, h->dem.dx, h->dem.dy};
+    cudaStream_t st = h->stream;
+    CK(cudaMemsetAsync(h->cw_a1, 0, (size_t)nn * sizeof(double), st));
+    CK(cudaMemsetAsync(h->cw_a2, 0, (size_t)nn * sizeof(double), st));
+    launch(h, K_COUPLE, [&] { k_couple_idw<<<blocks_for(h->n), kThreads, 0, st>>>(h->B, h->n, w, h->cw_a1, h->cw_a2); });
+    launch(h, K_COUPLE, [&] { k_couple_hs<<<blocks_for(nn), kThreads, 0, st>>>(h->cw_a1, h->cw_a2, nn, h->cw_hs); });
+    launch(h, K_COUPLE, [&] {
+        k_couple_rhs<<<blocks_for(nn), kThreads, 0, st>>>(w, h->cw_hs, h->cw_rhs, h->cw_ml, h->cw_g0);
+    });
+    CK(cudaGetLastError());
+    float2* g = h->cw_g0;
+    if (niter > 0) {
+        float2* other = h->cw_g1;
+        for (int it = 2; it <= niter; it++) {  // the first sweep leaves g = 0 (:497-501)
+            launch(h, K_COUPLE, [&] {
+                k_couple_jacobi<<<blocks_for(nn), kThreads, 0, st>>>(w, g, h->cw_rhs, h->cw_ml, other);
+            });
+            std::swap(g, other);
+        }
+        CK(cudaGetLastError());
+        if (hs_w) CK(cudaMemcpyAsync(hs_w, h->cw_hs, (size_t)nn * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (gradhs_w) CK(cudaMemcpyAsync(gradhs_w, g, (size_t)nn * sizeof(float2), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return GFSPH_OK;
+    }
+    // niter = 0: M g = rhs by the device CG (solvegc2 semantics), both
+    // components as two dofs per node
+    const int key[4] = {ix0, iy0, nwx, nwy};
+    if (!h->cw_cg || std::memcmp(key, h->cw_key, sizeof(key)) != 0) {
+        if (h->cw_cg) { gfsph_cg_destroy(h->cw_cg); h->cw_cg = nullptr; }
+        const int nelem = 2 * (nwx - 1) * (nwy - 1);
+        std::vector<int> im(3 * (size_t)nelem);
+        std::vector<float> gs(36 * (size_t)nelem, 0.f);
+        for (int cj = 0; cj < nwy - 1; cj++)
+            for (int ci = 0; ci < nwx - 1; ci++) {
+                int e = 2 * (cj * (nwx - 1) + ci), n0 = cj * nwx + ci;
+                int t[2][3] = {{n0, n0 + 1, n0 + 1 + nwx}, {n0, n0 + 1 + nwx, n0 + nwx}};
+                for (int q = 0; q < 2; q++) {
+                    float x[3], y[3];
+                    for (int k = 0; k < 3; k++) {
+                        im[3 * (size_t)(e + q) + k] = t[q][k] + 1;
+                        x[k] = w.xming + (float)(ix0 + t[q][k] % nwx) * w.dxg;
+                        y[k] = w.yming + (float)(iy0 + t[q][k] / nwx) * w.dyg;
+                    }
+                    float rj = (x[1] - x[0]) * (y[2] - y[0]) - (x[2] - x[0]) * (y[1] - y[0]);
+                    float coe = rj / 24.f;
+                    float* ge = &gs[36 * (size_t)(e + q)];
+                    for (int a = 0; a < 3; a++)
+                        for (int b = 0; b < 3; b++)
+                            for (int d = 0; d < 2; d++) ge[(b * 2 + d) * 6 + (a * 2 + d)] = (a == b ? 2.f : 1.f) * coe;
+                }
+            }
+        int s2 = gfsph_cg_create(nn, nelem, 3, 2, im.data(), gs.data(), &h->cw_cg);
+        if (s2) return s2;
+        std::memcpy(h->cw_key, key, sizeof(key));
+    }
+    std::vector<float> rhs(2 * (size_t)nn), fixed(2 * (size_t)nn, 0.f), sol(2 * (size_t)nn, 0.f);
+    std::vector<int> iffix(2 * (size_t)nn, 0);
+    CK(cudaMemcpyAsync(rhs.data(), h->cw_rhs, (size_t)nn * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    if (hs_w) CK(cudaMemcpyAsync(hs_w, h->cw_hs, (size_t)nn * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int iters = 0;
+    int s3 = gfsph_cg_solve(h->cw_cg, iffix.data(), fixed.data(), rhs.data(), sol.data(), tol, &iters);
+    if (s3 < 0) return s3;
+    if (gradhs_w) std::memcpy(gradhs_w, sol.data(), sol.size() * sizeof(float));
     return GFSPH_OK;
 }
 

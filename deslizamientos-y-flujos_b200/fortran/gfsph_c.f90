@@ -147,6 +147,14 @@ module gfsph_c
        real(c_float), value :: dx, dy
        real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
      end function
+     integer(c_int) function gfsph_gradhs(h, ix0, iy0, nwx, nwy, niter, tol, hs_w, gradhs_w) &
+         bind(c, name="gfsph_gradhs")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: h
+       integer(c_int), value :: ix0, iy0, nwx, nwy, niter
+       real(c_float), value :: tol
+       real(c_float), intent(out) :: hs_w(*), gradhs_w(*)
+     end function
      integer(c_int) function gfsph_set_pwp(h, pwp) bind(c, name="gfsph_set_pwp")
        import :: c_int, c_ptr, c_float
        type(c_ptr), value :: h

@@ -87,6 +87,7 @@ SIGNATURES = {
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
     "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "gfsph_gradhs": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, _FP, _FP]),
     "gfsph_set_pwp": (C.c_int, [C.c_void_p, _FP]),
     "gfsph_get_pwp": (C.c_int, [C.c_void_p, _FP]),
     "gfsph_ensemble_create": (C.c_int, [C.POINTER(Params), C.POINTER(Dem), C.c_int, C.POINTER(C.c_void_p)]),
@@ -224,6 +225,13 @@ class Sim:
         _check(lib().gfsph_download(self.h, _fp(out["x"]), _fp(out["v"]), _fp(out["rho"]), _fp(out["mass"]),
                                     _fp(out["hsml"]), _ip(out["flag"])), "gfsph_download")
         return out
+
+    def gradhs(self, ix0, iy0, nwx, nwy, niter=5, tol=1e-10):
+        """get_gradhs_w on a DEM node window: (hs_w (nwy, nwx), gradhs_w (nwy, nwx, 2))."""
+        hs = np.empty((nwy, nwx), np.float32)
+        g = np.empty((nwy, nwx, 2), np.float32)
+        _check(lib().gfsph_gradhs(self.h, ix0, iy0, nwx, nwy, niter, tol, _fp(hs), _fp(g)), "gfsph_gradhs")
+        return hs, g
 
     def pwp(self):
         """Uaux(1,:), the basal pore-water pressure (icpwp = 3)."""

@@ -204,6 +204,24 @@ int gfsph_stats(gfsph_handle* h, int* out, int nout);
 int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol);
 
 /*
+ * The SPH -> FEM coupling pass get_gradhs_w (SPH_GFL_SW_Interactions_2019.f90:368-564)
+ * on the node window [ix0, ix0+nwx) x [iy0, iy0+nwy) of the DEM background
+ * triangulation (SPH_FEM_topo_2019.f90:583-604: two triangles per DEM cell,
+ * (n, n+1, n+1+nx) and (n, n+1+nx, n+nx)), from the current particles:
+ *   hs_w[nwx*nwy]        node depths, inverse-distance averages of the depth
+ *                        of the particles in each node's triangles;
+ *   gradhs_w[2*nwx*nwy]  (x, y) per node: the P1 projection g of the element
+ *                        gradients, M g = sum_e (A_e/3) grad_e.
+ * niter >= 1 solves as the reference does: niter sweeps
+ * g += (rhs - M g)/mmatl from g = 0, the first of which leaves g = 0
+ * (:497-501; the reference uses 5).  niter = 0 solves M g = rhs with the
+ * device CG (solvegc2 semantics) to the squared-norm tolerance tol.
+ * Either output may be NULL.
+ */
+int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter, float tol, float* hs_w,
+                 float* gradhs_w);
+
+/*
  * Monte-Carlo ensembles (the realization loop of SPH_FEM_Driver_2019.f90:88-139
  * with Get_MC_pixel_Vars_SW at plot times): nreal independent runs on one
  * DEM, each with its own parameters (params[r], e.g. sampled mu = const(9)

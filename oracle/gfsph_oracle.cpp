@@ -1145,6 +1145,136 @@ int solvegc2_mode(int npoin, int nelem, int nnode, int ndofn, const int* intmat,
 
 } // namespace
 
+/* The window mesh of the DEM background triangulation
+ * (SPH_FEM_topo_2019.f90:583-604): nodes [ix0, ix0+nwx) x [iy0, iy0+nwy),
+ * two triangles per cell, (n, n+1, n+1+nx) and (n, n+1+nx, n+nx), numbered
+ * cell by cell, x fastest; node coordinates xming + i*deltxg (:284-291). */
+template <class R>
+struct WindowMesh {
+    int nwx, nwy, nelem;
+    std::vector<R> cx, cy;     /* node coordinates */
+    std::vector<int> im;       /* 3 nodes per element, 0-based window nodes */
+    std::vector<R> geome;      /* 7 per element: dN/dx (3), dN/dy (3), rj = 2 area (getgeom2D :1675-1716) */
+    WindowMesh(int ix0, int iy0, int nwx_, int nwy_, R xming, R yming, R dxg, R dyg)
+        : nwx(nwx_), nwy(nwy_), nelem(2 * (nwx_ - 1) * (nwy_ - 1)) {
+        cx.resize((size_t)nwx * nwy); cy.resize((size_t)nwx * nwy);
+        for (int j = 0; j < nwy; j++)
+            for (int i = 0; i < nwx; i++) {
+                cx[(size_t)j * nwx + i] = xming + (R)(ix0 + i) * dxg;
+                cy[(size_t)j * nwx + i] = yming + (R)(iy0 + j) * dyg;
+            }
+        im.resize(3 * (size_t)nelem);
+        geome.resize(7 * (size_t)nelem);
+        for (int j = 0; j < nwy - 1; j++)
+            for (int i = 0; i < nwx - 1; i++) {
+                int e = 2 * (j * (nwx - 1) + i), n0 = j * nwx + i;
+                int* a = &im[3 * (size_t)e];
+                a[0] = n0; a[1] = n0 + 1; a[2] = n0 + 1 + nwx;
+                a[3] = n0; a[4] = n0 + 1 + nwx; a[5] = n0 + nwx;
+            }
+        const R nxi[3] = {-1, 1, 0}, net[3] = {-1, 0, 1};
+        for (int e = 0; e < nelem; e++) {
+            const int* a = &im[3 * (size_t)e];
+            R x21 = cx[a[1]] - cx[a[0]], x31 = cx[a[2]] - cx[a[0]];
+            R y21 = cy[a[1]] - cy[a[0]], y31 = cy[a[2]] - cy[a[0]];
+            R rj = x21 * y31 - x31 * y21;
+            R rj1 = (R)1 / rj;
+            R xix = y31 * rj1, xiy = -x31 * rj1, etx = -y21 * rj1, ety = x21 * rj1;
+            R* g = &geome[7 * (size_t)e];
+            for (int k = 0; k < 3; k++) {
+                g[k] = xix * nxi[k] + etx * net[k];
+                g[k + 3] = xiy * nxi[k] + ety * net[k];
+            }
+            g[6] = rj;
+        }
+    }
+};
+
+/* get_gradhs_w, SPH_GFL_SW_Interactions_2019.f90:368-564, on the window
+ * mesh: which_element by the barycentric test of :309-344 (elements in
+ * order, the last one that contains the point wins), IDW of the particle
+ * depths to the element's nodes, element gradients, rhs = sum A/3 grad, and
+ * niter sweeps g += (rhs - M g)/mmatl from g = 0, the first of which leaves
+ * g = 0 (it divides the zeroed gradhs_w by mmatl, :497-501).  hs_in (when n
+ * is 0) replaces the IDW node depths. */
+template <class R, class A>
+int gradhs_mode(int ix0, int iy0, int nwx, int nwy, double xmin, double ymin, double dx, double dy, int n,
+                const double* x, const double* rho, const int* flag, const double* hs_in, int niter, double* hs_out,
+                double* g_out) {
+    WindowMesh<R> m(ix0, iy0, nwx, nwy, (R)(float)xmin, (R)(float)ymin, (R)(float)dx, (R)(float)dy);
+    const int nn = nwx * nwy;
+    std::vector<R> hs(nn, (R)0);
+    if (n > 0) {
+        std::vector<A> a1(nn, (A)0), a2(nn, (A)0);
+        for (int ip = 0; ip < n; ip++) {
+            if (flag && flag[ip]) continue;
+            R xx = (R)x[2 * ip], yy = (R)x[2 * ip + 1];
+            int which = -1;
+            for (int e = 0; e < m.nelem; e++) {
+                const int* a = &m.im[3 * (size_t)e];
+                R xmin_e = std::min(std::min(m.cx[a[0]], m.cx[a[1]]), m.cx[a[2]]);
+                R xmax_e = std::max(std::max(m.cx[a[0]], m.cx[a[1]]), m.cx[a[2]]);
+                R ymin_e = std::min(std::min(m.cy[a[0]], m.cy[a[1]]), m.cy[a[2]]);
+                R ymax_e = std::max(std::max(m.cy[a[0]], m.cy[a[1]]), m.cy[a[2]]);
+                if (xx < xmin_e - (R)dx || xx > xmax_e + (R)dx || yy < ymin_e - (R)dy || yy > ymax_e + (R)dy) continue;
+                R x1 = m.cx[a[0]], y1 = m.cy[a[0]], x2 = m.cx[a[1]], y2 = m.cy[a[1]], x3 = m.cx[a[2]], y3 = m.cy[a[2]];
+                R x31 = x1 - x3, y31 = y1 - y3, x32 = x2 - x3, y32 = y2 - y3;
+                R detx = x31 * y32 - y31 * x32;
+                R x30 = xx - x3, y30 = yy - y3;
+                R sh1 = (x30 * y32 - y30 * x32) / detx;
+                R sh2 = (y30 * x31 - x30 * y31) / detx;
+                R sh3 = ((R)1 - sh1) - sh2;
+                if (sh1 >= 0 && sh1 <= 1 && sh2 >= 0 && sh2 <= 1 && sh3 >= 0 && sh3 <= 1) which = e;
+            }
+            if (which < 0) continue;
+            const int* a = &m.im[3 * (size_t)which];
+            for (int k = 0; k < 3; k++) {
+                R xn = m.cx[a[k]], yn = m.cy[a[k]];
+                R rdist = std::sqrt((xn - xx) * (xn - xx) + (yn - yy) * (yn - yy));
+                a1[a[k]] = a1[a[k]] + (A)((R)rho[ip] / rdist);
+                a2[a[k]] = a2[a[k]] + (A)((R)1 / rdist);
+            }
+        }
+        for (int k = 0; k < nn; k++)
+            if (!(a2[k] < (A)1.e-6)) hs[k] = (R)(a1[k] / a2[k]);
+    } else {
+        for (int k = 0; k < nn; k++) hs[k] = (R)hs_in[k];
+    }
+    std::vector<R> rhs(2 * (size_t)nn, (R)0), ml(nn, (R)0), g(2 * (size_t)nn, (R)0), rh(2 * (size_t)nn);
+    for (int e = 0; e < m.nelem; e++) {
+        const int* a = &m.im[3 * (size_t)e];
+        const R* ge = &m.geome[7 * (size_t)e];
+        R dxe = 0, dye = 0;
+        for (int k = 0; k < 3; k++) { dxe = dxe + hs[a[k]] * ge[k]; dye = dye + hs[a[k]] * ge[k + 3]; }
+        R coe = ge[6] / (R)6;
+        for (int k = 0; k < 3; k++) {
+            rhs[2 * a[k]] = rhs[2 * a[k]] + dxe * coe;
+            rhs[2 * a[k] + 1] = rhs[2 * a[k] + 1] + dye * coe;
+            ml[a[k]] = ml[a[k]] + coe; /* mmatl (SPH_FEM_topo_2019.f90:1764-1769) */
+        }
+    }
+    for (int it = 2; it <= niter; it++) {
+        std::fill(rh.begin(), rh.end(), (R)0);
+        for (int e = 0; e < m.nelem; e++) {
+            const int* a = &m.im[3 * (size_t)e];
+            R coe = m.geome[7 * (size_t)e + 6] / (R)24;
+            for (int in = 0; in < 3; in++)
+                for (int jn = 0; jn < 3; jn++) {
+                    R cm = (in == jn) ? (R)2 : (R)1;
+                    for (int d = 0; d < 2; d++) rh[2 * a[in] + d] = rh[2 * a[in] + d] + (cm * coe) * g[2 * a[jn] + d];
+                }
+        }
+        for (int k = 0; k < nn; k++)
+            for (int d = 0; d < 2; d++) g[2 * k + d] = g[2 * k + d] + (rhs[2 * k + d] - rh[2 * k + d]) / ml[k];
+    }
+    for (int k = 0; k < nn; k++) {
+        hs_out[k] = (double)hs[k];
+        g_out[2 * k] = (double)g[2 * k];
+        g_out[2 * k + 1] = (double)g[2 * k + 1];
+    }
+    return 0;
+}
+
 extern "C" {
 
 int oracle_solvegc2(int mode, int npoin, int nelem, int nnode, int ndofn, const int* intmat, int* iffix,
@@ -1197,6 +1327,20 @@ int oracle_get(void* h, double* x, double* v, double* rho, double* mass, double*
     if (!h) return GFSPH_ERR_ARG;
     static_cast<OracleBase*>(h)->get(x, v, rho, mass, hsml, flag, dt, t, topol);
     return 0;
+}
+
+/* The coupling pass get_gradhs_w on a node window of the DEM background
+ * triangulation (see gradhs_mode).  hs_out: nwx*nwy; g_out: 2*nwx*nwy. */
+int oracle_gradhs(int mode, int ix0, int iy0, int nwx, int nwy, double xmin, double ymin, double dx, double dy, int n,
+                  const double* x, const double* rho, const int* flag, const double* hs_in, int niter, double* hs_out,
+                  double* g_out) {
+    if (nwx < 2 || nwy < 2 || !hs_out || !g_out || (n > 0 && (!x || !rho)) || (n == 0 && !hs_in)) return GFSPH_ERR_ARG;
+    switch (mode) {
+    case 0: return gradhs_mode<float, float>(ix0, iy0, nwx, nwy, xmin, ymin, dx, dy, n, x, rho, flag, hs_in, niter, hs_out, g_out);
+    case 1: return gradhs_mode<float, double>(ix0, iy0, nwx, nwy, xmin, ymin, dx, dy, n, x, rho, flag, hs_in, niter, hs_out, g_out);
+    case 2: return gradhs_mode<double, double>(ix0, iy0, nwx, nwy, xmin, ymin, dx, dy, n, x, rho, flag, hs_in, niter, hs_out, g_out);
+    default: return GFSPH_ERR_ARG;
+    }
 }
 
 int oracle_get_pwp(void* h, double* pwp) {

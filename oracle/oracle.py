@@ -64,6 +64,9 @@ def lib():
         L.oracle_advance.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.oracle_get.restype = C.c_int
         L.oracle_get.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP, _DP, _IP, _DP, _DP, _DP]
+        L.oracle_gradhs.restype = C.c_int
+        L.oracle_gradhs.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_int, _DP, _DP, _IP, _DP, C.c_int, _DP, _DP]
         L.oracle_get_pwp.restype = C.c_int
         L.oracle_get_pwp.argtypes = [C.c_void_p, _DP]
         L.oracle_free.restype = None
@@ -262,3 +265,21 @@ def solvegc2(mode, intmat, gstif, rhs, iffix=None, fixed=None, tol=1e-10, ndofn=
     if st:
         raise RuntimeError(f"oracle_solvegc2: {st}")
     return x, r, fix, it.value
+
+
+def gradhs(mode, ix0, iy0, nwx, nwy, dx, dy, x=None, rho=None, flag=None, hs=None, niter=5, xmin=0.0, ymin=0.0):
+    """get_gradhs_w on the node window [ix0, ix0+nwx) x [iy0, iy0+nwy) of the
+    DEM background triangulation: (hs_w (nwy, nwx), gradhs_w (nwy, nwx, 2)).
+    Either particles (x, rho, flag) or node depths hs (nwy, nwx)."""
+    n = 0 if x is None else np.asarray(x).shape[0]
+    xd = _d(x) if n else None
+    rd = _d(rho) if n else None
+    fl = np.ascontiguousarray(flag, np.int32) if (n and flag is not None) else None
+    hin = _d(hs).reshape(-1) if hs is not None else None
+    hs_out = np.zeros(nwx * nwy)
+    g_out = np.zeros(2 * nwx * nwy)
+    st = lib().oracle_gradhs(mode, ix0, iy0, nwx, nwy, xmin, ymin, dx, dy, n, _dp(xd), _dp(rd), _ip(fl), _dp(hin),
+                             niter, _dp(hs_out), _dp(g_out))
+    if st:
+        raise RuntimeError(f"oracle_gradhs: {st}")
+    return hs_out.reshape(nwy, nwx), g_out.reshape(nwy, nwx, 2)

@@ -303,3 +303,32 @@ def test_mu_of_I_steady_velocity_on_infinite_slope(oracle_mod, nfric):
     v_exact = inert * h / r * math.sqrt(9.8 * h)
     v = np.hypot(*st.v[0])
     assert abs(v - v_exact) < 2e-3 * v_exact, (v, v_exact)
+
+
+def test_gradhs_projects_a_linear_depth_exactly(oracle_mod):
+    """get_gradhs_w on node depths that vary linearly: every element gradient
+    is the slope, rhs = slope * mmatl, so the second sweep lands on the slope
+    and the later ones keep it; the first sweep leaves g = 0 as in the
+    reference (it divides the zeroed gradient by mmatl)."""
+    nwx, nwy, d = 30, 20, 5.0
+    yy, xx = np.mgrid[0:nwy, 0:nwx] * d
+    hs = 2.0 + 0.03 * xx - 0.02 * yy
+    _, g1 = oracle_mod.gradhs(2, 0, 0, nwx, nwy, d, d, hs=hs, niter=1)
+    assert np.all(g1 == 0)
+    for niter in (2, 5):
+        _, g = oracle_mod.gradhs(2, 0, 0, nwx, nwy, d, d, hs=hs, niter=niter)
+        assert np.allclose(g[..., 0], 0.03, atol=1e-12) and np.allclose(g[..., 1], -0.02, atol=1e-12)
+
+
+def test_gradhs_idw_carries_a_lone_particle_to_its_triangle(oracle_mod):
+    """One particle inside the lower-right triangle (n, n+1, n+1+nx) of cell
+    (3, 2): its depth goes to those three nodes and nowhere else; a particle
+    on the cell diagonal belongs to the later triangle (n, n+1+nx, n+nx)."""
+    nwx, nwy, d = 8, 6, 2.0
+    hs, _ = oracle_mod.gradhs(1, 0, 0, nwx, nwy, d, d, x=np.array([[3 * d + 1.5, 2 * d + 0.5]]),
+                              rho=np.array([1.7]), niter=1)
+    nz = sorted(zip(*np.nonzero(hs)))
+    assert nz == [(2, 3), (2, 4), (3, 4)] and np.allclose(hs[hs != 0], 1.7)
+    hs, _ = oracle_mod.gradhs(1, 0, 0, nwx, nwy, d, d, x=np.array([[3 * d + 1.0, 2 * d + 1.0]]),
+                              rho=np.array([0.9]), niter=1)
+    assert sorted(zip(*np.nonzero(hs))) == [(2, 3), (3, 3), (3, 4)]
