@@ -12,6 +12,7 @@
 #include "../../include/gfsph.h"
 #include "gfsph_kernels.cuh"
 #include "gfsph_couple.cuh"
+#include "gfsph_adjoint.cuh"
 
 using namespace gfsph;
 
@@ -21,7 +22,7 @@ enum KernelId {
     K_PREP, K_BOUNDS, K_GRID, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_TOP, K_BSCAN_ADD,
-    K_DENSITY_SPARSE, K_COUPLE,
+    K_DENSITY_SPARSE, K_COUPLE, K_ADJOINT,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
@@ -30,7 +31,7 @@ const char* kKernelNames[K_COUNT] = {
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)", "k_scan_top(blocks)",
-    "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "step_batches"};
+    "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "k_adjoint", "step_batches"};
 
 constexpr int kThreads = 128;
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
@@ -1200,6 +1201,206 @@ int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob) {
     k_exceedance<<<blocks_for(np, 256), 256, 0, s>>>(e->d_maxptr, R, np, threshold, e->d_prob);
     CK(cudaMemcpyAsync(prob, e->d_prob, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return GFSPH_OK;
+}
+
+// ---------------------------------------------------------------- adjoint
+
+}  // extern "C"
+
+struct gfsph_adjoint {
+    gfsph_handle* h = nullptr;
+    int n = 0, nsteps = 0, every = 1, nck = 0;
+    double t0 = 0.0;
+    float dt0 = 0.f;
+    float2 *ckx = nullptr, *ckv = nullptr;    // checkpoints (caller order), nck * n
+    float2 *segx = nullptr, *segv = nullptr;  // states of one segment, every * n
+    float *rho0 = nullptr, *mass0 = nullptr, *hsml0 = nullptr;
+    float2 *lx = nullptr, *lv = nullptr;      // running adjoints (caller order)
+    double* lm = nullptr;                     // dL/d volume, accumulated
+    double* lpar = nullptr;                   // dL/d tanfi, dL/d xi
+    float* gh = nullptr;
+    float2 *lx1 = nullptr, *lv2 = nullptr, *lvp = nullptr, *lin = nullptr, *lv0 = nullptr;
+    float* lh = nullptr;
+    double2* lxacc = nullptr;
+    double* lms = nullptr;
+};
+
+namespace {
+
+// The state of the handle (caller order) into x, v (and the constant fields).
+int adj_capture(gfsph_adjoint* a, float2* x, float2* v, bool fields) {
+    gfsph_handle* h = a->h;
+    cudaStream_t st = h->stream;
+    const int n = h->n;
+    launch(h, K_ADJOINT, [&] { k_unsort<<<blocks_for(n), kThreads, 0, st>>>(h->B, n, h->U); });
+    CK(cudaMemcpyAsync(x, h->U.pos, (size_t)n * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(v, h->U.vel, (size_t)n * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    if (fields) {
+        CK(cudaMemcpyAsync(a->rho0, h->U.rho, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(a->mass0, h->U.mass, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(a->hsml0, h->U.hsml, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
+    return 0;
+}
+
+int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v) {
+    gfsph_handle* h = a->h;
+    launch(h, K_ADJOINT, [&] {
+        k_adj_restore<<<blocks_for(a->n), kThreads, 0, h->stream>>>(h->B, a->n, x, v, a->rho0, a->mass0, a->hsml0);
+    });
+    CK(cudaGetLastError());
+    set_field<float>(h, offsetof(StepScalars, dt), a->dt0);
+    set_field<int>(h, offsetof(StepScalars, err), 0);
+    h->has_state = true;
+    return 0;
+}
+
+// One step of the handle from its current buffers; fails unless it ran.
+int adj_one_step(gfsph_handle* h) {
+    int done = 0, guard = 0;
+    for (;;) {
+        int st = enqueue_chunk(h, 1, 1e300);
+        if (st) return st;
+        st = finish_chunk(h, 1, 1e300, done, guard);
+        if (st < 0) return st;
+        if (done >= 1) break;
+    }
+    if (h->hS->nbig != 0 || h->hS->nout != 0) return GFSPH_ERR_UNSUPPORTED;
+    return 0;
+}
+
+void adj_free(gfsph_adjoint* a) {
+    dfree(a->ckx); dfree(a->ckv); dfree(a->segx); dfree(a->segv); dfree(a->rho0); dfree(a->mass0); dfree(a->hsml0);
+    dfree(a->lx); dfree(a->lv); dfree(a->lm); dfree(a->lpar); dfree(a->gh); dfree(a->lx1); dfree(a->lv2);
+    dfree(a->lvp); dfree(a->lin); dfree(a->lv0); dfree(a->lh); dfree(a->lxacc); dfree(a->lms);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint** out) {
+    if (!h || !out || nsteps < 1 || every < 1) return GFSPH_ERR_ARG;
+    *out = nullptr;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    const Rheo& c = h->rheo;
+    if (!(c.nfric == 5 || c.nfric == 6) || c.xi < 0.f || c.erosion || c.icpwp != 0 || c.pa_sph != 2 || c.sle != 0 ||
+        c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f)
+        return GFSPH_ERR_UNSUPPORTED;
+    gfsph_adjoint* a = new (std::nothrow) gfsph_adjoint();
+    if (!a) return GFSPH_ERR_ARG;
+    a->h = h; a->n = h->n; a->nsteps = nsteps; a->every = std::min(every, nsteps);
+    a->nck = (nsteps + a->every - 1) / a->every + 1;
+    const size_t n = (size_t)h->n;
+    int st = 0;
+    st |= dalloc(&a->ckx, n * a->nck); st |= dalloc(&a->ckv, n * a->nck);
+    st |= dalloc(&a->segx, n * a->every); st |= dalloc(&a->segv, n * a->every);
+    st |= dalloc(&a->rho0, n); st |= dalloc(&a->mass0, n); st |= dalloc(&a->hsml0, n);
+    st |= dalloc(&a->lx, n); st |= dalloc(&a->lv, n); st |= dalloc(&a->lm, n); st |= dalloc(&a->lpar, 2);
+    st |= dalloc(&a->gh, n); st |= dalloc(&a->lx1, n); st |= dalloc(&a->lv2, n); st |= dalloc(&a->lvp, n);
+    st |= dalloc(&a->lin, n); st |= dalloc(&a->lv0, n); st |= dalloc(&a->lh, n); st |= dalloc(&a->lxacc, n);
+    st |= dalloc(&a->lms, n);
+    if (st) { adj_free(a); delete a; return GFSPH_ERR_CUDA; }
+    st = read_scalars(h);
+    if (st) { adj_free(a); delete a; return st; }
+    a->t0 = h->hS->time;
+    a->dt0 = h->hS->dt;
+    st = adj_capture(a, a->ckx, a->ckv, true);
+    for (int t = 0, k = 1; !st && t < nsteps; k++) {
+        int chunk = std::min(a->every, nsteps - t);
+        for (int q = 0; q < chunk && !st; q++) st = adj_one_step(h);
+        t += chunk;
+        if (!st) st = adj_capture(a, a->ckx + n * k, a->ckv + n * k, false);
+    }
+    if (!st) {
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) st = cuda_status(e);
+    }
+    if (st) { adj_free(a); delete a; return st; }
+    *out = a;
+    return GFSPH_OK;
+}
+
+int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, const float* gh, float* gx0, float* gv0,
+                           float* gm, double* gmu, double* gxi) {
+    if (!a || !gx || !gv) return GFSPH_ERR_ARG;
+    gfsph_handle* h = a->h;
+    cudaStream_t st = h->stream;
+    const int n = a->n;
+    const size_t un = (size_t)n;
+    CK(cudaMemcpyAsync(a->lx, gx, un * sizeof(float2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(a->lv, gv, un * sizeof(float2), cudaMemcpyHostToDevice, st));
+    if (gh) CK(cudaMemcpyAsync(a->gh, gh, un * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(a->lm, 0, un * sizeof(double), st));
+    CK(cudaMemsetAsync(a->lpar, 0, 2 * sizeof(double), st));
+    const int nseg = a->nck - 1;
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+        const int t0 = sg * a->every, len = std::min(a->every, a->nsteps - t0);
+        // the segment's states: from its checkpoint, recomputed forward
+        CK(cudaMemcpyAsync(a->segx, a->ckx + un * sg, un * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(a->segv, a->ckv + un * sg, un * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        for (int q = 1; q < len; q++) {
+            int r = adj_restore(a, a->segx + un * (q - 1), a->segv + un * (q - 1));
+            if (!r) r = adj_one_step(h);
+            if (!r) r = adj_capture(a, a->segx + un * q, a->segv + un * q, false);
+            if (r) return r;
+        }
+        for (int q = len - 1; q >= 0; q--) {
+            const bool last = (t0 + q == a->nsteps - 1);
+            int r = adj_restore(a, a->segx + un * q, a->segv + un * q);
+            if (!r) r = adj_one_step(h);  // neighbour table, density, forces of this step
+            if (r) return r;
+            Search Q = make_search(h);
+            const int pb = blocks_for(n);
+            launch(h, K_ADJOINT, [&] {
+                k_adj_seed<<<pb, kThreads, 0, st>>>(h->A, n, a->lx, a->lv, (last && gh) ? a->gh : nullptr, a->lx1,
+                                                    a->lv2, a->lh, a->lxacc, a->lms);
+            });
+            if (h->rheo.av_vel) {
+                launch(h, K_ADJOINT, [&] {
+                    k_adj_xsph<<<pb, kThreads, 0, st>>>(h->A, Q, h->rheo, n, h->velfin, a->lv2, a->lvp, a->lh,
+                                                        a->lms, a->lxacc);
+                });
+            } else {
+                CK(cudaMemcpyAsync(a->lvp, a->lv2, un * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+            }
+            launch(h, K_ADJOINT, [&] {
+                k_adj_rk<<<pb, kThreads, 0, st>>>(h->A, Q, h->S, h->rheo, h->dem, n, a->lx1, a->lvp, a->lh, a->lin,
+                                                  a->lxacc, a->lv0, a->lpar);
+            });
+            launch(h, K_ADJOINT, [&] {
+                k_adj_gather<<<pb, kThreads, 0, st>>>(h->A, Q, h->rheo, n, a->lin, a->lh, a->lms, a->lxacc);
+            });
+            launch(h, K_ADJOINT, [&] {
+                k_adj_scatter<<<pb, kThreads, 0, st>>>(h->A, n, a->lxacc, a->lv0, a->lms, a->lx, a->lv, a->lm);
+            });
+            CK(cudaGetLastError());
+        }
+    }
+    if (gx0) CK(cudaMemcpyAsync(gx0, a->lx, un * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    if (gv0) CK(cudaMemcpyAsync(gv0, a->lv, un * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    std::vector<double> lm(un);
+    double par[2];
+    CK(cudaMemcpyAsync(lm.data(), a->lm, un * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(par, a->lpar, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (gm)
+        for (size_t k = 0; k < un; k++) gm[k] = (float)lm[k];
+    if (gmu) *gmu = par[0];
+    if (gxi) *gxi = par[1];
+    // leave the handle at the final state of the recorded run
+    int r = adj_restore(a, a->ckx + un * (a->nck - 1), a->ckv + un * (a->nck - 1));
+    if (r) return r;
+    set_field<double>(h, offsetof(StepScalars, time), a->t0 + (double)a->nsteps * (double)a->dt0);
+    CK(cudaStreamSynchronize(st));
+    return GFSPH_OK;
+}
+
+int gfsph_adjoint_destroy(gfsph_adjoint* a) {
+    if (!a) return GFSPH_ERR_ARG;
+    adj_free(a);
+    delete a;
     return GFSPH_OK;
 }
 

@@ -147,6 +147,24 @@ module gfsph_c
        real(c_float), value :: dx, dy
        real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
      end function
+     integer(c_int) function gfsph_adjoint_forward(h, nsteps, every, adj) bind(c, name="gfsph_adjoint_forward")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: nsteps, every
+       type(c_ptr), intent(out) :: adj
+     end function
+     integer(c_int) function gfsph_adjoint_backward(adj, gx, gv, gh, gx0, gv0, gm, gmu, gxi) &
+         bind(c, name="gfsph_adjoint_backward")
+       import :: c_int, c_ptr, c_float, c_double
+       type(c_ptr), value :: adj
+       real(c_float), intent(in) :: gx(*), gv(*), gh(*)
+       real(c_float), intent(out) :: gx0(*), gv0(*), gm(*)
+       real(c_double), intent(out) :: gmu, gxi
+     end function
+     integer(c_int) function gfsph_adjoint_destroy(adj) bind(c, name="gfsph_adjoint_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: adj
+     end function
      integer(c_int) function gfsph_gradhs(h, ix0, iy0, nwx, nwy, niter, tol, hs_w, gradhs_w) &
          bind(c, name="gfsph_gradhs")
        import :: c_int, c_ptr, c_float

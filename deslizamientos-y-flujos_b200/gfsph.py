@@ -87,6 +87,10 @@ SIGNATURES = {
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
     "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "gfsph_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "gfsph_adjoint_backward": (C.c_int, [C.c_void_p, _FP, _FP, _FP, _FP, _FP, _FP, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]),
+    "gfsph_adjoint_destroy": (C.c_int, [C.c_void_p]),
     "gfsph_gradhs": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, _FP, _FP]),
     "gfsph_set_pwp": (C.c_int, [C.c_void_p, _FP]),
     "gfsph_get_pwp": (C.c_int, [C.c_void_p, _FP]),
@@ -416,6 +420,42 @@ class Ensemble:
             for m in self.members:
                 m.close()
             lib().gfsph_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Adjoint:
+    """gfsph_adjoint_*: records `nsteps` steps of `sim` (keeping the state
+    every `every` steps) and returns gradients of a loss on the final state."""
+
+    def __init__(self, sim, nsteps, every=1):
+        self.sim = sim
+        h = C.c_void_p()
+        _check(lib().gfsph_adjoint_forward(sim.h, nsteps, every, C.byref(h)), "gfsph_adjoint_forward")
+        self.h = h
+
+    def backward(self, gx, gv, gh=None):
+        """dL/dx, dL/dv (n, 2) and dL/dh (n,) of the final state -> dict of
+        dL/dx0, dL/dv0, dL/dmass, dL/dtanfi (const(9)), dL/dxi (const(3))."""
+        n = self.sim.n
+        gx = np.ascontiguousarray(gx, np.float32)
+        gv = np.ascontiguousarray(gv, np.float32)
+        ghh = None if gh is None else np.ascontiguousarray(gh, np.float32)
+        out = dict(x0=np.empty((n, 2), np.float32), v0=np.empty((n, 2), np.float32), mass=np.empty(n, np.float32))
+        mu, xi = C.c_double(), C.c_double()
+        _check(lib().gfsph_adjoint_backward(self.h, _fp(gx), _fp(gv), _fp(ghh), _fp(out["x0"]), _fp(out["v0"]),
+                                            _fp(out["mass"]), C.byref(mu), C.byref(xi)), "gfsph_adjoint_backward")
+        out["tanfi"], out["xi"] = mu.value, xi.value
+        return out
+
+    def close(self):
+        if self.h:
+            lib().gfsph_adjoint_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -222,6 +222,31 @@ int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter,
                  float* gradhs_w);
 
 /*
+ * Adjoint of the step: gradients of a loss on the final state of nsteps steps
+ * with respect to the initial positions and velocities, the particle volumes
+ * and the basal rheology (tanfi = const(9), xi = const(3)), for
+ * back-analysis.  This is a new capability; the reference has none.
+ *
+ * gfsph_adjoint_forward runs nsteps steps from the handle's state (the
+ * handle ends at the final state) and keeps the state every `every` steps in
+ * device memory (16 bytes per particle per kept state).
+ * gfsph_adjoint_backward takes dL/dx, dL/dv (2n each, caller order) and
+ * optionally dL/dh (n, the final depth) of the final state and returns
+ * dL/dx0, dL/dv0 (2n), dL/dvolume (n), dL/dtanfi and dL/dxi.  It recomputes
+ * every step from the kept states (each step's neighbour list is held fixed,
+ * as the forward step freezes it) and leaves the handle at the final state.
+ *
+ * Supported: nfric 5/6 with xi >= 0, no erosion or pore pressure, pa_sph 2,
+ * sle 0, ic_adapt 0, one grid level (uniform smoothing lengths) and no
+ * particle leaving the DEM (GFSPH_ERR_UNSUPPORTED otherwise).
+ */
+typedef struct gfsph_adjoint gfsph_adjoint;
+int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint** out);
+int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, const float* gh, float* gx0,
+                           float* gv0, float* gm, double* gmu, double* gxi);
+int gfsph_adjoint_destroy(gfsph_adjoint* a);
+
+/*
  * Monte-Carlo ensembles (the realization loop of SPH_FEM_Driver_2019.f90:88-139
  * with Get_MC_pixel_Vars_SW at plot times): nreal independent runs on one
  * DEM, each with its own parameters (params[r], e.g. sampled mu = const(9)

@@ -58,6 +58,53 @@
 
 #include "../include/gfsph.h"
 
+/* FP64 forward-mode (tangent) numbers: the oracle instantiated on Dual gives
+ * the exact derivative of its FP64 step along one seeded direction (the
+ * reference gradient for the device adjoint).  Branches follow the values. */
+struct Dual {
+    double v, d;
+    Dual() : v(0), d(0) {}
+    Dual(double a) : v(a), d(0) {}
+    Dual(double a, double b) : v(a), d(b) {}
+    explicit operator double() const { return v; }
+    explicit operator float() const { return (float)v; }
+    explicit operator int() const { return (int)v; }
+    explicit operator long() const { return (long)v; }
+    Dual operator-() const { return Dual(-v, -d); }
+    Dual& operator+=(const Dual& b) { v += b.v; d += b.d; return *this; }
+    Dual& operator-=(const Dual& b) { v -= b.v; d -= b.d; return *this; }
+};
+inline Dual operator+(const Dual& a, const Dual& b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(const Dual& a, const Dual& b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator*(const Dual& a, const Dual& b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(const Dual& a, const Dual& b) {
+    double q = a.v / b.v;
+    return Dual(q, (a.d - q * b.d) / b.v);
+}
+inline bool operator<(const Dual& a, const Dual& b) { return a.v < b.v; }
+inline bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
+inline bool operator<=(const Dual& a, const Dual& b) { return a.v <= b.v; }
+inline bool operator>=(const Dual& a, const Dual& b) { return a.v >= b.v; }
+inline bool operator==(const Dual& a, const Dual& b) { return a.v == b.v; }
+inline bool operator!=(const Dual& a, const Dual& b) { return a.v != b.v; }
+namespace std {
+inline Dual sqrt(const Dual& x) {
+    double r = std::sqrt(x.v);
+    return Dual(r, r > 0 ? x.d / (2.0 * r) : 0.0);
+}
+inline Dual exp(const Dual& x) {
+    double e = std::exp(x.v);
+    return Dual(e, e * x.d);
+}
+inline Dual atan2(const Dual& y, const Dual& x) {
+    double q = x.v * x.v + y.v * y.v;
+    return Dual(std::atan2(y.v, x.v), q > 0 ? (x.v * y.d - y.v * x.d) / q : 0.0);
+}
+inline Dual cos(const Dual& x) { return Dual(std::cos(x.v), -std::sin(x.v) * x.d); }
+inline Dual sin(const Dual& x) { return Dual(std::sin(x.v), std::cos(x.v) * x.d); }
+inline Dual fabs(const Dual& x) { return x.v < 0 ? -x : x; }
+}  // namespace std
+
 namespace {
 
 /* default-real literal: the value a Fortran constant like 0.3 or 2./3. has */
@@ -1300,6 +1347,49 @@ int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, dou
     case 2: return run_mode<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
     default: return GFSPH_ERR_ARG;
     }
+}
+
+/* Forward-mode derivative of nsteps FP64 steps along one direction: the
+ * tangents seed_mu of const(9) (tanfi), seed_xi of const(3) (xi), seed_m of
+ * the volumes and seed_x, seed_v of the initial positions and velocities.
+ * Returns the final positions, velocities and depths and their tangents. */
+int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+                   const double* topol, int n, const double* x, const double* v, const double* rho,
+                   const double* mass, const double* hsml, const int* flag, int nsteps, double dt, double t,
+                   double seed_mu, double seed_xi, const double* seed_m, const double* seed_x, const double* seed_v,
+                   double* out_x, double* out_v, double* out_h, double* tan_x, double* tan_v, double* tan_h) {
+    if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || n < 0 || nx < 2 || ny < 2) return GFSPH_ERR_ARG;
+    if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
+    Oracle<Dual, Dual> o;
+    int st = o.setup(p, nx, ny, xmin, ymin, dx, dy, topol);
+    if (st) return st;
+    o.cst[9].d = seed_mu;
+    o.cst[3].d = seed_xi;
+    o.n = n;
+    o.x.resize(2 * (size_t)n); o.v.resize(2 * (size_t)n);
+    o.rho.resize(n); o.mass.resize(n); o.hsml.resize(n);
+    for (size_t k = 0; k < 2 * (size_t)n; k++) {
+        o.x[k] = Dual(x[k], seed_x ? seed_x[k] : 0.0);
+        o.v[k] = Dual(v[k], seed_v ? seed_v[k] : 0.0);
+    }
+    for (int k = 0; k < n; k++) {
+        o.rho[k] = Dual(rho[k]);
+        o.mass[k] = Dual(mass[k], seed_m ? seed_m[k] : 0.0);
+        o.hsml[k] = Dual(hsml[k]);
+    }
+    o.flag.assign(flag, flag + n);
+    o.p.assign(n, Dual(0.0));
+    o.ex.assign(2 * (size_t)n, Dual(0.0)); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
+    o.dt = Dual(dt);
+    o.time = t;
+    o.init_pwp(nullptr);
+    for (int s2 = 0; s2 < nsteps; s2++) o.step();
+    for (size_t k = 0; k < 2 * (size_t)n; k++) {
+        out_x[k] = o.x[k].v; out_v[k] = o.v[k].v;
+        tan_x[k] = o.x[k].d; tan_v[k] = o.v[k].d;
+    }
+    for (int k = 0; k < n; k++) { out_h[k] = o.rho[k].v; tan_h[k] = o.rho[k].d; }
+    return 0;
 }
 
 /* Persistent oracle run: create on a state, advance, read back, free. */

@@ -67,6 +67,10 @@ def lib():
         L.oracle_gradhs.restype = C.c_int
         L.oracle_gradhs.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_int, _DP, _DP, _IP, _DP, C.c_int, _DP, _DP]
+        L.oracle_tangent.restype = C.c_int
+        L.oracle_tangent.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_int, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
         L.oracle_get_pwp.restype = C.c_int
         L.oracle_get_pwp.argtypes = [C.c_void_p, _DP]
         L.oracle_free.restype = None
@@ -283,3 +287,22 @@ def gradhs(mode, ix0, iy0, nwx, nwy, dx, dy, x=None, rho=None, flag=None, hs=Non
     if st:
         raise RuntimeError(f"oracle_gradhs: {st}")
     return hs_out.reshape(nwy, nwx), g_out.reshape(nwy, nwx, 2)
+
+
+def tangent(params, nx, ny, dx, dy, state, nsteps, seed_mu=0.0, seed_xi=0.0, seed_m=None, seed_x=None,
+            seed_v=None, xmin=0.0, ymin=0.0):
+    """FP64 forward-mode derivative of nsteps steps from `state` along one
+    direction (tangents of const(9), const(3), volumes, positions,
+    velocities): returns (x, v, h, dx, dv, dh) at the end."""
+    n = state.x.shape[0]
+    out = [np.zeros((n, 2)), np.zeros((n, 2)), np.zeros(n), np.zeros((n, 2)), np.zeros((n, 2)), np.zeros(n)]
+    sm = _d(seed_m) if seed_m is not None else None
+    sx = _d(seed_x) if seed_x is not None else None
+    sv = _d(seed_v) if seed_v is not None else None
+    st = lib().oracle_tangent(C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), n, _dp(state.x),
+                              _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.hsml), _ip(state.flag),
+                              nsteps, state.dt, state.t, seed_mu, seed_xi, _dp(sm), _dp(sx), _dp(sv),
+                              *[_dp(a) for a in out])
+    if st:
+        raise RuntimeError(f"oracle_tangent: {st}")
+    return tuple(out)

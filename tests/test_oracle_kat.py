@@ -332,3 +332,40 @@ def test_gradhs_idw_carries_a_lone_particle_to_its_triangle(oracle_mod):
     hs, _ = oracle_mod.gradhs(1, 0, 0, nwx, nwy, d, d, x=np.array([[3 * d + 1.0, 2 * d + 1.0]]),
                               rho=np.array([0.9]), niter=1)
     assert sorted(zip(*np.nonzero(hs))) == [(2, 3), (3, 3), (3, 4)]
+
+
+def test_tangent_oracle_matches_central_differences(oracle_mod):
+    """The FP64 forward-mode oracle (the reference gradient of the device
+    adjoint) against central differences of the FP64 oracle, along tanfi,
+    xi and a random volume direction, over 20 steps of a channel release."""
+    w = workloads.fractal_channel(n_target=2000, dem_k=7, cell=5.0, erosion=None)
+    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv, mode=oracle_mod.MODE_FP64)
+    st0 = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=0.01)
+    rng = np.random.default_rng(0)
+    gx, gv, gh = rng.normal(size=(w.n, 2)), rng.normal(size=(w.n, 2)), rng.normal(size=w.n)
+
+    def loss(q, mass=None):
+        st = st0.copy()
+        if mass is not None:
+            st.mass = mass
+        oracle_mod.run(oracle_mod.MODE_FP64, q, nx, ny, w.dx, w.dy, st, 20)
+        return float((gx * st.x).sum() + (gv * st.v).sum() + (gh * st.rho).sum())
+
+    def directional(**seed):
+        _, _, _, dx, dv, dh = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, 20, **seed)
+        return float((gx * dx).sum() + (gv * dv).sum() + (gh * dh).sum())
+
+    for k, seed in ((8, "seed_mu"), (2, "seed_xi")):
+        qp = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+        qm = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+        qp.cst[k] = p.cst[k] * (1 + 1e-4)
+        qm.cst[k] = p.cst[k] * (1 - 1e-4)
+        fd = (loss(qp) - loss(qm)) / (qp.cst[k] - qm.cst[k])
+        tg = directional(**{seed: 1.0})
+        assert abs(fd - tg) <= 1e-5 * abs(tg), (k, fd, tg)
+    dm = rng.normal(size=w.n) * w.mass * 1e-3
+    fd = (loss(p, w.mass + dm) - loss(p, w.mass - dm)) / 2
+    tg = directional(seed_m=dm)
+    assert abs(fd - tg) <= 1e-5 * abs(tg)
