@@ -306,6 +306,46 @@ def cg_bench(args, gfsph, workloads, peak):
     return out
 
 
+def adjoint_bench(gfsph, workloads, torch):
+    """The adjoint of the calibration case's step: ~50k particles on a 512^2
+    DEM at 5 m (fixed smoothing lengths, no erosion, fixed dt), 100 steps
+    recorded with a checkpoint every 10 and swept back; the cost of one
+    adjoint step (its forward recomputations included) against one plain
+    forward step of the same run."""
+    w = workloads.fractal_channel(n_target=50_000, dem_k=9, cell=5.0, erosion=None)
+    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    nsteps, every = 100, 10
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    sim.step(3)
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    sim.set_time(0.0, p.dt)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.step(nsteps)
+    torch.cuda.synchronize()
+    t_fwd = (time.perf_counter() - t0) / nsteps
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    sim.set_time(0.0, p.dt)
+    rng = np.random.default_rng(0)
+    gx = rng.normal(size=(w.n, 2)).astype(np.float32)
+    gv = rng.normal(size=(w.n, 2)).astype(np.float32)
+    t0 = time.perf_counter()
+    adj = gfsph.Adjoint(sim, nsteps, every=every)
+    t_rec = (time.perf_counter() - t0) / nsteps
+    t0 = time.perf_counter()
+    g = adj.backward(gx, gv)
+    t_bwd = (time.perf_counter() - t0) / nsteps
+    adj.close()
+    sim.close()
+    return {"workload": f"{w.n} particles, {w.meta['dem']}, Voellmy, fixed hsml and dt", "steps": nsteps,
+            "checkpoint_every": every, "forward_ms_per_step": t_fwd * 1e3,
+            "recording_ms_per_step": t_rec * 1e3, "backward_ms_per_step": t_bwd * 1e3,
+            "backward_over_forward": t_bwd / t_fwd, "dL_dtanfi": g["tanfi"], "dL_dxi": g["xi"],
+            "note": "host clock; the backward step recomputes the forward step (neighbour table, density, "
+                    "forces) from the kept states, plus the segment's states when every > 1"}
+
+
 def couple_bench(sim, w, gfsph):
     """The coupling pass get_gradhs_w on the 500 x 500-node window of the DEM
     around the flow: node depths from the particles, element gradients,
@@ -449,6 +489,7 @@ def main():
     couple_line = couple_bench(sim, w, gfsph) if world == 1 else None
     sim.close()
     cg_line = cg_bench(args, gfsph, workloads, peak) if world == 1 else None
+    adj_line = adjoint_bench(gfsph, workloads, torch) if world == 1 else None
     ens_line = None
     if world == 1 and args.ensemble > 0:
         ens_line = ensemble_bench(args, torch, gfsph, workloads)
@@ -492,6 +533,8 @@ def main():
             line["cpu_baseline"] = cpu
         if cg_line:
             line["cg"] = cg_line
+        if adj_line:
+            line["adjoint"] = adj_line
         if couple_line:
             line["couple"] = couple_line
         if ens_line:

@@ -1216,6 +1216,7 @@ struct gfsph_adjoint {
     float2 *ckx = nullptr, *ckv = nullptr;    // checkpoints (caller order), nck * n
     float2 *segx = nullptr, *segv = nullptr;  // states of one segment, every * n
     float *rho0 = nullptr, *mass0 = nullptr, *hsml0 = nullptr;
+    float* rhoN = nullptr;                    // depth of the final state
     float2 *lx = nullptr, *lv = nullptr;      // running adjoints (caller order)
     double* lm = nullptr;                     // dL/d volume, accumulated
     double* lpar = nullptr;                   // dL/d tanfi, dL/d xi
@@ -1244,10 +1245,11 @@ int adj_capture(gfsph_adjoint* a, float2* x, float2* v, bool fields) {
     return 0;
 }
 
-int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v) {
+int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v, const float* rho = nullptr) {
     gfsph_handle* h = a->h;
     launch(h, K_ADJOINT, [&] {
-        k_adj_restore<<<blocks_for(a->n), kThreads, 0, h->stream>>>(h->B, a->n, x, v, a->rho0, a->mass0, a->hsml0);
+        k_adj_restore<<<blocks_for(a->n), kThreads, 0, h->stream>>>(h->B, a->n, x, v, rho ? rho : a->rho0, a->mass0,
+                                                                    a->hsml0);
     });
     CK(cudaGetLastError());
     set_field<float>(h, offsetof(StepScalars, dt), a->dt0);
@@ -1266,12 +1268,14 @@ int adj_one_step(gfsph_handle* h) {
         if (st < 0) return st;
         if (done >= 1) break;
     }
-    if (h->hS->nbig != 0 || h->hS->nout != 0) return GFSPH_ERR_UNSUPPORTED;
+    // every particle active and on level 0 (nbig and nout are cleared when a step ends)
+    if (h->hS->nactive != h->n || h->hS->nreg != h->hS->nactive) return GFSPH_ERR_UNSUPPORTED;
     return 0;
 }
 
 void adj_free(gfsph_adjoint* a) {
     dfree(a->ckx); dfree(a->ckv); dfree(a->segx); dfree(a->segv); dfree(a->rho0); dfree(a->mass0); dfree(a->hsml0);
+    dfree(a->rhoN);
     dfree(a->lx); dfree(a->lv); dfree(a->lm); dfree(a->lpar); dfree(a->gh); dfree(a->lx1); dfree(a->lv2);
     dfree(a->lvp); dfree(a->lin); dfree(a->lv0); dfree(a->lh); dfree(a->lxacc); dfree(a->lms);
 }
@@ -1296,7 +1300,7 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     int st = 0;
     st |= dalloc(&a->ckx, n * a->nck); st |= dalloc(&a->ckv, n * a->nck);
     st |= dalloc(&a->segx, n * a->every); st |= dalloc(&a->segv, n * a->every);
-    st |= dalloc(&a->rho0, n); st |= dalloc(&a->mass0, n); st |= dalloc(&a->hsml0, n);
+    st |= dalloc(&a->rho0, n); st |= dalloc(&a->mass0, n); st |= dalloc(&a->hsml0, n); st |= dalloc(&a->rhoN, n);
     st |= dalloc(&a->lx, n); st |= dalloc(&a->lv, n); st |= dalloc(&a->lm, n); st |= dalloc(&a->lpar, 2);
     st |= dalloc(&a->gh, n); st |= dalloc(&a->lx1, n); st |= dalloc(&a->lv2, n); st |= dalloc(&a->lvp, n);
     st |= dalloc(&a->lin, n); st |= dalloc(&a->lv0, n); st |= dalloc(&a->lh, n); st |= dalloc(&a->lxacc, n);
@@ -1313,9 +1317,14 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
         t += chunk;
         if (!st) st = adj_capture(a, a->ckx + n * k, a->ckv + n * k, false);
     }
-    if (!st) {
-        cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (!st) {  // U holds the final state after the last capture
+        std::vector<int> fl(n);
+        cudaError_t e = cudaMemcpyAsync(a->rhoN, h->U.rho, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(fl.data(), h->U.flag, n * sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) st = cuda_status(e);
+        for (size_t k = 0; !st && k < n; k++)
+            if (fl[k]) st = GFSPH_ERR_UNSUPPORTED;  // a particle left the DEM in the last step
     }
     if (st) { adj_free(a); delete a; return st; }
     *out = a;
@@ -1390,7 +1399,7 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
     if (gmu) *gmu = par[0];
     if (gxi) *gxi = par[1];
     // leave the handle at the final state of the recorded run
-    int r = adj_restore(a, a->ckx + un * (a->nck - 1), a->ckv + un * (a->nck - 1));
+    int r = adj_restore(a, a->ckx + un * (a->nck - 1), a->ckv + un * (a->nck - 1), a->rhoN);
     if (r) return r;
     set_field<double>(h, offsetof(StepScalars, time), a->t0 + (double)a->nsteps * (double)a->dt0);
     CK(cudaStreamSynchronize(st));
@@ -1493,7 +1502,10 @@ int gfsph_stats(gfsph_handle* h, int* out, int nout) {
     int st = read_scalars(h);
     if (st) return st;
     const StepScalars* s = h->hS;
-    const int v[8] = {s->nactive, s->nreg, s->nbig, s->nlev, s->ncells, h->kcap, h->cap_cells, s->nout};
+    // nbig and nout are cleared for the next step when a step ends; nactive
+    // and nreg hold the last search's counts
+    const int v[8] = {s->nactive, s->nreg, s->nactive - s->nreg, s->nlev, s->ncells, h->kcap, h->cap_cells,
+                      h->n - s->nactive};
     for (int k = 0; k < nout && k < 8; k++) out[k] = v[k];
     return GFSPH_OK;
 }

@@ -13,7 +13,7 @@ NSTEPS = 20
 
 
 def case(oracle_mod, n=3000):
-    w = workloads.fractal_channel(n_target=n, dem_k=7, cell=5.0, erosion=None)
+    w = workloads.fractal_channel(n_target=n, dem_k=8, cell=5.0, erosion=None)
     p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
     topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv, mode=oracle_mod.MODE_FP32)
     return w, p, topol
@@ -75,7 +75,16 @@ def test_checkpoint_interval_does_not_change_the_gradient(gfsph_lib, oracle_mod)
 
 
 def test_adjoint_refuses_runs_outside_its_scope(gfsph_lib, oracle_mod):
-    w = workloads.fractal_channel(n_target=1000, dem_k=7, cell=5.0)  # with erosion
+    w = workloads.fractal_channel(n_target=1000, dem_k=8, cell=5.0)  # with erosion
+    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    with pytest.raises(gfsph.GfsphError) as e:
+        gfsph.Adjoint(sim, 5)
+    assert e.value.status == gfsph.ERR_UNSUPPORTED
+    sim.close()
+    # a release that reaches past the DEM edge: particles leave the box
+    w = workloads.fractal_channel(n_target=1000, dem_k=7, cell=5.0, erosion=None)
     p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
     sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
     sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
