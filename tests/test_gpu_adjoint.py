@@ -58,7 +58,7 @@ def test_adjoint_matches_forward_mode_derivatives(gfsph_lib, oracle_mod):
     dv0 = rng.normal(size=(w.n, 2))
     checks["v0"] = (directional(seed_v=dv0), float((g["v0"] * dv0).sum()))
     for name, (ref, got) in checks.items():
-        assert abs(got - ref) <= 1e-3 * abs(ref), (name, got, ref)
+        assert abs(got - ref) <= 2e-4 * abs(ref), (name, got, ref)
 
 
 def test_checkpoint_interval_does_not_change_the_gradient(gfsph_lib, oracle_mod):
