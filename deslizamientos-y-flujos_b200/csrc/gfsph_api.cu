@@ -151,6 +151,8 @@ struct gfsph_handle {
     int* bmark = nullptr;   // block map: 1 where a block holds particles (cleared by k_hist)
     int* bstart = nullptr;  // its exclusive scan: slot of each occupied block
     int cap_blocks = 0;
+    float level_factor = kBigFactor;  // search tunables (gfsph_set_search / gfsph_autotune)
+    float cell_div = kCellDiv;
     // scalars
     StepScalars* S = nullptr;
     StepScalars* hS = nullptr;  // pinned mirror
@@ -273,7 +275,8 @@ int enqueue_search(gfsph_handle* h, int advance) {
     const int* ncel = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, ncells));
     if (!advance) { launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++; }
     launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
-    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_blocks, h->cap_cells, kMaxCells); }); nk++;
+    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_blocks, h->cap_cells, kMaxCells, h->level_factor,
+                                  h->cell_div); }); nk++;
     launch(h, K_MARK, [&] { k_mark<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark); }); nk++;
     launch(h, K_BSCAN_TILES, [&] {
         k_scan_tiles<<<nbscan, kScanThreads, 0, st>>>(h->bmark, h->bstart, h->tile_sum, nblk, S, 1);
@@ -385,6 +388,11 @@ int alloc_nbr(gfsph_handle* h, int kcap) {
     h->kcap = kcap;
     drop_graphs(h);
     return 0;
+}
+
+void free_pstate(PState* p) {
+    dfree(p->pos); dfree(p->vel); dfree(p->rho); dfree(p->mass); dfree(p->hsml); dfree(p->flag); dfree(p->id);
+    dfree(p->pwp);
 }
 
 void free_particles(gfsph_handle* h) {
@@ -1283,6 +1291,93 @@ void adj_free(gfsph_adjoint* a) {
 }  // namespace
 
 extern "C" {
+
+int gfsph_set_search(gfsph_handle* h, float level_factor, float cell_div) {
+    if (!h || !(level_factor >= 1.f && level_factor <= 16.f) || !(cell_div >= 1.f && cell_div <= 8.f))
+        return GFSPH_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    h->level_factor = level_factor;
+    h->cell_div = cell_div;
+    drop_graphs(h);
+    return GFSPH_OK;
+}
+
+int gfsph_get_search(gfsph_handle* h, float* level_factor, float* cell_div) {
+    if (!h) return GFSPH_ERR_ARG;
+    if (level_factor) *level_factor = h->level_factor;
+    if (cell_div) *cell_div = h->cell_div;
+    return GFSPH_OK;
+}
+
+int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_div, float* best_ms) {
+    if (!h || steps < 1) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    const size_t n = (size_t)h->n, np = (size_t)h->nx * h->ny;
+    cudaStream_t st = h->stream;
+    // snapshot of everything a step changes: particles, scalars, DEM rows
+    PState snap{};
+    StepScalars* ssnap = nullptr;
+    float *z = nullptr, *er = nullptr, *av = nullptr;
+    int s0 = alloc_pstate(&snap, (int)n);
+    s0 |= dalloc(&ssnap, 1); s0 |= dalloc(&z, np); s0 |= dalloc(&er, np); s0 |= dalloc(&av, np);
+    auto cleanup = [&] {
+        free_pstate(&snap);
+        dfree(ssnap); dfree(z); dfree(er); dfree(av);
+    };
+    if (s0) { cleanup(); return GFSPH_ERR_CUDA; }
+    auto copy_state = [&](PState& dst, const PState& src, StepScalars* sd, const StepScalars* ss, float* zd,
+                          const float* zs, float* ed, const float* es, float* ad, const float* as) -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        auto cp = [&](void* d, const void* s2, size_t bytes) {
+            if (e == cudaSuccess) e = cudaMemcpyAsync(d, s2, bytes, cudaMemcpyDeviceToDevice, st);
+        };
+        cp(dst.pos, src.pos, n * sizeof(float2)); cp(dst.vel, src.vel, n * sizeof(float2));
+        cp(dst.rho, src.rho, n * sizeof(float)); cp(dst.mass, src.mass, n * sizeof(float));
+        cp(dst.hsml, src.hsml, n * sizeof(float)); cp(dst.flag, src.flag, n * sizeof(int));
+        cp(dst.id, src.id, n * sizeof(int)); cp(dst.pwp, src.pwp, n * sizeof(float));
+        cp(sd, ss, sizeof(StepScalars));
+        cp(zd, zs, np * sizeof(float)); cp(ed, es, np * sizeof(float)); cp(ad, as, np * sizeof(float));
+        return e;
+    };
+    cudaError_t e = copy_state(snap, h->B, ssnap, h->S, z, h->d_z, er, h->d_eroded, av, h->d_avail);
+    if (e != cudaSuccess) { cleanup(); return cuda_status(e); }
+    const float lfs[4] = {1.5f, 2.f, 2.5f, 3.f}, cds[3] = {2.f, 3.f, 4.f};
+    const float lf0 = h->level_factor, cd0 = h->cell_div;
+    float best = 1e30f, blf = lf0, bcd = cd0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int status = GFSPH_OK;
+    for (float lf : lfs)
+        for (float cd : cds) {
+            int r = gfsph_set_search(h, lf, cd);
+            double t = 0.0;
+            int done = 0;
+            if (!r) r = cuda_status(copy_state(h->B, snap, h->S, ssnap, h->d_z, z, h->d_eroded, er, h->d_avail, av));
+            if (!r) r = gfsph_step(h, 1, 1e300, &t, &done);  // graph capture, capacity growth
+            if (!r) r = cuda_status(copy_state(h->B, snap, h->S, ssnap, h->d_z, z, h->d_eroded, er, h->d_avail, av));
+            if (!r) r = cuda_status(cudaEventRecord(e0, st));
+            if (!r) r = gfsph_step(h, steps, 1e300, &t, &done);
+            if (!r) r = cuda_status(cudaEventRecord(e1, st));
+            if (!r) r = cuda_status(cudaEventSynchronize(e1));
+            if (r < 0) { status = r; break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; blf = lf; bcd = cd; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int r = gfsph_set_search(h, status ? lf0 : blf, status ? cd0 : bcd);
+    if (!r) r = cuda_status(copy_state(h->B, snap, h->S, ssnap, h->d_z, z, h->d_eroded, er, h->d_avail, av));
+    if (!r) r = cuda_status(cudaStreamSynchronize(st));
+    cleanup();
+    if (status) return status;
+    if (r) return r;
+    if (level_factor) *level_factor = blf;
+    if (cell_div) *cell_div = bcd;
+    if (best_ms) *best_ms = best / (float)steps;
+    return GFSPH_OK;
+}
 
 int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint** out) {
     if (!h || !out || nsteps < 1 || every < 1) return GFSPH_ERR_ARG;

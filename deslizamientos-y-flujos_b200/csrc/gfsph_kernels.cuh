@@ -18,7 +18,8 @@ namespace gfsph {
 
 constexpr int kScanTile = 2048;  // cells per scan tile (256 threads x 8)
 constexpr int kScanThreads = 256;
-constexpr float kBigFactor = 2.5f;  // hsml above kBigFactor * mean(hsml) goes to the big list
+constexpr float kBigFactor = 2.5f;  // default level-0 bound: hsml above kBigFactor * mean(hsml) is coarse
+constexpr float kCellDiv = 2.f;     // default cell size of level k: Hc * 2^k / kCellDiv
 constexpr int kMaxLevels = 24;      // level k cell size Hc * 2^(k-1)
 constexpr int kBlkX = 32;           // cells per block along x
 constexpr int kBlkY = 8;            // cells per block along y
@@ -193,7 +194,11 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
 // over the same box, and one cell-key space covers all levels.  A particle
 // searches each level within hsml_i + (that level's hsml bound), so the
 // neighbour set is the reference's {j : r_ij < 2*(h_i+h_j)/2} exactly.
-__global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks, int cap_cells, int max_cells) {
+// level_factor and cell_div are the search's tunables (gfsph_set_search):
+// Hc = min(max, level_factor * mean hsml) and level k's cell size is
+// Hc * 2^k / cell_div; neither changes the neighbour sets.
+__global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks, int cap_cells, int max_cells, float level_factor,
+                       float cell_div) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (S->skip) return;
     if (S->bad) { S->err |= kErrNonFinite; S->skip = 1; return; }
@@ -208,14 +213,14 @@ __global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks, int cap_cells, in
     }
     S->dt_step = dt;
     float mean = (float)(S->hsum / (double)S->hcount);
-    float hc = fminf(hmx, kBigFactor * mean);
+    float hc = fminf(hmx, level_factor * mean);
     int nlev = 1;
     while (nlev < kMaxLevels && ldexpf(hc, nlev - 1) < hmx) nlev++;
     if (ldexpf(hc, nlev - 1) < hmx) { S->err |= kErrCells; S->need_cells = 0x3fffffff; S->skip = 1; return; }
     float lx = xmx - xmn, ly = ymx - ymn;
     long long off = 0, doff = 0;
     for (int k = 0; k < nlev; k++) {
-        float cell = ldexpf(hc, k - 1);
+        float cell = ldexpf(hc, k) / cell_div;
         float fx = lx / cell + 1.f, fy = ly / cell + 1.f;
         if (!(fx < 1.0e8f) || !(fy < 1.0e8f) || !(fx * fy < 2.0e9f)) {  // far beyond any capacity
             S->err |= kErrCells;

@@ -147,6 +147,22 @@ module gfsph_c
        real(c_float), value :: dx, dy
        real(c_float), intent(inout) :: topol(GFSPH_NTOPO, *)
      end function
+     integer(c_int) function gfsph_set_search(h, level_factor, cell_div) bind(c, name="gfsph_set_search")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: h
+       real(c_float), value :: level_factor, cell_div
+     end function
+     integer(c_int) function gfsph_get_search(h, level_factor, cell_div) bind(c, name="gfsph_get_search")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: h
+       real(c_float), intent(out) :: level_factor, cell_div
+     end function
+     integer(c_int) function gfsph_autotune(h, steps, level_factor, cell_div, best_ms) bind(c, name="gfsph_autotune")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: h
+       integer(c_int), value :: steps
+       real(c_float), intent(out) :: level_factor, cell_div, best_ms
+     end function
      integer(c_int) function gfsph_adjoint_forward(h, nsteps, every, adj) bind(c, name="gfsph_adjoint_forward")
        import :: c_int, c_ptr
        type(c_ptr), value :: h

@@ -87,6 +87,9 @@ SIGNATURES = {
     "gfsph_dem_topol": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _FP]),
     "gfsph_raster_idw_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "gfsph_set_search": (C.c_int, [C.c_void_p, C.c_float, C.c_float]),
+    "gfsph_get_search": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "gfsph_autotune": (C.c_int, [C.c_void_p, C.c_int, _FP, _FP, _FP]),
     "gfsph_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "gfsph_adjoint_backward": (C.c_int, [C.c_void_p, _FP, _FP, _FP, _FP, _FP, _FP, C.POINTER(C.c_double),
                                          C.POINTER(C.c_double)]),
@@ -229,6 +232,20 @@ class Sim:
         _check(lib().gfsph_download(self.h, _fp(out["x"]), _fp(out["v"]), _fp(out["rho"]), _fp(out["mass"]),
                                     _fp(out["hsml"]), _ip(out["flag"])), "gfsph_download")
         return out
+
+    def set_search(self, level_factor, cell_div):
+        _check(lib().gfsph_set_search(self.h, level_factor, cell_div), "gfsph_set_search")
+
+    def get_search(self):
+        a, b = C.c_float(), C.c_float()
+        _check(lib().gfsph_get_search(self.h, C.byref(a), C.byref(b)), "gfsph_get_search")
+        return a.value, b.value
+
+    def autotune(self, steps=8):
+        """Picks the fastest search tunables on the current state: (level_factor, cell_div, ms/step)."""
+        a, b, t = C.c_float(), C.c_float(), C.c_float()
+        _check(lib().gfsph_autotune(self.h, steps, C.byref(a), C.byref(b), C.byref(t)), "gfsph_autotune")
+        return a.value, b.value, t.value
 
     def gradhs(self, ix0, iy0, nwx, nwy, niter=5, tol=1e-10):
         """get_gradhs_w on a DEM node window: (hs_w (nwy, nwx), gradhs_w (nwy, nwx, 2))."""

@@ -222,6 +222,21 @@ int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter,
                  float* gradhs_w);
 
 /*
+ * Neighbour-search tunables, which change the speed of the search and never
+ * its neighbour sets: level-0 particles are those with hsml <= Hc =
+ * min(max hsml, level_factor * mean hsml) (default 2.5, range [1, 16]), and
+ * level k's cells are Hc * 2^k / cell_div wide (default 2, range [1, 8]).
+ * gfsph_autotune times `steps` steps for each of 12 candidate pairs from
+ * the current state (restored after every trial), keeps the fastest and
+ * returns it with its time per step; the handle's state is unchanged.  The
+ * per-particle sums then run in another neighbour order, so results may
+ * differ from the defaults' in the last FP32 bit.
+ */
+int gfsph_set_search(gfsph_handle* h, float level_factor, float cell_div);
+int gfsph_get_search(gfsph_handle* h, float* level_factor, float* cell_div);
+int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_div, float* best_ms_per_step);
+
+/*
  * Adjoint of the step: gradients of a loss on the final state of nsteps steps
  * with respect to the initial positions and velocities, the particle volumes
  * and the basal rheology (tanfi = const(9), xi = const(3)), for

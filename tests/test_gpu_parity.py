@@ -428,3 +428,46 @@ def test_rheologies_match_oracle(gfsph_lib, oracle_mod, rheo):
         for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
             assert rel_l2(g[key], ref) <= tol, (key, nsteps)
     sim.close()
+
+
+@pytest.mark.parametrize("tune", [(1.5, 3.0), (3.0, 4.0), (2.0, 1.0)])
+def test_search_tunables_keep_sets_and_results(gfsph_lib, oracle_mod, tune):
+    """Other level bounds and cell sizes: the same neighbour sets, and one step
+    still on the oracle."""
+    w = small_channel()
+    rng = np.random.default_rng(4)
+    w.hsml = w.hsml.copy()
+    w.hsml[rng.choice(w.n, 20, replace=False)] *= np.float32(5.0)
+    sim, st, p = setup_pair(w, oracle_mod)
+    sim.set_search(*tune)
+    assert sim.get_search() == tune
+    sim.density()
+    off, idx = sim.neighbours()
+    ref = oracle_mod.pairs(oracle_mod.MODE_FP32, p, w.x, w.hsml)
+    assert np.array_equal(off, ref["offsets"]) and np.array_equal(idx, ref["idx"])
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    sim.step(1)
+    g = sim.download()
+    ny, nx = w.z.shape
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, 1)
+    for key, r in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass), ("hsml", st.hsml)):
+        assert max_rel(g[key], r, floor=1e-3) <= 1e-6, key
+    sim.close()
+
+
+def test_autotune_keeps_the_state(gfsph_lib, oracle_mod):
+    w = small_channel()
+    sim, _, _ = setup_pair(w, oracle_mod)
+    sim.step(3)
+    before = sim.download()
+    t_before = sim.time()
+    z_before = sim.raster(gfsph.RASTER_Z)
+    lf, cd, ms = sim.autotune(steps=4)
+    assert (lf, cd) == sim.get_search() and ms > 0
+    after = sim.download()
+    for k in before:
+        assert np.array_equal(before[k], after[k]), k
+    assert sim.time() == t_before
+    assert np.array_equal(z_before, sim.raster(gfsph.RASTER_Z))
+    sim.step(2)  # still steps
+    sim.close()
