@@ -456,6 +456,7 @@ def main():
     peak, peak_kind = load_peaks()
     st_now = sim.download()
     search_stats = sim.stats()
+    sim_search = sim.get_search()
     nact = int((st_now["flag"] == 0).sum())
     b_launch = B_ALG.get(dom, 0) * nact
     achieved = b_launch / (dom_ms / 1000.0) / 1e9
@@ -523,7 +524,7 @@ def main():
                          "alg_bytes_per_launch": b_launch, "avg_launch_ms": dom_ms,
                          "step_achieved_gbs": 168 * n * args.steps / (ms_total / 1000.0) / 1e9 / world},
             "kernel_shares": shares,
-            "search": search_stats,
+            "search": {**search_stats, "level_factor": sim_search[0], "cell_div": sim_search[1]},
             "steady_state": {"value": steady, "unit": UNIT, "note": "K steps in one call, L2 not flushed"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

@@ -19,7 +19,7 @@ namespace gfsph {
 constexpr int kScanTile = 2048;  // cells per scan tile (256 threads x 8)
 constexpr int kScanThreads = 256;
 constexpr float kBigFactor = 2.5f;  // default level-0 bound: hsml above kBigFactor * mean(hsml) is coarse
-constexpr float kCellDiv = 2.f;     // default cell size of level k: Hc * 2^k / kCellDiv
+constexpr float kCellDiv = 3.f;     // default cell size of level k: Hc * 2^k / kCellDiv
 constexpr int kMaxLevels = 24;      // level k cell size Hc * 2^(k-1)
 constexpr int kBlkX = 32;           // cells per block along x
 constexpr int kBlkY = 8;            // cells per block along y

@@ -225,7 +225,7 @@ int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter,
  * Neighbour-search tunables, which change the speed of the search and never
  * its neighbour sets: level-0 particles are those with hsml <= Hc =
  * min(max hsml, level_factor * mean hsml) (default 2.5, range [1, 16]), and
- * level k's cells are Hc * 2^k / cell_div wide (default 2, range [1, 8]).
+ * level k's cells are Hc * 2^k / cell_div wide (default 3, range [1, 8]).
  * gfsph_autotune times `steps` steps for each of 12 candidate pairs from
  * the current state (restored after every trial), keeps the fastest and
  * returns it with its time per step; the handle's state is unchanged.  The
