@@ -381,6 +381,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ensemble", type=int, default=16, help="realizations of the ensemble line (0: none)")
     ap.add_argument("--ensemble-steps", type=int, default=40)
+    ap.add_argument("--no-extras", action="store_true", help="only the step: no ensemble, CG, coupling, adjoint")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
@@ -487,12 +488,13 @@ def main():
     e2e_ms = e0.elapsed_time(e1)
     _, _, e2e_value = combine_ranks(e2e_ms, n, e2e_steps, dist, "cuda")
 
-    couple_line = couple_bench(sim, w, gfsph) if world == 1 else None
+    extras = world == 1 and not args.no_extras
+    couple_line = couple_bench(sim, w, gfsph) if extras else None
     sim.close()
-    cg_line = cg_bench(args, gfsph, workloads, peak) if world == 1 else None
-    adj_line = adjoint_bench(gfsph, workloads, torch) if world == 1 else None
+    cg_line = cg_bench(args, gfsph, workloads, peak) if extras else None
+    adj_line = adjoint_bench(gfsph, workloads, torch) if extras else None
     ens_line = None
-    if world == 1 and args.ensemble > 0:
+    if extras and args.ensemble > 0:
         ens_line = ensemble_bench(args, torch, gfsph, workloads)
 
     cpu = None
