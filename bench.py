@@ -35,10 +35,9 @@ B_ALG = {"k_density": 24, "k_force_rk": 72, "k_xsph": 44, "k_hist": 28}  # bytes
 # particles, step 11; profiles/neighbour_kernels_fractal_channel_200k.md):
 # DRAM read + write bytes and warp instructions per launch, per particle.
 NCU_PER_PARTICLE = {
-    "k_density": {"dram_bytes": (5.256960e6 + 1.702400e6) / 200011, "warp_inst": 59987700 / 200011},
-    "k_iforce": {"dram_bytes": (43.446528e6 + 0.020224e6) / 200011, "warp_inst": 41244668 / 200011},
-    "k_force_rk": {"dram_bytes": 8.216832e6 / 200011, "warp_inst": 24964335 / 200011},
-    "k_xsph": {"dram_bytes": (45.841664e6 + 0.216064e6) / 200011, "warp_inst": 35318840 / 200011},
+    "k_density": {"dram_bytes": (5.053952e6 + 0.745472e6) / 200011, "warp_inst": 45954755 / 200011},
+    "k_iforce": {"dram_bytes": (43.920640e6 + 0.019968e6) / 200011, "warp_inst": 42718083 / 200011},
+    "k_force_rk": {"dram_bytes": 8.231424e6 / 200011, "warp_inst": 26332133 / 200011},
 }
 NCU_SOURCE = "profiles/neighbour_kernels_fractal_channel_200k.md (ncu, cold caches), scaled by active particles"
 ISSUE_PEAK = 148 * 4 * 1.965e9  # warp instructions/s: SMs x schedulers x max SM clock
