@@ -19,7 +19,7 @@ using namespace gfsph;
 namespace {
 
 enum KernelId {
-    K_PREP, K_BOUNDS, K_GRID, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
+    K_PREP, K_BOUNDS, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_TOP, K_BSCAN_ADD,
     K_DENSITY_SPARSE, K_COUPLE, K_ADJOINT,
@@ -27,7 +27,7 @@ enum KernelId {
     K_COUNT
 };
 const char* kKernelNames[K_COUNT] = {
-    "k_prep", "k_bounds", "k_grid", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
+    "k_prep", "k_bounds", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)", "k_scan_top(blocks)",
@@ -151,6 +151,7 @@ struct gfsph_handle {
     int* bmark = nullptr;   // block map: 1 where a block holds particles (cleared by k_hist)
     int* bstart = nullptr;  // its exclusive scan: slot of each occupied block
     int cap_blocks = 0;
+    BoundsPart* bparts = nullptr;  // k_bounds block partials
     float level_factor = kBigFactor;  // search tunables (gfsph_set_search / gfsph_autotune)
     float cell_div = kCellDiv;
     // scalars
@@ -274,9 +275,10 @@ int enqueue_search(gfsph_handle* h, int advance) {
     const int* nblk = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, nblocks));
     const int* ncel = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, ncells));
     if (!advance) { launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++; }
-    launch(h, K_BOUNDS, [&] { k_bounds<<<std::min(pb, 148 * 8), kThreads, 0, st>>>(h->B, n, h->rheo, h->dem, S); }); nk++;
-    launch(h, K_GRID, [&] { k_grid<<<1, 32, 0, st>>>(h->rheo, S, h->cap_blocks, h->cap_cells, kMaxCells, h->level_factor,
-                                  h->cell_div); }); nk++;
+    const GridArgs ga{h->cap_blocks, h->cap_cells, kMaxCells, h->level_factor, h->cell_div};
+    launch(h, K_BOUNDS, [&] {
+        k_bounds<<<kBoundsBlocks, kThreadsBounds, 0, st>>>(h->B, n, h->rheo, h->dem, S, h->bparts, ga);
+    }); nk++;
     launch(h, K_MARK, [&] { k_mark<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark); }); nk++;
     launch(h, K_BSCAN_TILES, [&] {
         k_scan_tiles<<<nbscan, kScanThreads, 0, st>>>(h->bmark, h->bstart, h->tile_sum, nblk, S, 1);
@@ -352,7 +354,7 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 16 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 15 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
 }
 
 int alloc_blocks(gfsph_handle* h, int cap) {
@@ -624,6 +626,7 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     st |= dalloc(&h->d_z, np); st |= dalloc(&h->d_eroded, np); st |= dalloc(&h->d_avail, np);
     st |= dalloc(&h->d_auxv, np);
     st |= dalloc(&h->S, 1);
+    st |= dalloc(&h->bparts, kBoundsBlocks);
     if (st) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
     if (cudaMallocHost((void**)&h->hS, sizeof(StepScalars)) != cudaSuccess) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
     cudaMemcpy(h->d_grad, grad.data(), np * sizeof(float2), cudaMemcpyHostToDevice);
@@ -659,7 +662,7 @@ int gfsph_destroy(gfsph_handle* h) {
     free_particles(h);
     dfree(h->count); dfree(h->start); dfree(h->tile_sum); dfree(h->bmark); dfree(h->bstart);
     dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
-    dfree(h->d_auxv); dfree(h->S); dfree(h->d_racc); dfree(h->d_rout);
+    dfree(h->d_auxv); dfree(h->S); dfree(h->bparts); dfree(h->d_racc); dfree(h->d_rout);
     dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
     dfree(h->cw_a1); dfree(h->cw_a2); dfree(h->cw_hs); dfree(h->cw_ml); dfree(h->cw_rhs); dfree(h->cw_g0);
     dfree(h->cw_g1);

@@ -25,6 +25,8 @@ constexpr int kBlkX = 32;           // cells per block along x
 constexpr int kBlkY = 8;            // cells per block along y
 constexpr int kBlockCells = kBlkX * kBlkY;
 constexpr long long kDenseCells = 1LL << 22;  // dense-mode budget (or 8 cells per particle)
+constexpr int kThreadsBounds = 128;
+constexpr int kBoundsBlocks = 148 * 2;
 
 // error bits in StepScalars::err
 constexpr int kErrCells = 1;
@@ -59,6 +61,7 @@ struct StepScalars {
     int nreg, nbig, nactive, nout;
     int need_cells, need_nbr, need_big, need_blocks;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
+    unsigned int bounds_ticket;  // blocks of k_bounds done (the last one resets it)
     int advance;      // 1 inside gfsph_step, 0 for search-only passes
 };
 
@@ -136,7 +139,31 @@ __device__ __forceinline__ int warp_sum(int v) {
 // flagged; then the Check_Out_Domain at the start of time_integration_sph
 // (SPH_MAIN_2019.f90:232, :1764-1788) and, over the particles still inside,
 // the bounds, max and mean of hsml for the cell grid.
-__global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
+// One launch: the per-particle part, block partials, and in the last block
+// the global bounds and grid_setup.
+struct BoundsPart {
+    float xmn, xmx, ymn, ymx, hmx, dtm;
+    double hsum;
+    int hcnt, bad;
+};
+
+__device__ __forceinline__ void bounds_merge(BoundsPart& a, const BoundsPart& b) {
+    a.xmn = fminf(a.xmn, b.xmn); a.xmx = fmaxf(a.xmx, b.xmx);
+    a.ymn = fminf(a.ymn, b.ymn); a.ymx = fmaxf(a.ymx, b.ymx);
+    a.hmx = fmaxf(a.hmx, b.hmx); a.dtm = fminf(a.dtm, b.dtm);
+    a.hsum += b.hsum; a.hcnt += b.hcnt; a.bad |= b.bad;
+}
+
+// Capacities and search tunables handed to grid_setup.
+struct GridArgs {
+    int cap_blocks, cap_cells, max_cells;
+    float level_factor, cell_div;
+};
+
+__device__ void grid_setup(const Rheo& c, StepScalars* S, const GridArgs ga);
+
+__global__ void __launch_bounds__(kThreadsBounds) k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S,
+                                                           BoundsPart* part, GridArgs ga) {
     if (step_skipped(S)) return;
     float xmn = 3.4e38f, xmx = -3.4e38f, ymn = 3.4e38f, ymx = -3.4e38f, hmx = 0.f, dtm = 1.e10f;
     double hs_sum = 0.0;
@@ -171,17 +198,47 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
             dtm = fminf(dtm, cc);
         }
     }
-    xmn = warp_min(xmn); xmx = warp_max(xmx); ymn = warp_min(ymn); ymx = warp_max(ymx);
-    hmx = warp_max(hmx); dtm = warp_min(dtm);
-    hs_sum = warp_sum(hs_sum);
-    hs_cnt = warp_sum(hs_cnt);
-    bad = __any_sync(0xffffffffu, bad);
-    if ((threadIdx.x & 31) == 0) {
-        atomicMin(&S->xmin_o, f2o(xmn)); atomicMax(&S->xmax_o, f2o(xmx));
-        atomicMin(&S->ymin_o, f2o(ymn)); atomicMax(&S->ymax_o, f2o(ymx));
-        atomicMax(&S->hmax_o, f2o(hmx)); atomicMin(&S->dtmin_o, f2o(dtm));
-        if (hs_cnt) { atomicAdd(&S->hsum, hs_sum); atomicAdd(&S->hcount, hs_cnt); }
-        if (bad) atomicOr(&S->bad, 1);
+    // block partials, then the last block to finish reduces them in block
+    // order (deterministic FP64 sum, no same-address atomics) and sets up
+    // the grids
+    __shared__ BoundsPart wp[kThreadsBounds / 32];
+    __shared__ bool last;
+    BoundsPart q{warp_min(xmn), warp_max(xmx), warp_min(ymn), warp_max(ymx), warp_max(hmx), warp_min(dtm),
+                 warp_sum(hs_sum), warp_sum(hs_cnt), __any_sync(0xffffffffu, bad) ? 1 : 0};
+    if ((threadIdx.x & 31) == 0) wp[threadIdx.x >> 5] = q;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        BoundsPart b = wp[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) bounds_merge(b, wp[k]);
+        part[blockIdx.x] = b;
+        __threadfence();
+        last = (atomicAdd(&S->bounds_ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    BoundsPart b{3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f, 0.f, 1.e10f, 0.0, 0, 0};
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+        BoundsPart o;
+        const volatile BoundsPart* vp = part + k;
+        o.xmn = vp->xmn; o.xmx = vp->xmx; o.ymn = vp->ymn; o.ymx = vp->ymx; o.hmx = vp->hmx; o.dtm = vp->dtm;
+        o.hsum = vp->hsum; o.hcnt = vp->hcnt; o.bad = vp->bad;
+        bounds_merge(b, o);
+    }
+    b.xmn = warp_min(b.xmn); b.xmx = warp_max(b.xmx); b.ymn = warp_min(b.ymn); b.ymx = warp_max(b.ymx);
+    b.hmx = warp_max(b.hmx); b.dtm = warp_min(b.dtm); b.hsum = warp_sum(b.hsum); b.hcnt = warp_sum(b.hcnt);
+    b.bad = __any_sync(0xffffffffu, b.bad) ? 1 : 0;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wp[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        BoundsPart t = wp[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); k++) bounds_merge(t, wp[k]);
+        S->xmin_o = f2o(t.xmn); S->xmax_o = f2o(t.xmx); S->ymin_o = f2o(t.ymn); S->ymax_o = f2o(t.ymx);
+        S->hmax_o = f2o(t.hmx); S->dtmin_o = f2o(t.dtm);
+        S->hsum = t.hsum; S->hcount = t.hcnt; S->bad = t.bad;
+        S->bounds_ticket = 0u;
+        grid_setup(c, S, ga);
     }
 }
 
@@ -197,9 +254,9 @@ __global__ void k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S) {
 // level_factor and cell_div are the search's tunables (gfsph_set_search):
 // Hc = min(max, level_factor * mean hsml) and level k's cell size is
 // Hc * 2^k / cell_div; neither changes the neighbour sets.
-__global__ void k_grid(Rheo c, StepScalars* S, int cap_blocks, int cap_cells, int max_cells, float level_factor,
-                       float cell_div) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void grid_setup(const Rheo& c, StepScalars* S, const GridArgs ga) {
+    const int cap_blocks = ga.cap_blocks, cap_cells = ga.cap_cells, max_cells = ga.max_cells;
+    const float level_factor = ga.level_factor, cell_div = ga.cell_div;
     if (S->skip) return;
     if (S->bad) { S->err |= kErrNonFinite; S->skip = 1; return; }
     float xmn = o2f(S->xmin_o), xmx = o2f(S->xmax_o), ymn = o2f(S->ymin_o), ymx = o2f(S->ymax_o);
@@ -292,27 +349,30 @@ __device__ __forceinline__ int block_of(const StepScalars* S, int k, int cx, int
 // neighbour search more tightly than the level's upper limit.
 __global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* bmark) {
     if (S->skip) return;
-    const int lane = threadIdx.x & 31;
-    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {  // warp-uniform trips
-        int i = base + threadIdx.x;
-        unsigned int h0 = 0u;
-        if (i < n && !B.flag[i]) {
-            float2 p = B.pos[i];
-            if (!out_of_box(dem, p.x, p.y)) {
-                float hs = B.hsml[i];
-                int k = level_of(hs, S);
-                int cx, cy;
-                cell_of(p, S, k, cx, cy);
-                if (S->sparse) {
-                    int b = block_of(S, k, cx, cy);
-                    if (bmark[b] == 0) bmark[b] = 1;
-                }
-                if (k == 0) h0 = f2o(hs);
-                else atomicMax(&S->lev_hmax_o[k], f2o(hs));
-            }
+    __shared__ unsigned int wmax[32];
+    unsigned int h0 = 0u;  // largest level-0 hsml seen by this thread
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (B.flag[i]) continue;
+        float2 p = B.pos[i];
+        if (out_of_box(dem, p.x, p.y)) continue;
+        float hs = B.hsml[i];
+        int k = level_of(hs, S);
+        int cx, cy;
+        cell_of(p, S, k, cx, cy);
+        if (S->sparse) {
+            int b = block_of(S, k, cx, cy);
+            if (bmark[b] == 0) bmark[b] = 1;
         }
-        h0 = __reduce_max_sync(0xffffffffu, h0);
-        if (lane == 0 && h0) atomicMax(&S->lev_hmax_o[0], h0);
+        if (k == 0) h0 = max(h0, f2o(hs));
+        else atomicMax(&S->lev_hmax_o[k], f2o(hs));
+    }
+    h0 = __reduce_max_sync(0xffffffffu, h0);
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = h0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int m = 0u;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = max(m, wmax[w]);
+        if (m) atomicMax(&S->lev_hmax_o[0], m);
     }
 }
 
