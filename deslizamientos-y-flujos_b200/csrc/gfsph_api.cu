@@ -22,7 +22,7 @@ enum KernelId {
     K_PREP, K_BOUNDS, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_TOP, K_BSCAN_ADD,
-    K_DENSITY_SPARSE, K_COUPLE, K_ADJOINT,
+    K_DENSITY_SPARSE, K_COUPLE, K_ADJOINT, K_NORM, K_NORM_BIG, K_STAGE,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
@@ -31,7 +31,7 @@ const char* kKernelNames[K_COUNT] = {
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)", "k_scan_top(blocks)",
-    "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "k_adjoint", "step_batches"};
+    "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "k_adjoint", "k_norm", "k_norm_big", "k_stage", "step_batches"};
 
 constexpr int kThreads = 128;
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
@@ -142,7 +142,10 @@ struct gfsph_handle {
     int* ncount = nullptr;
     int kcap = 0;
     float2* indv = nullptr;  // internal acceleration of every active particle
-    float* rho0 = nullptr;   // start-of-step depth (pore-water pressure update)
+    float* rho0 = nullptr;   // start-of-step depth (pore-water pressure update, normalised density)
+    // staged RK45 (nor_density or ic_cosTheta = 1)
+    StageCarry carry{};
+    float* rhoS = nullptr;   // the five depths of a step, k-major (nor_density)
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -204,8 +207,19 @@ void drop_graphs(gfsph_handle* h) {
     h->g1 = h->gK = nullptr;
 }
 
+// Adds the time of the last launch of kernel k to its profile.
+void collect_one(gfsph_handle* h, int k) {
+    float ms = 0.f;
+    cudaEventSynchronize(h->ev1[k]);
+    cudaEventElapsedTime(&ms, h->ev0[k], h->ev1[k]);
+    h->prof_ms[k] += ms;
+    h->prof_cnt[k] += 1;
+    h->pending[k] = false;
+}
+
 template <class F>
 void launch(gfsph_handle* h, int kid, F&& f) {
+    if (h->profile && h->pending[kid]) collect_one(h, kid);  // launched again before the step's collection
     if (h->profile) cudaEventRecord(h->ev0[kid], h->stream);
     f();
     if (h->profile) {
@@ -219,18 +233,15 @@ int profile_collect(gfsph_handle* h) {
     if (!h->profile) return 0;
     CK(cudaStreamSynchronize(h->stream));
     for (int k = 0; k < K_COUNT; k++)
-        if (h->pending[k]) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, h->ev0[k], h->ev1[k]);
-            h->prof_ms[k] += ms;
-            h->prof_cnt[k] += 1;
-            h->pending[k] = false;
-        }
+        if (h->pending[k]) collect_one(h, k);
     return 0;
 }
 
 // Side stream for the coarse-level kernels while a graph is captured.
 cudaStream_t side_stream(gfsph_handle* h) { return h->capturing ? h->stream2 : h->stream; }
+
+// Stage-dependent pressure: the step runs the staged RK45 kernels.
+bool staged(const gfsph_handle* h) { return h->rheo.nor_density || h->rheo.cos_theta; }
 
 void fork(gfsph_handle* h, int k) {
     if (!h->capturing) return;
@@ -309,6 +320,82 @@ int enqueue_search(gfsph_handle* h, int advance) {
     return nk;
 }
 
+// The five depths of a step with nor_density: call k of sum_density_Tools
+// reads the depths of call k-1 (rho0 for the first), clamped to h_inf after
+// the first (IntForces_SW ran in between).  Without nor_density every stage
+// uses the plain sum in A.rho.  Returns the number of kernels enqueued.
+int enqueue_norms(gfsph_handle* h, PState As[5]) {
+    const int n = h->n;
+    cudaStream_t st = h->stream;
+    const Rheo& c = h->rheo;
+    Search q = make_search(h);
+    int nk = 0;
+    for (int k = 0; k < 5; k++) {
+        As[k] = h->A;
+        if (c.nor_density) As[k].rho = h->rhoS + (size_t)k * n;
+    }
+    if (!c.nor_density) return 0;
+    for (int k = 0; k < 5; k++) {
+        const float* hp = k ? As[k - 1].rho : h->rho0;
+        const int clamp = k ? 1 : 0;
+        launch(h, K_NORM, [&] { k_norm<<<blocks_for(n), kThreads, 0, st>>>(h->A, q, h->S, c, n, hp, clamp, As[k].rho); });
+        launch(h, K_NORM_BIG, [&] {
+            k_norm_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, h->S, c, hp, clamp, As[k].rho);
+        });
+        nk += 2;
+    }
+    return nk;
+}
+
+// Pressure term of the first stage; with nor_density it takes the first
+// normalised depth.
+int enqueue_stage_begin(gfsph_handle* h, const PState As[5]) {
+    const Rheo& c = h->rheo;
+    Search q = make_search(h);
+    launch(h, K_STAGE, [&] {
+        if (c.cos_theta)
+            k_stage_begin<true><<<blocks_for(h->n), kThreads, 0, h->stream>>>(h->A, q, h->S, c, h->dem, As[0].rho);
+        else
+            k_stage_begin<false><<<blocks_for(h->n), kThreads, 0, h->stream>>>(h->A, q, h->S, c, h->dem, As[0].rho);
+    });
+    return 1;
+}
+
+// The staged RK45 body (nor_density or ic_cosTheta = 1): per stage the
+// internal force with that stage's pressure, then the stage of every
+// particle; the last stage finishes the step.  Everything on one stream.
+int enqueue_stages(gfsph_handle* h, PState As[5]) {
+    const int n = h->n;
+    cudaStream_t st = h->stream;
+    StepScalars* S = h->S;
+    const Rheo& c = h->rheo;
+    Search q = make_search(h);
+    const int pb = blocks_for(n);
+    int nk = enqueue_norms(h, As);
+    nk += enqueue_stage_begin(h, As);
+    for (int s = 0; s < 4; s++) {
+        launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, st>>>(As[s], q, S, c); }); nk++;
+        launch(h, K_IFORCE, [&] { k_iforce<<<pb, kThreads, 0, st>>>(As[s], q, S, c, n); }); nk++;
+        launch(h, K_STAGE, [&] {
+            if (s < 3) {
+                if (c.cos_theta)
+                    k_stage<true><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho, As[s + 1].rho);
+                else
+                    k_stage<false><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho,
+                                                            As[s + 1].rho);
+            } else if (c.cos_theta) {
+                k_stage_final<true><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
+                                                             h->carry, As[3].rho, As[4].rho);
+            } else {
+                k_stage_final<false><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
+                                                              h->carry, As[3].rho, As[4].rho);
+            }
+        });
+        nk++;
+    }
+    return nk;
+}
+
 int enqueue_step(gfsph_handle* h) {
     const int n = h->n;
     cudaStream_t st = h->stream;
@@ -316,6 +403,23 @@ int enqueue_step(gfsph_handle* h) {
     Search q = make_search(h);
     int pb = blocks_for(n);
     int nk = enqueue_search(h, 1);
+    if (staged(h)) {
+        PState As[5];
+        nk += enqueue_stages(h, As);
+        if (h->rheo.av_vel) {  // av_vel with the final depth
+            launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 128, 0, st>>>(As[4], q, S, h->rheo, h->B, h->velfin); });
+            launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(As[4], q, S, h->rheo, n, h->B, h->velfin); });
+            nk += 2;
+        }
+        if (h->rheo.erosion) {
+            launch(h, K_DEM_ERODE, [&] {
+                k_dem_erode<<<148 * 2, 256, 0, st>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S);
+            });
+            nk++;
+        }
+        launch(h, K_STEP_END, [&] { k_step_end<<<1, 32, 0, st>>>(S); }); nk++;
+        return nk;
+    }
     cudaStream_t sb = side_stream(h);
     fork(h, 1);
     launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); }); nk++;
@@ -354,7 +458,10 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    return 15 + 3 + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    // staged: 10 k_norm launches with nor_density, k_stage_begin, four
+    // stages of (k_force_big, k_iforce, k_stage)
+    const int body = staged(h) ? (h->rheo.nor_density ? 10 : 0) + 1 + 12 : 3;
+    return 15 + body + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
 }
 
 int alloc_blocks(gfsph_handle* h, int cap) {
@@ -405,6 +512,8 @@ void free_particles(gfsph_handle* h) {
     }
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
     dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv); dfree(h->rho0);
+    dfree(h->carry.v); dfree(h->carry.acc); dfree(h->carry.dx); dfree(h->carry.dv); dfree(h->carry.xo);
+    dfree(h->carry.out); dfree(h->rhoS);
     h->kcap = 0;
 }
 
@@ -504,9 +613,11 @@ int validate(const gfsph_params* p) {
     if (p->pa_sph != 1 && p->pa_sph != 2) return GFSPH_ERR_UNSUPPORTED;
     if (p->nnps != 2 && p->nnps != 4) return GFSPH_ERR_UNSUPPORTED;
     if (p->sle != 0 && p->sle != 1) return GFSPH_ERR_UNSUPPORTED;
-    if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
-    if (p->ic_adapt < 0 || p->ic_adapt > 2) return GFSPH_ERR_UNSUPPORTED;
-    if ((int)(p->cst[15] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;  // ic_cosTheta
+    if (p->summation_density != 1 || (p->nor_density != 0 && p->nor_density != 1)) return GFSPH_ERR_UNSUPPORTED;
+    if (p->ic_adapt != 0 && p->ic_adapt != 1 && p->ic_adapt != 2 && p->ic_adapt != 4 && p->ic_adapt != 10)
+        return GFSPH_ERR_UNSUPPORTED;
+    const int cos_theta = (int)(p->cst[15] + 0.01f);  // ic_cosTheta = const(16) (SPH_SW_2019.f90:6734)
+    if (cos_theta != 0 && cos_theta != 1) return GFSPH_ERR_UNSUPPORTED;
     const int fct = (int)(p->cst[19] + 0.1f);                          // ic_fct_dens
     if (fct != 0 && fct != 1) return GFSPH_ERR_UNSUPPORTED;
     if (p->icpwp != 0 && p->icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
@@ -587,6 +698,8 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     c.erosion = (k[20] > 1.e-9f) ? 1 : 0;
     c.skf = p->skf; c.pa_sph = p->pa_sph; c.sle = p->sle; c.av_vel = p->average_velocity ? 1 : 0;
     c.ic_adapt = p->ic_adapt;
+    c.nor_density = p->nor_density ? 1 : 0;
+    c.cos_theta = ((int)(k[15] + 0.01f) == 1) ? 1 : 0;
     pwp_factors(p, c);
     c.muI = (c.nfric == 8 || c.nfric == 26) ? 1 : (c.nfric == 27 ? 2 : 0);
     c.mu_a = k[2]; c.mu_r = k[5]; c.mu_b = k[6];
@@ -704,6 +817,12 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
         st |= dalloc(&h->cellA, n); st |= dalloc(&h->velfin, n); st |= dalloc(&h->pterm, n);
         st |= dalloc(&h->keyrank, n); st |= dalloc(&h->perm, n); st |= dalloc(&h->ncount, n);
         st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n); st |= dalloc(&h->indv, n); st |= dalloc(&h->rho0, n);
+        if (staged(h)) {
+            StageCarry& C = h->carry;
+            st |= dalloc(&C.v, n); st |= dalloc(&C.acc, n); st |= dalloc(&C.dx, n); st |= dalloc(&C.dv, n);
+            st |= dalloc(&C.xo, n); st |= dalloc(&C.out, n);
+            if (h->rheo.nor_density) st |= dalloc(&h->rhoS, 5 * (size_t)n);
+        }
         if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
         if (st) return st;
@@ -901,6 +1020,12 @@ int gfsph_density(gfsph_handle* h, float* rho_out) {
     int st = search_only(h);
     if (st) return st;
     int n = h->n;
+    if (h->rheo.nor_density) {  // the first call of the step: normalised with the depths held
+        Search q = make_search(h);
+        launch(h, K_NORM, [&] { k_norm<<<blocks_for(n), kThreads, 0, h->stream>>>(h->A, q, h->S, h->rheo, n, h->rho0, 0, h->rhoS); });
+        launch(h, K_NORM_BIG, [&] { k_norm_big<<<big_blocks(h), 128, 0, h->stream>>>(h->A, q, h->S, h->rheo, h->rho0, 0, h->rhoS); });
+        CK(cudaMemcpyAsync(h->A.rho, h->rhoS, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    }
     launch(h, K_COPY, [&] { k_copy_state<<<blocks_for(n), kThreads, 0, h->stream>>>(h->A, h->B, n); });
     if (rho_out) return gfsph_download(h, nullptr, nullptr, rho_out, nullptr, nullptr, nullptr);
     CK(cudaStreamSynchronize(h->stream));
@@ -915,8 +1040,15 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
     int n = h->n;
     cudaStream_t s = h->stream;
     Search q = make_search(h);
-    launch(h, K_IFORCE, [&] { k_iforce<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, n); });
-    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, s>>>(h->A, q, h->S, h->rheo); });
+    PState As[5];
+    if (staged(h)) {  // the first stage's depth and pressure term
+        enqueue_norms(h, As);
+        enqueue_stage_begin(h, As);
+    } else {
+        As[0] = h->A;
+    }
+    launch(h, K_IFORCE, [&] { k_iforce<<<blocks_for(n), kThreads, 0, s>>>(As[0], q, h->S, h->rheo, n); });
+    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });
     launch(h, K_FORCE_RK, [&] {
         k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 1,
                                                      h->velfin);
@@ -1388,7 +1520,7 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     if (!h->has_state) return GFSPH_ERR_STATE;
     const Rheo& c = h->rheo;
     if (!(c.nfric == 5 || c.nfric == 6) || c.xi < 0.f || c.erosion || c.icpwp != 0 || c.pa_sph != 2 || c.sle != 0 ||
-        c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f)
+        c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f || c.nor_density || c.cos_theta)
         return GFSPH_ERR_UNSUPPORTED;
     gfsph_adjoint* a = new (std::nothrow) gfsph_adjoint();
     if (!a) return GFSPH_ERR_ARG;

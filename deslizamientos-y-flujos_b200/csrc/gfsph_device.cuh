@@ -151,6 +151,9 @@ __device__ __forceinline__ void dem_lookup(const DemView& d, float xx, float yy,
 struct Rheo {
     float g, dens, xi, tauy0, constK, tanfi, hfrict0, comp, keros, slip, h_inf, cgra05;
     int nfric, erosion, skf, pa_sph, sle, av_vel, ic_adapt;
+    // stage-dependent pressure: normalised density (nor_density) and the
+    // terrain-normal gravity (ic_cosTheta = 1); either runs the staged RK45
+    int nor_density, cos_theta;
     // basal pore-water pressure (icpwp = 3) and the density factor of tanfi:
     // DFs_FSs_dens_and_pwp_factors (SPH_SW_2019.f90:8959-9060) for the
     // friction, mini_DFs_dens_and_pwp_factors (:11502-11580) for the update
@@ -188,16 +191,32 @@ __device__ __forceinline__ void ext_locals(const Rheo& c, float hdepth, float vx
     }
 }
 
-// Get_Grav_Ext_SW (SPH_SW_2019.f90:9241-9349, ic_cosTheta = 0) and
-// basal_friction_Ext_SW (:9355-9828) before its reversal filter.
+// g / sqrt(1 + |grad Z|^2), the gravity normal to the terrain of
+// ic_cosTheta = 1 (Get_Grav_Ext_SW :9264-9270, IntForces_SW :6775-6783).
+// deng = (1 + Zx^2 + Zy^2)**0.5 is taken as a correctly rounded square root.
+__device__ __forceinline__ float terrain_deng(float zpx, float zpy) { return sqrtf((1.f + zpx * zpx) + zpy * zpy); }
+
+// Get_Grav_Ext_SW (SPH_SW_2019.f90:9241-9349; ic_cosTheta = 0, or 1 when
+// COS) and basal_friction_Ext_SW (:9355-9828) before its reversal filter.
+// With ic_cosTheta = 1 the friction's gravz (gtanfi :9706, the mu(I) Froude
+// number :9658-9665) is g/deng; the Voellmy term keeps cgra = g (:9749).
+template <bool COS = false>
 __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& d, float xx, float yy, float vx,
                                                   float vy, float pwp, ExtLocal& L) {
     const bool frictional = (c.nfric >= 5 && c.nfric <= 8) || c.nfric == 26 || c.nfric == 27;
     const bool v2byr = (c.nfric == 7 || c.nfric == 8 || c.nfric == 26 || c.nfric == 27);
     float zpx, zpy, top[6];
     dem_lookup(d, xx, yy, zpx, zpy, v2byr, top);
-    L.gravx = -(c.g * zpx);
-    L.gravy = -(c.g * zpy);
+    float gz = c.g;
+    if (COS) {
+        const float deng = terrain_deng(zpx, zpy);
+        gz = c.g / deng;
+        L.gravx = -((c.g * zpx) / deng);
+        L.gravy = -((c.g * zpy) / deng);
+    } else {
+        L.gravx = -(c.g * zpx);
+        L.gravy = -(c.g * zpy);
+    }
     float hfrict = (L.h > c.hfrict0) ? L.h : c.hfrict0;
     L.frictx = 0.f; L.fricty = 0.f; L.totfrict = 0.f; L.cf5 = 0.f;
     if (c.nfric == 4) {  // Bingham regimes, :9552-9572
@@ -235,11 +254,11 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
         }
         float tanfi = c.tanfi;
         if (c.muI == 1) {  // nfric 8, 26
-            float froude = L.vmod / sqrtf(c.g * L.h);
+            float froude = L.vmod / sqrtf(gz * L.h);
             float ff = 1.f + c.mu_a * powr((froude * c.mu_r) / L.h, c.mu_b);
             tanfi = tanfi * ff;
         } else if (c.muI == 2) {  // nfric 27
-            float froude = L.vmod / sqrtf(c.g * L.h);
+            float froude = L.vmod / sqrtf(gz * L.h);
             float inert = (froude * c.mu_r) / L.h;
             tanfi = tanfi + (c.mu_a - tanfi) / (1.f + c.mu_b / inert);
         }
@@ -252,7 +271,7 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
             if (factpw > c.fact_pwp_max) factpw = c.fact_pwp_max;
             tanfi = tanfi * factpw;
         }
-        float gtanfi = ((c.g + cv2byr) * tanfi) * c.fact_dens;  // :9706
+        float gtanfi = ((gz + cv2byr) * tanfi) * c.fact_dens;  // :9706
         if (gtanfi < 0.f) gtanfi = 0.f;
         L.cf5 = gtanfi;
         L.frictx = ((L.cf5 * L.hu) * L.hvmodinv) * L.h;
@@ -312,12 +331,13 @@ __device__ __forceinline__ void reversal_filter(const Rheo& c, float dt, float v
 // External acceleration of one particle in one RK stage: ExtForces_SW(0)
 // particle loop, SPH_SW_2019.f90:8532-8716 (gravity, basal friction with the
 // reversal filter, Hungr erosion momentum :8664-8697).
+template <bool COS = false>
 __device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float dt, float xx, float yy, float vx,
                                           float vy, float hdepth, float pwp, float in0, float in1, float& ex0,
                                           float& ex1) {
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
-    grav_and_friction(c, d, xx, yy, vx, vy, pwp, L);
+    grav_and_friction<COS>(c, d, xx, yy, vx, vy, pwp, L);
     ex0 = 0.f + L.gravx;
     ex1 = 0.f + L.gravy;
     reversal_filter(c, dt, vx, vy, ex0 + in0, ex1 + in1, L);

@@ -185,17 +185,19 @@ __global__ void __launch_bounds__(kThreadsBounds) k_bounds(PState B, int n, Rheo
             hs_sum += (double)hs;
             hs_cnt += 1;
         }
-        if (c.ic_adapt == 1 || c.ic_adapt == 2) {
-            float hh = (h < c.h_inf) ? c.h_inf : h;
-            float cs = sqrtf(c.g * hh);
-            float cc = (1.e-6f > cs) ? 1.e-6f : cs;
-            if (c.ic_adapt == 2) {
-                float vv = v.x * v.x + v.y * v.y;
-                vv = sqrtf(vv);
-                cc = cc + vv;
+        if (c.ic_adapt != 0) {
+            float vv = 0.f;
+            if (c.ic_adapt != 1) vv = sqrtf(v.x * v.x + v.y * v.y);
+            if (c.ic_adapt != 4) {  // modes 1, 2, 10: hsml / (3 (c [+ |v|])) with h clamped to h_inf
+                float hh = (h < c.h_inf) ? c.h_inf : h;
+                float cs = sqrtf(c.g * hh);
+                float cc = (1.e-6f > cs) ? 1.e-6f : cs;
+                if (c.ic_adapt == 2) cc = cc + vv;
+                cc = hs / (3.f * cc);
+                dtm = fminf(dtm, cc);
             }
-            cc = hs / (3.f * cc);
-            dtm = fminf(dtm, cc);
+            if (c.ic_adapt == 4 || c.ic_adapt == 10)  // |DEM cell diagonal| / |v|, +inf at rest
+                dtm = fminf(dtm, sqrtf(dem.dx * dem.dx + dem.dy * dem.dy) / vv);
         }
     }
     // block partials, then the last block to finish reduces them in block
@@ -264,7 +266,7 @@ __device__ void grid_setup(const Rheo& c, StepScalars* S, const GridArgs ga) {
     if (S->xmin_o == 0xffffffffu || !(hmx > 0.f) || S->hcount == 0) { S->err |= kErrEmpty; S->skip = 1; return; }
     float dt = S->dt;
     if (S->advance) {
-        float dtmin = (c.ic_adapt == 1 || c.ic_adapt == 2) ? o2f(S->dtmin_o) : 1.e10f;
+        float dtmin = (c.ic_adapt != 0) ? o2f(S->dtmin_o) : 1.e10f;
         if (dtmin < dt) dt = dtmin;
         else if (c.ic_adapt != 0) dt = fminf(1.1f * dt, dtmin);
     }
@@ -563,8 +565,9 @@ __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, int*
 }
 
 // Gathers the state into the new (cell-sorted) order.
-// With icpwp = 3 also the pore-water pressure and rho0, the depth RK45 keeps
-// at its start (after the h_inf clamp of Adaptive_dt_sph_SW :6540, modes 1-2).
+// With icpwp = 3 also the pore-water pressure; with icpwp = 3 or nor_density
+// rho0, the depth RK45 keeps at its start (after the h_inf clamp of
+// Adaptive_dt_sph_SW :6540, modes 1, 2 and 10).
 __global__ void k_reorder(const PState B, int n, const int* perm, const int2* keyrank, PState A, int* cellA,
                           float4* xhm, const StepScalars* S, Rheo c, float* rho0) {
     if (S->skip) return;
@@ -576,10 +579,9 @@ __global__ void k_reorder(const PState B, int n, const int* perm, const int2* ke
         A.pos[s] = p;
         A.vel[s] = B.vel[o];
         A.rho[s] = r;
-        if (c.icpwp == 3) {
-            A.pwp[s] = B.pwp[o];
-            rho0[s] = ((c.ic_adapt == 1 || c.ic_adapt == 2) && r < c.h_inf) ? c.h_inf : r;
-        }
+        if (c.icpwp == 3) A.pwp[s] = B.pwp[o];
+        if (c.icpwp == 3 || c.nor_density)
+            rho0[s] = ((c.ic_adapt == 1 || c.ic_adapt == 2 || c.ic_adapt == 10) && r < c.h_inf) ? c.h_inf : r;
         A.mass[s] = m;
         A.hsml[s] = hs;
         A.flag[s] = B.flag[o];
@@ -955,6 +957,53 @@ __device__ __forceinline__ void erosion_scatter(const DemView& dem, StepScalars*
     }
 }
 
+// A particle out of the domain at the start of the step: copied through.
+__device__ __forceinline__ void rk_carry(const PState& A, const Rheo& c, const PState& B, float2* velfin, int i) {
+    B.pos[i] = A.pos[i]; B.vel[i] = A.vel[i]; velfin[i] = A.vel[i];
+    B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
+    B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
+    if (c.icpwp == 3) B.pwp[i] = 0.f;  // Get_Pwp_SW zeroes out-of-domain particles
+}
+
+// The end of the RK45 body of an active particle: the final update
+// (SPH_MAIN_2019.f90:908-922), Check_Out_Domain, Hungr erosion of the mass
+// and the DEM scatter of ExtForces_SW(1) (SPH_SW_2019.f90:8717-8760),
+// h_upgrade (:2925-2931) and the pore-pressure update, written to B.  h is
+// the step's final depth; (xx, xy, vx, vy) the last stage's state, kept as
+// the result when the particle left the domain in a stage (out).  Every lane
+// of the warp must call it (erosion_scatter).
+__device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, StepScalars* S, const Rheo& c,
+                                          const DemView& dem, const PState& B, float2* velfin, double2* auxv, int i,
+                                          float dt, float2 x0, float2 v0, float Dx0, float Dx1, float Dv0, float Dv1,
+                                          float xx, float xy, float vx, float vy, bool out, float h, float pwp) {
+    float m = A.mass[i];
+    float hs = A.hsml[i];
+    if (!out) {
+        float dt6 = dt / 6.f;
+        xx = x0.x + dt6 * Dx0;
+        xy = x0.y + dt6 * Dx1;
+        vx = v0.x + dt6 * Dv0;
+        vy = v0.y + dt6 * Dv1;
+        out = out_of_box(dem, xx, xy);
+    }
+    float er = 0.f;
+    if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h, pwp);
+    if (c.erosion) erosion_scatter(dem, S, xx, xy, dt * er, !out, auxv);
+    if (!out) {
+        if (c.erosion) m = m + ((dt * er) * m) / h;
+        if (c.sle == 1) hs = 2.f * sqrtf(m / h);
+    }
+    B.pos[i] = make_float2(xx, xy);
+    velfin[i] = make_float2(vx, vy);
+    B.vel[i] = make_float2(vx, vy);
+    B.rho[i] = h;
+    B.mass[i] = m;
+    B.hsml[i] = hs;
+    B.flag[i] = out ? 1 : 0;
+    B.id[i] = A.id[i];
+    if (c.icpwp == 3) B.pwp[i] = out ? 0.f : pwp_update(c, pwp, h, h - Q.rho0[i], dt);
+}
+
 // Internal acceleration of the level-0 particles, one thread each.
 __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip) return;
@@ -999,10 +1048,7 @@ __global__ void __launch_bounds__(128, 7) k_force_rk(PState A, Search Q, StepSca
             continue;
         }
         if (i >= nact) {  // carried particles (out of the domain at step start)
-            B.pos[i] = A.pos[i]; B.vel[i] = A.vel[i]; velfin[i] = A.vel[i];
-            B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
-            B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
-            if (c.icpwp == 3) B.pwp[i] = 0.f;  // Get_Pwp_SW zeroes out-of-domain particles
+            rk_carry(A, c, B, velfin, i);
             if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
             continue;
         }
@@ -1038,32 +1084,220 @@ __global__ void __launch_bounds__(128, 7) k_force_rk(PState A, Search Q, StepSca
                 }
             }
         }
-        float m = A.mass[i];
-        float hs = A.hsml[i];
-        if (!out) {
-            float dt6 = dt / 6.f;
-            xx = x0.x + dt6 * Dx0;
-            xy = x0.y + dt6 * Dx1;
-            vx = v0.x + dt6 * Dv0;
-            vy = v0.y + dt6 * Dv1;
-            out = out_of_box(dem, xx, xy);
+        rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, Dx0, Dx1, Dv0, Dv1, xx, xy, vx, vy, out, h, pwp);
+    }
+}
+
+// ---------------------------------------------------------------- staged RK45
+// With nor_density or ic_cosTheta = 1 the pressure changes from stage to
+// stage: each sum_density_Tools call divides the plain sum by
+// sum_j (m_j/h_j) W_ij taken with the depths of the call before it
+// (My_SPH_Tools_2019.f90:1790-1846), and ic_cosTheta = 1 takes g/deng at each
+// stage's position (IntForces_SW :6775-6783).  The step then runs stage by
+// stage.  The five depths of the step (four stages and the sum after the
+// final update) depend only on the frozen W_ij, the masses and the depths
+// before them, so they are computed first (k_norm); then each stage runs the
+// internal force over the neighbour table with that stage's pressure term
+// and the RK stage of every particle (k_stage), whose state is carried in
+// HBM between the launches; the last stage also finishes the step
+// (k_stage_final).  The pressure term of stage s+1 is written by stage s,
+// once the particle's stage position is known.
+
+// RK45 state carried between the stage launches (slot order).
+struct StageCarry {
+    float2* v;    // velocity of the last stage
+    float2* acc;  // ex + in of the last stage
+    float2* dx;   // Dx_RK
+    float2* dv;   // Dvx_RK
+    float2* xo;   // stage position of a particle that left the DEM box
+    int* out;     // 1 once it has (it is frozen for the rest of the step)
+};
+
+// Depth of the previous sum_density_Tools call as the next one reads it:
+// clamped to h_inf when IntForces_SW (:6769) has run in between.
+__device__ __forceinline__ float prev_depth(const Rheo& c, const float* hp, int j, int clamp_prev) {
+    float h = __ldg(hp + j);
+    return (clamp_prev && h < c.h_inf) ? c.h_inf : h;
+}
+
+// One normalised sum_density_Tools call for the level-0 particles, over the
+// neighbour table: h_i = num_i / (W(0,h_i) m_i/hp_i + sum_j (m_j/hp_j) W_ij),
+// num_i the plain sum of k_density (in A.rho), hp the previous call's depths.
+__global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S, Rheo c, int n, const float* hp,
+                                              int clamp_prev, float* hout) {
+    if (S->skip) return;
+    const int nreg = S->nreg;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
+        const float4 me = Q.xhm[i];
+        const float2 xi = make_float2(me.x, me.y);
+        const float hi = me.z;
+        double den = (double)((sph_kernel_w(c.skf, 0.f, hi) * me.w) / prev_depth(c, hp, i, clamp_prev));
+        const int cnt = Q.ncount[i];
+        const int* tab = Q.nbr + i;
+        for (int k = 0; k < cnt; k++) {
+            const int j = __ldg(tab + (size_t)k * n);
+            const float4 o = __ldg(&Q.xhm[j]);
+            PairGeom g;
+            pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
+            den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w(c.skf, g.r, g.mh));
         }
-        float er = 0.f;
-        if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h, pwp);
-        if (c.erosion) erosion_scatter(dem, S, xx, xy, dt * er, !out, auxv);
-        if (!out) {
-            if (c.erosion) m = m + ((dt * er) * m) / h;
-            if (c.sle == 1) hs = 2.f * sqrtf(m / h);
+        hout[i] = A.rho[i] / (float)den;
+    }
+}
+
+// The same for the level >= 1 particles, one warp each.
+__global__ void __launch_bounds__(128) k_norm_big(PState A, Search Q, StepScalars* S, Rheo c, const float* hp,
+                                                  int clamp_prev, float* hout) {
+    if (S->skip) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int b = warp; b < nbig; b += nwarps) {
+        const int i = nreg + b;
+        double den = 0.0;
+        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+            den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w(c.skf, g.r, g.mh));
+        });
+        den = warp_sum(den);
+        if (lane == 0) {
+            const float4 me = Q.xhm[i];
+            den = (double)((sph_kernel_w(c.skf, 0.f, me.z) * me.w) / prev_depth(c, hp, i, clamp_prev)) + den;
+            hout[i] = A.rho[i] / (float)den;
         }
-        B.pos[i] = make_float2(xx, xy);
-        velfin[i] = make_float2(vx, vy);
-        B.vel[i] = make_float2(vx, vy);
-        B.rho[i] = h;
-        B.mass[i] = m;
-        B.hsml[i] = hs;
-        B.flag[i] = out ? 1 : 0;
-        B.id[i] = A.id[i];
-        if (c.icpwp == 3) B.pwp[i] = out ? 0.f : pwp_update(c, pwp, h, h - Q.rho0[i], dt);
+    }
+}
+
+// Pressure term of IntForces_SW for depth h at (xx, yy): h clamped to h_inf
+// (:6769), p = (g_z/2) h^2 (:6797) with g_z = g/deng there when COS
+// (:6775-6783); p/h^2 for pa_sph 2, p for pa_sph 1.
+template <bool COS>
+__device__ __forceinline__ float stage_pterm(const Rheo& c, const DemView& dem, float h, float xx, float yy) {
+    const float hc = (h < c.h_inf) ? c.h_inf : h;
+    float cg05 = c.cgra05;
+    if (COS) {
+        float zpx, zpy, top[6];
+        dem_lookup(dem, xx, yy, zpx, zpy, false, top);
+        cg05 = 0.5f * (c.g / terrain_deng(zpx, zpy));
+    }
+    const float p = (cg05 * hc) * hc;
+    return (c.pa_sph == 1) ? p : p / (hc * hc);
+}
+
+// Pressure term of the first stage (positions of the step start).
+template <bool COS>
+__global__ void __launch_bounds__(128) k_stage_begin(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
+                                                     const float* h1) {
+    if (S->skip) return;
+    const int nact = S->nactive;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
+        const float2 p = A.pos[i];
+        Q.pterm[i] = stage_pterm<COS>(c, dem, h1[i], p.x, p.y);
+    }
+}
+
+// RK45 stage s = 0, 1, 2 of every active particle (SPH_MAIN_2019.f90:808-906):
+// x = x0 + c_s dt v, v = v0 + c_s dt (ex + in), the out-of-domain check,
+// ExtForces_SW(0) with the stage depth hs_ (clamped as IntForces_SW leaves
+// it) and the internal acceleration of this stage, the Dx/Dv sums; then the
+// pressure term of stage s+1 at its position with depth hnext.  A particle
+// that will leave the domain in stage s+1 keeps its old term, as IntForces_SW
+// skips it.
+template <bool COS>
+__global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
+                                               StageCarry C, int s, const float* hs_, const float* hnext) {
+    if (S->skip) return;
+    const int nact = S->nactive;
+    const float dt = S->dt_step;
+    const float f1 = (s == 0) ? 0.f : 0.5f, f2 = (s == 0) ? 1.f : 2.f;
+    const float f1n = (s == 2) ? 1.f : 0.5f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
+        if (s > 0 && C.out[i]) continue;
+        const float2 x0 = A.pos[i], v0 = A.vel[i];
+        float2 vp = v0, ap = make_float2(0.f, 0.f), dx = make_float2(0.f, 0.f), dv = make_float2(0.f, 0.f);
+        if (s > 0) { vp = C.v[i]; ap = C.acc[i]; dx = C.dx[i]; dv = C.dv[i]; }
+        const float fdt = f1 * dt;
+        const float xx = x0.x + fdt * vp.x, xy = x0.y + fdt * vp.y;
+        const float vx = v0.x + fdt * ap.x, vy = v0.y + fdt * ap.y;
+        if (out_of_box(dem, xx, xy)) {
+            C.out[i] = 1;
+            C.xo[i] = make_float2(xx, xy);
+            C.v[i] = make_float2(vx, vy);
+            continue;
+        }
+        if (s == 0) C.out[i] = 0;
+        const float h = hs_[i];
+        const float hc = (h < c.h_inf) ? c.h_inf : h;
+        const float2 fin = Q.indv[i];
+        const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
+        float ex0, ex1;
+        ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
+        const float a0 = ex0 + fin.x, a1 = ex1 + fin.y;
+        dv.x = dv.x + f2 * a0;
+        dv.y = dv.y + f2 * a1;
+        dx.x = dx.x + f2 * vx;
+        dx.y = dx.y + f2 * vy;
+        C.v[i] = make_float2(vx, vy);
+        C.acc[i] = make_float2(a0, a1);
+        C.dx[i] = dx;
+        C.dv[i] = dv;
+        const float fdn = f1n * dt;
+        const float nx_ = x0.x + fdn * vx, ny_ = x0.y + fdn * vy;
+        if (!out_of_box(dem, nx_, ny_)) Q.pterm[i] = stage_pterm<COS>(c, dem, hnext[i], nx_, ny_);
+    }
+}
+
+// The last stage (s = 3) and the end of the step (rk_finish) with the final
+// depth hfin.
+template <bool COS>
+__global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
+                                                     PState B, float2* velfin, double2* auxv, StageCarry C,
+                                                     const float* h4, const float* hfin) {
+    if (S->skip) return;
+    const int nact = S->nactive;
+    const float dt = S->dt_step;
+    // block-uniform trip count: every lane of a warp reaches erosion_scatter
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        if (i >= n) {
+            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
+            continue;
+        }
+        if (i >= nact) {
+            rk_carry(A, c, B, velfin, i);
+            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
+            continue;
+        }
+        const float2 x0 = A.pos[i], v0 = A.vel[i];
+        const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
+        bool out = C.out[i] != 0;
+        float xx, xy, vx, vy;
+        float2 dx = make_float2(0.f, 0.f), dv = make_float2(0.f, 0.f);
+        if (out) {
+            const float2 xo = C.xo[i], vo = C.v[i];
+            xx = xo.x; xy = xo.y; vx = vo.x; vy = vo.y;
+        } else {
+            const float2 vp = C.v[i], ap = C.acc[i];
+            dx = C.dx[i];
+            dv = C.dv[i];
+            const float fdt = 1.f * dt;
+            xx = x0.x + fdt * vp.x; xy = x0.y + fdt * vp.y;
+            vx = v0.x + fdt * ap.x; vy = v0.y + fdt * ap.y;
+            if (out_of_box(dem, xx, xy)) {
+                out = true;
+            } else {
+                const float h = h4[i];
+                const float hc = (h < c.h_inf) ? c.h_inf : h;
+                const float2 fin = Q.indv[i];
+                float ex0, ex1;
+                ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
+                dv.x = dv.x + 1.f * (ex0 + fin.x);
+                dv.y = dv.y + 1.f * (ex1 + fin.y);
+                dx.x = dx.x + 1.f * vx;
+                dx.y = dx.y + 1.f * vy;
+            }
+        }
+        rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, dx.x, dx.y, dv.x, dv.y, xx, xy, vx, vy, out,
+                  hfin[i], pwp);
     }
 }
 

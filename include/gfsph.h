@@ -53,8 +53,10 @@ extern "C" {
  * (read in blocks of 15 by Input_SW, SPH_SW_2019.f90:1151-1204).  The ones the
  * step uses: const(1) g, const(2) density, const(3) Voellmy xi (or Manning),
  * const(5) nfric, const(6) Bingham yield stress, const(7) Bingham viscosity,
- * const(9) tan(phi), const(10) hfrict0, const(15) comp, const(16) cos-theta
- * switch (must be 0), const(20) density-factor switch (must be 0), const(21)
+ * const(9) tan(phi), const(10) hfrict0, const(15) comp, const(16) ic_cosTheta
+ * (0 g, 1 g/sqrt(1+|grad Z|^2) in the pressure and the friction, IntForces_SW
+ * SPH_SW_2019.f90:6775-6783, Get_Grav_Ext_SW :9264-9270), const(20)
+ * density-factor switch (0 or 1), const(21)
  * erosion law (1 = Hungr), const(22) Hungr constant, const(47) slip factor
  * alpha, const(48) maximum erodible depth.
  */
@@ -66,8 +68,10 @@ typedef struct gfsph_params {
     int skf;               /* 1 cubic spline, 4 Wendland C2 (kernel_TOOLS My_SPH_Tools_2019.f90:2062) */
     int summation_density; /* must be 1 (sum_density_Tools) */
     int average_velocity;  /* 1 applies av_vel (XSPH, SPH_MAIN_2019.f90:3042-3099) */
-    int nor_density;       /* must be 0 */
-    int ic_adapt;          /* ic_adapt_dt_sph: 0 fixed, 1 hsml/(3c), 2 hsml/(3(c+|v|)) */
+    int nor_density;       /* 1 divides each density sum by sum_j (m_j/h_j) W_ij
+                              (sum_density_Tools My_SPH_Tools_2019.f90:1841-1846) */
+    int ic_adapt;          /* ic_adapt_dt_sph: 0 fixed, 1 hsml/(3c), 2 hsml/(3(c+|v|)),
+                              4 |DEM cell diagonal|/|v|, 10 min of modes 1 and 4 */
     float h_inf;           /* h_inf_SW */
     float dt;              /* initial dt_sph */
     int dem_deriv;         /* slopes when not supplied: 0 FEM projection (Get_Topol), 1 finite differences */
@@ -148,9 +152,10 @@ int gfsph_set_time(gfsph_handle* h, double t, float dt);
 
 /* Summation density on the current state without advancing it: the
  * neighbour search of grid_find_NEW_tools (My_SPH_Tools_2019.f90:1109-1370)
- * followed by sum_density_Tools (My_SPH_Tools_2019.f90:1763-1859).  Writes h
- * per particle (original order) and keeps the neighbour table for
- * gfsph_neighbours. */
+ * followed by sum_density_Tools (My_SPH_Tools_2019.f90:1763-1859); with
+ * nor_density normalised with the depths held (after the h_inf clamp of
+ * adaptive dt modes 1, 2 and 10).  Writes h per particle (original order) and
+ * keeps the neighbour table for gfsph_neighbours. */
 int gfsph_density(gfsph_handle* h, float* rho_out);
 
 /* Neighbour sets of the last search (start of the last step, or
@@ -161,7 +166,9 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx);
 
 /* Per-particle internal (pressure) acceleration of IntForces_SW
  * (SPH_SW_2019.f90:6669-6941) on the current state, (2,n), original order.
- * Runs the search and density first. */
+ * Runs the search and density first (the first RK45 stage's pressure: with
+ * nor_density the normalised depth, with ic_cosTheta = 1 g/deng at the
+ * particles' positions). */
 int gfsph_internal_forces(gfsph_handle* h, float* indvxdt);
 
 /* One raster per DEM node, nx*ny values, x fastest. */

@@ -46,7 +46,8 @@
  *   - Get_Z_Topo (SPH_FEM_topo_2019.f90:2420-2432) only warns when a point
  *     maps to the last node column/row and then reads the next row; the cell
  *     index is clamped to the last cell instead.
- *   - hsml = 2*(m/h)**(1./2) is evaluated with a correctly rounded sqrt.
+ *   - hsml = 2*(m/h)**(1./2) and deng = (1 + Zx^2 + Zy^2)**0.5 of
+ *     ic_cosTheta = 1 are evaluated with a correctly rounded sqrt.
  *   - Pair traversal order: generation order of grid_find (the linked list's
  *     order depends on the node-reuse history of earlier steps).
  */
@@ -161,7 +162,7 @@ struct Oracle {
     /* options */
     const gfsph_params* P;
     R cst[GFSPH_NCONST + 1]; /* 1-based like const(k) */
-    int nfric, ic_erosion;
+    int nfric = 0, ic_erosion = 0, ic_costheta = 0;
     /* DEM */
     int nx, ny, npoig;
     R xming, yming, dxg, dyg, xmaxg, ymaxg;
@@ -198,23 +199,31 @@ struct Oracle {
         }
     }
 
-    /* Adaptive_dt_sph_SW, SPH_SW_2019.f90:6521-6664 (modes 0, 1, 2) */
+    /* Adaptive_dt_sph_SW, SPH_SW_2019.f90:6521-6664 (modes 0, 1, 2, 4, 10).
+     * Modes 1, 2 and 10 clamp the depth to h_inf in place; mode 4 does not.
+     * dxg_mod = (dx^2 + dy^2)**0.5 is taken as a square root. */
     void adaptive_dt() {
         R dtmin = lit<R>(1.e10);
         R cgra = cst[1];
-        if (P->ic_adapt == 1 || P->ic_adapt == 2) {
+        const int mode = P->ic_adapt;
+        const R dxg_mod = std::sqrt(dxg * dxg + dyg * dyg);
+        if (mode == 1 || mode == 2 || mode == 4 || mode == 10) {
             for (int i = 0; i < n; i++) {
                 if (flag[i]) continue;
-                if (rho[i] < (R)P->h_inf) rho[i] = (R)P->h_inf;
-                R c = std::sqrt(cgra * rho[i]);
-                R cc = rmax<R>(lit<R>(1.e-6), c);
-                if (P->ic_adapt == 2) {
-                    R vv = v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1];
-                    vv = std::sqrt(vv);
-                    cc = cc + vv;
+                R vv = 0;
+                if (mode != 1) vv = std::sqrt(v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1]);
+                if (mode != 4) {
+                    if (rho[i] < (R)P->h_inf) rho[i] = (R)P->h_inf;
+                    R c = std::sqrt(cgra * rho[i]);
+                    R cc = rmax<R>(lit<R>(1.e-6), c);
+                    if (mode == 2) cc = cc + vv;
+                    cc = hsml[i] / ((R)3 * cc);
+                    dtmin = rmin<R>(cc, dtmin);
                 }
-                cc = hsml[i] / ((R)3 * cc);
-                dtmin = rmin<R>(cc, dtmin);
+                if (mode == 4 || mode == 10) {
+                    R cc = dxg_mod / vv;  /* +inf for a particle at rest */
+                    dtmin = rmin<R>(cc, dtmin);
+                }
             }
         }
         if (dtmin < dt) dt = dtmin;
@@ -322,30 +331,57 @@ struct Oracle {
          * are soil (itype 1), every pair is type 0 and keeps its order. */
     }
 
-    /* sum_density_Tools, My_SPH_Tools_2019.f90:1763-1859 (nor_density = F) */
+    /* sum_density_Tools, My_SPH_Tools_2019.f90:1763-1859.  With nor_density
+     * (:1841-1846) the sum is divided by wi = W(0,h_i) m_i/rho_i +
+     * sum_j (m_j/rho_j) W_ij (:1793-1810), taken with the depths of the
+     * previous call (after IntForces_SW's in-place h_inf clamp). */
     void sum_density() {
-        std::vector<A> acc(n);
+        std::vector<A> acc(n), wi;
+        const bool nor = P->nor_density != 0;
+        if (nor) wi.assign(n, (A)0);
         for (int i = 0; i < n; i++) {
             if (flag[i]) { acc[i] = (A)rho[i]; continue; }
             R sd = self_density_w<R>(P->skf, hsml[i]);
+            if (nor) wi[i] = (A)((sd * mass[i]) / rho[i]);
             acc[i] = (A)(sd * mass[i]);
         }
+        if (nor)
+            for (size_t k = 0; k < pairs.size(); k++) {
+                int i = pairs[k].i, j = pairs[k].j;
+                wi[i] = wi[i] + (A)((mass[j] / rho[j]) * pw[k]);
+                wi[j] = wi[j] + (A)((mass[i] / rho[i]) * pw[k]);
+            }
         for (size_t k = 0; k < pairs.size(); k++) {
             int i = pairs[k].i, j = pairs[k].j;
             acc[i] = acc[i] + (A)(mass[j] * pw[k]);
             acc[j] = acc[j] + (A)(mass[i] * pw[k]);
         }
         for (int i = 0; i < n; i++) rho[i] = (R)acc[i];
+        if (nor)
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                rho[i] = rho[i] / (R)wi[i];
+            }
     }
 
+    /* deng = (1 + Zx^2 + Zy^2)**0.5 of ic_cosTheta = 1 (taken as a square root) */
+    R terrain_deng(R zpx, R zpy) { return std::sqrt(((R)1 + zpx * zpx) + zpy * zpy); }
+
     /* IntForces_SW, SPH_SW_2019.f90:6669-6941 (ic_ws_Interact = 0, ic_SWalg = 0,
-     * ic_cosTheta = 0, no K0, no end-solid law) */
+     * no K0, no end-solid law).  ic_cosTheta = 1 (:6775-6783): the pressure
+     * of each particle takes g/deng at its current position. */
     void int_forces() {
         R cgra05 = cst[1] * lit<R>(0.5); /* gravz*0.5, gravz = const(1) */
         for (int i = 0; i < n; i++)
             if (rho[i] < (R)P->h_inf) rho[i] = (R)P->h_inf; /* :6769 */
         for (int i = 0; i < n; i++) {
             if (flag[i]) continue;
+            if (ic_costheta == 1) {
+                R zp, zpx, zpy, top[6];
+                get_z_topo(x[2 * i], x[2 * i + 1], zp, zpx, zpy, top, false);
+                R gravz = cst[1] / terrain_deng(zpx, zpy);
+                cgra05 = lit<R>(0.5) * gravz;
+            }
             p[i] = (cgra05 * rho[i]) * rho[i]; /* :6797 */
         }
         std::vector<A> a0(n, (A)0), a1(n, (A)0);
@@ -430,9 +466,16 @@ struct Oracle {
         bool v2byr = (nfric == 7 || nfric == 8 || nfric == 26 || nfric == 27);
         R zp, zpx, zpy;
         get_z_topo(x[2 * i], x[2 * i + 1], zp, zpx, zpy, top, v2byr);
-        L.gravz = cgra;
-        L.gravx = -(cgra * zpx);
-        L.gravy = -(cgra * zpy);
+        if (ic_costheta == 1) { /* :9264-9270 */
+            R deng = terrain_deng(zpx, zpy);
+            L.gravz = cgra / deng;
+            L.gravx = -((cgra * zpx) / deng);
+            L.gravy = -((cgra * zpy) / deng);
+        } else {
+            L.gravz = cgra;
+            L.gravx = -(cgra * zpx);
+            L.gravy = -(cgra * zpy);
+        }
         R hfrict = rmax<R>(L.h, cst[10]);
         L.frictx = 0; L.fricty = 0; L.totfrict = 0; L.cf5 = 0;
         R dens = cst[2];
@@ -744,6 +787,8 @@ struct Oracle {
         cst[0] = 0;
         for (int k = 1; k <= GFSPH_NCONST; k++) cst[k] = (R)P->cst[k - 1];
         nfric = (int)(cst[5] + lit<R>(0.01));
+        ic_costheta = (int)(cst[16] + lit<R>(0.01)); /* SPH_SW_2019.f90:6734 */
+        if (ic_costheta != 0 && ic_costheta != 1) return GFSPH_ERR_UNSUPPORTED;
         ic_erosion = (cst[21] > lit<R>(1.e-9)) ? 1 : 0;
         if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
         if (ic_erosion && (int)(cst[21] + lit<R>(0.1)) != 1) return GFSPH_ERR_UNSUPPORTED;
@@ -1340,7 +1385,7 @@ int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, dou
                double* pwp, int pwp_init, int nsteps, double* dt, double* t, double t_end, int* steps_done) {
     if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || !dt || !t || n < 0 || nx < 2 || ny < 2)
         return GFSPH_ERR_ARG;
-    if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
+    if (p->summation_density != 1) return GFSPH_ERR_UNSUPPORTED;
     switch (mode) {
     case 0: return run_mode<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
     case 1: return run_mode<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
@@ -1399,7 +1444,7 @@ void* oracle_new(int mode, const gfsph_params* p, int nx, int ny, double xmin, d
                  int* status) {
     *status = GFSPH_ERR_ARG;
     if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || n < 0 || nx < 2 || ny < 2) return nullptr;
-    if (p->summation_density != 1 || p->nor_density != 0) { *status = GFSPH_ERR_UNSUPPORTED; return nullptr; }
+    if (p->summation_density != 1) { *status = GFSPH_ERR_UNSUPPORTED; return nullptr; }
     switch (mode) {
     case 0: return make_obj<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);
     case 1: return make_obj<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);

@@ -83,6 +83,17 @@ def test_adjoint_refuses_runs_outside_its_scope(gfsph_lib, oracle_mod):
         gfsph.Adjoint(sim, 5)
     assert e.value.status == gfsph.ERR_UNSUPPORTED
     sim.close()
+    # stage-dependent pressure (nor_density, ic_cosTheta = 1)
+    w = workloads.fractal_channel(n_target=1000, dem_k=8, cell=5.0, erosion=None)
+    for const, opts in (({}, {"nor_density": 1}), ({16: 1.0}, {})):
+        w.const = {**w.const, **const}
+        p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0, **opts)
+        sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+        sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+        with pytest.raises(gfsph.GfsphError) as e:
+            gfsph.Adjoint(sim, 5)
+        assert e.value.status == gfsph.ERR_UNSUPPORTED
+        sim.close()
     # a release that reaches past the DEM edge: particles leave the box
     w = workloads.fractal_channel(n_target=1000, dem_k=7, cell=5.0, erosion=None)
     p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)

@@ -430,6 +430,102 @@ def test_rheologies_match_oracle(gfsph_lib, oracle_mod, rheo):
     sim.close()
 
 
+STAGED = {
+    "nor_density": ({}, {"nor_density": 1}),
+    "cos_theta": ({16: 1.0}, {}),
+    "both_pa1": ({16: 1.0}, {"nor_density": 1, "pa_sph": 1}),
+}
+
+
+@pytest.mark.parametrize("case", sorted(STAGED))
+def test_staged_pressure_options_match_oracle(gfsph_lib, oracle_mod, case):
+    """nor_density (sum_density_Tools :1841-1846) and ic_cosTheta = 1
+    (IntForces_SW :6775-6783, Get_Grav_Ext_SW :9264-9270): the pressure then
+    changes from stage to stage and the step runs stage by stage; 1 and 20
+    steps of the channel release (with Hungr erosion and the curvature term)
+    against the oracle in the GPU's precision scheme."""
+    const, opts = STAGED[case]
+    w = small_channel()
+    w.const = {**w.const, **const, 5: 7}
+    sim, st, p = setup_pair(w, oracle_mod, **opts)
+    ny, nx = w.z.shape
+    for nsteps in (1, 19):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        tol = 1e-6 if nsteps == 1 else 1e-5
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass), ("hsml", st.hsml)):
+            assert rel_l2(g[key], ref) <= tol, (key, nsteps, rel_l2(g[key], ref))
+    t, dt = sim.time()
+    assert abs(t - st.t) <= 1e-6 * st.t
+    sim.close()
+
+
+def test_staged_options_change_the_flow(gfsph_lib, oracle_mod):
+    """The options are live: 20 steps with nor_density or ic_cosTheta = 1
+    end elsewhere than the plain run."""
+    out = {}
+    for case, (const, opts) in [("plain", ({}, {})), *STAGED.items()]:
+        wc = workloads.fractal_channel(n_target=6000, dem_k=8, cell=5.0)
+        wc.const = {**wc.const, **const}
+        sim, _, _ = setup_pair(wc, oracle_mod, **opts)
+        sim.step(20)
+        out[case] = sim.download()
+        sim.close()
+    for case in STAGED:
+        assert rel_l2(out[case]["x"], out["plain"]["x"]) > 1e-6, case
+
+
+def test_normalised_density_and_forces_match_oracle(gfsph_lib, oracle_mod):
+    """One normalised sum_density_Tools call on the uploaded depths and the
+    internal force that follows, against the oracle (mode 1)."""
+    for w in (workloads.inclined_plane(), small_channel()):
+        sim, st, p = setup_pair(w, oracle_mod, nor_density=1)
+        rho_g = sim.density()
+        ref = oracle_mod.pairs(oracle_mod.MODE_FP32_DACC, p, w.x, w.hsml, mass=w.mass, rho=w.rho,
+                               want_sets=False, want_rho=True, want_force=True)
+        assert max_rel(rho_g, ref["rho"]) <= 1e-6
+        sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+        f_g = sim.internal_forces()
+        scale = np.abs(ref["force"]).max()
+        assert np.abs(f_g - ref["force"]).max() <= 1e-6 * scale
+        sim.close()
+
+
+def test_staged_profile_counts_launches(gfsph_lib, oracle_mod):
+    w = small_channel()
+    sim, _, _ = setup_pair(w, oracle_mod, nor_density=1)
+    sim.profile(True)
+    sim.step(3)
+    prof = sim.profile_read()
+    # per step: 5 normalised sums, k_stage_begin + 3 stages + the last, 4 internal forces
+    assert prof["k_norm"][1] == 15 and prof["k_stage"][1] == 15 and prof["k_iforce"][1] == 12
+    assert "k_force_rk" not in prof or prof["k_force_rk"][1] == 0
+    sim.close()
+
+
+@pytest.mark.parametrize("mode", [1, 2, 4, 10])
+def test_adaptive_dt_modes_match_oracle(gfsph_lib, oracle_mod, mode):
+    """Adaptive_dt_sph_SW modes 1, 2, 4 (DEM cell diagonal / |v|) and 10
+    (the smaller of 1 and 4) over 30 steps of the channel release: the same
+    dt sequence and state as the oracle in the GPU's precision scheme."""
+    w = small_channel()
+    sim, st, p = setup_pair(w, oracle_mod, ic_adapt=mode, dt=0.05)
+    ny, nx = w.z.shape
+    for nsteps in (1, 9, 20):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        t, dt = sim.time()
+        assert abs(dt - st.dt) <= 1e-6 * st.dt, (nsteps, dt, st.dt)
+        assert abs(t - st.t) <= 1e-6 * st.t, (nsteps, t, st.t)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho)):
+            assert rel_l2(g[key], ref) <= 1e-5, (key, nsteps)
+    sim.close()
+
+
 @pytest.mark.parametrize("tune", [(1.5, 3.0), (3.0, 4.0), (2.0, 1.0)])
 def test_search_tunables_keep_sets_and_results(gfsph_lib, oracle_mod, tune):
     """Other level bounds and cell sizes: the same neighbour sets, and one step

@@ -137,6 +137,43 @@ def single_particle_run(oracle_mod, const, tan_theta, steps, dt, sle=0, mode=2, 
     return st, w0 * m
 
 
+def test_normalised_density_keeps_a_uniform_layer_to_its_edges(oracle_mod):
+    """sum_density_Tools with nor_density (My_SPH_Tools_2019.f90:1841-1846):
+    sum_j m_j W_ij / sum_j (m_j/h_j) W_ij returns a uniform depth exactly,
+    also at the free edge where the plain sum falls short."""
+    s, n, h0 = 1.0, 24, 2.0
+    g = np.arange(n) * s
+    X, Y = np.meshgrid(g, g)
+    x = np.stack([X.ravel(), Y.ravel()], 1)
+    mass = np.full(n * n, s * s * h0)
+    hsml = np.full(n * n, 1.3 * s)
+    rho = np.full(n * n, h0)
+    nor = oracle_mod.pairs(2, params(nor_density=1), x, hsml, mass=mass, rho=rho, want_sets=False, want_rho=True)
+    plain = oracle_mod.pairs(2, params(), x, hsml, mass=mass, rho=rho, want_sets=False, want_rho=True)
+    assert np.allclose(nor["rho"], h0, rtol=1e-12)
+    inner = plain["rho"].reshape(n, n)[8:-8, 8:-8]
+    assert np.allclose(inner, inner.mean(), rtol=1e-12)
+    corner = plain["rho"].reshape(n, n)[0, 0]
+    assert corner < 0.7 * inner.mean()  # a corner particle sees a quarter of its neighbours
+
+
+@pytest.mark.parametrize("cos_theta", [0, 1])
+def test_inclined_plane_acceleration_with_and_without_cos_theta(oracle_mod, cos_theta):
+    """Get_Grav_Ext_SW (SPH_SW_2019.f90:9264-9285) and the Coulomb friction
+    on a plane of slope tan(t) = 0.5: a particle released at rest gains
+    g (tan t - mu) per second with ic_cosTheta = 0, and the textbook
+    g (sin t - mu cos t) with ic_cosTheta = 1 (g/deng along the normal)."""
+    tan_t, mu, dt = 0.5, 0.2, 0.01
+    st, _ = single_particle_run(oracle_mod, {3: 0.0, 9: mu, 16: float(cos_theta)}, tan_t, 1, dt)
+    if cos_theta:
+        c = 1.0 / math.sqrt(1.0 + tan_t * tan_t)
+        a = 9.8 * (tan_t * c - mu * c)
+    else:
+        a = 9.8 * (tan_t - mu)
+    assert abs(st.v[0, 1] - a * dt) <= 1e-6 * a * dt, (st.v[0, 1], a * dt)
+    assert abs(st.v[0, 0]) < 1e-12
+
+
 def test_voellmy_terminal_velocity_on_infinite_slope(oracle_mod):
     tan_t, mu, xi = 0.5, 0.2, 500.0
     st, h = single_particle_run(oracle_mod, {3: xi, 9: mu}, tan_t, 1500, 0.02)
@@ -152,6 +189,28 @@ def test_bingham_viscous_terminal_velocity(oracle_mod):
     vt = 9.8 * tan_t * 2000.0 * h * h / (3.0 * K)
     v = np.hypot(*st.v[0])
     assert abs(v - vt) / vt < 2e-3, (v, vt)
+
+
+@pytest.mark.parametrize("mode,dt0,v0,expect", [
+    (4, 10.0, (3.0, 4.0), math.sqrt(50.0) / 5.0),                # |DEM cell diagonal| / |v|
+    (4, 0.1, (3.0, 4.0), 0.11),                                    # growth capped at x1.1
+    (4, 0.1, (0.0, 0.0), 0.11),                                    # at rest: dxg/0 = +inf
+    (10, 10.0, (3.0, 4.0), 2.0 / (3.0 * math.sqrt(9.8 * 1.0))),  # hsml/(3c) is the smaller
+    (10, 10.0, (30.0, 40.0), math.sqrt(50.0) / 50.0),            # dxg/|v| is the smaller
+    (2, 10.0, (3.0, 4.0), 2.0 / (3.0 * (math.sqrt(9.8) + 5.0))),
+])
+def test_adaptive_dt_modes(oracle_mod, mode, dt0, v0, expect):
+    """Adaptive_dt_sph_SW (SPH_SW_2019.f90:6521-6664): the dt of the first
+    step of one particle (depth 1, hsml 2) on a flat 5 m DEM."""
+    nx, ny, d = 40, 40, 5.0
+    z = np.zeros((ny, nx))
+    p = params(sle=0, dt=dt0, ic_adapt=mode, average_velocity=0)
+    topol = oracle_mod.initial_topol(z, d, d, {}, deriv=1, mode=2)
+    st = oracle_mod.State(np.array([[100.0, 100.0]]), np.array([v0]), np.array([1.0]), np.array([4.0]),
+                          np.array([2.0]), topol, dt=dt0)
+    oracle_mod.run(2, p, nx, ny, d, d, st, 1)
+    # g, dt and the 1.1 growth factor enter as single-precision constants
+    assert abs(st.dt - expect) <= 1e-6 * expect, (st.dt, expect)
 
 
 def test_volume_conserved_without_erosion(oracle_mod):
