@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/gfsph.h"
@@ -146,6 +147,7 @@ struct gfsph_handle {
     // staged RK45 (nor_density or ic_cosTheta = 1)
     StageCarry carry{};
     float* rhoS = nullptr;   // the five depths of a step, k-major (nor_density)
+    int2* rcell = nullptr;   // cell of the reference's grid per slot (skf 2, 3)
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -240,6 +242,14 @@ int profile_collect(gfsph_handle* h) {
 // Side stream for the coarse-level kernels while a graph is captured.
 cudaStream_t side_stream(gfsph_handle* h) { return h->capturing ? h->stream2 : h->stream; }
 
+// Calls f with std::integral_constant<int, SK>, SK = scale_k of the kernel's
+// support: 3 for skf 2 and 3, else 2.
+template <class F>
+void with_sk(const gfsph_handle* h, F&& f) {
+    if (h->rheo.skf == 2 || h->rheo.skf == 3) f(std::integral_constant<int, 3>{});
+    else f(std::integral_constant<int, 2>{});
+}
+
 // Stage-dependent pressure: the step runs the staged RK45 kernels.
 bool staged(const gfsph_handle* h) { return h->rheo.nor_density || h->rheo.cos_theta; }
 
@@ -266,6 +276,7 @@ Search make_search(gfsph_handle* h) {
     q.pterm = h->pterm;
     q.indv = h->indv;
     q.rho0 = h->rho0;
+    q.rcell = h->rcell;
     q.kcap = h->kcap;
     return q;
 }
@@ -307,15 +318,20 @@ int enqueue_search(gfsph_handle* h, int advance) {
     launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, h->bstart, S, h->perm); }); nk++;
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
     launch(h, K_REORDER, [&] {
-        k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S, h->rheo, h->rho0);
+        k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S, h->rheo, h->rho0,
+                                           h->rcell);
     }); nk++;
     // the coarse-level kernels run beside the level-0 ones when graphs are
     // captured (side stream); serially otherwise
     cudaStream_t sb = side_stream(h);
     fork(h, 0);
-    launch(h, K_DENSITY_BIG, [&] { k_density_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); }); nk++;
-    launch(h, K_DENSITY, [&] { k_density<false><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
-    launch(h, K_DENSITY_SPARSE, [&] { k_density<true><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
+    with_sk(h, [&](auto sk) {
+        constexpr int SK = decltype(sk)::value;
+        launch(h, K_DENSITY_BIG, [&] { k_density_big<SK><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
+        launch(h, K_DENSITY, [&] { k_density<false, SK><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
+        launch(h, K_DENSITY_SPARSE, [&] { k_density<true, SK><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
+    });
+    nk += 3;
     join(h, 0);
     return nk;
 }
@@ -340,7 +356,9 @@ int enqueue_norms(gfsph_handle* h, PState As[5]) {
         const int clamp = k ? 1 : 0;
         launch(h, K_NORM, [&] { k_norm<<<blocks_for(n), kThreads, 0, st>>>(h->A, q, h->S, c, n, hp, clamp, As[k].rho); });
         launch(h, K_NORM_BIG, [&] {
-            k_norm_big<<<big_blocks(h), 128, 0, st>>>(h->A, q, h->S, c, hp, clamp, As[k].rho);
+            with_sk(h, [&](auto sk) {
+                k_norm_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(h->A, q, h->S, c, hp, clamp, As[k].rho);
+            });
         });
         nk += 2;
     }
@@ -374,7 +392,10 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
     int nk = enqueue_norms(h, As);
     nk += enqueue_stage_begin(h, As);
     for (int s = 0; s < 4; s++) {
-        launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, st>>>(As[s], q, S, c); }); nk++;
+        launch(h, K_FORCE_BIG, [&] {
+            with_sk(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[s], q, S, c); });
+        });
+        nk++;
         launch(h, K_IFORCE, [&] { k_iforce<<<pb, kThreads, 0, st>>>(As[s], q, S, c, n); }); nk++;
         launch(h, K_STAGE, [&] {
             if (s < 3) {
@@ -407,7 +428,11 @@ int enqueue_step(gfsph_handle* h) {
         PState As[5];
         nk += enqueue_stages(h, As);
         if (h->rheo.av_vel) {  // av_vel with the final depth
-            launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 128, 0, st>>>(As[4], q, S, h->rheo, h->B, h->velfin); });
+            launch(h, K_XSPH_BIG, [&] {
+                with_sk(h, [&](auto sk) {
+                    k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[4], q, S, h->rheo, h->B, h->velfin);
+                });
+            });
             launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(As[4], q, S, h->rheo, n, h->B, h->velfin); });
             nk += 2;
         }
@@ -422,7 +447,10 @@ int enqueue_step(gfsph_handle* h) {
     }
     cudaStream_t sb = side_stream(h);
     fork(h, 1);
-    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); }); nk++;
+    launch(h, K_FORCE_BIG, [&] {
+        with_sk(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
+    });
+    nk++;
     launch(h, K_IFORCE, [&] { k_iforce<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
     join(h, 1);
     launch(h, K_FORCE_RK, [&] {
@@ -430,7 +458,12 @@ int enqueue_step(gfsph_handle* h) {
     }); nk++;
     if (h->rheo.av_vel) {
         fork(h, 2);
-        launch(h, K_XSPH_BIG, [&] { k_xsph_big<<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo, h->B, h->velfin); }); nk++;
+        launch(h, K_XSPH_BIG, [&] {
+            with_sk(h, [&](auto sk) {
+                k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo, h->B, h->velfin);
+            });
+        });
+        nk++;
         launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B, h->velfin); }); nk++;
         join(h, 2);
     }
@@ -513,7 +546,7 @@ void free_particles(gfsph_handle* h) {
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
     dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv); dfree(h->rho0);
     dfree(h->carry.v); dfree(h->carry.acc); dfree(h->carry.dx); dfree(h->carry.dv); dfree(h->carry.xo);
-    dfree(h->carry.out); dfree(h->rhoS);
+    dfree(h->carry.out); dfree(h->rhoS); dfree(h->rcell);
     h->kcap = 0;
 }
 
@@ -609,7 +642,11 @@ int validate(const gfsph_params* p) {
     if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
     if (nfric == 4 && !(p->cst[5] >= 1.e-32f)) return GFSPH_ERR_ARG;  // SPH_SW_2019.f90:9547-9550
     if (erosion && (int)(p->cst[20] + 0.1f) != 1) return GFSPH_ERR_UNSUPPORTED;
-    if (p->skf != 1 && p->skf != 4) return GFSPH_ERR_UNSUPPORTED;
+    if (p->skf < 1 || p->skf > 4) return GFSPH_ERR_UNSUPPORTED;
+    // skf 2, 3 (support 3 h): the pair set depends on the reference's own
+    // grid, reproduced for nnps 2; nnps 4 grids the principal-axes rotation
+    // of FP32 running sums, which is order-dependent
+    if ((p->skf == 2 || p->skf == 3) && p->nnps != 2) return GFSPH_ERR_UNSUPPORTED;
     if (p->pa_sph != 1 && p->pa_sph != 2) return GFSPH_ERR_UNSUPPORTED;
     if (p->nnps != 2 && p->nnps != 4) return GFSPH_ERR_UNSUPPORTED;
     if (p->sle != 0 && p->sle != 1) return GFSPH_ERR_UNSUPPORTED;
@@ -823,6 +860,7 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
             st |= dalloc(&C.xo, n); st |= dalloc(&C.out, n);
             if (h->rheo.nor_density) st |= dalloc(&h->rhoS, 5 * (size_t)n);
         }
+        if (h->rheo.skf == 2 || h->rheo.skf == 3) st |= dalloc(&h->rcell, n);
         if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
         if (st) return st;
@@ -1023,7 +1061,12 @@ int gfsph_density(gfsph_handle* h, float* rho_out) {
     if (h->rheo.nor_density) {  // the first call of the step: normalised with the depths held
         Search q = make_search(h);
         launch(h, K_NORM, [&] { k_norm<<<blocks_for(n), kThreads, 0, h->stream>>>(h->A, q, h->S, h->rheo, n, h->rho0, 0, h->rhoS); });
-        launch(h, K_NORM_BIG, [&] { k_norm_big<<<big_blocks(h), 128, 0, h->stream>>>(h->A, q, h->S, h->rheo, h->rho0, 0, h->rhoS); });
+        launch(h, K_NORM_BIG, [&] {
+            with_sk(h, [&](auto sk) {
+                k_norm_big<decltype(sk)::value><<<big_blocks(h), 128, 0, h->stream>>>(h->A, q, h->S, h->rheo, h->rho0, 0,
+                                                                                     h->rhoS);
+            });
+        });
         CK(cudaMemcpyAsync(h->A.rho, h->rhoS, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
     }
     launch(h, K_COPY, [&] { k_copy_state<<<blocks_for(n), kThreads, 0, h->stream>>>(h->A, h->B, n); });
@@ -1048,7 +1091,9 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
         As[0] = h->A;
     }
     launch(h, K_IFORCE, [&] { k_iforce<<<blocks_for(n), kThreads, 0, s>>>(As[0], q, h->S, h->rheo, n); });
-    launch(h, K_FORCE_BIG, [&] { k_force_big<<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });
+    launch(h, K_FORCE_BIG, [&] {
+        with_sk(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });
+    });
     launch(h, K_FORCE_RK, [&] {
         k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 1,
                                                      h->velfin);
@@ -1084,7 +1129,11 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
             if (dalloc(&dpairs, pcap) || dalloc(&dcount, 1)) { dfree(dpairs); dfree(dcount); return GFSPH_ERR_CUDA; }
             cudaMemset(dcount, 0, sizeof(int));
             Search q = make_search(h);
-            launch(h, K_EXPORT, [&] { k_export_big<<<big_blocks(h), 128, 0, h->stream>>>(q, h->S, dpairs, dcount, pcap); });
+            launch(h, K_EXPORT, [&] {
+                with_sk(h, [&](auto sk) {
+                    k_export_big<decltype(sk)::value><<<big_blocks(h), 128, 0, h->stream>>>(q, h->S, dpairs, dcount, pcap);
+                });
+            });
             cudaStreamSynchronize(h->stream);
             int np = 0;
             cudaMemcpy(&np, dcount, sizeof(int), cudaMemcpyDeviceToHost);
@@ -1520,7 +1569,8 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     if (!h->has_state) return GFSPH_ERR_STATE;
     const Rheo& c = h->rheo;
     if (!(c.nfric == 5 || c.nfric == 6) || c.xi < 0.f || c.erosion || c.icpwp != 0 || c.pa_sph != 2 || c.sle != 0 ||
-        c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f || c.nor_density || c.cos_theta)
+        c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f || c.nor_density || c.cos_theta ||
+        (c.skf != 1 && c.skf != 4))
         return GFSPH_ERR_UNSUPPORTED;
     gfsph_adjoint* a = new (std::nothrow) gfsph_adjoint();
     if (!a) return GFSPH_ERR_ARG;

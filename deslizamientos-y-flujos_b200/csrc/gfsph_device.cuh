@@ -12,9 +12,19 @@ namespace gfsph {
 constexpr float kPi = 3.14159274101257324f;  // pi = 4.*atan(1.0) in default real
 constexpr float kTwoThirds = (float)(2.0 / 3.0);
 
+// x**5 as the Fortran compiler expands an integer power: x2 = x*x,
+// x3 = x2*x, x5 = x3*x2.
+__device__ __forceinline__ float ipow5(float x) {
+    const float x2 = x * x;
+    return (x2 * x) * x2;
+}
+
 // kernel_TOOLS, My_SPH_Tools_2019.f90:2062-2180 (2-D; skf 1 cubic spline,
-// skf 4 Wendland C2).  Returns w and dW/dx for the offset (dx0, dx1) at
-// distance r with smoothing length hs.
+// skf 2 Gaussian, skf 3 quintic, skf 4 Wendland C2).  Returns w and dW/dx
+// for the offset (dx0, dx1) at distance r with smoothing length hs.  The
+// Gaussian's exp is evaluated in FP64 and rounded once.  The quintic's
+// gradient for q <= 1 is the reference's (-120 + 120 q - 50 q^2)/h^2 dx
+// (:2141), which is not the derivative of its w.
 __device__ __forceinline__ void sph_kernel(int skf, float r, float dx0, float dx1, float hs, float& w,
                                            float& d0, float& d1) {
     float q = r / hs;
@@ -32,6 +42,33 @@ __device__ __forceinline__ void sph_kernel(int skf, float r, float dx0, float dx
             float t = ((((factor * 1.f) / 6.f) * 3.f) * (u * u)) / hs;
             d0 = -(t * (dx0 / r));
             d1 = -(t * (dx1 / r));
+        }
+    } else if (skf == 2) {
+        float factor = 1.f / ((hs * hs) * kPi);  // hsml**ndimn * pi**(ndimn/2.)
+        if (q >= 0.f && q <= 3.f) {
+            w = factor * (float)exp((double)(-(q * q)));
+            d0 = w * (-(((2.f * dx0) / hs) / hs));
+            d1 = w * (-(((2.f * dx1) / hs) / hs));
+        }
+    } else if (skf == 3) {
+        float factor = 7.f / (((478.f * kPi) * hs) * hs);
+        if (q >= 0.f && q <= 1.f) {
+            w = factor * ((ipow5(3.f - q) - 6.f * ipow5(2.f - q)) + 15.f * ipow5(1.f - q));
+            float t = ((-120.f + 120.f * q) - 50.f * (q * q)) / (hs * hs);
+            d0 = factor * (t * dx0);
+            d1 = factor * (t * dx1);
+        } else if (q > 1.f && q <= 2.f) {
+            w = factor * (ipow5(3.f - q) - 6.f * ipow5(2.f - q));
+            float a = 3.f - q, b = 2.f - q;
+            float t = (factor * (-(5.f * ((a * a) * (a * a))) + 30.f * ((b * b) * (b * b)))) / hs;
+            d0 = t * (dx0 / r);
+            d1 = t * (dx1 / r);
+        } else if (q > 2.f && q <= 3.f) {
+            w = factor * ipow5(3.f - q);
+            float a = 3.f - q;
+            float t = (factor * (-(5.f * ((a * a) * (a * a))))) / hs;
+            d0 = t * (dx0 / r);
+            d1 = t * (dx1 / r);
         }
     } else {  // skf == 4
         float factor = 7.f / (((4.f * kPi) * hs) * hs);
@@ -68,23 +105,25 @@ __device__ __forceinline__ bool pair_test(float2 xi, float2 xj, float hi, float 
     return g.r < 2.f * g.mh;
 }
 
-// The same test for a search over candidates, with a cheap early reject:
-// sqrt_rn(dr) < t implies dr < t*t in exact arithmetic, and
-// dr > fl(fl(t*t) * (1 + 1e-5)) implies dr >= t*t (the two roundings move
-// t*t by at most 2^-23 relative), so the reject never drops a pair that the
-// exact test keeps.
+// The same test for a search over candidates, r < SK*mh with SK = scale_k
+// (2 for skf 1 and 4, 3 for skf 2 and 3, My_SPH_Tools_2019.f90:1155-1161),
+// with a cheap early reject: sqrt_rn(dr) < t implies dr < t*t in exact
+// arithmetic, and dr > fl(fl(t*t) * (1 + 1e-5)) implies dr >= t*t (the two
+// roundings move t*t by at most 2^-23 relative), so the reject never drops a
+// pair that the exact test keeps.
+template <int SK = 2>
 __device__ __forceinline__ bool pair_search(float2 xi, float2 xj, float hi, float hj, PairGeom& g) {
     float d0 = xi.x - xj.x;
     float d1 = xi.y - xj.y;
     float dr = d0 * d0;
     dr = dr + d1 * d1;
-    float t = 2.f * ((hi + hj) / 2.f);
+    float t = (float)SK * ((hi + hj) / 2.f);
     if (dr > (t * t) * 1.00001f) return false;
     g.dx0 = d0;
     g.dx1 = d1;
     g.mh = (hi + hj) / 2.f;
     g.r = sqrtf(dr);
-    return g.r < 2.f * g.mh;
+    return g.r < (float)SK * g.mh;
 }
 
 // Float <-> order-preserving uint, for atomicMin/atomicMax reductions.

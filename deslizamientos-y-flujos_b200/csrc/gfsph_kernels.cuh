@@ -62,6 +62,9 @@ struct StepScalars {
     int need_cells, need_nbr, need_big, need_blocks;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
     unsigned int bounds_ticket;  // blocks of k_bounds done (the last one resets it)
+    // the reference's own grid of grid_find_NEW_tools (skf 2, 3): origin, cell, cells
+    float ref_xmin, ref_ymin, ref_delt;
+    int ref_ndx, ref_ndy;
     int advance;      // 1 inside gfsph_step, 0 for search-only passes
 };
 
@@ -88,6 +91,7 @@ struct Search {
     float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
     float2* indv;        // internal acceleration of every active particle (slot order)
     float* rho0;         // depth at the start of the step, after Adaptive_dt's h_inf clamp (icpwp = 3)
+    const int2* rcell;   // slot -> cell of the reference's own grid (skf 2, 3), else null
     int kcap;
 };
 
@@ -271,6 +275,18 @@ __device__ void grid_setup(const Rheo& c, StepScalars* S, const GridArgs ga) {
         else if (c.ic_adapt != 0) dt = fminf(1.1f * dt, dtmin);
     }
     S->dt_step = dt;
+    {  // the reference's grid: cells of 2*max(hsml) (grid_find_NEW_tools My_SPH_Tools_2019.f90:1168-1181)
+        const float delt = hmx * 2.f;
+        float len = xmx - xmn;
+        int nd = (int)(len / delt + 1.f);
+        S->ref_ndx = nd;
+        S->ref_xmin = (xmn - ((float)nd * delt - len) / 2.f) - 0.001f * len;
+        len = ymx - ymn;
+        nd = (int)(len / delt + 1.f);
+        S->ref_ndy = nd;
+        S->ref_ymin = (ymn - ((float)nd * delt - len) / 2.f) - 0.001f * len;
+        S->ref_delt = delt;
+    }
     float mean = (float)(S->hsum / (double)S->hcount);
     float hc = fminf(hmx, level_factor * mean);
     int nlev = 1;
@@ -569,7 +585,7 @@ __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, int*
 // rho0, the depth RK45 keeps at its start (after the h_inf clamp of
 // Adaptive_dt_sph_SW :6540, modes 1, 2 and 10).
 __global__ void k_reorder(const PState B, int n, const int* perm, const int2* keyrank, PState A, int* cellA,
-                          float4* xhm, const StepScalars* S, Rheo c, float* rho0) {
+                          float4* xhm, const StepScalars* S, Rheo c, float* rho0, int2* rcell) {
     if (S->skip) return;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = perm[s];
@@ -588,19 +604,44 @@ __global__ void k_reorder(const PState B, int n, const int* perm, const int2* ke
         A.id[s] = B.id[o];
         cellA[s] = keyrank[o].x;
         xhm[s] = make_float4(p.x, p.y, hs, m);
+        if (rcell && !B.flag[o]) {  // cell of the reference's grid (:1203-1204)
+            int ix = (int)((p.x - S->ref_xmin) / S->ref_delt + 1.f);
+            int iy = (int)((p.y - S->ref_ymin) / S->ref_delt + 1.f);
+            rcell[s] = make_int2(min(ix, S->ref_ndx), min(iy, S->ref_ndy));
+        }
     }
 }
 
+// Largest neighbour distance against a level whose hsml <= Hk:
+// r < SK*(hi + hj)/2 <= SK/2 (hi + Hk).
+template <int SK>
+__device__ __forceinline__ float support_span(float hi, float hk) {
+    return (SK == 2) ? hi + hk : 1.5f * (hi + hk);
+}
+
+// The reference's own cell test, needed for supports of 3 h (skf 2, 3):
+// grid_find pairs only particles in the same or adjacent cells of its grid
+// of 2*max(hsml) (My_SPH_Tools_2019.f90:1257-1264), so pairs up to 3 h apart
+// are kept or dropped by where that grid falls.  (With 2 h supports every
+// pair lies within one cell and the test is implied.)
+template <int SK>
+__device__ __forceinline__ bool ref_adjacent(const Search& Q, int2 ci, int j) {
+    if (SK == 2) return true;
+    const int2 cj = Q.rcell[j];
+    return abs(cj.x - ci.x) <= 1 && abs(cj.y - ci.y) <= 1;
+}
+
 // Stencil of level k around particle i: every j of level k has hsml_j <= Hk
-// (the level's largest smoothing length), so with r < hi + hj it lies within
-// floor((hi + Hk)/cell + 0.01) + 1 cells of i's cell in that level's grid,
-// whatever the rounding of the cell coordinates.  Returns false for an empty
-// level.
+// (the level's largest smoothing length), so with r < SK/2 (hi + hj) it lies
+// within floor(SK/2 (hi + Hk)/cell + 0.01) + 1 cells of i's cell in that
+// level's grid, whatever the rounding of the cell coordinates.  Returns false
+// for an empty level.
+template <int SK = 2>
 __device__ __forceinline__ bool level_stencil(const StepScalars* S, int k, float2 xi, float hi, int& x0, int& x1,
                                               int& y0, int& y1) {
     unsigned int hk = S->lev_hmax_o[k];
     if (hk == 0u) return false;
-    float rr = (hi + o2f(hk)) / S->lev_c[k] + 0.01f;
+    float rr = support_span<SK>(hi, o2f(hk)) / S->lev_c[k] + 0.01f;
     int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
     int cx, cy;
     cell_of(xi, S, k, cx, cy);
@@ -628,14 +669,15 @@ __device__ __forceinline__ void block_row_range(const Search& Q, const StepScala
     jb = Q.start[key + hi + 1];
 }
 
-// Pair test of particle i against the slots ja..jb-1.
-template <class F>
-__device__ __forceinline__ void visit_range(const Search& Q, int i, float2 xi, float hi, int ja, int jb, F& f) {
+// Pair test of particle i (reference-grid cell ci) against the slots ja..jb-1.
+template <int SK, class F>
+__device__ __forceinline__ void visit_range(const Search& Q, int i, float2 xi, float hi, int2 ci, int ja, int jb,
+                                            F& f) {
     for (int j = ja; j < jb; j++) {
         if (j == i) continue;
         float4 o = Q.xhm[j];
         PairGeom g;
-        if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+        if (pair_search<SK>(xi, make_float2(o.x, o.y), hi, o.z, g) && ref_adjacent<SK>(Q, ci, j)) f(j, o, g);
     }
 }
 
@@ -647,12 +689,12 @@ __device__ __forceinline__ void visit_range(const Search& Q, int i, float2 xi, f
 // sqrt(rr^2 - (d - 1)^2) + 1 cells in x (rr and d - 1 carry 0.01-cell
 // margins for the rounding of the cell coordinates).  A dense row is one key
 // range; a sparse row is one range per block column it crosses.
-template <bool SPARSE, class F>
+template <bool SPARSE, int SK, class F>
 __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScalars* S, int k, int i, float2 xi, float hi,
-                                                 F&& f) {
+                                                 int2 ci, F&& f) {
     const unsigned int hk = S->lev_hmax_o[k];
     if (hk == 0u) return;
-    const float rr = (hi + o2f(hk)) / S->lev_c[k] + 0.01f;
+    const float rr = support_span<SK>(hi, o2f(hk)) / S->lev_c[k] + 0.01f;
     const int R = (rr < 1.0e8f) ? (int)rr + 1 : 100000000;
     const float rr2 = rr * rr;
     int cx, cy;
@@ -671,7 +713,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
         const int x0 = max(cx - rx, 0), x1 = min(cx + rx, ndx - 1);
         if (!SPARSE) {
             const int rowoff = S->lev_off[k] + jy * ndx;
-            visit_range(Q, i, xi, hi, Q.start[rowoff + x0], Q.start[rowoff + x1 + 1], f);
+            visit_range<SK>(Q, i, xi, hi, ci, Q.start[rowoff + x0], Q.start[rowoff + x1 + 1], f);
             continue;
         }
         const int c0 = (int)((unsigned)x0 / kBlkX), c1 = (int)((unsigned)x1 / kBlkX);
@@ -702,7 +744,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
                 if (j == i) continue;
                 float4 o = Q.xhm[j];
                 PairGeom g;
-                if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+                if (pair_search<SK>(xi, make_float2(o.x, o.y), hi, o.z, g) && ref_adjacent<SK>(Q, ci, j)) f(j, o, g);
             }
             continue;
         }
@@ -712,7 +754,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
             s1 = Q.bstart[brow + bx + 1];  // end of this block = start of the next
             if (s1 == s0) continue;
             const int key = s0 * kBlockCells + row - bx * kBlkX;
-            visit_range(Q, i, xi, hi, Q.start[key + max(x0, bx * kBlkX)],
+            visit_range<SK>(Q, i, xi, hi, ci, Q.start[key + max(x0, bx * kBlkX)],
                         Q.start[key + min(x1, bx * kBlkX + kBlkX - 1) + 1], f);
         }
     }
@@ -726,7 +768,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
 // clamped to h_inf (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
 // Instantiated for both cell layouts; the launch whose layout this step does
 // not use returns at once.
-template <bool SPARSE>
+template <bool SPARSE, int SK>
 __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip || (S->sparse != 0) != SPARSE) return;
     const int nreg = S->nreg, nlev = S->nlev;
@@ -734,10 +776,11 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
         float4 me = Q.xhm[i];
         float2 xi = make_float2(me.x, me.y);
         float hi = me.z;
+        const int2 ci = (SK == 2) ? make_int2(0, 0) : Q.rcell[i];
         double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * me.w);
         int cnt = 0;
         for (int k = 0; k < nlev; k++)
-            level_neighbours<SPARSE>(Q, S, k, i, xi, hi, [&](int j, float4 o, const PairGeom& g) {
+            level_neighbours<SPARSE, SK>(Q, S, k, i, xi, hi, ci, [&](int j, float4 o, const PairGeom& g) {
                 if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
                 cnt++;
                 acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
@@ -759,14 +802,15 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
 // Visits every neighbour j of particle i cooperatively over one warp: the
 // lanes fetch the slot ranges of up to 32 (row, block column) segments of the
 // stencil at once, then share each segment's candidates.
-template <class F>
+template <int SK, class F>
 __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScalars* S, int i, int lane, F&& f) {
     const float4 me = Q.xhm[i];
     const float2 xi = make_float2(me.x, me.y);
     const float hi = me.z;
+    const int2 ci = (SK == 2) ? make_int2(0, 0) : Q.rcell[i];
     for (int k = 0; k < S->nlev; k++) {
         int x0, x1, y0, y1;
-        if (!level_stencil(S, k, xi, hi, x0, x1, y0, y1)) continue;
+        if (!level_stencil<SK>(S, k, xi, hi, x0, x1, y0, y1)) continue;
         const int bx0 = S->sparse ? (int)((unsigned)x0 / kBlkX) : 0;
         const int ncol = S->sparse ? (int)((unsigned)x1 / kBlkX) - bx0 + 1 : 1;
         const long long nseg = (long long)(y1 - y0 + 1) * ncol;
@@ -784,7 +828,8 @@ __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScala
                     if (j == i) continue;
                     float4 o = Q.xhm[j];
                     PairGeom g;
-                    if (pair_search(xi, make_float2(o.x, o.y), hi, o.z, g)) f(j, o, g);
+                    if (pair_search<SK>(xi, make_float2(o.x, o.y), hi, o.z, g) && ref_adjacent<SK>(Q, ci, j))
+                        f(j, o, g);
                 }
             }
         }
@@ -792,6 +837,7 @@ __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScala
 }
 
 // Summation density of the level >= 1 particles, one warp per particle.
+template <int SK>
 __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepScalars* S, Rheo c) {
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
@@ -800,7 +846,7 @@ __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepSca
     for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
         double acc = 0.0;
-        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
         });
         acc = warp_sum(acc);
@@ -836,6 +882,7 @@ __device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rh
 }
 
 // Internal acceleration of the level >= 1 particles, one warp per particle.
+template <int SK>
 __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
@@ -845,7 +892,7 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
         int i = nreg + b;
         float pi_ = Q.pterm[i], rhoi = A.rho[i];
         double a0 = 0.0, a1 = 0.0;
-        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
         });
         a0 = warp_sum(a0);
@@ -1146,6 +1193,7 @@ __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S
 }
 
 // The same for the level >= 1 particles, one warp each.
+template <int SK>
 __global__ void __launch_bounds__(128) k_norm_big(PState A, Search Q, StepScalars* S, Rheo c, const float* hp,
                                                   int clamp_prev, float* hout) {
     if (S->skip) return;
@@ -1155,7 +1203,7 @@ __global__ void __launch_bounds__(128) k_norm_big(PState A, Search Q, StepScalar
     for (int b = warp; b < nbig; b += nwarps) {
         const int i = nreg + b;
         double den = 0.0;
-        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w(c.skf, g.r, g.mh));
         });
         den = warp_sum(den);
@@ -1362,6 +1410,7 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
     }
 }
 
+template <int SK>
 __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B,
                                                    const float2* velfin) {
     if (S->skip || !c.av_vel) return;
@@ -1374,7 +1423,7 @@ __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalar
         float2 vi = velfin[i];
         float rhoi = A.rho[i];
         double a0 = 0.0, a1 = 0.0;
-        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
         });
         a0 = warp_sum(a0);
@@ -1424,13 +1473,14 @@ __global__ void k_step_end(StepScalars* S) {
 
 // Neighbour pairs of the level >= 1 particles, for the parity export: every
 // (big i, j) pair with r < hi + hj, written as slot pairs.
+template <int SK>
 __global__ void k_export_big(Search Q, StepScalars* S, int2* pairs, int* npairs, int cap) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nreg = S->nreg, nbig = S->nbig;
     for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
-        warp_neighbours(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+        warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             int k = atomicAdd(npairs, 1);
             if (k < cap) pairs[k] = make_int2(i, j);
         });

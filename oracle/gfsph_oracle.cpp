@@ -116,7 +116,18 @@ template <class R> inline R fpi() { return (R)(4.0f * atanf(1.0f)); } /* pi = 4.
 template <class R> inline R rmax(R a, R b) { return (a > b) ? a : b; } /* MAX(a,b) */
 template <class R> inline R rmin(R a, R b) { return (a < b) ? a : b; }
 
-/* kernel_TOOLS, My_SPH_Tools_2019.f90:2062-2180, 2-D, skf 1 and 4 */
+/* exp of a default real, evaluated in FP64 and rounded once */
+inline float rexp(float x) { return (float)std::exp((double)x); }
+inline double rexp(double x) { return std::exp(x); }
+inline Dual rexp(const Dual& x) { return std::exp(x); }
+
+/* x**5 with an integer exponent as the Fortran compiler expands it:
+ * x2 = x*x, x3 = x2*x, x5 = x3*x2 */
+template <class R> inline R ipow5(R x) { R x2 = x * x; return (x2 * x) * x2; }
+
+/* kernel_TOOLS, My_SPH_Tools_2019.f90:2062-2180, 2-D, skf 1 to 4.  The
+ * quintic's gradient for q <= 1 is the reference's (-120 + 120 q - 50 q**2)
+ * / h**2 dx (:2141) as written (not the derivative of its w). */
 template <class R>
 inline void kernel_tools(int skf, R r, R dx0, R dx1, R hs, R& w, R& d0, R& d1) {
     const R pi = fpi<R>();
@@ -135,6 +146,33 @@ inline void kernel_tools(int skf, R r, R dx0, R dx1, R hs, R& w, R& d0, R& d1) {
             R t = ((((factor * (R)1) / (R)6) * (R)3) * (u * u)) / hs;
             d0 = -(t * (dx0 / r));
             d1 = -(t * (dx1 / r));
+        }
+    } else if (skf == 2) {
+        R factor = (R)1 / ((hs * hs) * pi);                              /* :2116, pi**(2/2.) = pi */
+        if (q >= 0 && q <= 3) {                                           /* :2117-2122 */
+            w = factor * rexp(-(q * q));
+            d0 = w * (-((((R)2 * dx0) / hs) / hs));
+            d1 = w * (-((((R)2 * dx1) / hs) / hs));
+        }
+    } else if (skf == 3) {
+        R factor = (R)7 / ((((R)478 * pi) * hs) * hs);                  /* :2131 */
+        if (q >= 0 && q <= 1) {                                           /* :2138-2142 */
+            w = factor * ((ipow5((R)3 - q) - (R)6 * ipow5((R)2 - q)) + (R)15 * ipow5((R)1 - q));
+            R t = (((R)-120 + (R)120 * q) - (R)50 * (q * q)) / (hs * hs);
+            d0 = factor * (t * dx0);
+            d1 = factor * (t * dx1);
+        } else if (q > 1 && q <= 2) {                                     /* :2143-2147 */
+            w = factor * (ipow5((R)3 - q) - (R)6 * ipow5((R)2 - q));
+            R a = (R)3 - q, b = (R)2 - q;
+            R t = (factor * (-((R)5 * ((a * a) * (a * a))) + (R)30 * ((b * b) * (b * b)))) / hs;
+            d0 = t * (dx0 / r);
+            d1 = t * (dx1 / r);
+        } else if (q > 2 && q <= 3) {                                     /* :2148-2152 */
+            w = factor * ipow5((R)3 - q);
+            R a = (R)3 - q;
+            R t = (factor * (-((R)5 * ((a * a) * (a * a))))) / hs;
+            d0 = t * (dx0 / r);
+            d1 = t * (dx1 / r);
         }
     } else if (skf == 4) {
         R factor = (R)7 / ((((R)4 * pi) * hs) * hs);                    /* :2164 */
@@ -232,7 +270,7 @@ struct Oracle {
 
     /* grid_find_NEW_tools (nnps=2, My_SPH_Tools_2019.f90:1109-1370) and
      * grid_find_NEW_tools3 (nnps=4, :802-1104): counting sort into cells of
-     * size 2*max(hsml), half-stencil pair enumeration, r < 2*(hi+hj)/2. */
+     * size 2*max(hsml), half-stencil pair enumeration, r < scale_k*(hi+hj)/2. */
     void grid_find() {
         pairs.clear(); pw.clear(); pd0.clear(); pd1.clear();
         std::vector<R> xr(2 * (size_t)n);
@@ -296,7 +334,7 @@ struct Oracle {
             if (flag[i]) continue;
             list[start[cell[i]] + fill[cell[i]]++] = i;
         }
-        const int scale_k = 2; /* skf 1 and 4 */
+        const int scale_k = (P->skf == 2 || P->skf == 3) ? 3 : 2; /* :1155-1161 */
         for (int idy = 1; idy <= ndiv[1]; idy++)
             for (int idx = 1; idx <= ndiv[0]; idx++) {
                 long ic = (long)ndiv[0] * (idy - 1) + (idx - 1);
@@ -792,7 +830,7 @@ struct Oracle {
         ic_erosion = (cst[21] > lit<R>(1.e-9)) ? 1 : 0;
         if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
         if (ic_erosion && (int)(cst[21] + lit<R>(0.1)) != 1) return GFSPH_ERR_UNSUPPORTED;
-        if (P->skf != 1 && P->skf != 4) return GFSPH_ERR_UNSUPPORTED;
+        if (P->skf < 1 || P->skf > 4) return GFSPH_ERR_UNSUPPORTED;
         nx = nx_; ny = ny_; npoig = nx * ny;
         xming = (R)(float)xmin; yming = (R)(float)ymin; dxg = (R)(float)dx; dyg = (R)(float)dy;
         xmaxg = xming + (R)(nx - 1) * dxg;

@@ -47,7 +47,7 @@ def test_status_strings(gfsph_lib):
 def test_rejects_unsupported_options_before_touching_the_device(gfsph_lib):
     z = np.zeros((8, 8), np.float32)
     base = {1: 9.8, 2: 2000, 3: 500, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01}
-    for const, bad in (({}, dict(skf=2)), ({}, dict(nor_density=2)), ({}, dict(pa_sph=3)), ({16: 2.0}, {}),
+    for const, bad in (({}, dict(skf=5)), ({}, dict(skf=2, nnps=4)), ({}, dict(nor_density=2)), ({}, dict(pa_sph=3)), ({16: 2.0}, {}),
                        ({}, dict(ic_adapt=3))):
         p = gfsph_lib.make_params({**base, **const}, **bad)
         with pytest.raises(gfsph_lib.GfsphError) as e:

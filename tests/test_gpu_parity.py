@@ -45,12 +45,17 @@ def small_channel(n=6000, k=8):
     return workloads.fractal_channel(n_target=n, dem_k=k, cell=5.0)
 
 
-def test_neighbour_sets_bit_exact(gfsph_lib, oracle_mod):
+@pytest.mark.parametrize("skf", [1, 2, 3])
+def test_neighbour_sets_bit_exact(gfsph_lib, oracle_mod, skf):
+    """The sets of grid_find against the oracle's literal restatement; with
+    skf 2, 3 (support 3h) they include the drops of the reference's own grid.
+    The first cloud has a few large smoothing lengths (coarse levels)."""
     rng = np.random.default_rng(11)
     clouds = []
     n = 4000
     x = rng.uniform(0, 60, size=(n, 2)).astype(np.float32) + np.float32(100.0)
     h = rng.uniform(0.5, 2.0, size=n).astype(np.float32)
+    h[::400] *= np.float32(7.0)
     clouds.append((x, h))
     w = workloads.inclined_plane()
     clouds.append((w.x, w.hsml))
@@ -59,15 +64,17 @@ def test_neighbour_sets_bit_exact(gfsph_lib, oracle_mod):
     for x, h in clouds:
         z = np.zeros((64, 64), np.float32)
         cell = float(np.ceil((x.max() + 10) / 63.0))
-        p = gfsph.make_params({1: 9.8, 2: 2000, 3: 500, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01})
+        p = gfsph.make_params({1: 9.8, 2: 2000, 3: 500, 5: 5, 9: 0.2, 10: 0.01, 15: 0.01}, skf=skf,
+                              max_neighbours=256 if skf != 1 else 0)
         sim = gfsph.Sim(p, z, dx=cell, dy=cell)
         m = np.ones(x.shape[0], np.float32)
         sim.upload(x, np.zeros_like(x), m, m, h)
-        sim.density()
+        rho = sim.density()
         off, idx = sim.neighbours()
-        ref = oracle_mod.pairs(oracle_mod.MODE_FP32, p, x, h)
+        ref = oracle_mod.pairs(oracle_mod.MODE_FP32_DACC, p, x, h, mass=m, rho=m, want_rho=True)
         assert np.array_equal(off, ref["offsets"])
         assert np.array_equal(idx, ref["idx"])
+        assert max_rel(rho, ref["rho"]) <= 1e-6
         sim.close()
 
 
@@ -427,6 +434,25 @@ def test_rheologies_match_oracle(gfsph_lib, oracle_mod, rheo):
         tol = 1e-6 if nsteps == 1 else 1e-5
         for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
             assert rel_l2(g[key], ref) <= tol, (key, nsteps)
+    sim.close()
+
+
+@pytest.mark.parametrize("skf", [2, 3])
+def test_three_h_kernels_match_oracle(gfsph_lib, oracle_mod, skf):
+    """skf 2 (Gaussian) and 3 (quintic), support 3h, on the channel release:
+    one step and 20 steps against the oracle in the GPU's precision scheme
+    (the pair sets follow the reference's own grid every step)."""
+    w = small_channel()
+    sim, st, p = setup_pair(w, oracle_mod, skf=skf, max_neighbours=256)
+    ny, nx = w.z.shape
+    for nsteps in (1, 19):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        tol = 1e-6 if nsteps == 1 else 1e-5
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass), ("hsml", st.hsml)):
+            assert rel_l2(g[key], ref) <= tol, (key, nsteps, rel_l2(g[key], ref))
     sim.close()
 
 

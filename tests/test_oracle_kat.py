@@ -24,27 +24,40 @@ def params(const=None, **kw):
     return gfsph.make_params(c, **kw)
 
 
-@pytest.mark.parametrize("skf", [1, 4])
+@pytest.mark.parametrize("skf", [1, 2, 3, 4])
 def test_kernel_normalisation_and_gradient(oracle_mod, skf):
+    """kernel_TOOLS (My_SPH_Tools_2019.f90:2062-2180): unit integral over the
+    plane (the Gaussian cut at 3h keeps 1 - e^-9), gradient = dW/dr along the
+    offset, compact support 2h (skf 1, 4) or 3h (skf 2, 3).  The quintic's
+    gradient for q <= 1 is the reference's (-120 + 120 q - 50 q^2)/h^2 dx,
+    not the derivative of its w; it is checked as written."""
     hs = 1.3
-    g = np.linspace(-2.7, 2.7, 541)
+    sup = 3 if skf in (2, 3) else 2
+    g = np.linspace(-sup * hs - 0.1, sup * hs + 0.1, 120 * sup + 41)
     X, Y = np.meshgrid(g, g)
     r = np.hypot(X, Y).ravel()
     w, d0, d1 = oracle_mod.kernel(skf, r, X.ravel(), Y.ravel(), np.full(r.size, hs), mode=oracle_mod.MODE_FP64)
     cell = (g[1] - g[0]) ** 2
-    assert abs(w.sum() * cell - 1.0) < 2e-3
-    # gradient = derivative of W along the offset (central differences in r)
-    rr = np.linspace(0.05, 2 * hs - 0.05, 200)
+    target = 1.0 - math.exp(-9.0) if skf == 2 else 1.0
+    assert abs(w.sum() * cell - target) < 2e-3
+    rr = np.linspace(0.05, sup * hs - 0.05, 300)
     e = 1e-6
     wp, _, _ = oracle_mod.kernel(skf, rr + e, rr + e, 0 * rr, hs + 0 * rr, mode=oracle_mod.MODE_FP64)
     wm, _, _ = oracle_mod.kernel(skf, rr - e, rr - e, 0 * rr, hs + 0 * rr, mode=oracle_mod.MODE_FP64)
     _, gx, gy = oracle_mod.kernel(skf, rr, rr, 0 * rr, hs + 0 * rr, mode=oracle_mod.MODE_FP64)
     fd = (wp - wm) / (2 * e)
-    assert np.allclose(gx, fd, rtol=1e-5, atol=1e-7)
+    exact = np.ones(rr.size, bool)
+    if skf == 3:
+        q = rr / hs
+        exact = q > 1.0 + 1e-6
+        factor = 7.0 / (478.0 * math.pi * hs * hs)
+        as_written = factor * ((-120.0 + 120.0 * q - 50.0 * q * q) / hs ** 2 * rr)
+        assert np.allclose(gx[q <= 1.0], as_written[q <= 1.0], rtol=1e-9)
+        assert not np.allclose(gx[q < 0.9], fd[q < 0.9], rtol=1e-2)
+    assert np.allclose(gx[exact], fd[exact], rtol=1e-5, atol=1e-7)
     assert np.all(gy == 0)
-    # compact support 2h
-    w2, a, b = oracle_mod.kernel(skf, np.array([2 * hs * 1.0001]), np.array([2 * hs * 1.0001]), np.zeros(1),
-                                 np.array([hs]))
+    out = np.array([sup * hs * 1.0001])
+    w2, a, b = oracle_mod.kernel(skf, out, out, np.zeros(1), np.array([hs]))
     assert w2[0] == 0 and a[0] == 0
 
 
@@ -70,10 +83,28 @@ def test_dem_topol_library_matches_oracle(oracle_mod):
         assert np.allclose(a[:, :13], b[:, :13], rtol=2e-5, atol=2e-5)
 
 
-def brute_force_sets(x, h):
-    """O(N^2) neighbour sets with the reference's FP32 operations."""
+def reference_grid_cells(x, h):
+    """Cells of grid_find_NEW_tools' own grid (My_SPH_Tools_2019.f90:1168-1204)
+    in FP32: cells of 2*max(hsml), origin shifted to centre the cells."""
+    f = np.float32
+    delt = f(h.max()) * f(2)
+    cells = []
+    for d in range(2):
+        xmn, xmx = f(x[:, d].min()), f(x[:, d].max())
+        length = f(xmx - xmn)
+        nd = int(f(length / delt) + f(1))
+        xmin = f(f(xmn - f(f(f(nd) * delt) - length) / f(2)) - f(f(0.001) * length))
+        c = (((x[:, d] - xmin).astype(np.float32) / delt).astype(np.float32) + f(1)).astype(np.int64)
+        cells.append(np.minimum(c, nd))
+    return np.stack(cells, 1)
+
+
+def brute_force_sets(x, h, scale=2, grid=False):
+    """O(N^2) neighbour sets with the reference's FP32 operations; r < scale*h
+    and, when grid, only pairs in the same or adjacent cells of its grid."""
     x = x.astype(np.float32)
     h = h.astype(np.float32)
+    cells = reference_grid_cells(x, h) if grid else None
     n = x.shape[0]
     sets = []
     for i in range(n):
@@ -83,7 +114,9 @@ def brute_force_sets(x, h):
         dr = (dr + (d1 * d1).astype(np.float32)).astype(np.float32)
         mh = ((h[i] + h) / np.float32(2)).astype(np.float32)
         r = np.sqrt(dr).astype(np.float32)
-        m = r < (np.float32(2) * mh)
+        m = r < (np.float32(scale) * mh)
+        if grid:
+            m &= np.all(np.abs(cells - cells[i]) <= 1, axis=1)
         m[i] = False
         sets.append(np.nonzero(m)[0])
     return sets
@@ -91,6 +124,8 @@ def brute_force_sets(x, h):
 
 @pytest.mark.parametrize("nnps", [2, 4])
 def test_neighbour_sets_match_brute_force(oracle_mod, nnps):
+    """Supports of 2h: every pair with r < 2h lies within one cell of the
+    reference's grid, so the sets are those of an exhaustive search."""
     rng = np.random.default_rng(3)
     n = 700
     x = rng.uniform(0, 40, size=(n, 2)).astype(np.float32)
@@ -102,6 +137,24 @@ def test_neighbour_sets_match_brute_force(oracle_mod, nnps):
     off, idx = res["offsets"], res["idx"]
     for i in range(n):
         assert np.array_equal(np.sort(idx[off[i]:off[i + 1]]), ref[i]), i
+
+
+@pytest.mark.parametrize("skf", [2, 3])
+def test_neighbour_sets_of_3h_supports_follow_the_reference_grid(oracle_mod, skf):
+    """Supports of 3h (skf 2, 3): grid_find keeps r < 3h only for particles
+    in the same or adjacent cells of its 2*max(hsml) grid, so some pairs
+    within 3h are dropped and the sets depend on where the grid falls."""
+    rng = np.random.default_rng(5)
+    n = 600
+    x = rng.uniform(0, 40, size=(n, 2)).astype(np.float32)
+    h = rng.uniform(0.6, 1.6, size=n).astype(np.float32)
+    res = oracle_mod.pairs(0, params(skf=skf), x, h)
+    ref = brute_force_sets(x, h, scale=3, grid=True)
+    full = brute_force_sets(x, h, scale=3)
+    off, idx = res["offsets"], res["idx"]
+    for i in range(n):
+        assert np.array_equal(np.sort(idx[off[i]:off[i + 1]]), ref[i]), i
+    assert sum(len(a) for a in full) > sum(len(a) for a in ref)  # the grid drops pairs
 
 
 def test_still_layer_interior_force_is_zero(oracle_mod):
