@@ -242,12 +242,16 @@ int profile_collect(gfsph_handle* h) {
 // Side stream for the coarse-level kernels while a graph is captured.
 cudaStream_t side_stream(gfsph_handle* h) { return h->capturing ? h->stream2 : h->stream; }
 
-// Calls f with std::integral_constant<int, SK>, SK = scale_k of the kernel's
-// support: 3 for skf 2 and 3, else 2.
+// Calls f with std::integral_constant<int, skf>: the neighbour kernels are
+// compiled per SPH kernel function (skf 1 to 4).
 template <class F>
-void with_sk(const gfsph_handle* h, F&& f) {
-    if (h->rheo.skf == 2 || h->rheo.skf == 3) f(std::integral_constant<int, 3>{});
-    else f(std::integral_constant<int, 2>{});
+void with_skf(const gfsph_handle* h, F&& f) {
+    switch (h->rheo.skf) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 3: f(std::integral_constant<int, 3>{}); break;
+    default: f(std::integral_constant<int, 4>{}); break;
+    }
 }
 
 // Stage-dependent pressure: the step runs the staged RK45 kernels.
@@ -325,11 +329,11 @@ int enqueue_search(gfsph_handle* h, int advance) {
     // captured (side stream); serially otherwise
     cudaStream_t sb = side_stream(h);
     fork(h, 0);
-    with_sk(h, [&](auto sk) {
-        constexpr int SK = decltype(sk)::value;
-        launch(h, K_DENSITY_BIG, [&] { k_density_big<SK><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
-        launch(h, K_DENSITY, [&] { k_density<false, SK><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
-        launch(h, K_DENSITY_SPARSE, [&] { k_density<true, SK><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
+    with_skf(h, [&](auto sk) {
+        constexpr int SKF = decltype(sk)::value;
+        launch(h, K_DENSITY_BIG, [&] { k_density_big<SKF><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
+        launch(h, K_DENSITY, [&] { k_density<false, SKF><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
+        launch(h, K_DENSITY_SPARSE, [&] { k_density<true, SKF><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
     });
     nk += 3;
     join(h, 0);
@@ -354,9 +358,13 @@ int enqueue_norms(gfsph_handle* h, PState As[5]) {
     for (int k = 0; k < 5; k++) {
         const float* hp = k ? As[k - 1].rho : h->rho0;
         const int clamp = k ? 1 : 0;
-        launch(h, K_NORM, [&] { k_norm<<<blocks_for(n), kThreads, 0, st>>>(h->A, q, h->S, c, n, hp, clamp, As[k].rho); });
+        launch(h, K_NORM, [&] {
+            with_skf(h, [&](auto sk) {
+                k_norm<decltype(sk)::value><<<blocks_for(n), kThreads, 0, st>>>(h->A, q, h->S, c, n, hp, clamp, As[k].rho);
+            });
+        });
         launch(h, K_NORM_BIG, [&] {
-            with_sk(h, [&](auto sk) {
+            with_skf(h, [&](auto sk) {
                 k_norm_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(h->A, q, h->S, c, hp, clamp, As[k].rho);
             });
         });
@@ -393,10 +401,13 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
     nk += enqueue_stage_begin(h, As);
     for (int s = 0; s < 4; s++) {
         launch(h, K_FORCE_BIG, [&] {
-            with_sk(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[s], q, S, c); });
+            with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[s], q, S, c); });
         });
         nk++;
-        launch(h, K_IFORCE, [&] { k_iforce<<<pb, kThreads, 0, st>>>(As[s], q, S, c, n); }); nk++;
+        launch(h, K_IFORCE, [&] {
+            with_skf(h, [&](auto sk) { k_iforce<decltype(sk)::value><<<pb, kThreads, 0, st>>>(As[s], q, S, c, n); });
+        });
+        nk++;
         launch(h, K_STAGE, [&] {
             if (s < 3) {
                 if (c.cos_theta)
@@ -429,11 +440,15 @@ int enqueue_step(gfsph_handle* h) {
         nk += enqueue_stages(h, As);
         if (h->rheo.av_vel) {  // av_vel with the final depth
             launch(h, K_XSPH_BIG, [&] {
-                with_sk(h, [&](auto sk) {
+                with_skf(h, [&](auto sk) {
                     k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[4], q, S, h->rheo, h->B, h->velfin);
                 });
             });
-            launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(As[4], q, S, h->rheo, n, h->B, h->velfin); });
+            launch(h, K_XSPH, [&] {
+                with_skf(h, [&](auto sk) {
+                    k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(As[4], q, S, h->rheo, n, h->B, h->velfin);
+                });
+            });
             nk += 2;
         }
         if (h->rheo.erosion) {
@@ -448,10 +463,13 @@ int enqueue_step(gfsph_handle* h) {
     cudaStream_t sb = side_stream(h);
     fork(h, 1);
     launch(h, K_FORCE_BIG, [&] {
-        with_sk(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
+        with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
     });
     nk++;
-    launch(h, K_IFORCE, [&] { k_iforce<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); }); nk++;
+    launch(h, K_IFORCE, [&] {
+        with_skf(h, [&](auto sk) { k_iforce<decltype(sk)::value><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
+    });
+    nk++;
     join(h, 1);
     launch(h, K_FORCE_RK, [&] {
         k_force_rk<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
@@ -459,12 +477,17 @@ int enqueue_step(gfsph_handle* h) {
     if (h->rheo.av_vel) {
         fork(h, 2);
         launch(h, K_XSPH_BIG, [&] {
-            with_sk(h, [&](auto sk) {
+            with_skf(h, [&](auto sk) {
                 k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo, h->B, h->velfin);
             });
         });
         nk++;
-        launch(h, K_XSPH, [&] { k_xsph<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B, h->velfin); }); nk++;
+        launch(h, K_XSPH, [&] {
+            with_skf(h, [&](auto sk) {
+                k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B, h->velfin);
+            });
+        });
+        nk++;
         join(h, 2);
     }
     if (h->rheo.erosion) {
@@ -1060,9 +1083,14 @@ int gfsph_density(gfsph_handle* h, float* rho_out) {
     int n = h->n;
     if (h->rheo.nor_density) {  // the first call of the step: normalised with the depths held
         Search q = make_search(h);
-        launch(h, K_NORM, [&] { k_norm<<<blocks_for(n), kThreads, 0, h->stream>>>(h->A, q, h->S, h->rheo, n, h->rho0, 0, h->rhoS); });
+        launch(h, K_NORM, [&] {
+            with_skf(h, [&](auto sk) {
+                k_norm<decltype(sk)::value><<<blocks_for(n), kThreads, 0, h->stream>>>(h->A, q, h->S, h->rheo, n, h->rho0, 0,
+                                                                                   h->rhoS);
+            });
+        });
         launch(h, K_NORM_BIG, [&] {
-            with_sk(h, [&](auto sk) {
+            with_skf(h, [&](auto sk) {
                 k_norm_big<decltype(sk)::value><<<big_blocks(h), 128, 0, h->stream>>>(h->A, q, h->S, h->rheo, h->rho0, 0,
                                                                                      h->rhoS);
             });
@@ -1090,9 +1118,11 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
     } else {
         As[0] = h->A;
     }
-    launch(h, K_IFORCE, [&] { k_iforce<<<blocks_for(n), kThreads, 0, s>>>(As[0], q, h->S, h->rheo, n); });
+    launch(h, K_IFORCE, [&] {
+        with_skf(h, [&](auto sk) { k_iforce<decltype(sk)::value><<<blocks_for(n), kThreads, 0, s>>>(As[0], q, h->S, h->rheo, n); });
+    });
     launch(h, K_FORCE_BIG, [&] {
-        with_sk(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });
+        with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });
     });
     launch(h, K_FORCE_RK, [&] {
         k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 1,
@@ -1130,7 +1160,7 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
             cudaMemset(dcount, 0, sizeof(int));
             Search q = make_search(h);
             launch(h, K_EXPORT, [&] {
-                with_sk(h, [&](auto sk) {
+                with_skf(h, [&](auto sk) {
                     k_export_big<decltype(sk)::value><<<big_blocks(h), 128, 0, h->stream>>>(q, h->S, dpairs, dcount, pcap);
                 });
             });

@@ -25,11 +25,11 @@ __device__ __forceinline__ float ipow5(float x) {
 // Gaussian's exp is evaluated in FP64 and rounded once.  The quintic's
 // gradient for q <= 1 is the reference's (-120 + 120 q - 50 q^2)/h^2 dx
 // (:2141), which is not the derivative of its w.
-__device__ __forceinline__ void sph_kernel(int skf, float r, float dx0, float dx1, float hs, float& w,
-                                           float& d0, float& d1) {
+template <int SKF>
+__device__ __forceinline__ void sph_kernel(float r, float dx0, float dx1, float hs, float& w, float& d0, float& d1) {
     float q = r / hs;
     w = 0.f; d0 = 0.f; d1 = 0.f;
-    if (skf == 1) {
+    if (SKF == 1) {
         float factor = 15.f / (((7.f * kPi) * hs) * hs);
         if (q >= 0.f && q <= 1.f) {
             w = factor * ((kTwoThirds - q * q) + ((q * q) * q) / 2.f);
@@ -43,14 +43,14 @@ __device__ __forceinline__ void sph_kernel(int skf, float r, float dx0, float dx
             d0 = -(t * (dx0 / r));
             d1 = -(t * (dx1 / r));
         }
-    } else if (skf == 2) {
+    } else if (SKF == 2) {
         float factor = 1.f / ((hs * hs) * kPi);  // hsml**ndimn * pi**(ndimn/2.)
         if (q >= 0.f && q <= 3.f) {
             w = factor * (float)exp((double)(-(q * q)));
             d0 = w * (-(((2.f * dx0) / hs) / hs));
             d1 = w * (-(((2.f * dx1) / hs) / hs));
         }
-    } else if (skf == 3) {
+    } else if (SKF == 3) {
         float factor = 7.f / (((478.f * kPi) * hs) * hs);
         if (q >= 0.f && q <= 1.f) {
             w = factor * ((ipow5(3.f - q) - 6.f * ipow5(2.f - q)) + 15.f * ipow5(1.f - q));
@@ -83,11 +83,33 @@ __device__ __forceinline__ void sph_kernel(int skf, float r, float dx0, float dx
     }
 }
 
+template <int SKF>
+__device__ __forceinline__ float sph_kernel_w(float r, float hs) {
+    float w, a, b;
+    sph_kernel<SKF>(r, 0.f, 0.f, hs, w, a, b);
+    return w;
+}
+
+// The same with skf known only at run time.
+__device__ __forceinline__ void sph_kernel(int skf, float r, float dx0, float dx1, float hs, float& w, float& d0,
+                                           float& d1) {
+    switch (skf) {
+    case 1: sph_kernel<1>(r, dx0, dx1, hs, w, d0, d1); break;
+    case 2: sph_kernel<2>(r, dx0, dx1, hs, w, d0, d1); break;
+    case 3: sph_kernel<3>(r, dx0, dx1, hs, w, d0, d1); break;
+    default: sph_kernel<4>(r, dx0, dx1, hs, w, d0, d1); break;
+    }
+}
+
 __device__ __forceinline__ float sph_kernel_w(int skf, float r, float hs) {
     float w, a, b;
     sph_kernel(skf, r, 0.f, 0.f, hs, w, a, b);
     return w;
 }
+
+// scale_k of grid_find (My_SPH_Tools_2019.f90:1155-1161): the support in
+// units of the mean smoothing length.
+template <int SKF> struct SupportScale { static constexpr int value = (SKF == 2 || SKF == 3) ? 3 : 2; };
 
 // Neighbour test of grid_find (My_SPH_Tools_2019.f90:1010-1019):
 // dr = dx*dx + dy*dy, mh = (hi+hj)/2, r = sqrt(dr), neighbour iff r < 2*mh.

@@ -767,9 +767,12 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
 // accumulated in FP64.  Also stores the pressure term of IntForces_SW with h
 // clamped to h_inf (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
 // Instantiated for both cell layouts; the launch whose layout this step does
-// not use returns at once.
-template <bool SPARSE, int SK>
-__global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+// not use returns at once.  Held to 40 registers (12 blocks of 128 per SM):
+// the gathers are latency-bound, and 12 resident blocks beat 10 with the
+// 45 registers the compiler would take (4 % on the whole step).
+template <bool SPARSE, int SKF>
+__global__ void __launch_bounds__(128, 12) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+    constexpr int SK = SupportScale<SKF>::value;
     if (S->skip || (S->sparse != 0) != SPARSE) return;
     const int nreg = S->nreg, nlev = S->nlev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
@@ -777,13 +780,13 @@ __global__ void __launch_bounds__(128) k_density(PState A, Search Q, StepScalars
         float2 xi = make_float2(me.x, me.y);
         float hi = me.z;
         const int2 ci = (SK == 2) ? make_int2(0, 0) : Q.rcell[i];
-        double acc = (double)(sph_kernel_w(c.skf, 0.f, hi) * me.w);
+        double acc = (double)(sph_kernel_w<SKF>(0.f, hi) * me.w);
         int cnt = 0;
         for (int k = 0; k < nlev; k++)
             level_neighbours<SPARSE, SK>(Q, S, k, i, xi, hi, ci, [&](int j, float4 o, const PairGeom& g) {
                 if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
                 cnt++;
-                acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
+                acc += (double)(o.w * sph_kernel_w<SKF>(g.r, g.mh));
             });
         Q.ncount[i] = cnt;
         if (cnt > Q.kcap) {  // table too small: stop this step before any state is written
@@ -837,8 +840,9 @@ __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScala
 }
 
 // Summation density of the level >= 1 particles, one warp per particle.
-template <int SK>
+template <int SKF>
 __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    constexpr int SK = SupportScale<SKF>::value;
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -847,12 +851,12 @@ __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepSca
         int i = nreg + b;
         double acc = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
-            acc += (double)(o.w * sph_kernel_w(c.skf, g.r, g.mh));
+            acc += (double)(o.w * sph_kernel_w<SKF>(g.r, g.mh));
         });
         acc = warp_sum(acc);
         if (lane == 0) {
             float4 me = Q.xhm[i];
-            float h = (float)((double)(sph_kernel_w(c.skf, 0.f, me.z) * me.w) + acc);
+            float h = (float)((double)(sph_kernel_w<SKF>(0.f, me.z) * me.w) + acc);
             A.rho[i] = h;
             float hc = (h < c.h_inf) ? c.h_inf : h;
             float p = (c.cgra05 * hc) * hc;
@@ -862,10 +866,11 @@ __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepSca
 }
 
 // One pair term of IntForces_SW (SPH_SW_2019.f90:6905-6920) for particle i.
+template <int SKF>
 __device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rhoi, float pj, float rhoj, float mj,
                                               const PairGeom& g, double& a0, double& a1) {
     float w, d0, d1;
-    sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+    sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
     float h0, h1;
     if (c.pa_sph == 1) {
         rhoi = (rhoi < c.h_inf) ? c.h_inf : rhoi;
@@ -882,8 +887,9 @@ __device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rh
 }
 
 // Internal acceleration of the level >= 1 particles, one warp per particle.
-template <int SK>
+template <int SKF>
 __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    constexpr int SK = SupportScale<SKF>::value;
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -893,7 +899,7 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
         float pi_ = Q.pterm[i], rhoi = A.rho[i];
         double a0 = 0.0, a1 = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
-            pressure_pair(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
+            pressure_pair<SKF>(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
         });
         a0 = warp_sum(a0);
         a1 = warp_sum(a1);
@@ -904,6 +910,7 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
 // Internal acceleration of a level-0 particle over its neighbour table.  The
 // table is read four entries at a time so that four independent gather
 // chains are in flight per thread; the FP64 sum keeps the table order.
+template <int SKF>
 __device__ __forceinline__ void internal_force(const PState& A, const Search& Q, const Rheo& c, int i, int n,
                                                float& in0, float& in1) {
     float4 me = Q.xhm[i];
@@ -931,7 +938,7 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
         for (int u = 0; u < 4; u++) {
             PairGeom g;
             pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
-            pressure_pair(c, pi_, rhoi, pj[u], rj[u], o[u].w, g, a0, a1);
+            pressure_pair<SKF>(c, pi_, rhoi, pj[u], rj[u], o[u].w, g, a0, a1);
         }
     }
     for (; k < cnt; k++) {
@@ -939,7 +946,7 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
         float4 o = __ldg(&Q.xhm[j]);
         PairGeom g;
         pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-        pressure_pair(c, pi_, rhoi, __ldg(&Q.pterm[j]), __ldg(&A.rho[j]), o.w, g, a0, a1);
+        pressure_pair<SKF>(c, pi_, rhoi, __ldg(&Q.pterm[j]), __ldg(&A.rho[j]), o.w, g, a0, a1);
     }
     in0 = (float)a0;
     in1 = (float)a1;
@@ -1052,12 +1059,13 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
 }
 
 // Internal acceleration of the level-0 particles, one thread each.
+template <int SKF>
 __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip) return;
     const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         float in0, in1;
-        internal_force(A, Q, c, i, n, in0, in1);
+        internal_force<SKF>(A, Q, c, i, n, in0, in1);
         Q.indv[i] = make_float2(in0, in1);
     }
 }
@@ -1109,7 +1117,7 @@ __global__ void __launch_bounds__(128, 7) k_force_rk(PState A, Search Q, StepSca
         float ex0 = 0.f, ex1 = 0.f;
         float Dx0 = 0.f, Dx1 = 0.f, Dv0 = 0.f, Dv1 = 0.f;
         bool out = false;
-#pragma unroll
+#pragma unroll 1  // one copy of ExtForces_SW(0): the unrolled body overflows the instruction cache
         for (int s = 0; s < 4; s++) {
             const float f1 = (s == 0) ? 0.f : (s == 3 ? 1.f : 0.5f);
             const float f2 = (s == 0 || s == 3) ? 1.f : 2.f;
@@ -1170,6 +1178,7 @@ __device__ __forceinline__ float prev_depth(const Rheo& c, const float* hp, int 
 // One normalised sum_density_Tools call for the level-0 particles, over the
 // neighbour table: h_i = num_i / (W(0,h_i) m_i/hp_i + sum_j (m_j/hp_j) W_ij),
 // num_i the plain sum of k_density (in A.rho), hp the previous call's depths.
+template <int SKF>
 __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S, Rheo c, int n, const float* hp,
                                               int clamp_prev, float* hout) {
     if (S->skip) return;
@@ -1178,7 +1187,7 @@ __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S
         const float4 me = Q.xhm[i];
         const float2 xi = make_float2(me.x, me.y);
         const float hi = me.z;
-        double den = (double)((sph_kernel_w(c.skf, 0.f, hi) * me.w) / prev_depth(c, hp, i, clamp_prev));
+        double den = (double)((sph_kernel_w<SKF>(0.f, hi) * me.w) / prev_depth(c, hp, i, clamp_prev));
         const int cnt = Q.ncount[i];
         const int* tab = Q.nbr + i;
         for (int k = 0; k < cnt; k++) {
@@ -1186,16 +1195,17 @@ __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S
             const float4 o = __ldg(&Q.xhm[j]);
             PairGeom g;
             pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-            den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w(c.skf, g.r, g.mh));
+            den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w<SKF>(g.r, g.mh));
         }
         hout[i] = A.rho[i] / (float)den;
     }
 }
 
 // The same for the level >= 1 particles, one warp each.
-template <int SK>
+template <int SKF>
 __global__ void __launch_bounds__(128) k_norm_big(PState A, Search Q, StepScalars* S, Rheo c, const float* hp,
                                                   int clamp_prev, float* hout) {
+    constexpr int SK = SupportScale<SKF>::value;
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1204,12 +1214,12 @@ __global__ void __launch_bounds__(128) k_norm_big(PState A, Search Q, StepScalar
         const int i = nreg + b;
         double den = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
-            den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w(c.skf, g.r, g.mh));
+            den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w<SKF>(g.r, g.mh));
         });
         den = warp_sum(den);
         if (lane == 0) {
             const float4 me = Q.xhm[i];
-            den = (double)((sph_kernel_w(c.skf, 0.f, me.z) * me.w) / prev_depth(c, hp, i, clamp_prev)) + den;
+            den = (double)((sph_kernel_w<SKF>(0.f, me.z) * me.w) / prev_depth(c, hp, i, clamp_prev)) + den;
             hout[i] = A.rho[i] / (float)den;
         }
     }
@@ -1350,9 +1360,10 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
 }
 
 // One pair term of av_vel (SPH_MAIN_2019.f90:3072-3080) for particle i.
+template <int SKF>
 __device__ __forceinline__ void xsph_pair(const Rheo& c, float2 vi, float rhoi, float2 vj, float rhoj, float mj,
                                           const PairGeom& g, double& a0, double& a1) {
-    float w = sph_kernel_w(c.skf, g.r, g.mh);
+    float w = sph_kernel_w<SKF>(g.r, g.mh);
     float den = rhoi + rhoj;
     float t0 = (((2.f * mj) * (vi.x - vj.x)) / den) * w;
     float t1 = (((2.f * mj) * (vi.y - vj.y)) / den) * w;
@@ -1362,6 +1373,7 @@ __device__ __forceinline__ void xsph_pair(const Rheo& c, float2 vi, float rhoi, 
 
 // av_vel (SPH_MAIN_2019.f90:3042-3099) with the start-of-step W_ij, then
 // v += 0.3*av for particles still inside the domain (:987-993).
+template <int SKF>
 __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S, Rheo c, int n, PState B,
                                                const float2* velfin) {
     if (S->skip || !c.av_vel) return;
@@ -1395,7 +1407,7 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
             for (int u = 0; u < 4; u++) {
                 PairGeom g;
                 pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
-                xsph_pair(c, vi, rhoi, vj[u], rj[u], mj[u], g, a0, a1);
+                xsph_pair<SKF>(c, vi, rhoi, vj[u], rj[u], mj[u], g, a0, a1);
             }
         }
         for (; k < cnt; k++) {
@@ -1403,16 +1415,17 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
             float4 o = __ldg(&Q.xhm[j]);
             PairGeom g;
             pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-            xsph_pair(c, vi, rhoi, velfin[j], __ldg(&A.rho[j]), B.mass[j], g, a0, a1);
+            xsph_pair<SKF>(c, vi, rhoi, velfin[j], __ldg(&A.rho[j]), B.mass[j], g, a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
     }
 }
 
-template <int SK>
+template <int SKF>
 __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B,
                                                    const float2* velfin) {
+    constexpr int SK = SupportScale<SKF>::value;
     if (S->skip || !c.av_vel) return;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1424,7 +1437,7 @@ __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalar
         float rhoi = A.rho[i];
         double a0 = 0.0, a1 = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
-            xsph_pair(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
+            xsph_pair<SKF>(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
         });
         a0 = warp_sum(a0);
         a1 = warp_sum(a1);
@@ -1473,8 +1486,9 @@ __global__ void k_step_end(StepScalars* S) {
 
 // Neighbour pairs of the level >= 1 particles, for the parity export: every
 // (big i, j) pair with r < hi + hj, written as slot pairs.
-template <int SK>
+template <int SKF>
 __global__ void k_export_big(Search Q, StepScalars* S, int2* pairs, int* npairs, int cap) {
+    constexpr int SK = SupportScale<SKF>::value;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nreg = S->nreg, nbig = S->nbig;

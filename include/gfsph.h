@@ -63,9 +63,10 @@ extern "C" {
 typedef struct gfsph_params {
     float cst[GFSPH_NCONST];
     int pa_sph;            /* 1 or 2, SPH_SW_2019.f90:6905-6920 */
-    int nnps;              /* 2 or 4 (grid_find_NEW_tools / _tools3); neighbour sets are the same */
+    int nnps;              /* 2 or 4 (grid_find_NEW_tools / _tools3); the same sets for skf 1 and 4 */
     int sle;               /* 0 keep hsml, 1 hsml = 2 sqrt(m/h) (h_upgrade SPH_MAIN_2019.f90:2925-2931) */
-    int skf;               /* 1 cubic spline, 4 Wendland C2 (kernel_TOOLS My_SPH_Tools_2019.f90:2062) */
+    int skf;               /* 1 cubic spline, 2 Gaussian, 3 quintic, 4 Wendland C2 (kernel_TOOLS
+                              My_SPH_Tools_2019.f90:2062); 2 and 3 (support 3h) need nnps 2 */
     int summation_density; /* must be 1 (sum_density_Tools) */
     int average_velocity;  /* 1 applies av_vel (XSPH, SPH_MAIN_2019.f90:3042-3099) */
     int nor_density;       /* 1 divides each density sum by sum_j (m_j/h_j) W_ij
