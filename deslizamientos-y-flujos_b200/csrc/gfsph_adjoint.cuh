@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(128) k_adj_xsph(PState A, Search Q, Rheo c, in
         const int cnt = Q.ncount[k];
         double s = 0.0, a0 = 0.0, a1 = 0.0, dm = 0.0, dh = 0.0, dx0 = 0.0, dx1 = 0.0;
         for (int q = 0; q < cnt; q++) {
-            const int j = Q.nbr[(size_t)q * n + k];
+            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride];
             const float4 o = Q.xhm[j];
             PairGeom g;
             pair_test(xk, make_float2(o.x, o.y), me.z, o.z, g);
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(128) k_adj_gather(PState A, Search Q, Rheo c, 
         double dm = (double)(lhk * sph_kernel_w(c.skf, 0.f, me.z));
         double dx0 = 0.0, dx1 = 0.0;
         for (int q = 0; q < cnt; q++) {
-            const int j = Q.nbr[(size_t)q * n + k];
+            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride];
             const float4 o = Q.xhm[j];
             PairGeom g;
             pair_test(xk, make_float2(o.x, o.y), me.z, o.z, g);

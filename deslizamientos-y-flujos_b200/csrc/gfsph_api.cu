@@ -549,7 +549,8 @@ int alloc_cells(gfsph_handle* h, int cap) {
 
 int alloc_nbr(gfsph_handle* h, int kcap) {
     dfree(h->nbr);
-    if (dalloc(&h->nbr, (size_t)kcap * (size_t)std::max(h->n, 1))) return GFSPH_ERR_CUDA;
+    const size_t rows = ((size_t)std::max(h->n, 1) + 31) / 32 * 32;  // whole warps (tab_base)
+    if (dalloc(&h->nbr, (size_t)kcap * rows)) return GFSPH_ERR_CUDA;
     h->kcap = kcap;
     drop_graphs(h);
     return 0;
@@ -1142,14 +1143,14 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
     int st = read_scalars(h);
     if (st) return st;
     int nreg = h->hS->nreg, nbig = h->hS->nbig;
-    std::vector<int> cnt(n), id(n), tab((size_t)h->kcap * n);
+    std::vector<int> cnt(n), id(n), tab((size_t)h->kcap * (((size_t)n + 31) / 32 * 32));
     CK(cudaMemcpy(cnt.data(), h->ncount, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(id.data(), h->A.id, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(tab.data(), h->nbr, tab.size() * sizeof(int), cudaMemcpyDeviceToHost));
     std::vector<std::vector<int>> lists(n);
     for (int s = 0; s < nreg; s++) {
         auto& L = lists[id[s]];
-        for (int k = 0; k < cnt[s] && k < h->kcap; k++) L.push_back(id[tab[(size_t)k * n + s]]);
+        for (int k = 0; k < cnt[s] && k < h->kcap; k++) L.push_back(id[tab[tab_base(s, h->kcap) + (size_t)k * kTabStride]]);
     }
     if (nbig > 0) {  // pairs of the big particles, found on the device
         int pcap = 1 << 20;

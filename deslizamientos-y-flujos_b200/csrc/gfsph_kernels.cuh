@@ -86,7 +86,7 @@ struct Search {
     const int* start;    // cell key -> first particle slot (exclusive scan), ncells+1
     const int* cellA;    // slot -> cell key (all levels), -1 out of the domain
     const float4* xhm;   // slot -> (x, y, hsml, mass) at the start of the step
-    int* nbr;            // k-major neighbour table of the regular particles
+    int* nbr;            // neighbour table of the regular particles (layout: tab_base)
     int* ncount;
     float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
     float2* indv;        // internal acceleration of every active particle (slot order)
@@ -96,6 +96,15 @@ struct Search {
 };
 
 __device__ __forceinline__ bool step_skipped(const StepScalars* S) { return S->skip != 0; }
+
+// Neighbour-table layout, blocked by warps of 32 particles: entry k of
+// particle i is at tab_base(i, kcap) + 32 k.  The lanes of a warp read entry k
+// of their particles as one 128-byte line, and the entries a warp appends
+// while its lanes are at different k stay within its own 32 kcap words.
+__host__ __device__ __forceinline__ size_t tab_base(int i, int kcap) {
+    return (size_t)(i >> 5) * ((size_t)kcap << 5) + (size_t)(i & 31);
+}
+constexpr int kTabStride = 32;
 
 // ---------------------------------------------------------------- prologue
 // Decides whether the coming step runs and resets its reductions; run at the
@@ -762,7 +771,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
 
 // Neighbour search and summation density of the level-0 particles, fused:
 // every j with r < 2*(hi+hj)/2 (the pair set of grid_find, :987-1060), on
-// every level, is appended to the neighbour table (k-major, nbr[k*n + i]),
+// every level, is appended to the neighbour table (tab_base),
 // and h_i = W(0,h_i) m_i + sum_j m_j W_ij (sum_density_Tools :1796-1836) is
 // accumulated in FP64.  Also stores the pressure term of IntForces_SW with h
 // clamped to h_inf (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
@@ -781,10 +790,11 @@ __global__ void __launch_bounds__(128, 12) k_density(PState A, Search Q, StepSca
         float hi = me.z;
         const int2 ci = (SK == 2) ? make_int2(0, 0) : Q.rcell[i];
         double acc = (double)(sph_kernel_w<SKF>(0.f, hi) * me.w);
+        int* tab = Q.nbr + tab_base(i, Q.kcap);
         int cnt = 0;
         for (int k = 0; k < nlev; k++)
             level_neighbours<SPARSE, SK>(Q, S, k, i, xi, hi, ci, [&](int j, float4 o, const PairGeom& g) {
-                if (cnt < Q.kcap) Q.nbr[(size_t)cnt * n + i] = j;
+                if (cnt < Q.kcap) tab[(size_t)cnt * kTabStride] = j;
                 cnt++;
                 acc += (double)(o.w * sph_kernel_w<SKF>(g.r, g.mh));
             });
@@ -920,14 +930,14 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
     float rhoi = A.rho[i];
     double a0 = 0.0, a1 = 0.0;
     const int cnt = Q.ncount[i];
-    const int* tab = Q.nbr + i;
+    const int* tab = Q.nbr + tab_base(i, Q.kcap);
     int k = 0;
     for (; k + 4 <= cnt; k += 4) {
         int j[4];
         float4 o[4];
         float pj[4], rj[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * n);
+        for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             o[u] = __ldg(&Q.xhm[j[u]]);
@@ -942,7 +952,7 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
         }
     }
     for (; k < cnt; k++) {
-        int j = __ldg(tab + (size_t)k * n);
+        int j = __ldg(tab + (size_t)k * kTabStride);
         float4 o = __ldg(&Q.xhm[j]);
         PairGeom g;
         pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
@@ -1189,9 +1199,9 @@ __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S
         const float hi = me.z;
         double den = (double)((sph_kernel_w<SKF>(0.f, hi) * me.w) / prev_depth(c, hp, i, clamp_prev));
         const int cnt = Q.ncount[i];
-        const int* tab = Q.nbr + i;
+        const int* tab = Q.nbr + tab_base(i, Q.kcap);
         for (int k = 0; k < cnt; k++) {
-            const int j = __ldg(tab + (size_t)k * n);
+            const int j = __ldg(tab + (size_t)k * kTabStride);
             const float4 o = __ldg(&Q.xhm[j]);
             PairGeom g;
             pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
@@ -1386,7 +1396,7 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
         float2 vi = velfin[i];
         float rhoi = A.rho[i];
         const int cnt = Q.ncount[i];
-        const int* tab = Q.nbr + i;
+        const int* tab = Q.nbr + tab_base(i, Q.kcap);
         double a0 = 0.0, a1 = 0.0;
         int k = 0;
         for (; k + 4 <= cnt; k += 4) {
@@ -1395,7 +1405,7 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
             float2 vj[4];
             float rj[4], mj[4];
 #pragma unroll
-            for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * n);
+            for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 o[u] = __ldg(&Q.xhm[j[u]]);
@@ -1411,7 +1421,7 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
             }
         }
         for (; k < cnt; k++) {
-            int j = __ldg(tab + (size_t)k * n);
+            int j = __ldg(tab + (size_t)k * kTabStride);
             float4 o = __ldg(&Q.xhm[j]);
             PairGeom g;
             pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
