@@ -12,6 +12,8 @@
 // particles, and only those blocks get cells (slot-major keys: slot * 256 +
 // row * 32 + column), so the cell count follows the area the flow covers.
 #pragma once
+#include <climits>
+
 #include "gfsph_device.cuh"
 
 namespace gfsph {
@@ -962,6 +964,35 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
     in1 = (float)a1;
 }
 
+// DEM node box touched by the erosion scatter, kept per thread and reduced
+// per block before the four atomics on the step scalars (same-address
+// atomics from every warp serialise).
+struct NodeBox {
+    int x0, x1, y0, y1;
+};
+__device__ __forceinline__ NodeBox empty_node_box() { return NodeBox{INT_MAX, INT_MIN, INT_MAX, INT_MIN}; }
+
+// Every thread of the block must call it (one __syncthreads).
+__device__ __forceinline__ void flush_node_box(StepScalars* S, NodeBox b) {
+    __shared__ NodeBox wb[32];
+    const unsigned full = 0xffffffffu;
+    b.x0 = __reduce_min_sync(full, b.x0); b.x1 = __reduce_max_sync(full, b.x1);
+    b.y0 = __reduce_min_sync(full, b.y0); b.y1 = __reduce_max_sync(full, b.y1);
+    if ((threadIdx.x & 31) == 0) wb[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        NodeBox t = wb[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+            t.x0 = min(t.x0, wb[w].x0); t.x1 = max(t.x1, wb[w].x1);
+            t.y0 = min(t.y0, wb[w].y0); t.y1 = max(t.y1, wb[w].y1);
+        }
+        if (t.x1 >= t.x0) {
+            atomicMin(&S->ex0, t.x0); atomicMax(&S->ex1, t.x1);
+            atomicMin(&S->ey0, t.y0); atomicMax(&S->ey1, t.y1);
+        }
+    }
+}
+
 // DEM scatter of ExtForces_SW(1) (SPH_SW_2019.f90:8731-8750): the particle
 // adds base/dist and 1/dist to the 4x4 DEM nodes around its DEM cell.
 // Consecutive particles of the cell-sorted order mostly share a DEM cell, so
@@ -969,8 +1000,8 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
 // (five shuffle steps) sums every run at once and only the last lane of each
 // run issues the atomics.  Lanes with part == false take no part; every lane
 // of the warp must call this.
-__device__ __forceinline__ void erosion_scatter(const DemView& dem, StepScalars* S, float xx, float xy, float base,
-                                                bool part, double2* auxv) {
+__device__ __forceinline__ void erosion_scatter(const DemView& dem, float xx, float xy, float base, bool part,
+                                                double2* auxv, NodeBox& box) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int ipx = 0, ipy = 0, key = -1 - lane;  // non-participants: singleton runs with zero values
@@ -1015,9 +1046,9 @@ __device__ __forceinline__ void erosion_scatter(const DemView& dem, StepScalars*
                 atomicAdd(&auxv[ip].y, b);
             }
         }
-    if (tail && part) {
-        atomicMin(&S->ex0, ix0); atomicMax(&S->ex1, ix1);
-        atomicMin(&S->ey0, iy0); atomicMax(&S->ey1, iy1);
+    if (part) {
+        box.x0 = min(box.x0, ix0); box.x1 = max(box.x1, ix1);
+        box.y0 = min(box.y0, iy0); box.y1 = max(box.y1, iy1);
     }
 }
 
@@ -1039,7 +1070,8 @@ __device__ __forceinline__ void rk_carry(const PState& A, const Rheo& c, const P
 __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, StepScalars* S, const Rheo& c,
                                           const DemView& dem, const PState& B, float2* velfin, double2* auxv, int i,
                                           float dt, float2 x0, float2 v0, float Dx0, float Dx1, float Dv0, float Dv1,
-                                          float xx, float xy, float vx, float vy, bool out, float h, float pwp) {
+                                          float xx, float xy, float vx, float vy, bool out, float h, float pwp,
+                                          NodeBox& box) {
     float m = A.mass[i];
     float hs = A.hsml[i];
     if (!out) {
@@ -1052,7 +1084,7 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
     }
     float er = 0.f;
     if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h, pwp);
-    if (c.erosion) erosion_scatter(dem, S, xx, xy, dt * er, !out, auxv);
+    if (c.erosion) erosion_scatter(dem, xx, xy, dt * er, !out, auxv, box);
     if (!out) {
         if (c.erosion) m = m + ((dt * er) * m) / h;
         if (c.sle == 1) hs = 2.f * sqrtf(m / h);
@@ -1094,7 +1126,7 @@ __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars*
 // stages.  (A particle that leaves the DEM box mid-step is frozen; the
 // reference then keeps scattering its stale pressure into its neighbours for
 // the remaining stages, which is not reproduced.)
-__global__ void __launch_bounds__(128, 7) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
+__global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
                                                    PState B, float2* velfin, double2* auxv, int forces_only,
                                                    float2* indv_out) {
     if (S->skip) return;
@@ -1105,16 +1137,18 @@ __global__ void __launch_bounds__(128, 7) k_force_rk(PState A, Search Q, StepSca
             indv_out[i] = Q.indv[i];
         return;
     }
-    // block-uniform trip count: every lane of a warp reaches erosion_scatter
+    // block-uniform trip count: every lane of a warp reaches erosion_scatter,
+    // every thread the box flush
+    NodeBox box = empty_node_box();
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
         const int i = i0 + threadIdx.x;
         if (i >= n) {
-            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
+            if (c.erosion) erosion_scatter(dem, 0.f, 0.f, 0.f, false, auxv, box);
             continue;
         }
         if (i >= nact) {  // carried particles (out of the domain at step start)
             rk_carry(A, c, B, velfin, i);
-            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
+            if (c.erosion) erosion_scatter(dem, 0.f, 0.f, 0.f, false, auxv, box);
             continue;
         }
         const float2 fin = Q.indv[i];
@@ -1149,8 +1183,9 @@ __global__ void __launch_bounds__(128, 7) k_force_rk(PState A, Search Q, StepSca
                 }
             }
         }
-        rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, Dx0, Dx1, Dv0, Dv1, xx, xy, vx, vy, out, h, pwp);
+        rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, Dx0, Dx1, Dv0, Dv1, xx, xy, vx, vy, out, h, pwp, box);
     }
+    if (c.erosion) flush_node_box(S, box);
 }
 
 // ---------------------------------------------------------------- staged RK45
@@ -1323,16 +1358,18 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
     if (S->skip) return;
     const int nact = S->nactive;
     const float dt = S->dt_step;
-    // block-uniform trip count: every lane of a warp reaches erosion_scatter
+    // block-uniform trip count: every lane of a warp reaches erosion_scatter,
+    // every thread the box flush
+    NodeBox box = empty_node_box();
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
         const int i = i0 + threadIdx.x;
         if (i >= n) {
-            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
+            if (c.erosion) erosion_scatter(dem, 0.f, 0.f, 0.f, false, auxv, box);
             continue;
         }
         if (i >= nact) {
             rk_carry(A, c, B, velfin, i);
-            if (c.erosion) erosion_scatter(dem, S, 0.f, 0.f, 0.f, false, auxv);
+            if (c.erosion) erosion_scatter(dem, 0.f, 0.f, 0.f, false, auxv, box);
             continue;
         }
         const float2 x0 = A.pos[i], v0 = A.vel[i];
@@ -1365,8 +1402,9 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
             }
         }
         rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, dx.x, dx.y, dv.x, dv.y, xx, xy, vx, vy, out,
-                  hfin[i], pwp);
+                  hfin[i], pwp, box);
     }
+    if (c.erosion) flush_node_box(S, box);
 }
 
 // One pair term of av_vel (SPH_MAIN_2019.f90:3072-3080) for particle i.
