@@ -35,6 +35,7 @@ const char* kKernelNames[K_COUNT] = {
     "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "k_adjoint", "k_norm", "k_norm_big", "k_stage", "step_batches"};
 
 constexpr int kThreads = 128;
+static_assert(kThreads <= 32 * kScatterWarps, "erosion_scatter keeps shared terms for kScatterWarps warps");
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
 constexpr int kChunkSteps = 256;     // steps between host checks of the error word
 constexpr int kMaxCells = kScanTile * 8192;

@@ -996,59 +996,73 @@ __device__ __forceinline__ void flush_node_box(StepScalars* S, NodeBox b) {
 // DEM scatter of ExtForces_SW(1) (SPH_SW_2019.f90:8731-8750): the particle
 // adds base/dist and 1/dist to the 4x4 DEM nodes around its DEM cell.
 // Consecutive particles of the cell-sorted order mostly share a DEM cell, so
-// within a warp the lanes form runs of equal DEM cell; a segmented FP64 scan
-// (five shuffle steps) sums every run at once and only the last lane of each
-// run issues the atomics.  Lanes with part == false take no part; every lane
-// of the warp must call this.
+// within a warp the lanes form runs of equal DEM cell.  Each lane writes its
+// 32 FP32 terms (16 nodes x {base/dist, 1/dist}) to shared memory; then lane t
+// adds up term t over each run of lanes, in lane order and in FP64, and
+// issues that run's atomic for it.  The run boundaries are the same for every
+// lane, so the summing loop does not diverge.  Lanes with part == false take
+// no part; every lane of the warp must call this, in blocks of at most
+// kScatterWarps warps.
+constexpr int kScatterWarps = 4;
 __device__ __forceinline__ void erosion_scatter(const DemView& dem, float xx, float xy, float base, bool part,
                                                 double2* auxv, NodeBox& box) {
+    __shared__ float sterm[kScatterWarps][32][33];  // [term][lane], padded against bank conflicts
+    __shared__ int skey[kScatterWarps][33], spx[kScatterWarps][32], spy[kScatterWarps][32];
     const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    int ipx = 0, ipy = 0, key = -1 - lane;  // non-participants: singleton runs with zero values
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int ipx = 0, ipy = 0, key = -1 - lane;  // non-participants: singleton runs with zero terms
     if (part) {
         ipx = (int)((xx - dem.xmin) / dem.dx + 1.f);
         ipy = (int)((xy - dem.ymin) / dem.dy + 1.f);
         key = ipy * (dem.nx + 2) + ipx;
     }
     if (!__any_sync(full, part)) return;
-    const int prev = __shfl_up_sync(full, key, 1);
-    const bool head = (lane == 0) || (prev != key);
-    const unsigned heads = __ballot_sync(full, head);
-    const int first = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));  // head of my run
-    const int next = __shfl_down_sync(full, key, 1);
-    const bool tail = (lane == 31) || (next != key);
-    const int ix0 = max(1, ipx - 1), iy0 = max(1, ipy - 1);
-    const int ix1 = min(dem.nx, ipx + 2), iy1 = min(dem.ny, ipy + 2);
-    // every lane walks the same 4x4 offsets; nodes outside the DEM add zero
-    for (int ox = -1; ox <= 2; ox++)
-        for (int oy = -1; oy <= 2; oy++) {
-            const int ix = ipx + ox, iy = ipy + oy;
-            const bool inside = part && ix >= ix0 && ix <= ix1 && iy >= iy0 && iy <= iy1;
-            double a = 0.0, b = 0.0;
-            if (inside) {
-                float ddx = xx - (dem.xmin + (float)(ix - 1) * dem.dx);
-                ddx = ddx * ddx;
-                float ddy = xy - (dem.ymin + (float)(iy - 1) * dem.dy);
-                ddy = ddy * ddy;
-                float dist = sqrtf(ddx + ddy);
-                dist = (1.e-6f > dist) ? 1.e-6f : dist;
-                a = (double)(base / dist);
-                b = (double)(1.f / dist);
-            }
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                double ua = __shfl_up_sync(full, a, o), ub = __shfl_up_sync(full, b, o);
-                if (lane - o >= first) { a += ua; b += ub; }
-            }
-            if (tail && inside) {
-                int ip = (iy - 1) * dem.nx + (ix - 1);
-                atomicAdd(&auxv[ip].x, a);
-                atomicAdd(&auxv[ip].y, b);
-            }
+    float(*T)[33] = sterm[wid];
+    // the 4x4 nodes (ipx-1..ipx+2) x (ipy-1..ipy+2); nodes outside the DEM add zero
+    for (int o = 0; o < 16; o++) {
+        const int ix = ipx + (o >> 2) - 1, iy = ipy + (o & 3) - 1;
+        const bool inside = part && ix >= 1 && ix <= dem.nx && iy >= 1 && iy <= dem.ny;
+        float a = 0.f, b = 0.f;
+        if (inside) {
+            float ddx = xx - (dem.xmin + (float)(ix - 1) * dem.dx);
+            ddx = ddx * ddx;
+            float ddy = xy - (dem.ymin + (float)(iy - 1) * dem.dy);
+            ddy = ddy * ddy;
+            float dist = sqrtf(ddx + ddy);
+            dist = (1.e-6f > dist) ? 1.e-6f : dist;
+            a = base / dist;
+            b = 1.f / dist;
         }
+        T[o][lane] = a;
+        T[16 + o][lane] = b;
+    }
+    skey[wid][lane] = key;
+    if (lane == 0) skey[wid][32] = INT_MIN;  // no key: closes the last run
+    spx[wid][lane] = ipx;
+    spy[wid][lane] = ipy;
+    __syncwarp();
+    const int o = lane & 15, ox = (o >> 2) - 1, oy = (o & 3) - 1;
+    double acc = 0.0;
+    int kr = skey[wid][0];
+    for (int r = 0; r < 32; r++) {
+        acc += (double)T[lane][r];
+        const int kn = skey[wid][r + 1];
+        if (kn != kr) {  // run ends at lane r (the same r for every lane)
+            if (kr >= 0) {
+                const int ix = spx[wid][r] + ox, iy = spy[wid][r] + oy;
+                if (ix >= 1 && ix <= dem.nx && iy >= 1 && iy <= dem.ny) {
+                    double* dst = &auxv[(iy - 1) * dem.nx + (ix - 1)].x;
+                    atomicAdd(dst + (lane >> 4), acc);  // .x for base/dist, .y for 1/dist
+                }
+            }
+            acc = 0.0;
+            kr = kn;
+        }
+    }
+    __syncwarp();  // the terms are rewritten by the next call
     if (part) {
-        box.x0 = min(box.x0, ix0); box.x1 = max(box.x1, ix1);
-        box.y0 = min(box.y0, iy0); box.y1 = max(box.y1, iy1);
+        box.x0 = min(box.x0, max(1, ipx - 1)); box.x1 = max(box.x1, min(dem.nx, ipx + 2));
+        box.y0 = min(box.y0, max(1, ipy - 1)); box.y1 = max(box.y1, min(dem.ny, ipy + 2));
     }
 }
 
