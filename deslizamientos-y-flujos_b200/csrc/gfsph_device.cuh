@@ -139,7 +139,8 @@ __device__ __forceinline__ bool pair_search(float2 xi, float2 xj, float hi, floa
     float d1 = xi.y - xj.y;
     float dr = d0 * d0;
     dr = dr + d1 * d1;
-    float t = (float)SK * ((hi + hj) / 2.f);
+    // SK*((hi+hj)/2): for SK = 2 exactly hi+hj (scaling by 2 and 1/2 is exact)
+    float t = (SK == 2) ? hi + hj : (float)SK * ((hi + hj) / 2.f);
     if (dr > (t * t) * 1.00001f) return false;
     g.dx0 = d0;
     g.dx1 = d1;

@@ -28,7 +28,7 @@ constexpr int kBlkY = 8;            // cells per block along y
 constexpr int kBlockCells = kBlkX * kBlkY;
 constexpr long long kDenseCells = 1LL << 22;  // dense-mode budget (or 8 cells per particle)
 constexpr int kThreadsBounds = 128;
-constexpr int kBoundsBlocks = 148 * 2;
+constexpr int kBoundsBlocks = 148 * 8;
 
 // error bits in StepScalars::err
 constexpr int kErrCells = 1;
@@ -185,11 +185,13 @@ __global__ void __launch_bounds__(kThreadsBounds) k_bounds(PState B, int n, Rheo
     int hs_cnt = 0;
     int bad = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (B.flag[i]) continue;
+        // every load issued before the flag test, so that they overlap
+        const int fl = B.flag[i];
         float2 p = B.pos[i];
         float hs = B.hsml[i];
         float h = B.rho[i];
         float2 v = B.vel[i];
+        if (fl) continue;
         if (!(isfinite(p.x) && isfinite(p.y) && isfinite(hs) && isfinite(h) && isfinite(v.x) && isfinite(v.y))) bad = 1;
         bool out = out_of_box(dem, p.x, p.y);
         if (out && S->advance) B.flag[i] = 1;
