@@ -4,7 +4,7 @@
 //
 // Scope: frictional basal friction (nfric 5/6) with Voellmy xi >= 0, no
 // curvature, erosion or pore pressure, pa_sph 2, fixed hsml (sle 0), fixed dt,
-// all particles on level 0 and inside the DEM.  The step is differentiated
+// all particles regular (no coarse level) and inside the DEM.  The step is differentiated
 // with its neighbour list held fixed (the reference freezes its pair list per
 // step too); branches (reversal filter, h_inf/comp clamps) take the forward's
 // decisions.  With pa_sph 2 the pressure term p/h^2 = g/2 does not depend on

@@ -159,6 +159,7 @@ struct gfsph_handle {
     int cap_blocks = 0;
     BoundsPart* bparts = nullptr;  // k_bounds block partials
     float level_factor = kBigFactor;  // search tunables (gfsph_set_search / gfsph_autotune)
+    int reg_levels = kRegLevels;
     float cell_div = kCellDiv;
     // scalars
     StepScalars* S = nullptr;
@@ -286,7 +287,7 @@ Search make_search(gfsph_handle* h) {
     return q;
 }
 
-int big_blocks(const gfsph_handle*) { return 148 * 16; }  // 128 threads: one warp per level >= 1 particle
+int big_blocks(const gfsph_handle*) { return 148 * 16; }  // 128 threads: one warp per coarse-level particle
 
 // The cell search: bounds, grid, counting sort, reorder, neighbours+density.
 // Returns the number of kernels enqueued.
@@ -302,7 +303,7 @@ int enqueue_search(gfsph_handle* h, int advance) {
     const int* nblk = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, nblocks));
     const int* ncel = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, ncells));
     if (!advance) { launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++; }
-    const GridArgs ga{h->cap_blocks, h->cap_cells, kMaxCells, h->level_factor, h->cell_div};
+    const GridArgs ga{h->cap_blocks, h->cap_cells, kMaxCells, h->level_factor, h->cell_div, h->reg_levels};
     launch(h, K_BOUNDS, [&] {
         k_bounds<<<kBoundsBlocks, kThreadsBounds, 0, st>>>(h->B, n, h->rheo, h->dem, S, h->bparts, ga);
     }); nk++;
@@ -326,7 +327,7 @@ int enqueue_search(gfsph_handle* h, int advance) {
         k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S, h->rheo, h->rho0,
                                            h->rcell);
     }); nk++;
-    // the coarse-level kernels run beside the level-0 ones when graphs are
+    // the coarse-level kernels run beside the regular ones when graphs are
     // captured (side stream); serially otherwise
     cudaStream_t sb = side_stream(h);
     fork(h, 0);
@@ -1492,7 +1493,7 @@ int adj_one_step(gfsph_handle* h) {
         if (st < 0) return st;
         if (done >= 1) break;
     }
-    // every particle active and on level 0 (nbig and nout are cleared when a step ends)
+    // every particle active and regular (nbig and nout are cleared when a step ends)
     if (h->hS->nactive != h->n || h->hS->nreg != h->hS->nactive) return GFSPH_ERR_UNSUPPORTED;
     return 0;
 }

@@ -20,8 +20,9 @@ namespace gfsph {
 
 constexpr int kScanTile = 2048;  // cells per scan tile (256 threads x 8)
 constexpr int kScanThreads = 256;
-constexpr float kBigFactor = 2.5f;  // default level-0 bound: hsml above kBigFactor * mean(hsml) is coarse
+constexpr float kBigFactor = 1.5f;  // default level-0 bound Hc = kBigFactor * mean(hsml)
 constexpr float kCellDiv = 3.f;     // default cell size of level k: Hc * 2^k / kCellDiv
+constexpr int kRegLevels = 2;       // default regular levels: their particles take a thread and the table
 constexpr int kMaxLevels = 24;      // level k cell size Hc * 2^(k-1)
 constexpr int kBlkX = 32;           // cells per block along x
 constexpr int kBlkY = 8;            // cells per block along y
@@ -64,6 +65,7 @@ struct StepScalars {
     int need_cells, need_nbr, need_big, need_blocks;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
     unsigned int bounds_ticket;  // blocks of k_bounds done (the last one resets it)
+    int reg_levels;   // levels 0 .. reg_levels-1 are regular (thread + neighbour table)
     // the reference's own grid of grid_find_NEW_tools (skf 2, 3): origin, cell, cells
     float ref_xmin, ref_ymin, ref_delt;
     int ref_ndx, ref_ndy;
@@ -173,6 +175,7 @@ __device__ __forceinline__ void bounds_merge(BoundsPart& a, const BoundsPart& b)
 struct GridArgs {
     int cap_blocks, cap_cells, max_cells;
     float level_factor, cell_div;
+    int reg_levels;
 };
 
 __device__ void grid_setup(const Rheo& c, StepScalars* S, const GridArgs ga);
@@ -265,9 +268,12 @@ __global__ void __launch_bounds__(kThreadsBounds) k_bounds(PState B, int n, Rheo
 // reference sizes its single grid by 2*max(hsml) (grid_find :906-919), so one
 // thin-front particle whose hsml keeps growing inflates every cell.  Here
 // particles are split by smoothing length into levels: level 0 holds
-// hsml <= Hc = min(max, 2.5*mean), level k >= 1 holds hsml in
-// (Hc*2^(k-1), Hc*2^k]; level k has its own grid of cell size Hc*2^(k-1)
-// over the same box, and one cell-key space covers all levels.  A particle
+// hsml <= Hc = min(max, level_factor*mean), level k >= 1 holds hsml in
+// (Hc*2^(k-1), Hc*2^k]; level k has its own grid of cell size
+// Hc*2^k/cell_div over the same box, and one cell-key space covers all
+// levels.  The particles of the first reg_levels levels ("regular") take a
+// thread each and the neighbour table; those of the coarser levels, few and
+// with long neighbour lists, a warp each.  A particle
 // searches each level within hsml_i + (that level's hsml bound), so the
 // neighbour set is the reference's {j : r_ij < 2*(h_i+h_j)/2} exactly.
 // level_factor and cell_div are the search's tunables (gfsph_set_search):
@@ -276,6 +282,7 @@ __global__ void __launch_bounds__(kThreadsBounds) k_bounds(PState B, int n, Rheo
 __device__ void grid_setup(const Rheo& c, StepScalars* S, const GridArgs ga) {
     const int cap_blocks = ga.cap_blocks, cap_cells = ga.cap_cells, max_cells = ga.max_cells;
     const float level_factor = ga.level_factor, cell_div = ga.cell_div;
+    S->reg_levels = ga.reg_levels;
     if (S->skip) return;
     if (S->bad) { S->err |= kErrNonFinite; S->skip = 1; return; }
     float xmn = o2f(S->xmin_o), xmx = o2f(S->xmax_o), ymn = o2f(S->ymin_o), ymx = o2f(S->ymax_o);
@@ -562,8 +569,11 @@ __global__ void k_scatter(const int2* keyrank, int n, const int* start, const in
         perm[slot] = i;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int first1 = S->sparse ? bstart[S->lev_boff[1]] * kBlockCells : S->lev_off[1];
-        int nreg = (S->nlev > 1) ? start[first1] : nact;
+        // regular particles: levels 0 .. reg_levels-1 (slots before the first
+        // key of level reg_levels; lev_off[nlev] ends the key space)
+        const int r = min(S->nlev, S->reg_levels);
+        int first = S->sparse ? bstart[S->lev_boff[r]] * kBlockCells : S->lev_off[r];
+        int nreg = start[first];
         S->nreg = nreg;
         S->nbig = nact - nreg;
         S->nactive = nact;
@@ -773,7 +783,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
     }
 }
 
-// Neighbour search and summation density of the level-0 particles, fused:
+// Neighbour search and summation density of the regular particles, fused:
 // every j with r < 2*(hi+hj)/2 (the pair set of grid_find, :987-1060), on
 // every level, is appended to the neighbour table (tab_base),
 // and h_i = W(0,h_i) m_i + sum_j m_j W_ij (sum_density_Tools :1796-1836) is
@@ -853,7 +863,7 @@ __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScala
     }
 }
 
-// Summation density of the level >= 1 particles, one warp per particle.
+// Summation density of the coarse-level particles, one warp per particle.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepScalars* S, Rheo c) {
     constexpr int SK = SupportScale<SKF>::value;
@@ -900,7 +910,7 @@ __device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rh
     a1 += (double)(mj * h1);
 }
 
-// Internal acceleration of the level >= 1 particles, one warp per particle.
+// Internal acceleration of the coarse-level particles, one warp per particle.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
     constexpr int SK = SupportScale<SKF>::value;
@@ -921,7 +931,7 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
     }
 }
 
-// Internal acceleration of a level-0 particle over its neighbour table.  The
+// Internal acceleration of a regular particle over its neighbour table.  The
 // table is read four entries at a time so that four independent gather
 // chains are in flight per thread; the FP64 sum keeps the table order.
 template <int SKF>
@@ -1116,7 +1126,7 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
     if (c.icpwp == 3) B.pwp[i] = out ? 0.f : pwp_update(c, pwp, h, h - Q.rho0[i], dt);
 }
 
-// Internal acceleration of the level-0 particles, one thread each.
+// Internal acceleration of the regular particles, one thread each.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip) return;
@@ -1236,7 +1246,7 @@ __device__ __forceinline__ float prev_depth(const Rheo& c, const float* hp, int 
     return (clamp_prev && h < c.h_inf) ? c.h_inf : h;
 }
 
-// One normalised sum_density_Tools call for the level-0 particles, over the
+// One normalised sum_density_Tools call for the regular particles, over the
 // neighbour table: h_i = num_i / (W(0,h_i) m_i/hp_i + sum_j (m_j/hp_j) W_ij),
 // num_i the plain sum of k_density (in A.rho), hp the previous call's depths.
 template <int SKF>
@@ -1262,7 +1272,7 @@ __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S
     }
 }
 
-// The same for the level >= 1 particles, one warp each.
+// The same for the coarse-level particles, one warp each.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_norm_big(PState A, Search Q, StepScalars* S, Rheo c, const float* hp,
                                                   int clamp_prev, float* hout) {
@@ -1548,7 +1558,7 @@ __global__ void k_step_end(StepScalars* S) {
     prepare_step(S, 1);
 }
 
-// Neighbour pairs of the level >= 1 particles, for the parity export: every
+// Neighbour pairs of the coarse-level particles, for the parity export: every
 // (big i, j) pair with r < hi + hj, written as slot pairs.
 template <int SKF>
 __global__ void k_export_big(Search Q, StepScalars* S, int2* pairs, int* npairs, int cap) {

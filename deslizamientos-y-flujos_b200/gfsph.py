@@ -334,7 +334,7 @@ class Sim:
     def stats(self):
         v = np.zeros(8, np.int32)
         _check(lib().gfsph_stats(self.h, _ip(v), 8), "gfsph_stats")
-        keys = ("active", "level0", "coarse", "levels", "cells", "table_capacity", "cell_capacity", "outside")
+        keys = ("active", "regular", "coarse", "levels", "cells", "table_capacity", "cell_capacity", "outside")
         return dict(zip(keys, (int(a) for a in v)))
 
 

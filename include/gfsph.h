@@ -198,8 +198,9 @@ const char* gfsph_kernel_name(int kernel);
  * each kernel node). */
 long long gfsph_launch_count(gfsph_handle* h);
 
-/* Search statistics of the last step: out[0] active particles, [1] level-0
- * particles, [2] particles on the coarser levels, [3] levels, [4] cells,
+/* Search statistics of the last step: out[0] active particles, [1] regular
+ * particles (a thread each and the neighbour table), [2] particles on the
+ * coarse levels (a warp each), [3] levels, [4] cells,
  * [5] neighbour-table capacity per particle, [6] cell capacity, [7] particles
  * outside the DEM box.  Up to nout values are written. */
 int gfsph_stats(gfsph_handle* h, int* out, int nout);
@@ -231,9 +232,11 @@ int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter,
 
 /*
  * Neighbour-search tunables, which change the speed of the search and never
- * its neighbour sets: level-0 particles are those with hsml <= Hc =
- * min(max hsml, level_factor * mean hsml) (default 2.5, range [1, 16]), and
- * level k's cells are Hc * 2^k / cell_div wide (default 3, range [1, 8]).
+ * its neighbour sets: level 0 holds the particles with hsml <= Hc =
+ * min(max hsml, level_factor * mean hsml) (default 1.5, range [1, 16]), level
+ * k >= 1 those with hsml in (Hc 2^(k-1), Hc 2^k]; level k's cells are
+ * Hc * 2^k / cell_div wide (default 3, range [1, 8]).  Levels 0 and 1 are
+ * searched by a thread per particle, coarser ones by a warp per particle.
  * gfsph_autotune times `steps` steps for each of 12 candidate pairs from
  * the current state (restored after every trial), keeps the fastest and
  * returns it with its time per step; the handle's state is unchanged.  The

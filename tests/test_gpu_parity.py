@@ -552,7 +552,7 @@ def test_adaptive_dt_modes_match_oracle(gfsph_lib, oracle_mod, mode):
     sim.close()
 
 
-@pytest.mark.parametrize("tune", [(1.5, 3.0), (3.0, 4.0), (2.0, 1.0)])
+@pytest.mark.parametrize("tune", [(2.5, 3.0), (3.0, 4.0), (2.0, 1.0), (1.0, 2.0)])
 def test_search_tunables_keep_sets_and_results(gfsph_lib, oracle_mod, tune):
     """Other level bounds and cell sizes: the same neighbour sets, and one step
     still on the oracle."""
