@@ -20,18 +20,18 @@ using namespace gfsph;
 namespace {
 
 enum KernelId {
-    K_PREP, K_BOUNDS, K_HIST, K_SCAN_TILES, K_SCAN_TOP, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
+    K_PREP, K_BOUNDS, K_HIST, K_SCAN_TILES, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
-    K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_TOP, K_BSCAN_ADD,
+    K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_ADD,
     K_DENSITY_SPARSE, K_COUPLE, K_ADJOINT, K_NORM, K_NORM_BIG, K_STAGE,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
 const char* kKernelNames[K_COUNT] = {
-    "k_prep", "k_bounds", "k_hist", "k_scan_tiles", "k_scan_top", "k_scan_add",
+    "k_prep", "k_bounds", "k_hist", "k_scan_tiles", "k_scan_add",
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
-    "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)", "k_scan_top(blocks)",
+    "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)",
     "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "k_adjoint", "k_norm", "k_norm_big", "k_stage", "step_batches"};
 
 constexpr int kThreads = 128;
@@ -311,7 +311,6 @@ int enqueue_search(gfsph_handle* h, int advance) {
     launch(h, K_BSCAN_TILES, [&] {
         k_scan_tiles<<<nbscan, kScanThreads, 0, st>>>(h->bmark, h->bstart, h->tile_sum, nblk, S, 1);
     }); nk++;
-    launch(h, K_BSCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, nblk, S, 1); }); nk++;
     launch(h, K_BSCAN_ADD, [&] { k_scan_add<<<nbscan, kScanThreads, 0, st>>>(h->bstart, h->tile_sum, nblk, S, 1); }); nk++;
     launch(h, K_HIST, [&] {
         k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark, h->bstart, h->count, h->keyrank, h->cap_cells);
@@ -319,7 +318,6 @@ int enqueue_search(gfsph_handle* h, int advance) {
     launch(h, K_SCAN_TILES, [&] {
         k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, ncel, S, 0);
     }); nk++;
-    launch(h, K_SCAN_TOP, [&] { k_scan_top<<<1, 1024, 0, st>>>(h->tile_sum, ncel, S, 0); }); nk++;
     launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, ncel, S, 0); }); nk++;
     launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, h->bstart, S, h->perm); }); nk++;
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
@@ -430,6 +428,19 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
     return nk;
 }
 
+// The DEM update of the erosion (its last block ends the step), or the step
+// end alone.  Returns the number of kernels enqueued.
+int enqueue_step_end(gfsph_handle* h) {
+    StepScalars* S = h->S;
+    if (h->rheo.erosion)
+        launch(h, K_DEM_ERODE, [&] {
+            k_dem_erode<<<148 * 2, 256, 0, h->stream>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S);
+        });
+    else
+        launch(h, K_STEP_END, [&] { k_step_end<<<1, 32, 0, h->stream>>>(S); });
+    return 1;
+}
+
 int enqueue_step(gfsph_handle* h) {
     const int n = h->n;
     cudaStream_t st = h->stream;
@@ -453,13 +464,7 @@ int enqueue_step(gfsph_handle* h) {
             });
             nk += 2;
         }
-        if (h->rheo.erosion) {
-            launch(h, K_DEM_ERODE, [&] {
-                k_dem_erode<<<148 * 2, 256, 0, st>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S);
-            });
-            nk++;
-        }
-        launch(h, K_STEP_END, [&] { k_step_end<<<1, 32, 0, st>>>(S); }); nk++;
+        nk += enqueue_step_end(h);
         return nk;
     }
     cudaStream_t sb = side_stream(h);
@@ -492,11 +497,7 @@ int enqueue_step(gfsph_handle* h) {
         nk++;
         join(h, 2);
     }
-    if (h->rheo.erosion) {
-        launch(h, K_DEM_ERODE, [&] { k_dem_erode<<<148 * 2, 256, 0, st>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S); });
-        nk++;
-    }
-    launch(h, K_STEP_END, [&] { k_step_end<<<1, 32, 0, st>>>(S); }); nk++;
+    nk += enqueue_step_end(h);
     return nk;
 }
 
@@ -519,7 +520,7 @@ int kernels_per_step(const gfsph_handle* h) {
     // staged: 10 k_norm launches with nor_density, k_stage_begin, four
     // stages of (k_force_big, k_iforce, k_stage)
     const int body = staged(h) ? (h->rheo.nor_density ? 10 : 0) + 1 + 12 : 3;
-    return 15 + body + (h->rheo.av_vel ? 2 : 0) + (h->rheo.erosion ? 1 : 0) + 1;
+    return 13 + body + (h->rheo.av_vel ? 2 : 0) + 1;
 }
 
 int alloc_blocks(gfsph_handle* h, int cap) {

@@ -65,6 +65,8 @@ struct StepScalars {
     int need_cells, need_nbr, need_big, need_blocks;
     int ex0, ex1, ey0, ey1;  // DEM node box touched by erosion this step
     unsigned int bounds_ticket;  // blocks of k_bounds done (the last one resets it)
+    unsigned int scan_ticket[2];  // tiles of k_scan_tiles done: cells, block map
+    unsigned int end_ticket;      // blocks of k_dem_erode done
     int reg_levels;   // levels 0 .. reg_levels-1 are regular (thread + neighbour table)
     // the reference's own grid of grid_find_NEW_tools (skf 2, 3): origin, cell, cells
     float ref_xmin, ref_ymin, ref_delt;
@@ -387,7 +389,12 @@ __device__ __forceinline__ int block_of(const StepScalars* S, int k, int cx, int
 // neighbour search more tightly than the level's upper limit.
 __global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* bmark) {
     if (S->skip) return;
-    __shared__ unsigned int wmax[32];
+    // per-level largest hsml, reduced in shared memory first: every particle
+    // of a level would otherwise hit the same global word
+    __shared__ unsigned int lmax[kMaxLevels];
+    const int nlev = S->nlev;
+    for (int k = threadIdx.x; k < nlev; k += blockDim.x) lmax[k] = 0u;
+    __syncthreads();
     unsigned int h0 = 0u;  // largest level-0 hsml seen by this thread
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (B.flag[i]) continue;
@@ -402,16 +409,13 @@ __global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* 
             if (bmark[b] == 0) bmark[b] = 1;
         }
         if (k == 0) h0 = max(h0, f2o(hs));
-        else atomicMax(&S->lev_hmax_o[k], f2o(hs));
+        else atomicMax(&lmax[k], f2o(hs));
     }
     h0 = __reduce_max_sync(0xffffffffu, h0);
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = h0;
+    if ((threadIdx.x & 31) == 0 && h0) atomicMax(&lmax[0], h0);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int m = 0u;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = max(m, wmax[w]);
-        if (m) atomicMax(&S->lev_hmax_o[0], m);
-    }
+    for (int k = threadIdx.x; k < nlev; k += blockDim.x)
+        if (lmax[k]) atomicMax(&S->lev_hmax_o[k], lmax[k]);
 }
 
 // Cell key (slot of the particle's block * 256 + cell within the block) and
@@ -457,14 +461,65 @@ __global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* 
 // Exclusive scan of the histogram, tile pass: each block scans kScanTile
 // cells and writes its tile total.
 // only_sparse: the block-map scan, which dense steps skip.
-__global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const int* nptr, const StepScalars* S,
-                             int only_sparse) {
-    if (S->skip || S->err || (only_sparse && !S->sparse)) return;
+// Exclusive prefix of the tile sums, by one block (1 <= ntiles <= kScanTops *
+// blockDim.x): tile_sum[t] becomes the first index of tile t.
+constexpr int kScanTops = 32;
+__device__ void scan_tile_sums(int* tile_sum, int ntiles) {
+    __shared__ int wsum[32];
+    const int per = (ntiles + (int)blockDim.x - 1) / (int)blockDim.x;  // <= kScanTops
+    int loc[kScanTops];
+    int s = 0;
+    for (int k = 0; k < kScanTops; k++) {
+        if (k >= per) break;
+        int g = threadIdx.x * per + k;
+        int v = (g < ntiles) ? ((volatile int*)tile_sum)[g] : 0;
+        loc[k] = s;
+        s += v;
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int w = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
+        int wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < (int)(blockDim.x >> 5)) wsum[lane] = wi - w;
+    }
+    __syncthreads();
+    int off = wsum[wid] + incl - s;
+    for (int k = 0; k < kScanTops; k++) {
+        if (k >= per) break;
+        int g = threadIdx.x * per + k;
+        if (g < ntiles) tile_sum[g] = off + loc[k];
+    }
+}
+
+// Scan of count[0 .. *nptr] into start (exclusive), tile by tile; the last
+// tile to finish also scans the tile sums (the tile offsets k_scan_add adds).
+// which: 0 the cells, 1 the block map (only in the block-sparse layout).  A
+// step whose earlier kernels raised an error is stopped here.
+__global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const int* nptr, StepScalars* S,
+                             int which) {
+    if (S->skip || (which == 1 && !S->sparse)) return;
+    if (S->err) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) S->skip = 1;
+        return;
+    }
     int m = *nptr + 1;
+    const int ntiles = (m + kScanTile - 1) / kScanTile;
     int base = blockIdx.x * kScanTile;
     if (base >= m) return;
     __shared__ int sh[kScanTile];
     __shared__ int wsum[kScanThreads / 32];
+    __shared__ bool last;
     for (int k = threadIdx.x; k < kScanTile; k += kScanThreads) {
         int g = base + k;
         sh[k] = (g < m) ? count[g] : 0;
@@ -500,54 +555,19 @@ __global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const 
         int g = base + k;
         if (g < m) start[g] = sh[k];
     }
-}
-
-// Scan of the tile totals (one block of 1024 threads, up to 8192 tiles).
-// Also turns an error raised since the step began (k_hist) into a skip.
-__global__ void k_scan_top(int* tile_sum, const int* nptr, StepScalars* S, int only_sparse) {
-    if (S->skip || (only_sparse && !S->sparse)) return;
-    if (S->err) {
-        if (threadIdx.x == 0) S->skip = 1;
-        return;
-    }
-    int ntiles = (*nptr + 1 + kScanTile - 1) / kScanTile;
-    __shared__ int wsum[32];
-    const int per = 8;
-    int loc[per];
-    int s = 0;
-    for (int k = 0; k < per; k++) {
-        int g = threadIdx.x * per + k;
-        int v = (g < ntiles) ? tile_sum[g] : 0;
-        loc[k] = s;
-        s += v;
-    }
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int incl = s;
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) wsum[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        int w = wsum[lane];
-        int wi = w;
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += t;
-        }
-        wsum[lane] = wi - w;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = (atomicAdd(&S->scan_ticket[which], 1u) == (unsigned)ntiles - 1u);
     }
     __syncthreads();
-    int off = wsum[wid] + incl - s;
-    for (int k = 0; k < per; k++) {
-        int g = threadIdx.x * per + k;
-        if (g < ntiles) tile_sum[g] = off + loc[k];
-    }
+    if (!last) return;
+    __threadfence();
+    scan_tile_sums(tile_sum, ntiles);
+    if (threadIdx.x == 0) S->scan_ticket[which] = 0u;
 }
 
-__global__ void k_scan_add(int* start, const int* tile_sum, const int* nptr, const StepScalars* S, int only_sparse) {
-    if (S->skip || S->err || (only_sparse && !S->sparse)) return;
+__global__ void k_scan_add(int* start, const int* tile_sum, const int* nptr, const StepScalars* S, int which) {
+    if (S->skip || S->err || (which == 1 && !S->sparse)) return;
     int m = *nptr + 1;
     int base = blockIdx.x * kScanTile;
     if (base >= m) return;
@@ -1524,10 +1544,10 @@ __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalar
 
 // DEM update of ExtForces_SW(1) (SPH_SW_2019.f90:8795-8807) over the node box
 // touched this step; resets the scatter accumulators.
-__global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail, int nx, StepScalars* S) {
-    if (S->skip) return;
-    int x0 = S->ex0, x1 = S->ex1, y0 = S->ey0, y1 = S->ey1;
-    if (x1 < x0 || y1 < y0) return;
+
+// DEM update over the touched node box, grid-stride.
+__device__ __forceinline__ void erode_box(double2* auxv, float* z, float* eroded, float* avail, int nx, int x0, int x1,
+                                          int y0, int y1) {
     int w = x1 - x0 + 1, hgt = y1 - y0 + 1;
     long long tot = (long long)w * hgt;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot; k += (long long)gridDim.x * blockDim.x) {
@@ -1548,14 +1568,41 @@ __global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail
     }
 }
 
-__global__ void k_step_end(StepScalars* S) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// End of a step: time, dt and the counters; then the next step's decision
+// (prepare_step).  One thread.
+__device__ __forceinline__ void step_end(StepScalars* S) {
     if (!S->skip && S->advance) {
         S->dt = S->dt_step;
         S->time += (double)S->dt;
         S->steps_done += 1;
     }
     prepare_step(S, 1);
+}
+
+__global__ void k_step_end(StepScalars* S) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    step_end(S);
+}
+
+// DEM update of ExtForces_SW(1) (:8795-8807) over the node box touched this
+// step, resetting the scatter accumulators; the last block to finish also
+// ends the step (k_step_end), which saves a launch.
+__global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail, int nx, StepScalars* S) {
+    __shared__ bool last;
+    const int x0 = S->ex0, x1 = S->ex1, y0 = S->ey0, y1 = S->ey1;
+    if (!S->skip && x1 >= x0 && y1 >= y0) erode_box(auxv, z, eroded, avail, nx, x0, x1, y0, y1);
+    // the last block to finish ends the step (k_step_end)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = (atomicAdd(&S->end_ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        S->end_ticket = 0u;
+        step_end(S);
+    }
 }
 
 // Neighbour pairs of the coarse-level particles, for the parity export: every
