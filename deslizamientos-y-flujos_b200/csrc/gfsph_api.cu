@@ -136,6 +136,7 @@ struct gfsph_handle {
     int* cellA = nullptr;
     float2* velfin = nullptr;
     float* pterm = nullptr;
+    float2* pr = nullptr;    // (pterm, h) per slot
     int2* keyrank = nullptr;
     int* perm = nullptr;
     float2* f2tmp = nullptr;
@@ -149,6 +150,7 @@ struct gfsph_handle {
     StageCarry carry{};
     float* rhoS = nullptr;   // the five depths of a step, k-major (nor_density)
     int2* rcell = nullptr;   // cell of the reference's grid per slot (skf 2, 3)
+    float4* xsv = nullptr;   // (vx, vy, h, m) per slot after the RK update, for av_vel
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -280,9 +282,11 @@ Search make_search(gfsph_handle* h) {
     q.nbr = h->nbr;
     q.ncount = h->ncount;
     q.pterm = h->pterm;
+    q.pr = h->pr;
     q.indv = h->indv;
     q.rho0 = h->rho0;
     q.rcell = h->rcell;
+    q.xsv = h->xsv;
     q.kcap = h->kcap;
     return q;
 }
@@ -454,12 +458,12 @@ int enqueue_step(gfsph_handle* h) {
         if (h->rheo.av_vel) {  // av_vel with the final depth
             launch(h, K_XSPH_BIG, [&] {
                 with_skf(h, [&](auto sk) {
-                    k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[4], q, S, h->rheo, h->B, h->velfin);
+                    k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[4], q, S, h->rheo, h->B);
                 });
             });
             launch(h, K_XSPH, [&] {
                 with_skf(h, [&](auto sk) {
-                    k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(As[4], q, S, h->rheo, n, h->B, h->velfin);
+                    k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(As[4], q, S, h->rheo, n, h->B);
                 });
             });
             nk += 2;
@@ -485,13 +489,13 @@ int enqueue_step(gfsph_handle* h) {
         fork(h, 2);
         launch(h, K_XSPH_BIG, [&] {
             with_skf(h, [&](auto sk) {
-                k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo, h->B, h->velfin);
+                k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo, h->B);
             });
         });
         nk++;
         launch(h, K_XSPH, [&] {
             with_skf(h, [&](auto sk) {
-                k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B, h->velfin);
+                k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B);
             });
         });
         nk++;
@@ -573,7 +577,7 @@ void free_particles(gfsph_handle* h) {
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
     dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv); dfree(h->rho0);
     dfree(h->carry.v); dfree(h->carry.acc); dfree(h->carry.dx); dfree(h->carry.dv); dfree(h->carry.xo);
-    dfree(h->carry.out); dfree(h->rhoS); dfree(h->rcell);
+    dfree(h->carry.out); dfree(h->rhoS); dfree(h->rcell); dfree(h->xsv); dfree(h->pr);
     h->kcap = 0;
 }
 
@@ -881,6 +885,7 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
         st |= dalloc(&h->cellA, n); st |= dalloc(&h->velfin, n); st |= dalloc(&h->pterm, n);
         st |= dalloc(&h->keyrank, n); st |= dalloc(&h->perm, n); st |= dalloc(&h->ncount, n);
         st |= dalloc(&h->f2tmp, n); st |= dalloc(&h->xhm, n); st |= dalloc(&h->indv, n); st |= dalloc(&h->rho0, n);
+        st |= dalloc(&h->xsv, n); st |= dalloc(&h->pr, n);
         if (staged(h)) {
             StageCarry& C = h->carry;
             st |= dalloc(&C.v, n); st |= dalloc(&C.acc, n); st |= dalloc(&C.dx, n); st |= dalloc(&C.dv, n);

@@ -95,9 +95,11 @@ struct Search {
     int* nbr;            // neighbour table of the regular particles (layout: tab_base)
     int* ncount;
     float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
+    float2* pr;          // (pterm, h): what the internal force gathers per neighbour
     float2* indv;        // internal acceleration of every active particle (slot order)
     float* rho0;         // depth at the start of the step, after Adaptive_dt's h_inf clamp (icpwp = 3)
     const int2* rcell;   // slot -> cell of the reference's own grid (skf 2, 3), else null
+    float4* xsv;         // slot -> (vx, vy, h, m) after the RK update: what av_vel gathers
     int kcap;
 };
 
@@ -842,7 +844,9 @@ __global__ void __launch_bounds__(128, 12) k_density(PState A, Search Q, StepSca
         A.rho[i] = h;
         float hc = (h < c.h_inf) ? c.h_inf : h;
         float p = (c.cgra05 * hc) * hc;
-        Q.pterm[i] = (c.pa_sph == 1) ? p : p / (hc * hc);
+        const float pt = (c.pa_sph == 1) ? p : p / (hc * hc);
+        Q.pterm[i] = pt;
+        Q.pr[i] = make_float2(pt, h);
     }
 }
 
@@ -904,7 +908,9 @@ __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepSca
             A.rho[i] = h;
             float hc = (h < c.h_inf) ? c.h_inf : h;
             float p = (c.cgra05 * hc) * hc;
-            Q.pterm[i] = (c.pa_sph == 1) ? p : p / (hc * hc);
+            const float pt = (c.pa_sph == 1) ? p : p / (hc * hc);
+            Q.pterm[i] = pt;
+            Q.pr[i] = make_float2(pt, h);
         }
     }
 }
@@ -940,10 +946,11 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
     const int nreg = S->nreg, nbig = S->nbig;
     for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
-        float pi_ = Q.pterm[i], rhoi = A.rho[i];
+        const float2 pri = Q.pr[i];
         double a0 = 0.0, a1 = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
-            pressure_pair<SKF>(c, pi_, rhoi, Q.pterm[j], A.rho[j], o.w, g, a0, a1);
+            const float2 prj = Q.pr[j];
+            pressure_pair<SKF>(c, pri.x, pri.y, prj.x, prj.y, o.w, g, a0, a1);
         });
         a0 = warp_sum(a0);
         a1 = warp_sum(a1);
@@ -960,8 +967,8 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
     float4 me = Q.xhm[i];
     float2 xi = make_float2(me.x, me.y);
     float hi = me.z;
-    float pi_ = Q.pterm[i];
-    float rhoi = A.rho[i];
+    const float2 pri = __ldg(&Q.pr[i]);
+    const float pi_ = pri.x, rhoi = pri.y;
     double a0 = 0.0, a1 = 0.0;
     const int cnt = Q.ncount[i];
     const int* tab = Q.nbr + tab_base(i, Q.kcap);
@@ -969,28 +976,28 @@ __device__ __forceinline__ void internal_force(const PState& A, const Search& Q,
     for (; k + 4 <= cnt; k += 4) {
         int j[4];
         float4 o[4];
-        float pj[4], rj[4];
+        float2 prj[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             o[u] = __ldg(&Q.xhm[j[u]]);
-            pj[u] = __ldg(&Q.pterm[j[u]]);
-            rj[u] = __ldg(&A.rho[j[u]]);
+            prj[u] = __ldg(&Q.pr[j[u]]);
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             PairGeom g;
             pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
-            pressure_pair<SKF>(c, pi_, rhoi, pj[u], rj[u], o[u].w, g, a0, a1);
+            pressure_pair<SKF>(c, pi_, rhoi, prj[u].x, prj[u].y, o[u].w, g, a0, a1);
         }
     }
     for (; k < cnt; k++) {
         int j = __ldg(tab + (size_t)k * kTabStride);
         float4 o = __ldg(&Q.xhm[j]);
+        const float2 prj = __ldg(&Q.pr[j]);
         PairGeom g;
         pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-        pressure_pair<SKF>(c, pi_, rhoi, __ldg(&Q.pterm[j]), __ldg(&A.rho[j]), o.w, g, a0, a1);
+        pressure_pair<SKF>(c, pi_, rhoi, prj.x, prj.y, o.w, g, a0, a1);
     }
     in0 = (float)a0;
     in1 = (float)a1;
@@ -1099,8 +1106,10 @@ __device__ __forceinline__ void erosion_scatter(const DemView& dem, float xx, fl
 }
 
 // A particle out of the domain at the start of the step: copied through.
-__device__ __forceinline__ void rk_carry(const PState& A, const Rheo& c, const PState& B, float2* velfin, int i) {
+__device__ __forceinline__ void rk_carry(const PState& A, const Rheo& c, const PState& B, float2* velfin, float4* xsv,
+                                         int i) {
     B.pos[i] = A.pos[i]; B.vel[i] = A.vel[i]; velfin[i] = A.vel[i];
+    xsv[i] = make_float4(A.vel[i].x, A.vel[i].y, A.rho[i], A.mass[i]);
     B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
     B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
     if (c.icpwp == 3) B.pwp[i] = 0.f;  // Get_Pwp_SW zeroes out-of-domain particles
@@ -1137,6 +1146,7 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
     }
     B.pos[i] = make_float2(xx, xy);
     velfin[i] = make_float2(vx, vy);
+    Q.xsv[i] = make_float4(vx, vy, h, m);
     B.vel[i] = make_float2(vx, vy);
     B.rho[i] = h;
     B.mass[i] = m;
@@ -1193,7 +1203,7 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
             continue;
         }
         if (i >= nact) {  // carried particles (out of the domain at step start)
-            rk_carry(A, c, B, velfin, i);
+            rk_carry(A, c, B, velfin, Q.xsv, i);
             if (c.erosion) erosion_scatter(dem, 0.f, 0.f, 0.f, false, auxv, box);
             continue;
         }
@@ -1340,7 +1350,9 @@ __global__ void __launch_bounds__(128) k_stage_begin(PState A, Search Q, StepSca
     const int nact = S->nactive;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
         const float2 p = A.pos[i];
-        Q.pterm[i] = stage_pterm<COS>(c, dem, h1[i], p.x, p.y);
+        const float pt = stage_pterm<COS>(c, dem, h1[i], p.x, p.y);
+        Q.pterm[i] = pt;
+        Q.pr[i] = make_float2(pt, h1[i]);
     }
 }
 
@@ -1360,7 +1372,10 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
     const float f1 = (s == 0) ? 0.f : 0.5f, f2 = (s == 0) ? 1.f : 2.f;
     const float f1n = (s == 2) ? 1.f : 0.5f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
-        if (s > 0 && C.out[i]) continue;
+        if (s > 0 && C.out[i]) {  // frozen: its pressure term stays, its depth is the next call's
+            Q.pr[i] = make_float2(Q.pterm[i], hnext[i]);
+            continue;
+        }
         const float2 x0 = A.pos[i], v0 = A.vel[i];
         float2 vp = v0, ap = make_float2(0.f, 0.f), dx = make_float2(0.f, 0.f), dv = make_float2(0.f, 0.f);
         if (s > 0) { vp = C.v[i]; ap = C.acc[i]; dx = C.dx[i]; dv = C.dv[i]; }
@@ -1371,6 +1386,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
             C.out[i] = 1;
             C.xo[i] = make_float2(xx, xy);
             C.v[i] = make_float2(vx, vy);
+            Q.pr[i] = make_float2(Q.pterm[i], hnext[i]);
             continue;
         }
         if (s == 0) C.out[i] = 0;
@@ -1391,7 +1407,12 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
         C.dv[i] = dv;
         const float fdn = f1n * dt;
         const float nx_ = x0.x + fdn * vx, ny_ = x0.y + fdn * vy;
-        if (!out_of_box(dem, nx_, ny_)) Q.pterm[i] = stage_pterm<COS>(c, dem, hnext[i], nx_, ny_);
+        float pt = Q.pterm[i];
+        if (!out_of_box(dem, nx_, ny_)) {
+            pt = stage_pterm<COS>(c, dem, hnext[i], nx_, ny_);
+            Q.pterm[i] = pt;
+        }
+        Q.pr[i] = make_float2(pt, hnext[i]);
     }
 }
 
@@ -1414,7 +1435,7 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
             continue;
         }
         if (i >= nact) {
-            rk_carry(A, c, B, velfin, i);
+            rk_carry(A, c, B, velfin, Q.xsv, i);
             if (c.erosion) erosion_scatter(dem, 0.f, 0.f, 0.f, false, auxv, box);
             continue;
         }
@@ -1468,8 +1489,7 @@ __device__ __forceinline__ void xsph_pair(const Rheo& c, float2 vi, float rhoi, 
 // av_vel (SPH_MAIN_2019.f90:3042-3099) with the start-of-step W_ij, then
 // v += 0.3*av for particles still inside the domain (:987-993).
 template <int SKF>
-__global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S, Rheo c, int n, PState B,
-                                               const float2* velfin) {
+__global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S, Rheo c, int n, PState B) {
     if (S->skip || !c.av_vel) return;
     const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
@@ -1477,39 +1497,37 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
         float4 me = Q.xhm[i];
         float2 xi = make_float2(me.x, me.y);
         float hi = me.z;
-        float2 vi = velfin[i];
-        float rhoi = A.rho[i];
+        const float4 si = Q.xsv[i];
+        const float2 vi = make_float2(si.x, si.y);
+        const float rhoi = si.z;
         const int cnt = Q.ncount[i];
         const int* tab = Q.nbr + tab_base(i, Q.kcap);
         double a0 = 0.0, a1 = 0.0;
         int k = 0;
         for (; k + 4 <= cnt; k += 4) {
             int j[4];
-            float4 o[4];
-            float2 vj[4];
-            float rj[4], mj[4];
+            float4 o[4], sj[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 o[u] = __ldg(&Q.xhm[j[u]]);
-                vj[u] = velfin[j[u]];
-                rj[u] = __ldg(&A.rho[j[u]]);
-                mj[u] = B.mass[j[u]];
+                sj[u] = Q.xsv[j[u]];
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 PairGeom g;
                 pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
-                xsph_pair<SKF>(c, vi, rhoi, vj[u], rj[u], mj[u], g, a0, a1);
+                xsph_pair<SKF>(c, vi, rhoi, make_float2(sj[u].x, sj[u].y), sj[u].z, sj[u].w, g, a0, a1);
             }
         }
         for (; k < cnt; k++) {
             int j = __ldg(tab + (size_t)k * kTabStride);
             float4 o = __ldg(&Q.xhm[j]);
+            const float4 sj = Q.xsv[j];
             PairGeom g;
             pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-            xsph_pair<SKF>(c, vi, rhoi, velfin[j], __ldg(&A.rho[j]), B.mass[j], g, a0, a1);
+            xsph_pair<SKF>(c, vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, g, a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
@@ -1517,8 +1535,7 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
 }
 
 template <int SKF>
-__global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B,
-                                                   const float2* velfin) {
+__global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B) {
     constexpr int SK = SupportScale<SKF>::value;
     if (S->skip || !c.av_vel) return;
     const int lane = threadIdx.x & 31;
@@ -1527,11 +1544,13 @@ __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalar
     for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
         if (B.flag[i]) continue;  // uniform over the warp
-        float2 vi = velfin[i];
-        float rhoi = A.rho[i];
+        const float4 si = Q.xsv[i];
+        const float2 vi = make_float2(si.x, si.y);
+        const float rhoi = si.z;
         double a0 = 0.0, a1 = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
-            xsph_pair<SKF>(c, vi, rhoi, velfin[j], A.rho[j], B.mass[j], g, a0, a1);
+            const float4 sj = Q.xsv[j];
+            xsph_pair<SKF>(c, vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, g, a0, a1);
         });
         a0 = warp_sum(a0);
         a1 = warp_sum(a1);
