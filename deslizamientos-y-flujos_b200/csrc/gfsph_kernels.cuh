@@ -105,6 +105,29 @@ struct Search {
 
 __device__ __forceinline__ bool step_skipped(const StepScalars* S) { return S->skip != 0; }
 
+// The step scalars in shared memory for the serial set-up code that one
+// thread runs at the end of a kernel (grid set-up, step end): the block
+// copies the struct in and out in one parallel pass each, so the set-up does
+// not wait for a global round trip per field it reads.  Every thread of the
+// block calls both, and nothing else writes S meanwhile.
+static_assert(sizeof(StepScalars) % 4 == 0, "StepScalars is copied as 32-bit words");
+__device__ __forceinline__ StepScalars* scalars_to_smem(const StepScalars* S) {
+    __shared__ __align__(16) StepScalars sS;
+    const int nw = (int)(sizeof(StepScalars) / 4);
+    const unsigned int* src = reinterpret_cast<const unsigned int*>(S);
+    unsigned int* dst = reinterpret_cast<unsigned int*>(&sS);
+    for (int k = threadIdx.x; k < nw; k += blockDim.x) dst[k] = __ldcg(src + k);
+    __syncthreads();
+    return &sS;
+}
+__device__ __forceinline__ void scalars_from_smem(StepScalars* S, const StepScalars* L) {
+    __syncthreads();
+    const int nw = (int)(sizeof(StepScalars) / 4);
+    const unsigned int* src = reinterpret_cast<const unsigned int*>(L);
+    unsigned int* dst = reinterpret_cast<unsigned int*>(S);
+    for (int k = threadIdx.x; k < nw; k += blockDim.x) dst[k] = src[k];
+}
+
 // Neighbour-table layout, blocked by warps of 32 particles: entry k of
 // particle i is at tab_base(i, kcap) + 32 k.  The lanes of a warp read entry k
 // of their particles as one 128-byte line, and the entries a warp appends
@@ -134,8 +157,9 @@ __device__ __forceinline__ void prepare_step(StepScalars* S, int advance) {
 }
 
 __global__ void k_prep(StepScalars* S, int advance) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    prepare_step(S, advance);
+    StepScalars* L = scalars_to_smem(S);
+    if (threadIdx.x == 0) prepare_step(L, advance);
+    scalars_from_smem(S, L);
 }
 
 __device__ __forceinline__ float warp_min(float v) {
@@ -257,15 +281,17 @@ __global__ void __launch_bounds__(kThreadsBounds) k_bounds(PState B, int n, Rheo
     __syncthreads();
     if ((threadIdx.x & 31) == 0) wp[threadIdx.x >> 5] = b;
     __syncthreads();
+    StepScalars* L = scalars_to_smem(S);
     if (threadIdx.x == 0) {
         BoundsPart t = wp[0];
         for (int k = 1; k < (int)(blockDim.x >> 5); k++) bounds_merge(t, wp[k]);
-        S->xmin_o = f2o(t.xmn); S->xmax_o = f2o(t.xmx); S->ymin_o = f2o(t.ymn); S->ymax_o = f2o(t.ymx);
-        S->hmax_o = f2o(t.hmx); S->dtmin_o = f2o(t.dtm);
-        S->hsum = t.hsum; S->hcount = t.hcnt; S->bad = t.bad;
-        S->bounds_ticket = 0u;
-        grid_setup(c, S, ga);
+        L->xmin_o = f2o(t.xmn); L->xmax_o = f2o(t.xmx); L->ymin_o = f2o(t.ymn); L->ymax_o = f2o(t.ymx);
+        L->hmax_o = f2o(t.hmx); L->dtmin_o = f2o(t.dtm);
+        L->hsum = t.hsum; L->hcount = t.hcnt; L->bad = t.bad;
+        L->bounds_ticket = 0u;
+        grid_setup(c, L, ga);
     }
+    scalars_from_smem(S, L);
 }
 
 // dt update (Adaptive_dt_sph_SW :6658-6662) and the cell grids.  The
@@ -1599,8 +1625,9 @@ __device__ __forceinline__ void step_end(StepScalars* S) {
 }
 
 __global__ void k_step_end(StepScalars* S) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    step_end(S);
+    StepScalars* L = scalars_to_smem(S);
+    if (threadIdx.x == 0) step_end(L);
+    scalars_from_smem(S, L);
 }
 
 // DEM update of ExtForces_SW(1) (:8795-8807) over the node box touched this
@@ -1617,11 +1644,14 @@ __global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail
         last = (atomicAdd(&S->end_ticket, 1u) == gridDim.x - 1);
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        S->end_ticket = 0u;
-        step_end(S);
+    if (!last) return;
+    __threadfence();
+    StepScalars* L = scalars_to_smem(S);
+    if (threadIdx.x == 0) {
+        L->end_ticket = 0u;
+        step_end(L);
     }
+    scalars_from_smem(S, L);
 }
 
 // Neighbour pairs of the coarse-level particles, for the parity export: every
