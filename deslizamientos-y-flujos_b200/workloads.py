@@ -177,6 +177,45 @@ def fractal_channel(n_target=200_000, dem_k=10, cell=5.0, seed=2, facthsml=2.0, 
         meta=dict(dem=f"{nx}x{ny} at {cell} m", lattice=spacing, relief=relief))
 
 
+def multi_release(n_target=4_000_000, dem_k=12, cell=2.0, seed=3, nrel=4, facthsml=2.0, mean_depth=3.0,
+                  tauy0=1000.0, constK=50.0, relief=1200.0):
+    """Large-scale case: a seeded fBm DEM (Hurst 0.8) of 2^dem_k nodes a side
+    at `cell` m (4096^2 at 2 m: 8.2 km) sloping down along y, with nrel
+    elliptical releases (semi-axes 250 x 120 m) spread across the upper slope
+    on the one lattice spacing that gives ~n_target particles in all;
+    Bingham basal law (nfric 4, yield stress const(6) = tauy0, viscosity
+    const(7) = constK), no erosion, adaptive dt."""
+    nx = ny = 2 ** dem_k
+    L = nx * cell
+    rng = np.random.default_rng(seed)
+    f = diamond_square(dem_k, 0.8, rng)[:ny, :nx]
+    f = (f - f.min()) / (f.max() - f.min())
+    ys = np.arange(ny)[:, None] * cell
+    z = ((relief - 150.0) * (1.0 - ys / L) + 150.0 * f).astype(np.float32)
+    sa, sc = 250.0, 120.0
+    spacing = math.sqrt(nrel * math.pi * sa * sc / n_target)
+    xs, ms, vs, hs, hl = [], [], [], [], []
+    for r in range(nrel):
+        xc, yc = L * (r + 0.5) / nrel, 0.2 * L
+        mx = int(math.ceil(sc / spacing)) + 1
+        my = int(math.ceil(sa / spacing)) + 1
+        gx0, gy0 = xc - mx * spacing, yc - my * spacing
+        X, Y = np.meshgrid(gx0 + np.arange(2 * mx + 1) * spacing, gy0 + np.arange(2 * my + 1) * spacing)
+        mask = ((X - xc) / sc) ** 2 + ((Y - yc) / sa) ** 2 < 1.0
+        fld = smooth_field(X, Y, np.random.default_rng(seed + 100 + r))
+        depth = mean_depth * (1.0 + 0.25 * fld)
+        x, v, h, mass, hsml = lattice_particles(mask, depth, gx0, gy0, spacing, facthsml, 0.01)
+        xs.append(x); vs.append(v); hs.append(h); ms.append(mass); hl.append(hsml)
+    c = {1: 9.8, 2: 2000.0, 3: 0.0, 5: 4, 6: tauy0, 7: constK, 9: 0.0, 10: 0.01, 15: 0.01}
+    return Workload(
+        name=f"multi_release_{sum(a.shape[0] for a in xs) // 1000}k", const=c,
+        options=dict(pa_sph=2, nnps=2, sle=1, skf=1, average_velocity=1, ic_adapt=1, h_inf=0.01, dt=0.01,
+                     dem_deriv=1),
+        z=z, dx=cell, dy=cell, x=np.concatenate(xs), v=np.concatenate(vs), rho=np.concatenate(hs),
+        mass=np.concatenate(ms), hsml=np.concatenate(hl), steps=2000,
+        meta=dict(dem=f"{nx}x{ny} at {cell} m", lattice=spacing, releases=nrel))
+
+
 def mc_ensemble(nreal, n_base=200_000, dem_k=10, cell=5.0, seed=2024, mu=(0.08, 0.30), xi=(400.0, 0.3),
                 scale=(0.2, 2.0)):
     """Realizations of the Monte-Carlo hazard ensemble on the fractal channel
