@@ -34,7 +34,8 @@ def test_four_million_particles_bingham_multi_release(gfsph_lib):
     assert np.array_equal(g["mass"], w.mass)  # no erosion: every volume kept bit for bit
     assert not np.array_equal(g["hsml"], w.hsml)  # h_upgrade (sle 1) ran
     assert np.abs(g["v"]).max() > 0.0  # the releases started to move
-    assert 0.0 < dt <= p.dt * 1.1 ** 12 and t > 0.0
+    # adaptive dt grows by at most the single-precision factor 1.1 per step
+    assert 0.0 < dt <= p.dt * 1.1 ** 12 * (1.0 + 1e-5) and t > 0.0
     g2, (t2, dt2), _ = run(w, p, 12)
     assert t2 == t and dt2 == dt
     for k in g:
