@@ -76,6 +76,11 @@ module gfsph_c
        real(c_double), intent(out) :: t
        real(c_float), intent(out) :: dt
      end function
+     ! the handle's kernels on a CUDA stream (c_null_ptr: the handle's own)
+     integer(c_int) function gfsph_set_stream(handle, stream) bind(c, name="gfsph_set_stream")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: handle, stream
+     end function
      integer(c_int) function gfsph_set_time(handle, t, dt) bind(c, name="gfsph_set_time")
        import :: c_int, c_ptr, c_double, c_float
        type(c_ptr), value :: handle

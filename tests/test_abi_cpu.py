@@ -73,3 +73,36 @@ def test_fortran_interface_names_every_symbol():
         if s in ("gfsph_set_stream",):
             continue
         assert f'bind(c, name="{s}")' in src, s
+
+
+def _c_declarations():
+    """{name: argument count} of the functions include/gfsph.h declares."""
+    src = open(os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "gfsph.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(gfsph_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", src):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def _fortran_interfaces():
+    """{C name: argument count} of the BIND(C) interfaces of the Fortran module."""
+    path = os.path.join(os.path.dirname(os.path.dirname(__file__)), "deslizamientos-y-flujos_b200", "fortran",
+                        "gfsph_c.f90")
+    src = re.sub(r"&\s*\n\s*", " ", open(path).read())
+    out = {}
+    for m in re.finditer(r"function\s+\w+\s*\(([^)]*)\)\s*bind\(c,\s*name=\"(gfsph_[a-z0-9_]+)\"\)", src):
+        args = m.group(1).strip()
+        out[m.group(2)] = 0 if not args else args.count(",") + 1
+    return out
+
+
+def test_fortran_module_binds_every_entry_point():
+    """The Fortran module (the reference's side of the boundary) declares every
+    function of the C header, with the same number of arguments."""
+    c, f = _c_declarations(), _fortran_interfaces()
+    assert len(c) > 30
+    assert sorted(set(c) - set(f)) == []
+    for name, nargs in c.items():
+        assert f[name] == nargs, (name, nargs, f[name])
