@@ -31,14 +31,16 @@ import numpy as np  # noqa: E402
 METRIC = "SPH particle-steps/s"
 UNIT = "particle-steps/s"
 B_ALG = {"k_density": 24, "k_force_rk": 72, "k_xsph": 44, "k_hist": 28}  # bytes per particle and launch
-# From one ncu --set full capture of the fractal-channel workload (200,011
-# particles, step 9; profiles/neighbour_kernels_fractal_channel_200k.md):
-# DRAM read + write bytes and warp instructions per launch, per particle.
+# From ncu on the fractal-channel workload (200,011 particles): warp
+# instructions per launch averaged over every launch of the 300 timed steps
+# (steps 11-310; the neighbour work grows as the flow spreads:
+# profiles/neighbour_kernels_fractal_channel_200k.md), and DRAM read + write
+# bytes per launch from one --set full capture of step 9; both per particle.
 NCU_PER_PARTICLE = {
-    "k_density": {"dram_bytes": (4.835328e6 + 1.737984e6) / 200011, "warp_inst": 43570925 / 200011},
-    "k_iforce": {"dram_bytes": (43.911680e6 + 0.100352e6) / 200011, "warp_inst": 41176670 / 200011},
-    "k_force_rk": {"dram_bytes": 8.113920e6 / 200011, "warp_inst": 21424072 / 200011},
-    "k_xsph": {"dram_bytes": (46.309120e6 + 0.197632e6) / 200011, "warp_inst": 33754265 / 200011},
+    "k_density": {"dram_bytes": (4.835328e6 + 1.737984e6) / 200011, "warp_inst": 80.09e6 / 200011},
+    "k_iforce": {"dram_bytes": (43.911680e6 + 0.100352e6) / 200011, "warp_inst": 42.43e6 / 200011},
+    "k_force_rk": {"dram_bytes": 8.113920e6 / 200011, "warp_inst": 21.54e6 / 200011},
+    "k_xsph": {"dram_bytes": (46.309120e6 + 0.197632e6) / 200011, "warp_inst": 36.52e6 / 200011},
 }
 NCU_SOURCE = "profiles/neighbour_kernels_fractal_channel_200k.md (ncu, cold caches), scaled by active particles"
 ISSUE_PEAK = 148 * 4 * 1.965e9  # warp instructions/s: SMs x schedulers x max SM clock
