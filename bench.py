@@ -141,25 +141,31 @@ def _oracle_case(n_target=20_000):
     return oracle, w, p, nx, ny, st
 
 
-def cpu_reference_rate(seconds_budget, warm_steps=20):
-    """The reference path on the host (the FP32 oracle port, one thread) on a
-    bounded sample of the workload: the same DEM and physics with a
-    20k-particle release, timed over the same early phase of the flow as the
-    GPU measurement.  Returns (particle-steps/s, steps, n, seconds, sample)."""
+def cpu_reference_rate(seconds_budget, warm_steps=20, omp=False, steps=None):
+    """The reference path on the host (the FP32 oracle port) on a bounded
+    sample of the workload: the same DEM and physics with a 20k-particle
+    release, timed over the same early phase of the flow as the GPU
+    measurement.  One thread (the reference is single-threaded), or with
+    omp=True the OpenMP build of the port on every host core this process
+    may use; steps fixes the timed steps (else the budget sets them).
+    Returns (particle-steps/s, steps, n, seconds, threads, sample)."""
     oracle, w, p, nx, ny, st = _oracle_case()
-    run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st)
+    threads = oracle.omp_threads() if omp else 1
+    run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st, omp=omp)
     run.advance(warm_steps)
     t0 = time.perf_counter()
     run.advance(1)
     one = max(time.perf_counter() - t0, 1e-4)
-    steps = max(1, min(400, int(seconds_budget / one)))
+    if steps is None:
+        steps = max(1, min(400, int(seconds_budget / one)))
     t0 = time.perf_counter()
     run.advance(steps)
     el = time.perf_counter() - t0
     run.close()
+    how = f"OpenMP build, {threads} host threads" if omp else "1 host thread"
     desc = (f"steps {warm_steps + 2}..{warm_steps + 1 + steps} of the fractal-channel workload with a "
-            f"{w.n}-particle release (same DEM and physics), FP32 oracle port, 1 host thread")
-    return w.n * steps / el, steps, w.n, el, desc
+            f"{w.n}-particle release (same DEM and physics), FP32 oracle port, {how}")
+    return w.n * steps / el, steps, w.n, el, threads, desc
 
 
 def run_reference_arm(args, rank, world):
@@ -516,8 +522,16 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, steps, nc, el, desc = cpu_reference_rate(args.cpu_seconds)
+        rate, steps, nc, el, _, desc = cpu_reference_rate(args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "sample": desc}
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        if oracle.omp_available():
+            # the same steps as the single-thread sample
+            rate, steps, nc, el, threads, desc = cpu_reference_rate(args.cpu_seconds, omp=True, steps=steps)
+            cpu["openmp"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+        else:
+            cpu["openmp"] = {"unavailable": "the OpenMP build of the oracle was not made (no -fopenmp compiler)"}
 
     if rank == 0:
         line = {

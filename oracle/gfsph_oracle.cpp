@@ -37,6 +37,15 @@
  * terminal velocity, mass conservation, brute-force neighbour sets) in
  * tests/test_oracle_kat.py.
  *
+ * Threads: built without OpenMP (the checker) every loop runs serially in
+ * the order above.  The same source built with -fopenmp is a timing-only
+ * variant of the CPU baseline: per-particle loops split over threads; the
+ * pair list generated by ranges of cells holding equal numbers of particles
+ * and concatenated in cell order (the serial list); the erosion terms of
+ * each particle computed in parallel and added to the DEM nodes in particle
+ * order (the serial sums); the pair sums accumulated per thread and added in
+ * thread order, so those round differently from the checker's.
+ *
  * Deviations from the literal Fortran, each one a place where the literal
  * code reads undefined or out-of-range data:
  *   - Bingham (nfric = 4): SPH_SW_2019.f90:9616-9618 overwrite the regime
@@ -56,6 +65,9 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "../include/gfsph.h"
 
@@ -219,6 +231,11 @@ struct Oracle {
     /* pairs */
     std::vector<Pair> pairs;
     std::vector<R> pw, pd0, pd1;
+    /* OpenMP build only: per-range pair lists and per-thread partial sums,
+     * kept between steps so that their storage is reused */
+    std::vector<std::vector<Pair>> rp;
+    std::vector<std::vector<R>> rw, r0, r1;
+    std::vector<A> part;
     R dt;
     double time;
     std::vector<A> auxv1, auxv2; /* erosion scatter, ExtForces_SW(1) */
@@ -335,38 +352,125 @@ struct Oracle {
             list[start[cell[i]] + fill[cell[i]]++] = i;
         }
         const int scale_k = (P->skf == 2 || P->skf == 3) ? 3 : 2; /* :1155-1161 */
-        for (int idy = 1; idy <= ndiv[1]; idy++)
-            for (int idx = 1; idx <= ndiv[0]; idx++) {
-                long ic = (long)ndiv[0] * (idy - 1) + (idx - 1);
-                for (int a = 0; a < cnt[ic]; a++) {
-                    int it = list[start[ic] + a];
-                    int jx0 = std::max(1, idx - 1), jx1 = std::min(ndiv[0], idx + 1);
-                    int jy1 = std::min(ndiv[1], idy + 1);
-                    for (int jdy = idy; jdy <= jy1; jdy++)
-                        for (int jdx = jx0; jdx <= jx1; jdx++) {
-                            long jc = (long)ndiv[0] * (jdy - 1) + (jdx - 1);
-                            if (jc < ic) continue;
-                            int b0 = (jc == ic) ? a + 1 : 0;
-                            for (int b = b0; b < cnt[jc]; b++) {
-                                int jt = list[start[jc] + b];
-                                R d0 = x[2 * it] - x[2 * jt];
-                                R dr = d0 * d0;
-                                R d1 = x[2 * it + 1] - x[2 * jt + 1];
-                                dr = dr + d1 * d1;
-                                R mh = (hsml[it] + hsml[jt]) / (R)2;
-                                R r = std::sqrt(dr);
-                                if (r < (R)scale_k * mh) {
-                                    R w, g0, g1;
-                                    kernel_tools<R>(P->skf, r, d0, d1, mh, w, g0, g1);
-                                    pairs.push_back({it, jt});
-                                    pw.push_back(w); pd0.push_back(g0); pd1.push_back(g1);
-                                }
+        /* the pairs of the particles of cell ic (row idy, column idx, 1-based)
+         * with the same and the following cells of the half stencil */
+        auto cell_pairs = [&](long ic, std::vector<Pair>& pp, std::vector<R>& ww, std::vector<R>& g0s,
+                              std::vector<R>& g1s) {
+            const int idx = (int)(ic % ndiv[0]) + 1, idy = (int)(ic / ndiv[0]) + 1;
+            for (int a = 0; a < cnt[ic]; a++) {
+                int it = list[start[ic] + a];
+                int jx0 = std::max(1, idx - 1), jx1 = std::min(ndiv[0], idx + 1);
+                int jy1 = std::min(ndiv[1], idy + 1);
+                for (int jdy = idy; jdy <= jy1; jdy++)
+                    for (int jdx = jx0; jdx <= jx1; jdx++) {
+                        long jc = (long)ndiv[0] * (jdy - 1) + (jdx - 1);
+                        if (jc < ic) continue;
+                        int b0 = (jc == ic) ? a + 1 : 0;
+                        for (int b = b0; b < cnt[jc]; b++) {
+                            int jt = list[start[jc] + b];
+                            R d0 = x[2 * it] - x[2 * jt];
+                            R dr = d0 * d0;
+                            R d1 = x[2 * it + 1] - x[2 * jt + 1];
+                            dr = dr + d1 * d1;
+                            R mh = (hsml[it] + hsml[jt]) / (R)2;
+                            R r = std::sqrt(dr);
+                            if (r < (R)scale_k * mh) {
+                                R w, g0, g1;
+                                kernel_tools<R>(P->skf, r, d0, d1, mh, w, g0, g1);
+                                pp.push_back({it, jt});
+                                ww.push_back(w); g0s.push_back(g0); g1s.push_back(g1);
                             }
                         }
-                }
+                    }
             }
+        };
+        /* cells in row-major order (idy outer, idx inner), as grid_find walks them */
+#ifdef _OPENMP
+        const int T = omp_get_max_threads();
+        if (T > 1) {
+            /* contiguous cell ranges holding about the same number of
+             * particles, taken by the threads in any order and concatenated
+             * in range order: the same pair list as the serial walk */
+            const int nch = 16 * T;
+            std::vector<long> cut(nch + 1, ndivt);
+            cut[0] = 0;
+            const long per = ((long)start[ndivt - 1] + cnt[ndivt - 1] + nch - 1) / nch;
+            for (long c = 0, k = 1; c < ndivt && k < nch; c++)
+                if (start[c] + cnt[c] >= per * k) cut[k++] = c + 1;
+            for (int k = 1; k <= nch; k++) cut[k] = std::max(cut[k], cut[k - 1]);
+            rp.resize(nch); rw.resize(nch); r0.resize(nch); r1.resize(nch);
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int k = 0; k < nch; k++) {
+                /* filled through vectors on this thread's stack: the
+                 * neighbouring ranges' vector headers share cache lines */
+                std::vector<Pair> lp; std::vector<R> lw, l0, l1;
+                lp.swap(rp[k]); lw.swap(rw[k]); l0.swap(r0[k]); l1.swap(r1[k]);
+                lp.clear(); lw.clear(); l0.clear(); l1.clear();
+                for (long ic = cut[k]; ic < cut[k + 1]; ic++) cell_pairs(ic, lp, lw, l0, l1);
+                lp.swap(rp[k]); lw.swap(rw[k]); l0.swap(r0[k]); l1.swap(r1[k]);
+            }
+            std::vector<size_t> off(nch + 1, 0);
+            for (int k = 0; k < nch; k++) off[k + 1] = off[k] + rp[k].size();
+            pairs.resize(off[nch]); pw.resize(off[nch]); pd0.resize(off[nch]); pd1.resize(off[nch]);
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int k = 0; k < nch; k++) {
+                std::copy(rp[k].begin(), rp[k].end(), pairs.begin() + off[k]);
+                std::copy(rw[k].begin(), rw[k].end(), pw.begin() + off[k]);
+                std::copy(r0[k].begin(), r0[k].end(), pd0.begin() + off[k]);
+                std::copy(r1[k].begin(), r1[k].end(), pd1.begin() + off[k]);
+            }
+            return;
+        }
+#endif
+        for (long ic = 0; ic < ndivt; ic++) cell_pairs(ic, pairs, pw, pd0, pd1);
         /* Pint_Update_SW_tools (My_SPH_Tools_2019.f90:1652-1758): all particles
          * are soil (itype 1), every pair is type 0 and keeps its order. */
+    }
+
+    /* Accumulator view handed to a pair body: a(c, i) is the c-th sum of
+     * particle i. */
+    struct ArrayAcc {
+        A** a;
+        A& operator()(int c, int i) const { return a[c][i]; }
+    };
+
+    /* A loop over the pairs that adds pair k's terms into nc (<= 4)
+     * accumulator arrays of n entries: f(k, a) adds into a(c, i) and
+     * a(c, j).  Serially in pair order (the checker).  The OpenMP build
+     * splits the pairs into one contiguous block per thread, each adding
+     * into its own zeroed copy of the arrays, and adds the copies to the
+     * arrays in thread order: the same terms, summed in another order. */
+    template <class F>
+    void pair_loop(int nc, A** acc, F&& f) {
+#ifdef _OPENMP
+        const int T = omp_get_max_threads();
+        if (T > 1 && pairs.size() > 4096) {
+            part.resize((size_t)T * nc * n);
+#pragma omp parallel
+            {
+                const int t = omp_get_thread_num();
+                A* mine[4];
+                for (int c = 0; c < nc; c++) {
+                    mine[c] = part.data() + ((size_t)t * nc + c) * n;
+                    std::fill(mine[c], mine[c] + n, (A)0);
+                }
+                ArrayAcc own{mine};
+#pragma omp barrier
+#pragma omp for schedule(static)
+                for (long k = 0; k < (long)pairs.size(); k++) f((size_t)k, own);
+#pragma omp for schedule(static)
+                for (int i = 0; i < n; i++)
+                    for (int c = 0; c < nc; c++) {
+                        A sacc = acc[c][i];
+                        for (int u = 0; u < T; u++) sacc = sacc + part[((size_t)u * nc + c) * n + i];
+                        acc[c][i] = sacc;
+                    }
+            }
+            return;
+        }
+#endif
+        ArrayAcc all{acc};
+        for (size_t k = 0; k < pairs.size(); k++) f(k, all);
     }
 
     /* sum_density_Tools, My_SPH_Tools_2019.f90:1763-1859.  With nor_density
@@ -383,16 +487,21 @@ struct Oracle {
             if (nor) wi[i] = (A)((sd * mass[i]) / rho[i]);
             acc[i] = (A)(sd * mass[i]);
         }
-        if (nor)
-            for (size_t k = 0; k < pairs.size(); k++) {
+        if (nor) {
+            A* arr[1] = {wi.data()};
+            pair_loop(1, arr, [&](size_t k, auto& a) {
                 int i = pairs[k].i, j = pairs[k].j;
-                wi[i] = wi[i] + (A)((mass[j] / rho[j]) * pw[k]);
-                wi[j] = wi[j] + (A)((mass[i] / rho[i]) * pw[k]);
-            }
-        for (size_t k = 0; k < pairs.size(); k++) {
-            int i = pairs[k].i, j = pairs[k].j;
-            acc[i] = acc[i] + (A)(mass[j] * pw[k]);
-            acc[j] = acc[j] + (A)(mass[i] * pw[k]);
+                a(0, i) = a(0, i) + (A)((mass[j] / rho[j]) * pw[k]);
+                a(0, j) = a(0, j) + (A)((mass[i] / rho[i]) * pw[k]);
+            });
+        }
+        {
+            A* arr[1] = {acc.data()};
+            pair_loop(1, arr, [&](size_t k, auto& a) {
+                int i = pairs[k].i, j = pairs[k].j;
+                a(0, i) = a(0, i) + (A)(mass[j] * pw[k]);
+                a(0, j) = a(0, j) + (A)(mass[i] * pw[k]);
+            });
         }
         for (int i = 0; i < n; i++) rho[i] = (R)acc[i];
         if (nor)
@@ -423,7 +532,8 @@ struct Oracle {
             p[i] = (cgra05 * rho[i]) * rho[i]; /* :6797 */
         }
         std::vector<A> a0(n, (A)0), a1(n, (A)0);
-        for (size_t k = 0; k < pairs.size(); k++) {
+        A* arr[2] = {a0.data(), a1.data()};
+        pair_loop(2, arr, [&](size_t k, auto& a) {
             int i = pairs[k].i, j = pairs[k].j;
             R mi = mass[i], mj = mass[j];
             R g[2] = {pd0[k], pd1[k]};
@@ -436,11 +546,10 @@ struct Oracle {
                 } else { /* :6914-6920 */
                     h = -(p[i] / (rho[i] * rho[i]) + p[j] / (rho[j] * rho[j])) * g[d];
                 }
-                A* ai = d ? &a1[0] : &a0[0];
-                ai[i] = ai[i] + (A)(mj * h);
-                ai[j] = ai[j] - (A)(mi * h);
+                a(d, i) = a(d, i) + (A)(mj * h);
+                a(d, j) = a(d, j) - (A)(mi * h);
             }
-        }
+        });
         for (int i = 0; i < n; i++) { in[2 * i] = (R)a0[i]; in[2 * i + 1] = (R)a1[i]; }
     }
 
@@ -641,9 +750,10 @@ struct Oracle {
     /* ExtForces_SW(0): SPH_SW_2019.f90:8483 and the particle loop :8532-8716 */
     void ext_forces0() {
         std::fill(ex.begin(), ex.end(), (R)0);
-        R top[6];
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < n; i++) {
             if (flag[i]) continue;
+            R top[6];
             Local L;
             ext_locals(i, rho[i], L);
             grav_and_friction(i, L, top);
@@ -666,9 +776,10 @@ struct Oracle {
         if (!ic_erosion) return;
         std::fill(auxv1.begin(), auxv1.end(), (A)0);
         std::fill(auxv2.begin(), auxv2.end(), (A)0);
-        R top[6];
-        for (int i = 0; i < n; i++) {
-            if (flag[i]) continue;
+        /* particle i's terms for its (up to 4 x 4) DEM nodes, in the
+         * order they are added: emit(ip, base / dist, 1 / dist) */
+        auto node_terms = [&](int i, auto&& emit) {
+            R top[6];
             Local L;
             ext_locals(i, rho[i], L);
             grav_and_friction(i, L, top);
@@ -685,11 +796,41 @@ struct Oracle {
                     R dx2 = xx - coorgx(ix - 1); dx2 = dx2 * dx2;
                     R dy2 = yy - coorgy(iy - 1); dy2 = dy2 * dy2;
                     R dist = rmax<R>(lit<R>(1.e-6), std::sqrt(dx2 + dy2));
-                    auxv1[ip] = auxv1[ip] + (A)(base / dist);
-                    auxv2[ip] = auxv2[ip] + (A)((R)1 / dist);
+                    emit(ip, (A)(base / dist), (A)((R)1 / dist));
                 }
             mass[i] = mass[i] + ((dt * er) * mass[i]) / rho[i];
+        };
+        bool done = false;
+#ifdef _OPENMP
+        if (omp_get_max_threads() > 1) {
+            /* terms computed in parallel, added to the nodes in particle
+             * order: the same sums as the serial loop */
+            std::vector<int> tip((size_t)16 * n, -1);
+            std::vector<A> tv1((size_t)16 * n), tv2((size_t)16 * n);
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                int m = 0;
+                node_terms(i, [&](int ip, A a1, A a2) {
+                    tip[16 * (size_t)i + m] = ip; tv1[16 * (size_t)i + m] = a1; tv2[16 * (size_t)i + m] = a2; m++;
+                });
+            }
+            for (size_t e = 0; e < tip.size(); e++) {
+                if (tip[e] < 0) continue;
+                auxv1[tip[e]] = auxv1[tip[e]] + tv1[e];
+                auxv2[tip[e]] = auxv2[tip[e]] + tv2[e];
+            }
+            done = true;
         }
+#endif
+        for (int i = 0; i < n && !done; i++) {
+            if (flag[i]) continue;
+            node_terms(i, [&](int ip, A a1, A a2) {
+                auxv1[ip] = auxv1[ip] + a1;
+                auxv2[ip] = auxv2[ip] + a2;
+            });
+        }
+#pragma omp parallel for schedule(static)
         for (int ip = 0; ip < npoig; ip++) {
             if ((R)auxv2[ip] > lit<R>(1.e-6)) {
                 R xnum = (R)(auxv1[ip] / auxv2[ip]);
@@ -740,18 +881,18 @@ struct Oracle {
     /* av_vel, SPH_MAIN_2019.f90:3042-3099, and v += av (:987-993) */
     void av_vel() {
         std::vector<A> a0(n, (A)0), a1(n, (A)0);
-        for (size_t k = 0; k < pairs.size(); k++) {
+        A* arr[2] = {a0.data(), a1.data()};
+        pair_loop(2, arr, [&](size_t k, auto& a) {
             int i = pairs[k].i, j = pairs[k].j;
             for (int d = 0; d < 2; d++) {
                 R dvx = v[2 * i + d] - v[2 * j + d];
                 R den = rho[i] + rho[j];
                 R ti = ((((R)2 * mass[j]) * dvx) / den) * pw[k];
                 R tj = ((((R)2 * mass[i]) * dvx) / den) * pw[k];
-                A* a = d ? &a1[0] : &a0[0];
-                a[i] = a[i] - (A)ti;
-                a[j] = a[j] + (A)tj;
+                a(d, i) = a(d, i) - (A)ti;
+                a(d, j) = a(d, j) + (A)tj;
             }
-        }
+        });
         const R eps = lit<R>(0.3);
         for (int i = 0; i < n; i++) {
             if (flag[i]) continue;

@@ -13,32 +13,56 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libgfsph_oracle.so")
+# the same source built with OpenMP: only for timing the CPU baseline on all
+# host cores (its pair sums are added in another order than the checker's)
+LIB_OMP = os.path.join(HERE, "_build", "libgfsph_oracle_omp.so")
 NTOPO = 16
 
 MODE_FP32 = 0        # reference FP32 build
 MODE_FP32_DACC = 1   # FP32 state, FP64 sums (the GPU scheme)
 MODE_FP64 = 2        # reference FP64 build
 
-_lib = None
+_libs = {}
 _DP = C.POINTER(C.c_double)
 _IP = C.POINTER(C.c_int)
 
 
 def build():
+    """Builds the checker library (and the OpenMP one where the compiler
+    takes -fopenmp) when missing or older than the source."""
     src = os.path.join(HERE, "gfsph_oracle.cpp")
     hdr = os.path.join(HERE, "..", "include", "gfsph.h")
-    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(src), os.path.getmtime(hdr)):
-        return LIB
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    newest = max(os.path.getmtime(src), os.path.getmtime(hdr))
+    if not (os.path.exists(LIB) and os.path.getmtime(LIB) >= newest
+            and (not os.path.exists(LIB_OMP) or os.path.getmtime(LIB_OMP) >= newest)):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
+def omp_available():
+    return os.path.exists(LIB_OMP)
+
+
+def omp_threads():
+    """Threads the OpenMP library runs with (OMP_NUM_THREADS, else every
+    host core this process may use)."""
+    env = os.environ.get("OMP_NUM_THREADS", "").split(",")[0].strip()
+    if env.isdigit() and int(env) > 0:
+        return int(env)
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def lib(omp=False):
+    path = LIB_OMP if omp else LIB
+    if path not in _libs:
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(LIB)
+        if not os.path.exists(path):
+            raise RuntimeError("the OpenMP oracle library was not built (no compiler with -fopenmp)")
+        L = C.CDLL(path)
         L.oracle_run.restype = C.c_int
         L.oracle_run.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                  C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, _DP, C.c_int, C.c_int, _DP,
@@ -78,8 +102,8 @@ def lib():
         L.oracle_solvegc2.restype = C.c_int
         L.oracle_solvegc2.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP, _DP, _DP, _DP,
                                       C.c_double, _IP]
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def _d(a):
@@ -210,19 +234,22 @@ class Run:
     """A persistent oracle run: the state stays inside the oracle between
     advance() calls, so timing advance() measures only the steps."""
 
-    def __init__(self, mode, params, nx, ny, dx, dy, state, xmin=0.0, ymin=0.0):
+    def __init__(self, mode, params, nx, ny, dx, dy, state, xmin=0.0, ymin=0.0, omp=False):
+        """omp=True runs the OpenMP library (timing only)."""
         self.params = params
         self.n = state.x.shape[0]
         self.topol_shape = state.topol.shape
+        self.L = lib(omp)
         stv = C.c_int(0)
-        self.h = lib().oracle_new(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), self.n,
+        self.h = None
+        self.h = self.L.oracle_new(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), self.n,
                                   _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.hsml),
                                   _ip(state.flag), _dp(state.pwp), state.dt, state.t, C.byref(stv))
         if not self.h:
             raise RuntimeError(f"oracle_new: {stv.value}")
 
     def advance(self, nsteps, t_end=1e300):
-        return lib().oracle_advance(self.h, nsteps, t_end)
+        return self.L.oracle_advance(self.h, nsteps, t_end)
 
     def state(self, with_topol=False):
         n = self.n
@@ -231,17 +258,17 @@ class Run:
         flag = np.zeros(n, np.int32)
         dt, t = C.c_double(), C.c_double()
         topol = np.zeros(self.topol_shape) if with_topol else None
-        lib().oracle_get(self.h, _dp(x), _dp(v), _dp(rho), _dp(mass), _dp(hsml), _ip(flag), C.byref(dt), C.byref(t),
+        self.L.oracle_get(self.h, _dp(x), _dp(v), _dp(rho), _dp(mass), _dp(hsml), _ip(flag), C.byref(dt), C.byref(t),
                          _dp(topol))
         pwp = None
         if self.params.icpwp == 3:
             pwp = np.zeros(n)
-            lib().oracle_get_pwp(self.h, _dp(pwp))
+            self.L.oracle_get_pwp(self.h, _dp(pwp))
         return State(x, v, rho, mass, hsml, topol if with_topol else np.zeros(1), flag, dt.value, t.value, pwp)
 
     def close(self):
         if self.h:
-            lib().oracle_free(self.h)
+            self.L.oracle_free(self.h)
             self.h = None
 
     def __del__(self):
