@@ -150,8 +150,8 @@ def cpu_reference_rate(seconds_budget, warm_steps=20, omp=False, steps=None):
     may use; steps fixes the timed steps (else the budget sets them).
     Returns (particle-steps/s, steps, n, seconds, threads, sample)."""
     oracle, w, p, nx, ny, st = _oracle_case()
-    threads = oracle.omp_threads() if omp else 1
     run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st, omp=omp)
+    threads = run.threads
     run.advance(warm_steps)
     t0 = time.perf_counter()
     run.advance(1)

@@ -1665,6 +1665,18 @@ int oracle_get_pwp(void* h, double* pwp) {
 
 void oracle_free(void* h) { delete static_cast<OracleBase*>(h); }
 
+/* Threads of the OpenMP build's parallel regions entered from the calling
+ * thread (t > 0 sets them); returns the count in effect, 1 without OpenMP. */
+int oracle_set_threads(int t) {
+#ifdef _OPENMP
+    if (t > 0) omp_set_num_threads(t);
+    return omp_get_max_threads();
+#else
+    (void)t;
+    return 1;
+#endif
+}
+
 /* Neighbour sets (CSR, sorted), summation density and internal forces of the
  * reference on one state. Any of offsets/rho_out/indvxdt may be NULL. */
 int oracle_pairs(int mode, const gfsph_params* p, int n, const double* x, const double* hsml, const double* mass,

@@ -43,16 +43,39 @@ def omp_available():
     return os.path.exists(LIB_OMP)
 
 
+def _cgroup_cpus():
+    """CPUs the container's CPU quota allows (cgroup v2 or v1), else None."""
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as f:
+            q, per = f.read().split()[:2]
+        if q != "max":
+            return max(1, -(-int(q) // int(per)))
+    except (OSError, ValueError):
+        pass
+    try:
+        with open("/sys/fs/cgroup/cpu/cpu.cfs_quota_us") as f:
+            q = int(f.read())
+        with open("/sys/fs/cgroup/cpu/cpu.cfs_period_us") as f:
+            per = int(f.read())
+        if q > 0 and per > 0:
+            return max(1, -(-q // per))
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def omp_threads():
-    """Threads the OpenMP library runs with (OMP_NUM_THREADS, else every
-    host core this process may use)."""
+    """Threads the OpenMP library runs with: OMP_NUM_THREADS, else every
+    host core this process may use, capped by the container's CPU quota."""
     env = os.environ.get("OMP_NUM_THREADS", "").split(",")[0].strip()
     if env.isdigit() and int(env) > 0:
         return int(env)
     try:
-        return len(os.sched_getaffinity(0))
+        n = len(os.sched_getaffinity(0))
     except AttributeError:
-        return os.cpu_count() or 1
+        n = os.cpu_count() or 1
+    q = _cgroup_cpus()
+    return min(n, q) if q else n
 
 
 def lib(omp=False):
@@ -99,6 +122,8 @@ def lib(omp=False):
         L.oracle_get_pwp.argtypes = [C.c_void_p, _DP]
         L.oracle_free.restype = None
         L.oracle_free.argtypes = [C.c_void_p]
+        L.oracle_set_threads.restype = C.c_int
+        L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_solvegc2.restype = C.c_int
         L.oracle_solvegc2.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP, _DP, _DP, _DP,
                                       C.c_double, _IP]
@@ -240,6 +265,7 @@ class Run:
         self.n = state.x.shape[0]
         self.topol_shape = state.topol.shape
         self.L = lib(omp)
+        self.threads = self.L.oracle_set_threads(omp_threads() if omp else 0)
         stv = C.c_int(0)
         self.h = None
         self.h = self.L.oracle_new(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), self.n,

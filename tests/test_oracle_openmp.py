@@ -39,5 +39,13 @@ def test_openmp_build_matches_checker(mode, rtol):
         assert np.abs(x - y).max() <= rtol * scale, k
 
 
-def test_thread_count_reported():
-    assert oracle.omp_threads() >= 1
+def test_thread_count_set_in_the_library():
+    w = workloads.fractal_channel(n_target=6000, dem_k=8, cell=5.0)
+    p = workloads.make_params(w, gfsph)
+    ny, nx = w.z.shape
+    topol = oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv)
+    st = oracle.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    r = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st, omp=True)
+    assert r.threads == oracle.omp_threads() >= 1
+    r.close()
+    assert oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st).threads == 1
