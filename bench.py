@@ -527,9 +527,12 @@ def main():
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
         if oracle.omp_available():
-            # the same steps as the single-thread sample
-            rate, steps, nc, el, threads, desc = cpu_reference_rate(args.cpu_seconds, omp=True, steps=steps)
-            cpu["openmp"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+            try:
+                # the same steps as the single-thread sample
+                rate, steps, nc, el, threads, desc = cpu_reference_rate(args.cpu_seconds, omp=True, steps=steps)
+                cpu["openmp"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+            except (OSError, RuntimeError) as e:
+                cpu["openmp"] = {"unavailable": f"{type(e).__name__}: {e}"}
         else:
             cpu["openmp"] = {"unavailable": "the OpenMP build of the oracle was not made (no -fopenmp compiler)"}
 
