@@ -39,6 +39,7 @@ static_assert(kThreads <= 32 * kScatterWarps, "erosion_scatter keeps shared term
 constexpr int kGraphSteps = 8;       // steps captured per multi-step graph
 constexpr int kChunkSteps = 256;     // steps between host checks of the error word
 constexpr int kMaxCells = kScanTile * 8192;
+constexpr int kMaxNeighbours = 65536;  // largest initial neighbour-table capacity a handle accepts
 
 __global__ void k_copy_state(PState A, PState B, int n) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
@@ -94,7 +95,10 @@ template <class T>
 int dalloc(T** p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
-    return cudaMalloc((void**)p, count * sizeof(T)) == cudaSuccess ? 0 : GFSPH_ERR_CUDA;
+    if (cudaMalloc((void**)p, count * sizeof(T)) == cudaSuccess) return 0;
+    *p = nullptr;
+    cudaGetLastError();  // a failed allocation is not sticky: later checks see only new errors
+    return GFSPH_ERR_CUDA;
 }
 template <class T>
 void dfree(T*& p) {
@@ -527,39 +531,45 @@ int kernels_per_step(const gfsph_handle* h) {
     return 13 + body + (h->rheo.av_vel ? 2 : 0) + 1;
 }
 
+// The three buffer (re)allocations below drop the graphs (which hold the old
+// buffers) and zero the capacity before freeing; on failure they leave the
+// buffers freed and the capacity 0.
 int alloc_blocks(gfsph_handle* h, int cap) {
     if (cap > kMaxCells) return GFSPH_ERR_CAPACITY;
+    drop_graphs(h);
+    h->cap_blocks = 0;
     dfree(h->bmark); dfree(h->bstart);
     int st = 0;
     st |= dalloc(&h->bmark, (size_t)cap + 1);
     st |= dalloc(&h->bstart, (size_t)cap + 1);
-    if (st) return GFSPH_ERR_CUDA;
+    if (st) { dfree(h->bmark); dfree(h->bstart); return GFSPH_ERR_CUDA; }
     CK(cudaMemsetAsync(h->bmark, 0, ((size_t)cap + 1) * sizeof(int), h->stream));
     h->cap_blocks = cap;
-    drop_graphs(h);
     return 0;
 }
 
 int alloc_cells(gfsph_handle* h, int cap) {
     if (cap > kMaxCells) return GFSPH_ERR_CAPACITY;
+    drop_graphs(h);
+    h->cap_cells = 0;
     dfree(h->count); dfree(h->start); dfree(h->tile_sum);
     int st = 0;
     st |= dalloc(&h->count, (size_t)cap + 1);
     st |= dalloc(&h->start, (size_t)cap + 1);
     st |= dalloc(&h->tile_sum, 8192);
-    if (st) return GFSPH_ERR_CUDA;
+    if (st) { dfree(h->count); dfree(h->start); dfree(h->tile_sum); return GFSPH_ERR_CUDA; }
     CK(cudaMemsetAsync(h->count, 0, ((size_t)cap + 1) * sizeof(int), h->stream));
     h->cap_cells = cap;
-    drop_graphs(h);
     return 0;
 }
 
 int alloc_nbr(gfsph_handle* h, int kcap) {
+    drop_graphs(h);
+    h->kcap = 0;
     dfree(h->nbr);
     const size_t rows = ((size_t)std::max(h->n, 1) + 31) / 32 * 32;  // whole warps (tab_base)
     if (dalloc(&h->nbr, (size_t)kcap * rows)) return GFSPH_ERR_CUDA;
     h->kcap = kcap;
-    drop_graphs(h);
     return 0;
 }
 
@@ -579,6 +589,21 @@ void free_particles(gfsph_handle* h) {
     dfree(h->carry.v); dfree(h->carry.acc); dfree(h->carry.dx); dfree(h->carry.dv); dfree(h->carry.xo);
     dfree(h->carry.out); dfree(h->rhoS); dfree(h->rcell); dfree(h->xsv); dfree(h->pr);
     h->kcap = 0;
+}
+
+// After a failed device allocation: the handle keeps no particle state, no
+// graphs and no buffers (every call but gfsph_upload then returns
+// GFSPH_ERR_STATE); the next gfsph_upload allocates afresh.  Returns err.
+int drop_state(gfsph_handle* h, int err) {
+    drop_graphs(h);
+    free_particles(h);
+    dfree(h->count); dfree(h->start); dfree(h->tile_sum); dfree(h->bmark); dfree(h->bstart);
+    h->cap_cells = 0;
+    h->cap_blocks = 0;
+    h->n = 0;
+    h->has_state = false;
+    h->searched = false;
+    return err;
 }
 
 int alloc_pstate(PState* p, int n) {
@@ -614,7 +639,7 @@ int grow_after_error(gfsph_handle* h) {
         if (want > kMaxCells) want = kMaxCells;
         if (want < s->need_cells) return GFSPH_ERR_CAPACITY;
         int st = alloc_cells(h, (int)want);
-        if (st) return st;
+        if (st) return st == GFSPH_ERR_CUDA ? drop_state(h, st) : st;
         set_field<int>(h, offsetof(StepScalars, ncells), 0);
     }
     if (e & kErrBlocks) {
@@ -622,12 +647,12 @@ int grow_after_error(gfsph_handle* h) {
         if (want > kMaxCells) want = kMaxCells;
         if (want < s->need_blocks) return GFSPH_ERR_CAPACITY;
         int st = alloc_blocks(h, (int)want);
-        if (st) return st;
+        if (st) return st == GFSPH_ERR_CUDA ? drop_state(h, st) : st;
     }
     if (e & kErrNbr) {
         int want = std::max(s->need_nbr + 16, h->kcap * 3 / 2);
         int st = alloc_nbr(h, want);
-        if (st) return st;
+        if (st) return st == GFSPH_ERR_CUDA ? drop_state(h, st) : st;
     }
     set_field<int>(h, offsetof(StepScalars, err), 0);
     set_field<int>(h, offsetof(StepScalars, need_nbr), 0);
@@ -680,6 +705,7 @@ int validate(const gfsph_params* p) {
     if ((p->skf == 2 || p->skf == 3) && p->nnps != 2) return GFSPH_ERR_UNSUPPORTED;
     if (p->pa_sph != 1 && p->pa_sph != 2) return GFSPH_ERR_UNSUPPORTED;
     if (p->nnps != 2 && p->nnps != 4) return GFSPH_ERR_UNSUPPORTED;
+    if (p->max_neighbours < 0 || p->max_neighbours > kMaxNeighbours) return GFSPH_ERR_ARG;
     if (p->sle != 0 && p->sle != 1) return GFSPH_ERR_UNSUPPORTED;
     if (p->summation_density != 1 || (p->nor_density != 0 && p->nor_density != 1)) return GFSPH_ERR_UNSUPPORTED;
     if (p->ic_adapt != 0 && p->ic_adapt != 1 && p->ic_adapt != 2 && p->ic_adapt != 4 && p->ic_adapt != 10)
@@ -878,7 +904,9 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
             if (itype[i] != 1) return GFSPH_ERR_UNSUPPORTED;  // only soil particles (ic_ws_Interact = 0)
     if (n != h->n) {
         CK(cudaStreamSynchronize(h->stream));
+        drop_graphs(h);
         free_particles(h);
+        h->has_state = false;
         h->n = n;
         int st = 0;
         st |= alloc_pstate(&h->A, n); st |= alloc_pstate(&h->B, n); st |= alloc_pstate(&h->U, n);
@@ -893,18 +921,18 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
             if (h->rheo.nor_density) st |= dalloc(&h->rhoS, 5 * (size_t)n);
         }
         if (h->rheo.skf == 2 || h->rheo.skf == 3) st |= dalloc(&h->rcell, n);
-        if (st) { free_particles(h); h->n = 0; return GFSPH_ERR_CUDA; }
+        if (st) return drop_state(h, GFSPH_ERR_CUDA);
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
-        if (st) return st;
-        drop_graphs(h);
+        if (st) return drop_state(h, st);
     }
     if (h->cap_cells == 0) {
         int st = alloc_cells(h, 1 << 18);
-        if (st) return st;
+        if (st) return drop_state(h, st);
+        set_field<int>(h, offsetof(StepScalars, ncells), 0);
     }
     if (h->cap_blocks == 0) {
         int st = alloc_blocks(h, 1 << 16);
-        if (st) return st;
+        if (st) return drop_state(h, st);
     }
     cudaStream_t st = h->stream;
     CK(cudaMemcpyAsync(h->B.pos, x, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, st));
@@ -1247,7 +1275,10 @@ int gfsph_hazard_reset(gfsph_handle* h) {
         int st = 0;
         st |= dalloc(&h->haz_sum_h, np); st |= dalloc(&h->haz_sum_v, np);
         st |= dalloc(&h->haz_max_h, np); st |= dalloc(&h->haz_max_v, np); st |= dalloc(&h->haz_cnt, np);
-        if (st) return GFSPH_ERR_CUDA;
+        if (st) {
+            dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
+            return GFSPH_ERR_CUDA;
+        }
     }
     cudaStream_t s = h->stream;
     CK(cudaMemsetAsync(h->haz_sum_h, 0, (size_t)np * sizeof(double), s));
@@ -1478,6 +1509,7 @@ int adj_capture(gfsph_adjoint* a, float2* x, float2* v, bool fields) {
 
 int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v, const float* rho = nullptr) {
     gfsph_handle* h = a->h;
+    if (h->n != a->n) return GFSPH_ERR_STATE;  // the handle's buffers were dropped or resized
     launch(h, K_ADJOINT, [&] {
         k_adj_restore<<<blocks_for(a->n), kThreads, 0, h->stream>>>(h->B, a->n, x, v, rho ? rho : a->rho0, a->mass0,
                                                                     a->hsml0);
@@ -1654,6 +1686,9 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
                            float* gm, double* gmu, double* gxi) {
     if (!a || !gx || !gv) return GFSPH_ERR_ARG;
     gfsph_handle* h = a->h;
+    // the handle must still hold a state of the recorded size (an upload of
+    // another size, or a failed allocation, since the forward run voids it)
+    if (!h->has_state || h->n != a->n) return GFSPH_ERR_STATE;
     cudaStream_t st = h->stream;
     const int n = a->n;
     const size_t un = (size_t)n;

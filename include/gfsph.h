@@ -40,7 +40,10 @@ extern "C" {
 #define GFSPH_OK 0
 #define GFSPH_T_END_REACHED 1        /* warning: stopped early because time >= t_end */
 #define GFSPH_ERR_ARG (-1)           /* bad argument (null pointer, bad size) */
-#define GFSPH_ERR_CUDA (-2)          /* CUDA runtime error */
+#define GFSPH_ERR_CUDA (-2)          /* CUDA runtime error; when a device allocation failed
+                                        (in gfsph_upload or while growing the grid or the
+                                        neighbour table during a step) the handle holds no
+                                        state until the next gfsph_upload */
 #define GFSPH_ERR_CAPACITY (-3)      /* cell grid / neighbour table could not be grown */
 #define GFSPH_ERR_UNSUPPORTED (-4)   /* option outside the implemented path */
 #define GFSPH_ERR_STATE (-5)         /* call out of order (e.g. step before upload) */
@@ -76,7 +79,8 @@ typedef struct gfsph_params {
     float h_inf;           /* h_inf_SW */
     float dt;              /* initial dt_sph */
     int dem_deriv;         /* slopes when not supplied: 0 FEM projection (Get_Topol), 1 finite differences */
-    int max_neighbours;    /* initial neighbour-table capacity per particle; 0 = 96 (grows on demand) */
+    int max_neighbours;    /* initial neighbour-table capacity per particle, 0..65536;
+                              0 = 96 (grows on demand) */
     int icpwp;             /* 0 none, 3 basal pore-water pressure with one point (Get_Pwp_SW, nUaux = 1) */
     float pwp0rel;         /* icpwp = 3: initial Uaux = pwp0rel * rho * const(14) (Input_SW SPH_SW_2019.f90:1829-1852) */
     int reserved[6];

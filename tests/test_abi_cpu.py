@@ -56,6 +56,11 @@ def test_rejects_unsupported_options_before_touching_the_device(gfsph_lib):
     p = gfsph_lib.make_params({1: 9.8, 2: 2000, 3: 500, 5: 1, 9: 0.2, 10: 0.01, 15: 0.01})  # Manning
     with pytest.raises(gfsph_lib.GfsphError):
         gfsph_lib.Sim(p, z, dx=1.0, dy=1.0)
+    for mn in (-1, 65537):  # initial neighbour-table capacity outside 0..65536
+        p = gfsph_lib.make_params(base, max_neighbours=mn)
+        with pytest.raises(gfsph_lib.GfsphError) as e:
+            gfsph_lib.Sim(p, z, dx=1.0, dy=1.0)
+        assert e.value.status == -1
 
 
 def test_no_cpu_fallback_without_device(gfsph_lib):
