@@ -745,6 +745,7 @@ const char* gfsph_strerror(int s) {
     case GFSPH_ERR_NO_DEVICE: return "no usable CUDA device";
     case GFSPH_ERR_NONFINITE: return "non-finite value in the particle state";
     case GFSPH_ERR_DOMAIN: return "no particle inside the DEM box";
+    case GFSPH_ERR_HOST: return "host memory allocation failed";
     default: return "unknown status";
     }
 }
@@ -752,7 +753,7 @@ const char* gfsph_strerror(int s) {
 int gfsph_num_kernels(void) { return K_COUNT; }
 const char* gfsph_kernel_name(int k) { return (k >= 0 && k < K_COUNT) ? kKernelNames[k] : nullptr; }
 
-int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out) {
+int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out) try {
     if (!p || !dem || !out) return GFSPH_ERR_ARG;
     *out = nullptr;
     int st = validate(p);
@@ -764,7 +765,7 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return GFSPH_ERR_NO_DEVICE;
 
     gfsph_handle* h = new (std::nothrow) gfsph_handle();
-    if (!h) return GFSPH_ERR_ARG;
+    if (!h) return GFSPH_ERR_HOST;
     cudaGetDevice(&h->dev);
     if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
@@ -802,7 +803,16 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     // DEM rows on the host, as Topo_main leaves them before the time loop
     int nx = dem->nx, ny = dem->ny;
     size_t np = (size_t)nx * ny;
-    std::vector<float> topol(np * GFSPH_NTOPO, 0.f);
+    std::vector<float> topol, z, er, av;
+    std::vector<float2> grad, curvB;
+    std::vector<float4> curvA;
+    try {
+        topol.assign(np * GFSPH_NTOPO, 0.f);
+        grad.resize(np); curvB.resize(np); curvA.resize(np); z.resize(np); er.resize(np); av.resize(np);
+    } catch (...) {
+        gfsph_destroy(h);
+        return GFSPH_ERR_HOST;
+    }
     if (dem->topol) {
         for (size_t ip = 0; ip < np; ip++)
             for (int r = 0; r < 15; r++) topol[ip * GFSPH_NTOPO + r] = dem->topol[ip * (size_t)dem->ntopo + r];
@@ -815,9 +825,6 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
         if (k[20] > 1.e-9f) avail = (k[47] > 1.e-6f) ? k[47] : 999.f;
         for (size_t ip = 0; ip < np; ip++) topol[ip * GFSPH_NTOPO + 14] = avail;
     }
-    std::vector<float2> grad(np), curvB(np);
-    std::vector<float4> curvA(np);
-    std::vector<float> z(np), er(np), av(np);
     for (size_t ip = 0; ip < np; ip++) {
         const float* t = &topol[ip * GFSPH_NTOPO];
         z[ip] = t[0];
@@ -860,9 +867,11 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     if (cudaGetLastError() != cudaSuccess) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
     *out = h;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_destroy(gfsph_handle* h) {
+int gfsph_destroy(gfsph_handle* h) try {
     if (!h) return GFSPH_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
@@ -887,17 +896,21 @@ int gfsph_destroy(gfsph_handle* h) {
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_set_stream(gfsph_handle* h, void* stream) {
+int gfsph_set_stream(gfsph_handle* h, void* stream) try {
     if (!h) return GFSPH_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
     h->stream = stream ? (cudaStream_t)stream : h->own_stream;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const float* rho, const float* mass,
-                 const float* hsml, const int* itype, const int* out_flag) {
+                 const float* hsml, const int* itype, const int* out_flag) try {
     if (!h || n < 1 || !x || !v || !rho || !mass || !hsml) return GFSPH_ERR_ARG;
     if (itype)
         for (int i = 0; i < n; i++)
@@ -953,9 +966,11 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
     h->has_state = true;
     h->searched = false;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass, float* hsml, int* out_flag) {
+int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass, float* hsml, int* out_flag) try {
     if (!h) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     int n = h->n;
@@ -969,9 +984,11 @@ int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass,
     if (out_flag) CK(cudaMemcpyAsync(out_flag, h->U.flag, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_set_pwp(gfsph_handle* h, const float* pwp) {
+int gfsph_set_pwp(gfsph_handle* h, const float* pwp) try {
     if (!h || !pwp) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     int n = h->n;
@@ -980,9 +997,11 @@ int gfsph_set_pwp(gfsph_handle* h, const float* pwp) {
     launch(h, K_UNSORT, [&] { k_gather_by_id<<<blocks_for(n), kThreads, 0, st>>>(h->U.pwp, h->B.id, n, h->B.pwp); });
     CK(cudaStreamSynchronize(st));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_get_pwp(gfsph_handle* h, float* pwp) {
+int gfsph_get_pwp(gfsph_handle* h, float* pwp) try {
     if (!h || !pwp) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     int n = h->n;
@@ -991,23 +1010,29 @@ int gfsph_get_pwp(gfsph_handle* h, float* pwp) {
     CK(cudaMemcpyAsync(pwp, h->U.pwp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_get_time(gfsph_handle* h, double* t, float* dt) {
+int gfsph_get_time(gfsph_handle* h, double* t, float* dt) try {
     if (!h) return GFSPH_ERR_ARG;
     int st = read_scalars(h);
     if (st) return st;
     if (t) *t = h->hS->time;
     if (dt) *dt = h->hS->dt;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_set_time(gfsph_handle* h, double t, float dt) {
+int gfsph_set_time(gfsph_handle* h, double t, float dt) try {
     if (!h || !(dt > 0.f)) return GFSPH_ERR_ARG;
     set_field<double>(h, offsetof(StepScalars, time), t);
     set_field<float>(h, offsetof(StepScalars, dt), dt);
     CK(cudaStreamSynchronize(h->stream));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 }  // extern "C"
@@ -1071,7 +1096,7 @@ int finish_chunk(gfsph_handle* h, int chunk, double t_end, int& done, int& guard
 
 extern "C" {
 
-int gfsph_step(gfsph_handle* h, int nsteps, double t_end, double* t_out, int* steps_done) {
+int gfsph_step(gfsph_handle* h, int nsteps, double t_end, double* t_out, int* steps_done) try {
     if (!h || nsteps < 0) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     int done = 0, guard = 0, status = GFSPH_OK;
@@ -1089,6 +1114,8 @@ int gfsph_step(gfsph_handle* h, int nsteps, double t_end, double* t_out, int* st
     if (t_out) *t_out = h->hS->time;
     if (steps_done) *steps_done = done;
     return status;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 // search + density on the current state (no advance); the state in B is
@@ -1112,7 +1139,7 @@ static int search_only(gfsph_handle* h) {
     return GFSPH_ERR_CAPACITY;
 }
 
-int gfsph_density(gfsph_handle* h, float* rho_out) {
+int gfsph_density(gfsph_handle* h, float* rho_out) try {
     if (!h) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     int st = search_only(h);
@@ -1138,9 +1165,11 @@ int gfsph_density(gfsph_handle* h, float* rho_out) {
     if (rho_out) return gfsph_download(h, nullptr, nullptr, rho_out, nullptr, nullptr, nullptr);
     CK(cudaStreamSynchronize(h->stream));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
+int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) try {
     if (!h || !indvxdt) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     int st = search_only(h);
@@ -1170,9 +1199,11 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) {
     CK(cudaMemcpyAsync(indvxdt, h->f2tmp, (size_t)n * sizeof(float2), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
+int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) try {
     if (!h || !offsets) return GFSPH_ERR_ARG;
     if (!h->searched) return GFSPH_ERR_STATE;
     int n = h->n;
@@ -1205,7 +1236,13 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
             int np = 0;
             cudaMemcpy(&np, dcount, sizeof(int), cudaMemcpyDeviceToHost);
             if (np > pcap) { dfree(dpairs); dfree(dcount); pcap = np; continue; }
-            std::vector<int2> pr(np);
+            std::vector<int2> pr;
+            try {
+                pr.resize(np);
+            } catch (...) {
+                dfree(dpairs); dfree(dcount);
+                return GFSPH_ERR_HOST;
+            }
             cudaMemcpy(pr.data(), dpairs, (size_t)np * sizeof(int2), cudaMemcpyDeviceToHost);
             dfree(dpairs); dfree(dcount);
             for (const int2& q2 : pr) lists[id[q2.x]].push_back(id[q2.y]);
@@ -1225,9 +1262,11 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) {
     offsets[n] = tot;
     CK(cudaGetLastError());
     return (tot > cap) ? GFSPH_ERR_CAPACITY : GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_raster(gfsph_handle* h, int kind, float* out) {
+int gfsph_raster(gfsph_handle* h, int kind, float* out) try {
     if (!h || !out) return GFSPH_ERR_ARG;
     int np = h->nx * h->ny;
     cudaStream_t s = h->stream;
@@ -1266,9 +1305,11 @@ int gfsph_raster(gfsph_handle* h, int kind, float* out) {
     if (kind <= GFSPH_RASTER_COUNT) CK(cudaMemcpyAsync(out, h->d_rout, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_hazard_reset(gfsph_handle* h) {
+int gfsph_hazard_reset(gfsph_handle* h) try {
     if (!h) return GFSPH_ERR_ARG;
     int np = h->nx * h->ny;
     if (!h->haz_cnt) {
@@ -1288,9 +1329,11 @@ int gfsph_hazard_reset(gfsph_handle* h) {
     CK(cudaMemsetAsync(h->haz_cnt, 0, (size_t)np * sizeof(int), s));
     CK(cudaStreamSynchronize(s));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_hazard_sample(gfsph_handle* h) {
+int gfsph_hazard_sample(gfsph_handle* h) try {
     if (!h) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     if (!h->haz_cnt) {
@@ -1304,22 +1347,28 @@ int gfsph_hazard_sample(gfsph_handle* h) {
     });
     CK(cudaGetLastError());
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_profile(gfsph_handle* h, int enable) {
+int gfsph_profile(gfsph_handle* h, int enable) try {
     if (!h) return GFSPH_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
     h->profile = enable == 1;
     h->profile_level = enable;
     for (int k = 0; k < K_COUNT; k++) { h->prof_ms[k] = 0; h->prof_cnt[k] = 0; h->pending[k] = false; }
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_profile_read(gfsph_handle* h, int kernel, double* total_ms, long long* launches) {
+int gfsph_profile_read(gfsph_handle* h, int kernel, double* total_ms, long long* launches) try {
     if (!h || kernel < 0 || kernel >= K_COUNT) return GFSPH_ERR_ARG;
     if (total_ms) *total_ms = h->prof_ms[kernel];
     if (launches) *launches = h->prof_cnt[kernel];
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 long long gfsph_launch_count(gfsph_handle* h) { return h ? h->launches : -1; }
@@ -1350,7 +1399,7 @@ __global__ void k_exceedance(unsigned int* const* maxh, int nreal, int np, float
 
 extern "C" {
 
-int gfsph_ensemble_create(const gfsph_params* params, const gfsph_dem* dem, int nreal, gfsph_ensemble** out) {
+int gfsph_ensemble_create(const gfsph_params* params, const gfsph_dem* dem, int nreal, gfsph_ensemble** out) try {
     if (!params || !dem || !out || nreal < 1) return GFSPH_ERR_ARG;
     *out = nullptr;
     for (int r = 0; r < nreal; r++) {
@@ -1370,7 +1419,13 @@ int gfsph_ensemble_create(const gfsph_params* params, const gfsph_dem* dem, int 
         if (st) return st;
     }
     gfsph_ensemble* e = new (std::nothrow) gfsph_ensemble();
-    if (!e) return GFSPH_ERR_ARG;
+    if (!e) return GFSPH_ERR_HOST;
+    try {
+        e->members.reserve(nreal);  // no push_back below can throw with a handle in hand
+    } catch (...) {
+        delete e;
+        return GFSPH_ERR_HOST;
+    }
     e->nx = dem->nx; e->ny = dem->ny;
     for (int r = 0; r < nreal; r++) {
         gfsph_dem dm = d;
@@ -1390,62 +1445,74 @@ int gfsph_ensemble_create(const gfsph_params* params, const gfsph_dem* dem, int 
     }
     *out = e;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_ensemble_destroy(gfsph_ensemble* e) {
+int gfsph_ensemble_destroy(gfsph_ensemble* e) try {
     if (!e) return GFSPH_ERR_ARG;
     for (gfsph_handle* h : e->members) gfsph_destroy(h);
     dfree(e->d_maxptr);
     dfree(e->d_prob);
     delete e;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_ensemble_member(gfsph_ensemble* e, int r, gfsph_handle** out) {
+int gfsph_ensemble_member(gfsph_ensemble* e, int r, gfsph_handle** out) try {
     if (!e || !out || r < 0 || r >= (int)e->members.size()) return GFSPH_ERR_ARG;
     *out = e->members[r];
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_ensemble_step(gfsph_ensemble* e, int nsteps, double t_end, int* min_steps_done) {
+int gfsph_ensemble_step(gfsph_ensemble* e, int nsteps, double t_end, int* min_steps_done) try {
     if (!e || nsteps < 0) return GFSPH_ERR_ARG;
     const int R = (int)e->members.size();
     for (gfsph_handle* h : e->members)
         if (!h->has_state) return GFSPH_ERR_STATE;
     std::vector<int> done(R, 0), guard(R, 0), active(R, 1);
-    int status = GFSPH_OK;
-    for (;;) {
+    int status = GFSPH_OK, err = GFSPH_OK;
+    while (err == GFSPH_OK) {
         bool any = false;
         std::vector<int> chunk(R, 0);
-        for (int r = 0; r < R; r++) {  // every member's chunk goes out before any wait
+        for (int r = 0; r < R && err == GFSPH_OK; r++) {  // every member's chunk goes out before any wait
             if (!active[r] || done[r] >= nsteps) { active[r] = 0; continue; }
+            int st = enqueue_chunk(e->members[r], std::min(kChunkSteps, nsteps - done[r]), t_end);
+            if (st) { err = st; break; }
             chunk[r] = std::min(kChunkSteps, nsteps - done[r]);
-            int st = enqueue_chunk(e->members[r], chunk[r], t_end);
-            if (st) return st;
             any = true;
         }
         if (!any) break;
+        // every enqueued chunk is waited for, also after an error, so that no
+        // member has work in flight when this returns
         for (int r = 0; r < R; r++) {
             if (!chunk[r]) continue;
             int st = finish_chunk(e->members[r], chunk[r], t_end, done[r], guard[r]);
-            if (st < 0) return st;
+            if (st < 0) { if (err == GFSPH_OK) err = st; active[r] = 0; continue; }
             if (st == 0) { active[r] = 0; status = GFSPH_T_END_REACHED; }
         }
     }
     if (min_steps_done) *min_steps_done = *std::min_element(done.begin(), done.end());
-    return status;
+    return err != GFSPH_OK ? err : status;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_ensemble_sample(gfsph_ensemble* e) {
+int gfsph_ensemble_sample(gfsph_ensemble* e) try {
     if (!e) return GFSPH_ERR_ARG;
     for (gfsph_handle* h : e->members) {
         int st = gfsph_hazard_sample(h);
         if (st) return st;
     }
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob) {
+int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob) try {
     if (!e || !prob) return GFSPH_ERR_ARG;
     const int R = (int)e->members.size();
     const int np = e->nx * e->ny;
@@ -1464,6 +1531,8 @@ int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob) {
     CK(cudaMemcpyAsync(prob, e->d_prob, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 // ---------------------------------------------------------------- adjoint
@@ -1547,7 +1616,7 @@ void adj_free(gfsph_adjoint* a) {
 
 extern "C" {
 
-int gfsph_set_search(gfsph_handle* h, float level_factor, float cell_div) {
+int gfsph_set_search(gfsph_handle* h, float level_factor, float cell_div) try {
     if (!h || !(level_factor >= 1.f && level_factor <= 16.f) || !(cell_div >= 1.f && cell_div <= 8.f))
         return GFSPH_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
@@ -1555,16 +1624,20 @@ int gfsph_set_search(gfsph_handle* h, float level_factor, float cell_div) {
     h->cell_div = cell_div;
     drop_graphs(h);
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_get_search(gfsph_handle* h, float* level_factor, float* cell_div) {
+int gfsph_get_search(gfsph_handle* h, float* level_factor, float* cell_div) try {
     if (!h) return GFSPH_ERR_ARG;
     if (level_factor) *level_factor = h->level_factor;
     if (cell_div) *cell_div = h->cell_div;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_div, float* best_ms) {
+int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_div, float* best_ms) try {
     if (!h || steps < 1) return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
     const size_t n = (size_t)h->n, np = (size_t)h->nx * h->ny;
@@ -1632,9 +1705,11 @@ int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_
     if (cell_div) *cell_div = bcd;
     if (best_ms) *best_ms = best / (float)steps;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint** out) {
+int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint** out) try {
     if (!h || !out || nsteps < 1 || every < 1) return GFSPH_ERR_ARG;
     *out = nullptr;
     if (!h->has_state) return GFSPH_ERR_STATE;
@@ -1644,7 +1719,7 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
         (c.skf != 1 && c.skf != 4))
         return GFSPH_ERR_UNSUPPORTED;
     gfsph_adjoint* a = new (std::nothrow) gfsph_adjoint();
-    if (!a) return GFSPH_ERR_ARG;
+    if (!a) return GFSPH_ERR_HOST;
     a->h = h; a->n = h->n; a->nsteps = nsteps; a->every = std::min(every, nsteps);
     a->nck = (nsteps + a->every - 1) / a->every + 1;
     const size_t n = (size_t)h->n;
@@ -1669,7 +1744,13 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
         if (!st) st = adj_capture(a, a->ckx + n * k, a->ckv + n * k, false);
     }
     if (!st) {  // U holds the final state after the last capture
-        std::vector<int> fl(n);
+        std::vector<int> fl;
+        try {
+            fl.resize(n);
+        } catch (...) {
+            adj_free(a); delete a;
+            return GFSPH_ERR_HOST;
+        }
         cudaError_t e = cudaMemcpyAsync(a->rhoN, h->U.rho, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(fl.data(), h->U.flag, n * sizeof(int), cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -1680,10 +1761,12 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     if (st) { adj_free(a); delete a; return st; }
     *out = a;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, const float* gh, float* gx0, float* gv0,
-                           float* gm, double* gmu, double* gxi) {
+                           float* gm, double* gmu, double* gxi) try {
     if (!a || !gx || !gv) return GFSPH_ERR_ARG;
     gfsph_handle* h = a->h;
     // the handle must still hold a state of the recorded size (an upload of
@@ -1758,17 +1841,21 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
     set_field<double>(h, offsetof(StepScalars, time), a->t0 + (double)a->nsteps * (double)a->dt0);
     CK(cudaStreamSynchronize(st));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_adjoint_destroy(gfsph_adjoint* a) {
+int gfsph_adjoint_destroy(gfsph_adjoint* a) try {
     if (!a) return GFSPH_ERR_ARG;
     adj_free(a);
     delete a;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter, float tol, float* hs_w,
-                 float* gradhs_w) {
+                 float* gradhs_w) try {
     if (!h || nwx < 2 || nwy < 2 || ix0 < 0 || iy0 < 0 || ix0 + nwx > h->nx || iy0 + nwy > h->ny || niter < 0)
         return GFSPH_ERR_ARG;
     if (!h->has_state) return GFSPH_ERR_STATE;
@@ -1849,9 +1936,11 @@ int gfsph_gradhs(gfsph_handle* h, int ix0, int iy0, int nwx, int nwy, int niter,
     if (s3 < 0) return s3;
     if (gradhs_w) std::memcpy(gradhs_w, sol.data(), sol.size() * sizeof(float));
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_stats(gfsph_handle* h, int* out, int nout) {
+int gfsph_stats(gfsph_handle* h, int* out, int nout) try {
     if (!h || !out || nout < 1) return GFSPH_ERR_ARG;
     int st = read_scalars(h);
     if (st) return st;
@@ -1862,6 +1951,8 @@ int gfsph_stats(gfsph_handle* h, int* out, int nout) {
                       h->n - s->nactive};
     for (int k = 0; k < nout && k < 8; k++) out[k] = v[k];
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 }  // extern "C"

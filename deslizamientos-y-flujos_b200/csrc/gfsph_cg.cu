@@ -250,7 +250,7 @@ void cg_free(gfsph_cg* c) {
 extern "C" {
 
 int gfsph_cg_create(int npoin, int nelem, int nnode, int ndofn, const int* intmat, const float* gstif,
-                    gfsph_cg** out) {
+                    gfsph_cg** out) try {
     if (!out || !intmat || !gstif || npoin < 1 || nelem < 1 || nnode < 1 || ndofn < 1) return GFSPH_ERR_ARG;
     *out = nullptr;
     int ndev = 0;
@@ -326,17 +326,21 @@ int gfsph_cg_create(int npoin, int nelem, int nnode, int ndofn, const int* intma
     if (cudaGetLastError() != cudaSuccess) { cg_free(c); delete c; return GFSPH_ERR_CUDA; }
     *out = c;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_cg_destroy(gfsph_cg* c) {
+int gfsph_cg_destroy(gfsph_cg* c) try {
     if (!c) return GFSPH_ERR_ARG;
     cudaStreamSynchronize(c->stream);
     cg_free(c);
     delete c;
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
-int gfsph_cg_solve(gfsph_cg* c, int* iffix, const float* fixed, float* rcg, float* ficg, float tol, int* iterations) {
+int gfsph_cg_solve(gfsph_cg* c, int* iffix, const float* fixed, float* rcg, float* ficg, float tol, int* iterations) try {
     if (!c || !iffix || !fixed || !rcg || !ficg) return GFSPH_ERR_ARG;
     const int n = c->n;
     // getqmat (:124-159): Jacobi preconditioner; free dofs with a vanishing
@@ -413,16 +417,20 @@ int gfsph_cg_solve(gfsph_cg* c, int* iffix, const float* fixed, float* rcg, floa
     }
     if (iterations) *iterations = iters;
     return cudaGetLastError() == cudaSuccess ? GFSPH_OK : GFSPH_ERR_CUDA;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 int gfsph_solvegc2(int npoin, int nelem, int nnode, int ndofn, const int* intmat, int* iffix, const float* fixed,
-                   const float* gstif, float* rcg, float* ficg, float tol, int* iterations) {
+                   const float* gstif, float* rcg, float* ficg, float tol, int* iterations) try {
     gfsph_cg* c = nullptr;
     int st = gfsph_cg_create(npoin, nelem, nnode, ndofn, intmat, gstif, &c);
     if (st) return st;
     st = gfsph_cg_solve(c, iffix, fixed, rcg, ficg, tol, iterations);
     gfsph_cg_destroy(c);
     return st;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }
 
 long long gfsph_cg_launch_count(gfsph_cg* c) { return c ? c->launches : -1; }

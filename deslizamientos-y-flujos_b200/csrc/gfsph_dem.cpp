@@ -105,7 +105,7 @@ void fill_curvature(float* t) {
 
 }  // namespace
 
-extern "C" int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol) {
+extern "C" int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, float* topol) try {
     if (!topol || nx < 3 || ny < 3 || !(dx > 0.f) || !(dy > 0.f)) return GFSPH_ERR_ARG;
     size_t np = (size_t)nx * ny;
     if (mode == 1) {
@@ -157,4 +157,6 @@ extern "C" int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, flo
     project(m, 3, e2, topol, r2);
     for (size_t node = 0; node < np; node++) fill_curvature(&topol[node * GFSPH_NTOPO]);
     return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }

@@ -88,7 +88,7 @@ int scratch_address(double2** out) {
 
 extern "C" int gfsph_raster_idw_noalloc(int n, const float* d_x, const float* d_rho, const int* d_flag, int nx,
                                         int ny, float xmin, float ymin, float dx, float dy, float* d_out,
-                                        void* stream) {
+                                        void* stream) try {
     if (n < 0 || (n > 0 && (!d_x || !d_rho)) || !d_out || nx < 2 || ny < 2 || !(dx > 0.f) || !(dy > 0.f))
         return GFSPH_ERR_ARG;
     if ((long long)nx * (long long)ny > (long long)kNoAllocMaxNodes) return GFSPH_ERR_CAPACITY;
@@ -109,4 +109,6 @@ extern "C" int gfsph_raster_idw_noalloc(int n, const float* d_x, const float* d_
     k_noalloc_finish<<<gb, 256, 0, s>>>(acc, d_out, np);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GFSPH_OK : GFSPH_ERR_CUDA;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
 }

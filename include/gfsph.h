@@ -50,6 +50,7 @@ extern "C" {
 #define GFSPH_ERR_NO_DEVICE (-6)     /* no usable CUDA device */
 #define GFSPH_ERR_NONFINITE (-7)     /* a non-finite value appeared in the state */
 #define GFSPH_ERR_DOMAIN (-8)        /* all particles left the DEM box */
+#define GFSPH_ERR_HOST (-9)          /* host memory could not be allocated */
 
 /*
  * Control parameters.  cst[k-1] holds the reference's const(k)
