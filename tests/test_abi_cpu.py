@@ -41,6 +41,7 @@ def test_library_is_built_for_sm100a(gfsph_lib):
 def test_status_strings(gfsph_lib):
     assert gfsph_lib.strerror(0) == "ok"
     assert "CUDA device" in gfsph_lib.strerror(-6)
+    assert gfsph_lib.strerror(-9) == "host memory allocation failed"
     assert gfsph_lib.lib().gfsph_version() >= 1
 
 
