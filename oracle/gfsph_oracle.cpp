@@ -290,6 +290,7 @@ struct Oracle {
      * size 2*max(hsml), half-stencil pair enumeration, r < scale_k*(hi+hj)/2. */
     void grid_find() {
         pairs.clear(); pw.clear(); pd0.clear(); pd1.clear();
+        if (!any_active()) return;  /* no pairs (and no cell size) without a particle in the box */
         std::vector<R> xr(2 * (size_t)n);
         if (P->nnps == 4) {
             R xg0 = 0, xg1 = 0; int cnt = 0;
@@ -951,13 +952,24 @@ struct Oracle {
         if (P->average_velocity) av_vel();
     }
 
-    /* one iteration of the DTGT loop, SPH_FEM_Driver_2019.f90:1580-1630 */
-    void step() {
+    bool any_active() const {
+        for (int i = 0; i < n; i++)
+            if (!flag[i]) return true;
+        return false;
+    }
+
+    /* one iteration of the DTGT loop, SPH_FEM_Driver_2019.f90:1580-1630.
+     * A step that starts with every particle out of the DEM box returns
+     * GFSPH_ERR_DOMAIN, as the device does: the reference's grid_find would
+     * size its cells by the largest hsml of no particle (zero). */
+    int step() {
+        if (!any_active()) return GFSPH_ERR_DOMAIN;
         adaptive_dt();
         check_out_domain();           /* time_integration_sph :232 */
         rk45();
         check_out_domain();           /* :266 */
         time += (double)dt;
+        return 0;
     }
 
     int setup(const gfsph_params* p_, int nx_, int ny_, double xmin, double ymin, double dx, double dy,
@@ -1048,7 +1060,7 @@ struct OracleObj : OracleBase {
         int done = 0;
         for (int s = 0; s < nsteps; s++) {
             if (o.time >= t_end) break;
-            o.step();
+            if (o.step()) break;
             done++;
         }
         return done;
@@ -1123,10 +1135,11 @@ int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, do
     o.dt = (R)*dt;
     o.time = *t;
     o.init_pwp(pwp_init ? nullptr : pwp);
-    int done = 0;
+    int done = 0, status = 0;
     for (int s = 0; s < nsteps; s++) {
         if (o.time >= t_end) break;
-        o.step();
+        status = o.step();
+        if (status) break;
         done++;
     }
     for (size_t k = 0; k < 2 * (size_t)n; k++) { x[k] = (double)o.x[k]; v[k] = (double)o.v[k]; }
@@ -1139,7 +1152,7 @@ int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, do
     *dt = (double)o.dt;
     *t = o.time;
     if (steps_done) *steps_done = done;
-    return 0;
+    return status;
 }
 
 template <class R, class A>
@@ -1607,13 +1620,14 @@ int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ym
     o.dt = Dual(dt);
     o.time = t;
     o.init_pwp(nullptr);
-    for (int s2 = 0; s2 < nsteps; s2++) o.step();
+    int status = 0;
+    for (int s2 = 0; s2 < nsteps && !status; s2++) status = o.step();
     for (size_t k = 0; k < 2 * (size_t)n; k++) {
         out_x[k] = o.x[k].v; out_v[k] = o.v[k].v;
         tan_x[k] = o.x[k].d; tan_v[k] = o.v[k].d;
     }
     for (int k = 0; k < n; k++) { out_h[k] = o.rho[k].v; tan_h[k] = o.rho[k].d; }
-    return 0;
+    return status;
 }
 
 /* Persistent oracle run: create on a state, advance, read back, free. */

@@ -481,3 +481,92 @@ def test_tangent_oracle_matches_central_differences(oracle_mod):
     fd = (loss(p, w.mass + dm) - loss(p, w.mass - dm)) / 2
     tg = directional(seed_m=dm)
     assert abs(fd - tg) <= 1e-5 * abs(tg)
+
+
+def f32(x):
+    """The value a single-precision parameter carries into the FP64 oracle."""
+    return float(np.float32(x))
+
+
+def test_rk4_integrates_a_constant_acceleration_exactly(oracle_mod):
+    """RK45 (SPH_MAIN_2019.f90:746-1005) is the classical fourth-order scheme
+    with weights 1, 2, 2, 1 over 6: under a constant acceleration (a lone
+    particle sliding down a plane against Coulomb friction) it reproduces
+    v = a t and y = y0 + a t^2 / 2 to rounding over many steps."""
+    tan_t, mu, dt, steps = 0.5, 0.2, 0.05, 200
+    st, _ = single_particle_run(oracle_mod, {3: 0.0, 9: mu}, tan_t, steps, dt)
+    a = f32(9.8) * (tan_t - f32(mu))  # g and mu enter as single-precision constants, dt from the state
+    t = steps * dt
+    assert abs(st.v[0, 1] - a * t) <= 1e-11 * a * t, (st.v[0, 1], a * t)
+    assert abs((st.x[0, 1] - 100.0) - 0.5 * a * t * t) <= 1e-11 * a * t * t, (st.x[0, 1], 0.5 * a * t * t)
+    assert st.x[0, 0] == 50.0 and st.v[0, 0] == 0.0
+
+
+def test_momentum_conserved_on_a_flat_frictionless_bed(oracle_mod):
+    """IntForces_SW (SPH_SW_2019.f90:6905-6920) adds m_j h_ij grad W to i and
+    -m_i h_ij grad W to j, and av_vel (SPH_MAIN_2019.f90:3042-3099) adds
+    -2 m_j (v_i - v_j) W / (h_i + h_j) to i and the mirror term to j: both are
+    antisymmetric, so with no bed slope and no friction (tan phi = 0,
+    Voellmy xi -> infinity) the total momentum sum m v stays fixed while the
+    individual velocities change."""
+    rng = np.random.default_rng(11)
+    s, n = 1.0, 16
+    g = np.arange(n) * s + 60.0
+    X, Y = np.meshgrid(g, g)
+    x = np.stack([X.ravel(), Y.ravel()], 1) + rng.uniform(-0.2, 0.2, (n * n, 2))
+    v = rng.normal(0.0, 1.0, (n * n, 2))
+    mass = rng.uniform(1.5, 2.5, n * n)
+    hsml = np.full(n * n, 1.3 * s)
+    nx = ny = 40
+    d = 5.0
+    p = params({3: 1e30, 9: 0.0}, sle=0, dt=0.01, ic_adapt=0, average_velocity=1)
+    topol = oracle_mod.initial_topol(np.zeros((ny, nx)), d, d, {}, deriv=1, mode=2)
+    st = oracle_mod.State(x, v, np.full(n * n, 2.0), mass, hsml, topol, dt=0.01)
+    p0 = (mass[:, None] * v).sum(0)
+    oracle_mod.run(2, p, nx, ny, d, d, st, 10)
+    assert st.flag.sum() == 0
+    p1 = (st.mass[:, None] * st.v).sum(0)
+    scale = (mass[:, None] * np.abs(v)).sum()
+    assert np.abs(p1 - p0).max() <= 1e-12 * scale, (p0, p1)
+    assert np.abs(st.v - v).max() > 1e-2  # the pair forces did act
+
+
+def test_h_upgrade_takes_the_smoothing_length_from_volume_and_depth(oracle_mod):
+    """h_upgrade with sle = 1 (SPH_MAIN_2019.f90, after RK45): hsml =
+    2 (m / h)^(1/2) from each particle's volume and its new depth."""
+    w = workloads.inclined_plane()
+    p = workloads.make_params(w, gfsph, sle=1)
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, mode=2)
+    st = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=0.01)
+    oracle_mod.run(2, p, nx, ny, w.dx, w.dy, st, 3)
+    assert not np.allclose(st.hsml, w.hsml)
+    assert np.allclose(st.hsml, 2.0 * np.sqrt(st.mass / st.rho), rtol=1e-14, atol=0.0)
+
+
+def test_a_particle_leaving_the_dem_is_flagged_and_frozen(oracle_mod):
+    """Check_Out_Domain (time_integration_sph :232, :266 and every RK stage):
+    a particle outside [xmin, xmax] x [ymin, ymax] gets If_Out_Domain = 1 and
+    is skipped by every later update, so it stops where it left."""
+    nx = ny = 20
+    d = 5.0
+    xmax = (nx - 1) * d
+    p = params({3: 1e30, 9: 0.0}, sle=0, dt=0.05, ic_adapt=0, average_velocity=0)
+    topol = oracle_mod.initial_topol(np.zeros((ny, nx)), d, d, {}, deriv=1, mode=2)
+    vx = 10.0
+    st = oracle_mod.State(np.array([[xmax - 3.0, 40.0]]), np.array([[vx, 0.0]]), np.array([1.0]),
+                          np.array([4.0]), np.array([2.0]), topol, dt=0.05)
+    oracle_mod.run(2, p, nx, ny, d, d, st, 4)  # 2 m in 4 steps: still inside
+    assert st.flag[0] == 0 and st.x[0, 0] < xmax
+    for _ in range(10):  # 0.5 m per step: crosses xmax within 4 more steps
+        oracle_mod.run(2, p, nx, ny, d, d, st, 1)
+        if st.flag[0]:
+            break
+    assert st.flag[0] == 1
+    x_out = st.x[0].copy()
+    assert xmax < x_out[0] <= xmax + vx * f32(0.05) * 1.0001
+    # with no particle left in the box the next step reports the empty domain
+    # (GFSPH_ERR_DOMAIN, as the device does) and changes nothing
+    with pytest.raises(RuntimeError, match="-8"):
+        oracle_mod.run(2, p, nx, ny, d, d, st, 5)
+    assert st.flag[0] == 1 and np.array_equal(st.x[0], x_out)
