@@ -11,6 +11,9 @@ module gfsph_c
 
   integer(c_int), parameter :: GFSPH_NCONST = 110, GFSPH_NTOPO = 16
   integer(c_int), parameter :: GFSPH_OK = 0, GFSPH_T_END_REACHED = 1
+  integer(c_int), parameter :: GFSPH_ERR_ARG = -1, GFSPH_ERR_CUDA = -2, GFSPH_ERR_CAPACITY = -3, &
+                               GFSPH_ERR_UNSUPPORTED = -4, GFSPH_ERR_STATE = -5, GFSPH_ERR_NO_DEVICE = -6, &
+                               GFSPH_ERR_NONFINITE = -7, GFSPH_ERR_DOMAIN = -8, GFSPH_ERR_HOST = -9
   integer(c_int), parameter :: GFSPH_RASTER_DEPTH_IDW = 0, GFSPH_RASTER_MAX_DEPTH = 1, &
                                GFSPH_RASTER_MAX_VEL = 2, GFSPH_RASTER_SUM_DEPTH = 3, &
                                GFSPH_RASTER_SUM_VEL = 4, GFSPH_RASTER_COUNT = 5, &

@@ -76,9 +76,19 @@ def test_no_cpu_fallback_without_device(gfsph_lib):
 def test_fortran_interface_names_every_symbol():
     src = open(os.path.join(ROOT, "deslizamientos-y-flujos_b200", "fortran", "gfsph_c.f90")).read().lower()
     for s in declared_symbols():
-        if s in ("gfsph_set_stream",):
-            continue
         assert f'bind(c, name="{s}")' in src, s
+
+
+def test_fortran_module_names_every_status_code():
+    """GFSPH_OK .. GFSPH_ERR_* of the header, each with the header's value."""
+    hdr = open(os.path.join(ROOT, "include", "gfsph.h")).read()
+    codes = {m.group(1): int(m.group(2)) for m in
+             re.finditer(r"#define (GFSPH_(?:OK|T_END_REACHED|ERR_[A-Z_]+))\s+\(?(-?\d+)\)?", hdr)}
+    assert len(codes) >= 11
+    f90 = open(os.path.join(ROOT, "deslizamientos-y-flujos_b200", "fortran", "gfsph_c.f90")).read()
+    for name, value in codes.items():
+        m = re.search(rf"\b{name}\s*=\s*(-?\d+)", f90)
+        assert m and int(m.group(1)) == value, name
 
 
 def _c_declarations():
