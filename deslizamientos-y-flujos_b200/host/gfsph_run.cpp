@@ -175,9 +175,11 @@ int main(int argc, char** argv) {
         while (tnow < (double)m.time_end && (max_steps < 0 || total < max_steps)) {
             int budget = (max_steps < 0) ? 1000000000 : (int)std::min<long long>(max_steps - total, 1000000000LL);
             int done = 0;
-            int st = check(gfsph_step(hd, budget, tnow + time_plot, &tnow, &done), "gfsph_step");
+            int st = gfsph_step(hd, budget, tnow + time_plot, &tnow, &done);
+            // every particle has left the DEM: the run ends with this plot time
+            const bool all_left = (st == GFSPH_ERR_DOMAIN);
+            if (!all_left) check(st, "gfsph_step");
             total += done;
-            (void)st;
             check(gfsph_download(hd, rx.data(), rv.data(), rh.data(), rm.data(), rs.data(), rf.data()), "gfsph_download");
             check(gfsph_hazard_sample(hd), "gfsph_hazard_sample");
             double vol = 0.0, hmax = 0.0, vmax = 0.0;
@@ -196,6 +198,10 @@ int main(int argc, char** argv) {
             std::snprintf(name, sizeof(name), ".depth_%04d.asc", iplot);
             write_asc(join(out, problem + name), t, raster);
             iplot++;
+            if (all_left) {
+                std::printf("gfsph_run: every particle has left the DEM at t = %.4f s\n", tnow);
+                break;
+            }
         }
         check(gfsph_raster(hd, GFSPH_RASTER_MAX_DEPTH, raster.data()), "gfsph_raster");
         write_asc(join(out, problem + ".max_depth.asc"), t, raster);

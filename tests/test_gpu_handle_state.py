@@ -81,3 +81,39 @@ def test_adjoint_refuses_a_resized_handle(gfsph_lib):
     assert status_of(adj.backward, g, g) == ERR_STATE
     adj.close()
     sim.close()
+
+
+def test_every_particle_leaving_the_dem_ends_the_run(gfsph_lib, oracle_mod):
+    """A patch launched across the +x edge of a flat, frictionless 95 m box:
+    the first step that starts with no particle inside returns
+    GFSPH_ERR_DOMAIN (-8), the time stops there, as the oracle's does (to
+    one step: a particle's exit could flip by one step at the edge), and the
+    state stays readable with every particle flagged."""
+    nx = ny = 20
+    d = 5.0
+    g = np.arange(8) * 1.0 + 80.0
+    X, Y = np.meshgrid(g, g - 40.0)  # x 80-87 m, y 40-47 m
+    x = np.stack([X.ravel(), Y.ravel()], 1).astype(np.float32)
+    n = x.shape[0]
+    v = np.tile(np.float32([20.0, 0.0]), (n, 1))
+    rho = np.full(n, 1.0, np.float32)
+    mass = np.full(n, 1.0, np.float32)
+    hsml = np.full(n, 1.3, np.float32)
+    z = np.zeros((ny, nx), np.float32)
+    p = gfsph.make_params({1: 9.8, 2: 2000.0, 3: 1e30, 5: 5, 9: 0.0, 10: 0.01, 15: 0.01},
+                          sle=0, dt=0.01, ic_adapt=0, average_velocity=0)
+    sim = gfsph.Sim(p, z, dx=d, dy=d)
+    sim.upload(x, v, rho, mass, hsml)
+    assert status_of(sim.step, 400) == -8
+    t_gpu, _ = sim.time()
+    out = sim.download()
+    sim.close()
+    assert np.all(out["flag"] == 1)
+    topol = oracle_mod.initial_topol(z.astype(np.float64), d, d, {}, deriv=1, mode=oracle_mod.MODE_FP32_DACC)
+    st = oracle_mod.State(x, v, rho, mass, hsml, topol, dt=0.01)
+    run = oracle_mod.Run(oracle_mod.MODE_FP32_DACC, p, nx, ny, d, d, st)
+    done = run.advance(400)
+    t_ref = run.state().t
+    run.close()
+    assert 0 < done < 400
+    assert abs(t_gpu - t_ref) <= 0.0101, (t_gpu, t_ref)
