@@ -114,6 +114,14 @@ MasterDat read_master(const std::string& path) {
     return m;
 }
 
+// A grid of nx x ny DEM nodes that the library takes (3 x 3 nodes or more)
+// and whose node count fits an int; nx, ny as read (checked before the cast).
+static void check_grid(double nx, double ny, const std::string& path) {
+    if (!(nx >= 3.0 && ny >= 3.0 && nx * ny <= 2147483647.0))
+        throw std::runtime_error(path + ": a DEM grid of " + std::to_string(nx) + " x " + std::to_string(ny) +
+                                 " nodes is outside 3 x 3 .. 2^31 - 1 nodes");
+}
+
 // Topo_main (SPH_FEM_topo_2019.f90:208-260) with Get_DTM (:1155-1445).
 TopoData read_top(const std::string& path) {
     FortranReader r(path);
@@ -124,6 +132,7 @@ TopoData read_top(const std::string& path) {
     if (t.ictop == 0) {
         r.label();
         auto v = r.values(2);
+        check_grid(to_real(v[0], path), to_real(v[1], path), path);
         t.nx = (int)to_real(v[0], path);
         t.ny = (int)to_real(v[1], path);
         r.label();
@@ -149,8 +158,13 @@ TopoData read_top(const std::string& path) {
         throw std::runtime_error(path + ": ictop " + std::to_string(t.ictop) + " is not supported (0, 10, 11, 15, 16 are)");
     r.label();
     auto v = r.values(2);
-    int np_dtm = (int)to_real(v[0], path);
+    const float np_read = to_real(v[0], path);
     float deltx = to_real(v[1], path);
+    if (!(np_read >= 1.f && np_read <= 2147483647.f))
+        throw std::runtime_error(path + ": the DTM point count " + std::to_string(np_read) + " is out of range");
+    if (!(deltx > 0.f) || !std::isfinite(deltx))
+        throw std::runtime_error(path + ": the DTM lattice spacing must be positive");
+    int np_dtm = (int)np_read;
     float xw0 = 0.f, xw1 = 0.f, yw0 = 0.f, yw1 = 0.f;
     if (t.ictop == 15 || t.ictop == 16) {
         r.label();
@@ -169,6 +183,7 @@ TopoData read_top(const std::string& path) {
         if (py[k] >= ymaxg) ymaxg = py[k];
         if (pz[k] >= zmaxg) zmaxg = pz[k];
     }
+    check_grid((double)((xmaxg - xming) / deltx + 1.f), (double)((ymaxg - yming) / deltx + 1.f), path);
     int nx = (int)((xmaxg - xming) / deltx + 1.f);
     int ny = (int)((ymaxg - yming) / deltx + 1.f);
     float dxg = (xmaxg - xming) / (float)(nx - 1);
@@ -232,6 +247,8 @@ SwDat read_dat(const std::string& path) {
     d.n_hist = r.read_int();
     r.label();
     d.ndimn = r.read_int();
+    if (d.ndimn != 2)
+        throw std::runtime_error(path + ": ndimn " + std::to_string(d.ndimn) + " is not supported (the depth-integrated model is 2-D)");
     r.label();
     auto v = r.values(4);
     d.ic_soil = (int)to_real(v[0], path); d.ic_water = (int)to_real(v[1], path);

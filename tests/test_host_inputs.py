@@ -62,3 +62,51 @@ def test_written_inputs_with_pore_pressure_parse(gfsph_lib, tmp_path):
     workloads.write_reference_inputs(w, str(tmp_path), "pw")
     meta = parse("pw", str(tmp_path))
     assert meta["icpwp"] == 3 and abs(meta["pwp0rel"] - 0.75) < 1e-7
+
+
+def _damage(ext, how):
+    def f(name, text):
+        if not name.endswith(ext):
+            return text
+        if how == "missing":
+            return None
+        if how == "empty":
+            return ""
+        if how == "half":
+            return text[: len(text) // 2]
+        if how == "junk":
+            return text.replace("0", "x")
+        return how(text)
+    return f
+
+
+DAMAGE = [
+    (ext, how) for ext in (".MASTER.dat", "plane.dat", ".top", ".pts") for how in ("missing", "empty", "half", "junk")
+] + [
+    (".top", lambda t: t.replace("200 400", "0 0", 1)),
+    (".top", lambda t: t.replace("200 400", "-5 400", 1)),
+    (".top", lambda t: t.replace("200 400", "2000000000 2000000000", 1)),
+    ("plane.dat", lambda t: t.replace("ndimn\n  2", "ndimn\n  3", 1)),
+    (".pts", lambda t: t.replace("1941 2 2 2 2", "1941 2 0 0 2", 1)),
+]
+
+
+@pytest.mark.parametrize("ext,how", DAMAGE)
+def test_damaged_inputs_are_refused_with_a_message(gfsph_lib, tmp_path, ext, how):
+    """A missing, empty, truncated or garbled input file, or a DEM grid, a
+    dimension or a lattice outside what the step takes, ends the driver with
+    status 2 and a message naming the file: never a crash or a silent run."""
+    w = workloads.inclined_plane()
+    src = tmp_path / "src"
+    src.mkdir()
+    workloads.write_reference_inputs(w, str(src), "plane")
+    dst = tmp_path / "dst"
+    dst.mkdir()
+    mutate = _damage(ext, how)
+    for name in os.listdir(src):
+        text = mutate(name, (src / name).read_text())
+        if text is not None:
+            (dst / name).write_text(text)
+    out = subprocess.run([RUN, "plane", "--dir", str(dst), "--parse-only"], capture_output=True, text=True)
+    assert out.returncode == 2, (out.returncode, out.stderr)
+    assert "plane" in out.stderr
