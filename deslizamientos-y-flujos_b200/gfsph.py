@@ -459,6 +459,8 @@ class Adjoint:
     def backward(self, gx, gv, gh=None):
         """dL/dx, dL/dv (n, 2) and dL/dh (n,) of the final state -> dict of
         dL/dx0, dL/dv0, dL/dmass, dL/dtanfi (const(9)), dL/dxi (const(3))."""
+        if not self.h or not self.sim.h:  # the record steps its handle, which must still exist
+            raise GfsphError(-5, "gfsph_adjoint_backward")
         n = self.sim.n
         gx = np.ascontiguousarray(gx, np.float32)
         gv = np.ascontiguousarray(gv, np.float32)

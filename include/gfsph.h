@@ -270,6 +270,10 @@ int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_
  * Supported: nfric 5/6 with xi >= 0, no erosion or pore pressure, pa_sph 2,
  * sle 0, ic_adapt 0, one grid level (uniform smoothing lengths) and no
  * particle leaving the DEM (GFSPH_ERR_UNSUPPORTED otherwise).
+ *
+ * The record refers to its handle: call gfsph_adjoint_backward only while
+ * that handle exists (gfsph_adjoint_destroy does not touch it, so the record
+ * may be destroyed before or after the handle).
  */
 typedef struct gfsph_adjoint gfsph_adjoint;
 int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint** out);
@@ -284,7 +288,9 @@ int gfsph_adjoint_destroy(gfsph_adjoint* a);
  * and xi = const(3)) and particles, advanced together: every member's graph
  * launches go out on its own stream before any wait, so small realizations
  * share the GPU.  Each member is an ordinary handle (gfsph_ensemble_member)
- * for upload, download and rasters; its DEM copy erodes independently.
+ * for upload, download and rasters; its DEM copy erodes independently.  The
+ * ensemble owns its members: gfsph_ensemble_destroy frees them, and a
+ * member must not be passed to gfsph_destroy.
  */
 typedef struct gfsph_ensemble gfsph_ensemble;
 int gfsph_ensemble_create(const gfsph_params* params /* nreal entries */, const gfsph_dem* dem, int nreal,

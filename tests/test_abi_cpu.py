@@ -122,3 +122,17 @@ def test_fortran_module_binds_every_entry_point():
     assert sorted(set(c) - set(f)) == []
     for name, nargs in c.items():
         assert f[name] == nargs, (name, nargs, f[name])
+
+
+def test_adjoint_record_refuses_a_closed_sim(gfsph_lib):
+    """The record steps its handle: once the Sim is closed the binding refuses
+    the backward pass (GFSPH_ERR_STATE) instead of passing a freed handle."""
+    class ClosedSim:
+        h = None
+        n = 4
+    adj = gfsph_lib.Adjoint.__new__(gfsph_lib.Adjoint)
+    adj.sim, adj.h = ClosedSim(), None
+    g = np.zeros((4, 2), np.float32)
+    with pytest.raises(gfsph_lib.GfsphError) as e:
+        adj.backward(g, g)
+    assert e.value.status == -5
