@@ -516,8 +516,15 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
     h->capturing = true;
     for (int s = 0; s < steps; s++) enqueue_step(h);
     h->capturing = false;
+    // a launch that failed during the capture (bad configuration) is reported
+    // after the capture has been ended, so the stream leaves capture mode
+    const cudaError_t le = cudaGetLastError();
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->launches = before;  // capture launches nothing
+    if (le != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_status(le);
+    }
     if (e != cudaSuccess) return cuda_status(e);
     e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
@@ -732,6 +739,18 @@ extern "C" int gfsph_dem_topol(int mode, int nx, int ny, float dx, float dy, flo
 extern "C" {
 
 int gfsph_version(void) { return 1; }
+
+int gfsph_binary_version(int* version) try {
+    if (!version) return GFSPH_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return GFSPH_ERR_NO_DEVICE;
+    cudaFuncAttributes a{};
+    CK(cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(&k_prep)));
+    *version = a.binaryVersion;
+    return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
+}
 
 const char* gfsph_strerror(int s) {
     switch (s) {
@@ -1047,6 +1066,7 @@ int enqueue_chunk(gfsph_handle* h, int chunk, double t_end) {
     if (h->profile) {
         for (int s = 0; s < chunk; s++) {
             enqueue_step(h);
+            CK(cudaGetLastError());  // a launch of this step failed
             int st = profile_collect(h);
             if (st) return st;
         }

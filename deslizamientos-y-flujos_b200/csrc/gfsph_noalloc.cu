@@ -10,6 +10,7 @@
 // exits.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/gfsph.h"
@@ -68,7 +69,9 @@ __global__ void k_noalloc_finish(const double2* acc, float* out, int np) {
 }
 
 // Device address of the scratch array on the current device; looked up once
-// per device, on the first call made with that device current.
+// per device, on the first call made with that device current.  The cached
+// address belongs to the device's primary context: it does not survive a
+// cudaDeviceReset (the module is loaded again afterwards).
 int scratch_address(double2** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return GFSPH_ERR_NO_DEVICE;
@@ -90,6 +93,11 @@ extern "C" int gfsph_raster_idw_noalloc(int n, const float* d_x, const float* d_
                                         int ny, float xmin, float ymin, float dx, float dy, float* d_out,
                                         void* stream) try {
     if (n < 0 || (n > 0 && (!d_x || !d_rho)) || !d_out || nx < 2 || ny < 2 || !(dx > 0.f) || !(dy > 0.f))
+        return GFSPH_ERR_ARG;
+    // d_x is read as float2 (interleaved x, y): it must be 8-byte aligned;
+    // the other arrays hold 4-byte elements
+    if ((reinterpret_cast<uintptr_t>(d_x) & 7u) || (reinterpret_cast<uintptr_t>(d_rho) & 3u) ||
+        (reinterpret_cast<uintptr_t>(d_flag) & 3u) || (reinterpret_cast<uintptr_t>(d_out) & 3u))
         return GFSPH_ERR_ARG;
     if ((long long)nx * (long long)ny > (long long)kNoAllocMaxNodes) return GFSPH_ERR_CAPACITY;
     double2* acc = nullptr;

@@ -294,5 +294,9 @@ module gfsph_c
      integer(c_int) function gfsph_version() bind(c, name="gfsph_version")
        import :: c_int
      end function
+     integer(c_int) function gfsph_binary_version(version) bind(c, name="gfsph_binary_version")
+       import :: c_int
+       integer(c_int), intent(out) :: version
+     end function
   end interface
 end module gfsph_c

@@ -110,6 +110,7 @@ SIGNATURES = {
     "gfsph_solvegc2": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _FP, _FP, _FP, _FP, C.c_float, _IP]),
     "gfsph_strerror": (C.c_char_p, [C.c_int]),
     "gfsph_version": (C.c_int, []),
+    "gfsph_binary_version": (C.c_int, [_IP]),
 }
 
 

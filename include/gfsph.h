@@ -339,11 +339,14 @@ int gfsph_solvegc2(int npoin, int nelem, int nnode, int ndofn, const int* intmat
  * framework that owns the allocator).  It has no counterpart in the
  * reference.  Inputs and output are device pointers owned by the caller:
  * d_x (2,n), d_rho (n), d_flag (n, may be NULL = all inside), d_out (nx*ny).
+ * d_x is read as interleaved (x, y) pairs and must be 8-byte aligned, the
+ * other arrays 4-byte aligned (GFSPH_ERR_ARG otherwise).
  * The per-node accumulators live in a fixed device array of
  * GFSPH_NOALLOC_MAX_NODES nodes (16 MiB, held by every GPU that loads the
  * library until exit); larger grids are rejected with GFSPH_ERR_CAPACITY.
  * The first call on a device looks up that array's device address (make it
- * before any stream capture).  Every call shares the array: calls that
+ * before any stream capture); the address is kept for the life of the
+ * process, so after a cudaDeviceReset this entry point must not be used.  Every call shares the array: calls that
  * overlap on the GPU race.  The work is enqueued on `stream`
  * (cudaStream_t, NULL = default stream) and nothing is allocated or freed. */
 #define GFSPH_NOALLOC_MAX_NODES (1 << 20)
@@ -352,6 +355,12 @@ int gfsph_raster_idw_noalloc(int n, const float* d_x, const float* d_rho, const 
 
 const char* gfsph_strerror(int status);
 int gfsph_version(void);
+
+/* The architecture the library's kernels were built for, as the CUDA runtime
+ * reports it for a loaded kernel (cudaFuncGetAttributes binaryVersion,
+ * major * 10 + minor: 100 for sm_100a).  Needs a device.  No counterpart in
+ * the reference. */
+int gfsph_binary_version(int* version);
 
 #ifdef __cplusplus
 }

@@ -117,3 +117,4 @@ def test_every_particle_leaving_the_dem_ends_the_run(gfsph_lib, oracle_mod):
     run.close()
     assert 0 < done < 400
     assert abs(t_gpu - t_ref) <= 0.0101, (t_gpu, t_ref)
+

@@ -60,3 +60,11 @@ def test_gfsph_run_with_basal_pore_pressure(gfsph_lib, tmp_path):
         assert out.returncode == 0, out.stderr
         speeds[icpwp] = np.loadtxt(os.path.join(d, "plane.gfsph.log"))[-1, 5]
     assert speeds[3] > 1.2 * speeds[0]
+
+
+def test_kernels_report_sm100(gfsph_lib):
+    """The runtime reports the loaded kernels as built for compute capability 10.0."""
+    import ctypes as C
+    v = C.c_int(0)
+    assert gfsph_lib.lib().gfsph_binary_version(C.byref(v)) == 0
+    assert v.value == 100

@@ -37,19 +37,38 @@ def test_noalloc_raster_matches_the_handle_raster(gfsph_lib, oracle_mod):
     L = gfsph.lib()
     stream = torch.cuda.current_stream().cuda_stream
     tol = 1e-5 * max(float(ref.max()), 1.0)  # the tolerance of the handle raster against the oracle
-    for _ in range(2):  # the second call must not see the first call's sums
-        st = L.gfsph_raster_idw_noalloc(w.n, C.c_void_p(x.data_ptr()), C.c_void_p(rho.data_ptr()),
-                                        C.c_void_p(flag.data_ptr()), nx, ny, 0.0, 0.0, w.dx, w.dy,
+
+    def call(depth, flags):
+        st = L.gfsph_raster_idw_noalloc(w.n, C.c_void_p(x.data_ptr()), C.c_void_p(depth.data_ptr()),
+                                        C.c_void_p(flags.data_ptr()), nx, ny, 0.0, 0.0, w.dx, w.dy,
                                         C.c_void_p(out.data_ptr()), C.c_void_p(stream))
         assert st == 0, gfsph.strerror(st)
         torch.cuda.synchronize()
-        got = out.cpu().numpy()
+        return out.cpu().numpy()
+
+    # Every call must start from cleared accumulators, and the calls differ in
+    # their inputs so that sums left over from the call before would show: after
+    # a call with every depth x7, a call with every particle flagged must give
+    # zeros (not the x7 raster), and the real call must give the handle raster
+    # (stale sums would give (7h + h)/2 = 4h at every node).
+    got = call(rho * 7.0, flag)
+    assert np.abs(got - 7.0 * ref).max() <= 7.0 * tol
+    got = call(rho, torch.ones_like(flag))
+    assert np.all(got == 0.0)
+    for _ in range(2):  # then the real call twice in a row
+        got = call(rho, flag)
         assert np.abs(got - ref).max() <= tol
         assert got.max() > 0
+    # a misaligned position array is refused, not read
+    xb = torch.zeros(2 * w.n + 1, dtype=torch.float32, device=dev)
+    st = L.gfsph_raster_idw_noalloc(w.n, C.c_void_p(xb.data_ptr() + 4), C.c_void_p(rho.data_ptr()),
+                                    C.c_void_p(flag.data_ptr()), nx, ny, 0.0, 0.0, w.dx, w.dy,
+                                    C.c_void_p(out.data_ptr()), C.c_void_p(stream))
+    assert st == -1
 
 
 def test_noalloc_raster_rejects_grids_above_its_fixed_size(gfsph_lib):
     L = gfsph.lib()
     big = 2048  # 2048 x 2048 nodes > 2^20
-    st = L.gfsph_raster_idw_noalloc(0, None, None, None, big, big, 0.0, 0.0, 1.0, 1.0, C.c_void_p(1), None)
+    st = L.gfsph_raster_idw_noalloc(0, None, None, None, big, big, 0.0, 0.0, 1.0, 1.0, C.c_void_p(256), None)
     assert st == -3
