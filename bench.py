@@ -30,19 +30,23 @@ import numpy as np  # noqa: E402
 
 METRIC = "SPH particle-steps/s"
 UNIT = "particle-steps/s"
-B_ALG = {"k_density": 24, "k_force_rk": 72, "k_xsph": 44, "k_hist": 28}  # bytes per particle and launch
-# From ncu on the fractal-channel workload (200,011 particles): warp
-# instructions per launch averaged over every launch of the 300 timed steps
-# (steps 11-310; the neighbour work grows as the flow spreads:
-# profiles/neighbour_kernels_fractal_channel_200k.md), and DRAM read + write
-# bytes per launch from one --set full capture of step 9; both per particle.
-NCU_PER_PARTICLE = {
-    "k_density": {"dram_bytes": (4.835328e6 + 1.737984e6) / 200011, "warp_inst": 80.09e6 / 200011},
-    "k_iforce": {"dram_bytes": (43.911680e6 + 0.100352e6) / 200011, "warp_inst": 42.43e6 / 200011},
-    "k_force_rk": {"dram_bytes": 8.113920e6 / 200011, "warp_inst": 21.54e6 / 200011},
-    "k_xsph": {"dram_bytes": (46.309120e6 + 0.197632e6) / 200011, "warp_inst": 36.52e6 / 200011},
-}
-NCU_SOURCE = "profiles/neighbour_kernels_fractal_channel_200k.md (ncu, cold caches), scaled by active particles"
+# Algorithmic bytes per particle and launch: the compulsory traffic of each
+# pass, 168 B per particle-step in all (bin 28, density 24, force + RK4 +
+# h-update 72, av_vel 44).  The force pass runs as two kernels: k_iforce reads
+# x, y, hsml, m, h and the neighbour count (24 B); k_force_rk reads v and the
+# flag (12 B) and writes x, y, v, hsml, flag and the step-start copies (36 B).
+# The internal acceleration handed between them (8 B written, 8 B read) is an
+# artefact of the split and is not counted.
+B_ALG = {"k_density": 24, "k_iforce": 24, "k_force_rk": 48, "k_xsph": 44, "k_hist": 28}
+# From ncu on this workload (200,011 particles), per particle: DRAM read +
+# write bytes per launch and warp instructions per launch, averaged over the
+# launches of NCU_STEPS (the steps the driver's default run times:
+# `bench.py --steps 20 --warmup 5`).  The issue-bound figure is printed only
+# when the run times those same steps, since the neighbour work per step grows
+# as the flow spreads.
+NCU_STEPS = None  # (first, last) step of the capture; None: no capture of the current kernels yet
+NCU_PER_PARTICLE = {}
+NCU_SOURCE = "profiles/ (ncu, cold caches), scaled by active particles"
 ISSUE_PEAK = 148 * 4 * 1.965e9  # warp instructions/s: SMs x schedulers x max SM clock
 
 
@@ -128,12 +132,14 @@ def dist_setup(n_gpus):
     return rank, world, local
 
 
-def _oracle_case(n_target=20_000):
+def _oracle_case(n_target, seed=2):
+    """The benchmark workload (the same release the GPU arm runs) as an
+    oracle state."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import gfsph
     import oracle
     import workloads
-    w = workloads.fractal_channel(n_target=n_target)
+    w = workloads.fractal_channel(n_target=n_target, seed=seed)
     p = workloads.make_params(w, gfsph)
     topol = oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv)
     ny, nx = w.z.shape
@@ -141,71 +147,91 @@ def _oracle_case(n_target=20_000):
     return oracle, w, p, nx, ny, st
 
 
-def cpu_reference_rate(seconds_budget, warm_steps=20, omp=False, steps=None):
-    """The reference path on the host (the FP32 oracle port) on a bounded
-    sample of the workload: the same DEM and physics with a 20k-particle
-    release, timed over the same early phase of the flow as the GPU
-    measurement.  One thread (the reference is single-threaded), or with
-    omp=True the OpenMP build of the port on every host core this process
-    may use; steps fixes the timed steps (else the budget sets them).
-    Returns (particle-steps/s, steps, n, seconds, threads, sample)."""
-    oracle, w, p, nx, ny, st = _oracle_case()
-    run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st, omp=omp)
-    threads = run.threads
+def _warm_state(oracle, w, p, nx, ny, st, warm_steps):
+    """The reference FP32 state after the GPU arm's warm-up steps (serial
+    oracle, mode 0), so that the CPU legs time the same steps of the flow."""
+    run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st)
     run.advance(warm_steps)
-    t0 = time.perf_counter()
-    run.advance(1)
-    one = max(time.perf_counter() - t0, 1e-4)
-    if steps is None:
-        steps = max(1, min(400, int(seconds_budget / one)))
-    t0 = time.perf_counter()
-    run.advance(steps)
-    el = time.perf_counter() - t0
+    snap = run.state(with_topol=True)
     run.close()
-    how = f"OpenMP build, {threads} host threads" if omp else "1 host thread"
-    desc = (f"steps {warm_steps + 2}..{warm_steps + 1 + steps} of the fractal-channel workload with a "
-            f"{w.n}-particle release (same DEM and physics), FP32 oracle port, {how}")
-    return w.n * steps / el, steps, w.n, el, threads, desc
+    return snap
 
 
-def run_reference_arm(args, rank, world):
-    """The reference's CPU path (the FP32 oracle port: the Fortran reference
-    cannot be built here), one host thread.  Each bench step is a bounded
-    sample of oracle steps, restarted from the same early-flow state, so the
-    whole run stays within a few minutes."""
-    if rank != 0:
-        return 0
-    oracle, w, p, nx, ny, st = _oracle_case()
-    warm = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st)
-    warm.advance(20)
-    snap = warm.state(with_topol=True)
-    warm.close()
+def cpu_reference_rate(n_target, warm_steps, seconds_budget):
+    """The reference path on the host (the FP32 oracle port) on the benchmark
+    workload itself: the same ~200k-particle release, from the state after the
+    GPU arm's warm-up steps, over as many of the following steps as fit the
+    time budget.  One host thread (the reference is single-threaded), then the
+    OpenMP build of the port over the same steps on every host core this
+    process may use.  Returns the cpu_baseline object."""
+    oracle, w, p, nx, ny, st = _oracle_case(n_target)
+    snap = _warm_state(oracle, w, p, nx, ny, st, warm_steps)
     run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, snap)
     t0 = time.perf_counter()
     run.advance(1)
     one = max(time.perf_counter() - t0, 1e-4)
     run.close()
-    per = max(1, min(100, int(120.0 / max(args.steps + args.warmup, 1) / one)))
-    total_steps = 0
-    el = 0.0
-    for k in range(args.warmup + args.steps):
-        run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, snap)
+    steps = max(1, min(400, int(seconds_budget / one)))
+
+    def timed(omp):
+        r = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, snap, omp=omp)
         t0 = time.perf_counter()
-        run.advance(per)
-        dt_ = time.perf_counter() - t0
-        run.close()
-        if k >= args.warmup:
-            el += dt_
-            total_steps += per
-    value = w.n * total_steps / el
-    desc = (f"{per} oracle steps per bench step from the state after 20 steps of the fractal-channel workload "
-            f"with a {w.n}-particle release (same DEM and physics), FP32, 1 host thread")
+        r.advance(steps)
+        el = time.perf_counter() - t0
+        threads = r.threads
+        r.close()
+        return w.n * steps / el, threads
+
+    where = (f"steps {warm_steps + 1}..{warm_steps + steps} of the benchmark workload itself ({w.n} particles, "
+             f"the GPU arm's release), FP32 oracle port")
+    rate, _ = timed(False)
+    cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "sample": where + ", 1 host thread"}
+    if oracle.omp_available():
+        try:
+            rate, threads = timed(True)
+            cpu["openmp"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": where + f", OpenMP build, {threads} host threads"}
+        except (OSError, RuntimeError) as e:
+            cpu["openmp"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    else:
+        cpu["openmp"] = {"unavailable": "the OpenMP build of the oracle was not made (no -fopenmp compiler)"}
+    return cpu
+
+
+def bench_config(n, w):
+    """The `config` object both arms print: the same workload and steps."""
+    return {"workload": "fractal_channel: 1024^2 DEM at 5 m, ~200k-particle elliptical release, "
+                        "Voellmy + Hungr erosion, adaptive dt",
+            "n_particles": n, "dem": w.meta["dem"], "lattice_m": round(w.meta["lattice"], 4),
+            "timed_steps": "the K steps after the W warm-up steps of the flow, in both arms",
+            "l2": "GPU arm: flushed before every timed step (256 MiB write)",
+            "parallelism": "one GPU, or one host thread in the reference arm"}
+
+
+def run_reference_arm(args, rank, world):
+    """The reference's CPU path (the FP32 oracle port: the Fortran reference
+    cannot be built here) on the GPU arm's workload: the same ~200k-particle
+    release, W untimed warm-up steps, then K timed steps, one oracle step per
+    bench step, on one host thread (the reference is single-threaded)."""
+    if rank != 0:
+        return 0
+    oracle, w, p, nx, ny, st = _oracle_case(args.n)
+    run = oracle.Run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st)
+    run.advance(args.warmup)
+    el = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run.advance(1)
+        el += time.perf_counter() - t0
+    run.close()
+    value = w.n * args.steps / el
+    desc = (f"steps {args.warmup + 1}..{args.warmup + args.steps} of the benchmark workload itself ({w.n} "
+            f"particles), FP32 oracle port (mode 0, the reference's FP32 scheme), 1 host thread")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "fractal_channel: 1024^2 DEM at 5 m, elliptical release (bounded sample)",
-                   "parallelism": "single host thread (the reference is single-threaded)"},
+        "config": bench_config(w.n, w),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -426,6 +452,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    # The clock sampler (200 ms period) runs from the warm-up through the
+    # timed steps and their two replays below, so that the timed region,
+    # a few ms long, is bracketed by samples taken under the same load.
+    clk = ClockSampler(local).__enter__()
     # warm-up (graph capture, capacity growth)
     for _ in range(args.warmup):
         sim.step(1)
@@ -434,15 +464,13 @@ def main():
     sim.profile(2)
     l0 = sim.launch_count()
     barrier()
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            sim.step(1)
-        barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        sim.step(1)
+    barrier()
     launches = sim.launch_count() - l0
     ms_local, nsteps = sim.profile_read().get("step_batches", (0.0, 0))
     ms_total, n_job, value = combine_ranks(ms_local, n, args.steps, dist, "cuda")
-    clocks = clk.summary()
 
     # The passes below replay the timed steps (warm-up + 1 .. warm-up + K) on a
     # fresh handle from the same release: the run is deterministic, and the
@@ -474,6 +502,10 @@ def main():
         s2.step(1)
     kprof = s2.profile_read()
     s2.close()
+    torch.cuda.synchronize()
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
+    clocks["window"] = "warm-up, timed steps and their two replays"
     tot = sum(ms for ms, _ in kprof.values())
     dom = max(kprof, key=lambda k: kprof[k][0])
     dom_ms = kprof[dom][0] / kprof[dom][1]
@@ -485,6 +517,12 @@ def main():
     b_launch = B_ALG.get(dom, 0) * nact
     achieved = b_launch / (dom_ms / 1000.0) / 1e9
     shares = {k: round(ms / tot, 4) for k, (ms, _) in sorted(kprof.items(), key=lambda kv: -kv[1][0])}
+    issue = None
+    if dom in NCU_PER_PARTICLE and NCU_STEPS == (args.warmup + 1, args.warmup + args.steps):
+        wi = NCU_PER_PARTICLE[dom]["warp_inst"] * nact
+        issue = {"warp_inst_per_launch": wi, "achieved_warp_inst_per_s": wi / (dom_ms / 1000.0),
+                 "peak_warp_inst_per_s": ISSUE_PEAK, "frac": wi / (dom_ms / 1000.0) / ISSUE_PEAK,
+                 "ncu_steps": list(NCU_STEPS)}
 
     # ---- e2e through the C ABI with pinned host buffers
     pin = {k: torch.empty(a.shape, dtype=torch.float32 if a.dtype == np.float32 else torch.int32,
@@ -522,41 +560,19 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, steps, nc, el, _, desc = cpu_reference_rate(args.cpu_seconds)
-        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "sample": desc}
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle
-        if oracle.omp_available():
-            try:
-                # the same steps as the single-thread sample
-                rate, steps, nc, el, threads, desc = cpu_reference_rate(args.cpu_seconds, omp=True, steps=steps)
-                cpu["openmp"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
-            except (OSError, RuntimeError) as e:
-                cpu["openmp"] = {"unavailable": f"{type(e).__name__}: {e}"}
-        else:
-            cpu["openmp"] = {"unavailable": "the OpenMP build of the oracle was not made (no -fopenmp compiler)"}
+        cpu = cpu_reference_rate(args.n, args.warmup, args.cpu_seconds)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "fractal_channel: 1024^2 DEM at 5 m, ~200k-particle elliptical release, "
-                                   "Voellmy + Hungr erosion, adaptive dt",
-                       "n_particles": n, "dem": w.meta["dem"], "lattice_m": round(w.meta["lattice"], 4),
-                       "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "config": {**bench_config(n, w), **({"parallelism": "replicas, one per GPU"} if world > 1 else {})},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": (NCU_PER_PARTICLE[dom]["dram_bytes"] * nact) if dom in NCU_PER_PARTICLE else None,
                          "traffic_source": NCU_SOURCE,
-                         "issue_bound": ({"warp_inst_per_launch": NCU_PER_PARTICLE[dom]["warp_inst"] * nact,
-                                          "achieved_warp_inst_per_s":
-                                              NCU_PER_PARTICLE[dom]["warp_inst"] * nact / (dom_ms / 1000.0),
-                                          "peak_warp_inst_per_s": ISSUE_PEAK,
-                                          "frac": NCU_PER_PARTICLE[dom]["warp_inst"] * nact / (dom_ms / 1000.0)
-                                          / ISSUE_PEAK}
-                                         if dom in NCU_PER_PARTICLE else None),
+                         "issue_bound": issue,
                          "alg_bytes_per_launch": b_launch, "avg_launch_ms": dom_ms,
                          "step_achieved_gbs": 168 * n * args.steps / (ms_total / 1000.0) / 1e9 / world},
             "kernel_shares": shares,

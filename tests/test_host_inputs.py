@@ -11,7 +11,7 @@ import workloads
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 RUN = os.path.join(ROOT, "deslizamientos-y-flujos_b200", "gfsph_run")
-PICACHO = "/root/reference/EJEMPLOS/Picacho Landslide/Input files"
+GOLDEN = os.path.join(ROOT, "tests", "golden", "picacho")
 
 
 def parse(name, directory):
@@ -35,9 +35,17 @@ def test_written_inputs_read_back(gfsph_lib, tmp_path):
     assert r["z_mean"] == pytest.approx(float(w.z.astype(np.float64).mean()), rel=1e-5)
 
 
-@pytest.mark.skipif(not os.path.isdir(PICACHO), reason="reference example not available")
-def test_picacho_example_reads(gfsph_lib):
-    r = parse("Picacho", PICACHO)
+def picacho_inputs(directory):
+    """The reference's Picacho example inputs (tests/golden/picacho) in `directory`."""
+    import sys
+    if GOLDEN not in sys.path:
+        sys.path.insert(0, GOLDEN)
+    import make_fixture
+    return make_fixture.extract(str(directory))
+
+
+def test_picacho_example_reads(gfsph_lib, tmp_path):
+    r = parse("Picacho", picacho_inputs(tmp_path))
     assert (r["nx"], r["ny"], r["dx"]) == (442, 291, 10.0)
     assert r["ictop"] == 10 and r["fdiff"] == 0
     assert (r["nnps"], r["skf"], r["nfric"], r["icpwp"]) == (4, 1, 7, 3)
