@@ -1,10 +1,12 @@
 // Reverse-mode (adjoint) kernels of one SPH step, for gradients of a loss on
 // the final state with respect to the rheology (tanfi = const(9), xi =
-// const(3)), the particle volumes and the initial positions and velocities.
+// const(3), the Bingham yield stress const(6)), the particle volumes and the
+// initial positions and velocities.
 //
-// Scope: frictional basal friction (nfric 5/6) with Voellmy xi >= 0, no
-// curvature, erosion or pore pressure, pa_sph 2, fixed hsml (sle 0), fixed dt,
-// all particles regular (no coarse level) and inside the DEM.  The step is differentiated
+// Scope: frictional basal friction (nfric 5/6) with Voellmy xi >= 0 or the
+// Bingham law (nfric 4), no curvature, erosion or pore pressure, pa_sph 2,
+// fixed hsml (sle 0), fixed dt, all particles regular (no coarse level) and
+// inside the DEM.  The step is differentiated
 // with its neighbour list held fixed (the reference freezes its pair list per
 // step too); branches (reversal filter, h_inf/comp clamps) take the forward's
 // decisions.  With pa_sph 2 the pressure term p/h^2 = g/2 does not depend on
@@ -69,8 +71,61 @@ __device__ __forceinline__ void dem_slope_jac(const DemView& d, float xx, float 
 // same FP32 code as the forward kernel.
 struct ExtGrad {
     float x, y, vx, vy, hc, in0, in1;
-    double mu, xi;
+    double mu, xi, tauy;
 };
+
+// Vector-Jacobian product of the Bingham friction f = frict / h of
+// basal_friction_Ext_SW (nfric 4, SPH_SW_2019.f90:9552-9572) in its regime at
+// (v, h), for a sliding particle (|h v| >= 1e-5, h >= comp): given lf = dL/df,
+// adds dL/d(vx, vy, hc, tauy).  Regimes: a_hat = 6 K |h v| / (tauy hf^2) with
+// hf = max(h, hfrict0); a_hat > 50: f = (3K/dens) v / hf^2 (viscous);
+// a_hat < 0.01: f = (tauy/dens) vhat / h (plastic); otherwise
+// f = tauy / (dens xh h) vhat, xh the smaller root of
+// 48 x^2 - (32 a_hat + 114) x + 65 = 0.
+__device__ __forceinline__ void bingham_vjp(const Rheo& c, const ExtLocal& L, float vx, float vy, float lf0, float lf1,
+                                            ExtGrad& g) {
+    const float h = L.h;
+    const bool hf_is_h = h > c.hfrict0;
+    // the regime as the forward decides it, in FP32
+    const float hfr = hf_is_h ? h : c.hfrict0;
+    const float a_hat = ((6.f * c.constK) * L.hvmod) / (c.tauy0 * (hfr * hfr));
+    if (a_hat <= 50.f && L.hvmodinv == 0.f) return;  // the forward's friction is 0 here
+    const double hd = h, vm = sqrt((double)vx * vx + (double)vy * vy);
+    const double vh0 = vx / vm, vh1 = vy / vm;
+    const double hf = hfr;
+    const double K = c.constK, ty = c.tauy0, dens = c.dens;
+    const double a = (6.0 * K * hd * vm) / (ty * hf * hf);
+    const double pv = vh0 * lf0 + vh1 * lf1;  // lf . vhat
+    if (a_hat > 50.f) {
+        const double k = (3.0 * K / dens) / (hf * hf);
+        g.vx += (float)(k * lf0);
+        g.vy += (float)(k * lf1);
+        if (hf_is_h) g.hc += (float)(-2.0 * k * ((double)vx * lf0 + (double)vy * lf1) / hd);
+        return;
+    }
+    double F, dF_dv, dF_dh, dF_dty;  // f = F vhat
+    if (a_hat < 0.01f) {
+        F = ty / (dens * hd);
+        dF_dv = 0.0;
+        dF_dh = -F / hd;
+        dF_dty = F / ty;
+    } else {
+        const double B = 32.0 * a + 114.0, sq = sqrt(B * B - 4.0 * 48.0 * 65.0);
+        const double xh = (B - sq) / 96.0;
+        const double dxh_da = (32.0 / 96.0) * (1.0 - B / sq);
+        F = ty / (dens * xh * hd);
+        const double dF_da = -F / xh * dxh_da;
+        const double da_dh = hf_is_h ? -a / hd : a / hd;  // a ~ h/hf^2
+        dF_dv = dF_da * (a / vm);
+        dF_dh = -F / hd + dF_da * da_dh;
+        dF_dty = F / ty + dF_da * (-a / ty);
+    }
+    // d(F vhat)/dv = (F/|v|)(I - vhat vhat^T) + vhat dF/d|v| vhat^T
+    g.vx += (float)((F / vm) * (lf0 - vh0 * pv) + vh0 * dF_dv * pv);
+    g.vy += (float)((F / vm) * (lf1 - vh1 * pv) + vh1 * dF_dv * pv);
+    g.hc += (float)(dF_dh * pv);
+    g.tauy += dF_dty * pv;
+}
 
 __device__ __forceinline__ void ext_vjp(const Rheo& c, const DemView& dem, float dt, float xx, float yy, float vx,
                                         float vy, float hc, float in0, float in1, float lex0, float lex1,
@@ -112,9 +167,12 @@ __device__ __forceinline__ void ext_vjp(const Rheo& c, const DemView& dem, float
         float t0 = (L.cf5 * (lex0 - ah0 * pd)) / an, t1 = (L.cf5 * (lex1 - ah1 * pd)) / an;
         lg0 = lex0 - t0; lg1 = lex1 - t1;
         g.in0 -= t0; g.in1 -= t1;
-        g.mu -= (double)(c.g * pd);
+        if (c.nfric != 4) g.mu -= (double)(c.g * pd);  // a Bingham particle at rest has no friction (cf5 = 0)
     } else if (branch == 4) {
         lg0 = lex0; lg1 = lex1;
+    } else if (c.nfric == 4) {  // sliding under the Bingham law: ex = grav - f
+        lg0 = lex0; lg1 = lex1;
+        bingham_vjp(c, L, vx, vy, -lex0, -lex1, g);
     } else {
         lg0 = lex0; lg1 = lex1;
         const float vm = sqrtf(vx * vx + vy * vy);
@@ -171,24 +229,26 @@ __global__ void __launch_bounds__(128) k_adj_xsph(PState A, Search Q, Rheo c, in
         const int cnt = Q.ncount[k];
         double s = 0.0, a0 = 0.0, a1 = 0.0, dm = 0.0, dh = 0.0, dx0 = 0.0, dx1 = 0.0;
         for (int q = 0; q < cnt; q++) {
-            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride];
+            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride].x;
             const float4 o = Q.xhm[j];
             PairGeom g;
             pair_test(xk, make_float2(o.x, o.y), me.z, o.z, g);
             float w, d0, d1;
             sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+            // the pair terms in FP64: their sums over the neighbours cancel
+            // strongly (antisymmetric in k, j)
             const float2 vj = velfin[j], lj = lv2[j];
-            const float den = hk + A.rho[j], mj = o.w;
-            const float ckj = (2.f * mj * w) / den, cjk = (2.f * mk * w) / den;
-            const float D0 = vj.x - vk.x, D1 = vj.y - vk.y;
-            const float pk = lk.x * D0 + lk.y * D1;   // lambda_k . (v_j - v_k)
-            const float pj = -(lj.x * D0 + lj.y * D1);  // lambda_j . (v_k - v_j)
+            const double den = (double)hk + (double)A.rho[j], mj = o.w, wd = w;
+            const double ckj = (2.0 * mj * wd) / den, cjk = (2.0 * (double)mk * wd) / den;
+            const double D0 = (double)vj.x - vk.x, D1 = (double)vj.y - vk.y;
+            const double pk = lk.x * D0 + lk.y * D1;     // lambda_k . (v_j - v_k)
+            const double pj = -(lj.x * D0 + lj.y * D1);  // lambda_j . (v_k - v_j)
             s += ckj;
             a0 += cjk * lj.x;
             a1 += cjk * lj.y;
-            dm += (2.f * w / den) * pj;
+            dm += (2.0 * wd / den) * pj;
             dh -= (ckj * pk + cjk * pj) / den;
-            const float lw = (2.f * mj / den) * pk + (2.f * mk / den) * pj;
+            const double lw = (2.0 * mj / den) * pk + (2.0 * (double)mk / den) * pj;
             dx0 += lw * d0;
             dx1 += lw * d1;
         }
@@ -207,7 +267,7 @@ __global__ void __launch_bounds__(128) k_adj_rk(PState A, Search Q, const StepSc
                                                 const float2* lx1, const float2* lvp, float* lh, float2* lin,
                                                 double2* lxacc, float2* lv0, double* lpar) {
     const float dt = S->dt_step;
-    double smu = 0.0, sxi = 0.0;
+    double smu = 0.0, sxi = 0.0, sty = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float2 fin = Q.indv[i];
         const float in0 = fin.x, in1 = fin.y;
@@ -228,7 +288,7 @@ __global__ void __launch_bounds__(128) k_adj_rk(PState A, Search Q, const StepSc
         }
         const float2 lx = lx1[i], lv = lvp[i];
         const float dt6 = dt / 6.f;
-        ExtGrad g{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0};
+        ExtGrad g{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0, 0.0};
         float lxs0[4], lxs1[4], lvs0[4], lvs1[4], lex0[4], lex1[4];
 #pragma unroll
         for (int s = 0; s < 4; s++) {
@@ -265,12 +325,15 @@ __global__ void __launch_bounds__(128) k_adj_rk(PState A, Search Q, const StepSc
         if (h >= c.h_inf) lh[i] += g.hc;
         smu += g.mu;
         sxi += g.xi;
+        sty += g.tauy;
     }
     smu = warp_sum(smu);
     sxi = warp_sum(sxi);
+    sty = warp_sum(sty);
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&lpar[0], smu);
         atomicAdd(&lpar[1], sxi);
+        atomicAdd(&lpar[2], sty);
     }
 }
 
@@ -287,26 +350,28 @@ __global__ void __launch_bounds__(128) k_adj_gather(PState A, Search Q, Rheo c, 
         double dm = (double)(lhk * sph_kernel_w(c.skf, 0.f, me.z));
         double dx0 = 0.0, dx1 = 0.0;
         for (int q = 0; q < cnt; q++) {
-            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride];
+            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride].x;
             const float4 o = Q.xhm[j];
             PairGeom g;
             pair_test(xk, make_float2(o.x, o.y), me.z, o.z, g);
             float w, d0, d1, ca, cb;
             sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
             sph_kernel_hess(c.skf, g.r, g.mh, ca, cb);
-            const float mj = o.w, pj = Q.pterm[j], lhj = lh[j];
+            // the pair terms in FP64: their sums over the neighbours cancel
+            // strongly (the kernel gradient is antisymmetric in k, j)
+            const double mj = o.w, pj = Q.pterm[j], lhj = lh[j];
             const float2 laj = lin[j];
-            const float cp = pk + pj;
-            dm += (double)(lhj * w) + (double)(cp * (laj.x * d0 + laj.y * d1));
-            const float fd = lhk * mj + lhj * mk;
-            dx0 += (double)(fd * d0);
-            dx1 += (double)(fd * d1);
+            const double cp = (double)pk + pj;
+            dm += lhj * (double)w + cp * ((double)laj.x * d0 + (double)laj.y * d1);
+            const double fd = (double)lhk * mj + lhj * (double)mk;
+            dx0 += fd * d0;
+            dx1 += fd * d1;
             // (P_k + P_j) H(d_kj) (m_k lambda_j - m_j lambda_k), H = ca dhat dhat^T + cb I
-            const float u0 = mk * laj.x - mj * lak.x, u1 = mk * laj.y - mj * lak.y;
-            const float dh0 = g.dx0 / g.r, dh1 = g.dx1 / g.r;
-            const float du = dh0 * u0 + dh1 * u1;
-            dx0 += (double)(cp * (ca * dh0 * du + cb * u0));
-            dx1 += (double)(cp * (ca * dh1 * du + cb * u1));
+            const double u0 = (double)mk * laj.x - mj * lak.x, u1 = (double)mk * laj.y - mj * lak.y;
+            const double dh0 = (double)g.dx0 / g.r, dh1 = (double)g.dx1 / g.r;
+            const double du = dh0 * u0 + dh1 * u1;
+            dx0 += cp * ((double)ca * dh0 * du + (double)cb * u0);
+            dx1 += cp * ((double)ca * dh1 * du + (double)cb * u1);
         }
         lm[k] += dm;
         double2 ax = lxacc[k];

@@ -140,12 +140,12 @@ struct gfsph_handle {
     int* cellA = nullptr;
     float2* velfin = nullptr;
     float* pterm = nullptr;
-    float2* pr = nullptr;    // (pterm, h) per slot
+    float4* pr = nullptr;    // (pterm, h, m, 0) per slot
     int2* keyrank = nullptr;
     int* perm = nullptr;
     float2* f2tmp = nullptr;
     float4* xhm = nullptr;
-    int* nbr = nullptr;
+    int4* nbr = nullptr;     // neighbour table: {j, W, dW/dx, dW/dy} per entry
     int* ncount = nullptr;
     int kcap = 0;
     float2* indv = nullptr;  // internal acceleration of every active particle
@@ -185,6 +185,8 @@ struct gfsph_handle {
     // outputs
     double2* d_racc = nullptr;
     float* d_rout = nullptr;
+    double* d_lam = nullptr;    // raster misfit: dL/dR per node
+    double* d_lpart = nullptr;  // raster misfit: block sums of the loss
     double *haz_sum_h = nullptr, *haz_sum_v = nullptr;
     unsigned int *haz_max_h = nullptr, *haz_max_v = nullptr;
     int* haz_cnt = nullptr;
@@ -897,7 +899,8 @@ int gfsph_destroy(gfsph_handle* h) try {
     free_particles(h);
     dfree(h->count); dfree(h->start); dfree(h->tile_sum); dfree(h->bmark); dfree(h->bstart);
     dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
-    dfree(h->d_auxv); dfree(h->S); dfree(h->bparts); dfree(h->d_racc); dfree(h->d_rout);
+    dfree(h->d_auxv); dfree(h->S); dfree(h->bparts); dfree(h->d_racc); dfree(h->d_rout); dfree(h->d_lam);
+    dfree(h->d_lpart);
     dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
     dfree(h->cw_a1); dfree(h->cw_a2); dfree(h->cw_hs); dfree(h->cw_ml); dfree(h->cw_rhs); dfree(h->cw_g0);
     dfree(h->cw_g1);
@@ -1230,14 +1233,16 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) try {
     int st = read_scalars(h);
     if (st) return st;
     int nreg = h->hS->nreg, nbig = h->hS->nbig;
-    std::vector<int> cnt(n), id(n), tab((size_t)h->kcap * (((size_t)n + 31) / 32 * 32));
+    std::vector<int> cnt(n), id(n);
+    std::vector<int4> tab((size_t)h->kcap * (((size_t)n + 31) / 32 * 32));
     CK(cudaMemcpy(cnt.data(), h->ncount, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(id.data(), h->A.id, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(tab.data(), h->nbr, tab.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tab.data(), h->nbr, tab.size() * sizeof(int4), cudaMemcpyDeviceToHost));
     std::vector<std::vector<int>> lists(n);
     for (int s = 0; s < nreg; s++) {
         auto& L = lists[id[s]];
-        for (int k = 0; k < cnt[s] && k < h->kcap; k++) L.push_back(id[tab[tab_base(s, h->kcap) + (size_t)k * kTabStride]]);
+        for (int k = 0; k < cnt[s] && k < h->kcap; k++)
+            L.push_back(id[tab[tab_base(s, h->kcap) + (size_t)k * kTabStride].x]);
     }
     if (nbig > 0) {  // pairs of the big particles, found on the device
         int pcap = 1 << 20;
@@ -1324,6 +1329,40 @@ int gfsph_raster(gfsph_handle* h, int kind, float* out) try {
     }
     if (kind <= GFSPH_RASTER_COUNT) CK(cudaMemcpyAsync(out, h->d_rout, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
+}
+
+int gfsph_raster_misfit(gfsph_handle* h, const float* target, double* loss, float* gx, float* gh) try {
+    if (!h || !target || !loss) return GFSPH_ERR_ARG;
+    if (!h->has_state) return GFSPH_ERR_STATE;
+    const int np = h->nx * h->ny, n = h->n;
+    cudaStream_t s = h->stream;
+    const int gb = blocks_for(np, 256);
+    if (!h->d_racc && dalloc(&h->d_racc, np)) return GFSPH_ERR_CUDA;
+    if (!h->d_lam && dalloc(&h->d_lam, np)) return GFSPH_ERR_CUDA;
+    if (!h->d_lpart && dalloc(&h->d_lpart, 148 * 64)) return GFSPH_ERR_CUDA;
+    if (!h->d_rout && dalloc(&h->d_rout, np)) return GFSPH_ERR_CUDA;
+    std::vector<double> part(gb);
+    CK(cudaMemcpyAsync(h->d_rout, target, (size_t)np * sizeof(float), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(h->d_racc, 0, (size_t)np * sizeof(double2), s));
+    launch(h, K_RASTER, [&] { k_raster_idw<<<blocks_for(n), kThreads, 0, s>>>(h->B, n, h->dem, h->d_racc); });
+    launch(h, K_RASTER, [&] { k_misfit_nodes<<<gb, 256, 0, s>>>(h->d_racc, h->d_rout, np, h->d_lam, h->d_lpart); });
+    if (gx || gh) {
+        // U, the scratch of the caller-order copies, holds the gradients
+        launch(h, K_RASTER, [&] {
+            k_misfit_particles<<<blocks_for(n), kThreads, 0, s>>>(h->B, n, h->dem, h->d_racc, h->d_lam, h->U.pos,
+                                                                  h->U.rho);
+        });
+        if (gx) CK(cudaMemcpyAsync(gx, h->U.pos, (size_t)n * sizeof(float2), cudaMemcpyDeviceToHost, s));
+        if (gh) CK(cudaMemcpyAsync(gh, h->U.rho, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaMemcpyAsync(part.data(), h->d_lpart, (size_t)gb * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double l = 0.0;
+    for (int b = 0; b < gb; b++) l += part[b];
+    *loss = l;
     return GFSPH_OK;
 } catch (...) {  // a C++ exception never crosses the C ABI
     return GFSPH_ERR_HOST;
@@ -1559,6 +1598,8 @@ int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob) t
 
 }  // extern "C"
 
+constexpr int kAdjParams = 3;  // dL/d tanfi, dL/d xi, dL/d Bingham yield stress
+
 struct gfsph_adjoint {
     gfsph_handle* h = nullptr;
     int n = 0, nsteps = 0, every = 1, nck = 0;
@@ -1570,7 +1611,9 @@ struct gfsph_adjoint {
     float* rhoN = nullptr;                    // depth of the final state
     float2 *lx = nullptr, *lv = nullptr;      // running adjoints (caller order)
     double* lm = nullptr;                     // dL/d volume, accumulated
-    double* lpar = nullptr;                   // dL/d tanfi, dL/d xi
+    double* lpar = nullptr;                   // dL/d tanfi, dL/d xi, dL/d Bingham yield stress
+    double par[kAdjParams] = {};              // the same on the host after a backward pass
+    bool has_par = false;
     float* gh = nullptr;
     float2 *lx1 = nullptr, *lv2 = nullptr, *lvp = nullptr, *lin = nullptr, *lv0 = nullptr;
     float* lh = nullptr;
@@ -1734,7 +1777,8 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     *out = nullptr;
     if (!h->has_state) return GFSPH_ERR_STATE;
     const Rheo& c = h->rheo;
-    if (!(c.nfric == 5 || c.nfric == 6) || c.xi < 0.f || c.erosion || c.icpwp != 0 || c.pa_sph != 2 || c.sle != 0 ||
+    if (!(c.nfric == 4 || c.nfric == 5 || c.nfric == 6) || (c.nfric != 4 && c.xi < 0.f) || c.erosion ||
+        c.icpwp != 0 || c.pa_sph != 2 || c.sle != 0 ||
         c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f || c.nor_density || c.cos_theta ||
         (c.skf != 1 && c.skf != 4))
         return GFSPH_ERR_UNSUPPORTED;
@@ -1747,7 +1791,7 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     st |= dalloc(&a->ckx, n * a->nck); st |= dalloc(&a->ckv, n * a->nck);
     st |= dalloc(&a->segx, n * a->every); st |= dalloc(&a->segv, n * a->every);
     st |= dalloc(&a->rho0, n); st |= dalloc(&a->mass0, n); st |= dalloc(&a->hsml0, n); st |= dalloc(&a->rhoN, n);
-    st |= dalloc(&a->lx, n); st |= dalloc(&a->lv, n); st |= dalloc(&a->lm, n); st |= dalloc(&a->lpar, 2);
+    st |= dalloc(&a->lx, n); st |= dalloc(&a->lv, n); st |= dalloc(&a->lm, n); st |= dalloc(&a->lpar, kAdjParams);
     st |= dalloc(&a->gh, n); st |= dalloc(&a->lx1, n); st |= dalloc(&a->lv2, n); st |= dalloc(&a->lvp, n);
     st |= dalloc(&a->lin, n); st |= dalloc(&a->lv0, n); st |= dalloc(&a->lh, n); st |= dalloc(&a->lxacc, n);
     st |= dalloc(&a->lms, n);
@@ -1799,7 +1843,7 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
     CK(cudaMemcpyAsync(a->lv, gv, un * sizeof(float2), cudaMemcpyHostToDevice, st));
     if (gh) CK(cudaMemcpyAsync(a->gh, gh, un * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(a->lm, 0, un * sizeof(double), st));
-    CK(cudaMemsetAsync(a->lpar, 0, 2 * sizeof(double), st));
+    CK(cudaMemsetAsync(a->lpar, 0, kAdjParams * sizeof(double), st));
     const int nseg = a->nck - 1;
     for (int sg = nseg - 1; sg >= 0; sg--) {
         const int t0 = sg * a->every, len = std::min(a->every, a->nsteps - t0);
@@ -1847,19 +1891,28 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
     if (gx0) CK(cudaMemcpyAsync(gx0, a->lx, un * sizeof(float2), cudaMemcpyDeviceToHost, st));
     if (gv0) CK(cudaMemcpyAsync(gv0, a->lv, un * sizeof(float2), cudaMemcpyDeviceToHost, st));
     std::vector<double> lm(un);
-    double par[2];
     CK(cudaMemcpyAsync(lm.data(), a->lm, un * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(par, a->lpar, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(a->par, a->lpar, kAdjParams * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    a->has_par = true;
     if (gm)
         for (size_t k = 0; k < un; k++) gm[k] = (float)lm[k];
-    if (gmu) *gmu = par[0];
-    if (gxi) *gxi = par[1];
+    if (gmu) *gmu = a->par[0];
+    if (gxi) *gxi = a->par[1];
     // leave the handle at the final state of the recorded run
     int r = adj_restore(a, a->ckx + un * (a->nck - 1), a->ckv + un * (a->nck - 1), a->rhoN);
     if (r) return r;
     set_field<double>(h, offsetof(StepScalars, time), a->t0 + (double)a->nsteps * (double)a->dt0);
     CK(cudaStreamSynchronize(st));
+    return GFSPH_OK;
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
+}
+
+int gfsph_adjoint_param(gfsph_adjoint* a, int which, double* value) try {
+    if (!a || !value || which < 0 || which >= kAdjParams) return GFSPH_ERR_ARG;
+    if (!a->has_par) return GFSPH_ERR_STATE;
+    *value = a->par[which];
     return GFSPH_OK;
 } catch (...) {  // a C++ exception never crosses the C ABI
     return GFSPH_ERR_HOST;

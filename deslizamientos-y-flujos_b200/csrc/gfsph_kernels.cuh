@@ -92,10 +92,12 @@ struct Search {
     const int* start;    // cell key -> first particle slot (exclusive scan), ncells+1
     const int* cellA;    // slot -> cell key (all levels), -1 out of the domain
     const float4* xhm;   // slot -> (x, y, hsml, mass) at the start of the step
-    int* nbr;            // neighbour table of the regular particles (layout: tab_base)
+    int4* nbr;           // neighbour table of the regular particles (layout: tab_base); entry
+                         // {j, W_ij, dW_ij/dx, dW_ij/dy} (the FP32 bits of the kernel values,
+                         // computed once per pair by the search, as grid_find stores w and dwdx)
     int* ncount;
     float* pterm;        // p/h^2 (pa_sph 2) or p (pa_sph 1)
-    float2* pr;          // (pterm, h): what the internal force gathers per neighbour
+    float4* pr;          // (pterm, h, m, 0): what the internal force gathers per neighbour
     float2* indv;        // internal acceleration of every active particle (slot order)
     float* rho0;         // depth at the start of the step, after Adaptive_dt's h_inf clamp (icpwp = 3)
     const int2* rcell;   // slot -> cell of the reference's own grid (skf 2, 3), else null
@@ -130,8 +132,9 @@ __device__ __forceinline__ void scalars_from_smem(StepScalars* S, const StepScal
 
 // Neighbour-table layout, blocked by warps of 32 particles: entry k of
 // particle i is at tab_base(i, kcap) + 32 k.  The lanes of a warp read entry k
-// of their particles as one 128-byte line, and the entries a warp appends
-// while its lanes are at different k stay within its own 32 kcap words.
+// of their particles as one 512-byte run (16-byte entries), and the entries a
+// warp appends while its lanes are at different k stay within its own
+// 32 kcap entries.
 __host__ __device__ __forceinline__ size_t tab_base(int i, int kcap) {
     return (size_t)(i >> 5) * ((size_t)kcap << 5) + (size_t)(i & 31);
 }
@@ -842,7 +845,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
 // the gathers are latency-bound, and 12 resident blocks beat 10 with the
 // 45 registers the compiler would take (4 % on the whole step).
 template <bool SPARSE, int SKF>
-__global__ void __launch_bounds__(128, 12) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+__global__ void __launch_bounds__(128, 10) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     constexpr int SK = SupportScale<SKF>::value;
     if (S->skip || (S->sparse != 0) != SPARSE) return;
     const int nreg = S->nreg, nlev = S->nlev;
@@ -852,13 +855,19 @@ __global__ void __launch_bounds__(128, 12) k_density(PState A, Search Q, StepSca
         float hi = me.z;
         const int2 ci = (SK == 2) ? make_int2(0, 0) : Q.rcell[i];
         double acc = (double)(sph_kernel_w<SKF>(0.f, hi) * me.w);
-        int* tab = Q.nbr + tab_base(i, Q.kcap);
+        int4* tab = Q.nbr + tab_base(i, Q.kcap);
         int cnt = 0;
         for (int k = 0; k < nlev; k++)
             level_neighbours<SPARSE, SK>(Q, S, k, i, xi, hi, ci, [&](int j, float4 o, const PairGeom& g) {
-                if (cnt < Q.kcap) tab[(size_t)cnt * kTabStride] = j;
+                // W and grad W of the pair, once per step: the internal force,
+                // av_vel and the normalisation read them from the table
+                float w, d0, d1;
+                sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+                if (cnt < Q.kcap)  // streamed out: the gathers keep L2
+                    __stcs(tab + (size_t)cnt * kTabStride,
+                           make_int4(j, __float_as_int(w), __float_as_int(d0), __float_as_int(d1)));
                 cnt++;
-                acc += (double)(o.w * sph_kernel_w<SKF>(g.r, g.mh));
+                acc += (double)(o.w * w);
             });
         Q.ncount[i] = cnt;
         if (cnt > Q.kcap) {  // table too small: stop this step before any state is written
@@ -872,7 +881,7 @@ __global__ void __launch_bounds__(128, 12) k_density(PState A, Search Q, StepSca
         float p = (c.cgra05 * hc) * hc;
         const float pt = (c.pa_sph == 1) ? p : p / (hc * hc);
         Q.pterm[i] = pt;
-        Q.pr[i] = make_float2(pt, h);
+        Q.pr[i] = make_float4(pt, h, me.w, 0.f);
     }
 }
 
@@ -936,17 +945,15 @@ __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepSca
             float p = (c.cgra05 * hc) * hc;
             const float pt = (c.pa_sph == 1) ? p : p / (hc * hc);
             Q.pterm[i] = pt;
-            Q.pr[i] = make_float2(pt, h);
+            Q.pr[i] = make_float4(pt, h, me.w, 0.f);
         }
     }
 }
 
-// One pair term of IntForces_SW (SPH_SW_2019.f90:6905-6920) for particle i.
-template <int SKF>
-__device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rhoi, float pj, float rhoj, float mj,
-                                              const PairGeom& g, double& a0, double& a1) {
-    float w, d0, d1;
-    sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+// One pair term of IntForces_SW (SPH_SW_2019.f90:6905-6920) for particle i,
+// from the pair's kernel gradient (d0, d1).
+__device__ __forceinline__ void pressure_terms(const Rheo& c, float pi_, float rhoi, float pj, float rhoj, float mj,
+                                               float d0, float d1, double& a0, double& a1) {
     float h0, h1;
     if (c.pa_sph == 1) {
         rhoi = (rhoi < c.h_inf) ? c.h_inf : rhoi;
@@ -962,6 +969,15 @@ __device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rh
     a1 += (double)(mj * h1);
 }
 
+// The same with the pair geometry: the kernel gradient evaluated here.
+template <int SKF>
+__device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rhoi, float pj, float rhoj, float mj,
+                                              const PairGeom& g, double& a0, double& a1) {
+    float w, d0, d1;
+    sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+    pressure_terms(c, pi_, rhoi, pj, rhoj, mj, d0, d1, a0, a1);
+}
+
 // Internal acceleration of the coarse-level particles, one warp per particle.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
@@ -972,10 +988,10 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
     const int nreg = S->nreg, nbig = S->nbig;
     for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
-        const float2 pri = Q.pr[i];
+        const float4 pri = Q.pr[i];
         double a0 = 0.0, a1 = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
-            const float2 prj = Q.pr[j];
+            const float4 prj = Q.pr[j];
             pressure_pair<SKF>(c, pri.x, pri.y, prj.x, prj.y, o.w, g, a0, a1);
         });
         a0 = warp_sum(a0);
@@ -984,46 +1000,34 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
     }
 }
 
-// Internal acceleration of a regular particle over its neighbour table.  The
-// table is read four entries at a time so that four independent gather
-// chains are in flight per thread; the FP64 sum keeps the table order.
-template <int SKF>
-__device__ __forceinline__ void internal_force(const PState& A, const Search& Q, const Rheo& c, int i, int n,
-                                               float& in0, float& in1) {
-    float4 me = Q.xhm[i];
-    float2 xi = make_float2(me.x, me.y);
-    float hi = me.z;
-    const float2 pri = __ldg(&Q.pr[i]);
+// Internal acceleration of a regular particle over its neighbour table: per
+// entry the stored kernel gradient and one gather of (p-term, h, m) of the
+// neighbour.  The table is read four entries at a time so that four
+// independent gathers are in flight per thread; the FP64 sum keeps the table
+// order.
+__device__ __forceinline__ void internal_force(const Search& Q, const Rheo& c, int i, float& in0, float& in1) {
+    const float4 pri = __ldg(&Q.pr[i]);
     const float pi_ = pri.x, rhoi = pri.y;
     double a0 = 0.0, a1 = 0.0;
     const int cnt = Q.ncount[i];
-    const int* tab = Q.nbr + tab_base(i, Q.kcap);
+    const int4* tab = Q.nbr + tab_base(i, Q.kcap);
     int k = 0;
     for (; k + 4 <= cnt; k += 4) {
-        int j[4];
-        float4 o[4];
-        float2 prj[4];
+        int4 e[4];
+        float4 prj[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
+        for (int u = 0; u < 4; u++) e[u] = __ldcs(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            o[u] = __ldg(&Q.xhm[j[u]]);
-            prj[u] = __ldg(&Q.pr[j[u]]);
-        }
+        for (int u = 0; u < 4; u++) prj[u] = __ldg(&Q.pr[e[u].x]);
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            PairGeom g;
-            pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
-            pressure_pair<SKF>(c, pi_, rhoi, prj[u].x, prj[u].y, o[u].w, g, a0, a1);
-        }
+        for (int u = 0; u < 4; u++)
+            pressure_terms(c, pi_, rhoi, prj[u].x, prj[u].y, prj[u].z, __int_as_float(e[u].z), __int_as_float(e[u].w),
+                           a0, a1);
     }
     for (; k < cnt; k++) {
-        int j = __ldg(tab + (size_t)k * kTabStride);
-        float4 o = __ldg(&Q.xhm[j]);
-        const float2 prj = __ldg(&Q.pr[j]);
-        PairGeom g;
-        pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-        pressure_pair<SKF>(c, pi_, rhoi, prj.x, prj.y, o.w, g, a0, a1);
+        const int4 e = __ldcs(tab + (size_t)k * kTabStride);
+        const float4 prj = __ldg(&Q.pr[e.x]);
+        pressure_terms(c, pi_, rhoi, prj.x, prj.y, prj.z, __int_as_float(e.z), __int_as_float(e.w), a0, a1);
     }
     in0 = (float)a0;
     in1 = (float)a1;
@@ -1189,7 +1193,7 @@ __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars*
     const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         float in0, in1;
-        internal_force<SKF>(A, Q, c, i, n, in0, in1);
+        internal_force(Q, c, i, in0, in1);
         Q.indv[i] = make_float2(in0, in1);
     }
 }
@@ -1312,17 +1316,14 @@ __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S
     const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         const float4 me = Q.xhm[i];
-        const float2 xi = make_float2(me.x, me.y);
         const float hi = me.z;
         double den = (double)((sph_kernel_w<SKF>(0.f, hi) * me.w) / prev_depth(c, hp, i, clamp_prev));
         const int cnt = Q.ncount[i];
-        const int* tab = Q.nbr + tab_base(i, Q.kcap);
+        const int4* tab = Q.nbr + tab_base(i, Q.kcap);
         for (int k = 0; k < cnt; k++) {
-            const int j = __ldg(tab + (size_t)k * kTabStride);
-            const float4 o = __ldg(&Q.xhm[j]);
-            PairGeom g;
-            pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-            den += (double)((o.w / prev_depth(c, hp, j, clamp_prev)) * sph_kernel_w<SKF>(g.r, g.mh));
+            const int4 e = __ldg(tab + (size_t)k * kTabStride);  // read again by the next calls of the step
+            const int j = e.x;
+            den += (double)((__ldg(&A.mass[j]) / prev_depth(c, hp, j, clamp_prev)) * __int_as_float(e.y));
         }
         hout[i] = A.rho[i] / (float)den;
     }
@@ -1378,7 +1379,7 @@ __global__ void __launch_bounds__(128) k_stage_begin(PState A, Search Q, StepSca
         const float2 p = A.pos[i];
         const float pt = stage_pterm<COS>(c, dem, h1[i], p.x, p.y);
         Q.pterm[i] = pt;
-        Q.pr[i] = make_float2(pt, h1[i]);
+        Q.pr[i] = make_float4(pt, h1[i], A.mass[i], 0.f);
     }
 }
 
@@ -1399,7 +1400,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
     const float f1n = (s == 2) ? 1.f : 0.5f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
         if (s > 0 && C.out[i]) {  // frozen: its pressure term stays, its depth is the next call's
-            Q.pr[i] = make_float2(Q.pterm[i], hnext[i]);
+            Q.pr[i] = make_float4(Q.pterm[i], hnext[i], A.mass[i], 0.f);
             continue;
         }
         const float2 x0 = A.pos[i], v0 = A.vel[i];
@@ -1412,7 +1413,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
             C.out[i] = 1;
             C.xo[i] = make_float2(xx, xy);
             C.v[i] = make_float2(vx, vy);
-            Q.pr[i] = make_float2(Q.pterm[i], hnext[i]);
+            Q.pr[i] = make_float4(Q.pterm[i], hnext[i], A.mass[i], 0.f);
             continue;
         }
         if (s == 0) C.out[i] = 0;
@@ -1438,7 +1439,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
             pt = stage_pterm<COS>(c, dem, hnext[i], nx_, ny_);
             Q.pterm[i] = pt;
         }
-        Q.pr[i] = make_float2(pt, hnext[i]);
+        Q.pr[i] = make_float4(pt, hnext[i], A.mass[i], 0.f);
     }
 }
 
@@ -1500,16 +1501,22 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
     if (c.erosion) flush_node_box(S, box);
 }
 
-// One pair term of av_vel (SPH_MAIN_2019.f90:3072-3080) for particle i.
-template <int SKF>
-__device__ __forceinline__ void xsph_pair(const Rheo& c, float2 vi, float rhoi, float2 vj, float rhoj, float mj,
-                                          const PairGeom& g, double& a0, double& a1) {
-    float w = sph_kernel_w<SKF>(g.r, g.mh);
+// One pair term of av_vel (SPH_MAIN_2019.f90:3072-3080) for particle i with
+// the pair's kernel value w.
+__device__ __forceinline__ void xsph_terms(float2 vi, float rhoi, float2 vj, float rhoj, float mj, float w, double& a0,
+                                           double& a1) {
     float den = rhoi + rhoj;
     float t0 = (((2.f * mj) * (vi.x - vj.x)) / den) * w;
     float t1 = (((2.f * mj) * (vi.y - vj.y)) / den) * w;
     a0 -= (double)t0;
     a1 -= (double)t1;
+}
+
+// The same with the pair geometry: the kernel value evaluated here.
+template <int SKF>
+__device__ __forceinline__ void xsph_pair(float2 vi, float rhoi, float2 vj, float rhoj, float mj, const PairGeom& g,
+                                          double& a0, double& a1) {
+    xsph_terms(vi, rhoi, vj, rhoj, mj, sph_kernel_w<SKF>(g.r, g.mh), a0, a1);
 }
 
 // av_vel (SPH_MAIN_2019.f90:3042-3099) with the start-of-step W_ij, then
@@ -1520,40 +1527,28 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
     const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         if (B.flag[i]) continue;
-        float4 me = Q.xhm[i];
-        float2 xi = make_float2(me.x, me.y);
-        float hi = me.z;
         const float4 si = Q.xsv[i];
         const float2 vi = make_float2(si.x, si.y);
         const float rhoi = si.z;
         const int cnt = Q.ncount[i];
-        const int* tab = Q.nbr + tab_base(i, Q.kcap);
+        const int4* tab = Q.nbr + tab_base(i, Q.kcap);
         double a0 = 0.0, a1 = 0.0;
         int k = 0;
         for (; k + 4 <= cnt; k += 4) {
-            int j[4];
-            float4 o[4], sj[4];
+            int4 e[4];
+            float4 sj[4];
 #pragma unroll
-            for (int u = 0; u < 4; u++) j[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
+            for (int u = 0; u < 4; u++) e[u] = __ldcs(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                o[u] = __ldg(&Q.xhm[j[u]]);
-                sj[u] = Q.xsv[j[u]];
-            }
+            for (int u = 0; u < 4; u++) sj[u] = Q.xsv[e[u].x];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                PairGeom g;
-                pair_test(xi, make_float2(o[u].x, o[u].y), hi, o[u].z, g);
-                xsph_pair<SKF>(c, vi, rhoi, make_float2(sj[u].x, sj[u].y), sj[u].z, sj[u].w, g, a0, a1);
-            }
+            for (int u = 0; u < 4; u++)
+                xsph_terms(vi, rhoi, make_float2(sj[u].x, sj[u].y), sj[u].z, sj[u].w, __int_as_float(e[u].y), a0, a1);
         }
         for (; k < cnt; k++) {
-            int j = __ldg(tab + (size_t)k * kTabStride);
-            float4 o = __ldg(&Q.xhm[j]);
-            const float4 sj = Q.xsv[j];
-            PairGeom g;
-            pair_test(xi, make_float2(o.x, o.y), hi, o.z, g);
-            xsph_pair<SKF>(c, vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, g, a0, a1);
+            const int4 e = __ldcs(tab + (size_t)k * kTabStride);
+            const float4 sj = Q.xsv[e.x];
+            xsph_terms(vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, __int_as_float(e.y), a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
@@ -1576,7 +1571,7 @@ __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalar
         double a0 = 0.0, a1 = 0.0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
             const float4 sj = Q.xsv[j];
-            xsph_pair<SKF>(c, vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, g, a0, a1);
+            xsph_pair<SKF>(vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, g, a0, a1);
         });
         a0 = warp_sum(a0);
         a1 = warp_sum(a1);
@@ -1704,6 +1699,81 @@ __global__ void k_raster_idw_finish(const double2* acc, float* out, int np) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
         double2 a = acc[k];
         out[k] = ((float)a.y >= 1.e-6f) ? (float)(a.x / a.y) : (float)a.x;
+    }
+}
+
+// Misfit of the depth raster against a target raster, L = sum_nodes (R - T)^2
+// with R the IDW raster above, for back-analysis: per node lam = dL/dR =
+// 2 (R - T) and the node's share of L, summed per block (the host adds the
+// block sums in block order).
+__global__ void k_misfit_nodes(const double2* acc, const float* target, int np, double* lam, double* part) {
+    __shared__ double sh[32];
+    double l = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+        const double2 a = acc[k];
+        const double R = ((float)a.y >= 1.e-6f) ? a.x / a.y : a.x;
+        const double d = R - (double)target[k];
+        lam[k] = 2.0 * d;
+        l += d * d;
+    }
+    l = warp_sum(l);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// dL/dh and dL/dx of every particle inside the domain, through the IDW
+// weights w = 1/dhat, dhat = max(dist, 1e-6)/distg, of its 4x4 nodes: with
+// S = sum w and R = sum h w / S, dR/dh_i = w_i / S and dR/dw_i = (h_i - R)/S
+// (where S < 1e-6 the raster is sum h w itself: w_i and h_i);
+// dw/dp = -(distg / dist^2) (p - node)/dist.  Written in caller order.
+__global__ void k_misfit_particles(const PState B, int n, DemView dem, const double2* acc, const double* lam,
+                                   float2* gx, float* gh) {
+    const float distg = sqrtf(dem.dx * dem.dx + dem.dy * dem.dy);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int o = B.id[i];
+        if (B.flag[i]) {
+            gx[o] = make_float2(0.f, 0.f);
+            gh[o] = 0.f;
+            continue;
+        }
+        const float2 p = B.pos[i];
+        const double h = B.rho[i];
+        const int ipx = (int)((p.x - dem.xmin) / dem.dx + 1.f);
+        const int ipy = (int)((p.y - dem.ymin) / dem.dy + 1.f);
+        const int ix0 = max(1, ipx - 1), iy0 = max(1, ipy - 1), ix1 = min(dem.nx, ipx + 2), iy1 = min(dem.ny, ipy + 2);
+        double dh = 0.0, d0 = 0.0, d1 = 0.0;
+        for (int ix = ix0; ix <= ix1; ix++)
+            for (int iy = iy0; iy <= iy1; iy++) {
+                const int ip = (iy - 1) * dem.nx + (ix - 1);
+                const double ex = (double)p.x - (double)(dem.xmin + (float)(ix - 1) * dem.dx);
+                const double ey = (double)p.y - (double)(dem.ymin + (float)(iy - 1) * dem.dy);
+                const double dist = sqrt(ex * ex + ey * ey);
+                const double dhat = fmax(dist, 1.e-6) / (double)distg;
+                const double w = 1.0 / dhat;
+                const double2 a = acc[ip];
+                const double L = lam[ip];
+                double dRdh, dRdw;
+                if ((float)a.y >= 1.e-6f) {
+                    dRdh = w / a.y;
+                    dRdw = (h - a.x / a.y) / a.y;
+                } else {
+                    dRdh = w;
+                    dRdw = h;
+                }
+                dh += L * dRdh;
+                if (dist > 1.e-6) {
+                    const double c = -L * dRdw * (double)distg / (dist * dist * dist);
+                    d0 += c * ex;
+                    d1 += c * ey;
+                }
+            }
+        gx[o] = make_float2((float)d0, (float)d1);
+        gh[o] = (float)dh;
     }
 }
 

@@ -112,6 +112,13 @@ module gfsph_c
        integer(c_int), value :: kind
        real(c_float), intent(out) :: out(*)
      end function
+     integer(c_int) function gfsph_raster_misfit(h, target, loss, gx, gh) bind(c, name="gfsph_raster_misfit")
+       import :: c_int, c_ptr, c_float, c_double
+       type(c_ptr), value :: h
+       real(c_float), intent(in) :: target(*)
+       real(c_double), intent(out) :: loss
+       real(c_float), intent(out) :: gx(*), gh(*)
+     end function
      integer(c_int) function gfsph_hazard_sample(handle) bind(c, name="gfsph_hazard_sample")
        import :: c_int, c_ptr
        type(c_ptr), value :: handle
@@ -184,6 +191,12 @@ module gfsph_c
        real(c_float), intent(in) :: gx(*), gv(*), gh(*)
        real(c_float), intent(out) :: gx0(*), gv0(*), gm(*)
        real(c_double), intent(out) :: gmu, gxi
+     end function
+     integer(c_int) function gfsph_adjoint_param(a, which, val) bind(c, name="gfsph_adjoint_param")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a
+       integer(c_int), value :: which
+       real(c_double), intent(out) :: val
      end function
      integer(c_int) function gfsph_adjoint_destroy(adj) bind(c, name="gfsph_adjoint_destroy")
        import :: c_int, c_ptr
@@ -265,6 +278,11 @@ module gfsph_c
      integer(c_long_long) function gfsph_cg_launch_count(cg) bind(c, name="gfsph_cg_launch_count")
        import :: c_long_long, c_ptr
        type(c_ptr), value :: cg
+     end function
+     integer(c_int) function gfsph_cg_device_ms(cg, ms) bind(c, name="gfsph_cg_device_ms")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: cg
+       real(c_double), intent(out) :: ms
      end function
      ! drop-in for: call solvegc2(npoin, nelem, nnode, ndofn, ntotv, nevab, intmat, iffix, fixed, gstif, rcg, ficg, tolCG)
      integer(c_int) function gfsph_solvegc2(npoin, nelem, nnode, ndofn, intmat, iffix, fixed, gstif, rcg, ficg, &

@@ -76,6 +76,7 @@ SIGNATURES = {
     "gfsph_internal_forces": (C.c_int, [C.c_void_p, _FP]),
     "gfsph_raster": (C.c_int, [C.c_void_p, C.c_int, _FP]),
     "gfsph_hazard_sample": (C.c_int, [C.c_void_p]),
+    "gfsph_raster_misfit": (C.c_int, [C.c_void_p, _FP, C.POINTER(C.c_double), _FP, _FP]),
     "gfsph_hazard_reset": (C.c_int, [C.c_void_p]),
     "gfsph_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "gfsph_profile": (C.c_int, [C.c_void_p, C.c_int]),
@@ -93,6 +94,7 @@ SIGNATURES = {
     "gfsph_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "gfsph_adjoint_backward": (C.c_int, [C.c_void_p, _FP, _FP, _FP, _FP, _FP, _FP, C.POINTER(C.c_double),
                                          C.POINTER(C.c_double)]),
+    "gfsph_adjoint_param": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "gfsph_adjoint_destroy": (C.c_int, [C.c_void_p]),
     "gfsph_gradhs": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, _FP, _FP]),
     "gfsph_set_pwp": (C.c_int, [C.c_void_p, _FP]),
@@ -107,6 +109,7 @@ SIGNATURES = {
     "gfsph_cg_solve": (C.c_int, [C.c_void_p, _IP, _FP, _FP, _FP, C.c_float, _IP]),
     "gfsph_cg_destroy": (C.c_int, [C.c_void_p]),
     "gfsph_cg_launch_count": (C.c_longlong, [C.c_void_p]),
+    "gfsph_cg_device_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "gfsph_solvegc2": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _FP, _FP, _FP, _FP, C.c_float, _IP]),
     "gfsph_strerror": (C.c_char_p, [C.c_int]),
     "gfsph_version": (C.c_int, []),
@@ -305,6 +308,16 @@ class Sim:
         _check(lib().gfsph_raster(self.h, kind, _fp(out)), "gfsph_raster")
         return out
 
+    def raster_misfit(self, target):
+        """L = sum (R - T)^2 of the depth raster R against `target` (ny, nx),
+        with dL/dx (n, 2) and dL/dh (n,) of the current state."""
+        t = np.ascontiguousarray(target, np.float32)
+        loss = C.c_double()
+        gx = np.empty((self.n, 2), np.float32)
+        gh = np.empty(self.n, np.float32)
+        _check(lib().gfsph_raster_misfit(self.h, _fp(t), C.byref(loss), _fp(gx), _fp(gh)), "gfsph_raster_misfit")
+        return loss.value, gx, gh
+
     def hazard_sample(self):
         _check(lib().gfsph_hazard_sample(self.h), "gfsph_hazard_sample")
 
@@ -369,6 +382,12 @@ class CG:
 
     def launch_count(self):
         return int(lib().gfsph_cg_launch_count(self.h))
+
+    def device_ms(self):
+        """Device time of the last solve (its kernels, without the host copies)."""
+        ms = C.c_double(0.0)
+        _check(lib().gfsph_cg_device_ms(self.h, C.byref(ms)), "gfsph_cg_device_ms")
+        return ms.value
 
     def close(self):
         if self.h:
@@ -459,7 +478,8 @@ class Adjoint:
 
     def backward(self, gx, gv, gh=None):
         """dL/dx, dL/dv (n, 2) and dL/dh (n,) of the final state -> dict of
-        dL/dx0, dL/dv0, dL/dmass, dL/dtanfi (const(9)), dL/dxi (const(3))."""
+        dL/dx0, dL/dv0, dL/dmass, dL/dtanfi (const(9)), dL/dxi (const(3)),
+        dL/dtauy (const(6), the Bingham yield stress)."""
         if not self.h or not self.sim.h:  # the record steps its handle, which must still exist
             raise GfsphError(-5, "gfsph_adjoint_backward")
         n = self.sim.n
@@ -471,6 +491,9 @@ class Adjoint:
         _check(lib().gfsph_adjoint_backward(self.h, _fp(gx), _fp(gv), _fp(ghh), _fp(out["x0"]), _fp(out["v0"]),
                                             _fp(out["mass"]), C.byref(mu), C.byref(xi)), "gfsph_adjoint_backward")
         out["tanfi"], out["xi"] = mu.value, xi.value
+        ty = C.c_double()
+        _check(lib().gfsph_adjoint_param(self.h, 2, C.byref(ty)), "gfsph_adjoint_param")
+        out["tauy"] = ty.value  # dL/d(Bingham yield stress, const(6))
         return out
 
     def close(self):

@@ -180,6 +180,16 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt);
 /* One raster per DEM node, nx*ny values, x fastest. */
 int gfsph_raster(gfsph_handle* h, int kind, float* out);
 
+/* Misfit of the depth raster (GFSPH_RASTER_DEPTH_IDW) of the current state
+ * against a target raster T (nx*ny): L = sum over DEM nodes of (R - T)^2, and,
+ * when gx / gh are not NULL, its gradient with respect to the current
+ * positions dL/dx (2,n) and depths dL/dh (n), caller order, zero for
+ * particles outside the DEM.  After gfsph_adjoint_forward these are the
+ * final-state gradients gfsph_adjoint_backward takes (with dL/dv = 0), which
+ * gives dL/d(rheology) and dL/d(volumes) of a deposit-raster calibration.
+ * No counterpart in the reference (it has no back-analysis). */
+int gfsph_raster_misfit(gfsph_handle* h, const float* target, double* loss, float* gx, float* gh);
+
 /* Adds the current particles to the per-node hazard statistics
  * (Get_MC_pixel_Vars_SW, SPH_SW_2019.f90:20717-20833: sum/max of h and |v|
  * over the particles in each node's cell).  Called at plot times. */
@@ -267,9 +277,10 @@ int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_
  * every step from the kept states (each step's neighbour list is held fixed,
  * as the forward step freezes it) and leaves the handle at the final state.
  *
- * Supported: nfric 5/6 with xi >= 0, no erosion or pore pressure, pa_sph 2,
- * sle 0, ic_adapt 0, one grid level (uniform smoothing lengths) and no
- * particle leaving the DEM (GFSPH_ERR_UNSUPPORTED otherwise).
+ * Supported: nfric 5/6 with xi >= 0 and the Bingham law nfric 4, no erosion
+ * or pore pressure, pa_sph 2, sle 0, ic_adapt 0, one grid level (uniform
+ * smoothing lengths) and no particle leaving the DEM (GFSPH_ERR_UNSUPPORTED
+ * otherwise).
  *
  * The record refers to its handle: call gfsph_adjoint_backward only while
  * that handle exists (gfsph_adjoint_destroy does not touch it, so the record
@@ -279,6 +290,13 @@ typedef struct gfsph_adjoint gfsph_adjoint;
 int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint** out);
 int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, const float* gh, float* gx0,
                            float* gv0, float* gm, double* gmu, double* gxi);
+/* One rheology gradient of the last gfsph_adjoint_backward on a: which = 0
+ * dL/dtanfi (const(9)), 1 dL/dxi (const(3)), 2 dL/d(Bingham yield stress,
+ * const(6); nfric 4).  GFSPH_ERR_STATE before the first backward pass. */
+#define GFSPH_ADJ_TANFI 0
+#define GFSPH_ADJ_XI 1
+#define GFSPH_ADJ_TAUY 2
+int gfsph_adjoint_param(gfsph_adjoint* a, int which, double* value);
 int gfsph_adjoint_destroy(gfsph_adjoint* a);
 
 /*
@@ -308,7 +326,8 @@ int gfsph_ensemble_exceedance(gfsph_ensemble* e, float threshold, float* prob);
 
 /*
  * Conjugate gradients of solvegc2 (SPH_GCsolver_2019.f90:16-316) on the device:
- * Jacobi-preconditioned CG on the element-by-element system sum_e gstif_e,
+ * Jacobi-preconditioned CG on the element-by-element system sum_e gstif_e
+ * (every iteration of a solve runs in one persistent cooperative kernel),
  * prescribed dofs (iffix != 0) held at their `fixed` values and masked out
  * of the products (kbyp, :273-313), stop when r.r / r0.r0 <= tol (squared
  * norms, :112), at most 10*ntotv iterations.  Vectors and dot products are
@@ -329,6 +348,10 @@ int gfsph_cg_solve(gfsph_cg* cg, int* iffix, const float* fixed, float* rcg, flo
                    int* iterations);
 int gfsph_cg_destroy(gfsph_cg* cg);
 long long gfsph_cg_launch_count(gfsph_cg* cg);
+/* Device time of the last gfsph_cg_solve on cg (CUDA events around its
+ * kernels: set-up, every iteration, results), without the host copies.  No
+ * counterpart in the reference. */
+int gfsph_cg_device_ms(gfsph_cg* cg, double* ms);
 /* solvegc2 with the reference's argument list (create + solve + destroy). */
 int gfsph_solvegc2(int npoin, int nelem, int nnode, int ndofn, const int* intmat, int* iffix, const float* fixed,
                    const float* gstif, float* rcg, float* ficg, float tol, int* iterations);

@@ -1587,14 +1587,16 @@ int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, dou
 }
 
 /* Forward-mode derivative of nsteps FP64 steps along one direction: the
- * tangents seed_mu of const(9) (tanfi), seed_xi of const(3) (xi), seed_m of
- * the volumes and seed_x, seed_v of the initial positions and velocities.
- * Returns the final positions, velocities and depths and their tangents. */
+ * tangents seed_mu of const(9) (tanfi), seed_xi of const(3) (xi), seed_ty of
+ * const(6) (the Bingham yield stress), seed_m of the volumes and seed_x,
+ * seed_v of the initial positions and velocities.  Returns the final
+ * positions, velocities and depths and their tangents. */
 int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
                    const double* topol, int n, const double* x, const double* v, const double* rho,
                    const double* mass, const double* hsml, const int* flag, int nsteps, double dt, double t,
-                   double seed_mu, double seed_xi, const double* seed_m, const double* seed_x, const double* seed_v,
-                   double* out_x, double* out_v, double* out_h, double* tan_x, double* tan_v, double* tan_h) {
+                   double seed_mu, double seed_xi, double seed_ty, const double* seed_m, const double* seed_x,
+                   const double* seed_v, double* out_x, double* out_v, double* out_h, double* tan_x, double* tan_v,
+                   double* tan_h) {
     if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || n < 0 || nx < 2 || ny < 2) return GFSPH_ERR_ARG;
     if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
     Oracle<Dual, Dual> o;
@@ -1602,6 +1604,7 @@ int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ym
     if (st) return st;
     o.cst[9].d = seed_mu;
     o.cst[3].d = seed_xi;
+    o.cst[6].d = seed_ty;
     o.n = n;
     o.x.resize(2 * (size_t)n); o.v.resize(2 * (size_t)n);
     o.rho.resize(n); o.mass.resize(n); o.hsml.resize(n);

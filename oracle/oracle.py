@@ -117,7 +117,7 @@ def lib(omp=False):
         L.oracle_tangent.restype = C.c_int
         L.oracle_tangent.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                      _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_int, C.c_double, C.c_double,
-                                     C.c_double, C.c_double, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
+                                     C.c_double, C.c_double, C.c_double, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
         L.oracle_get_pwp.restype = C.c_int
         L.oracle_get_pwp.argtypes = [C.c_void_p, _DP]
         L.oracle_free.restype = None
@@ -343,9 +343,9 @@ def gradhs(mode, ix0, iy0, nwx, nwy, dx, dy, x=None, rho=None, flag=None, hs=Non
 
 
 def tangent(params, nx, ny, dx, dy, state, nsteps, seed_mu=0.0, seed_xi=0.0, seed_m=None, seed_x=None,
-            seed_v=None, xmin=0.0, ymin=0.0):
+            seed_v=None, xmin=0.0, ymin=0.0, seed_ty=0.0):
     """FP64 forward-mode derivative of nsteps steps from `state` along one
-    direction (tangents of const(9), const(3), volumes, positions,
+    direction (tangents of const(9), const(3), const(6), volumes, positions,
     velocities): returns (x, v, h, dx, dv, dh) at the end."""
     n = state.x.shape[0]
     out = [np.zeros((n, 2)), np.zeros((n, 2)), np.zeros(n), np.zeros((n, 2)), np.zeros((n, 2)), np.zeros(n)]
@@ -354,7 +354,7 @@ def tangent(params, nx, ny, dx, dy, state, nsteps, seed_mu=0.0, seed_xi=0.0, see
     sv = _d(seed_v) if seed_v is not None else None
     st = lib().oracle_tangent(C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), n, _dp(state.x),
                               _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.hsml), _ip(state.flag),
-                              nsteps, state.dt, state.t, seed_mu, seed_xi, _dp(sm), _dp(sx), _dp(sv),
+                              nsteps, state.dt, state.t, seed_mu, seed_xi, seed_ty, _dp(sm), _dp(sx), _dp(sv),
                               *[_dp(a) for a in out])
     if st:
         raise RuntimeError(f"oracle_tangent: {st}")

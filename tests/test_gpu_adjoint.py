@@ -103,3 +103,180 @@ def test_adjoint_refuses_runs_outside_its_scope(gfsph_lib, oracle_mod):
         gfsph.Adjoint(sim, 5)
     assert e.value.status == gfsph.ERR_UNSUPPORTED
     sim.close()
+
+
+def test_twenty_directions_match_central_differences(gfsph_lib, oracle_mod):
+    """20 seeded random directions in (tanfi, xi, the volumes) at once: the
+    device adjoint's directional derivative against central differences of
+    the FP64 oracle with relative steps of 1e-4, within 1e-4 relative.
+
+    Directions in the initial positions and velocities are checked against
+    the exact FP64 tangent instead (the test above): central differences are
+    ill-posed there.  The release starts at rest, where the Coulomb friction's
+    direction v/|v| is not differentiable (a step in v0 switches the reversal
+    filter from its at-rest to its sliding branch once |v| > 1e-5), and the
+    lattice puts pairs within ~1e-5 m of q = 1, where the reference's cubic
+    spline jumps by 5e-8 W (its 2./3. is a single-precision literal in the
+    FP64 build too, kernel_TOOLS My_SPH_Tools_2019.f90:2101), so steps of
+    positions cross the jump."""
+    w, p, topol = case(oracle_mod)
+    rng = np.random.default_rng(20)
+    gx = rng.normal(size=(w.n, 2)).astype(np.float32)
+    gv = rng.normal(size=(w.n, 2)).astype(np.float32)
+    gh = rng.normal(size=w.n).astype(np.float32)
+    g, _, _ = gpu_gradients(w, p, topol, gx, gv, gh)
+    ny, nx = w.z.shape
+    eps = 1e-4
+    m64 = w.mass.astype(np.float64)
+
+    def loss(q, mass):
+        st = oracle_mod.State(w.x, w.v, w.rho, mass, w.hsml, topol, dt=p.dt)
+        oracle_mod.run(oracle_mod.MODE_FP64, q, nx, ny, w.dx, w.dy, st, NSTEPS)
+        return float((gx * st.x).sum() + (gv * st.v).sum() + (gh * st.rho).sum())
+
+    worst = 0.0
+    for k in range(20):
+        u = rng.normal(size=2)
+        dm = rng.normal(size=w.n) * w.mass
+        qp = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+        qm = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+        for idx, ui in ((8, u[0]), (2, u[1])):  # tanfi = const(9), xi = const(3)
+            qp.cst[idx] = p.cst[idx] * (1 + eps * ui)
+            qm.cst[idx] = p.cst[idx] * (1 - eps * ui)
+        fd = (loss(qp, m64 + eps * dm) - loss(qm, m64 - eps * dm)) / (2 * eps)
+        # the parameters travel as FP32: the steps actually taken
+        dmu = (float(qp.cst[8]) - float(qm.cst[8])) / (2 * eps)
+        dxi = (float(qp.cst[2]) - float(qm.cst[2])) / (2 * eps)
+        got = g["tanfi"] * dmu + g["xi"] * dxi + float((g["mass"].astype(np.float64) * dm).sum())
+        rel = abs(got - fd) / abs(fd)
+        worst = max(worst, rel)
+        assert rel <= 1e-4, (k, got, fd, rel)
+    print(f"worst relative difference over 20 directions: {worst:.2e}")
+
+
+def test_bingham_yield_stress_gradient(gfsph_lib, oracle_mod):
+    """dL/d(yield stress const(6)) of the Bingham law (nfric 4) against the
+    FP64 forward-mode oracle, with the positions and volumes."""
+    w = workloads.fractal_channel(n_target=3000, dem_k=8, cell=5.0, erosion=None)
+    w.const = {**w.const, 5: 4, 6: 1000.0, 7: 50.0, 3: 0.0, 9: 0.0}
+    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv, mode=oracle_mod.MODE_FP32)
+    rng = np.random.default_rng(6)
+    gx = rng.normal(size=(w.n, 2)).astype(np.float32)
+    gv = rng.normal(size=(w.n, 2)).astype(np.float32)
+    gh = rng.normal(size=w.n).astype(np.float32)
+    g, final, _ = gpu_gradients(w, p, topol, gx, gv, gh)
+    assert np.abs(final["v"]).max() > 0.1
+    ny, nx = w.z.shape
+    st0 = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+
+    def directional(**seed):
+        _, _, _, dx, dv, dh = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, NSTEPS, **seed)
+        return float((gx * dx).sum() + (gv * dv).sum() + (gh * dh).sum())
+
+    ref = directional(seed_ty=1.0)
+    assert ref != 0.0 and abs(g["tauy"] - ref) <= 2e-4 * abs(ref), (g["tauy"], ref)
+    dm = rng.normal(size=w.n) * w.mass
+    ref = directional(seed_m=dm)
+    assert abs(float((g["mass"] * dm).sum()) - ref) <= 2e-4 * abs(ref)
+    dx0 = rng.normal(size=(w.n, 2))
+    ref = directional(seed_x=dx0)
+    assert abs(float((g["x0"] * dx0).sum()) - ref) <= 2e-4 * abs(ref)
+    assert g["tanfi"] == 0.0  # no frictional term under the Bingham law
+
+
+def idw_raster64(w, x, h):
+    """The depth raster of SPH_SW_2019.f90:14310-14400 in FP64 (numpy): IDW of h
+    over the 4x4 DEM nodes around each particle."""
+    ny, nx = w.z.shape
+    a1 = np.zeros(nx * ny)
+    a5 = np.zeros(nx * ny)
+    distg = np.hypot(w.dx, w.dy)
+    ipx = ((x[:, 0] - 0.0) / w.dx + 1.0).astype(np.int64)
+    ipy = ((x[:, 1] - 0.0) / w.dy + 1.0).astype(np.int64)
+    for ox in range(-1, 3):
+        for oy in range(-1, 3):
+            ix, iy = ipx + ox, ipy + oy
+            ok = (ix >= 1) & (ix <= nx) & (iy >= 1) & (iy <= ny)
+            d = np.hypot(x[ok, 0] - (ix[ok] - 1) * w.dx, x[ok, 1] - (iy[ok] - 1) * w.dy)
+            wgt = distg / np.maximum(d, 1e-6)
+            ip = (iy[ok] - 1) * nx + (ix[ok] - 1)
+            np.add.at(a1, ip, h[ok] * wgt)
+            np.add.at(a5, ip, wgt)
+    return np.where(a5.astype(np.float32) >= 1e-6, a1 / np.where(a5 > 0, a5, 1.0), a1)
+
+
+def test_raster_misfit_and_its_gradient(gfsph_lib, oracle_mod):
+    """gfsph_raster_misfit: L = sum (R - T)^2 of the IDW depth raster against a
+    target, and dL/dx, dL/dh against central differences of an FP64 raster
+    (steps of 1e-6 m and 1e-6 relative, small enough that no particle changes
+    DEM cell)."""
+    w = workloads.fractal_channel(n_target=3000, dem_k=8, cell=5.0, erosion=None)
+    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    sim.step(10)
+    st = sim.download()
+    rng = np.random.default_rng(8)
+    target = (sim.raster(gfsph.RASTER_DEPTH_IDW) * rng.uniform(0.5, 1.5, size=w.z.shape)).astype(np.float32)
+    loss, gx, gh = sim.raster_misfit(target)
+    sim.close()
+    x64, h64 = st["x"].astype(np.float64), st["rho"].astype(np.float64)
+    t64 = target.astype(np.float64).reshape(-1)
+    L64 = float(((idw_raster64(w, x64, h64) - t64) ** 2).sum())
+    assert abs(loss - L64) <= 1e-5 * L64
+    for k in range(3):
+        dx = rng.normal(size=x64.shape)
+        dh = rng.normal(size=h64.shape) * h64
+        e = 1e-6
+        lp = float(((idw_raster64(w, x64 + e * dx, h64 + e * dh) - t64) ** 2).sum())
+        lm = float(((idw_raster64(w, x64 - e * dx, h64 - e * dh) - t64) ** 2).sum())
+        fd = (lp - lm) / (2 * e)
+        got = float((gx.astype(np.float64) * dx).sum() + (gh.astype(np.float64) * dh).sum())
+        assert abs(got - fd) <= 1e-4 * abs(fd), (k, got, fd)
+
+
+def test_calibration_gradient_of_the_deposit_misfit(gfsph_lib, oracle_mod):
+    """The deposit-raster calibration loss end to end: a target raster T from
+    a run at mu = 0.18, xi = 350; L = sum (R - T)^2 after 100 steps at
+    mu = 0.15, xi = 400; dL/dmu and dL/dxi from gfsph_raster_misfit followed
+    by gfsph_adjoint_backward.  The reference is exact in FP64: the oracle's
+    forward-mode tangents of the final positions and depths, composed with the
+    gradient of the FP64 raster misfit (central differences of the raster
+    along the tangent, steps of 1e-7 m that cross no DEM cell edge; central
+    differences of the whole trajectory would be polluted by particles that
+    cross one and jump the raster).  The misfit is ~1% of the raster after
+    100 steps, so the FP32 trajectory's ~1e-5 drift from FP64 enters L and
+    its gradient about 100-fold: the tolerance is 5e-3."""
+    w, p, topol = case(oracle_mod)
+    N = 100
+    ny, nx = w.z.shape
+    pt = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    pt.cst[8], pt.cst[2] = 0.18, 350.0
+    st = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    oracle_mod.run(oracle_mod.MODE_FP64, pt, nx, ny, w.dx, w.dy, st, N)
+    target = idw_raster64(w, st.x, st.rho).astype(np.float32).reshape(ny, nx)
+    t64 = target.astype(np.float64).reshape(-1)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy, topol=topol.astype(np.float32))
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    adj = gfsph.Adjoint(sim, N, every=10)
+    loss, gxr, ghr = sim.raster_misfit(target)
+    g = adj.backward(gxr, np.zeros_like(gxr), ghr)
+    adj.close()
+    sim.close()
+    s0 = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    oracle_mod.run(oracle_mod.MODE_FP64, p, nx, ny, w.dx, w.dy, s0, N)
+
+    def L(x, h):
+        return float(((idw_raster64(w, x, h) - t64) ** 2).sum())
+
+    L64 = L(s0.x, s0.rho)
+    assert abs(loss - L64) <= 5e-3 * L64, (loss, L64)
+    st0 = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    for key, seed in (("tanfi", "seed_mu"), ("xi", "seed_xi")):
+        _, _, _, tx, _, th = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, N, **{seed: 1.0})
+        tau = 1e-7 / np.abs(tx).max()
+        ref = (L(s0.x + tau * tx, s0.rho + tau * th) - L(s0.x - tau * tx, s0.rho - tau * th)) / (2 * tau)
+        rel = abs(g[key] - ref) / abs(ref)
+        print(f"dL/d{key}: device {g[key]:.6e}, FP64 {ref:.6e}, relative difference {rel:.2e}")
+        assert rel <= 5e-3, (key, g[key], ref)

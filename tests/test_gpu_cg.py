@@ -84,3 +84,34 @@ def test_solvegc2_one_shot_matches_handle(gfsph_lib):
                           gfsph._fp(rr), gfsph._fp(xx), 1e-16, C.byref(its))
     assert st == 0 and its.value == it
     assert np.array_equal(xx, x) and np.array_equal(rr, r)
+
+
+def test_persistent_cg_residual_determinism_and_launches(gfsph_lib, oracle_mod):
+    """Every iteration runs inside one cooperative launch (four kernels per
+    solve: set-up, preconditioner and residual, the iterations, results); the
+    returned residual is solvegc2's (the one before the last update), and two
+    solves are bit-identical."""
+    intmat, coords, g, b = mass_system(41, 37)
+    b32 = b.astype(np.float32)
+    cg = gfsph.CG(intmat, g.astype(np.float32))
+    l0 = cg.launch_count()
+    x, r, fix, it = cg.solve(b32, tol=1e-8)
+    assert cg.launch_count() - l0 == 4
+    assert cg.device_ms() > 0.0
+    xo, ro, fo, ito = oracle_mod.solvegc2(2, intmat, g.astype(np.float32).astype(np.float64),
+                                         b32.astype(np.float64), tol=1e-8)
+    assert it == ito
+    assert np.allclose(x, xo, rtol=1e-6, atol=1e-6)
+    assert np.allclose(r, ro, rtol=1e-5, atol=1e-6 * np.abs(ro).max())
+    x2, r2, _, it2 = cg.solve(b32, tol=1e-8)
+    assert it2 == it and np.array_equal(x2, x) and np.array_equal(r2, r)
+    cg.close()
+
+
+def test_cg_zero_system_is_not_iterated(gfsph_lib):
+    """rnormX below the tolerance (:93-103): the solution is 0, no iteration."""
+    intmat, coords, g, b = mass_system(9, 7)
+    cg = gfsph.CG(intmat, g.astype(np.float32))
+    x, r, fix, it = cg.solve(np.zeros(coords.shape[0], np.float32), tol=1e-10)
+    assert it == 0 and np.all(x == 0.0) and np.all(r == 0.0)
+    cg.close()

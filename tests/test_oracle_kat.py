@@ -483,6 +483,35 @@ def test_tangent_oracle_matches_central_differences(oracle_mod):
     assert abs(fd - tg) <= 1e-5 * abs(tg)
 
 
+def test_tangent_oracle_yield_stress_matches_central_differences(oracle_mod):
+    """The same along the Bingham yield stress const(6) (nfric 4,
+    SPH_SW_2019.f90:9552-9572) on a sliding release."""
+    w = workloads.fractal_channel(n_target=2000, dem_k=7, cell=5.0, erosion=None)
+    w.const = {**w.const, 5: 4, 6: 1000.0, 7: 50.0, 3: 0.0, 9: 0.0}
+    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv, mode=oracle_mod.MODE_FP64)
+    st0 = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=0.01)
+    rng = np.random.default_rng(3)
+    gx, gv, gh = rng.normal(size=(w.n, 2)), rng.normal(size=(w.n, 2)), rng.normal(size=w.n)
+
+    def loss(q):
+        st = st0.copy()
+        oracle_mod.run(oracle_mod.MODE_FP64, q, nx, ny, w.dx, w.dy, st, 20)
+        assert np.abs(st.v).max() > 0.1  # the flow moves
+        return float((gx * st.x).sum() + (gv * st.v).sum() + (gh * st.rho).sum())
+
+    qp = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    qm = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    qp.cst[5] = p.cst[5] * (1 + 1e-4)
+    qm.cst[5] = p.cst[5] * (1 - 1e-4)
+    fd = (loss(qp) - loss(qm)) / (float(qp.cst[5]) - float(qm.cst[5]))
+    _, _, _, dx, dv, dh = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, 20, seed_ty=1.0)
+    tg = float((gx * dx).sum() + (gv * dv).sum() + (gh * dh).sum())
+    assert tg != 0.0
+    assert abs(fd - tg) <= 1e-5 * abs(tg), (fd, tg)
+
+
 def f32(x):
     """The value a single-precision parameter carries into the FP64 oracle."""
     return float(np.float32(x))
