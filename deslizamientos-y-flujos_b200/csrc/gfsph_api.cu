@@ -127,6 +127,7 @@ struct gfsph_handle {
     // DEM
     int nx = 0, ny = 0;
     DemView dem;
+    bool dem_shared = false;    // the slope and curvature rows belong to another handle (ensembles)
     float2* d_grad = nullptr;
     float4* d_curvA = nullptr;
     float2* d_curvB = nullptr;
@@ -774,7 +775,37 @@ const char* gfsph_strerror(int s) {
 int gfsph_num_kernels(void) { return K_COUNT; }
 const char* gfsph_kernel_name(int k) { return (k >= 0 && k < K_COUNT) ? kKernelNames[k] : nullptr; }
 
+}  // extern "C"
+
+namespace {
+
+__global__ void k_fill(float* a, size_t n, float v) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) a[k] = v;
+}
+
+// gfsph_create; with `share` the new handle uses share's device copy of the
+// DEM slope and curvature rows (which erosion never changes) instead of its
+// own, and takes its own copies of Z and the eroded depth from share (which
+// must not have stepped yet) and its erodible depth from its parameters
+// (Input_SW SPH_SW_2019.f90:1288-1307) or from share when the DEM was given
+// as topol rows.  share must outlive the new handle.
+int create_handle(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle* share, gfsph_handle** out);
+
+}  // namespace
+
+extern "C" {
+
 int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out) try {
+    return create_handle(p, dem, nullptr, out);
+} catch (...) {  // a C++ exception never crosses the C ABI
+    return GFSPH_ERR_HOST;
+}
+
+}  // extern "C"
+
+namespace {
+
+int create_handle(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle* share, gfsph_handle** out) {
     if (!p || !dem || !out) return GFSPH_ERR_ARG;
     *out = nullptr;
     int st = validate(p);
@@ -821,9 +852,33 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     c.mu_a = k[2]; c.mu_r = k[5]; c.mu_b = k[6];
     if (c.muI) c.xi = 0.f;  // const(3) is a mu(I) parameter, not xi (:9653)
 
-    // DEM rows on the host, as Topo_main leaves them before the time loop
     int nx = dem->nx, ny = dem->ny;
     size_t np = (size_t)nx * ny;
+    if (share) {
+        if (share->nx != nx || share->ny != ny) { gfsph_destroy(h); return GFSPH_ERR_ARG; }
+        h->nx = nx; h->ny = ny;
+        h->dem_shared = true;
+        h->d_grad = share->d_grad; h->d_curvA = share->d_curvA; h->d_curvB = share->d_curvB;
+        st = 0;
+        st |= dalloc(&h->d_z, np); st |= dalloc(&h->d_eroded, np); st |= dalloc(&h->d_avail, np);
+        st |= dalloc(&h->d_auxv, np);
+        st |= dalloc(&h->S, 1);
+        st |= dalloc(&h->bparts, kBoundsBlocks);
+        if (st) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
+        if (cudaMallocHost((void**)&h->hS, sizeof(StepScalars)) != cudaSuccess) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
+        cudaMemcpy(h->d_z, share->d_z, np * sizeof(float), cudaMemcpyDeviceToDevice);
+        cudaMemcpy(h->d_eroded, share->d_eroded, np * sizeof(float), cudaMemcpyDeviceToDevice);
+        if (dem->topol) {
+            cudaMemcpy(h->d_avail, share->d_avail, np * sizeof(float), cudaMemcpyDeviceToDevice);
+        } else {
+            float avail = 0.f;
+            if (k[20] > 1.e-9f) avail = (k[47] > 1.e-6f) ? k[47] : 999.f;
+            k_fill<<<blocks_for((long long)np, 256), 256>>>(h->d_avail, np, avail);
+        }
+        cudaMemset(h->d_auxv, 0, np * sizeof(double2));
+        h->dem = share->dem;  // (the synchronous copy of the scalars below orders the fill before any step)
+    } else {
+    // DEM rows on the host, as Topo_main leaves them before the time loop
     std::vector<float> topol, z, er, av;
     std::vector<float2> grad, curvB;
     std::vector<float4> curvA;
@@ -876,6 +931,7 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     d.xmax = d.xmin + (float)(nx - 1) * d.dx;
     d.ymax = d.ymin + (float)(ny - 1) * d.dy;
     d.grad = h->d_grad; d.curvA = h->d_curvA; d.curvB = h->d_curvB;
+    }
     std::memset(h->hS, 0, sizeof(StepScalars));
     h->hS->dt = p->dt;
     h->hS->time = 0.0;
@@ -888,9 +944,11 @@ int gfsph_create(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle** out
     if (cudaGetLastError() != cudaSuccess) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
     *out = h;
     return GFSPH_OK;
-} catch (...) {  // a C++ exception never crosses the C ABI
-    return GFSPH_ERR_HOST;
 }
+
+}  // namespace
+
+extern "C" {
 
 int gfsph_destroy(gfsph_handle* h) try {
     if (!h) return GFSPH_ERR_ARG;
@@ -898,7 +956,8 @@ int gfsph_destroy(gfsph_handle* h) try {
     drop_graphs(h);
     free_particles(h);
     dfree(h->count); dfree(h->start); dfree(h->tile_sum); dfree(h->bmark); dfree(h->bstart);
-    dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
+    if (!h->dem_shared) { dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); }
+    dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
     dfree(h->d_auxv); dfree(h->S); dfree(h->bparts); dfree(h->d_racc); dfree(h->d_rout); dfree(h->d_lam);
     dfree(h->d_lpart);
     dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
@@ -1486,19 +1545,26 @@ int gfsph_ensemble_create(const gfsph_params* params, const gfsph_dem* dem, int 
         return GFSPH_ERR_HOST;
     }
     e->nx = dem->nx; e->ny = dem->ny;
+    // member 0 holds the one device copy of the DEM slope and curvature rows;
+    // the others use it and keep their own Z, eroded and erodible depth
     for (int r = 0; r < nreal; r++) {
-        gfsph_dem dm = d;
-        if (!dem->topol) {  // erodible depth per member (Input_SW SPH_SW_2019.f90:1288-1307)
-            const float* k = params[r].cst;
-            float avail = 0.f;
-            if (k[20] > 1.e-9f) avail = (k[47] > 1.e-6f) ? k[47] : 999.f;
-            size_t np = (size_t)dem->nx * dem->ny;
-            for (size_t ip = 0; ip < np; ip++) topol[ip * GFSPH_NTOPO + 14] = avail;
-            dm.topol = topol.data();
-            dm.ntopo = GFSPH_NTOPO;
-        }
         gfsph_handle* h = nullptr;
-        int st = gfsph_create(&params[r], &dm, &h);
+        int st;
+        if (r == 0) {
+            gfsph_dem dm = d;
+            if (!dem->topol) {  // erodible depth of member 0 (Input_SW SPH_SW_2019.f90:1288-1307)
+                const float* k = params[0].cst;
+                float avail = 0.f;
+                if (k[20] > 1.e-9f) avail = (k[47] > 1.e-6f) ? k[47] : 999.f;
+                size_t np = (size_t)dem->nx * dem->ny;
+                for (size_t ip = 0; ip < np; ip++) topol[ip * GFSPH_NTOPO + 14] = avail;
+                dm.topol = topol.data();
+                dm.ntopo = GFSPH_NTOPO;
+            }
+            st = gfsph_create(&params[0], &dm, &h);
+        } else {
+            st = create_handle(&params[r], dem, e->members[0], &h);
+        }
         if (st) { gfsph_ensemble_destroy(e); return st; }
         e->members.push_back(h);
     }
@@ -1510,7 +1576,8 @@ int gfsph_ensemble_create(const gfsph_params* params, const gfsph_dem* dem, int 
 
 int gfsph_ensemble_destroy(gfsph_ensemble* e) try {
     if (!e) return GFSPH_ERR_ARG;
-    for (gfsph_handle* h : e->members) gfsph_destroy(h);
+    // member 0 last: the others use its DEM rows
+    for (size_t r = e->members.size(); r-- > 0;) gfsph_destroy(e->members[r]);
     dfree(e->d_maxptr);
     dfree(e->d_prob);
     delete e;

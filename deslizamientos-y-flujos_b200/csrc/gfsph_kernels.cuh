@@ -836,18 +836,14 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
 
 // Neighbour search and summation density of the regular particles, fused:
 // every j with r < 2*(hi+hj)/2 (the pair set of grid_find, :987-1060), on
-// every level, is appended to the neighbour table (tab_base),
-// and h_i = W(0,h_i) m_i + sum_j m_j W_ij (sum_density_Tools :1796-1836) is
-// accumulated in FP64.  Also stores the pressure term of IntForces_SW with h
-// clamped to h_inf (:6769, :6797): p/h^2 (pa_sph 2) or p (pa_sph 1).
-// Instantiated for both cell layouts; the launch whose layout this step does
-// not use returns at once.  Held to 40 registers (12 blocks of 128 per SM):
-// the gathers are latency-bound, and 12 resident blocks beat 10 with the
-// 45 registers the compiler would take (4 % on the whole step).
+// every level, is appended to the neighbour table (tab_base) with the pair's
+// kernel value and gradient, and h_i = W(0,h_i) m_i + sum_j m_j W_ij
+// (sum_density_Tools :1796-1836) is accumulated in FP64.  Also stores the
+// pressure term of IntForces_SW with h clamped to h_inf (:6769, :6797): p/h^2
+// (pa_sph 2) or p (pa_sph 1).
 template <bool SPARSE, int SKF>
-__global__ void __launch_bounds__(128, 10) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+__device__ __forceinline__ void density_regular(PState& A, const Search& Q, StepScalars* S, const Rheo& c) {
     constexpr int SK = SupportScale<SKF>::value;
-    if (S->skip || (S->sparse != 0) != SPARSE) return;
     const int nreg = S->nreg, nlev = S->nlev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
         float4 me = Q.xhm[i];
@@ -883,6 +879,16 @@ __global__ void __launch_bounds__(128, 10) k_density(PState A, Search Q, StepSca
         Q.pterm[i] = pt;
         Q.pr[i] = make_float4(pt, h, me.w, 0.f);
     }
+}
+
+// Instantiated for both cell layouts; the launch whose layout this step does
+// not use returns at once (one kernel with both walks would spill in the
+// dense walk).  Held to 48 registers (10 blocks of 128 per SM): the gathers
+// are latency-bound.
+template <bool SPARSE, int SKF>
+__global__ void __launch_bounds__(128, 10) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+    if (S->skip || (S->sparse != 0) != SPARSE) return;
+    density_regular<SPARSE, SKF>(A, Q, S, c);
 }
 
 // Visits every neighbour j of particle i cooperatively over one warp: the

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <fstream>
 #include <sstream>
@@ -258,8 +259,11 @@ SwDat read_dat(const std::string& path) {
         v = r.values(2);
         d.icunk_s = (int)to_real(v[0], path);
         d.h_inf = to_real(v[1], path);
-        if (d.icunk_s != 7 && d.icunk_s != 8)
-            throw std::runtime_error(path + ": icunk_s " + std::to_string(d.icunk_s) + " is not supported (7, 8 are)");
+        if (d.icunk_s != 7 && d.icunk_s != 8 && d.icunk_s != 200)
+            throw std::runtime_error(path + ": icunk_s " + std::to_string(d.icunk_s) +
+                                     " is not supported (7, 8 and the restart 200 are)");
+        // the pts name (Read_Source_plus_New :5058-5059) or, for a restart,
+        // the problem name (Get_Restart_Info_SW :3302-3305): a label and a name
         r.label();
         d.pts_name = split_items(r.label()).at(0);
     }
@@ -387,6 +391,70 @@ Particles read_pts(const std::string& path, float h_inf, int icunk_s, float xshi
     P.facthsml = facthsml;
     P.np_src = np_src;
     return P;
+}
+
+RestartState read_restart(const std::string& path) {
+    FortranReader r(path);
+    RestartState s;
+    r.label();                          // ' ----- npoin_s      time at restart ----- '
+    auto v = r.values(2);               // npoin_s, time_sph_restart (:3312)
+    const long long n = (long long)to_real(v[0], path);
+    if (n < 1 || n > 0x7fffffffLL) throw std::runtime_error(path + ": npoin_s out of range");
+    s.time = std::strtod(v[1].c_str(), nullptr);
+    r.label();                          // the column header
+    s.itype.resize(n); s.x.resize(2 * n); s.v.resize(2 * n);
+    s.h.resize(n); s.mass.resize(n); s.hsml.resize(n); s.pwp.resize(n);
+    for (long long i = 0; i < n; i++) {  // ipoin, itype, x, y, vx, vy, h, mass, hsml, u (:3318-3319)
+        v = r.values(10);
+        s.itype[i] = (int)to_real(v[1], path);
+        s.x[2 * i] = to_real(v[2], path); s.x[2 * i + 1] = to_real(v[3], path);
+        s.v[2 * i] = to_real(v[4], path); s.v[2 * i + 1] = to_real(v[5], path);
+        s.h[i] = to_real(v[6], path); s.mass[i] = to_real(v[7], path);
+        s.hsml[i] = to_real(v[8], path); s.pwp[i] = to_real(v[9], path);
+    }
+    return s;
+}
+
+TopoRestart read_topo_restart(const std::string& path, int npoig) {
+    FortranReader r(path);
+    TopoRestart t;
+    r.label();
+    auto v = r.values(2);               // npoig, time (:2904)
+    if ((long long)to_real(v[0], path) != npoig)
+        throw std::runtime_error(path + ": its node count differs from the DEM's");
+    t.time = std::strtod(v[1].c_str(), nullptr);
+    r.label();
+    t.z.resize(npoig); t.eroded.resize(npoig); t.avail.resize(npoig);
+    for (int i = 0; i < npoig; i++) {   // ip, Topol(1), Topol(14), Topol(15) (:2910)
+        v = r.values(4);
+        t.z[i] = to_real(v[1], path); t.eroded[i] = to_real(v[2], path); t.avail[i] = to_real(v[3], path);
+    }
+    return t;
+}
+
+void write_restart(const std::string& path, const RestartState& s) {
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + path);
+    std::fprintf(f, " ----- npoin_s      time at restart -----  %.17G\n", s.time);
+    std::fprintf(f, " %d %.17G\n", s.n(), s.time);
+    std::fprintf(f, " ipoin...itype....x ............   y ..........   vx............. vy ..........   h........   "
+                    "mass..........   hsml ..........   pwp   \n");
+    for (int i = 0; i < s.n(); i++)
+        std::fprintf(f, "%7d  %5d  %16.9E  %16.9E  %16.9E  %16.9E  %16.9E  %16.9E  %16.9E  %16.9E\n", i + 1, s.itype[i],
+                     (double)s.x[2 * i], (double)s.x[2 * i + 1], (double)s.v[2 * i], (double)s.v[2 * i + 1],
+                     (double)s.h[i], (double)s.mass[i], (double)s.hsml[i], (double)s.pwp[i]);
+    if (std::fclose(f) != 0) throw std::runtime_error("cannot write " + path);
+}
+
+void write_topo_restart(const std::string& path, const TopoRestart& t) {
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + path);
+    std::fprintf(f, " ----- npoig      time at restart -----  %.17G\n", t.time);
+    std::fprintf(f, " %zu %.17G\n", t.z.size(), t.time);
+    std::fprintf(f, " ipoig...Topol (1,:)....Topol (14,:) ..........Topol (16,:)  \n");
+    for (size_t i = 0; i < t.z.size(); i++)
+        std::fprintf(f, "%7zu    %16.9E  %16.9E  %16.9E\n", i + 1, (double)t.z[i], (double)t.eroded[i], (double)t.avail[i]);
+    if (std::fclose(f) != 0) throw std::runtime_error("cannot write " + path);
 }
 
 }  // namespace gfsph_host

@@ -35,9 +35,9 @@ struct TopoData {
 struct SwDat {
     int ic_swalg = 0, n_hist = 0, ndimn = 2;
     int ic_soil = 1, ic_water = 0, ic_vps = 0, ic_abs = 0;
-    int icunk_s = 7;
+    int icunk_s = 7;            // 7, 8: .pts source; 200: restart (Get_Restart_Info_SW)
     float h_inf = 0.01f;
-    std::string pts_name;
+    std::string pts_name;       // the .pts name, or the problem name of a restart
     int pa_sph = 2, nnps = 2, sle = 1, skf = 1;
     bool sum_den = true, av_vel = true, virt_part = false, nor_dens = false;
     float cst[110] = {};        // const(1..110)
@@ -55,11 +55,36 @@ struct Particles {
     int n() const { return (int)h.size(); }
 };
 
+// A restart state: OutputSave_SW writes it (SPH_SW_2019.f90:12416-12460),
+// Get_Restart_Info_SW reads it (:3270-3337) when icunk_s = 200.
+struct RestartState {
+    double time = 0.0;
+    std::vector<int> itype;
+    std::vector<float> x, v;    // (2, n)
+    std::vector<float> h, mass, hsml, pwp;
+    int n() const { return (int)h.size(); }
+};
+
+// The eroded DEM rows of a restart: Topol(1), Topol(14), Topol(15) per node
+// (OutputSave_SW :12473-12481, Get_Topo_restart SPH_FEM_topo_2019.f90:2883-2920).
+struct TopoRestart {
+    double time = 0.0;
+    std::vector<float> z, eroded, avail;
+};
+
 // Each reader throws std::runtime_error with the file and the item on failure.
 MasterDat read_master(const std::string& path);
 TopoData read_top(const std::string& path);
 SwDat read_dat(const std::string& path);
 Particles read_pts(const std::string& path, float h_inf, int icunk_s, float xshift, float yshift);
+RestartState read_restart(const std::string& path);
+TopoRestart read_topo_restart(const std::string& path, int npoig);
+// Writers of the same files.  The fields and their order are the
+// reference's; the numbers carry 9 significant digits (17 for the time)
+// instead of its g14.7, so that an FP32 state is read back bit for bit (the
+// reference reads these files list-directed, whatever the width).
+void write_restart(const std::string& path, const RestartState& s);
+void write_topo_restart(const std::string& path, const TopoRestart& t);
 
 // Fortran list-directed and a60-label reading over a text file.
 class FortranReader {

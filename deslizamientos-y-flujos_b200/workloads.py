@@ -269,12 +269,14 @@ def p1_mass_matrices(intmat, coords):
     return (a2 / 24.0)[:, None, None] * m[None, :, :]
 
 
-def write_reference_inputs(w, directory, name):
+def write_reference_inputs(w, directory, name, out_step=100, restart=False):
     """Writes a workload in the reference's own input formats, so that the
     Fortran program (or gfsph_run) can read it: <name>.MASTER.dat,
     <name>.dat, <name>.top (ictop = 100: a grid file with finite-difference
     slopes) and <name>.pts (the particles as source points on their
-    lattice).  w.options may carry icpwp (0 or 3) and pwp0rel."""
+    lattice).  w.options may carry icpwp (0 or 3) and pwp0rel.  out_step is
+    print_step = save_step = plot_step; restart=True writes icunk_s = 200,
+    which reads the particles from restart.dat (Get_Restart_Info_SW)."""
     import os
     os.makedirs(directory, exist_ok=True)
     o = w.options
@@ -299,14 +301,18 @@ def write_reference_inputs(w, directory, name):
         f.write("SPH_problem_type SPH_t_integ_Alg\n  1 4\n")
         f.write("sph problem name\n" + name + "\n")
         f.write("dt time_end maxtimesteps\n  %g %g 1000000\n" % (dt, dt * w.steps))
-        f.write("print_step save_step plot_step\n  100 100 100\n")
+        f.write("print_step save_step plot_step\n  %d %d %d\n" % (out_step, out_step, out_step))
         f.write("dt_sph ic_adapt\n  %g %d\n" % (dt, o["ic_adapt"]))
         f.write("Ntime curves max pts\n  0 6\nwin\n0\n")
     with open(os.path.join(directory, name + ".dat"), "w") as f:
         f.write("1\n " + name + "\n ic_SW_Alg\n  0\nnhist\n  0\nndimn\n  2\n")
         f.write("ic_soil ic_water ic_vps ic_abs\n  1 0 0 0\n")
-        f.write("Soil unkno h_inf_SW\n  7 %g\n" % o["h_inf"])
-        f.write("pts file name\n  " + name + "\n")
+        if restart:
+            f.write("Soil unkno h_inf_SW\n  200 %g\n" % o["h_inf"])
+            f.write("problem name (restart)\n  " + name + "\n")
+        else:
+            f.write("Soil unkno h_inf_SW\n  7 %g\n" % o["h_inf"])
+            f.write("pts file name\n  " + name + "\n")
         f.write("pa_sph nnps sle skf\n  %d %d %d %d\n" % (o["pa_sph"], o["nnps"], o["sle"], o["skf"]))
         f.write("sum_den av_vel virt_part nor_dens\n  T %s F F\n" % ("T" if o["average_velocity"] else "F"))
         for b in range(blocks):

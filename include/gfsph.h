@@ -306,7 +306,9 @@ int gfsph_adjoint_destroy(gfsph_adjoint* a);
  * and xi = const(3)) and particles, advanced together: every member's graph
  * launches go out on its own stream before any wait, so small realizations
  * share the GPU.  Each member is an ordinary handle (gfsph_ensemble_member)
- * for upload, download and rasters; its DEM copy erodes independently.  The
+ * for upload, download and rasters.  The DEM slope and curvature rows (which
+ * erosion does not change) are one device copy for all members; each member
+ * keeps its own Z, eroded and erodible depth, which erode independently.  The
  * ensemble owns its members: gfsph_ensemble_destroy frees them, and a
  * member must not be passed to gfsph_destroy.
  */

@@ -91,3 +91,27 @@ def test_rejects_mixed_dem_derivatives(gfsph_lib):
     with pytest.raises(gfsph.GfsphError) as e:
         gfsph.Ensemble([p0, p1], w.z, dx=w.dx, dy=w.dy)
     assert e.value.status == gfsph.ERR_ARG
+
+
+def test_members_match_the_oracle(gfsph_lib, oracle_mod):
+    """Two members of an ensemble (sharing the DEM rows of member 0) against
+    the oracle in the GPU's precision scheme: the first member and the last."""
+    w = workloads.fractal_channel(n_target=3000, dem_k=8, cell=5.0)
+    params, parts = realizations(w, 6, seed=3)
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=params[0].dem_deriv, mode=oracle_mod.MODE_FP32)
+    ens = gfsph.Ensemble(params, w.z, dx=w.dx, dy=w.dy)
+    for m, pr in zip(ens.members, parts):
+        m.upload(*pr)
+    ens.step(10)
+    ny, nx = w.z.shape
+    for r in (0, 5):
+        x, v, rho, mass, hsml = parts[r]
+        st = oracle_mod.State(x, v, rho, mass, hsml, topol, dt=params[r].dt)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, params[r], nx, ny, w.dx, w.dy, st, 10)
+        g = ens.members[r].download()
+        assert np.array_equal(g["flag"], st.flag)
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
+            ref = np.asarray(ref, np.float64)
+            err = np.linalg.norm(g[key] - ref) / np.linalg.norm(ref)
+            assert err <= 1e-5, (r, key, err)
+    ens.close()

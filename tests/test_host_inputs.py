@@ -118,3 +118,39 @@ def test_damaged_inputs_are_refused_with_a_message(gfsph_lib, tmp_path, ext, how
     out = subprocess.run([RUN, "plane", "--dir", str(dst), "--parse-only"], capture_output=True, text=True)
     assert out.returncode == 2, (out.returncode, out.stderr)
     assert "plane" in out.stderr
+
+
+def test_restart_input_reads_the_reference_layout(gfsph_lib, tmp_path):
+    """icunk_s = 200: the particles come from restart.dat, written here in the
+    layout of OutputSave_SW (SPH_SW_2019.f90:12416-12460: two header lines,
+    npoin_s and the time, a column header, then i7, i5 and 8 values per line
+    in g14.7); the driver reads them list-directed as Get_Restart_Info_SW
+    does (:3270-3337) and hands them to the step unchanged."""
+    import workloads
+    w = workloads.inclined_plane()
+    workloads.write_reference_inputs(w, str(tmp_path), "plane", restart=True)
+    rng = np.random.default_rng(4)
+    v = rng.normal(size=(w.n, 2)).astype(np.float32)
+    pwp = np.zeros(w.n, np.float32)
+    with open(tmp_path / "restart.dat", "w") as f:
+        f.write(" ----- npoin_s      time at restart -----    12.50000    \n")
+        f.write("        %d   12.50000    \n" % w.n)
+        f.write(" ipoin...itype....x ............   y ..........   vx............. vy ..........   h........   "
+                "mass..........   hsml ..........   pwp   \n")
+        for i in range(w.n):
+            vals = (w.x[i, 0], w.x[i, 1], v[i, 0], v[i, 1], w.rho[i], w.mass[i], w.hsml[i], pwp[i])
+            f.write("%7d  %5d" % (i + 1, 1) + "".join("  %14.7E" % float(a) for a in vals) + "\n")
+    r = parse("plane", str(tmp_path))
+    assert r["n"] == w.n
+    dump = str(tmp_path / "plane.dump")
+    out = subprocess.run([RUN, "plane", "--dir", str(tmp_path), "--dump", dump], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    import gfsph
+    got, _ = workloads.from_driver_dump(dump, gfsph)
+
+    def g7(a):  # the value a g14.7 field carries, read back in single precision
+        return np.array([np.float32(float("%14.7E" % float(b))) for b in np.ravel(a)], np.float32).reshape(np.shape(a))
+
+    assert np.array_equal(got.x, g7(w.x)) and np.array_equal(got.v, g7(v))
+    assert np.array_equal(got.rho, g7(w.rho)) and np.array_equal(got.mass, g7(w.mass))
+    assert np.array_equal(got.hsml, g7(w.hsml))
