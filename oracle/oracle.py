@@ -359,3 +359,161 @@ def tangent(params, nx, ny, dx, dy, state, nsteps, seed_mu=0.0, seed_xi=0.0, see
     if st:
         raise RuntimeError(f"oracle_tangent: {st}")
     return tuple(out)
+
+
+# ---------------------------------------------------------------- set-up
+# Restatements of the reference's input set-up in single precision (irk =
+# k_real), used to check the C++ host reader: every operation is an FP32
+# numpy operation in the reference's order, and the inverse-distance sums
+# are added with np.add.at in the reference's loop order (source point, then
+# the node columns, then the node rows), so the sums round as the Fortran
+# loops do.  Decimal input is converted straight to single precision
+# (strtof), as a list-directed read of a default real does.
+
+_strtof = None
+
+
+def _f32(tokens):
+    global _strtof
+    if _strtof is None:
+        libc = C.CDLL(None)
+        _strtof = libc.strtof
+        _strtof.restype = C.c_float
+        _strtof.argtypes = [C.c_char_p, C.c_void_p]
+    return np.array([_strtof(t.replace("d", "e").replace("D", "e").encode(), None) for t in tokens], np.float32)
+
+
+def _lines(path):
+    with open(path) as f:
+        return [ln.rstrip("\n") for ln in f]
+
+
+def _idw_block(px, py, x0, y0, dx, dy, nx, ny, lo, hi):
+    """Node indices (row-major, 0-based) and validity of the block of nodes
+    [ipx + lo, ipx + hi] x [ipy + lo', ...] around each point, flattened in
+    the reference's loop order: point, node column, node row."""
+    f1 = np.float32(1.0)
+    ipx = ((px - x0) / dx + f1).astype(np.int64)  # Fortran real -> integer truncates
+    ipy = ((py - y0) / dy + f1).astype(np.int64)
+    return ipx, ipy
+
+
+def get_dtm(top_path):
+    """Get_DTM (SPH_FEM_topo_2019.f90:1155-1445) for ictop 10 and 11: the
+    scattered (x, y, z) points of the .top file to the regular grid by
+    inverse-distance weights over the 4x4 nodes around each point.  Returns
+    dict(nx, ny, xmin, ymin, dx, dy, xshift, yshift, z (ny, nx) float32)."""
+    L = _lines(top_path)
+    ictop = int(L[1].split()[0])
+    if ictop not in (10, 11):
+        raise ValueError("get_dtm restates ictop 10 and 11")
+    np_dtm, deltx = L[3].split()[:2]
+    np_dtm = int(float(np_dtm))
+    deltx = _f32([deltx])[0]
+    tok = " ".join(L[5:5 + np_dtm]).split()
+    pts = _f32(tok[:3 * np_dtm]).reshape(np_dtm, 3)
+    xx, yy, zz = pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy()
+    xming, xmaxg, yming, ymaxg = xx.min(), xx.max(), yy.min(), yy.max()
+    zmaxg = zz.max()
+    f1 = np.float32(1.0)
+    npoigx = int((xmaxg - xming) / deltx + f1)
+    npoigy = int((ymaxg - yming) / deltx + f1)
+    deltxg = (xmaxg - xming) / np.float32(npoigx - 1)
+    deltyg = (ymaxg - yming) / np.float32(npoigy - 1)
+    xshift = yshift = np.float32(0.0)
+    if ictop == 11:  # relative coordinates
+        xshift, yshift = xming, yming
+        xx = xx - xming
+        yy = yy - yming
+        xmaxg, ymaxg = xmaxg - xming, ymaxg - yming
+        xming = yming = np.float32(0.0)
+    cx = xming + np.arange(npoigx).astype(np.float32) * deltxg
+    cy = yming + np.arange(npoigy).astype(np.float32) * deltyg
+    distg = np.sqrt(deltxg * deltxg + deltyg * deltyg)
+    inside = (xx >= xming) & (xx <= xmaxg) & (yy >= yming) & (yy <= ymaxg)
+    ipx = ((xx - xming) / deltxg + f1).astype(np.int64)
+    ipy = ((yy - yming) / deltyg + f1).astype(np.int64)
+    a = np.arange(4)
+    inx = (ipx[:, None, None] - 1 + a[None, :, None]) * np.ones((1, 1, 4), np.int64)   # columns ipx-1 .. ipx+2
+    iny = (ipy[:, None, None] - 1 + a[None, None, :]) * np.ones((1, 4, 1), np.int64)   # rows ipy-1 .. ipy+2
+    ok = inside[:, None, None] & (inx >= 1) & (inx <= npoigx) & (iny >= 1) & (iny <= npoigy)
+    inx, iny, ok = inx.reshape(-1), iny.reshape(-1), ok.reshape(-1)
+    src = np.repeat(np.arange(np_dtm), 16)[ok]
+    inx, iny = inx[ok], iny[ok]
+    dxs = xx[src] - cx[inx - 1]
+    dys = yy[src] - cy[iny - 1]
+    dist = np.maximum(np.float32(1.e-6), np.sqrt(dxs * dxs + dys * dys))
+    dist = dist / distg
+    node = (iny - 1) * npoigx + (inx - 1)
+    a1 = np.zeros(npoigx * npoigy, np.float32)
+    a2 = np.zeros(npoigx * npoigy, np.float32)
+    np.add.at(a1, node, zz[src] / dist)
+    np.add.at(a2, node, f1 / dist)
+    z = np.where(a2 >= np.float32(1.e-6), a1 / np.where(a2 > 0, a2, f1), zmaxg).astype(np.float32)
+    return dict(nx=npoigx, ny=npoigy, xmin=xming, ymin=yming, dx=deltxg, dy=deltyg, xshift=xshift, yshift=yshift,
+                z=z.reshape(npoigy, npoigx))
+
+
+def read_source_plus_new(pts_path, h_inf, xshift=0.0, yshift=0.0):
+    """Read_Source_plus_New (SPH_SW_2019.f90:4999-5272): the source points of
+    the .pts file resampled on a lattice by inverse-distance weights; every
+    lattice node that received a weight becomes a particle with depth
+    sum(h/d)/sum(1/d) (clamped to h_inf), volume dA * h * (number of its four
+    lattice cells whose corners all received weights), dA = dx dy / 4, and
+    smoothing length max(delt2Dx, delt2Dy) * facthsml as read.  Returns
+    dict(x (n, 2), h, mass, hsml) in float32, lattice order."""
+    L = _lines(pts_path)
+    hdr = L[1].split()
+    np_src = int(float(hdr[0]))
+    dx_s, d2x, d2y, fact = _f32(hdr[1:5])
+    delt2d = max(d2x, d2y)
+    tok = " ".join(L[3:3 + np_src]).split()
+    pts = _f32(tok[:3 * np_src]).reshape(np_src, 3)
+    xs = pts[:, 0] - np.float32(xshift)
+    ys = pts[:, 1] - np.float32(yshift)
+    hs = pts[:, 2]
+    f1 = np.float32(1.0)
+    xmin, xmax, ymin, ymax = xs.min(), xs.max(), ys.min(), ys.max()
+    npx = int((xmax - xmin) / d2x + f1)
+    npy = int((ymax - ymin) / d2y + f1)
+    d2x = (xmax - xmin) / np.float32(npx - 1)
+    d2y = (ymax - ymin) / np.float32(npy - 1)
+    gx = xmin + np.arange(npx).astype(np.float32) * d2x
+    gy = ymin + np.arange(npy).astype(np.float32) * d2y
+    dist2d = np.sqrt(d2x * d2x + d2y * d2y)
+    ndx = int(max(np.float32(2.0), dx_s / d2x))
+    ndy = int(max(np.float32(2.0), dx_s / d2y))
+    ipx = ((xs - xmin) / d2x + f1).astype(np.int64)
+    ipy = ((ys - ymin) / d2y + f1).astype(np.int64)
+    ax = np.arange(-ndx + 1, ndx + 2)   # columns ipx - ndx + 1 .. ipx + ndx + 1
+    ay = np.arange(-ndy, ndy + 1)       # rows ipy - ndy .. ipy + ndy
+    inx = ipx[:, None, None] + ax[None, :, None] + 0 * ay[None, None, :]
+    iny = ipy[:, None, None] + 0 * ax[None, :, None] + ay[None, None, :]
+    ok = (inx >= 1) & (inx <= npx) & (iny >= 1) & (iny <= npy)
+    inx, iny, ok = inx.reshape(-1), iny.reshape(-1), ok.reshape(-1)
+    src = np.repeat(np.arange(np_src), ax.size * ay.size)[ok]
+    inx, iny = inx[ok], iny[ok]
+    dxs = xs[src] - gx[inx - 1]
+    dys = ys[src] - gy[iny - 1]
+    dist = np.maximum(np.float32(1.e-6), np.sqrt(dxs * dxs + dys * dys))
+    dist = dist / dist2d
+    node = (iny - 1) * npx + (inx - 1)
+    a2 = np.zeros(npx * npy, np.float32)
+    a3 = np.zeros(npx * npy, np.float32)
+    np.add.at(a2, node, f1 / dist)
+    np.add.at(a3, node, hs[src] / dist)
+    w = (a2 >= np.float32(1.e-6)).reshape(npy, npx)
+    full = w[:-1, :-1] & w[:-1, 1:] & w[1:, :-1] & w[1:, 1:]
+    a4 = np.zeros((npy, npx), np.int64)
+    a4[:-1, :-1] += full
+    a4[:-1, 1:] += full
+    a4[1:, :-1] += full
+    a4[1:, 1:] += full
+    keep = w.reshape(-1)
+    h = (a3[keep] / a2[keep]).astype(np.float32)
+    h = np.where(h < np.float32(h_inf), np.float32(h_inf), h).astype(np.float32)
+    d_area = d2x * d2y / np.float32(4.0)
+    mass = (d_area * h * a4.reshape(-1)[keep].astype(np.float32)).astype(np.float32)
+    yy, xx = np.meshgrid(gy, gx, indexing="ij")
+    x = np.stack([xx.reshape(-1)[keep], yy.reshape(-1)[keep]], 1).astype(np.float32)
+    return dict(x=x, h=h, mass=mass, hsml=np.full(h.size, delt2d * fact, np.float32))

@@ -154,3 +154,28 @@ def test_restart_input_reads_the_reference_layout(gfsph_lib, tmp_path):
     assert np.array_equal(got.x, g7(w.x)) and np.array_equal(got.v, g7(v))
     assert np.array_equal(got.rho, g7(w.rho)) and np.array_equal(got.mass, g7(w.mass))
     assert np.array_equal(got.hsml, g7(w.hsml))
+
+
+def test_picacho_setup_matches_the_oracle_restatement(gfsph_lib, oracle_mod, tmp_path):
+    """The C++ reader's DEM and particles for the reference's own example
+    against the oracle's independent restatements of Get_DTM
+    (SPH_FEM_topo_2019.f90:1155-1445, ictop 10: the scattered .top points to
+    the grid by inverse-distance weights) and Read_Source_plus_New
+    (SPH_SW_2019.f90:4999-5272: the .pts source resampled on its lattice),
+    bit for bit; the driver leaves out the lattice nodes of zero volume."""
+    import gfsph
+    d = picacho_inputs(tmp_path)
+    dump = os.path.join(str(tmp_path), "picacho.dump")
+    out = subprocess.run([RUN, "Picacho", "--dir", d, "--dump", dump], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    w, p = workloads.from_driver_dump(dump, gfsph)
+    dem = oracle_mod.get_dtm(os.path.join(d, "Picacho.top"))
+    assert (dem["nx"], dem["ny"]) == (442, 291)
+    assert np.float32(w.meta["xmin"]) == dem["xmin"] and np.float32(w.meta["ymin"]) == dem["ymin"]
+    assert np.float32(w.dx) == dem["dx"] and np.float32(w.dy) == dem["dy"]
+    assert np.array_equal(w.z, dem["z"])
+    src = oracle_mod.read_source_plus_new(os.path.join(d, "Picacho.pts"), p.h_inf, dem["xshift"], dem["yshift"])
+    keep = src["mass"] > 0
+    assert keep.sum() == w.n
+    for key, got in (("x", w.x), ("h", w.rho), ("mass", w.mass), ("hsml", w.hsml)):
+        assert np.array_equal(got, src[key][keep]), key
