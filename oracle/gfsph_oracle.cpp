@@ -220,6 +220,11 @@ struct Oracle {
     /* particles */
     int n;
     std::vector<R> x, v, rho, mass, hsml, x0, v0, p;
+    /* mode 3 (a precision experiment, not the reference): the RK45 position
+     * updates carried in FP64 (xd), everything else as in mode 1; x holds
+     * the single-precision positions that every other term reads */
+    bool pos64 = false;
+    std::vector<double> xd, x0d;
     std::vector<R> uaux, rho0; /* basal pore-water pressure Uaux(1,:) (icpwp = 3) and rho at the RK45 start */
     /* pore-water-pressure and density factors: DFs_FSs_dens_and_pwp_factors
      * (ExtForces_SW, SPH_SW_2019.f90:8959-9109) for the friction, and
@@ -912,6 +917,7 @@ struct Oracle {
         std::fill(Dv.begin(), Dv.end(), (R)0);
         grid_find();
         x0 = x; v0 = v;
+        if (pos64) x0d = xd;
         rho0 = rho;
         const R f1[4] = {0, lit<R>(0.5), lit<R>(0.5), 1};
         const R f2[4] = {1, 2, 2, 1};
@@ -920,8 +926,9 @@ struct Oracle {
             for (int i = 0; i < n; i++) {
                 if (flag[i]) continue;
                 for (int d = 0; d < 2; d++) {
-                    x[2 * i + d] = x0[2 * i + d] + fdt * v[2 * i + d];
-                    v[2 * i + d] = v0[2 * i + d] + fdt * (ex[2 * i + d] + in[2 * i + d]);
+                    const size_t k = 2 * i + d;
+                    x[k] = pos64 ? (R)(x0d[k] + (double)fdt * (double)v[k]) : x0[k] + fdt * v[k];
+                    v[k] = v0[k] + fdt * (ex[k] + in[k]);
                 }
             }
             check_out_domain();
@@ -938,10 +945,19 @@ struct Oracle {
         }
         R dt6 = dt / (R)6;
         for (int i = 0; i < n; i++) {
-            if (flag[i]) continue;
+            if (flag[i]) {
+                if (pos64) { xd[2 * i] = (double)x[2 * i]; xd[2 * i + 1] = (double)x[2 * i + 1]; }
+                continue;
+            }
             for (int d = 0; d < 2; d++) {
-                x[2 * i + d] = x0[2 * i + d] + dt6 * Dx[2 * i + d];
-                v[2 * i + d] = v0[2 * i + d] + dt6 * Dv[2 * i + d];
+                const size_t k = 2 * i + d;
+                if (pos64) {
+                    xd[k] = x0d[k] + (double)dt6 * (double)Dx[k];
+                    x[k] = (R)xd[k];
+                } else {
+                    x[k] = x0[k] + dt6 * Dx[k];
+                }
+                v[k] = v0[k] + dt6 * Dv[k];
             }
         }
         sum_density();
@@ -1069,7 +1085,7 @@ struct OracleObj : OracleBase {
              double* topol) override {
         int n = o.n;
         for (size_t k = 0; k < 2 * (size_t)n; k++) {
-            if (x) x[k] = (double)o.x[k];
+            if (x) x[k] = o.pos64 ? o.xd[k] : (double)o.x[k];
             if (v) v[k] = (double)o.v[k];
         }
         for (int k = 0; k < n; k++) {
@@ -1092,13 +1108,15 @@ template <class R, class A>
 OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
                      const double* topol, int n, const double* x, const double* v, const double* rho,
                      const double* mass, const double* hsml, const int* flag, const double* pwp, double dt, double t,
-                     int* status) {
+                     int* status, bool pos64 = false) {
     OracleObj<R, A>* ob = new OracleObj<R, A>();
     ob->params = *p;
     Oracle<R, A>& o = ob->o;
     int st = o.setup(&ob->params, nx, ny, xmin, ymin, dx, dy, topol);
     if (st) { delete ob; *status = st; return nullptr; }
     o.n = n;
+    o.pos64 = pos64;
+    if (pos64) o.xd.assign(x, x + 2 * (size_t)n);
     auto cp = [&](std::vector<R>& dst, const double* src, size_t m) {
         dst.resize(m);
         for (size_t k = 0; k < m; k++) dst[k] = (R)src[k];
@@ -1645,6 +1663,7 @@ void* oracle_new(int mode, const gfsph_params* p, int nx, int ny, double xmin, d
     case 0: return make_obj<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);
     case 1: return make_obj<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);
     case 2: return make_obj<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status);
+    case 3: return make_obj<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, dt, t, status, true);
     default: return nullptr;
     }
 }

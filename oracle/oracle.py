@@ -21,6 +21,7 @@ NTOPO = 16
 MODE_FP32 = 0        # reference FP32 build
 MODE_FP32_DACC = 1   # FP32 state, FP64 sums (the GPU scheme)
 MODE_FP64 = 2        # reference FP64 build
+MODE_POS64 = 3       # precision experiment: mode 1 with the RK45 position updates in FP64 (Run only)
 
 _libs = {}
 _DP = C.POINTER(C.c_double)

@@ -15,7 +15,9 @@ Cases (seeded synthetic inputs of the benchmark configurations):
              DEM at 5 m, Voellmy mu 0.15 xi 400, Hungr erosion, adaptive dt),
              10,000 steps, hazard samples every 100 steps.
 Arms: the serial oracle in the reference's FP32 scheme (mode 0, the shipped
-build) or in FP64 (mode 2, irk = k_double), and the GPU through the C ABI.
+build), in the GPU's scheme (mode 1: FP32 with FP64 sums), in FP64 (mode 2,
+irk = k_double), or mode 1 with the RK45 position updates carried in FP64
+(mode 3, a precision experiment), and the GPU through the C ABI.
 
 Outputs, all evaluated in FP64 from each arm's particle states with the same
 code (so only the states differ): the final IDW depth raster
@@ -152,7 +154,7 @@ def main():
     sub = ap.add_subparsers(dest="cmd", required=True)
     a = sub.add_parser("oracle")
     a.add_argument("--case", choices=sorted(CASES), required=True)
-    a.add_argument("--mode", type=int, choices=[0, 2], required=True)
+    a.add_argument("--mode", type=int, choices=[0, 1, 2, 3], required=True)
     a.add_argument("--out", required=True)
     b = sub.add_parser("gpu")
     b.add_argument("--case", choices=sorted(CASES), required=True)
