@@ -358,44 +358,99 @@ def cg_bench(args, gfsph, workloads, peak):
     return out
 
 
-def adjoint_bench(gfsph, workloads, torch):
-    """The adjoint of the calibration case's step: ~50k particles on a 512^2
-    DEM at 5 m (fixed smoothing lengths, no erosion, fixed dt), 100 steps
-    recorded with a checkpoint every 10 and swept back; the cost of one
-    adjoint step (its forward recomputations included) against one plain
-    forward step of the same run."""
+def adjoint_bench(gfsph, workloads, torch, nsteps=1000, every=100):
+    """The adjoint of the calibration case (config 5's shape): ~50k particles
+    on a 512^2 DEM at 5 m (fixed smoothing lengths, no erosion, fixed dt),
+    `nsteps` steps recorded with a checkpoint every `every` and swept back
+    (the config runs 5,000 steps; the cost per step does not depend on how
+    many).  Device time from CUDA events on the handle's stream around the
+    plain forward run, the recording run and the backward sweep (which
+    recomputes each step's forward pass from its segment's checkpoint)."""
     w = workloads.fractal_channel(n_target=50_000, dem_k=9, cell=5.0, erosion=None)
     p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
-    nsteps, every = 100, 10
+    stream = torch.cuda.Stream()
     sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.set_stream(stream.cuda_stream)
     sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
     sim.step(3)
-    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
-    sim.set_time(0.0, p.dt)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    sim.step(nsteps)
-    torch.cuda.synchronize()
-    t_fwd = (time.perf_counter() - t0) / nsteps
-    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
-    sim.set_time(0.0, p.dt)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / nsteps
+
+    def restart():
+        sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+        sim.set_time(0.0, p.dt)
+
+    restart()
+    _, t_fwd = timed(lambda: sim.step(nsteps))
+    restart()
     rng = np.random.default_rng(0)
     gx = rng.normal(size=(w.n, 2)).astype(np.float32)
     gv = rng.normal(size=(w.n, 2)).astype(np.float32)
-    t0 = time.perf_counter()
-    adj = gfsph.Adjoint(sim, nsteps, every=every)
-    t_rec = (time.perf_counter() - t0) / nsteps
-    t0 = time.perf_counter()
-    g = adj.backward(gx, gv)
-    t_bwd = (time.perf_counter() - t0) / nsteps
+    adj, t_rec = timed(lambda: gfsph.Adjoint(sim, nsteps, every=every))
+    g, t_bwd = timed(lambda: adj.backward(gx, gv))
     adj.close()
     sim.close()
     return {"workload": f"{w.n} particles, {w.meta['dem']}, Voellmy, fixed hsml and dt", "steps": nsteps,
-            "checkpoint_every": every, "forward_ms_per_step": t_fwd * 1e3,
-            "recording_ms_per_step": t_rec * 1e3, "backward_ms_per_step": t_bwd * 1e3,
-            "backward_over_forward": t_bwd / t_fwd, "dL_dtanfi": g["tanfi"], "dL_dxi": g["xi"],
-            "note": "host clock; the backward step recomputes the forward step (neighbour table, density, "
-                    "forces) from the kept states, plus the segment's states when every > 1"}
+            "checkpoint_every": every, "forward_ms_per_step": t_fwd, "recording_ms_per_step": t_rec,
+            "backward_ms_per_step": t_bwd, "backward_over_forward": t_bwd / t_fwd, "dL_dtanfi": g["tanfi"],
+            "dL_dxi": g["xi"],
+            "note": "device time (CUDA events on the handle's stream); the backward step includes the forward "
+                    "recomputation of its segment's states and of its own step from the kept checkpoints"}
+
+
+def coupled_bench(gfsph, workloads, torch, nsteps=10):
+    """Config 3 as one run: the 4M-particle Bingham case on the 4096^2 DEM at
+    2 m with, every step, the SPH step and the coupling pass get_gradhs_w on
+    a 500 x 500-node window of the DEM background triangulation (498,002
+    triangles) around the first release, its projection solved by the device
+    CG to 1e-10 (squared-norm ratio).  Device time from CUDA events around
+    the steps, after 3 warm-up steps; the coupling pass copies its nodal
+    outputs to the host each step, as a caller would read them."""
+    w = workloads.multi_release()
+    p = workloads.make_params(w, gfsph)
+    stream = torch.cuda.Stream()
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    ny, nx = w.z.shape
+    nw = 500
+    c = np.floor(w.x[: w.n // 8].mean(axis=0) / w.dx).astype(int)  # inside the first release
+    ix0 = int(min(max(c[0] - nw // 2, 0), nx - nw))
+    iy0 = int(min(max(c[1] - nw // 2, 0), ny - nw))
+
+    def one():
+        sim.step(1)
+        sim.gradhs(ix0, iy0, nw, nw, niter=0, tol=1e-10)
+
+    for _ in range(3):
+        one()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(nsteps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / nsteps
+    e0.record(stream)
+    sim.step(nsteps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_step = e0.elapsed_time(e1) / nsteps
+    sim.close()
+    return {"workload": f"{w.n} particles, {w.meta['dem']}, Bingham, coupling window {nw}x{nw} nodes "
+                        f"({2 * (nw - 1) ** 2} triangles) with the CG projection every step",
+            "steps": nsteps, "ms_per_coupled_step": ms, "ms_per_sph_step": ms_step,
+            "particle_steps_per_s": w.n / (ms / 1e3), "sph_particle_steps_per_s": w.n / (ms_step / 1e3),
+            "note": "device time (CUDA events), 3 warm-up steps; the config's 2,000 steps at this rate take "
+                    f"{2000 * ms / 1e3:.1f} s"}
 
 
 def couple_bench(sim, w, gfsph):
@@ -573,6 +628,7 @@ def main():
     sim.close()
     cg_line = cg_bench(args, gfsph, workloads, peak) if extras else None
     adj_line = adjoint_bench(gfsph, workloads, torch) if extras else None
+    big_line = coupled_bench(gfsph, workloads, torch) if extras else None
     ens_line = None
     if extras and args.ensemble > 0:
         ens_line = ensemble_bench(args, torch, gfsph, workloads)
@@ -607,6 +663,8 @@ def main():
             line["cg"] = cg_line
         if adj_line:
             line["adjoint"] = adj_line
+        if big_line:
+            line["coupled_large_case"] = big_line
         if couple_line:
             line["couple"] = couple_line
         if ens_line:
