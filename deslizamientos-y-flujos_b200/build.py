@@ -52,14 +52,16 @@ def build(verbose=False, force=False):
     api_o = os.path.join(BUILD_DIR, "gfsph_api.o")
     noalloc_o = os.path.join(BUILD_DIR, "gfsph_noalloc.o")
     cg_o = os.path.join(BUILD_DIR, "gfsph_cg.o")
+    gfl_o = os.path.join(BUILD_DIR, "gfsph_gfl.o")
     dem_o = os.path.join(BUILD_DIR, "gfsph_dem.o")
     _run([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "gfsph_api.cu"), "-o", api_o], log)
     _run([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "gfsph_noalloc.cu"), "-o", noalloc_o], log)
     _run([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "gfsph_cg.cu"), "-o", cg_o], log)
+    _run([nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, "gfsph_gfl.cu"), "-o", gfl_o], log)
     _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-c",
           os.path.join(CSRC, "gfsph_dem.cpp"), "-o", dem_o], log)
     tmp = OUT + ".tmp"
-    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", api_o, noalloc_o, cg_o, dem_o,
+    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", api_o, noalloc_o, cg_o, gfl_o, dem_o,
           "-o", tmp, "-lcudart"], log)
     os.replace(tmp, OUT)
     # the C++ host driver (reads the reference's input files, drives the ABI)

@@ -39,6 +39,15 @@ module gfsph_c
      type(c_ptr)    :: z
   end type gfsph_dem
 
+  type, bind(c) :: gfsph_gfl_params
+     real(c_float)  :: constF(15)              ! constF(1:15) of the GFL .dat as Input_GFL keeps them
+     integer(c_int) :: ntype                   ! 2 under a still-water level, 3 over a dry bed
+     integer(c_int) :: ngaus                   ! Gauss points per triangle (1 or 3)
+     integer(c_int) :: niter                   ! consistent-mass sweeps of solve
+     real(c_float)  :: swl                     ! still-water level
+     real(c_float)  :: comp                    ! dry depth of check
+  end type gfsph_gfl_params
+
   interface
      integer(c_int) function gfsph_create(params, dem, handle) bind(c, name="gfsph_create")
        import :: c_int, c_ptr, gfsph_params, gfsph_dem
@@ -304,6 +313,52 @@ module gfsph_c
        integer(c_int), value :: n, nx, ny
        type(c_ptr), value :: d_x, d_rho, d_flag, d_out, stream
        real(c_float), value :: xmin, ymin, dx, dy
+     end function
+     ! the GFL step: replaces Init_GFL's set-up and calls of time_integration_gfl on one mesh
+     integer(c_int) function gfsph_gfl_create(params, npoin, nelem, coord, intmat, z, gfl) &
+          bind(c, name="gfsph_gfl_create")
+       import :: c_int, c_ptr, c_float, gfsph_gfl_params
+       type(gfsph_gfl_params), intent(in) :: params
+       integer(c_int), value :: npoin, nelem
+       real(c_float), intent(in) :: coord(2, npoin), z(npoin)
+       integer(c_int), intent(in) :: intmat(3, nelem)
+       type(c_ptr), intent(out) :: gfl
+     end function
+     integer(c_int) function gfsph_gfl_destroy(gfl) bind(c, name="gfsph_gfl_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: gfl
+     end function
+     integer(c_int) function gfsph_gfl_set_state(gfl, unkno, time) bind(c, name="gfsph_gfl_set_state")
+       import :: c_int, c_ptr, c_float, c_double
+       type(c_ptr), value :: gfl
+       real(c_float), intent(in) :: unkno(3, *)
+       real(c_double), value :: time
+     end function
+     integer(c_int) function gfsph_gfl_get_state(gfl, unkno, time) bind(c, name="gfsph_gfl_get_state")
+       import :: c_int, c_ptr, c_float, c_double
+       type(c_ptr), value :: gfl
+       real(c_float), intent(out) :: unkno(3, *)
+       real(c_double), intent(out) :: time
+     end function
+     integer(c_int) function gfsph_gfl_set_wir(gfl, hs_w, gradhs_w) bind(c, name="gfsph_gfl_set_wir")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: gfl
+       real(c_float), intent(in) :: hs_w(*), gradhs_w(2, *)
+     end function
+     integer(c_int) function gfsph_gfl_step(gfl, nsteps, dt) bind(c, name="gfsph_gfl_step")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: gfl
+       integer(c_int), value :: nsteps
+       real(c_float), value :: dt
+     end function
+     integer(c_int) function gfsph_gfl_topol(gfl, topol, topel) bind(c, name="gfsph_gfl_topol")
+       import :: c_int, c_ptr, c_float
+       type(c_ptr), value :: gfl
+       real(c_float), intent(out) :: topol(9, *), topel(9, *)
+     end function
+     integer(c_long_long) function gfsph_gfl_launch_count(gfl) bind(c, name="gfsph_gfl_launch_count")
+       import :: c_long_long, c_ptr
+       type(c_ptr), value :: gfl
      end function
      type(c_ptr) function gfsph_strerror(status) bind(c, name="gfsph_strerror")
        import :: c_int, c_ptr

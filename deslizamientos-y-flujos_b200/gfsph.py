@@ -63,6 +63,14 @@ _IP = C.POINTER(C.c_int)
 _lib = None
 
 # every symbol include/gfsph.h declares, with its ctypes signature
+class GflParams(C.Structure):
+    """gfsph_gfl_params: constF[k-1] = constF(k) of the GFL .dat, the flow
+    type (2 under a still-water level, 3 over a dry bed), Gauss points per
+    triangle, consistent-mass sweeps, still-water level, dry depth."""
+    _fields_ = [("constF", C.c_float * 15), ("ntype", C.c_int), ("ngaus", C.c_int), ("niter", C.c_int),
+                ("swl", C.c_float), ("comp", C.c_float)]
+
+
 SIGNATURES = {
     "gfsph_create": (C.c_int, [C.POINTER(Params), C.POINTER(Dem), C.POINTER(C.c_void_p)]),
     "gfsph_destroy": (C.c_int, [C.c_void_p]),
@@ -111,6 +119,14 @@ SIGNATURES = {
     "gfsph_cg_launch_count": (C.c_longlong, [C.c_void_p]),
     "gfsph_cg_device_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "gfsph_solvegc2": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _FP, _FP, _FP, _FP, C.c_float, _IP]),
+    "gfsph_gfl_create": (C.c_int, [C.POINTER(GflParams), C.c_int, C.c_int, _FP, _IP, _FP, C.POINTER(C.c_void_p)]),
+    "gfsph_gfl_destroy": (C.c_int, [C.c_void_p]),
+    "gfsph_gfl_set_state": (C.c_int, [C.c_void_p, _FP, C.c_double]),
+    "gfsph_gfl_get_state": (C.c_int, [C.c_void_p, _FP, C.POINTER(C.c_double)]),
+    "gfsph_gfl_set_wir": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "gfsph_gfl_step": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
+    "gfsph_gfl_topol": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "gfsph_gfl_launch_count": (C.c_longlong, [C.c_void_p]),
     "gfsph_strerror": (C.c_char_p, [C.c_int]),
     "gfsph_version": (C.c_int, []),
     "gfsph_binary_version": (C.c_int, [_IP]),
@@ -392,6 +408,68 @@ class CG:
     def close(self):
         if self.h:
             lib().gfsph_cg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Gfl:
+    """The GFL Taylor-Galerkin shallow-water step on the device (gfsph_gfl_*).
+
+    coord (npoin, 2), intmat (nelem, 3) 1-based counter-clockwise, z (npoin);
+    const: {k: constF(k)}; the state unkno (npoin, 3) = h, hu, hv."""
+
+    def __init__(self, coord, intmat, z, const, ntype=3, ngaus=3, niter=3, swl=0.0, comp=0.01):
+        p = GflParams()
+        for k, v in const.items():
+            p.constF[k - 1] = v
+        p.ntype, p.ngaus, p.niter, p.swl, p.comp = ntype, ngaus, niter, swl, comp
+        c = np.ascontiguousarray(coord, np.float32)
+        im = np.ascontiguousarray(intmat, np.int32)
+        zz = np.ascontiguousarray(z, np.float32)
+        self.npoin, self.nelem = c.shape[0], im.shape[0]
+        h = C.c_void_p()
+        _check(lib().gfsph_gfl_create(C.byref(p), self.npoin, self.nelem, _fp(c), _ip(im), _fp(zz), C.byref(h)),
+               "gfsph_gfl_create")
+        self.h = h
+
+    def set_state(self, unkno, time=0.0):
+        u = np.ascontiguousarray(unkno, np.float32)
+        _check(lib().gfsph_gfl_set_state(self.h, _fp(u), time), "gfsph_gfl_set_state")
+
+    def state(self):
+        u = np.empty((self.npoin, 3), np.float32)
+        t = C.c_double()
+        _check(lib().gfsph_gfl_get_state(self.h, _fp(u), C.byref(t)), "gfsph_gfl_get_state")
+        return u, t.value
+
+    def set_wir(self, hs_w=None, gradhs_w=None):
+        if hs_w is None:
+            _check(lib().gfsph_gfl_set_wir(self.h, None, None), "gfsph_gfl_set_wir")
+            return
+        a = np.ascontiguousarray(hs_w, np.float32)
+        b = np.ascontiguousarray(gradhs_w, np.float32)
+        _check(lib().gfsph_gfl_set_wir(self.h, _fp(a), _fp(b)), "gfsph_gfl_set_wir")
+
+    def step(self, nsteps, dt):
+        _check(lib().gfsph_gfl_step(self.h, nsteps, dt), "gfsph_gfl_step")
+
+    def topol(self):
+        t = np.empty((self.npoin, 9), np.float32)
+        e = np.empty((self.nelem, 9), np.float32)
+        _check(lib().gfsph_gfl_topol(self.h, _fp(t), _fp(e)), "gfsph_gfl_topol")
+        return t, e
+
+    def launch_count(self):
+        return int(lib().gfsph_gfl_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            lib().gfsph_gfl_destroy(self.h)
             self.h = None
 
     def __del__(self):

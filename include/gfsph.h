@@ -378,6 +378,53 @@ int gfsph_solvegc2(int npoin, int nelem, int nnode, int ndofn, const int* intmat
 int gfsph_raster_idw_noalloc(int n, const float* d_x, const float* d_rho, const int* d_flag, int nx, int ny,
                              float xmin, float ymin, float dx, float dy, float* d_out, void* stream);
 
+/*
+ * The Taylor-Galerkin shallow-water step of the GFL module
+ * (Time_Integration_GFL, GFL_MAIN_2019.f90:216-284) on the device: the mesh
+ * side of the SPH <-> FEM coupling (SPH_FEM_Driver_2019.f90:1630-1650).
+ * gfsph_gfl_create does the set-up of Init_GFL (:65-214: element geometry,
+ * lumped mass, Get_Topol's nodal slopes and curvatures, the boundary nodes
+ * and their tangents, the boundary sides) on the host in single precision;
+ * gfsph_gfl_step runs nsteps steps of first_step, second_step, solve
+ * (niter sweeps of the consistent-mass system), addthem and check, with the
+ * reference's summation orders (results equal an FP32 restatement bit for
+ * bit).  Scope: nsour 1, itens 0 (const(11)), no pore pressure, every
+ * boundary node a wall (no prescribed, absorbing or loaded nodes), no
+ * atmospheric pressure or wind, a fixed dt per call, nfric 0-8 with Manning
+ * added when const(3) != 0; GFSPH_ERR_UNSUPPORTED outside it.
+ */
+typedef struct gfsph_gfl gfsph_gfl;
+typedef struct gfsph_gfl_params {
+    float constF[15]; /* constF[k-1] = constF(k) of the .dat as Input_GFL keeps them (absolute values; hfrict0
+                         above 1e-32, dens above 0.001 for nfric 2, else GFSPH_ERR_ARG): cgra, dens, Manning,
+                         Coriolis, nfric, tauy, K, -, tanfi8, hfrict0, itens, tanfi0, Bfact, hrelpw, - */
+    int ntype;        /* 2: flow under a still-water level swl (pressure of h - HH); 3: flow over a dry bed */
+    int ngaus;        /* Gauss points per triangle: 1 or 3 */
+    int niter;        /* sweeps of the consistent-mass iteration in solve (>= 1) */
+    float swl;        /* still-water level (ntype 2) */
+    float comp;       /* depth below which a node is dry (check) */
+} gfsph_gfl_params;
+
+/* coord (npoin, 2), intmat (nelem, 3) 1-based and counter-clockwise, z the
+ * nodal bed elevation (npoin).  The state h, hu, hv starts at zero. */
+int gfsph_gfl_create(const gfsph_gfl_params* p, int npoin, int nelem, const float* coord, const int* intmat,
+                     const float* z, gfsph_gfl** out);
+int gfsph_gfl_destroy(gfsph_gfl* g);
+/* unkno (npoin, 3): h, hu, hv per node; time is the GFL clock (the tanfi decay) */
+int gfsph_gfl_set_state(gfsph_gfl* g, const float* unkno, double time);
+int gfsph_gfl_get_state(gfsph_gfl* g, float* unkno, double* time);
+/* The soil of the SPH flow under the water (WIR interaction, ntype 2):
+ * hs_w (npoin) raises the bed and gradhs_w (npoin, 2), as gfsph_gradhs
+ * returns it, adds to the nodal slopes; the element slopes take the element
+ * gradient of hs_w (get_gradhs_w, SPH_GFL_SW_Interactions_2019.f90:469-481).
+ * NULL, NULL switches it off. */
+int gfsph_gfl_set_wir(gfsph_gfl* g, const float* hs_w, const float* gradhs_w);
+int gfsph_gfl_step(gfsph_gfl* g, int nsteps, float dt);
+/* The set-up's nodal (npoin, 9) and element (nelem, 9) topography rows
+ * (Topol and Topel: Z, Zx, Zy, 1+Zx^2, ZxZy, 1+Zy^2, curvatures); either may be NULL. */
+int gfsph_gfl_topol(gfsph_gfl* g, float* topol, float* topel);
+long long gfsph_gfl_launch_count(gfsph_gfl* g);
+
 const char* gfsph_strerror(int status);
 int gfsph_version(void);
 

@@ -71,51 +71,95 @@
 
 #include "../include/gfsph.h"
 
-/* FP64 forward-mode (tangent) numbers: the oracle instantiated on Dual gives
- * the exact derivative of its FP64 step along one seeded direction (the
- * reference gradient for the device adjoint).  Branches follow the values. */
-struct Dual {
-    double v, d;
-    Dual() : v(0), d(0) {}
-    Dual(double a) : v(a), d(0) {}
-    Dual(double a, double b) : v(a), d(b) {}
-    explicit operator double() const { return v; }
+/* Forward-mode (tangent) numbers: the oracle instantiated on DualT gives the
+ * exact derivative of its step along one seeded direction (the reference
+ * gradient for the device adjoint).  The value is carried in T (double for
+ * the FP64 step; float for the single-precision step, rounded as the FP32
+ * arithmetic rounds it), the derivative always in double.  Branches follow
+ * the values. */
+template <class T>
+struct DualT {
+    T v;
+    double d;
+    DualT() : v(0), d(0) {}
+    DualT(double a) : v((T)a), d(0) {}
+    DualT(double a, double b) : v((T)a), d(b) {}
+    template <class U>
+    DualT(const DualT<U>& o) : v((T)o.v), d(o.d) {}
+    explicit operator double() const { return (double)v; }
     explicit operator float() const { return (float)v; }
     explicit operator int() const { return (int)v; }
     explicit operator long() const { return (long)v; }
-    Dual operator-() const { return Dual(-v, -d); }
-    Dual& operator+=(const Dual& b) { v += b.v; d += b.d; return *this; }
-    Dual& operator-=(const Dual& b) { v -= b.v; d -= b.d; return *this; }
+    DualT operator-() const { return DualT(-v, -d); }
+    DualT& operator+=(const DualT& b) { v = v + b.v; d += b.d; return *this; }
+    DualT& operator-=(const DualT& b) { v = v - b.v; d -= b.d; return *this; }
+    static DualT make(T a, double b) { DualT r; r.v = a; r.d = b; return r; }
+    friend DualT operator+(const DualT& a, const DualT& b) { return make(a.v + b.v, a.d + b.d); }
+    friend DualT operator-(const DualT& a, const DualT& b) { return make(a.v - b.v, a.d - b.d); }
+    friend DualT operator*(const DualT& a, const DualT& b) {
+        return make(a.v * b.v, a.d * (double)b.v + (double)a.v * b.d);
+    }
+    friend DualT operator/(const DualT& a, const DualT& b) {
+        T q = a.v / b.v;
+        return make(q, (a.d - (double)q * b.d) / (double)b.v);
+    }
+    friend bool operator<(const DualT& a, const DualT& b) { return a.v < b.v; }
+    friend bool operator>(const DualT& a, const DualT& b) { return a.v > b.v; }
+    friend bool operator<=(const DualT& a, const DualT& b) { return a.v <= b.v; }
+    friend bool operator>=(const DualT& a, const DualT& b) { return a.v >= b.v; }
+    friend bool operator==(const DualT& a, const DualT& b) { return a.v == b.v; }
+    friend bool operator!=(const DualT& a, const DualT& b) { return a.v != b.v; }
+    /* scalars: an int or float operand joins the arithmetic in T (as in
+     * float op int), a double one promotes to double (as float op double) */
+#define GF_SCALAR(op)                                                                                             \
+    friend DualT operator op(const DualT& a, int b) { return a op make((T)b, 0.0); }                              \
+    friend DualT operator op(int b, const DualT& a) { return make((T)b, 0.0) op a; }                              \
+    friend DualT operator op(const DualT& a, float b) { return a op make((T)b, 0.0); }                            \
+    friend DualT operator op(float b, const DualT& a) { return make((T)b, 0.0) op a; }                            \
+    friend DualT<double> operator op(const DualT& a, double b) { return DualT<double>(a) op DualT<double>(b); }     \
+    friend DualT<double> operator op(double b, const DualT& a) { return DualT<double>(b) op DualT<double>(a); }
+    GF_SCALAR(+) GF_SCALAR(-) GF_SCALAR(*) GF_SCALAR(/)
+#undef GF_SCALAR
+#define GF_SCALAR_CMP(op)                                                                   \
+    friend bool operator op(const DualT& a, double b) { return (double)a.v op b; }          \
+    friend bool operator op(double b, const DualT& a) { return b op (double)a.v; }
+    GF_SCALAR_CMP(<) GF_SCALAR_CMP(>) GF_SCALAR_CMP(<=) GF_SCALAR_CMP(>=) GF_SCALAR_CMP(==) GF_SCALAR_CMP(!=)
+#undef GF_SCALAR_CMP
 };
-inline Dual operator+(const Dual& a, const Dual& b) { return Dual(a.v + b.v, a.d + b.d); }
-inline Dual operator-(const Dual& a, const Dual& b) { return Dual(a.v - b.v, a.d - b.d); }
-inline Dual operator*(const Dual& a, const Dual& b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
-inline Dual operator/(const Dual& a, const Dual& b) {
-    double q = a.v / b.v;
-    return Dual(q, (a.d - q * b.d) / b.v);
-}
-inline bool operator<(const Dual& a, const Dual& b) { return a.v < b.v; }
-inline bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
-inline bool operator<=(const Dual& a, const Dual& b) { return a.v <= b.v; }
-inline bool operator>=(const Dual& a, const Dual& b) { return a.v >= b.v; }
-inline bool operator==(const Dual& a, const Dual& b) { return a.v == b.v; }
-inline bool operator!=(const Dual& a, const Dual& b) { return a.v != b.v; }
+using Dual = DualT<double>;
+using DualF = DualT<float>;
+/* mixed single/double operands promote to double, as float op double does */
+#define GF_MIXED(op)                                                                          \
+    inline Dual operator op(const DualF& a, const Dual& b) { return Dual(a) op b; }           \
+    inline Dual operator op(const Dual& a, const DualF& b) { return a op Dual(b); }
+GF_MIXED(+) GF_MIXED(-) GF_MIXED(*) GF_MIXED(/)
+#undef GF_MIXED
+#define GF_MIXED_CMP(op)                                                                      \
+    inline bool operator op(const DualF& a, const Dual& b) { return (double)a.v op b.v; }     \
+    inline bool operator op(const Dual& a, const DualF& b) { return a.v op (double)b.v; }
+GF_MIXED_CMP(<) GF_MIXED_CMP(>) GF_MIXED_CMP(<=) GF_MIXED_CMP(>=) GF_MIXED_CMP(==) GF_MIXED_CMP(!=)
+#undef GF_MIXED_CMP
 namespace std {
-inline Dual sqrt(const Dual& x) {
-    double r = std::sqrt(x.v);
-    return Dual(r, r > 0 ? x.d / (2.0 * r) : 0.0);
+template <class T>
+inline DualT<T> sqrt(const DualT<T>& x) {
+    T r = std::sqrt(x.v);
+    return DualT<T>::make(r, r > 0 ? x.d / (2.0 * (double)r) : 0.0);
 }
 inline Dual exp(const Dual& x) {
     double e = std::exp(x.v);
     return Dual(e, e * x.d);
 }
-inline Dual atan2(const Dual& y, const Dual& x) {
-    double q = x.v * x.v + y.v * y.v;
-    return Dual(std::atan2(y.v, x.v), q > 0 ? (x.v * y.d - y.v * x.d) / q : 0.0);
+template <class T>
+inline DualT<T> atan2(const DualT<T>& y, const DualT<T>& x) {
+    double xv = x.v, yv = y.v, q = xv * xv + yv * yv;
+    return DualT<T>::make(std::atan2(y.v, x.v), q > 0 ? (xv * y.d - yv * x.d) / q : 0.0);
 }
-inline Dual cos(const Dual& x) { return Dual(std::cos(x.v), -std::sin(x.v) * x.d); }
-inline Dual sin(const Dual& x) { return Dual(std::sin(x.v), std::cos(x.v) * x.d); }
-inline Dual fabs(const Dual& x) { return x.v < 0 ? -x : x; }
+template <class T>
+inline DualT<T> cos(const DualT<T>& x) { return DualT<T>::make(std::cos(x.v), -std::sin((double)x.v) * x.d); }
+template <class T>
+inline DualT<T> sin(const DualT<T>& x) { return DualT<T>::make(std::sin(x.v), std::cos((double)x.v) * x.d); }
+template <class T>
+inline DualT<T> fabs(const DualT<T>& x) { return x.v < 0 ? -x : x; }
 }  // namespace std
 
 namespace {
@@ -132,6 +176,10 @@ template <class R> inline R rmin(R a, R b) { return (a < b) ? a : b; }
 inline float rexp(float x) { return (float)std::exp((double)x); }
 inline double rexp(double x) { return std::exp(x); }
 inline Dual rexp(const Dual& x) { return std::exp(x); }
+inline DualF rexp(const DualF& x) {
+    double e = std::exp((double)x.v);
+    return DualF::make((float)e, e * x.d);
+}
 
 /* x**5 with an integer exponent as the Fortran compiler expands it:
  * x2 = x*x, x3 = x2*x, x5 = x3*x2 */
@@ -1604,12 +1652,15 @@ int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, dou
     }
 }
 
+} /* extern "C" */
+
 /* Forward-mode derivative of nsteps FP64 steps along one direction: the
  * tangents seed_mu of const(9) (tanfi), seed_xi of const(3) (xi), seed_ty of
  * const(6) (the Bingham yield stress), seed_m of the volumes and seed_x,
  * seed_v of the initial positions and velocities.  Returns the final
  * positions, velocities and depths and their tangents. */
-int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+template <class R>
+int tangent_run(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
                    const double* topol, int n, const double* x, const double* v, const double* rho,
                    const double* mass, const double* hsml, const int* flag, int nsteps, double dt, double t,
                    double seed_mu, double seed_xi, double seed_ty, const double* seed_m, const double* seed_x,
@@ -1617,7 +1668,7 @@ int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ym
                    double* tan_h) {
     if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || n < 0 || nx < 2 || ny < 2) return GFSPH_ERR_ARG;
     if (p->summation_density != 1 || p->nor_density != 0) return GFSPH_ERR_UNSUPPORTED;
-    Oracle<Dual, Dual> o;
+    Oracle<R, Dual> o;
     int st = o.setup(p, nx, ny, xmin, ymin, dx, dy, topol);
     if (st) return st;
     o.cst[9].d = seed_mu;
@@ -1627,28 +1678,52 @@ int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ym
     o.x.resize(2 * (size_t)n); o.v.resize(2 * (size_t)n);
     o.rho.resize(n); o.mass.resize(n); o.hsml.resize(n);
     for (size_t k = 0; k < 2 * (size_t)n; k++) {
-        o.x[k] = Dual(x[k], seed_x ? seed_x[k] : 0.0);
-        o.v[k] = Dual(v[k], seed_v ? seed_v[k] : 0.0);
+        o.x[k] = R(x[k], seed_x ? seed_x[k] : 0.0);
+        o.v[k] = R(v[k], seed_v ? seed_v[k] : 0.0);
     }
     for (int k = 0; k < n; k++) {
-        o.rho[k] = Dual(rho[k]);
-        o.mass[k] = Dual(mass[k], seed_m ? seed_m[k] : 0.0);
-        o.hsml[k] = Dual(hsml[k]);
+        o.rho[k] = R(rho[k]);
+        o.mass[k] = R(mass[k], seed_m ? seed_m[k] : 0.0);
+        o.hsml[k] = R(hsml[k]);
     }
     o.flag.assign(flag, flag + n);
-    o.p.assign(n, Dual(0.0));
-    o.ex.assign(2 * (size_t)n, Dual(0.0)); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
-    o.dt = Dual(dt);
+    o.p.assign(n, R(0.0));
+    o.ex.assign(2 * (size_t)n, R(0.0)); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
+    o.dt = R(dt);
     o.time = t;
     o.init_pwp(nullptr);
     int status = 0;
     for (int s2 = 0; s2 < nsteps && !status; s2++) status = o.step();
     for (size_t k = 0; k < 2 * (size_t)n; k++) {
-        out_x[k] = o.x[k].v; out_v[k] = o.v[k].v;
+        out_x[k] = (double)o.x[k].v; out_v[k] = (double)o.v[k].v;
         tan_x[k] = o.x[k].d; tan_v[k] = o.v[k].d;
     }
-    for (int k = 0; k < n; k++) { out_h[k] = o.rho[k].v; tan_h[k] = o.rho[k].d; }
+    for (int k = 0; k < n; k++) { out_h[k] = (double)o.rho[k].v; tan_h[k] = o.rho[k].d; }
     return status;
+}
+
+extern "C" {
+
+/* The FP64 step (values and derivatives in double). */
+int oracle_tangent(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+                   const double* topol, int n, const double* x, const double* v, const double* rho,
+                   const double* mass, const double* hsml, const int* flag, int nsteps, double dt, double t,
+                   double seed_mu, double seed_xi, double seed_ty, const double* seed_m, const double* seed_x,
+                   const double* seed_v, double* out_x, double* out_v, double* out_h, double* tan_x, double* tan_v,
+                   double* tan_h) {
+    return tangent_run<Dual>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, seed_mu, seed_xi, seed_ty, seed_m, seed_x, seed_v, out_x, out_v, out_h, tan_x, tan_v, tan_h);
+}
+
+/* The single-precision step of mode 1 (FP32 values, FP64 sums), rounded as
+ * its FP32 arithmetic rounds, with the derivatives in double: the exact
+ * derivative of the trajectory the device computes. */
+int oracle_tangent32(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
+                   const double* topol, int n, const double* x, const double* v, const double* rho,
+                   const double* mass, const double* hsml, const int* flag, int nsteps, double dt, double t,
+                   double seed_mu, double seed_xi, double seed_ty, const double* seed_m, const double* seed_x,
+                   const double* seed_v, double* out_x, double* out_v, double* out_h, double* tan_x, double* tan_v,
+                   double* tan_h) {
+    return tangent_run<DualF>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, nsteps, dt, t, seed_mu, seed_xi, seed_ty, seed_m, seed_x, seed_v, out_x, out_v, out_h, tan_x, tan_v, tan_h);
 }
 
 /* Persistent oracle run: create on a state, advance, read back, free. */

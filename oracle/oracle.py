@@ -31,11 +31,14 @@ _IP = C.POINTER(C.c_int)
 def build():
     """Builds the checker library (and the OpenMP one where the compiler
     takes -fopenmp) when missing or older than the source."""
-    src = os.path.join(HERE, "gfsph_oracle.cpp")
-    hdr = os.path.join(HERE, "..", "include", "gfsph.h")
-    newest = max(os.path.getmtime(src), os.path.getmtime(hdr))
+    def mtime(*names):
+        return max(os.path.getmtime(os.path.join(HERE, f)) for f in names)
+
+    hdr = os.path.join("..", "include", "gfsph.h")
+    newest = mtime("gfsph_oracle.cpp", "gfl_oracle.cpp", hdr)
+    newest_omp = mtime("gfsph_oracle.cpp", hdr)  # the OpenMP build holds the SPH step only
     if not (os.path.exists(LIB) and os.path.getmtime(LIB) >= newest
-            and (not os.path.exists(LIB_OMP) or os.path.getmtime(LIB_OMP) >= newest)):
+            and (not os.path.exists(LIB_OMP) or os.path.getmtime(LIB_OMP) >= newest_omp)):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB
 
@@ -115,16 +118,21 @@ def lib(omp=False):
         L.oracle_gradhs.restype = C.c_int
         L.oracle_gradhs.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_int, _DP, _DP, _IP, _DP, C.c_int, _DP, _DP]
-        L.oracle_tangent.restype = C.c_int
-        L.oracle_tangent.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
-                                     _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_int, C.c_double, C.c_double,
-                                     C.c_double, C.c_double, C.c_double, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
+        for fn in (L.oracle_tangent, L.oracle_tangent32):
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                           _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, C.c_int, C.c_double, C.c_double,
+                           C.c_double, C.c_double, C.c_double, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP]
         L.oracle_get_pwp.restype = C.c_int
         L.oracle_get_pwp.argtypes = [C.c_void_p, _DP]
         L.oracle_free.restype = None
         L.oracle_free.argtypes = [C.c_void_p]
         L.oracle_set_threads.restype = C.c_int
         L.oracle_set_threads.argtypes = [C.c_int]
+        if hasattr(L, "oracle_gfl_run"):
+            L.oracle_gfl_run.restype = C.c_int
+            L.oracle_gfl_run.argtypes = [C.c_int, C.c_int, _DP, _IP, _DP, _DP, C.c_int, C.c_int, C.c_int, C.c_double,
+                                         C.c_double, _DP, _DP, _DP, C.c_int, C.c_double, _DP, _DP, _DP]
         L.oracle_solvegc2.restype = C.c_int
         L.oracle_solvegc2.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _DP, _DP, _DP, _DP,
                                       C.c_double, _IP]
@@ -344,16 +352,20 @@ def gradhs(mode, ix0, iy0, nwx, nwy, dx, dy, x=None, rho=None, flag=None, hs=Non
 
 
 def tangent(params, nx, ny, dx, dy, state, nsteps, seed_mu=0.0, seed_xi=0.0, seed_m=None, seed_x=None,
-            seed_v=None, xmin=0.0, ymin=0.0, seed_ty=0.0):
-    """FP64 forward-mode derivative of nsteps steps from `state` along one
+            seed_v=None, xmin=0.0, ymin=0.0, seed_ty=0.0, single=False):
+    """Forward-mode derivative of nsteps steps from `state` along one
     direction (tangents of const(9), const(3), const(6), volumes, positions,
-    velocities): returns (x, v, h, dx, dv, dh) at the end."""
+    velocities): returns (x, v, h, dx, dv, dh) at the end.  The FP64 step, or
+    with single=True the single-precision step of MODE_FP32 (its values
+    rounded as it rounds them, the derivatives in FP64): the exact
+    derivative of the trajectory the device computes."""
     n = state.x.shape[0]
     out = [np.zeros((n, 2)), np.zeros((n, 2)), np.zeros(n), np.zeros((n, 2)), np.zeros((n, 2)), np.zeros(n)]
     sm = _d(seed_m) if seed_m is not None else None
     sx = _d(seed_x) if seed_x is not None else None
     sv = _d(seed_v) if seed_v is not None else None
-    st = lib().oracle_tangent(C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), n, _dp(state.x),
+    fn = lib().oracle_tangent32 if single else lib().oracle_tangent
+    st = fn(C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol), n, _dp(state.x),
                               _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.hsml), _ip(state.flag),
                               nsteps, state.dt, state.t, seed_mu, seed_xi, seed_ty, _dp(sm), _dp(sx), _dp(sv),
                               *[_dp(a) for a in out])
@@ -518,3 +530,29 @@ def read_source_plus_new(pts_path, h_inf, xshift=0.0, yshift=0.0):
     yy, xx = np.meshgrid(gy, gx, indexing="ij")
     x = np.stack([xx.reshape(-1)[keep], yy.reshape(-1)[keep]], 1).astype(np.float32)
     return dict(x=x, h=h, mass=mass, hsml=np.full(h.size, delt2d * fact, np.float32))
+
+
+def gfl_run(coord, intmat, z, const, unkno, nsteps, dt, ntype=3, ngaus=3, niter=3, swl=0.0, comp=0.01, hs_w=None,
+            gradhs_w=None, time=0.0):
+    """The GFL Taylor-Galerkin step (gfl_oracle.cpp) nsteps times on the P1
+    mesh coord (npoin, 2), intmat (nelem, 3) 1-based, nodal Z; const {k:
+    constF(k)}; unkno (npoin, 3) of h, hu, hv.  Returns (unkno, time, topol
+    (npoin, 9), topel (nelem, 9)) in float64 holding single-precision values."""
+    coord = _d(coord)
+    intmat = np.ascontiguousarray(intmat, np.int32)
+    npoin, nelem = coord.shape[0], intmat.shape[0]
+    c15 = np.zeros(15)
+    for k, v in const.items():
+        if 1 <= k <= 14:
+            c15[k] = v
+    u = _d(unkno).copy()
+    t = C.c_double(time)
+    topol = np.zeros((npoin, 9))
+    topel = np.zeros((nelem, 9))
+    hs = _d(hs_w) if hs_w is not None else None
+    gh = _d(gradhs_w) if gradhs_w is not None else None
+    st = lib().oracle_gfl_run(npoin, nelem, _dp(coord), _ip(intmat), _dp(_d(z)), _dp(c15), ntype, ngaus, niter, swl,
+                              comp, _dp(hs), _dp(gh), _dp(u), nsteps, dt, C.byref(t), _dp(topol), _dp(topel))
+    if st:
+        raise RuntimeError(f"oracle_gfl_run: {st}")
+    return u, t.value, topol, topel

@@ -483,6 +483,31 @@ def test_tangent_oracle_matches_central_differences(oracle_mod):
     assert abs(fd - tg) <= 1e-5 * abs(tg)
 
 
+def test_single_precision_tangent_follows_the_fp32_trajectory(oracle_mod):
+    """The tangent on single-precision dual numbers: its values are the FP32
+    oracle's (FP32 state, FP64 sums) bit for bit, so its derivative is that of
+    the trajectory the device computes; it stays within 1e-3 of the FP64
+    tangent along tanfi and a volume direction."""
+    w = workloads.fractal_channel(n_target=1000, dem_k=7, cell=5.0, erosion=None)
+    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv, mode=oracle_mod.MODE_FP32)
+    st0 = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+    x32, v32, h32, _, _, _ = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, 10, seed_mu=1.0, single=True)
+    st = st0.copy()
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, 10)
+    assert np.array_equal(x32, st.x) and np.array_equal(v32, st.v) and np.array_equal(h32, st.rho)
+    rng = np.random.default_rng(3)
+    gx, gh = rng.normal(size=(w.n, 2)), rng.normal(size=w.n)
+    dm = rng.normal(size=w.n) * w.mass
+    for seed in (dict(seed_mu=1.0), dict(seed_m=dm)):
+        a = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, 10, single=True, **seed)
+        b = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, 10, **seed)
+        la = float((gx * a[3]).sum() + (gh * a[5]).sum())
+        lb = float((gx * b[3]).sum() + (gh * b[5]).sum())
+        assert la != 0.0 and abs(la - lb) <= 1e-3 * abs(lb), (seed.keys(), la, lb)
+
+
 def test_tangent_oracle_yield_stress_matches_central_differences(oracle_mod):
     """The same along the Bingham yield stress const(6) (nfric 4,
     SPH_SW_2019.f90:9552-9572) on a sliding release."""
