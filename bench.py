@@ -358,6 +358,58 @@ def cg_bench(args, gfsph, workloads, peak):
     return out
 
 
+def gfl_bench(args, gfsph, workloads, peak, nsteps=100):
+    """The GFL Taylor-Galerkin step on the coupled case's mesh: the 500 x
+    500-node window of the DEM background triangulation at 2 m (498,002
+    triangles), a dam break over a sloping bed with Manning and Voellmy
+    friction, 3 Gauss points, 3 consistent-mass sweeps.  Device time from CUDA
+    events around `nsteps` steps (one call).  Algorithmic bytes per step: per
+    node h, hu, hv read and written (24), Topol (36), the lumped mass (4) and
+    its adjacency row pointer (4); per element the connectivity (12), the
+    geometry (28), Topel (36) and its three adjacency entries (24); and per
+    further sweep the adjacency, the element areas and three node vectors
+    (rhs, the iterate in and out: 36 per node)."""
+    nw = 500
+    intmat, coord = workloads.p1_mesh(nw, nw, 2.0)
+    x, y = coord[:, 0], coord[:, 1]
+    z = (50.0 - 0.05 * x + 2.0 * np.sin(y / 40.0)).astype(np.float32)
+    u = np.zeros((coord.shape[0], 3), np.float32)
+    u[:, 0] = np.where(x < 300.0, 4.0, 0.0)
+    const = {1: 9.8, 2: 2000.0, 3: 0.03, 5: 5, 9: 0.2, 10: 0.02}
+    g = gfsph.Gfl(coord, intmat, z, const, ntype=3, ngaus=3, niter=3)
+    g.set_state(u)
+    dt = 0.02
+    g.step(10, dt)
+    t0 = time.perf_counter()
+    g.step(nsteps, dt)
+    host_s = time.perf_counter() - t0
+    dev_ms = g.device_ms()
+    launches = g.launch_count()
+    out_state, _ = g.state()
+    g.close()
+    npoin, nelem = coord.shape[0], intmat.shape[0]
+    niter = 3
+    bytes_step = npoin * (24 + 36 + 4 + 4) + nelem * (12 + 28 + 36 + 24) + (niter - 1) * (nelem * 28 + npoin * 36)
+    per_step = dev_ms / 1e3 / nsteps
+    out = {"mesh": f"{npoin} nodes, {nelem} triangles (500 x 500 window at 2 m)", "steps": nsteps,
+           "device_ms_per_step": per_step * 1e3, "host_ms_per_step": host_s * 1e3 / nsteps,
+           "node_steps_per_s": npoin / per_step, "launches_per_step": launches / (nsteps + 10),
+           "bytes_per_step": bytes_step, "achieved_gbs": bytes_step / per_step / 1e9,
+           "frac_of_hbm": bytes_step / per_step / 1e9 / peak, "finite": bool(np.isfinite(out_state).all()),
+           "note": "device time (CUDA events around the step call's kernels); the working set (~120 MB) is "
+                   "about the size of L2"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        k = 2
+        t0 = time.perf_counter()
+        oracle.gfl_run(coord.astype(np.float32), intmat, z, const, u, k, dt)
+        t_cpu = time.perf_counter() - t0
+        out["cpu_port"] = {"ms_per_step": t_cpu * 1e3 / k, "cores": 1, "kind": "port",
+                           "sample": f"set-up and {k} steps of the same mesh, FP32 restatement (set-up included)"}
+    return out
+
+
 def adjoint_bench(gfsph, workloads, torch, nsteps=1000, every=100):
     """The adjoint of the calibration case (config 5's shape): ~50k particles
     on a 512^2 DEM at 5 m (fixed smoothing lengths, no erosion, fixed dt),
@@ -627,6 +679,7 @@ def main():
     couple_line = couple_bench(sim, w, gfsph) if extras else None
     sim.close()
     cg_line = cg_bench(args, gfsph, workloads, peak) if extras else None
+    gfl_line = gfl_bench(args, gfsph, workloads, peak) if extras else None
     adj_line = adjoint_bench(gfsph, workloads, torch) if extras else None
     big_line = coupled_bench(gfsph, workloads, torch) if extras else None
     ens_line = None
@@ -661,6 +714,8 @@ def main():
             line["cpu_baseline"] = cpu
         if cg_line:
             line["cg"] = cg_line
+        if gfl_line:
+            line["gfl"] = gfl_line
         if adj_line:
             line["adjoint"] = adj_line
         if big_line:

@@ -402,6 +402,8 @@ struct gfsph_gfl {
     float *unkno = nullptr, *fnode = nullptr, *gp = nullptr, *rhs1 = nullptr, *rhs0a = nullptr, *rhs0b = nullptr;
     bool wir = false;
     long long launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the last gfsph_gfl_step
+    double last_ms = 0.0;
 };
 
 namespace {
@@ -412,6 +414,8 @@ void gfl_free(gfsph_gfl* g) {
                     g->fnode, g->gp, g->rhs1, g->rhs0a, g->rhs0b};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
     if (g->stream) cudaStreamDestroy(g->stream);
 }
 
@@ -640,7 +644,8 @@ int gfsph_gfl_create(const gfsph_gfl_params* p, int npoin, int nelem, const floa
     st |= dal(&g->mmatl, np); st |= dal(&g->hs_w, np); st |= dal(&g->gradhs_w, np);
     st |= dal(&g->unkno, 3 * np); st |= dal(&g->fnode, 9 * np); st |= dal(&g->gp, 9 * ne * (size_t)p->ngaus);
     st |= dal(&g->rhs1, 3 * np); st |= dal(&g->rhs0a, 3 * np); st |= dal(&g->rhs0b, 3 * np);
-    if (st || cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (st || cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&g->ev0) != cudaSuccess || cudaEventCreate(&g->ev1) != cudaSuccess) {
         gfl_free(g);
         delete g;
         return GFSPH_ERR_CUDA;
@@ -722,6 +727,7 @@ int gfsph_gfl_step(gfsph_gfl* g, int nsteps, float dt) try {
     GflDev d = view(g);
     const GflConst& c = g->c;
     cudaStream_t s = g->stream;
+    cudaEventRecord(g->ev0, s);
     for (int k = 0; k < nsteps; k++) {
         // tanfi of frictlaws: tanfi8 + (tanfi0 - tanfi8) exp(-time/Bfact) (:3856-3860)
         float tanfi = c.tanfi8;
@@ -739,7 +745,10 @@ int gfsph_gfl_step(gfsph_gfl* g, int nsteps, float dt) try {
         g->launches += 3 + (g->P.niter - 1) + 1;
         g->time = g->time + (double)dt;
     }
+    cudaEventRecord(g->ev1, s);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return GFSPH_ERR_CUDA;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess) g->last_ms = ms;
     return GFSPH_OK;
 } catch (...) {  // a C++ exception never crosses the C ABI
     return GFSPH_ERR_HOST;
@@ -755,5 +764,11 @@ int gfsph_gfl_topol(gfsph_gfl* g, float* topol, float* topel) try {
 }
 
 long long gfsph_gfl_launch_count(gfsph_gfl* g) { return g ? g->launches : -1; }
+
+int gfsph_gfl_device_ms(gfsph_gfl* g, double* ms) {
+    if (!g || !ms) return GFSPH_ERR_ARG;
+    *ms = g->last_ms;
+    return GFSPH_OK;
+}
 
 }  // extern "C"

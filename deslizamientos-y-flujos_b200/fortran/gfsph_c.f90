@@ -360,6 +360,11 @@ module gfsph_c
        import :: c_long_long, c_ptr
        type(c_ptr), value :: gfl
      end function
+     integer(c_int) function gfsph_gfl_device_ms(gfl, ms) bind(c, name="gfsph_gfl_device_ms")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: gfl
+       real(c_double), intent(out) :: ms
+     end function
      type(c_ptr) function gfsph_strerror(status) bind(c, name="gfsph_strerror")
        import :: c_int, c_ptr
        integer(c_int), value :: status

@@ -127,6 +127,7 @@ SIGNATURES = {
     "gfsph_gfl_step": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
     "gfsph_gfl_topol": (C.c_int, [C.c_void_p, _FP, _FP]),
     "gfsph_gfl_launch_count": (C.c_longlong, [C.c_void_p]),
+    "gfsph_gfl_device_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "gfsph_strerror": (C.c_char_p, [C.c_int]),
     "gfsph_version": (C.c_int, []),
     "gfsph_binary_version": (C.c_int, [_IP]),
@@ -466,6 +467,12 @@ class Gfl:
 
     def launch_count(self):
         return int(lib().gfsph_gfl_launch_count(self.h))
+
+    def device_ms(self):
+        """Device time of the last step call (its kernels)."""
+        ms = C.c_double(0.0)
+        _check(lib().gfsph_gfl_device_ms(self.h, C.byref(ms)), "gfsph_gfl_device_ms")
+        return ms.value
 
     def close(self):
         if self.h:

@@ -424,6 +424,9 @@ int gfsph_gfl_step(gfsph_gfl* g, int nsteps, float dt);
  * (Topol and Topel: Z, Zx, Zy, 1+Zx^2, ZxZy, 1+Zy^2, curvatures); either may be NULL. */
 int gfsph_gfl_topol(gfsph_gfl* g, float* topol, float* topel);
 long long gfsph_gfl_launch_count(gfsph_gfl* g);
+/* Device time of the last gfsph_gfl_step (CUDA events around its kernels).
+ * No counterpart in the reference. */
+int gfsph_gfl_device_ms(gfsph_gfl* g, double* ms);
 
 const char* gfsph_strerror(int status);
 int gfsph_version(void);
