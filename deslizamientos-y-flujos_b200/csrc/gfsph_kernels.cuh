@@ -859,9 +859,9 @@ __device__ __forceinline__ void density_regular(PState& A, const Search& Q, Step
                 // av_vel and the normalisation read them from the table
                 float w, d0, d1;
                 sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
-                if (cnt < Q.kcap)  // streamed out: the gathers keep L2
-                    __stcs(tab + (size_t)cnt * kTabStride,
-                           make_int4(j, __float_as_int(w), __float_as_int(d0), __float_as_int(d1)));
+                if (cnt < Q.kcap)  // kept in L2 for the internal force (written back to front)
+                    tab[(size_t)cnt * kTabStride] =
+                        make_int4(j, __float_as_int(w), __float_as_int(d0), __float_as_int(d1));
                 cnt++;
                 acc += (double)(o.w * w);
             });
@@ -1022,7 +1022,7 @@ __device__ __forceinline__ void internal_force(const Search& Q, const Rheo& c, i
         int4 e[4];
         float4 prj[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) e[u] = __ldcs(tab + (size_t)(k + u) * kTabStride);
+        for (int u = 0; u < 4; u++) e[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
         for (int u = 0; u < 4; u++) prj[u] = __ldg(&Q.pr[e[u].x]);
 #pragma unroll
@@ -1031,7 +1031,7 @@ __device__ __forceinline__ void internal_force(const Search& Q, const Rheo& c, i
                            a0, a1);
     }
     for (; k < cnt; k++) {
-        const int4 e = __ldcs(tab + (size_t)k * kTabStride);
+        const int4 e = __ldg(tab + (size_t)k * kTabStride);
         const float4 prj = __ldg(&Q.pr[e.x]);
         pressure_terms(c, pi_, rhoi, prj.x, prj.y, prj.z, __int_as_float(e.z), __int_as_float(e.w), a0, a1);
     }
@@ -1192,12 +1192,20 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
     if (c.icpwp == 3) B.pwp[i] = out ? 0.f : pwp_update(c, pwp, h, h - Q.rho0[i], dt);
 }
 
-// Internal acceleration of the regular particles, one thread each.
+// Internal acceleration of the regular particles, one thread each.  The
+// warps take the particles from the last to the first warp of the table:
+// the neighbour search has just written the table front to back, so its
+// last-written part (still in L2) is read first, and av_vel, which walks
+// the table front to back after this pass, starts on the part this pass
+// read last.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars* S, Rheo c, int n) {
     if (S->skip) return;
     const int nreg = S->nreg;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
+    const int nw = (nreg + 31) >> 5;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nw * 32; t += gridDim.x * blockDim.x) {
+        const int i = (nw - 1 - (t >> 5)) * 32 + (t & 31);
+        if (i >= nreg) continue;
         float in0, in1;
         internal_force(Q, c, i, in0, in1);
         Q.indv[i] = make_float2(in0, in1);
