@@ -23,7 +23,7 @@ enum KernelId {
     K_PREP, K_BOUNDS, K_HIST, K_SCAN_TILES, K_SCAN_ADD, K_SCATTER, K_CELL_SORT,
     K_REORDER, K_DENSITY, K_DENSITY_BIG, K_IFORCE, K_FORCE_BIG, K_FORCE_RK, K_XSPH, K_XSPH_BIG, K_DEM_ERODE,
     K_STEP_END, K_COPY, K_UNSORT, K_RASTER, K_HAZARD, K_EXPORT, K_MARK, K_BSCAN_TILES, K_BSCAN_ADD,
-    K_DENSITY_SPARSE, K_COUPLE, K_ADJOINT, K_NORM, K_NORM_BIG, K_STAGE,
+    K_DENSITY_SPARSE, K_COUPLE, K_ADJOINT, K_NORM, K_NORM_BIG, K_STAGE, K_WIR,
     K_STEPS,  // not a kernel: device time of whole gfsph_step batches (profile level 2)
     K_COUNT
 };
@@ -32,7 +32,7 @@ const char* kKernelNames[K_COUNT] = {
     "k_scatter", "k_cell_sort", "k_reorder", "k_density", "k_density_big", "k_iforce", "k_force_big",
     "k_force_rk", "k_xsph", "k_xsph_big", "k_dem_erode", "k_step_end", "k_copy_state", "k_unsort",
     "k_raster_idw", "k_hazard", "k_export_big", "k_mark", "k_scan_tiles(blocks)",
-    "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "k_adjoint", "k_norm", "k_norm_big", "k_stage", "step_batches"};
+    "k_scan_add(blocks)", "k_density(sparse)", "k_couple", "k_adjoint", "k_norm", "k_norm_big", "k_stage", "k_wir", "step_batches"};
 
 constexpr int kThreads = 128;
 static_assert(kThreads <= 32 * kScatterWarps, "erosion_scatter keeps shared terms for kScatterWarps warps");
@@ -156,6 +156,16 @@ struct gfsph_handle {
     float* rhoS = nullptr;   // the five depths of a step, k-major (nor_density)
     int2* rcell = nullptr;   // cell of the reference's grid per slot (skf 2, 3)
     float4* xsv = nullptr;   // (vx, vy, h, m) per slot after the RK update, for av_vel
+    // soil and water (ic_ws_Interact = 1): material per caller index and per
+    // slot; Z + hs and its gradient at the water particles; the soil-water
+    // pair sums; Z + hs per DEM node and its FP64 accumulators
+    unsigned char* spec_u = nullptr;
+    unsigned char* spec_a = nullptr;
+    float* zpw = nullptr;
+    float2* gzw = nullptr;
+    float2* bxy = nullptr;
+    float* wir_hsz = nullptr;
+    double2* wir_acc = nullptr;
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -266,7 +276,7 @@ void with_skf(const gfsph_handle* h, F&& f) {
 }
 
 // Stage-dependent pressure: the step runs the staged RK45 kernels.
-bool staged(const gfsph_handle* h) { return h->rheo.nor_density || h->rheo.cos_theta; }
+bool staged(const gfsph_handle* h) { return h->rheo.nor_density || h->rheo.cos_theta || h->rheo.ws; }
 
 void fork(gfsph_handle* h, int k) {
     if (!h->capturing) return;
@@ -294,6 +304,10 @@ Search make_search(gfsph_handle* h) {
     q.rho0 = h->rho0;
     q.rcell = h->rcell;
     q.xsv = h->xsv;
+    q.spec = h->spec_a;
+    q.zpw = h->zpw;
+    q.gzw = h->gzw;
+    q.bxy = h->bxy;
     q.kcap = h->kcap;
     return q;
 }
@@ -334,7 +348,7 @@ int enqueue_search(gfsph_handle* h, int advance) {
     launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
     launch(h, K_REORDER, [&] {
         k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S, h->rheo, h->rho0,
-                                           h->rcell);
+                                           h->rcell, h->spec_u, h->spec_a);
     }); nk++;
     // the coarse-level kernels run beside the regular ones when graphs are
     // captured (side stream); serially otherwise
@@ -398,6 +412,28 @@ int enqueue_stage_begin(gfsph_handle* h, const PState As[5]) {
     return 1;
 }
 
+// The soil surface under the water in stage s (ic_ws_Interact = 1): the
+// soil depths spread over the DEM nodes at the stage positions, Z + hs per
+// node, then Zp at the water particles and every particle's pressure term.
+int enqueue_wir_stage(gfsph_handle* h, const PState As[5], int s) {
+    const int n = h->n;
+    cudaStream_t st = h->stream;
+    StepScalars* S = h->S;
+    const Rheo& c = h->rheo;
+    Search q = make_search(h);
+    const int np = h->nx * h->ny;
+    launch(h, K_WIR, [&] {
+        k_wir_scatter<<<blocks_for(n), kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho, h->wir_acc);
+    });
+    launch(h, K_WIR, [&] {
+        k_wir_nodes<<<blocks_for((long long)np, 256), 256, 0, st>>>(h->wir_acc, h->d_z, h->wir_hsz, np, S);
+    });
+    launch(h, K_WIR, [&] {
+        k_wir_press<<<blocks_for(n), kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho, h->wir_hsz);
+    });
+    return 3;
+}
+
 // The staged RK45 body (nor_density or ic_cosTheta = 1): per stage the
 // internal force with that stage's pressure, then the stage of every
 // particle; the last stage finishes the step.  Everything on one stream.
@@ -409,7 +445,16 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
     Search q = make_search(h);
     const int pb = blocks_for(n);
     int nk = enqueue_norms(h, As);
-    nk += enqueue_stage_begin(h, As);
+    if (c.ws) {
+        with_skf(h, [&](auto sk) {
+            launch(h, K_WIR, [&] {
+                k_wir_pairs_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(h->A, q, S, c);
+            });
+        });
+        nk += 1 + enqueue_wir_stage(h, As, 0);
+    } else {
+        nk += enqueue_stage_begin(h, As);
+    }
     for (int s = 0; s < 4; s++) {
         launch(h, K_FORCE_BIG, [&] {
             with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[s], q, S, c); });
@@ -435,6 +480,7 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
             }
         });
         nk++;
+        if (c.ws && s < 3) nk += enqueue_wir_stage(h, As, s + 1);
     }
     return nk;
 }
@@ -535,9 +581,10 @@ int build_graph(gfsph_handle* h, int steps, cudaGraphExec_t* out) {
 }
 
 int kernels_per_step(const gfsph_handle* h) {
-    // staged: 10 k_norm launches with nor_density, k_stage_begin, four
-    // stages of (k_force_big, k_iforce, k_stage)
-    const int body = staged(h) ? (h->rheo.nor_density ? 10 : 0) + 1 + 12 : 3;
+    // staged: 10 k_norm launches with nor_density, k_stage_begin (with soil
+    // and water: k_wir_pairs_big and per stage k_wir_scatter, k_wir_nodes,
+    // k_wir_press), four stages of (k_force_big, k_iforce, k_stage)
+    const int body = staged(h) ? (h->rheo.nor_density ? 10 : 0) + (h->rheo.ws ? 13 : 1) + 12 : 3;
     return 13 + body + (h->rheo.av_vel ? 2 : 0) + 1;
 }
 
@@ -598,6 +645,7 @@ void free_particles(gfsph_handle* h) {
     dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv); dfree(h->rho0);
     dfree(h->carry.v); dfree(h->carry.acc); dfree(h->carry.dx); dfree(h->carry.dv); dfree(h->carry.xo);
     dfree(h->carry.out); dfree(h->rhoS); dfree(h->rcell); dfree(h->xsv); dfree(h->pr);
+    dfree(h->spec_u); dfree(h->spec_a); dfree(h->zpw); dfree(h->gzw); dfree(h->bxy);
     h->kcap = 0;
 }
 
@@ -732,6 +780,12 @@ int validate(const gfsph_params* p) {
     if (p->cst[0] < 0.f) return GFSPH_ERR_UNSUPPORTED;                 // inclined-plane gravity input
     if (p->cst[14] <= 1.e-8f || p->cst[9] <= 1.e-8f) return GFSPH_ERR_ARG;  // comp, hfrict0 (:1357-1365)
     if (!(p->dt > 0.f)) return GFSPH_ERR_ARG;
+    if (p->ws_interact != 0 && p->ws_interact != 1) return GFSPH_ERR_UNSUPPORTED;
+    if (p->sw_alg != 0 && p->sw_alg != 1) return GFSPH_ERR_UNSUPPORTED;
+    // soil and water: no erosion, pore pressure, normalised density or
+    // terrain-normal gravity with them here
+    if (p->ws_interact == 1 && (erosion || p->icpwp != 0 || p->nor_density != 0 || cos_theta != 0))
+        return GFSPH_ERR_UNSUPPORTED;
     return 0;
 }
 
@@ -851,6 +905,12 @@ int create_handle(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle* sha
     c.muI = (c.nfric == 8 || c.nfric == 26) ? 1 : (c.nfric == 27 ? 2 : 0);
     c.mu_a = k[2]; c.mu_r = k[5]; c.mu_b = k[6];
     if (c.muI) c.xi = 0.f;  // const(3) is a mu(I) parameter, not xi (:9653)
+    c.ws = p->ws_interact;
+    c.swalg = p->sw_alg;
+    {
+        const float densw = (k[17] < 1.e-3f) ? 1000.f : k[17];  // :9001
+        c.dens_ws = densw / c.dens;
+    }
 
     int nx = dem->nx, ny = dem->ny;
     size_t np = (size_t)nx * ny;
@@ -932,6 +992,11 @@ int create_handle(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle* sha
     d.ymax = d.ymin + (float)(ny - 1) * d.dy;
     d.grad = h->d_grad; d.curvA = h->d_curvA; d.curvB = h->d_curvB;
     }
+    if (c.ws) {
+        st = dalloc(&h->wir_hsz, np) | dalloc(&h->wir_acc, np);
+        if (st) { gfsph_destroy(h); return GFSPH_ERR_CUDA; }
+        cudaMemset(h->wir_acc, 0, np * sizeof(double2));
+    }
     std::memset(h->hS, 0, sizeof(StepScalars));
     h->hS->dt = p->dt;
     h->hS->time = 0.0;
@@ -959,7 +1024,7 @@ int gfsph_destroy(gfsph_handle* h) try {
     if (!h->dem_shared) { dfree(h->d_grad); dfree(h->d_curvA); dfree(h->d_curvB); }
     dfree(h->d_z); dfree(h->d_eroded); dfree(h->d_avail);
     dfree(h->d_auxv); dfree(h->S); dfree(h->bparts); dfree(h->d_racc); dfree(h->d_rout); dfree(h->d_lam);
-    dfree(h->d_lpart);
+    dfree(h->d_lpart); dfree(h->wir_hsz); dfree(h->wir_acc);
     dfree(h->haz_sum_h); dfree(h->haz_sum_v); dfree(h->haz_max_h); dfree(h->haz_max_v); dfree(h->haz_cnt);
     dfree(h->cw_a1); dfree(h->cw_a2); dfree(h->cw_hs); dfree(h->cw_ml); dfree(h->cw_rhs); dfree(h->cw_g0);
     dfree(h->cw_g1);
@@ -994,8 +1059,11 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
                  const float* hsml, const int* itype, const int* out_flag) try {
     if (!h || n < 1 || !x || !v || !rho || !mass || !hsml) return GFSPH_ERR_ARG;
     if (itype)
-        for (int i = 0; i < n; i++)
-            if (itype[i] != 1) return GFSPH_ERR_UNSUPPORTED;  // only soil particles (ic_ws_Interact = 0)
+        for (int i = 0; i < n; i++) {
+            if (itype[i] == 1) continue;
+            // water particles only with ic_ws_Interact = 1; no other types
+            if (itype[i] != 2 || !h->rheo.ws) return GFSPH_ERR_UNSUPPORTED;
+        }
     if (n != h->n) {
         CK(cudaStreamSynchronize(h->stream));
         drop_graphs(h);
@@ -1015,6 +1083,10 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
             if (h->rheo.nor_density) st |= dalloc(&h->rhoS, 5 * (size_t)n);
         }
         if (h->rheo.skf == 2 || h->rheo.skf == 3) st |= dalloc(&h->rcell, n);
+        if (h->rheo.ws) {
+            st |= dalloc(&h->spec_u, n); st |= dalloc(&h->spec_a, n); st |= dalloc(&h->zpw, n);
+            st |= dalloc(&h->gzw, n); st |= dalloc(&h->bxy, n);
+        }
         if (st) return drop_state(h, GFSPH_ERR_CUDA);
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
         if (st) return drop_state(h, st);
@@ -1037,6 +1109,13 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
     if (out_flag) CK(cudaMemcpyAsync(h->B.flag, out_flag, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
     else CK(cudaMemsetAsync(h->B.flag, 0, (size_t)n * sizeof(int), st));
     launch(h, K_UNSORT, [&] { k_iota<<<blocks_for(n), kThreads, 0, st>>>(h->B.id, n); });
+    if (h->rheo.ws) {  // the material of each particle, in caller order
+        std::vector<unsigned char> sp((size_t)n, 1);
+        if (itype)
+            for (int i = 0; i < n; i++) sp[i] = (unsigned char)itype[i];
+        CK(cudaMemcpyAsync(h->spec_u, sp.data(), (size_t)n, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));  // sp is a local
+    }
     if (h->rheo.icpwp == 3)
         launch(h, K_UNSORT, [&] {
             k_pwp_init<<<blocks_for(n), kThreads, 0, st>>>(h->B.pwp, h->B.rho, n, h->P.pwp0rel, h->P.cst[13]);
@@ -1301,7 +1380,7 @@ int gfsph_neighbours(gfsph_handle* h, int cap, int* offsets, int* idx) try {
     for (int s = 0; s < nreg; s++) {
         auto& L = lists[id[s]];
         for (int k = 0; k < cnt[s] && k < h->kcap; k++)
-            L.push_back(id[tab[tab_base(s, h->kcap) + (size_t)k * kTabStride].x]);
+            L.push_back(id[tab[tab_base(s, h->kcap) + (size_t)k * kTabStride].x & ~kCrossBit]);
     }
     if (nbig > 0) {  // pairs of the big particles, found on the device
         int pcap = 1 << 20;
@@ -1846,7 +1925,7 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     const Rheo& c = h->rheo;
     if (!(c.nfric == 4 || c.nfric == 5 || c.nfric == 6) || (c.nfric != 4 && c.xi < 0.f) || c.erosion ||
         c.icpwp != 0 || c.pa_sph != 2 || c.sle != 0 ||
-        c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f || c.nor_density || c.cos_theta ||
+        c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f || c.nor_density || c.cos_theta || c.ws ||
         (c.skf != 1 && c.skf != 4))
         return GFSPH_ERR_UNSUPPORTED;
     gfsph_adjoint* a = new (std::nothrow) gfsph_adjoint();

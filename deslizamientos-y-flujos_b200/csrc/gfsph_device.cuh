@@ -225,6 +225,12 @@ struct Rheo {
     // Mu2, r, I0 = const(3), (6), (7)), basal_friction_Ext_SW :9651-9668
     int muI;
     float mu_a, mu_r, mu_b;
+    // soil and water particles (ic_ws_Interact = 1, ic_SWalg sw_alg): pairs of
+    // one material only in the density, forces and av_vel; the soil-water
+    // pairs push the soil by -dens_ws g m_j grad W (SPH_SW_2019.f90:8502-8521,
+    // dens_ws = densw/dens :8999-9002); the water is a Manning fluid
+    int ws, swalg;
+    float dens_ws;
 };
 
 // x**y for a real exponent, evaluated in FP64 and rounded once.
@@ -410,6 +416,53 @@ __device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float
         ex0 = ex0 - ((er * vx) * L.hinv) * c.slip;
         ex1 = ex1 - ((er * vy) * L.hinv) * c.slip;
     }
+}
+
+// The same for ic_ws_Interact = 1 (no erosion, pore pressure or terrain-
+// normal gravity in its scope).  ex starts from the particle's soil-water pair
+// sum b (ExtForces_SW :8502-8521).  A water particle (:8600-8606) is a
+// Manning fluid, nfric 1 with n = const(3) (basal_friction_Ext_SW
+// :9426-9430), not frictional in the reversal filter; with ic_SWalg = 1 its
+// gravity is -g (h + Zp) grad Zp / h over the soil surface Zp = Z + hs
+// (Get_Grav_Ext_SW :9322-9331).
+__device__ __forceinline__ void ext_accel_wir(const Rheo& c, const DemView& d, float dt, float xx, float yy, float vx,
+                                              float vy, float hdepth, float in0, float in1, bool water, float zp,
+                                              float2 gzp, float2 b, float& ex0, float& ex1) {
+    ExtLocal L;
+    ext_locals(c, hdepth, vx, vy, L);
+    Rheo cw = c;
+    if (water) {
+        cw.nfric = 1;
+        cw.muI = 0;
+        cw.icpwp = 0;
+    }
+    float gz = c.g;
+    if (water) {
+        float zpx, zpy, top[6];
+        dem_lookup(d, xx, yy, zpx, zpy, false, top);
+        L.gravx = -(c.g * zpx);
+        L.gravy = -(c.g * zpy);
+        const float hfrict = (L.h > c.hfrict0) ? L.h : c.hfrict0;
+        const float cf1 = (c.g * c.xi) * c.xi;  // cmanning = const(3)
+        const float p73 = powr(hfrict, 7.f / 3.f);
+        L.frictx = ((cf1 * L.hu) * L.hvmod) / p73;
+        L.fricty = ((cf1 * L.hv) * L.hvmod) / p73;
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+        L.cf5 = 0.f;
+    } else {
+        grav_and_friction<false>(c, d, xx, yy, vx, vy, 0.f, L);
+    }
+    if (water && c.swalg == 1) {
+        const float hhsz = hdepth + zp;
+        ex0 = b.x - (gz * (hhsz * gzp.x)) / hdepth;
+        ex1 = b.y - (gz * (hhsz * gzp.y)) / hdepth;
+    } else {
+        ex0 = b.x + L.gravx;
+        ex1 = b.y + L.gravy;
+    }
+    reversal_filter(cw, dt, vx, vy, ex0 + in0, ex1 + in1, L);
+    ex0 = ex0 - L.frictx / L.h;
+    ex1 = ex1 - L.fricty / L.h;
 }
 
 // Hungr erosion rate after the RK update (ExtForces_SW(1), :8717-8760):

@@ -102,8 +102,18 @@ struct Search {
     float* rho0;         // depth at the start of the step, after Adaptive_dt's h_inf clamp (icpwp = 3)
     const int2* rcell;   // slot -> cell of the reference's own grid (skf 2, 3), else null
     float4* xsv;         // slot -> (vx, vy, h, m) after the RK update: what av_vel gathers
+    // ic_ws_Interact = 1: slot -> material (1 soil, 2 water); at the water
+    // particles Z + hs of the current stage and its gradient; per particle the
+    // sum of its soil-water pair terms.  A soil-water pair is kept in the
+    // neighbour table with the sign bit of j set (type 1 of
+    // Pint_Update_SW_tools): the density, the internal force and av_vel skip it.
+    const unsigned char* spec;
+    float* zpw;
+    float2* gzw;
+    float2* bxy;
     int kcap;
 };
+constexpr int kCrossBit = (int)0x80000000;
 
 __device__ __forceinline__ bool step_skipped(const StepScalars* S) { return S->skip != 0; }
 
@@ -659,7 +669,8 @@ __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, int*
 // rho0, the depth RK45 keeps at its start (after the h_inf clamp of
 // Adaptive_dt_sph_SW :6540, modes 1, 2 and 10).
 __global__ void k_reorder(const PState B, int n, const int* perm, const int2* keyrank, PState A, int* cellA,
-                          float4* xhm, const StepScalars* S, Rheo c, float* rho0, int2* rcell) {
+                          float4* xhm, const StepScalars* S, Rheo c, float* rho0, int2* rcell,
+                          const unsigned char* spec_u, unsigned char* spec_a) {
     if (S->skip) return;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = perm[s];
@@ -676,6 +687,7 @@ __global__ void k_reorder(const PState B, int n, const int* perm, const int2* ke
         A.hsml[s] = hs;
         A.flag[s] = B.flag[o];
         A.id[s] = B.id[o];
+        if (c.ws) spec_a[s] = spec_u[B.id[o]];
         cellA[s] = keyrank[o].x;
         xhm[s] = make_float4(p.x, p.y, hs, m);
         if (rcell && !B.flag[o]) {  // cell of the reference's grid (:1203-1204)
@@ -853,17 +865,20 @@ __device__ __forceinline__ void density_regular(PState& A, const Search& Q, Step
         double acc = (double)(sph_kernel_w<SKF>(0.f, hi) * me.w);
         int4* tab = Q.nbr + tab_base(i, Q.kcap);
         int cnt = 0;
+        const unsigned char si = c.ws ? Q.spec[i] : 0;
         for (int k = 0; k < nlev; k++)
             level_neighbours<SPARSE, SK>(Q, S, k, i, xi, hi, ci, [&](int j, float4 o, const PairGeom& g) {
                 // W and grad W of the pair, once per step: the internal force,
                 // av_vel and the normalisation read them from the table
                 float w, d0, d1;
                 sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+                const bool cross = c.ws && Q.spec[j] != si;
                 if (cnt < Q.kcap)  // kept in L2 for the internal force (written back to front)
                     tab[(size_t)cnt * kTabStride] =
-                        make_int4(j, __float_as_int(w), __float_as_int(d0), __float_as_int(d1));
+                        make_int4(cross ? (j | kCrossBit) : j, __float_as_int(w), __float_as_int(d0),
+                                  __float_as_int(d1));
                 cnt++;
-                acc += (double)(o.w * w);
+                if (!cross) acc += (double)(o.w * w);
             });
         Q.ncount[i] = cnt;
         if (cnt > Q.kcap) {  // table too small: stop this step before any state is written
@@ -939,7 +954,9 @@ __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepSca
     for (int b = warp; b < nbig; b += nwarps) {
         int i = nreg + b;
         double acc = 0.0;
+        const unsigned char si = c.ws ? Q.spec[i] : 0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+            if (c.ws && Q.spec[j] != si) return;  // type 1: not in the density (:1829)
             acc += (double)(o.w * sph_kernel_w<SKF>(g.r, g.mh));
         });
         acc = warp_sum(acc);
@@ -996,7 +1013,9 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
         int i = nreg + b;
         const float4 pri = Q.pr[i];
         double a0 = 0.0, a1 = 0.0;
+        const unsigned char si = c.ws ? Q.spec[i] : 0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+            if (c.ws && Q.spec[j] != si) return;  // type 0 only (:6899)
             const float4 prj = Q.pr[j];
             pressure_pair<SKF>(c, pri.x, pri.y, prj.x, prj.y, o.w, g, a0, a1);
         });
@@ -1024,16 +1043,18 @@ __device__ __forceinline__ void internal_force(const Search& Q, const Rheo& c, i
 #pragma unroll
         for (int u = 0; u < 4; u++) e[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
-        for (int u = 0; u < 4; u++) prj[u] = __ldg(&Q.pr[e[u].x]);
+        for (int u = 0; u < 4; u++) prj[u] = __ldg(&Q.pr[e[u].x & ~kCrossBit]);
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            pressure_terms(c, pi_, rhoi, prj[u].x, prj[u].y, prj[u].z, __int_as_float(e[u].z), __int_as_float(e[u].w),
-                           a0, a1);
+            if (e[u].x >= 0)  // type 0 only (:6899)
+                pressure_terms(c, pi_, rhoi, prj[u].x, prj[u].y, prj[u].z, __int_as_float(e[u].z),
+                               __int_as_float(e[u].w), a0, a1);
     }
     for (; k < cnt; k++) {
         const int4 e = __ldg(tab + (size_t)k * kTabStride);
-        const float4 prj = __ldg(&Q.pr[e.x]);
-        pressure_terms(c, pi_, rhoi, prj.x, prj.y, prj.z, __int_as_float(e.z), __int_as_float(e.w), a0, a1);
+        const float4 prj = __ldg(&Q.pr[e.x & ~kCrossBit]);
+        if (e.x >= 0)
+            pressure_terms(c, pi_, rhoi, prj.x, prj.y, prj.z, __int_as_float(e.z), __int_as_float(e.w), a0, a1);
     }
     in0 = (float)a0;
     in1 = (float)a1;
@@ -1397,6 +1418,158 @@ __global__ void __launch_bounds__(128) k_stage_begin(PState A, Search Q, StepSca
     }
 }
 
+// ---------------------------------------------------- soil and water (ic_ws_Interact = 1)
+// Position of an active particle in RK45 stage s (s = 0: the step start; a
+// frozen particle has none).  The same arithmetic as k_stage's.
+__device__ __forceinline__ bool wir_stage_pos(const PState& A, const StageCarry& C, int s, float dt, int i,
+                                              float2& p) {
+    if (s == 0) {
+        p = A.pos[i];
+        return true;
+    }
+    if (C.out[i]) return false;
+    const float f1 = (s == 3) ? 1.f : 0.5f;
+    const float2 x0 = A.pos[i], vp = C.v[i];
+    const float fdt = f1 * dt;
+    p = make_float2(x0.x + fdt * vp.x, x0.y + fdt * vp.y);
+    return true;
+}
+
+// Get_hs_at_w_SW (SPH_SW_2019.f90:17789-17857): each soil particle's depth
+// spread over the 4 x 4 DEM nodes around it with weights 1/max(1e-6, dist),
+// summed in FP64.
+__global__ void __launch_bounds__(128) k_wir_scatter(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
+                                                     StageCarry C, int s, const float* hdep, double2* acc) {
+    if (S->skip) return;
+    const int nact = S->nactive;
+    const float dt = S->dt_step;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
+        if (Q.spec[i] != 1) continue;
+        float2 p;
+        if (!wir_stage_pos(A, C, s, dt, i, p) || out_of_box(dem, p.x, p.y)) continue;
+        const float h = hdep[i];
+        const int ipx = (int)((p.x - dem.xmin) / dem.dx + 1.f), ipy = (int)((p.y - dem.ymin) / dem.dy + 1.f);
+        const int x0 = max(1, ipx - 1), y0 = max(1, ipy - 1), x1 = min(dem.nx, ipx + 2), y1 = min(dem.ny, ipy + 2);
+        for (int inx = x0; inx <= x1; inx++)
+            for (int iny = y0; iny <= y1; iny++) {
+                const int ip = (iny - 1) * dem.nx + (inx - 1);
+                float dx2 = p.x - (dem.xmin + (float)(inx - 1) * dem.dx);
+                dx2 = dx2 * dx2;
+                float dy2 = p.y - (dem.ymin + (float)(iny - 1) * dem.dy);
+                dy2 = dy2 * dy2;
+                float dist = sqrtf(dx2 + dy2);
+                dist = (1.e-6f > dist) ? 1.e-6f : dist;
+                atomicAdd(&acc[ip].x, (double)(h / dist));
+                atomicAdd(&acc[ip].y, (double)(1.f / dist));
+            }
+    }
+}
+
+// Z + hs at the DEM nodes (:17861-17867); the accumulators are left zeroed
+// for the next stage.
+__global__ void k_wir_nodes(double2* acc, const float* z, float* hsz, int np, const StepScalars* S) {
+    if (S->skip) return;
+    for (int ip = blockIdx.x * blockDim.x + threadIdx.x; ip < np; ip += gridDim.x * blockDim.x) {
+        const double2 a = acc[ip];
+        hsz[ip] = (a.y > (double)1.e-6f) ? z[ip] + (float)(a.x / a.y) : z[ip];
+        acc[ip] = make_double2(0.0, 0.0);
+    }
+}
+
+// One soil-water pair term of ExtForces_SW (:8502-8521) for particle i from
+// its table entry (gradient d of W_ij with x_i - x_j): a soil particle gets
+// -dens_ws g m_j grad W; a water particle, with ic_SWalg = 0, +g m_j grad W
+// of the pair taken from the soil side (-d here).
+__device__ __forceinline__ void wir_pair_term(const Rheo& c, bool water, float mj, float d0, float d1, double& b0,
+                                              double& b1) {
+    if (!water) {
+        b0 -= (double)(((c.dens_ws * c.g) * mj) * d0);
+        b1 -= (double)(((c.dens_ws * c.g) * mj) * d1);
+    } else if (c.swalg == 0) {
+        b0 += (double)(-((c.g * mj) * d0));
+        b1 += (double)(-((c.g * mj) * d1));
+    }
+}
+
+// Per active particle in stage s: at a water particle Z + hs of the soil
+// and its gradient, bilinear on its DEM cell (:17869-17933; a particle on the
+// far edge of the DEM takes the last cell); then the pressure term of the
+// stage (IntForces_SW :6793-6828): g/2 (h^2 - Zp^2) for the water with
+// ic_SWalg = 1, g/2 h^2 otherwise, h clamped to h_inf.  In stage 0 also the
+// soil-water pair sum of every regular particle, from its table.
+__global__ void __launch_bounds__(128) k_wir_press(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
+                                                   StageCarry C, int s, const float* hdep, const float* hsz) {
+    if (S->skip) return;
+    const int nact = S->nactive, nreg = S->nreg;
+    const float dt = S->dt_step;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
+        const bool water = Q.spec[i] == 2;
+        if (s == 0 && i < nreg) {
+            double b0 = 0.0, b1 = 0.0;
+            const int cnt = Q.ncount[i];
+            const int4* tab = Q.nbr + tab_base(i, Q.kcap);
+            for (int k = 0; k < cnt; k++) {
+                const int4 e = tab[(size_t)k * kTabStride];
+                if (e.x >= 0) continue;
+                wir_pair_term(c, water, Q.xhm[e.x & ~kCrossBit].w, __int_as_float(e.z), __int_as_float(e.w), b0, b1);
+            }
+            Q.bxy[i] = make_float2((float)b0, (float)b1);
+        }
+        float2 p;
+        if (!wir_stage_pos(A, C, s, dt, i, p) || out_of_box(dem, p.x, p.y)) {  // keeps its term
+            Q.pr[i] = make_float4(Q.pterm[i], hdep[i], A.mass[i], 0.f);
+            continue;
+        }
+        float zp = 0.f;
+        if (water) {
+            int ipx = (int)((p.x - dem.xmin) / dem.dx + 1.f), ipy = (int)((p.y - dem.ymin) / dem.dy + 1.f);
+            ipx = min(max(ipx, 1), dem.nx - 1);
+            ipy = min(max(ipy, 1), dem.ny - 1);
+            const int n1 = (ipy - 1) * dem.nx + (ipx - 1), n2 = n1 + 1, n3 = n1 + 1 + dem.nx, n4 = n3 - 1;
+            const float xref = dem.xmin + (float)(ipx - 1) * dem.dx, yref = dem.ymin + (float)(ipy - 1) * dem.dy;
+            const float xi = (p.x - xref) / dem.dx, eta = (p.y - yref) / dem.dy;
+            const float sh1 = (1.f - xi) * (1.f - eta), sh2 = xi * (1.f - eta), sh3 = xi * eta, sh4 = (1.f - xi) * eta;
+            const float d1x = (-1.f + eta) / dem.dx, d2x = (1.f - eta) / dem.dx, d3x = eta / dem.dx, d4x = (-eta) / dem.dx;
+            const float d1y = (-1.f + xi) / dem.dy, d2y = (-xi) / dem.dy, d3y = xi / dem.dy, d4y = (1.f - xi) / dem.dy;
+            const float h1 = hsz[n1], h2 = hsz[n2], h3 = hsz[n3], h4 = hsz[n4];
+            zp = ((sh1 * h1 + sh2 * h2) + sh3 * h3) + sh4 * h4;
+            Q.zpw[i] = zp;
+            Q.gzw[i] = make_float2(((h1 * d1x + h2 * d2x) + h3 * d3x) + h4 * d4x,
+                                   ((h1 * d1y + h2 * d2y) + h3 * d3y) + h4 * d4y);
+        }
+        const float h = hdep[i];
+        const float hc = (h < c.h_inf) ? c.h_inf : h;
+        const float p_ = (water && c.swalg == 1) ? c.cgra05 * (hc * hc - zp * zp) : (c.cgra05 * hc) * hc;
+        const float pt = (c.pa_sph == 1) ? p_ : p_ / (hc * hc);
+        Q.pterm[i] = pt;
+        Q.pr[i] = make_float4(pt, h, A.mass[i], 0.f);
+    }
+}
+
+// The soil-water pair sums of the coarse-level particles, one warp each.
+template <int SKF>
+__global__ void __launch_bounds__(128) k_wir_pairs_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    constexpr int SK = SupportScale<SKF>::value;
+    if (S->skip) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nreg = S->nreg, nbig = S->nbig;
+    for (int b = warp; b < nbig; b += nwarps) {
+        const int i = nreg + b;
+        const unsigned char si = Q.spec[i];
+        double b0 = 0.0, b1 = 0.0;
+        warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+            if (Q.spec[j] == si) return;
+            float w, d0, d1;
+            sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+            wir_pair_term(c, si == 2, o.w, d0, d1, b0, b1);
+        });
+        b0 = warp_sum(b0);
+        b1 = warp_sum(b1);
+        if (lane == 0) Q.bxy[i] = make_float2((float)b0, (float)b1);
+    }
+}
+
 // RK45 stage s = 0, 1, 2 of every active particle (SPH_MAIN_2019.f90:808-906):
 // x = x0 + c_s dt v, v = v0 + c_s dt (ex + in), the out-of-domain check,
 // ExtForces_SW(0) with the stage depth hs_ (clamped as IntForces_SW leaves
@@ -1436,7 +1609,11 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
         const float2 fin = Q.indv[i];
         const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
         float ex0, ex1;
-        ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
+        if (c.ws)
+            ext_accel_wir(c, dem, dt, xx, xy, vx, vy, hc, fin.x, fin.y, Q.spec[i] == 2, Q.zpw[i], Q.gzw[i], Q.bxy[i],
+                          ex0, ex1);
+        else
+            ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
         const float a0 = ex0 + fin.x, a1 = ex1 + fin.y;
         dv.x = dv.x + f2 * a0;
         dv.y = dv.y + f2 * a1;
@@ -1446,6 +1623,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
         C.acc[i] = make_float2(a0, a1);
         C.dx[i] = dx;
         C.dv[i] = dv;
+        if (c.ws) continue;  // the next stage's pressure needs its soil surface: k_wir_press
         const float fdn = f1n * dt;
         const float nx_ = x0.x + fdn * vx, ny_ = x0.y + fdn * vy;
         float pt = Q.pterm[i];
@@ -1502,7 +1680,11 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
                 const float hc = (h < c.h_inf) ? c.h_inf : h;
                 const float2 fin = Q.indv[i];
                 float ex0, ex1;
-                ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
+                if (c.ws)
+                    ext_accel_wir(c, dem, dt, xx, xy, vx, vy, hc, fin.x, fin.y, Q.spec[i] == 2, Q.zpw[i], Q.gzw[i],
+                                  Q.bxy[i], ex0, ex1);
+                else
+                    ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
                 dv.x = dv.x + 1.f * (ex0 + fin.x);
                 dv.y = dv.y + 1.f * (ex1 + fin.y);
                 dx.x = dx.x + 1.f * vx;
@@ -1554,15 +1736,17 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
 #pragma unroll
             for (int u = 0; u < 4; u++) e[u] = __ldcs(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
-            for (int u = 0; u < 4; u++) sj[u] = Q.xsv[e[u].x];
+            for (int u = 0; u < 4; u++) sj[u] = Q.xsv[e[u].x & ~kCrossBit];
 #pragma unroll
             for (int u = 0; u < 4; u++)
-                xsph_terms(vi, rhoi, make_float2(sj[u].x, sj[u].y), sj[u].z, sj[u].w, __int_as_float(e[u].y), a0, a1);
+                if (e[u].x >= 0)  // type 0 only (SPH_MAIN_2019.f90:3071)
+                    xsph_terms(vi, rhoi, make_float2(sj[u].x, sj[u].y), sj[u].z, sj[u].w, __int_as_float(e[u].y), a0,
+                               a1);
         }
         for (; k < cnt; k++) {
             const int4 e = __ldcs(tab + (size_t)k * kTabStride);
-            const float4 sj = Q.xsv[e.x];
-            xsph_terms(vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, __int_as_float(e.y), a0, a1);
+            const float4 sj = Q.xsv[e.x & ~kCrossBit];
+            if (e.x >= 0) xsph_terms(vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, __int_as_float(e.y), a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
@@ -1583,7 +1767,9 @@ __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalar
         const float2 vi = make_float2(si.x, si.y);
         const float rhoi = si.z;
         double a0 = 0.0, a1 = 0.0;
+        const unsigned char si_ = c.ws ? Q.spec[i] : 0;
         warp_neighbours<SK>(Q, S, i, lane, [&](int j, float4 o, const PairGeom& g) {
+            if (c.ws && Q.spec[j] != si_) return;  // type 0 only (SPH_MAIN_2019.f90:3071)
             const float4 sj = Q.xsv[j];
             xsph_pair<SKF>(vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, g, a0, a1);
         });

@@ -28,7 +28,9 @@ module gfsph_c
      integer(c_int) :: dem_deriv, max_neighbours
      integer(c_int) :: icpwp                   ! 0 or 3 (Get_Pwp_SW, nUaux = 1)
      real(c_float)  :: pwp0rel                 ! initial Uaux = pwp0rel * rho * const(14)
-     integer(c_int) :: reserved(6)
+     integer(c_int) :: ws_interact              ! ic_ws_Interact (0 or 1)
+     integer(c_int) :: sw_alg                   ! ic_SWalg (0 or 1) with ws_interact = 1
+     integer(c_int) :: reserved(4)
   end type gfsph_params
 
   type, bind(c) :: gfsph_dem

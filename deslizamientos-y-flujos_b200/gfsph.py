@@ -46,7 +46,8 @@ class Params(C.Structure):
         ("pa_sph", C.c_int), ("nnps", C.c_int), ("sle", C.c_int), ("skf", C.c_int),
         ("summation_density", C.c_int), ("average_velocity", C.c_int), ("nor_density", C.c_int),
         ("ic_adapt", C.c_int), ("h_inf", C.c_float), ("dt", C.c_float), ("dem_deriv", C.c_int),
-        ("max_neighbours", C.c_int), ("icpwp", C.c_int), ("pwp0rel", C.c_float), ("reserved", C.c_int * 6),
+        ("max_neighbours", C.c_int), ("icpwp", C.c_int), ("pwp0rel", C.c_float), ("ws_interact", C.c_int),
+        ("sw_alg", C.c_int), ("reserved", C.c_int * 4),
     ]
 
 
@@ -174,7 +175,8 @@ def _ip(a):
 
 
 def make_params(const=None, *, pa_sph=2, nnps=2, sle=1, skf=1, summation_density=1, average_velocity=1,
-                nor_density=0, ic_adapt=0, h_inf=0.01, dt=0.01, dem_deriv=1, max_neighbours=0, icpwp=0, pwp0rel=0.0):
+                nor_density=0, ic_adapt=0, h_inf=0.01, dt=0.01, dem_deriv=1, max_neighbours=0, icpwp=0, pwp0rel=0.0,
+                ws_interact=0, sw_alg=0):
     """Params from a {k: value} map of the reference's const(k) (1-based)."""
     p = Params()
     for k, val in (const or {}).items():
@@ -183,6 +185,7 @@ def make_params(const=None, *, pa_sph=2, nnps=2, sle=1, skf=1, summation_density
     p.summation_density, p.average_velocity, p.nor_density = summation_density, average_velocity, nor_density
     p.ic_adapt, p.h_inf, p.dt, p.dem_deriv, p.max_neighbours = ic_adapt, h_inf, dt, dem_deriv, max_neighbours
     p.icpwp, p.pwp0rel = icpwp, pwp0rel
+    p.ws_interact, p.sw_alg = ws_interact, sw_alg
     return p
 
 
@@ -234,15 +237,18 @@ class Sim:
         except Exception:
             pass
 
-    def upload(self, x, v, rho, mass, hsml, flag=None):
+    def upload(self, x, v, rho, mass, hsml, flag=None, itype=None):
+        """itype: the material of each particle (1 soil, 2 water; water only
+        with ws_interact = 1); None is all soil."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         n = x.shape[0]
         self._up = [x, np.ascontiguousarray(v, dtype=np.float32), np.ascontiguousarray(rho, dtype=np.float32),
                     np.ascontiguousarray(mass, dtype=np.float32), np.ascontiguousarray(hsml, dtype=np.float32),
-                    None if flag is None else np.ascontiguousarray(flag, dtype=np.int32)]
+                    None if flag is None else np.ascontiguousarray(flag, dtype=np.int32),
+                    None if itype is None else np.ascontiguousarray(itype, dtype=np.int32)]
         a = self._up
-        _check(lib().gfsph_upload(self.h, n, _fp(a[0]), _fp(a[1]), _fp(a[2]), _fp(a[3]), _fp(a[4]), None, _ip(a[5])),
-               "gfsph_upload")
+        _check(lib().gfsph_upload(self.h, n, _fp(a[0]), _fp(a[1]), _fp(a[2]), _fp(a[3]), _fp(a[4]), _ip(a[6]),
+                                  _ip(a[5])), "gfsph_upload")
         self.n = n
 
     def download(self, out=None):

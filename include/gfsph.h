@@ -84,7 +84,11 @@ typedef struct gfsph_params {
                               0 = 96 (grows on demand) */
     int icpwp;             /* 0 none, 3 basal pore-water pressure with one point (Get_Pwp_SW, nUaux = 1) */
     float pwp0rel;         /* icpwp = 3: initial Uaux = pwp0rel * rho * const(14) (Input_SW SPH_SW_2019.f90:1829-1852) */
-    int reserved[6];
+    int ws_interact;       /* ic_ws_Interact: 0 one material; 1 soil and water particles (ic_soil = ic_water = 1,
+                              Input_SW SPH_SW_2019.f90:947-951): species from gfsph_set_species */
+    int sw_alg;            /* ic_SWalg with ws_interact 1: 0 both as landslides; 1 water over the soil surface
+                              (pressure g/2 (h^2 - Zp^2), Zp = Z + hs, SPH_SW_2019.f90:6809-6828) */
+    int reserved[4];
 } gfsph_params;
 
 /*
@@ -126,8 +130,16 @@ int gfsph_destroy(gfsph_handle* h);
 
 /* Replaces the particle arrays filled by Setup_Global_Arrays_SW
  * (SPH_SW_2019.f90:6223-6246).  x, v: (2,n); rho, mass, hsml: (n); itype (n)
- * must be 1 (soil) for every particle; out_flag (n) is If_Out_Domain (may be
- * NULL = all inside). */
+ * is 1 (soil) for every particle, or 1 or 2 (water) with ws_interact = 1
+ * (NULL = all soil); out_flag (n) is If_Out_Domain (may be NULL = all
+ * inside).  With soil and water (ic_ws_Interact = 1, SPH_SW_2019.f90:947-951)
+ * the density, internal force and av_vel take pairs of one material only
+ * (Pint_Update_SW_tools My_SPH_Tools_2019.f90:1652-1710); the soil-water pairs
+ * push the soil (ExtForces_SW :8502-8521); the water is a Manning fluid whose
+ * bed, with sw_alg 1, is the soil surface Z + hs (Get_hs_at_w_SW
+ * :17789-17938, IntForces_SW :6809-6828, Get_Grav_Ext_SW :9322-9331).  That
+ * option runs the staged RK45 (the soil surface of every stage); it excludes
+ * erosion, pore pressure, nor_density and ic_cosTheta = 1, and the adjoint. */
 int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const float* rho,
                  const float* mass, const float* hsml, const int* itype, const int* out_flag);
 

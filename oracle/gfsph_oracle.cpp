@@ -292,6 +292,26 @@ struct Oracle {
     R dt;
     double time;
     std::vector<A> auxv1, auxv2; /* erosion scatter, ExtForces_SW(1) */
+    /* soil and water particles (ic_ws_Interact = 1): itype 1 soil, 2 water;
+     * the pair types of Pint_Update_SW_tools (0 same material, 1 soil-water);
+     * Z + hs at the DEM nodes and, at the water particles, its value and
+     * gradient (Get_hs_at_w_SW) */
+    int ws = 0, swalg = 0;
+    std::vector<int> itype;
+    std::vector<char> ptype;
+    std::vector<R> hsz, zpw, gzw;
+
+    /* the flag array of the interface: bit 0 out of the domain, bit 1 water */
+    void set_flags(const int* f) {
+        flag.resize(n);
+        itype.resize(n);
+        for (int i = 0; i < n; i++) {
+            flag[i] = f[i] & 1;
+            itype[i] = (f[i] & 2) ? 2 : 1;
+        }
+    }
+    int out_flag(int i) const { return flag[i] | (itype[i] == 2 ? 2 : 0); }
+    bool cross(size_t k) const { return ws && ptype[k]; }
 
     R& T(int k, int ip) { return topol[(size_t)ip * GFSPH_NTOPO + (k - 1)]; }
     R coorgx(int ix) { return xming + (R)ix * dxg; } /* 0-based ix */
@@ -477,8 +497,9 @@ struct Oracle {
         }
 #endif
         for (long ic = 0; ic < ndivt; ic++) cell_pairs(ic, pairs, pw, pd0, pd1);
-        /* Pint_Update_SW_tools (My_SPH_Tools_2019.f90:1652-1758): all particles
-         * are soil (itype 1), every pair is type 0 and keeps its order. */
+        /* Pint_Update_SW_tools (My_SPH_Tools_2019.f90:1652-1758) follows in
+         * pint_update: with one material every pair is type 0 and keeps its
+         * order. */
     }
 
     /* Accumulator view handed to a pair body: a(c, i) is the c-th sum of
@@ -527,6 +548,72 @@ struct Oracle {
         for (size_t k = 0; k < pairs.size(); k++) f(k, all);
     }
 
+    /* Pint_Update_SW_tools, My_SPH_Tools_2019.f90:1652-1710, soil (1) and
+     * water (2): a pair of one material is type 0, a soil-water pair type 1,
+     * ordered soil first (the gradient changes sign with the order). */
+    void pint_update() {
+        if (!ws) return;
+        ptype.assign(pairs.size(), 0);
+        for (size_t k = 0; k < pairs.size(); k++) {
+            int i = pairs[k].i, j = pairs[k].j;
+            if (itype[j] < itype[i]) {
+                pairs[k].i = j;
+                pairs[k].j = i;
+                pd0[k] = -pd0[k];
+                pd1[k] = -pd1[k];
+            }
+            ptype[k] = (itype[i] != itype[j]) ? 1 : 0;
+        }
+    }
+
+    /* Get_hs_at_w_SW, SPH_SW_2019.f90:17789-17938: the soil depth spread
+     * over the DEM nodes (inverse distance over the 4 x 4 nodes around each
+     * soil particle; the sums in A), Z + hs per node, and at each water
+     * particle its bilinear value and gradient on the particle's DEM cell.
+     * A water particle on the far edge of the DEM takes the last cell. */
+    void hs_at_w() {
+        std::vector<A> a1((size_t)npoig, (A)0), a2((size_t)npoig, (A)0);
+        for (int i = 0; i < n; i++) {
+            if (flag[i] || itype[i] != 1) continue;
+            R xx = x[2 * i], yy = x[2 * i + 1];
+            int ipx = (int)((xx - xming) / dxg + (R)1), ipy = (int)((yy - yming) / dyg + (R)1);
+            int inx0 = std::max(1, ipx - 1), iny0 = std::max(1, ipy - 1);
+            int inx1 = std::min(nx, ipx + 2), iny1 = std::min(ny, ipy + 2);
+            for (int inx = inx0; inx <= inx1; inx++)
+                for (int iny = iny0; iny <= iny1; iny++) {
+                    size_t ip = (size_t)(iny - 1) * nx + (inx - 1);
+                    R dx2 = xx - coorgx(inx - 1);
+                    dx2 = dx2 * dx2;
+                    R dy2 = yy - coorgy(iny - 1);
+                    dy2 = dy2 * dy2;
+                    R dist = rmax<R>(lit<R>(1.e-6), std::sqrt(dx2 + dy2));
+                    a1[ip] = a1[ip] + (A)(rho[i] / dist);
+                    a2[ip] = a2[ip] + (A)((R)1 / dist);
+                }
+        }
+        hsz.resize(npoig);
+        for (int ip = 0; ip < npoig; ip++)
+            hsz[ip] = (a2[ip] > (A)lit<R>(1.e-6)) ? T(1, ip) + (R)(a1[ip] / a2[ip]) : T(1, ip);
+        zpw.assign(n, (R)0);
+        gzw.assign(2 * (size_t)n, (R)0);
+        for (int i = 0; i < n; i++) {
+            if (flag[i] || itype[i] != 2) continue;
+            R xx = x[2 * i], yy = x[2 * i + 1];
+            int ipx = (int)((xx - xming) / dxg + (R)1), ipy = (int)((yy - yming) / dyg + (R)1);
+            ipx = std::min(std::max(ipx, 1), nx - 1);
+            ipy = std::min(std::max(ipy, 1), ny - 1);
+            size_t n1 = (size_t)(ipy - 1) * nx + (ipx - 1), n2 = n1 + 1, n3 = n1 + 1 + nx, n4 = n3 - 1;
+            R xref = xming + (R)(ipx - 1) * dxg, yref = yming + (R)(ipy - 1) * dyg;
+            R xi = (xx - xref) / dxg, eta = (yy - yref) / dyg;
+            R sh1 = ((R)1 - xi) * ((R)1 - eta), sh2 = xi * ((R)1 - eta), sh3 = xi * eta, sh4 = ((R)1 - xi) * eta;
+            R d1x = ((R)-1 + eta) / dxg, d2x = ((R)1 - eta) / dxg, d3x = eta / dxg, d4x = (-eta) / dxg;
+            R d1y = ((R)-1 + xi) / dyg, d2y = (-xi) / dyg, d3y = xi / dyg, d4y = ((R)1 - xi) / dyg;
+            zpw[i] = ((sh1 * hsz[n1] + sh2 * hsz[n2]) + sh3 * hsz[n3]) + sh4 * hsz[n4];
+            gzw[2 * i] = ((hsz[n1] * d1x + hsz[n2] * d2x) + hsz[n3] * d3x) + hsz[n4] * d4x;
+            gzw[2 * i + 1] = ((hsz[n1] * d1y + hsz[n2] * d2y) + hsz[n3] * d3y) + hsz[n4] * d4y;
+        }
+    }
+
     /* sum_density_Tools, My_SPH_Tools_2019.f90:1763-1859.  With nor_density
      * (:1841-1846) the sum is divided by wi = W(0,h_i) m_i/rho_i +
      * sum_j (m_j/rho_j) W_ij (:1793-1810), taken with the depths of the
@@ -552,6 +639,7 @@ struct Oracle {
         {
             A* arr[1] = {acc.data()};
             pair_loop(1, arr, [&](size_t k, auto& a) {
+                if (cross(k)) return; /* type 0 only, :1829 */
                 int i = pairs[k].i, j = pairs[k].j;
                 a(0, i) = a(0, i) + (A)(mass[j] * pw[k]);
                 a(0, j) = a(0, j) + (A)(mass[i] * pw[k]);
@@ -573,6 +661,7 @@ struct Oracle {
      * of each particle takes g/deng at its current position. */
     void int_forces() {
         R cgra05 = cst[1] * lit<R>(0.5); /* gravz*0.5, gravz = const(1) */
+        if (ws) hs_at_w(); /* :6763-6764, before the clamp */
         for (int i = 0; i < n; i++)
             if (rho[i] < (R)P->h_inf) rho[i] = (R)P->h_inf; /* :6769 */
         for (int i = 0; i < n; i++) {
@@ -583,11 +672,17 @@ struct Oracle {
                 R gravz = cst[1] / terrain_deng(zpx, zpy);
                 cgra05 = lit<R>(0.5) * gravz;
             }
-            p[i] = (cgra05 * rho[i]) * rho[i]; /* :6797 */
+            if (ws && swalg == 1 && itype[i] == 2) { /* water over the soil surface, :6819-6826 */
+                R zp = zpw[i];
+                p[i] = cgra05 * (rho[i] * rho[i] - zp * zp);
+            } else {
+                p[i] = (cgra05 * rho[i]) * rho[i]; /* :6797 */
+            }
         }
         std::vector<A> a0(n, (A)0), a1(n, (A)0);
         A* arr[2] = {a0.data(), a1.data()};
         pair_loop(2, arr, [&](size_t k, auto& a) {
+            if (cross(k)) return; /* type 0 only, :6899 */
             int i = pairs[k].i, j = pairs[k].j;
             R mi = mass[i], mj = mass[j];
             R g[2] = {pd0[k], pd1[k]};
@@ -661,7 +756,7 @@ struct Oracle {
     /* Get_Grav_Ext_SW (SPH_SW_2019.f90:9241-9349, ic_cosTheta = 0) followed by
      * basal_friction_Ext_SW (:9355-9901) up to, not including, its reversal
      * filter.  Returns via L the friction and the (possibly recomputed) vmod. */
-    void grav_and_friction(int i, Local& L, R top[6]) {
+    void grav_and_friction(int i, Local& L, R top[6], int nfric) {
         R cgra = cst[1];
         bool frictional = (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27;
         bool v2byr = (nfric == 7 || nfric == 8 || nfric == 26 || nfric == 27);
@@ -680,7 +775,14 @@ struct Oracle {
         R hfrict = rmax<R>(L.h, cst[10]);
         L.frictx = 0; L.fricty = 0; L.totfrict = 0; L.cf5 = 0;
         R dens = cst[2];
-        if (nfric == 4) { /* Bingham, :9538-9572 (regime value kept, see header) */
+        if (nfric == 1) { /* Manning, :9426-9430 (the water of ic_ws_Interact 1) */
+            R cmanning = cst[3];
+            R cf1 = (cgra * cmanning) * cmanning;
+            R p73 = (R)std::pow((double)hfrict, (double)lit<R>(7.0 / 3.0));
+            L.frictx = ((cf1 * L.hu) * L.hvmod) / p73;
+            L.fricty = ((cf1 * L.hv) * L.hvmod) / p73;
+            L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+        } else if (nfric == 4) { /* Bingham, :9538-9572 (regime value kept, see header) */
             R tauy0 = cst[6], constK = cst[7];
             R a_hat = (((R)6 * constK) * L.hvmod) / (tauy0 * (hfrict * hfrict));
             if (a_hat > (R)50) {
@@ -761,7 +863,7 @@ struct Oracle {
     }
 
     /* the reversal filter of basal_friction_Ext_SW, SPH_SW_2019.f90:9829-9895 */
-    void reversal_filter(int i, Local& L, R acc0, R acc1) {
+    void reversal_filter(int i, Local& L, R acc0, R acc1, int nfric) {
         bool frictional = (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27;
         R dc0 = -(L.frictx * L.hinv), dc1 = -(L.fricty * L.hinv);
         if (L.vmod > lit<R>(1.e-5)) {
@@ -804,16 +906,41 @@ struct Oracle {
     /* ExtForces_SW(0): SPH_SW_2019.f90:8483 and the particle loop :8532-8716 */
     void ext_forces0() {
         std::fill(ex.begin(), ex.end(), (R)0);
+        if (ws) { /* soil-water pairs, :8502-8521 (dens_ws = densw/dens, :8999-9002) */
+            R densw = (cst[18] < lit<R>(1.e-3)) ? (R)1000 : cst[18];
+            R dens_ws = densw / cst[2];
+            R cgra = cst[1];
+            std::vector<A> b0(n, (A)0), b1(n, (A)0);
+            for (size_t k = 0; k < pairs.size(); k++) {
+                if (!ptype[k]) continue;
+                int i = pairs[k].i, j = pairs[k].j; /* i soil, j water */
+                R g[2] = {pd0[k], pd1[k]};
+                A* b[2] = {b0.data(), b1.data()};
+                for (int d = 0; d < 2; d++) {
+                    b[d][i] = b[d][i] - (A)(((dens_ws * cgra) * mass[j]) * g[d]);
+                    if (swalg == 0) b[d][j] = b[d][j] + (A)((cgra * mass[i]) * g[d]);
+                }
+            }
+            for (int i = 0; i < n; i++) { ex[2 * i] = (R)b0[i]; ex[2 * i + 1] = (R)b1[i]; }
+        }
 #pragma omp parallel for schedule(static)
         for (int i = 0; i < n; i++) {
             if (flag[i]) continue;
             R top[6];
             Local L;
             ext_locals(i, rho[i], L);
-            grav_and_friction(i, L, top);
-            ex[2 * i] = ex[2 * i] + L.gravx;
-            ex[2 * i + 1] = ex[2 * i + 1] + L.gravy;
-            reversal_filter(i, L, ex[2 * i] + in[2 * i], ex[2 * i + 1] + in[2 * i + 1]);
+            const bool water = ws && itype[i] == 2;
+            const int nf = water ? 1 : nfric; /* :8600-8606: the water is a Manning fluid */
+            grav_and_friction(i, L, top, nf);
+            if (water && swalg == 1) { /* Get_Grav_Ext_SW :9322-9331 */
+                R hhsz = rho[i] + zpw[i];
+                ex[2 * i] = ex[2 * i] - (L.gravz * (hhsz * gzw[2 * i])) / rho[i];
+                ex[2 * i + 1] = ex[2 * i + 1] - (L.gravz * (hhsz * gzw[2 * i + 1])) / rho[i];
+            } else {
+                ex[2 * i] = ex[2 * i] + L.gravx;
+                ex[2 * i + 1] = ex[2 * i + 1] + L.gravy;
+            }
+            reversal_filter(i, L, ex[2 * i] + in[2 * i], ex[2 * i + 1] + in[2 * i + 1], nf);
             ex[2 * i] = ex[2 * i] - L.frictx / L.h;
             ex[2 * i + 1] = ex[2 * i + 1] - L.fricty / L.h;
             if (ic_erosion) { /* Hungr, Get_Erosion_Rate_SW :10329-10331; momentum :8664-8697 */
@@ -836,7 +963,7 @@ struct Oracle {
             R top[6];
             Local L;
             ext_locals(i, rho[i], L);
-            grav_and_friction(i, L, top);
+            grav_and_friction(i, L, top, nfric);
             R er = (cst[22] * L.h) * L.vmod;
             R base = dt * er;
             R xx = x[2 * i], yy = x[2 * i + 1];
@@ -937,6 +1064,7 @@ struct Oracle {
         std::vector<A> a0(n, (A)0), a1(n, (A)0);
         A* arr[2] = {a0.data(), a1.data()};
         pair_loop(2, arr, [&](size_t k, auto& a) {
+            if (cross(k)) return; /* type 0 only, SPH_MAIN_2019.f90:3071 */
             int i = pairs[k].i, j = pairs[k].j;
             for (int d = 0; d < 2; d++) {
                 R dvx = v[2 * i + d] - v[2 * j + d];
@@ -964,6 +1092,7 @@ struct Oracle {
         std::fill(Dx.begin(), Dx.end(), (R)0);
         std::fill(Dv.begin(), Dv.end(), (R)0);
         grid_find();
+        pint_update();
         x0 = x; v0 = v;
         if (pos64) x0d = xd;
         rho0 = rho;
@@ -1048,6 +1177,11 @@ struct Oracle {
         if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
         if (ic_erosion && (int)(cst[21] + lit<R>(0.1)) != 1) return GFSPH_ERR_UNSUPPORTED;
         if (P->skf < 1 || P->skf > 4) return GFSPH_ERR_UNSUPPORTED;
+        ws = P->ws_interact;
+        swalg = P->sw_alg;
+        if (ws < 0 || ws > 1 || swalg < 0 || swalg > 1) return GFSPH_ERR_UNSUPPORTED;
+        if (ws && (ic_erosion || P->icpwp != 0 || P->nor_density != 0 || ic_costheta != 0))
+            return GFSPH_ERR_UNSUPPORTED;
         nx = nx_; ny = ny_; npoig = nx * ny;
         xming = (R)(float)xmin; yming = (R)(float)ymin; dxg = (R)(float)dx; dyg = (R)(float)dy;
         xmaxg = xming + (R)(nx - 1) * dxg;
@@ -1140,7 +1274,7 @@ struct OracleObj : OracleBase {
             if (rho) rho[k] = (double)o.rho[k];
             if (mass) mass[k] = (double)o.mass[k];
             if (hsml) hsml[k] = (double)o.hsml[k];
-            if (flag) flag[k] = o.flag[k];
+            if (flag) flag[k] = o.out_flag(k);
         }
         if (topol)
             for (size_t k = 0; k < o.topol.size(); k++) topol[k] = (double)o.topol[k];
@@ -1171,7 +1305,7 @@ OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double 
     };
     cp(o.x, x, 2 * (size_t)n); cp(o.v, v, 2 * (size_t)n);
     cp(o.rho, rho, n); cp(o.mass, mass, n); cp(o.hsml, hsml, n);
-    o.flag.assign(flag, flag + n);
+    o.set_flags(flag);
     o.p.assign(n, (R)0);
     o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
     o.dt = (R)dt;
@@ -1195,7 +1329,7 @@ int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, do
     };
     cp(o.x, x, 2 * (size_t)n); cp(o.v, v, 2 * (size_t)n);
     cp(o.rho, rho, n); cp(o.mass, mass, n); cp(o.hsml, hsml, n);
-    o.flag.assign(flag, flag + n);
+    o.set_flags(flag);
     o.p.assign(n, (R)0);
     o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
     o.dt = (R)*dt;
@@ -1210,7 +1344,7 @@ int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, do
     }
     for (size_t k = 0; k < 2 * (size_t)n; k++) { x[k] = (double)o.x[k]; v[k] = (double)o.v[k]; }
     for (int k = 0; k < n; k++) {
-        rho[k] = (double)o.rho[k]; mass[k] = (double)o.mass[k]; hsml[k] = (double)o.hsml[k]; flag[k] = o.flag[k];
+        rho[k] = (double)o.rho[k]; mass[k] = (double)o.mass[k]; hsml[k] = (double)o.hsml[k]; flag[k] = o.out_flag(k);
     }
     for (size_t k = 0; k < o.topol.size(); k++) topol[k] = (double)o.topol[k];
     if (pwp)
@@ -1228,6 +1362,8 @@ int pairs_mode(const gfsph_params* p, int n, const double* x, const double* hsml
     Oracle<R, A> o;
     o.P = p;
     o.n = n;
+    o.ws = p->ws_interact; /* the pair types; the forces of ic_ws_Interact 1 need the DEM */
+    if (o.ws && indvxdt) return GFSPH_ERR_UNSUPPORTED;
     o.x.resize(2 * (size_t)n); o.hsml.resize(n); o.mass.resize(n); o.rho.resize(n);
     for (size_t k = 0; k < 2 * (size_t)n; k++) o.x[k] = (R)x[k];
     for (int k = 0; k < n; k++) {
@@ -1235,9 +1371,10 @@ int pairs_mode(const gfsph_params* p, int n, const double* x, const double* hsml
         o.mass[k] = mass ? (R)mass[k] : (R)0;
         o.rho[k] = rho_in ? (R)rho_in[k] : (R)0;
     }
-    o.flag.assign(flag, flag + n);
+    o.set_flags(flag);
     for (int k = 1; k <= GFSPH_NCONST; k++) o.cst[k] = (R)p->cst[k - 1];
     o.grid_find();
+    o.pint_update();
     if (offsets) {
         std::vector<std::vector<int>> nb(n);
         for (auto& pr : o.pairs) { nb[pr.i].push_back(pr.j); nb[pr.j].push_back(pr.i); }
@@ -1686,7 +1823,7 @@ int tangent_run(const gfsph_params* p, int nx, int ny, double xmin, double ymin,
         o.mass[k] = R(mass[k], seed_m ? seed_m[k] : 0.0);
         o.hsml[k] = R(hsml[k]);
     }
-    o.flag.assign(flag, flag + n);
+    o.set_flags(flag);
     o.p.assign(n, R(0.0));
     o.ex.assign(2 * (size_t)n, R(0.0)); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
     o.dt = R(dt);

@@ -1,0 +1,122 @@
+"""Soil and water particles (ic_ws_Interact = 1) on the device against the
+oracle (FP32 state, FP64 sums): a Bingham soil cap on a gentle slope with a
+water pond over its downslope edge, for both ic_SWalg forms, and the options
+refused with them."""
+import numpy as np
+import pytest
+
+import gfsph
+import workloads
+
+pytestmark = pytest.mark.gpu
+
+CONST = {1: 9.8, 2: 2000.0, 3: 0.03, 5: 4, 6: 1000.0, 7: 50.0, 10: 0.01, 15: 0.01, 18: 1000.0}
+
+
+def soil_and_pond():
+    """A gentle 2% slope (120 x 120 DEM at 2 m, Z = 0.02 (238 - y)); a
+    Bingham soil cap (radius 30 m, 6 m high) centred at (120, 80) m on a 1.5 m
+    lattice, and a 1.5 m-deep water pond over x 90..150, y 100..140 m on the
+    same lattice, its first 10 m over the cap's edge."""
+    cell = 2.0
+    n = 120
+    yy = np.arange(n, dtype=np.float64)[:, None] * cell * np.ones((1, n))
+    z = (0.02 * ((n - 1) * cell - yy)).astype(np.float32)
+    sp = 1.5
+    g = np.arange(0.0, 240.0, sp)
+    X, Y = np.meshgrid(g, g)
+    r2 = (X - 120.0) ** 2 + (Y - 80.0) ** 2
+    mask = r2 < 30.0 ** 2
+    depth = 6.0 * (1.0 - r2 / 30.0 ** 2)
+    xs, vs, hs_, ms, hsm = workloads.lattice_particles(mask, depth, 0.0, 0.0, sp, 2.0, 0.01)
+    pond = (X >= 90.0) & (X <= 150.0) & (Y >= 100.0) & (Y <= 140.0)
+    xw, vw, hw, mw, hsw = workloads.lattice_particles(pond, np.full(X.shape, 1.5), 0.0, 0.0, sp, 2.0, 0.01)
+    x = np.concatenate([xs, xw]).astype(np.float32)
+    v = np.zeros_like(x)
+    rho = np.concatenate([hs_, hw]).astype(np.float32)
+    mass = np.concatenate([ms, mw]).astype(np.float32)
+    hsml = np.concatenate([hsm, hsw]).astype(np.float32)
+    itype = np.r_[np.ones(len(xs), np.int32), np.full(len(xw), 2, np.int32)]
+    w = workloads.Workload(name="soil_and_pond", const=CONST, options={}, z=z, dx=cell, dy=cell, x=xs, v=vs,
+                           rho=hs_, mass=ms, hsml=hsm, steps=30, meta={})
+    return w, x, v, rho, mass, hsml, itype
+
+
+def run_pair(oracle_mod, sw_alg, steps):
+    w, x, v, rho, mass, hsml, itype = soil_and_pond()
+    p = gfsph.make_params(CONST, sle=1, ic_adapt=0, dt=0.01, ws_interact=1, sw_alg=sw_alg)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.upload(x, v, rho, mass, hsml, itype=itype)
+    sim.step(steps)
+    got = sim.download()
+    sim.close()
+    ny, nx = w.z.shape
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, CONST, deriv=p.dem_deriv)
+    flag = np.where(itype == 2, 2, 0).astype(np.int32)
+    st = oracle_mod.State(x, v, rho, mass, hsml, topol, flag=flag, dt=p.dt)
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, steps)
+    return got, st, itype
+
+
+@pytest.mark.parametrize("sw_alg", [0, 1])
+def test_soil_and_water_one_step_matches_oracle(gfsph_lib, oracle_mod, sw_alg):
+    got, st, itype = run_pair(oracle_mod, sw_alg, 1)
+    assert np.array_equal(got["flag"], st.flag & 1)
+    for k, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("hsml", st.hsml)):
+        ref = ref.astype(np.float32)
+        scale = np.abs(ref).max()
+        assert np.abs(got[k] - ref).max() <= 1e-6 * max(scale, 1.0), (k, np.abs(got[k] - ref).max())
+    assert np.abs(got["v"][itype == 2]).max() > 1e-3  # the water moves
+
+
+@pytest.mark.parametrize("sw_alg", [0, 1])
+def test_soil_and_water_thirty_steps_match_oracle(gfsph_lib, oracle_mod, sw_alg):
+    """30 steps: relative L2 of positions 1e-6, of velocities and depths 1e-5
+    (the soil surface is an FP64 atomic sum per DEM node, whose last bits can
+    differ from the oracle's sequential sum)."""
+    got, st, itype = run_pair(oracle_mod, sw_alg, 30)
+    for k, ref, tol in (("x", st.x, 1e-6), ("v", st.v, 1e-5), ("rho", st.rho, 1e-5)):
+        ref = ref.astype(np.float64)
+        err = np.linalg.norm(got[k].astype(np.float64) - ref) / np.linalg.norm(ref)
+        assert err <= tol, (k, err)
+
+
+def test_water_changes_the_soil_flow(gfsph_lib):
+    """The pond pushes the soil: the cap's velocities differ from the same cap
+    run without the water."""
+    w, x, v, rho, mass, hsml, itype = soil_and_pond()
+    out = {}
+    for with_water in (True, False):
+        keep = slice(None) if with_water else slice(0, w.n)
+        p = gfsph.make_params(CONST, sle=1, ic_adapt=0, dt=0.01, ws_interact=1, sw_alg=1)
+        sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+        sim.upload(x[keep], v[keep], rho[keep], mass[keep], hsml[keep], itype=itype[keep])
+        sim.step(20)
+        out[with_water] = sim.download()["v"][:w.n]
+        sim.close()
+    assert np.abs(out[True] - out[False]).max() > 1e-3
+
+
+def test_soil_and_water_refusals(gfsph_lib):
+    w, x, v, rho, mass, hsml, itype = soil_and_pond()
+    # water particles without ic_ws_Interact = 1
+    p = gfsph.make_params(CONST, sle=1, ic_adapt=0, dt=0.01)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    with pytest.raises(gfsph.GfsphError) as e:
+        sim.upload(x, v, rho, mass, hsml, itype=itype)
+    assert e.value.status == gfsph.ERR_UNSUPPORTED
+    sim.close()
+    # options outside the scope of the two materials
+    for const, kw in (({21: 1, 22: 0.005}, {}), ({}, {"icpwp": 3}), ({}, {"nor_density": 1}), ({16: 1.0}, {})):
+        p = gfsph.make_params({**CONST, **const}, sle=1, ic_adapt=0, dt=0.01, ws_interact=1, **kw)
+        with pytest.raises(gfsph.GfsphError) as e:
+            gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+        assert e.value.status == gfsph.ERR_UNSUPPORTED
+    # the adjoint
+    p = gfsph.make_params({**CONST, 5: 5, 9: 0.2}, sle=0, ic_adapt=0, dt=0.01, ws_interact=1)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    sim.upload(x, v, rho, mass, hsml, itype=itype)
+    with pytest.raises(gfsph.GfsphError) as e:
+        gfsph.Adjoint(sim, 5)
+    assert e.value.status == gfsph.ERR_UNSUPPORTED
+    sim.close()

@@ -624,3 +624,63 @@ def test_a_particle_leaving_the_dem_is_flagged_and_frozen(oracle_mod):
     with pytest.raises(RuntimeError, match="-8"):
         oracle_mod.run(2, p, nx, ny, d, d, st, 5)
     assert st.flag[0] == 1 and np.array_equal(st.x[0], x_out)
+
+
+def test_soil_and_water_densities_count_their_own_material(oracle_mod):
+    """ic_ws_Interact = 1: the pairs of a soil and a water particle are type 1
+    (Pint_Update_SW_tools, My_SPH_Tools_2019.f90:1652-1710) and the
+    summation density takes type 0 only (:1829): interleaved soil and water
+    lattices give each material the density it has alone."""
+    s = 1.0
+    g = np.arange(0.0, 30.0, s)
+    X, Y = np.meshgrid(g, g)
+    soil = np.stack([X.ravel(), Y.ravel()], 1) + 50.0
+    water = soil + 0.5 * s
+    x = np.concatenate([soil, water])
+    n = x.shape[0]
+    hs = np.full(n, 2.0 * s)
+    mass = np.full(n, 4.0)
+    flag = np.r_[np.zeros(len(soil), np.int32), np.full(len(water), 2, np.int32)]
+    p = params(ws_interact=1)
+    both = oracle_mod.pairs(oracle_mod.MODE_FP32_DACC, p, x, hs, mass, flag=flag, want_sets=False, want_rho=True)
+    alone = oracle_mod.pairs(oracle_mod.MODE_FP32_DACC, params(), soil, hs[:len(soil)], mass[:len(soil)],
+                             want_sets=False, want_rho=True)
+    assert np.allclose(both["rho"][:len(soil)], alone["rho"], rtol=1e-6)
+    assert np.allclose(both["rho"][len(soil):], alone["rho"], rtol=1e-6)
+    mixed = oracle_mod.pairs(oracle_mod.MODE_FP32_DACC, params(), x, hs, mass, flag=flag, want_sets=False,
+                             want_rho=True)
+    assert mixed["rho"][len(soil) // 2] > 1.5 * alone["rho"][len(soil) // 2]  # one material: every pair counts
+
+
+def test_still_water_over_a_soil_layer_stays_still(oracle_mod):
+    """ic_ws_Interact = 1, ic_SWalg = 1: a water layer over a flat soil layer
+    on a flat bed.  The water pressure g/2 (h^2 - Zp^2) with Zp = Z + hs (the
+    soil surface, Get_hs_at_w_SW SPH_SW_2019.f90:17789-17938) and the
+    gravity term -g (h + Zp) grad Zp / h leave the interior at rest; the
+    soil-water pairs push the soil by -(densw/dens) g m_j grad W (:8502-8521),
+    which cancels in the interior of the interleaved lattices."""
+    nxy = 60
+    z = np.zeros((nxy, nxy))
+    s = 1.0
+    g = np.arange(10.0, 50.0, s)
+    X, Y = np.meshgrid(g, g)
+    soil = np.stack([X.ravel(), Y.ravel()], 1)
+    water = soil + 0.5 * s
+    x = np.concatenate([soil, water])
+    n = x.shape[0]
+    depth = np.r_[np.full(len(soil), 1.0), np.full(len(water), 2.0)]
+    hs = np.full(n, 2.0 * s)
+    w0 = oracle_mod.kernel(1, np.zeros(1), np.zeros(1), np.zeros(1), np.full(1, 2.0 * s), mode=oracle_mod.MODE_FP64)[0]
+    mass = depth * s * s  # a uniform layer of depth h on a unit lattice
+    flag = np.r_[np.zeros(len(soil), np.int32), np.full(len(water), 2, np.int32)]
+    p = params({1: 9.8, 2: 2000.0, 3: 0.03, 5: 4, 6: 5000.0, 7: 1000.0, 10: 0.01, 15: 0.01, 18: 1000.0},
+               ws_interact=1, sw_alg=1, sle=0, ic_adapt=0, dt=0.005)
+    topol = oracle_mod.initial_topol(z, 5.0, 5.0, {1: 9.8}, deriv=1)
+    st = oracle_mod.State(x, np.zeros((n, 2)), depth, mass, hs, topol, flag=flag, dt=0.005)
+    oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nxy, nxy, 5.0, 5.0, st, 20)
+    interior = (np.abs(x - 30.0).max(1) < 8.0)
+    v = np.hypot(st.v[:, 0], st.v[:, 1])
+    assert np.isfinite(st.v).all()
+    assert v[interior].max() < 1e-3, v[interior].max()
+    assert (st.flag & 2 == 2).sum() == len(water)  # the species come back in bit 1 of the flags
+    del w0
