@@ -16,6 +16,15 @@
  * Fortran left-to-right evaluation order, without FMA contraction
  * (build with -ffp-contract=off).
  *
+ * Soil and water particles (ic_ws_Interact = 1, ic_SWalg 0 or 1): the
+ * material of each particle travels in bit 1 of the flag array of this
+ * interface (value 2: water, itype 2), bit 0 being If_Out_Domain.  The pair
+ * types of Pint_Update_SW_tools, the soil surface of Get_hs_at_w_SW at every
+ * stage, the water's pressure, Manning friction and gravity, and the
+ * soil-water pair terms of ExtForces_SW are restated; the sums of the soil
+ * surface are A-typed like the pair sums.  A water particle on the far edge
+ * of the DEM takes the last DEM cell (the reference reads past the row).
+ *
  * Precision modes (template <R, A>: R = state and arithmetic, A = accumulators
  * of the pair sums and of the erosion scatter):
  *   mode 0  R=float,  A=float  : the reference as shipped (irk = k_real,
