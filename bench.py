@@ -358,6 +358,55 @@ def cg_bench(args, gfsph, workloads, peak):
     return out
 
 
+def wir_bench(args, gfsph, workloads, torch, nsteps=50):
+    """Soil and water particles (ic_ws_Interact = 1, ic_SWalg = 1): the soil
+    cap and water pond of workloads.soil_and_pond scaled to ~190k particles
+    (0.33 m lattice, 240 x 240 DEM at 2 m).  The staged RK45 with the soil
+    surface under the water rebuilt at every stage.  Device time from CUDA
+    events on the handle's stream around `nsteps` steps after 10 warm-up
+    steps; the oracle port times a bounded sample of the same state."""
+    w, a = workloads.soil_and_pond(spacing=0.33, scale=2.0)
+    n = a["x"].shape[0]
+    p = workloads.make_params(w, gfsph)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(a["x"], a["v"], a["rho"], a["mass"], a["hsml"], itype=a["itype"])
+    sim.step(10)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(nsteps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / nsteps
+    st = sim.download()
+    launches = sim.kernels_per_step() if hasattr(sim, "kernels_per_step") else None
+    sim.close()
+    out = {"workload": f"soil and water: {n} particles ({int((a['itype'] == 2).sum())} water), "
+                       f"{w.meta['dem']}, Bingham soil, Manning water over the soil surface (ic_SWalg 1)",
+           "steps": nsteps, "device_ms_per_step": ms, "particle_steps_per_s": n / (ms / 1e3),
+           "finite": bool(np.isfinite(st["x"]).all()),
+           "note": "device time (CUDA events on the handle's stream); per step 3 extra launches per RK stage "
+                   "rebuild the soil surface"}
+    if launches is not None:
+        out["launches_per_step"] = launches
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        topol = oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv)
+        flag = np.where(a["itype"] == 2, 2, 0).astype(np.int32)
+        so = oracle.State(st["x"], st["v"], st["rho"], st["mass"], st["hsml"], topol, flag=flag | st["flag"],
+                          dt=p.dt)
+        ny, nx = w.z.shape
+        k = 2
+        t0 = time.perf_counter()
+        oracle.run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, so, k)
+        t_cpu = time.perf_counter() - t0
+        out["cpu_port"] = {"particle_steps_per_s": n * k / t_cpu, "cores": 1, "kind": "port",
+                           "sample": f"{k} steps of the same state after the GPU run, FP32 oracle port"}
+    return out
+
+
 def gfl_bench(args, gfsph, workloads, peak, nsteps=100):
     """The GFL Taylor-Galerkin step on the coupled case's mesh: the 500 x
     500-node window of the DEM background triangulation at 2 m (498,002
@@ -680,6 +729,7 @@ def main():
     sim.close()
     cg_line = cg_bench(args, gfsph, workloads, peak) if extras else None
     gfl_line = gfl_bench(args, gfsph, workloads, peak) if extras else None
+    wir_line = wir_bench(args, gfsph, workloads, torch) if extras else None
     adj_line = adjoint_bench(gfsph, workloads, torch) if extras else None
     big_line = coupled_bench(gfsph, workloads, torch) if extras else None
     ens_line = None
@@ -716,6 +766,8 @@ def main():
             line["cg"] = cg_line
         if gfl_line:
             line["gfl"] = gfl_line
+        if wir_line:
+            line["wir"] = wir_line
         if adj_line:
             line["adjoint"] = adj_line
         if big_line:

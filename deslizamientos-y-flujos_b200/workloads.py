@@ -238,6 +238,40 @@ def mc_ensemble(nreal, n_base=200_000, dem_k=10, cell=5.0, seed=2024, mu=(0.08, 
     return out
 
 
+def soil_and_pond(spacing=1.5, scale=1.0):
+    """Soil and water particles (ic_ws_Interact = 1): a gentle 2% slope
+    (DEM at 2 m, Z = 0.02 (ymax - y)), a Bingham soil cap (radius 30 m, 6 m
+    high) centred at (120, 80) m, and a 1.5 m-deep water pond over x 90..150,
+    y 100..140 m, its first 10 m over the cap's edge; both on a lattice of
+    `spacing`.  `scale` stretches the scene (and the DEM) in both directions.
+    Returns the workload of the soil (its const and DEM) and the joint
+    particle arrays with the material per particle (1 soil, 2 water)."""
+    cell = 2.0
+    n = int(round(120 * scale))
+    yy = np.arange(n, dtype=np.float64)[:, None] * cell * np.ones((1, n))
+    z = (0.02 * ((n - 1) * cell - yy)).astype(np.float32)
+    g = np.arange(0.0, (n - 1) * cell, spacing)
+    X, Y = np.meshgrid(g, g)
+    cx, cy, r0 = 120.0 * scale, 80.0 * scale, 30.0 * scale
+    r2 = (X - cx) ** 2 + (Y - cy) ** 2
+    depth = 6.0 * (1.0 - r2 / r0 ** 2)
+    xs, vs, hs_, ms, hsm = lattice_particles(r2 < r0 ** 2, depth, 0.0, 0.0, spacing, 2.0, 0.01)
+    pond = (X >= 90.0 * scale) & (X <= 150.0 * scale) & (Y >= 100.0 * scale) & (Y <= 140.0 * scale)
+    xw, vw, hw, mw, hsw = lattice_particles(pond, np.full(X.shape, 1.5), 0.0, 0.0, spacing, 2.0, 0.01)
+    const = {1: 9.8, 2: 2000.0, 3: 0.03, 5: 4, 6: 1000.0, 7: 50.0, 10: 0.01, 15: 0.01, 18: 1000.0}
+    w = Workload(name="soil_and_pond", const=const,
+                 options=dict(pa_sph=2, nnps=2, sle=1, skf=1, average_velocity=1, ic_adapt=0, h_inf=0.01, dt=0.01,
+                              dem_deriv=1, ws_interact=1, sw_alg=1),
+                 z=z, dx=cell, dy=cell, x=xs, v=vs, rho=hs_, mass=ms, hsml=hsm, steps=1000,
+                 meta=dict(dem=f"{n}x{n} at {cell} m", lattice=spacing))
+    x = np.concatenate([xs, xw]).astype(np.float32)
+    arrays = dict(x=x, v=np.zeros_like(x), rho=np.concatenate([hs_, hw]).astype(np.float32),
+                  mass=np.concatenate([ms, mw]).astype(np.float32),
+                  hsml=np.concatenate([hsm, hsw]).astype(np.float32),
+                  itype=np.r_[np.ones(len(xs), np.int32), np.full(len(xw), 2, np.int32)])
+    return w, arrays
+
+
 def make_params(w, gfsph_module, **over):
     opts = dict(w.options)
     opts.update(over)

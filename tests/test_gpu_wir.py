@@ -14,32 +14,8 @@ CONST = {1: 9.8, 2: 2000.0, 3: 0.03, 5: 4, 6: 1000.0, 7: 50.0, 10: 0.01, 15: 0.0
 
 
 def soil_and_pond():
-    """A gentle 2% slope (120 x 120 DEM at 2 m, Z = 0.02 (238 - y)); a
-    Bingham soil cap (radius 30 m, 6 m high) centred at (120, 80) m on a 1.5 m
-    lattice, and a 1.5 m-deep water pond over x 90..150, y 100..140 m on the
-    same lattice, its first 10 m over the cap's edge."""
-    cell = 2.0
-    n = 120
-    yy = np.arange(n, dtype=np.float64)[:, None] * cell * np.ones((1, n))
-    z = (0.02 * ((n - 1) * cell - yy)).astype(np.float32)
-    sp = 1.5
-    g = np.arange(0.0, 240.0, sp)
-    X, Y = np.meshgrid(g, g)
-    r2 = (X - 120.0) ** 2 + (Y - 80.0) ** 2
-    mask = r2 < 30.0 ** 2
-    depth = 6.0 * (1.0 - r2 / 30.0 ** 2)
-    xs, vs, hs_, ms, hsm = workloads.lattice_particles(mask, depth, 0.0, 0.0, sp, 2.0, 0.01)
-    pond = (X >= 90.0) & (X <= 150.0) & (Y >= 100.0) & (Y <= 140.0)
-    xw, vw, hw, mw, hsw = workloads.lattice_particles(pond, np.full(X.shape, 1.5), 0.0, 0.0, sp, 2.0, 0.01)
-    x = np.concatenate([xs, xw]).astype(np.float32)
-    v = np.zeros_like(x)
-    rho = np.concatenate([hs_, hw]).astype(np.float32)
-    mass = np.concatenate([ms, mw]).astype(np.float32)
-    hsml = np.concatenate([hsm, hsw]).astype(np.float32)
-    itype = np.r_[np.ones(len(xs), np.int32), np.full(len(xw), 2, np.int32)]
-    w = workloads.Workload(name="soil_and_pond", const=CONST, options={}, z=z, dx=cell, dy=cell, x=xs, v=vs,
-                           rho=hs_, mass=ms, hsml=hsm, steps=30, meta={})
-    return w, x, v, rho, mass, hsml, itype
+    w, a = workloads.soil_and_pond()
+    return w, a["x"], a["v"], a["rho"], a["mass"], a["hsml"], a["itype"]
 
 
 def run_pair(oracle_mod, sw_alg, steps):
