@@ -358,6 +358,41 @@ def cg_bench(args, gfsph, workloads, peak):
     return out
 
 
+def plane_bench(args, gfsph, workloads, torch):
+    """The granular collapse on the 30-degree plane (~2k particles, 200 x 400
+    DEM at 5 m, Voellmy, fixed dt 0.01 s): all 2,000 steps on the device
+    (CUDA events on the handle's stream), and on the CPU the FP32 oracle port
+    over the same 2,000 steps, one thread."""
+    w = workloads.inclined_plane()
+    p = workloads.make_params(w, gfsph)
+    sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(w.x, w.v, w.rho, w.mass, w.hsml)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(w.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.close()
+    out = {"workload": f"inclined plane: {w.n} particles, {w.meta['dem']}, Voellmy, {w.steps} steps",
+           "device_s": ms / 1e3, "particle_steps_per_s": w.n * w.steps / (ms / 1e3),
+           "note": "device time of the whole run (CUDA events); at 2k particles a step is launch-bound"}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        topol = oracle.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv)
+        st = oracle.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+        ny, nx = w.z.shape
+        t0 = time.perf_counter()
+        oracle.run(oracle.MODE_FP32, p, nx, ny, w.dx, w.dy, st, w.steps)
+        t_cpu = time.perf_counter() - t0
+        out["cpu_port"] = {"s": t_cpu, "particle_steps_per_s": w.n * w.steps / t_cpu, "cores": 1, "kind": "port",
+                           "sample": f"the same {w.steps} steps, FP32 oracle port"}
+    return out
+
+
 def wir_bench(args, gfsph, workloads, torch, nsteps=50):
     """Soil and water particles (ic_ws_Interact = 1, ic_SWalg = 1): the soil
     cap and water pond of workloads.soil_and_pond scaled to ~190k particles
@@ -730,6 +765,7 @@ def main():
     cg_line = cg_bench(args, gfsph, workloads, peak) if extras else None
     gfl_line = gfl_bench(args, gfsph, workloads, peak) if extras else None
     wir_line = wir_bench(args, gfsph, workloads, torch) if extras else None
+    plane_line = plane_bench(args, gfsph, workloads, torch) if extras else None
     adj_line = adjoint_bench(gfsph, workloads, torch) if extras else None
     big_line = coupled_bench(gfsph, workloads, torch) if extras else None
     ens_line = None
@@ -768,6 +804,8 @@ def main():
             line["gfl"] = gfl_line
         if wir_line:
             line["wir"] = wir_line
+        if plane_line:
+            line["plane"] = plane_line
         if adj_line:
             line["adjoint"] = adj_line
         if big_line:

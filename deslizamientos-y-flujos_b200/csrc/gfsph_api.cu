@@ -106,6 +106,25 @@ void dfree(T*& p) {
     p = nullptr;
 }
 
+// Launch of a step kernel with programmatic stream serialisation: the
+// kernel may start (and wait in PDL_ENTRY) while the one before it in the
+// stream finishes.  The stream capture records the dependency as a
+// programmatic edge.
+template <typename... KArgs, typename... Args>
+void pdl_launch(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 int blocks_for(long long work, int threads = kThreads) {
     long long b = (work + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -327,27 +346,27 @@ int enqueue_search(gfsph_handle* h, int advance) {
     int nbscan = (h->cap_blocks + kScanTile - 1) / kScanTile;
     const int* nblk = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, nblocks));
     const int* ncel = reinterpret_cast<const int*>(reinterpret_cast<const char*>(S) + offsetof(StepScalars, ncells));
-    if (!advance) { launch(h, K_PREP, [&] { k_prep<<<1, 32, 0, st>>>(S, advance); }); nk++; }
+    if (!advance) { launch(h, K_PREP, [&] { pdl_launch(k_prep, 1, 32, st, S, advance); }); nk++; }
     const GridArgs ga{h->cap_blocks, h->cap_cells, kMaxCells, h->level_factor, h->cell_div, h->reg_levels};
     launch(h, K_BOUNDS, [&] {
-        k_bounds<<<kBoundsBlocks, kThreadsBounds, 0, st>>>(h->B, n, h->rheo, h->dem, S, h->bparts, ga);
+        pdl_launch(k_bounds, kBoundsBlocks, kThreadsBounds, st, h->B, n, h->rheo, h->dem, S, h->bparts, ga);
     }); nk++;
-    launch(h, K_MARK, [&] { k_mark<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark); }); nk++;
+    launch(h, K_MARK, [&] { pdl_launch(k_mark, pb, kThreads, st, h->B, n, h->dem, S, h->bmark); }); nk++;
     launch(h, K_BSCAN_TILES, [&] {
-        k_scan_tiles<<<nbscan, kScanThreads, 0, st>>>(h->bmark, h->bstart, h->tile_sum, nblk, S, 1);
+        pdl_launch(k_scan_tiles, nbscan, kScanThreads, st, h->bmark, h->bstart, h->tile_sum, nblk, S, 1);
     }); nk++;
-    launch(h, K_BSCAN_ADD, [&] { k_scan_add<<<nbscan, kScanThreads, 0, st>>>(h->bstart, h->tile_sum, nblk, S, 1); }); nk++;
+    launch(h, K_BSCAN_ADD, [&] { pdl_launch(k_scan_add, nbscan, kScanThreads, st, h->bstart, h->tile_sum, nblk, S, 1); }); nk++;
     launch(h, K_HIST, [&] {
-        k_hist<<<pb, kThreads, 0, st>>>(h->B, n, h->dem, S, h->bmark, h->bstart, h->count, h->keyrank, h->cap_cells);
+        pdl_launch(k_hist, pb, kThreads, st, h->B, n, h->dem, S, h->bmark, h->bstart, h->count, h->keyrank, h->cap_cells);
     }); nk++;
     launch(h, K_SCAN_TILES, [&] {
-        k_scan_tiles<<<nscan, kScanThreads, 0, st>>>(h->count, h->start, h->tile_sum, ncel, S, 0);
+        pdl_launch(k_scan_tiles, nscan, kScanThreads, st, h->count, h->start, h->tile_sum, ncel, S, 0);
     }); nk++;
-    launch(h, K_SCAN_ADD, [&] { k_scan_add<<<nscan, kScanThreads, 0, st>>>(h->start, h->tile_sum, ncel, S, 0); }); nk++;
-    launch(h, K_SCATTER, [&] { k_scatter<<<pb, kThreads, 0, st>>>(h->keyrank, n, h->start, h->bstart, S, h->perm); }); nk++;
-    launch(h, K_CELL_SORT, [&] { k_cell_sort<<<148 * 4, 128, 0, st>>>(h->perm, h->B.id, h->start, h->count, S); }); nk++;
+    launch(h, K_SCAN_ADD, [&] { pdl_launch(k_scan_add, nscan, kScanThreads, st, h->start, h->tile_sum, ncel, S, 0); }); nk++;
+    launch(h, K_SCATTER, [&] { pdl_launch(k_scatter, pb, kThreads, st, h->keyrank, n, h->start, h->bstart, S, h->perm); }); nk++;
+    launch(h, K_CELL_SORT, [&] { pdl_launch(k_cell_sort, 148 * 4, 128, st, h->perm, h->B.id, h->start, h->count, S); }); nk++;
     launch(h, K_REORDER, [&] {
-        k_reorder<<<pb, kThreads, 0, st>>>(h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S, h->rheo, h->rho0,
+        pdl_launch(k_reorder, pb, kThreads, st, h->B, n, h->perm, h->keyrank, h->A, h->cellA, h->xhm, S, h->rheo, h->rho0,
                                            h->rcell, h->spec_u, h->spec_a);
     }); nk++;
     // the coarse-level kernels run beside the regular ones when graphs are
@@ -356,9 +375,17 @@ int enqueue_search(gfsph_handle* h, int advance) {
     fork(h, 0);
     with_skf(h, [&](auto sk) {
         constexpr int SKF = decltype(sk)::value;
-        launch(h, K_DENSITY_BIG, [&] { k_density_big<SKF><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
-        launch(h, K_DENSITY, [&] { k_density<false, SKF><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
-        launch(h, K_DENSITY_SPARSE, [&] { k_density<true, SKF><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
+        launch(h, K_DENSITY_BIG, [&] { pdl_launch(k_density_big<SKF>, big_blocks(h), 128, sb, h->A, q, S, h->rheo); });
+        // the two materials' pair types compiled in only when there are two
+        if (h->rheo.ws) {
+            launch(h, K_DENSITY, [&] { pdl_launch(k_density<false, SKF, true>, pb, kThreads, st, h->A, q, S, h->rheo, n); });
+            launch(h, K_DENSITY_SPARSE,
+                   [&] { pdl_launch(k_density<true, SKF, true>, pb, kThreads, st, h->A, q, S, h->rheo, n); });
+        } else {
+            launch(h, K_DENSITY, [&] { pdl_launch(k_density<false, SKF, false>, pb, kThreads, st, h->A, q, S, h->rheo, n); });
+            launch(h, K_DENSITY_SPARSE,
+                   [&] { pdl_launch(k_density<true, SKF, false>, pb, kThreads, st, h->A, q, S, h->rheo, n); });
+        }
     });
     nk += 3;
     join(h, 0);
@@ -385,12 +412,12 @@ int enqueue_norms(gfsph_handle* h, PState As[5]) {
         const int clamp = k ? 1 : 0;
         launch(h, K_NORM, [&] {
             with_skf(h, [&](auto sk) {
-                k_norm<decltype(sk)::value><<<blocks_for(n), kThreads, 0, st>>>(h->A, q, h->S, c, n, hp, clamp, As[k].rho);
+                pdl_launch(k_norm<decltype(sk)::value>, blocks_for(n), kThreads, st, h->A, q, h->S, c, n, hp, clamp, As[k].rho);
             });
         });
         launch(h, K_NORM_BIG, [&] {
             with_skf(h, [&](auto sk) {
-                k_norm_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(h->A, q, h->S, c, hp, clamp, As[k].rho);
+                pdl_launch(k_norm_big<decltype(sk)::value>, big_blocks(h), 128, st, h->A, q, h->S, c, hp, clamp, As[k].rho);
             });
         });
         nk += 2;
@@ -405,9 +432,9 @@ int enqueue_stage_begin(gfsph_handle* h, const PState As[5]) {
     Search q = make_search(h);
     launch(h, K_STAGE, [&] {
         if (c.cos_theta)
-            k_stage_begin<true><<<blocks_for(h->n), kThreads, 0, h->stream>>>(h->A, q, h->S, c, h->dem, As[0].rho);
+            pdl_launch(k_stage_begin<true>, blocks_for(h->n), kThreads, h->stream, h->A, q, h->S, c, h->dem, As[0].rho);
         else
-            k_stage_begin<false><<<blocks_for(h->n), kThreads, 0, h->stream>>>(h->A, q, h->S, c, h->dem, As[0].rho);
+            pdl_launch(k_stage_begin<false>, blocks_for(h->n), kThreads, h->stream, h->A, q, h->S, c, h->dem, As[0].rho);
     });
     return 1;
 }
@@ -423,13 +450,13 @@ int enqueue_wir_stage(gfsph_handle* h, const PState As[5], int s) {
     Search q = make_search(h);
     const int np = h->nx * h->ny;
     launch(h, K_WIR, [&] {
-        k_wir_scatter<<<blocks_for(n), kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho, h->wir_acc);
+        pdl_launch(k_wir_scatter, blocks_for(n), kThreads, st, h->A, q, S, c, h->dem, h->carry, s, As[s].rho, h->wir_acc);
     });
     launch(h, K_WIR, [&] {
-        k_wir_nodes<<<blocks_for((long long)np, 256), 256, 0, st>>>(h->wir_acc, h->d_z, h->wir_hsz, np, S);
+        pdl_launch(k_wir_nodes, blocks_for((long long)np, 256), 256, st, h->wir_acc, h->d_z, h->wir_hsz, np, S);
     });
     launch(h, K_WIR, [&] {
-        k_wir_press<<<blocks_for(n), kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho, h->wir_hsz);
+        pdl_launch(k_wir_press, blocks_for(n), kThreads, st, h->A, q, S, c, h->dem, h->carry, s, As[s].rho, h->wir_hsz);
     });
     return 3;
 }
@@ -448,7 +475,7 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
     if (c.ws) {
         with_skf(h, [&](auto sk) {
             launch(h, K_WIR, [&] {
-                k_wir_pairs_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(h->A, q, S, c);
+                pdl_launch(k_wir_pairs_big<decltype(sk)::value>, big_blocks(h), 128, st, h->A, q, S, c);
             });
         });
         nk += 1 + enqueue_wir_stage(h, As, 0);
@@ -457,25 +484,30 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
     }
     for (int s = 0; s < 4; s++) {
         launch(h, K_FORCE_BIG, [&] {
-            with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[s], q, S, c); });
+            with_skf(h, [&](auto sk) { pdl_launch(k_force_big<decltype(sk)::value>, big_blocks(h), 128, st, As[s], q, S, c); });
         });
         nk++;
         launch(h, K_IFORCE, [&] {
-            with_skf(h, [&](auto sk) { k_iforce<decltype(sk)::value><<<pb, kThreads, 0, st>>>(As[s], q, S, c, n); });
+            with_skf(h, [&](auto sk) {
+                if (c.ws)
+                    pdl_launch(k_iforce<decltype(sk)::value, true>, pb, kThreads, st, As[s], q, S, c, n);
+                else
+                    pdl_launch(k_iforce<decltype(sk)::value, false>, pb, kThreads, st, As[s], q, S, c, n);
+            });
         });
         nk++;
         launch(h, K_STAGE, [&] {
             if (s < 3) {
                 if (c.cos_theta)
-                    k_stage<true><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho, As[s + 1].rho);
+                    pdl_launch(k_stage<true>, pb, kThreads, st, h->A, q, S, c, h->dem, h->carry, s, As[s].rho, As[s + 1].rho);
                 else
-                    k_stage<false><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, h->carry, s, As[s].rho,
+                    pdl_launch(k_stage<false>, pb, kThreads, st, h->A, q, S, c, h->dem, h->carry, s, As[s].rho,
                                                             As[s + 1].rho);
             } else if (c.cos_theta) {
-                k_stage_final<true><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
+                pdl_launch(k_stage_final<true>, pb, kThreads, st, h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
                                                              h->carry, As[3].rho, As[4].rho);
             } else {
-                k_stage_final<false><<<pb, kThreads, 0, st>>>(h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
+                pdl_launch(k_stage_final<false>, pb, kThreads, st, h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
                                                               h->carry, As[3].rho, As[4].rho);
             }
         });
@@ -491,10 +523,10 @@ int enqueue_step_end(gfsph_handle* h) {
     StepScalars* S = h->S;
     if (h->rheo.erosion)
         launch(h, K_DEM_ERODE, [&] {
-            k_dem_erode<<<148 * 2, 256, 0, h->stream>>>(h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S);
+            pdl_launch(k_dem_erode, 148 * 2, 256, h->stream, h->d_auxv, h->d_z, h->d_eroded, h->d_avail, h->nx, S);
         });
     else
-        launch(h, K_STEP_END, [&] { k_step_end<<<1, 32, 0, h->stream>>>(S); });
+        launch(h, K_STEP_END, [&] { pdl_launch(k_step_end, 1, 32, h->stream, S); });
     return 1;
 }
 
@@ -511,12 +543,15 @@ int enqueue_step(gfsph_handle* h) {
         if (h->rheo.av_vel) {  // av_vel with the final depth
             launch(h, K_XSPH_BIG, [&] {
                 with_skf(h, [&](auto sk) {
-                    k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, st>>>(As[4], q, S, h->rheo, h->B);
+                    pdl_launch(k_xsph_big<decltype(sk)::value>, big_blocks(h), 128, st, As[4], q, S, h->rheo, h->B);
                 });
             });
             launch(h, K_XSPH, [&] {
                 with_skf(h, [&](auto sk) {
-                    k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(As[4], q, S, h->rheo, n, h->B);
+                    if (h->rheo.ws)
+                        pdl_launch(k_xsph<decltype(sk)::value, true>, pb, kThreads, st, As[4], q, S, h->rheo, n, h->B);
+                    else
+                        pdl_launch(k_xsph<decltype(sk)::value, false>, pb, kThreads, st, As[4], q, S, h->rheo, n, h->B);
                 });
             });
             nk += 2;
@@ -527,28 +562,28 @@ int enqueue_step(gfsph_handle* h) {
     cudaStream_t sb = side_stream(h);
     fork(h, 1);
     launch(h, K_FORCE_BIG, [&] {
-        with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo); });
+        with_skf(h, [&](auto sk) { pdl_launch(k_force_big<decltype(sk)::value>, big_blocks(h), 128, sb, h->A, q, S, h->rheo); });
     });
     nk++;
     launch(h, K_IFORCE, [&] {
-        with_skf(h, [&](auto sk) { k_iforce<decltype(sk)::value><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n); });
+        with_skf(h, [&](auto sk) { pdl_launch(k_iforce<decltype(sk)::value, false>, pb, kThreads, st, h->A, q, S, h->rheo, n); });
     });
     nk++;
     join(h, 1);
     launch(h, K_FORCE_RK, [&] {
-        k_force_rk<<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
+        pdl_launch(k_force_rk, pb, kThreads, st, h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
     }); nk++;
     if (h->rheo.av_vel) {
         fork(h, 2);
         launch(h, K_XSPH_BIG, [&] {
             with_skf(h, [&](auto sk) {
-                k_xsph_big<decltype(sk)::value><<<big_blocks(h), 128, 0, sb>>>(h->A, q, S, h->rheo, h->B);
+                pdl_launch(k_xsph_big<decltype(sk)::value>, big_blocks(h), 128, sb, h->A, q, S, h->rheo, h->B);
             });
         });
         nk++;
         launch(h, K_XSPH, [&] {
             with_skf(h, [&](auto sk) {
-                k_xsph<decltype(sk)::value><<<pb, kThreads, 0, st>>>(h->A, q, S, h->rheo, n, h->B);
+                pdl_launch(k_xsph<decltype(sk)::value, false>, pb, kThreads, st, h->A, q, S, h->rheo, n, h->B);
             });
         });
         nk++;
@@ -1346,7 +1381,7 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) try {
         As[0] = h->A;
     }
     launch(h, K_IFORCE, [&] {
-        with_skf(h, [&](auto sk) { k_iforce<decltype(sk)::value><<<blocks_for(n), kThreads, 0, s>>>(As[0], q, h->S, h->rheo, n); });
+        with_skf(h, [&](auto sk) { k_iforce<decltype(sk)::value, false><<<blocks_for(n), kThreads, 0, s>>>(As[0], q, h->S, h->rheo, n); });
     });
     launch(h, K_FORCE_BIG, [&] {
         with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });

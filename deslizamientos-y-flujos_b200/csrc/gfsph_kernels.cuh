@@ -86,6 +86,17 @@ struct PState {
     float* pwp;  // basal pore-water pressure Uaux(1,:) (icpwp = 3)
 };
 
+// Programmatic dependent launch: every kernel of the step is launched with
+// programmatic stream serialisation, so the next kernel's launch and block
+// set-up overlap this one's tail.  Each kernel first waits for the kernels
+// before it to finish and their writes to be visible (griddepcontrol.wait,
+// a no-op for an ordinary launch), then lets its dependents launch.
+#define PDL_ENTRY()                                              \
+    do {                                                         \
+        asm volatile("griddepcontrol.wait;" ::: "memory");       \
+        asm volatile("griddepcontrol.launch_dependents;" :::);   \
+    } while (0)
+
 // Scratch of the neighbour search (sorted order).
 struct Search {
     const int* bstart;   // block-map entry -> slot of its block (exclusive scan of the marks), nblocks+1
@@ -170,6 +181,7 @@ __device__ __forceinline__ void prepare_step(StepScalars* S, int advance) {
 }
 
 __global__ void k_prep(StepScalars* S, int advance) {
+    PDL_ENTRY();
     StepScalars* L = scalars_to_smem(S);
     if (threadIdx.x == 0) prepare_step(L, advance);
     scalars_from_smem(S, L);
@@ -223,6 +235,7 @@ __device__ void grid_setup(const Rheo& c, StepScalars* S, const GridArgs ga);
 
 __global__ void __launch_bounds__(kThreadsBounds) k_bounds(PState B, int n, Rheo c, DemView dem, StepScalars* S,
                                                            BoundsPart* part, GridArgs ga) {
+    PDL_ENTRY();
     if (step_skipped(S)) return;
     float xmn = 3.4e38f, xmx = -3.4e38f, ymn = 3.4e38f, ymx = -3.4e38f, hmx = 0.f, dtm = 1.e10f;
     double hs_sum = 0.0;
@@ -429,6 +442,7 @@ __device__ __forceinline__ int block_of(const StepScalars* S, int k, int cx, int
 // largest smoothing length of every level, which bounds the stencils of the
 // neighbour search more tightly than the level's upper limit.
 __global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* bmark) {
+    PDL_ENTRY();
     if (S->skip) return;
     // per-level largest hsml, reduced in shared memory first: every particle
     // of a level would otherwise hit the same global word
@@ -466,6 +480,7 @@ __global__ void k_mark(const PState B, int n, DemView dem, StepScalars* S, int* 
 // histogram holds, nothing is counted and the step stops with kErrCells.
 __global__ void k_hist(const PState B, int n, DemView dem, StepScalars* S, int* bmark, const int* bstart, int* count,
                        int2* keyrank, int cap_cells) {
+    PDL_ENTRY();
     if (S->skip) return;
     const bool sparse = S->sparse != 0;
     const long long ncells = sparse ? (long long)bstart[S->nblocks] * kBlockCells : (long long)S->ncells;
@@ -549,6 +564,7 @@ __device__ void scan_tile_sums(int* tile_sum, int ntiles) {
 // step whose earlier kernels raised an error is stopped here.
 __global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const int* nptr, StepScalars* S,
                              int which) {
+    PDL_ENTRY();
     if (S->skip || (which == 1 && !S->sparse)) return;
     if (S->err) {
         if (blockIdx.x == 0 && threadIdx.x == 0) S->skip = 1;
@@ -608,6 +624,7 @@ __global__ void k_scan_tiles(const int* count, int* start, int* tile_sum, const 
 }
 
 __global__ void k_scan_add(int* start, const int* tile_sum, const int* nptr, const StepScalars* S, int which) {
+    PDL_ENTRY();
     if (S->skip || S->err || (which == 1 && !S->sparse)) return;
     int m = *nptr + 1;
     int base = blockIdx.x * kScanTile;
@@ -622,6 +639,7 @@ __global__ void k_scan_add(int* start, const int* tile_sum, const int* nptr, con
 // Scatter (grid_find :952-958): particles to start[cell] + rank (level 0
 // first, then the higher levels), out-of-domain particles behind them.
 __global__ void k_scatter(const int2* keyrank, int n, const int* start, const int* bstart, StepScalars* S, int* perm) {
+    PDL_ENTRY();
     if (S->skip) return;
     int nact = start[S->ncells];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -656,6 +674,7 @@ __device__ __forceinline__ void insertion_sort_by_id(int* perm, const int* id_ol
 // Also zeroes the histogram it no longer needs, so the counts start at zero
 // in the next step without a clearing pass.
 __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, int* count, const StepScalars* S) {
+    PDL_ENTRY();
     if (S->skip) return;
     int nc = S->ncells;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
@@ -671,6 +690,7 @@ __global__ void k_cell_sort(int* perm, const int* id_old, const int* start, int*
 __global__ void k_reorder(const PState B, int n, const int* perm, const int2* keyrank, PState A, int* cellA,
                           float4* xhm, const StepScalars* S, Rheo c, float* rho0, int2* rcell,
                           const unsigned char* spec_u, unsigned char* spec_a) {
+    PDL_ENTRY();
     if (S->skip) return;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = perm[s];
@@ -853,7 +873,7 @@ __device__ __forceinline__ void level_neighbours(const Search& Q, const StepScal
 // (sum_density_Tools :1796-1836) is accumulated in FP64.  Also stores the
 // pressure term of IntForces_SW with h clamped to h_inf (:6769, :6797): p/h^2
 // (pa_sph 2) or p (pa_sph 1).
-template <bool SPARSE, int SKF>
+template <bool SPARSE, int SKF, bool WS>
 __device__ __forceinline__ void density_regular(PState& A, const Search& Q, StepScalars* S, const Rheo& c) {
     constexpr int SK = SupportScale<SKF>::value;
     const int nreg = S->nreg, nlev = S->nlev;
@@ -865,14 +885,14 @@ __device__ __forceinline__ void density_regular(PState& A, const Search& Q, Step
         double acc = (double)(sph_kernel_w<SKF>(0.f, hi) * me.w);
         int4* tab = Q.nbr + tab_base(i, Q.kcap);
         int cnt = 0;
-        const unsigned char si = c.ws ? Q.spec[i] : 0;
+        const unsigned char si = WS ? Q.spec[i] : 0;
         for (int k = 0; k < nlev; k++)
             level_neighbours<SPARSE, SK>(Q, S, k, i, xi, hi, ci, [&](int j, float4 o, const PairGeom& g) {
                 // W and grad W of the pair, once per step: the internal force,
                 // av_vel and the normalisation read them from the table
                 float w, d0, d1;
                 sph_kernel<SKF>(g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
-                const bool cross = c.ws && Q.spec[j] != si;
+                const bool cross = WS && Q.spec[j] != si;
                 if (cnt < Q.kcap)  // kept in L2 for the internal force (written back to front)
                     tab[(size_t)cnt * kTabStride] =
                         make_int4(cross ? (j | kCrossBit) : j, __float_as_int(w), __float_as_int(d0),
@@ -900,10 +920,11 @@ __device__ __forceinline__ void density_regular(PState& A, const Search& Q, Step
 // not use returns at once (one kernel with both walks would spill in the
 // dense walk).  Held to 48 registers (10 blocks of 128 per SM): the gathers
 // are latency-bound.
-template <bool SPARSE, int SKF>
+template <bool SPARSE, int SKF, bool WS>
 __global__ void __launch_bounds__(128, 10) k_density(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+    PDL_ENTRY();
     if (S->skip || (S->sparse != 0) != SPARSE) return;
-    density_regular<SPARSE, SKF>(A, Q, S, c);
+    density_regular<SPARSE, SKF, WS>(A, Q, S, c);
 }
 
 // Visits every neighbour j of particle i cooperatively over one warp: the
@@ -946,6 +967,7 @@ __device__ __forceinline__ void warp_neighbours(const Search& Q, const StepScala
 // Summation density of the coarse-level particles, one warp per particle.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_density_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    PDL_ENTRY();
     constexpr int SK = SupportScale<SKF>::value;
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
@@ -1004,6 +1026,7 @@ __device__ __forceinline__ void pressure_pair(const Rheo& c, float pi_, float rh
 // Internal acceleration of the coarse-level particles, one warp per particle.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    PDL_ENTRY();
     constexpr int SK = SupportScale<SKF>::value;
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
@@ -1030,6 +1053,7 @@ __global__ void __launch_bounds__(128) k_force_big(PState A, Search Q, StepScala
 // neighbour.  The table is read four entries at a time so that four
 // independent gathers are in flight per thread; the FP64 sum keeps the table
 // order.
+template <bool WS>
 __device__ __forceinline__ void internal_force(const Search& Q, const Rheo& c, int i, float& in0, float& in1) {
     const float4 pri = __ldg(&Q.pr[i]);
     const float pi_ = pri.x, rhoi = pri.y;
@@ -1043,17 +1067,17 @@ __device__ __forceinline__ void internal_force(const Search& Q, const Rheo& c, i
 #pragma unroll
         for (int u = 0; u < 4; u++) e[u] = __ldg(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
-        for (int u = 0; u < 4; u++) prj[u] = __ldg(&Q.pr[e[u].x & ~kCrossBit]);
+        for (int u = 0; u < 4; u++) prj[u] = __ldg(&Q.pr[WS ? (e[u].x & ~kCrossBit) : e[u].x]);
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            if (e[u].x >= 0)  // type 0 only (:6899)
+            if (!WS || e[u].x >= 0)  // type 0 only (:6899)
                 pressure_terms(c, pi_, rhoi, prj[u].x, prj[u].y, prj[u].z, __int_as_float(e[u].z),
                                __int_as_float(e[u].w), a0, a1);
     }
     for (; k < cnt; k++) {
         const int4 e = __ldg(tab + (size_t)k * kTabStride);
-        const float4 prj = __ldg(&Q.pr[e.x & ~kCrossBit]);
-        if (e.x >= 0)
+        const float4 prj = __ldg(&Q.pr[WS ? (e.x & ~kCrossBit) : e.x]);
+        if (!WS || e.x >= 0)
             pressure_terms(c, pi_, rhoi, prj.x, prj.y, prj.z, __int_as_float(e.z), __int_as_float(e.w), a0, a1);
     }
     in0 = (float)a0;
@@ -1219,8 +1243,9 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
 // last-written part (still in L2) is read first, and av_vel, which walks
 // the table front to back after this pass, starts on the part this pass
 // read last.
-template <int SKF>
+template <int SKF, bool WS>
 __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars* S, Rheo c, int n) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nreg = S->nreg;
     const int nw = (nreg + 31) >> 5;
@@ -1228,7 +1253,7 @@ __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars*
         const int i = (nw - 1 - (t >> 5)) * 32 + (t & 31);
         if (i >= nreg) continue;
         float in0, in1;
-        internal_force(Q, c, i, in0, in1);
+        internal_force<WS>(Q, c, i, in0, in1);
         Q.indv[i] = make_float2(in0, in1);
     }
 }
@@ -1250,6 +1275,7 @@ __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars*
 __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
                                                    PState B, float2* velfin, double2* auxv, int forces_only,
                                                    float2* indv_out) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive;
     const float dt = S->dt_step;
@@ -1347,6 +1373,7 @@ __device__ __forceinline__ float prev_depth(const Rheo& c, const float* hp, int 
 template <int SKF>
 __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S, Rheo c, int n, const float* hp,
                                               int clamp_prev, float* hout) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
@@ -1368,6 +1395,7 @@ __global__ void __launch_bounds__(128) k_norm(PState A, Search Q, StepScalars* S
 template <int SKF>
 __global__ void __launch_bounds__(128) k_norm_big(PState A, Search Q, StepScalars* S, Rheo c, const float* hp,
                                                   int clamp_prev, float* hout) {
+    PDL_ENTRY();
     constexpr int SK = SupportScale<SKF>::value;
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
@@ -1408,6 +1436,7 @@ __device__ __forceinline__ float stage_pterm(const Rheo& c, const DemView& dem, 
 template <bool COS>
 __global__ void __launch_bounds__(128) k_stage_begin(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
                                                      const float* h1) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
@@ -1440,6 +1469,7 @@ __device__ __forceinline__ bool wir_stage_pos(const PState& A, const StageCarry&
 // summed in FP64.
 __global__ void __launch_bounds__(128) k_wir_scatter(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
                                                      StageCarry C, int s, const float* hdep, double2* acc) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive;
     const float dt = S->dt_step;
@@ -1468,6 +1498,7 @@ __global__ void __launch_bounds__(128) k_wir_scatter(PState A, Search Q, StepSca
 // Z + hs at the DEM nodes (:17861-17867); the accumulators are left zeroed
 // for the next stage.
 __global__ void k_wir_nodes(double2* acc, const float* z, float* hsz, int np, const StepScalars* S) {
+    PDL_ENTRY();
     if (S->skip) return;
     for (int ip = blockIdx.x * blockDim.x + threadIdx.x; ip < np; ip += gridDim.x * blockDim.x) {
         const double2 a = acc[ip];
@@ -1499,6 +1530,7 @@ __device__ __forceinline__ void wir_pair_term(const Rheo& c, bool water, float m
 // soil-water pair sum of every regular particle, from its table.
 __global__ void __launch_bounds__(128) k_wir_press(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
                                                    StageCarry C, int s, const float* hdep, const float* hsz) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive, nreg = S->nreg;
     const float dt = S->dt_step;
@@ -1549,6 +1581,7 @@ __global__ void __launch_bounds__(128) k_wir_press(PState A, Search Q, StepScala
 // The soil-water pair sums of the coarse-level particles, one warp each.
 template <int SKF>
 __global__ void __launch_bounds__(128) k_wir_pairs_big(PState A, Search Q, StepScalars* S, Rheo c) {
+    PDL_ENTRY();
     constexpr int SK = SupportScale<SKF>::value;
     if (S->skip) return;
     const int lane = threadIdx.x & 31;
@@ -1580,6 +1613,7 @@ __global__ void __launch_bounds__(128) k_wir_pairs_big(PState A, Search Q, StepS
 template <bool COS>
 __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
                                                StageCarry C, int s, const float* hs_, const float* hnext) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive;
     const float dt = S->dt_step;
@@ -1641,6 +1675,7 @@ template <bool COS>
 __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
                                                      PState B, float2* velfin, double2* auxv, StageCarry C,
                                                      const float* h4, const float* hfin) {
+    PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive;
     const float dt = S->dt_step;
@@ -1717,8 +1752,9 @@ __device__ __forceinline__ void xsph_pair(float2 vi, float rhoi, float2 vj, floa
 
 // av_vel (SPH_MAIN_2019.f90:3042-3099) with the start-of-step W_ij, then
 // v += 0.3*av for particles still inside the domain (:987-993).
-template <int SKF>
+template <int SKF, bool WS>
 __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S, Rheo c, int n, PState B) {
+    PDL_ENTRY();
     if (S->skip || !c.av_vel) return;
     const int nreg = S->nreg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nreg; i += gridDim.x * blockDim.x) {
@@ -1736,17 +1772,17 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
 #pragma unroll
             for (int u = 0; u < 4; u++) e[u] = __ldcs(tab + (size_t)(k + u) * kTabStride);
 #pragma unroll
-            for (int u = 0; u < 4; u++) sj[u] = Q.xsv[e[u].x & ~kCrossBit];
+            for (int u = 0; u < 4; u++) sj[u] = Q.xsv[WS ? (e[u].x & ~kCrossBit) : e[u].x];
 #pragma unroll
             for (int u = 0; u < 4; u++)
-                if (e[u].x >= 0)  // type 0 only (SPH_MAIN_2019.f90:3071)
+                if (!WS || e[u].x >= 0)  // type 0 only (SPH_MAIN_2019.f90:3071)
                     xsph_terms(vi, rhoi, make_float2(sj[u].x, sj[u].y), sj[u].z, sj[u].w, __int_as_float(e[u].y), a0,
                                a1);
         }
         for (; k < cnt; k++) {
             const int4 e = __ldcs(tab + (size_t)k * kTabStride);
-            const float4 sj = Q.xsv[e.x & ~kCrossBit];
-            if (e.x >= 0) xsph_terms(vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, __int_as_float(e.y), a0, a1);
+            const float4 sj = Q.xsv[WS ? (e.x & ~kCrossBit) : e.x];
+            if (!WS || e.x >= 0) xsph_terms(vi, rhoi, make_float2(sj.x, sj.y), sj.z, sj.w, __int_as_float(e.y), a0, a1);
         }
         float av0 = 0.3f * (float)a0, av1 = 0.3f * (float)a1;
         B.vel[i] = make_float2(vi.x + av0, vi.y + av1);
@@ -1755,6 +1791,7 @@ __global__ void __launch_bounds__(128) k_xsph(PState A, Search Q, StepScalars* S
 
 template <int SKF>
 __global__ void __launch_bounds__(128) k_xsph_big(PState A, Search Q, StepScalars* S, Rheo c, PState B) {
+    PDL_ENTRY();
     constexpr int SK = SupportScale<SKF>::value;
     if (S->skip || !c.av_vel) return;
     const int lane = threadIdx.x & 31;
@@ -1820,6 +1857,7 @@ __device__ __forceinline__ void step_end(StepScalars* S) {
 }
 
 __global__ void k_step_end(StepScalars* S) {
+    PDL_ENTRY();
     StepScalars* L = scalars_to_smem(S);
     if (threadIdx.x == 0) step_end(L);
     scalars_from_smem(S, L);
@@ -1829,6 +1867,7 @@ __global__ void k_step_end(StepScalars* S) {
 // step, resetting the scatter accumulators; the last block to finish also
 // ends the step (k_step_end), which saves a launch.
 __global__ void k_dem_erode(double2* auxv, float* z, float* eroded, float* avail, int nx, StepScalars* S) {
+    PDL_ENTRY();
     __shared__ bool last;
     const int x0 = S->ex0, x1 = S->ex1, y0 = S->ey0, y1 = S->ey1;
     if (!S->skip && x1 >= x0 && y1 >= y0) erode_box(auxv, z, eroded, avail, nx, x0, x1, y0, y1);
