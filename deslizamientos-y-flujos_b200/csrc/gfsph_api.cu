@@ -817,6 +817,7 @@ int validate(const gfsph_params* p) {
     if (!(p->dt > 0.f)) return GFSPH_ERR_ARG;
     if (p->ws_interact != 0 && p->ws_interact != 1) return GFSPH_ERR_UNSUPPORTED;
     if (p->sw_alg != 0 && p->sw_alg != 1) return GFSPH_ERR_UNSUPPORTED;
+    if (p->ws_interact == 0 && p->sw_alg != 0) return GFSPH_ERR_UNSUPPORTED;  // ic_SWalg 1 of one material: not built
     // soil and water: no erosion, pore pressure, normalised density or
     // terrain-normal gravity with them here
     if (p->ws_interact == 1 && (erosion || p->icpwp != 0 || p->nor_density != 0 || cos_theta != 0))

@@ -267,6 +267,31 @@ SwDat read_dat(const std::string& path) {
         r.label();
         d.pts_name = split_items(r.label()).at(0);
     }
+    if (d.ic_water == 1) {  // Get_water_points (:2226-2273)
+        r.label();
+        if (d.ic_soil == 1) {
+            d.icunk_w = r.read_int();
+        } else {
+            v = r.values(2);
+            d.icunk_w = (int)to_real(v[0], path);
+            d.h_inf = to_real(v[1], path);
+        }
+        if (d.icunk_w != 7 && d.icunk_w != 8)
+            throw std::runtime_error(path + ": icunk_w " + std::to_string(d.icunk_w) +
+                                     " is not supported (7 and 8, a .pts source, are)");
+        // Read_Source_plus_New_WATER (:5329-5336): a label and the problem name (a16)
+        r.label();
+        std::string nm = r.label();
+        if (nm.size() > 16) nm = nm.substr(0, 16);
+        d.water_pts_name = split_items(nm).at(0);
+        if (d.ic_soil != 1) throw std::runtime_error(path + ": water without soil particles is not supported");
+        if (d.ic_swalg != 0 && d.ic_swalg != 1)
+            throw std::runtime_error(path + ": ic_SWAlg " + std::to_string(d.ic_swalg) +
+                                     " with soil and water is the debris-flow mixture (ic_ws_Interact = 2), not built");
+    } else if (d.ic_swalg != 0) {
+        throw std::runtime_error(path + ": ic_SWAlg " + std::to_string(d.ic_swalg) +
+                                 " is supported only with soil and water particles (ic_soil = ic_water = 1)");
+    }
     r.label();
     v = r.values(4);
     d.pa_sph = (int)to_real(v[0], path); d.nnps = (int)to_real(v[1], path);

@@ -38,6 +38,8 @@ struct SwDat {
     int icunk_s = 7;            // 7, 8: .pts source; 200: restart (Get_Restart_Info_SW)
     float h_inf = 0.01f;
     std::string pts_name;       // the .pts name, or the problem name of a restart
+    int icunk_w = 0;            // water points (Get_water_points): 7, 8 a .pts source
+    std::string water_pts_name; // the water .pts name (Read_Source_plus_New_WATER :5329-5336)
     int pa_sph = 2, nnps = 2, sle = 1, skf = 1;
     bool sum_den = true, av_vel = true, virt_part = false, nor_dens = false;
     float cst[110] = {};        // const(1..110)

@@ -206,24 +206,39 @@ int main(int argc, char** argv) {
         const bool restart = (d.icunk_s == 200);
         int dropped = 0;
         std::vector<float> x, v0, h, mass, hsml, pwp0;
+        std::vector<int> itype;  // 1 soil, 2 water (ic_ws_Interact = 1)
+        const bool wir = (d.ic_soil == 1 && d.ic_water == 1);
         double time0 = 0.0;
         Particles P;
         if (restart) {  // Get_Restart_Info_SW opens restart.dat whatever the problem name (:3307)
             RestartState R = read_restart(join(dir, "restart.dat"));
             for (int k : R.itype)
-                if (k != 1) throw std::runtime_error("restart.dat: only soil particles (itype 1) are supported");
-            x = R.x; v0 = R.v; h = R.h; mass = R.mass; hsml = R.hsml; pwp0 = R.pwp;
+                if (k != 1 && !(k == 2 && wir))
+                    throw std::runtime_error("restart.dat: itype " + std::to_string(k) +
+                                             " (soil 1, and water 2 with ic_water = 1, are supported)");
+            x = R.x; v0 = R.v; h = R.h; mass = R.mass; hsml = R.hsml; pwp0 = R.pwp; itype = R.itype;
             time0 = R.time;
         } else {
+            auto add = [&](const Particles& Q, int type) {
+                for (int i = 0; i < Q.n(); i++) {
+                    if (!(Q.mass[i] > 0.f)) { dropped++; continue; }  // lattice nodes with no complete cell: zero volume
+                    x.push_back(Q.x[2 * i]); x.push_back(Q.x[2 * i + 1]);
+                    h.push_back(Q.h[i]); mass.push_back(Q.mass[i]); hsml.push_back(Q.hsml[i]);
+                    itype.push_back(type);
+                }
+            };
             // Read_Source_plus_New opens problem_name_Global.pts whatever name the .dat gives (:5058-5061)
             P = read_pts(find_file(dir, problem, pexts), d.h_inf, d.icunk_s, t.xshift, t.yshift);
-            for (int i = 0; i < P.n(); i++) {
-                if (!(P.mass[i] > 0.f)) { dropped++; continue; }  // lattice nodes with no complete cell: zero volume
-                x.push_back(P.x[2 * i]); x.push_back(P.x[2 * i + 1]);
-                h.push_back(P.h[i]); mass.push_back(P.mass[i]); hsml.push_back(P.hsml[i]);
+            add(P, 1);
+            if (wir) {  // the water after the soil (npoin = npoin_s + npoin_w, :997); no expansion lines
+                Particles W = read_pts(find_file(dir, d.water_pts_name, pexts), d.h_inf, 7, t.xshift, t.yshift);
+                add(W, 2);
+                P.total_volume += W.total_volume;
             }
             v0.assign(x.size(), 0.f);
         }
+        int n_water = 0;
+        for (int k : itype) n_water += (k == 2);
         const int n = (int)h.size();
         double total_volume = P.total_volume;
         if (restart)
@@ -233,10 +248,11 @@ int main(int argc, char** argv) {
                         "\"ic_adapt\": %d, \"nx\": %d, \"ny\": %d, \"xmin\": %.6f, \"ymin\": %.6f, \"dx\": %g, \"dy\": %g, "
                         "\"ictop\": %d, \"fdiff\": %d, \"n\": %d, \"dropped\": %d, \"volume\": %.6f, \"hsml\": %g, "
                         "\"pa_sph\": %d, \"nnps\": %d, \"sle\": %d, \"skf\": %d, \"nfric\": %d, \"icpwp\": %d, \"pwp0rel\": %g, \"h_inf\": %g, "
-                        "\"const\": [",
+                        "\"n_water\": %d, \"ws_interact\": %d, \"sw_alg\": %d, \"const\": [",
                         "", m.dt, m.time_end, m.plot_step, m.dt_sph, m.ic_adapt, t.nx, t.ny, (double)t.xmin,
                         (double)t.ymin, t.dx, t.dy, t.ictop, t.fdiff ? 1 : 0, n, dropped, total_volume,
-                        n ? hsml[0] : 0.f, d.pa_sph, d.nnps, d.sle, d.skf, (int)(d.cst[4] + 0.01f), d.icpwp, d.pwp0rel, d.h_inf);
+                        n ? hsml[0] : 0.f, d.pa_sph, d.nnps, d.sle, d.skf, (int)(d.cst[4] + 0.01f), d.icpwp, d.pwp0rel, d.h_inf,
+                        n_water, wir ? 1 : 0, d.ic_swalg);
             for (int k = 0; k < 60; k++) std::printf("%s%g", k ? ", " : "", d.cst[k]);
             double zsum = 0.0;
             for (float z : t.z) zsum += z;
@@ -254,6 +270,8 @@ int main(int argc, char** argv) {
         p.dem_deriv = t.fdiff ? 1 : 0;
         p.icpwp = d.icpwp;
         p.pwp0rel = d.pwp0rel;
+        p.ws_interact = wir ? 1 : 0;  // Input_SW :947-951
+        p.sw_alg = d.ic_swalg;
         gfsph_dem dem;
         std::memset(&dem, 0, sizeof(dem));
         dem.nx = t.nx; dem.ny = t.ny; dem.xmin = t.xmin; dem.ymin = t.ymin; dem.dx = t.dx; dem.dy = t.dy;
@@ -281,7 +299,7 @@ int main(int argc, char** argv) {
         if (!dump.empty()) {
             FILE* f = std::fopen(dump.c_str(), "wb");
             if (!f) throw std::runtime_error("cannot write " + dump);
-            const int ver = 1, psz = (int)sizeof(p);
+            const int ver = 2, psz = (int)sizeof(p);
             std::fwrite("GFSPHDMP", 1, 8, f);
             std::fwrite(&ver, 4, 1, f); std::fwrite(&psz, 4, 1, f); std::fwrite(&p, sizeof(p), 1, f);
             std::fwrite(&t.nx, 4, 1, f); std::fwrite(&t.ny, 4, 1, f);
@@ -292,12 +310,13 @@ int main(int argc, char** argv) {
             std::fwrite(x.data(), 4, x.size(), f); std::fwrite(v0.data(), 4, v0.size(), f);
             std::fwrite(h.data(), 4, h.size(), f); std::fwrite(mass.data(), 4, mass.size(), f);
             std::fwrite(hsml.data(), 4, hsml.size(), f);
+            std::fwrite(itype.data(), 4, itype.size(), f);  // version 2: the material per particle
             std::fclose(f);
             return 0;
         }
         gfsph_handle* hd = nullptr;
         check(gfsph_create(&p, &dem, &hd), "gfsph_create");
-        check(gfsph_upload(hd, n, x.data(), v0.data(), h.data(), mass.data(), hsml.data(), nullptr, nullptr),
+        check(gfsph_upload(hd, n, x.data(), v0.data(), h.data(), mass.data(), hsml.data(), itype.data(), nullptr),
               "gfsph_upload");
         if (restart) {
             if (d.icpwp == 3) check(gfsph_set_pwp(hd, pwp0.data()), "gfsph_set_pwp");
@@ -333,7 +352,7 @@ int main(int argc, char** argv) {
             check(gfsph_download(hd, rx.data(), rv.data(), rh.data(), rm.data(), rs.data(), rf.data()), "gfsph_download");
             RestartState R;
             R.time = tnow;
-            R.itype.assign(n, 1);
+            R.itype = itype;
             R.x = rx; R.v = rv; R.h = rh; R.mass = rm; R.hsml = rs;
             R.pwp.assign(n, 0.f);
             if (d.icpwp == 3) check(gfsph_get_pwp(hd, R.pwp.data()), "gfsph_get_pwp");

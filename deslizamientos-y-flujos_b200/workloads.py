@@ -303,14 +303,17 @@ def p1_mass_matrices(intmat, coords):
     return (a2 / 24.0)[:, None, None] * m[None, :, :]
 
 
-def write_reference_inputs(w, directory, name, out_step=100, restart=False):
+def write_reference_inputs(w, directory, name, out_step=100, restart=False, water=None):
     """Writes a workload in the reference's own input formats, so that the
     Fortran program (or gfsph_run) can read it: <name>.MASTER.dat,
     <name>.dat, <name>.top (ictop = 100: a grid file with finite-difference
     slopes) and <name>.pts (the particles as source points on their
     lattice).  w.options may carry icpwp (0 or 3) and pwp0rel.  out_step is
     print_step = save_step = plot_step; restart=True writes icunk_s = 200,
-    which reads the particles from restart.dat (Get_Restart_Info_SW)."""
+    which reads the particles from restart.dat (Get_Restart_Info_SW).
+    water: soil and water (ic_soil = ic_water = 1, ic_SWAlg = w.options'
+    sw_alg): a dict with the water's x, rho and lattice, written as
+    <name>_w.pts and read through Read_Source_plus_New_WATER (icunk_w 7)."""
     import os
     os.makedirs(directory, exist_ok=True)
     o = w.options
@@ -339,14 +342,17 @@ def write_reference_inputs(w, directory, name, out_step=100, restart=False):
         f.write("dt_sph ic_adapt\n  %g %d\n" % (dt, o["ic_adapt"]))
         f.write("Ntime curves max pts\n  0 6\nwin\n0\n")
     with open(os.path.join(directory, name + ".dat"), "w") as f:
-        f.write("1\n " + name + "\n ic_SW_Alg\n  0\nnhist\n  0\nndimn\n  2\n")
-        f.write("ic_soil ic_water ic_vps ic_abs\n  1 0 0 0\n")
+        f.write("1\n " + name + "\n ic_SW_Alg\n  %d\nnhist\n  0\nndimn\n  2\n" % int(o.get("sw_alg", 0)))
+        f.write("ic_soil ic_water ic_vps ic_abs\n  1 %d 0 0\n" % (1 if water is not None else 0))
         if restart:
             f.write("Soil unkno h_inf_SW\n  200 %g\n" % o["h_inf"])
             f.write("problem name (restart)\n  " + name + "\n")
         else:
             f.write("Soil unkno h_inf_SW\n  7 %g\n" % o["h_inf"])
             f.write("pts file name\n  " + name + "\n")
+        if water is not None:
+            f.write("Water unkno\n  7\n")
+            f.write("water pts file name\n  " + name + "_w\n")
         f.write("pa_sph nnps sle skf\n  %d %d %d %d\n" % (o["pa_sph"], o["nnps"], o["sle"], o["skf"]))
         f.write("sum_den av_vel virt_part nor_dens\n  T %s F F\n" % ("T" if o["average_velocity"] else "F"))
         for b in range(blocks):
@@ -370,12 +376,18 @@ def write_reference_inputs(w, directory, name, out_step=100, restart=False):
                 k += 1
     lattice = float(w.meta["lattice"])
     facthsml = float(w.hsml[0]) / lattice
-    with open(os.path.join(directory, name + ".pts"), "w") as f:
-        f.write("npoin source  grid spacing  facthsml\n")
-        f.write("%d %.9g %.9g %.9g %.9g\n" % (w.n, lattice, lattice, lattice, facthsml))
-        f.write("X Y h\n")
-        for (xx, yy), hh in zip(w.x.astype(np.float64), w.rho.astype(np.float64)):
-            f.write("%.9g %.9g %.9g\n" % (float(xx), float(yy), float(hh)))
+    def write_pts(path, xs, hs, lat, fh):
+        with open(path, "w") as f:
+            f.write("npoin source  grid spacing  facthsml\n")
+            f.write("%d %.9g %.9g %.9g %.9g\n" % (len(hs), lat, lat, lat, fh))
+            f.write("X Y h\n")
+            for (xx, yy), hh in zip(np.asarray(xs, np.float64), np.asarray(hs, np.float64)):
+                f.write("%.9g %.9g %.9g\n" % (float(xx), float(yy), float(hh)))
+
+    write_pts(os.path.join(directory, name + ".pts"), w.x, w.rho, lattice, facthsml)
+    if water is not None:
+        write_pts(os.path.join(directory, name + "_w.pts"), water["x"], water["rho"], float(water["lattice"]),
+                  float(water.get("facthsml", facthsml)))
 
 
 def from_driver_dump(path, gfsph_module):
@@ -387,7 +399,7 @@ def from_driver_dump(path, gfsph_module):
     if b[:8] != b"GFSPHDMP":
         raise ValueError(path + ": not a gfsph_run dump")
     ver, psz = np.frombuffer(b, np.int32, 2, 8)
-    if ver != 1 or psz != C.sizeof(gfsph_module.Params):
+    if ver not in (1, 2) or psz != C.sizeof(gfsph_module.Params):
         raise ValueError(path + ": dump version or params size mismatch")
     off = 16
     p = gfsph_module.Params.from_buffer_copy(b[off:off + psz])
@@ -410,7 +422,8 @@ def from_driver_dump(path, gfsph_module):
     x = take(2 * n, (n, 2))
     v = take(2 * n, (n, 2))
     rho, mass, hsml = take(n, (n,)), take(n, (n,)), take(n, (n,))
+    itype = np.frombuffer(b, np.int32, n, off).copy() if ver >= 2 else np.ones(n, np.int32)
     const = {k + 1: float(p.cst[k]) for k in range(len(p.cst)) if p.cst[k] != 0.0}
     w = Workload(name=os.path.basename(path), const=const, options={}, z=z, dx=dx, dy=dy, x=x, v=v, rho=rho,
-                 mass=mass, hsml=hsml, meta=dict(xmin=xmin, ymin=ymin))
+                 mass=mass, hsml=hsml, meta=dict(xmin=xmin, ymin=ymin, itype=itype))
     return w, p

@@ -1188,7 +1188,7 @@ struct Oracle {
         if (P->skf < 1 || P->skf > 4) return GFSPH_ERR_UNSUPPORTED;
         ws = P->ws_interact;
         swalg = P->sw_alg;
-        if (ws < 0 || ws > 1 || swalg < 0 || swalg > 1) return GFSPH_ERR_UNSUPPORTED;
+        if (ws < 0 || ws > 1 || swalg < 0 || swalg > 1 || (ws == 0 && swalg != 0)) return GFSPH_ERR_UNSUPPORTED;
         if (ws && (ic_erosion || P->icpwp != 0 || P->nor_density != 0 || ic_costheta != 0))
             return GFSPH_ERR_UNSUPPORTED;
         nx = nx_; ny = ny_; npoig = nx * ny;

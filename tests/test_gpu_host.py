@@ -155,3 +155,21 @@ def test_gid_results_agree_with_the_depth_raster(gfsph_lib, tmp_path):
         ref = depth.reshape(-1)[ip]
         assert np.allclose(nodes[:, 3], ref, rtol=2e-4, atol=1e-5)
         assert '"dis"' in blk and '"vel"' in blk
+
+
+def test_driver_runs_soil_and_water(gfsph_lib, tmp_path):
+    """gfsph_run on soil and water inputs (ic_soil = ic_water = 1, ic_SWAlg 1):
+    the run steps both materials, and its restart file carries the water's
+    itype 2 rows after the soil's, as OutputSave_SW writes them."""
+    w, a = workloads.soil_and_pond()
+    water = dict(x=a["x"][a["itype"] == 2], rho=a["rho"][a["itype"] == 2], lattice=1.5)
+    d = str(tmp_path)
+    workloads.write_reference_inputs(w, d, "pond", out_step=10, water=water)
+    meta = json.loads(subprocess.run([RUN, "pond", "--dir", d, "--parse-only"], capture_output=True,
+                                     text=True).stdout)
+    run_driver(d, "pond", 20)
+    st = np.loadtxt(os.path.join(d, "pond.restart.dat"), skiprows=3)
+    assert st.shape[0] == meta["n"] and int((st[:, 1] == 2).sum()) == meta["n_water"] > 0
+    assert (np.diff(st[:, 1]) >= 0).all()  # soil first, then water
+    water_rows = st[:, 1] == 2
+    assert np.abs(st[water_rows, 4:6]).max() > 1e-3  # the water moved

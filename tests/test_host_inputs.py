@@ -179,3 +179,30 @@ def test_picacho_setup_matches_the_oracle_restatement(gfsph_lib, oracle_mod, tmp
     assert keep.sum() == w.n
     for key, got in (("x", w.x), ("h", w.rho), ("mass", w.mass), ("hsml", w.hsml)):
         assert np.array_equal(got, src[key][keep]), key
+
+
+def test_soil_and_water_inputs_parse(gfsph_lib, tmp_path):
+    """ic_soil = ic_water = 1 with ic_SWAlg 1: the water points of
+    Get_water_points (SPH_SW_2019.f90:2226-2273) through
+    Read_Source_plus_New_WATER (icunk_w 7, a .pts named in the .dat) follow
+    the soil's; the run takes ic_ws_Interact = 1.  Without water, ic_SWAlg 1
+    is refused, and so is the debris-flow mixture (ic_SWAlg 3)."""
+    w, a = workloads.soil_and_pond()
+    w.meta["lattice"] = 1.5
+    water = dict(x=a["x"][a["itype"] == 2], rho=a["rho"][a["itype"] == 2], lattice=1.5)
+    d = str(tmp_path / "wir")
+    workloads.write_reference_inputs(w, d, "pond", water=water)
+    meta = parse("pond", d)
+    assert meta["ws_interact"] == 1 and meta["sw_alg"] == 1
+    soil_only = str(tmp_path / "soil")
+    w.options = {**w.options, "sw_alg": 0}
+    workloads.write_reference_inputs(w, soil_only, "pond")
+    alone = parse("pond", soil_only)
+    assert meta["n_water"] > 0 and meta["n"] == alone["n"] + meta["n_water"]
+    assert abs(meta["n_water"] - len(water["rho"])) <= 0.1 * len(water["rho"])
+    for sw, wat in ((1, False), (3, True)):
+        dd = str(tmp_path / f"bad{sw}")
+        w.options = {**w.options, "sw_alg": sw}
+        workloads.write_reference_inputs(w, dd, "pond", water=water if wat else None)
+        out = subprocess.run([RUN, "pond", "--dir", dd, "--parse-only"], capture_output=True, text=True)
+        assert out.returncode != 0 and "ic_SWAlg" in out.stderr
