@@ -39,14 +39,14 @@ UNIT = "particle-steps/s"
 # artefact of the split and is not counted.
 B_ALG = {"k_density": 24, "k_iforce": 24, "k_force_rk": 48, "k_xsph": 44, "k_hist": 28}
 # From ncu on this workload (200,011 particles), per particle: DRAM read +
-# write bytes per launch and warp instructions per launch, averaged over the
-# launches of NCU_STEPS (the steps the driver's default run times:
-# `bench.py --steps 20 --warmup 5`).  The issue-bound figure is printed only
-# when the run times those same steps, since the neighbour work per step grows
-# as the flow spreads.
-NCU_STEPS = None  # (first, last) step of the capture; None: no capture of the current kernels yet
-NCU_PER_PARTICLE = {}
-NCU_SOURCE = "profiles/ (ncu, cold caches), scaled by active particles"
+# write bytes per launch and warp instructions per launch of k_density, the
+# mean of its launches at steps 6, 16 and 25 (first, middle and last of the
+# steps `bench.py --steps 20 --warmup 5` times; one launch each, cold caches).
+# The issue-bound figure is printed only when the run times those same steps,
+# since the neighbour work per step grows as the flow spreads.
+NCU_STEPS = (6, 25)
+NCU_PER_PARTICLE = {"k_density": {"warp_inst": 68.12e6 / 200011, "dram_bytes": 104.36e6 / 200011}}
+NCU_SOURCE = "profiles/neighbour_kernels_fractal_channel_200k.md (ncu, cold caches, steps 6/16/25), scaled by active particles"
 ISSUE_PEAK = 148 * 4 * 1.965e9  # warp instructions/s: SMs x schedulers x max SM clock
 
 

@@ -14,12 +14,15 @@
 // One step, five kernels (niter + 3 launches):
 //   k_gfl_nodes   fluxes and sources at the nodes (first_step :1890-1958);
 //   k_gfl_elems   per element: the half-step values at the Gauss points
-//                 (first_step :1964-2048) and, at each of them, the fluxes
-//                 and sources of second_step (:2157-2300);
-//   k_gfl_rhs     per node, gathered over its elements in element order and
-//                 then its boundary sides in side order, as second_step adds
-//                 them (:2300-2355): the right-hand side; the wall
-//                 projection of solve (:2629-2656) and its first sweep;
+//                 (first_step :1964-2048), at each of them the fluxes and
+//                 sources of second_step (:2157-2300), and the term each
+//                 Gauss point adds to each of the element's nodes (:2300-2312),
+//                 one float4 per (element, node, Gauss point);
+//   k_gfl_rhs     per node, those terms gathered over its elements in element
+//                 order (Gauss points in order), then its boundary sides in side
+//                 order, as second_step adds them (:2300-2355): the right-hand
+//                 side; the wall projection of solve (:2629-2656) and its first
+//                 sweep;
 //   k_gfl_mass    the further sweeps u += (rhs - M u)/ML with the wall
 //                 filter (:2660-2785), M u gathered in element order;
 //   k_gfl_update  addthem (:3199-3215) and check (:3306-3345).
@@ -72,7 +75,8 @@ struct GflDev {
     const float2* gradhs_w;   // WIR: its nodal gradient
     float* unkno;             // (3, npoin) h, hu, hv
     float* fnode;             // (9, npoin): fluxp(3), fluyp(3), gpoin(3)
-    float* gp;                // (9, ngaus * nelem): fluxe2(3), fluye2(3), gelem2(3) at each Gauss point
+    float4* gt;               // per element, local node and Gauss point (3 x 3 float4): the rhs terms of
+                              // second_step for h, hu, hv (w unused)
     float* rhs1;              // (3, npoin)
     float* rhs0[2];           // (3, npoin), double buffer of the sweeps
 };
@@ -271,12 +275,20 @@ __global__ void k_gfl_elems(GflDev d, GflConst c, float tanfi, float dt) {
                 HH = 0.f;
                 pres = (cgra05 * h) * h;
             }
-            float* o = d.gp + 9 * ((size_t)ie * c.ngaus + ig);
+            float o[9];
             o[0] = hu; o[1] = (hu * hu) * hinv + pres; o[2] = (hu * hv) * hinv;
             o[3] = hv; o[4] = o[2]; o[5] = (hv * hv) * hinv + pres;
             float frx, fry, slx, sly, cx, cy;
             frictlaws(c, tanfi, mt, h, hu, hv, HH, frx, fry, slx, sly, cx, cy);
             sources(c, frx, fry, slx, sly, cx, cy, hu, hv, o + 6);
+            // the terms this Gauss point adds to each node's rhs (:2300-2312)
+            const float dvolu = d.geome[7 * (size_t)ie + 6] / (float)(2 * c.ngaus);
+            for (int in = 0; in < 3; in++) {
+                float t[3];
+                for (int ia = 0; ia < 3; ia++)
+                    t[ia] = (((gx[in] * o[ia] + gy[in] * o[3 + ia]) + sh[in] * o[6 + ia]) * dvolu) * dt;
+                d.gt[3 * (3 * (size_t)ie + in) + ig] = make_float4(t[0], t[1], t[2], 0.f);
+            }
         }
     }
 }
@@ -294,15 +306,11 @@ __global__ void k_gfl_rhs(GflDev d, GflConst c, float dt) {
     for (int ip = blockIdx.x * blockDim.x + threadIdx.x; ip < d.npoin; ip += gridDim.x * blockDim.x) {
         float r[3] = {0.f, 0.f, 0.f};
         for (int q = d.adj_ptr[ip]; q < d.adj_ptr[ip + 1]; q++) {
-            const int2 a = d.adj[q];  // element, local node
-            const float anx = d.geome[7 * (size_t)a.x + a.y], any = d.geome[7 * (size_t)a.x + 3 + a.y];
-            const float dvolu = d.geome[7 * (size_t)a.x + 6] / (float)(2 * c.ngaus);
+            const int2 a = d.adj[q];  // element, local node: its terms in Gauss point order
+            const float4* row = d.gt + 3 * (3 * (size_t)a.x + a.y);
             for (int ig = 0; ig < c.ngaus; ig++) {
-                float sh[3];
-                gauss_point(c.ngaus, ig, sh);
-                const float xni = sh[a.y];
-                const float* o = d.gp + 9 * ((size_t)a.x * c.ngaus + ig);
-                for (int ia = 0; ia < 3; ia++) r[ia] = r[ia] + (((anx * o[ia] + any * o[3 + ia]) + xni * o[6 + ia]) * dvolu) * dt;
+                const float4 t = row[ig];
+                r[0] = r[0] + t.x; r[1] = r[1] + t.y; r[2] = r[2] + t.z;
             }
         }
         for (int q = d.bside_ptr[ip]; q < d.bside_ptr[ip + 1]; q++) {
@@ -399,7 +407,8 @@ struct gfsph_gfl {
     float *geome = nullptr, *d_topel = nullptr, *d_topol = nullptr, *mmatl = nullptr, *hs_w = nullptr;
     float4* side_geom = nullptr;
     float2 *rtang = nullptr, *gradhs_w = nullptr;
-    float *unkno = nullptr, *fnode = nullptr, *gp = nullptr, *rhs1 = nullptr, *rhs0a = nullptr, *rhs0b = nullptr;
+    float4* gt = nullptr;
+    float *unkno = nullptr, *fnode = nullptr, *rhs1 = nullptr, *rhs0a = nullptr, *rhs0b = nullptr;
     bool wir = false;
     long long launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the last gfsph_gfl_step
@@ -411,7 +420,7 @@ namespace {
 void gfl_free(gfsph_gfl* g) {
     void* ptrs[] = {g->elem, g->adj_ptr, g->bside_ptr, g->bnode, g->adj, g->bside, g->side_nodes, g->geome,
                     g->d_topel, g->d_topol, g->mmatl, g->hs_w, g->side_geom, g->rtang, g->gradhs_w, g->unkno,
-                    g->fnode, g->gp, g->rhs1, g->rhs0a, g->rhs0b};
+                    g->fnode, g->gt, g->rhs1, g->rhs0a, g->rhs0b};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -425,7 +434,7 @@ GflDev view(gfsph_gfl* g) {
     d.topol = g->d_topol; d.mmatl = g->mmatl; d.adj_ptr = g->adj_ptr; d.adj = g->adj; d.bside_ptr = g->bside_ptr;
     d.bside = g->bside; d.side_nodes = g->side_nodes; d.side_geom = g->side_geom; d.bnode = g->bnode;
     d.rtang = g->rtang; d.hs_w = g->wir ? g->hs_w : nullptr; d.gradhs_w = g->gradhs_w; d.unkno = g->unkno;
-    d.fnode = g->fnode; d.gp = g->gp; d.rhs1 = g->rhs1; d.rhs0[0] = g->rhs0a; d.rhs0[1] = g->rhs0b;
+    d.fnode = g->fnode; d.gt = g->gt; d.rhs1 = g->rhs1; d.rhs0[0] = g->rhs0a; d.rhs0[1] = g->rhs0b;
     return d;
 }
 
@@ -642,7 +651,7 @@ int gfsph_gfl_create(const gfsph_gfl_params* p, int npoin, int nelem, const floa
     st |= dal(&g->side_geom, ns); st |= dal(&g->bnode, np); st |= dal(&g->rtang, nb);
     st |= dal(&g->geome, 7 * ne); st |= dal(&g->d_topel, 9 * ne); st |= dal(&g->d_topol, 9 * np);
     st |= dal(&g->mmatl, np); st |= dal(&g->hs_w, np); st |= dal(&g->gradhs_w, np);
-    st |= dal(&g->unkno, 3 * np); st |= dal(&g->fnode, 9 * np); st |= dal(&g->gp, 9 * ne * (size_t)p->ngaus);
+    st |= dal(&g->unkno, 3 * np); st |= dal(&g->fnode, 9 * np); st |= dal(&g->gt, 9 * ne);
     st |= dal(&g->rhs1, 3 * np); st |= dal(&g->rhs0a, 3 * np); st |= dal(&g->rhs0b, 3 * np);
     if (st || cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&g->ev0) != cudaSuccess || cudaEventCreate(&g->ev1) != cudaSuccess) {
