@@ -497,16 +497,17 @@ def gfl_bench(args, gfsph, workloads, peak, nsteps=100):
     return out
 
 
-def adjoint_bench(gfsph, workloads, torch, nsteps=1000, every=100):
+def adjoint_bench(gfsph, workloads, torch, nsteps=1000, every=100, sle=0):
     """The adjoint of the calibration case (config 5's shape): ~50k particles
-    on a 512^2 DEM at 5 m (fixed smoothing lengths, no erosion, fixed dt),
-    `nsteps` steps recorded with a checkpoint every `every` and swept back
-    (the config runs 5,000 steps; the cost per step does not depend on how
-    many).  Device time from CUDA events on the handle's stream around the
-    plain forward run, the recording run and the backward sweep (which
-    recomputes each step's forward pass from its segment's checkpoint)."""
+    on a 512^2 DEM at 5 m (no erosion, fixed dt; fixed smoothing lengths, or
+    with sle = 1 their update after every step), `nsteps` steps recorded with
+    a checkpoint every `every` and swept back (the config runs 5,000 steps;
+    the cost per step does not depend on how many).  Device time from CUDA
+    events on the handle's stream around the plain forward run, the recording
+    run and the backward sweep (which recomputes each step's forward pass from
+    its segment's checkpoint)."""
     w = workloads.fractal_channel(n_target=50_000, dem_k=9, cell=5.0, erosion=None)
-    p = workloads.make_params(w, gfsph, sle=0, ic_adapt=0)
+    p = workloads.make_params(w, gfsph, sle=sle, ic_adapt=0)
     stream = torch.cuda.Stream()
     sim = gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
     sim.set_stream(stream.cuda_stream)
@@ -536,7 +537,8 @@ def adjoint_bench(gfsph, workloads, torch, nsteps=1000, every=100):
     g, t_bwd = timed(lambda: adj.backward(gx, gv))
     adj.close()
     sim.close()
-    return {"workload": f"{w.n} particles, {w.meta['dem']}, Voellmy, fixed hsml and dt", "steps": nsteps,
+    hs = "hsml updated every step (sle 1)" if sle else "fixed hsml"
+    return {"workload": f"{w.n} particles, {w.meta['dem']}, Voellmy, {hs}, fixed dt", "steps": nsteps,
             "checkpoint_every": every, "forward_ms_per_step": t_fwd, "recording_ms_per_step": t_rec,
             "backward_ms_per_step": t_bwd, "backward_over_forward": t_bwd / t_fwd, "dL_dtanfi": g["tanfi"],
             "dL_dxi": g["xi"],
@@ -795,6 +797,12 @@ def main():
     wir_line = wir_bench(args, gfsph, workloads, torch) if extras else None
     plane_line = plane_bench(args, gfsph, workloads, torch) if extras else None
     adj_line = adjoint_bench(gfsph, workloads, torch) if extras else None
+    adj1_line = None
+    if extras:
+        try:
+            adj1_line = adjoint_bench(gfsph, workloads, torch, nsteps=200, every=20, sle=1)
+        except gfsph.GfsphError as e:  # e.g. a coarse grid level appeared: outside the adjoint's scope
+            adj1_line = {"unavailable": str(e)}
     big_line = coupled_bench(gfsph, workloads, torch) if extras else None
     ens_line = None
     if extras and args.ensemble > 0:
@@ -828,6 +836,8 @@ def main():
             line["cpu_baseline"] = cpu
         if cg_line:
             line["cg"] = cg_line
+        if adj1_line:
+            line["adjoint_sle1"] = adj1_line
         if gfl_line:
             line["gfl"] = gfl_line
         if wir_line:

@@ -5,8 +5,9 @@
 //
 // Scope: frictional basal friction (nfric 5/6) with Voellmy xi >= 0 or the
 // Bingham law (nfric 4), no curvature, erosion or pore pressure, pa_sph 2,
-// fixed hsml (sle 0), fixed dt, all particles regular (no coarse level) and
-// inside the DEM.  The step is differentiated
+// fixed hsml (sle 0) or its update hsml' = 2 sqrt(m/h) after every step
+// (sle 1, h_upgrade SPH_MAIN_2019.f90:2925-2931), fixed dt, all particles
+// regular (no coarse level) and inside the DEM.  The step is differentiated
 // with its neighbour list held fixed (the reference freezes its pair list per
 // step too); branches (reversal filter, h_inf/comp clamps) take the forward's
 // decisions.  With pa_sph 2 the pressure term p/h^2 = g/2 does not depend on
@@ -41,6 +42,35 @@ __device__ __forceinline__ void sph_kernel_hess(int skf, float r, float mh, floa
             float a = 1.f - q / 2.f;
             ca = s * ((7.5f * q) * (a * a));
             cb = s * (-(5.f * ((a * a) * a)));
+        }
+    }
+}
+
+// Derivatives of the kernel with respect to its smoothing length mh at
+// separation r, with W = f(h) g(q), q = r/h, f = C/h^2 in 2-D and
+// grad W = G d (d the separation vector, G = f g'(q) / (h r)):
+// dW/dh = -(2 W + f q g'(q)) / h and dG/dh = -(f / (r h^2)) (q g''(q) + 3 g'(q)),
+// written with g'(q)/q where r -> 0 would divide 0 by 0.
+__device__ __forceinline__ void sph_kernel_dh(int skf, float r, float mh, double& dwdh, double& dgdh) {
+    const double h = mh, q = (double)r / h;
+    dwdh = 0.0; dgdh = 0.0;
+    if (skf == 1) {
+        const double f = 15.0 / (7.0 * 3.14159265358979323846 * h * h);
+        if (q <= 1.0) {
+            const double g = 2.0 / 3.0 - q * q + 0.5 * q * q * q, gp = -2.0 * q + 1.5 * q * q;
+            dwdh = -(f / h) * (2.0 * g + q * gp);
+            dgdh = -(f / (h * h * h)) * (-8.0 + 7.5 * q);
+        } else if (q <= 2.0) {
+            const double u = 2.0 - q, g = u * u * u / 6.0, gp = -0.5 * u * u, gpp = u;
+            dwdh = -(f / h) * (2.0 * g + q * gp);
+            dgdh = -(f / ((double)r * h * h)) * (q * gpp + 3.0 * gp);
+        }
+    } else {  // skf 4, Wendland C2
+        const double f = 7.0 / (4.0 * 3.14159265358979323846 * h * h);
+        if (q <= 2.0) {
+            const double a = 1.0 - 0.5 * q, g = a * a * a * a * (2.0 * q + 1.0), gp = -5.0 * q * a * a * a;
+            dwdh = -(f / h) * (2.0 * g + q * gp);
+            dgdh = -(f / (h * h * h)) * (-20.0 * a * a * a + 7.5 * q * a * a);
         }
     }
 }
@@ -204,15 +234,28 @@ __device__ __forceinline__ void ext_vjp(const Rheo& c, const DemView& dem, float
 // Seeds the step's adjoints in sorted order from the caller-order ones:
 // lx1 = dL/dx', lv2 = dL/dv'' (after XSPH), lh = dL/dh (final depth, last
 // step only); clears the accumulators.
+// With sle 1, lhs_o = dL/d hsml' of the next step (caller order, zero after
+// the last) goes back through h_upgrade, hsml' = 2 sqrt(m/h):
+// d hsml'/dh = -hsml'/(2h), d hsml'/dm = hsml'/(2m).
 __global__ void k_adj_seed(const PState A, int n, const float2* lx_o, const float2* lv_o, const float* gh_o,
-                           float2* lx1, float2* lv2, float* lh, double2* lxacc, double* lm) {
+                           float2* lx1, float2* lv2, float* lh, double2* lxacc, double* lm, const float* lhs_o,
+                           double* lhsacc) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = A.id[s];
         lx1[s] = lx_o[o];
         lv2[s] = lv_o[o];
-        lh[s] = gh_o ? gh_o[o] : 0.f;
+        float lhv = gh_o ? gh_o[o] : 0.f;
+        double lmv = 0.0;
+        if (lhs_o) {
+            const double ls = lhs_o[o], hh = A.rho[s], mm = A.mass[s];
+            const double hs1 = 2.0 * sqrt(mm / hh);
+            lhv += (float)(-ls * hs1 / (2.0 * hh));
+            lmv = ls * hs1 / (2.0 * mm);
+            lhsacc[s] = 0.0;
+        }
+        lh[s] = lhv;
         lxacc[s] = make_double2(0.0, 0.0);
-        lm[s] = 0.0;
+        lm[s] = lmv;
     }
 }
 
@@ -220,14 +263,14 @@ __global__ void k_adj_seed(const PState A, int n, const float2* lx_o, const floa
 // c_kj = 2 m_j W_kj / (h_k + h_j), W at the start-of-step geometry.
 __global__ void __launch_bounds__(128) k_adj_xsph(PState A, Search Q, Rheo c, int n, const float2* velfin,
                                                   const float2* lv2, float2* lvp, float* lh, double* lm,
-                                                  double2* lxacc) {
+                                                  double2* lxacc, double* lhsacc) {
     const float eps = 0.3f;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const float4 me = Q.xhm[k];
         const float2 xk = make_float2(me.x, me.y), vk = velfin[k], lk = lv2[k];
         const float hk = A.rho[k], mk = me.w;
         const int cnt = Q.ncount[k];
-        double s = 0.0, a0 = 0.0, a1 = 0.0, dm = 0.0, dh = 0.0, dx0 = 0.0, dx1 = 0.0;
+        double s = 0.0, a0 = 0.0, a1 = 0.0, dm = 0.0, dh = 0.0, dx0 = 0.0, dx1 = 0.0, dhs = 0.0;
         for (int q = 0; q < cnt; q++) {
             const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride].x;
             const float4 o = Q.xhm[j];
@@ -251,7 +294,13 @@ __global__ void __launch_bounds__(128) k_adj_xsph(PState A, Search Q, Rheo c, in
             const double lw = (2.0 * mj / den) * pk + (2.0 * (double)mk / den) * pj;
             dx0 += lw * d0;
             dx1 += lw * d1;
+            if (lhsacc) {  // W_kj through mh = (hs_k + hs_j)/2
+                double dwdh, dgdh;
+                sph_kernel_dh(c.skf, g.r, g.mh, dwdh, dgdh);
+                dhs += 0.5 * lw * dwdh;
+            }
         }
+        if (lhsacc) lhsacc[k] += eps * dhs;
         lvp[k] = make_float2((float)(lk.x * (1.0 - eps * s) + eps * a0), (float)(lk.y * (1.0 - eps * s) + eps * a1));
         lh[k] += (float)(eps * dh);
         lm[k] += eps * dm;
@@ -340,15 +389,18 @@ __global__ void __launch_bounds__(128) k_adj_rk(PState A, Search Q, const StepSc
 // Adjoint of the summation density h_k = W0 m_k + sum_j m_j W_kj and of the
 // internal force a_k = -sum_j m_j (P_k + P_j) grad W_kj, gathered at k.
 __global__ void __launch_bounds__(128) k_adj_gather(PState A, Search Q, Rheo c, int n, const float2* lin,
-                                                    const float* lh, double* lm, double2* lxacc) {
+                                                    const float* lh, double* lm, double2* lxacc, double* lhsacc) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const float4 me = Q.xhm[k];
         const float2 xk = make_float2(me.x, me.y);
         const float mk = me.w, pk = Q.pterm[k], lhk = lh[k];
         const float2 lak = lin[k];
         const int cnt = Q.ncount[k];
-        double dm = (double)(lhk * sph_kernel_w(c.skf, 0.f, me.z));
+        const float w0 = sph_kernel_w(c.skf, 0.f, me.z);
+        double dm = (double)(lhk * w0);
         double dx0 = 0.0, dx1 = 0.0;
+        // the self term W(0, hs_k) m_k: dW/dh = -2 W/h
+        double dhs = lhsacc ? (double)lhk * (double)mk * (-2.0 * (double)w0 / (double)me.z) : 0.0;
         for (int q = 0; q < cnt; q++) {
             const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride].x;
             const float4 o = Q.xhm[j];
@@ -372,7 +424,14 @@ __global__ void __launch_bounds__(128) k_adj_gather(PState A, Search Q, Rheo c, 
             const double du = dh0 * u0 + dh1 * u1;
             dx0 += cp * ((double)ca * dh0 * du + (double)cb * u0);
             dx1 += cp * ((double)ca * dh1 * du + (double)cb * u1);
+            if (lhsacc) {  // W_kj and grad W_kj through mh = (hs_k + hs_j)/2
+                double dwdh, dgdh;
+                sph_kernel_dh(c.skf, g.r, g.mh, dwdh, dgdh);
+                dhs += 0.5 * dwdh * fd;
+                dhs += 0.5 * cp * dgdh * ((double)g.dx0 * u0 + (double)g.dx1 * u1);
+            }
         }
+        if (lhsacc) lhsacc[k] += dhs;
         lm[k] += dm;
         double2 ax = lxacc[k];
         lxacc[k] = make_double2(ax.x + dx0, ax.y + dx1);
@@ -382,19 +441,20 @@ __global__ void __launch_bounds__(128) k_adj_gather(PState A, Search Q, Rheo c, 
 // The step's input adjoints back to the caller's order; volumes accumulate
 // over the steps.
 __global__ void k_adj_scatter(const PState A, int n, const double2* lxacc, const float2* lv0, const double* lm,
-                              float2* lx_o, float2* lv_o, double* lm_o) {
+                              float2* lx_o, float2* lv_o, double* lm_o, const double* lhsacc, float* lhs_o) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         int o = A.id[s];
         double2 a = lxacc[s];
         lx_o[o] = make_float2((float)a.x, (float)a.y);
         lv_o[o] = lv0[s];
         lm_o[o] += lm[s];
+        if (lhsacc) lhs_o[o] = (float)lhsacc[s];
     }
 }
 
 // Puts a stored state (caller order) back into the step buffers.
 __global__ void k_adj_restore(PState B, int n, const float2* x, const float2* v, const float* rho, const float* mass,
-                              const float* hsml) {
+                              const float* hsml) {  // hsml: the state's own (sle 1) or the run's constant ones
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         B.pos[s] = x[s]; B.vel[s] = v[s]; B.rho[s] = rho[s]; B.mass[s] = mass[s]; B.hsml[s] = hsml[s];
         B.flag[s] = 0; B.id[s] = s; B.pwp[s] = 0.f;

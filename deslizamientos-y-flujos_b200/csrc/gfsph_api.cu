@@ -1801,18 +1801,24 @@ struct gfsph_adjoint {
     float* lh = nullptr;
     double2* lxacc = nullptr;
     double* lms = nullptr;
+    // sle 1: the smoothing lengths of every checkpoint and segment state, and
+    // dL/d hsml handed from a step to the one before it (caller order)
+    bool sle = false;
+    float *ckh = nullptr, *segh = nullptr, *lhs = nullptr;
+    double* lhsacc = nullptr;
 };
 
 namespace {
 
 // The state of the handle (caller order) into x, v (and the constant fields).
-int adj_capture(gfsph_adjoint* a, float2* x, float2* v, bool fields) {
+int adj_capture(gfsph_adjoint* a, float2* x, float2* v, bool fields, float* hs = nullptr) {
     gfsph_handle* h = a->h;
     cudaStream_t st = h->stream;
     const int n = h->n;
     launch(h, K_ADJOINT, [&] { k_unsort<<<blocks_for(n), kThreads, 0, st>>>(h->B, n, h->U); });
     CK(cudaMemcpyAsync(x, h->U.pos, (size_t)n * sizeof(float2), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(v, h->U.vel, (size_t)n * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    if (hs) CK(cudaMemcpyAsync(hs, h->U.hsml, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st));
     if (fields) {
         CK(cudaMemcpyAsync(a->rho0, h->U.rho, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(a->mass0, h->U.mass, (size_t)n * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -1821,12 +1827,13 @@ int adj_capture(gfsph_adjoint* a, float2* x, float2* v, bool fields) {
     return 0;
 }
 
-int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v, const float* rho = nullptr) {
+int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v, const float* rho = nullptr,
+                const float* hs = nullptr) {
     gfsph_handle* h = a->h;
     if (h->n != a->n) return GFSPH_ERR_STATE;  // the handle's buffers were dropped or resized
     launch(h, K_ADJOINT, [&] {
         k_adj_restore<<<blocks_for(a->n), kThreads, 0, h->stream>>>(h->B, a->n, x, v, rho ? rho : a->rho0, a->mass0,
-                                                                    a->hsml0);
+                                                                    hs ? hs : a->hsml0);
     });
     CK(cudaGetLastError());
     set_field<float>(h, offsetof(StepScalars, dt), a->dt0);
@@ -1855,6 +1862,7 @@ void adj_free(gfsph_adjoint* a) {
     dfree(a->rhoN);
     dfree(a->lx); dfree(a->lv); dfree(a->lm); dfree(a->lpar); dfree(a->gh); dfree(a->lx1); dfree(a->lv2);
     dfree(a->lvp); dfree(a->lin); dfree(a->lv0); dfree(a->lh); dfree(a->lxacc); dfree(a->lms);
+    dfree(a->ckh); dfree(a->segh); dfree(a->lhs); dfree(a->lhsacc);
 }
 
 }  // namespace
@@ -1960,7 +1968,7 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     if (!h->has_state) return GFSPH_ERR_STATE;
     const Rheo& c = h->rheo;
     if (!(c.nfric == 4 || c.nfric == 5 || c.nfric == 6) || (c.nfric != 4 && c.xi < 0.f) || c.erosion ||
-        c.icpwp != 0 || c.pa_sph != 2 || c.sle != 0 ||
+        c.icpwp != 0 || c.pa_sph != 2 ||
         c.ic_adapt != 0 || c.muI != 0 || c.fact_dens != 1.f || c.nor_density || c.cos_theta || c.ws ||
         (c.skf != 1 && c.skf != 4))
         return GFSPH_ERR_UNSUPPORTED;
@@ -1977,17 +1985,22 @@ int gfsph_adjoint_forward(gfsph_handle* h, int nsteps, int every, gfsph_adjoint*
     st |= dalloc(&a->gh, n); st |= dalloc(&a->lx1, n); st |= dalloc(&a->lv2, n); st |= dalloc(&a->lvp, n);
     st |= dalloc(&a->lin, n); st |= dalloc(&a->lv0, n); st |= dalloc(&a->lh, n); st |= dalloc(&a->lxacc, n);
     st |= dalloc(&a->lms, n);
+    a->sle = (c.sle == 1);
+    if (a->sle) {
+        st |= dalloc(&a->ckh, n * a->nck); st |= dalloc(&a->segh, n * a->every);
+        st |= dalloc(&a->lhs, n); st |= dalloc(&a->lhsacc, n);
+    }
     if (st) { adj_free(a); delete a; return GFSPH_ERR_CUDA; }
     st = read_scalars(h);
     if (st) { adj_free(a); delete a; return st; }
     a->t0 = h->hS->time;
     a->dt0 = h->hS->dt;
-    st = adj_capture(a, a->ckx, a->ckv, true);
+    st = adj_capture(a, a->ckx, a->ckv, true, a->sle ? a->ckh : nullptr);
     for (int t = 0, k = 1; !st && t < nsteps; k++) {
         int chunk = std::min(a->every, nsteps - t);
         for (int q = 0; q < chunk && !st; q++) st = adj_one_step(h);
         t += chunk;
-        if (!st) st = adj_capture(a, a->ckx + n * k, a->ckv + n * k, false);
+        if (!st) st = adj_capture(a, a->ckx + n * k, a->ckv + n * k, false, a->sle ? a->ckh + n * k : nullptr);
     }
     if (!st) {  // U holds the final state after the last capture
         std::vector<int> fl;
@@ -2026,33 +2039,37 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
     if (gh) CK(cudaMemcpyAsync(a->gh, gh, un * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(a->lm, 0, un * sizeof(double), st));
     CK(cudaMemsetAsync(a->lpar, 0, kAdjParams * sizeof(double), st));
+    if (a->sle) CK(cudaMemsetAsync(a->lhs, 0, un * sizeof(float), st));  // no step after the last
     const int nseg = a->nck - 1;
     for (int sg = nseg - 1; sg >= 0; sg--) {
         const int t0 = sg * a->every, len = std::min(a->every, a->nsteps - t0);
         // the segment's states: from its checkpoint, recomputed forward
         CK(cudaMemcpyAsync(a->segx, a->ckx + un * sg, un * sizeof(float2), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(a->segv, a->ckv + un * sg, un * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        if (a->sle) CK(cudaMemcpyAsync(a->segh, a->ckh + un * sg, un * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        auto seg_h = [&](int q) -> float* { return a->sle ? a->segh + un * q : nullptr; };
         for (int q = 1; q < len; q++) {
-            int r = adj_restore(a, a->segx + un * (q - 1), a->segv + un * (q - 1));
+            int r = adj_restore(a, a->segx + un * (q - 1), a->segv + un * (q - 1), nullptr, seg_h(q - 1));
             if (!r) r = adj_one_step(h);
-            if (!r) r = adj_capture(a, a->segx + un * q, a->segv + un * q, false);
+            if (!r) r = adj_capture(a, a->segx + un * q, a->segv + un * q, false, seg_h(q));
             if (r) return r;
         }
         for (int q = len - 1; q >= 0; q--) {
             const bool last = (t0 + q == a->nsteps - 1);
-            int r = adj_restore(a, a->segx + un * q, a->segv + un * q);
+            int r = adj_restore(a, a->segx + un * q, a->segv + un * q, nullptr, seg_h(q));
             if (!r) r = adj_one_step(h);  // neighbour table, density, forces of this step
             if (r) return r;
             Search Q = make_search(h);
             const int pb = blocks_for(n);
             launch(h, K_ADJOINT, [&] {
                 k_adj_seed<<<pb, kThreads, 0, st>>>(h->A, n, a->lx, a->lv, (last && gh) ? a->gh : nullptr, a->lx1,
-                                                    a->lv2, a->lh, a->lxacc, a->lms);
+                                                    a->lv2, a->lh, a->lxacc, a->lms, a->sle ? a->lhs : nullptr,
+                                                    a->lhsacc);
             });
             if (h->rheo.av_vel) {
                 launch(h, K_ADJOINT, [&] {
                     k_adj_xsph<<<pb, kThreads, 0, st>>>(h->A, Q, h->rheo, n, h->velfin, a->lv2, a->lvp, a->lh,
-                                                        a->lms, a->lxacc);
+                                                        a->lms, a->lxacc, a->lhsacc);
                 });
             } else {
                 CK(cudaMemcpyAsync(a->lvp, a->lv2, un * sizeof(float2), cudaMemcpyDeviceToDevice, st));
@@ -2062,10 +2079,11 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
                                                   a->lxacc, a->lv0, a->lpar);
             });
             launch(h, K_ADJOINT, [&] {
-                k_adj_gather<<<pb, kThreads, 0, st>>>(h->A, Q, h->rheo, n, a->lin, a->lh, a->lms, a->lxacc);
+                k_adj_gather<<<pb, kThreads, 0, st>>>(h->A, Q, h->rheo, n, a->lin, a->lh, a->lms, a->lxacc, a->lhsacc);
             });
             launch(h, K_ADJOINT, [&] {
-                k_adj_scatter<<<pb, kThreads, 0, st>>>(h->A, n, a->lxacc, a->lv0, a->lms, a->lx, a->lv, a->lm);
+                k_adj_scatter<<<pb, kThreads, 0, st>>>(h->A, n, a->lxacc, a->lv0, a->lms, a->lx, a->lv, a->lm,
+                                                       a->lhsacc, a->lhs);
             });
             CK(cudaGetLastError());
         }
@@ -2082,7 +2100,8 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
     if (gmu) *gmu = a->par[0];
     if (gxi) *gxi = a->par[1];
     // leave the handle at the final state of the recorded run
-    int r = adj_restore(a, a->ckx + un * (a->nck - 1), a->ckv + un * (a->nck - 1), a->rhoN);
+    int r = adj_restore(a, a->ckx + un * (a->nck - 1), a->ckv + un * (a->nck - 1), a->rhoN,
+                        a->sle ? a->ckh + un * (a->nck - 1) : nullptr);
     if (r) return r;
     set_field<double>(h, offsetof(StepScalars, time), a->t0 + (double)a->nsteps * (double)a->dt0);
     CK(cudaStreamSynchronize(st));

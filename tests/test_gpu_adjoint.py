@@ -73,6 +73,48 @@ def test_adjoint_matches_forward_mode_derivatives(gfsph_lib, oracle_mod):
         assert abs(got - ref64) <= 2e-4 * abs(ref64), (name, got, ref64)
 
 
+@pytest.mark.parametrize("every", [1, 7])
+def test_adjoint_with_the_smoothing_length_update(gfsph_lib, oracle_mod, every):
+    """sle 1: every step ends with hsml' = 2 sqrt(m/h) (h_upgrade,
+    SPH_MAIN_2019.f90:2925-2931), so the next step's kernel values depend on
+    the depths and volumes of this one.  The device adjoint against the
+    single-precision trajectory's exact derivative (within 2e-5 of the
+    direction's scale) and the FP64 one (within 2e-4 of it), along tanfi, xi,
+    the volumes and the initial positions and velocities; checkpoints every
+    step or every 7 (the smoothing lengths are part of every stored state)."""
+    w = workloads.fractal_channel(n_target=3000, dem_k=8, cell=5.0, erosion=None)
+    p = workloads.make_params(w, gfsph, sle=1, ic_adapt=0)
+    topol = oracle_mod.initial_topol(w.z, w.dx, w.dy, w.const, deriv=p.dem_deriv, mode=oracle_mod.MODE_FP32)
+    rng = np.random.default_rng(11)
+    gx = rng.normal(size=(w.n, 2)).astype(np.float32)
+    gv = rng.normal(size=(w.n, 2)).astype(np.float32)
+    gh = rng.normal(size=w.n).astype(np.float32)
+    g, final, _ = gpu_gradients(w, p, topol, gx, gv, gh, every=every)
+    assert np.abs(final["hsml"] - w.hsml).max() > 1e-3  # the smoothing lengths did change
+    ny, nx = w.z.shape
+    st0 = oracle_mod.State(w.x, w.v, w.rho, w.mass, w.hsml, topol, dt=p.dt)
+
+    def directional(single, **seed):
+        _, _, _, dx, dv, dh = oracle_mod.tangent(p, nx, ny, w.dx, w.dy, st0, NSTEPS, single=single, **seed)
+        return float((gx * dx).sum() + (gv * dv).sum() + (gh * dh).sum())
+
+    dm = rng.normal(size=w.n) * w.mass
+    dx0 = rng.normal(size=(w.n, 2))
+    dv0 = rng.normal(size=(w.n, 2))
+    for name, seed, got, scale in (
+            ("tanfi", dict(seed_mu=1.0), g["tanfi"], abs(g["tanfi"])),
+            ("xi", dict(seed_xi=1.0), g["xi"], abs(g["xi"])),
+            ("mass", dict(seed_m=dm), float((g["mass"] * dm).sum()), float(np.abs(g["mass"] * dm).sum())),
+            ("x0", dict(seed_x=dx0), float((g["x0"] * dx0).sum()), float(np.abs(g["x0"] * dx0).sum())),
+            ("v0", dict(seed_v=dv0), float((g["v0"] * dv0).sum()), float(np.abs(g["v0"] * dv0).sum()))):
+        ref32 = directional(True, **seed)
+        ref64 = directional(False, **seed)
+        print(f"sle 1, {name}: device {got:.9g} single-trajectory {ref32:.9g} FP64 {ref64:.9g} "
+              f"|dev-32|/scale {abs(got - ref32) / scale:.2e}")
+        assert abs(got - ref32) <= 2e-5 * scale, (name, got, ref32, scale)
+        assert abs(got - ref64) <= 2e-4 * scale, (name, got, ref64, scale)
+
+
 def test_checkpoint_interval_does_not_change_the_gradient(gfsph_lib, oracle_mod):
     w, p, topol = case(oracle_mod, n=1500)
     rng = np.random.default_rng(2)
