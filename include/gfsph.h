@@ -290,9 +290,10 @@ int gfsph_autotune(gfsph_handle* h, int steps, float* level_factor, float* cell_
  * as the forward step freezes it) and leaves the handle at the final state.
  *
  * Supported: nfric 5/6 with xi >= 0 and the Bingham law nfric 4, no erosion
- * or pore pressure, pa_sph 2, sle 0, ic_adapt 0, one grid level (uniform
- * smoothing lengths) and no particle leaving the DEM (GFSPH_ERR_UNSUPPORTED
- * otherwise).
+ * or pore pressure, pa_sph 2, sle 0 or 1 (with sle 1 the smoothing lengths of
+ * every step are differentiated through h_upgrade and every pair's kernel),
+ * ic_adapt 0, one grid level and no particle leaving the DEM
+ * (GFSPH_ERR_UNSUPPORTED otherwise), one material (ws_interact 0).
  *
  * The record refers to its handle: call gfsph_adjoint_backward only while
  * that handle exists (gfsph_adjoint_destroy does not touch it, so the record
