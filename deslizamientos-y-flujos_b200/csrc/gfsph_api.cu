@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
@@ -185,6 +186,7 @@ struct gfsph_handle {
     float2* bxy = nullptr;
     float* wir_hsz = nullptr;
     double2* wir_acc = nullptr;
+    float* mass0_u = nullptr;  // mass per caller index at upload (nfric 3's m0)
     // cells
     int* count = nullptr;
     int* start = nullptr;
@@ -327,6 +329,7 @@ Search make_search(gfsph_handle* h) {
     q.zpw = h->zpw;
     q.gzw = h->gzw;
     q.bxy = h->bxy;
+    q.mass0 = h->mass0_u;
     q.kcap = h->kcap;
     return q;
 }
@@ -681,6 +684,7 @@ void free_particles(gfsph_handle* h) {
     dfree(h->carry.v); dfree(h->carry.acc); dfree(h->carry.dx); dfree(h->carry.dv); dfree(h->carry.xo);
     dfree(h->carry.out); dfree(h->rhoS); dfree(h->rcell); dfree(h->xsv); dfree(h->pr);
     dfree(h->spec_u); dfree(h->spec_a); dfree(h->zpw); dfree(h->gzw); dfree(h->bxy);
+    dfree(h->mass0_u);
     h->kcap = 0;
 }
 
@@ -785,11 +789,40 @@ void pwp_factors(const gfsph_params* p, Rheo& c) {
     c.alphas2 = k[13] * k[13];
 }
 
+// Which quadratic nfric 23 solves for m = const(8) (SPH_SW_2019.f90:9578-9598):
+// 0 for m = 1, 1 for m = 2, 2 for m within 1e-3 of 1/3 or m = 1/2, -1 for
+// any other m (the reference stops there).
+int hb_case(float m) {
+    if (m == 1.f) return 0;
+    if (m == 2.f) return 1;
+    if (std::fabs(m - 0.333333f) <= 1.e-3f || m == 0.5f) return 2;
+    return -1;
+}
+
+// The per-run constants of the Herschel-Bulkley laws, in the FP32 operations
+// of SPH_SW_2019.f90:9541-9545 and :9609-9612 (real powers in FP64, rounded
+// once).
+void hb_constants(const float* k, Rheo& c) {
+    const float m = k[7];
+    c.m_vexp = m;
+    c.hb_m = hb_case(m);
+    const float cm = m / ((m + 1.f) * (2.f * m + 1.f));
+    c.hb_a0 = (1.f / cm) * (float)std::pow((double)(k[6] / k[5]), (double)(1.f / m));
+    c.hb_cm = 1.f;
+    if (c.nfric == 25) c.hb_cm = (float)std::pow((double)((2.f * m + 1.f) / m), (double)m);
+}
+
 int validate(const gfsph_params* p) {
     int nfric = (int)(p->cst[4] + 0.01f);
     bool erosion = p->cst[20] > 1.e-9f;
-    if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
-    if (nfric == 4 && !(p->cst[5] >= 1.e-32f)) return GFSPH_ERR_ARG;  // SPH_SW_2019.f90:9547-9550
+    if (!(nfric == 1 || nfric == 2 || nfric == 3 || nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 11 ||
+          (nfric >= 23 && nfric <= 27)))
+        return GFSPH_ERR_UNSUPPORTED;
+    // Bingham and Herschel-Bulkley need a yield stress above 1e-32 (SPH_SW_2019.f90:9547-9550)
+    if ((nfric == 4 || (nfric >= 23 && nfric <= 25)) && !(p->cst[5] >= 1.e-32f)) return GFSPH_ERR_ARG;
+    if (nfric == 23 && hb_case(p->cst[7]) < 0) return GFSPH_ERR_UNSUPPORTED;
+    // nfric 24/25 with m <= 0: (v/h)**m is infinite for a particle at rest
+    if ((nfric == 24 || nfric == 25) && !(p->cst[7] > 0.f)) return GFSPH_ERR_ARG;
     if (erosion && (int)(p->cst[20] + 0.1f) != 1) return GFSPH_ERR_UNSUPPORTED;
     if (p->skf < 1 || p->skf > 4) return GFSPH_ERR_UNSUPPORTED;
     // skf 2, 3 (support 3 h): the pair set depends on the reference's own
@@ -822,6 +855,12 @@ int validate(const gfsph_params* p) {
     // terrain-normal gravity with them here
     if (p->ws_interact == 1 && (erosion || p->icpwp != 0 || p->nor_density != 0 || cos_theta != 0))
         return GFSPH_ERR_UNSUPPORTED;
+    // soil-water interface erosion (const(50) > 0) and friction (const(55) > 0), Input_SW
+    // SPH_SW_2019.f90:1328-1345: not built
+    if (p->ws_interact == 1 && (p->cst[49] > 0.f || p->cst[54] > 0.f)) return GFSPH_ERR_UNSUPPORTED;
+    // grain crushing (const(36) > 0.01, :1312-1317), the solid-end laws (const(43) > 0, :1319-1325)
+    // and the late Voellmy xi const(41) of ExtForces_SW (:8424-8434): not built
+    if (p->cst[35] > 0.01f || p->cst[42] > 0.f || p->cst[40] > 1.e-6f) return GFSPH_ERR_UNSUPPORTED;
     return 0;
 }
 
@@ -941,6 +980,7 @@ int create_handle(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle* sha
     c.muI = (c.nfric == 8 || c.nfric == 26) ? 1 : (c.nfric == 27 ? 2 : 0);
     c.mu_a = k[2]; c.mu_r = k[5]; c.mu_b = k[6];
     if (c.muI) c.xi = 0.f;  // const(3) is a mu(I) parameter, not xi (:9653)
+    hb_constants(k, c);
     c.ws = p->ws_interact;
     c.swalg = p->sw_alg;
     {
@@ -1100,6 +1140,9 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
             // water particles only with ic_ws_Interact = 1; no other types
             if (itype[i] != 2 || !h->rheo.ws) return GFSPH_ERR_UNSUPPORTED;
         }
+    if (h->rheo.nfric == 3)  // nsoilB = (m - m0)/m; the reference stops for m <= 1e-6 (SPH_SW_2019.f90:9450-9453)
+        for (int i = 0; i < n; i++)
+            if (!(mass[i] > 1.e-6f)) return GFSPH_ERR_ARG;
     if (n != h->n) {
         CK(cudaStreamSynchronize(h->stream));
         drop_graphs(h);
@@ -1123,6 +1166,7 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
             st |= dalloc(&h->spec_u, n); st |= dalloc(&h->spec_a, n); st |= dalloc(&h->zpw, n);
             st |= dalloc(&h->gzw, n); st |= dalloc(&h->bxy, n);
         }
+        if (h->rheo.nfric == 3) st |= dalloc(&h->mass0_u, n);
         if (st) return drop_state(h, GFSPH_ERR_CUDA);
         st = alloc_nbr(h, h->P.max_neighbours > 0 ? h->P.max_neighbours : 96);
         if (st) return drop_state(h, st);
@@ -1141,6 +1185,8 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
     CK(cudaMemcpyAsync(h->B.vel, v, (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->B.rho, rho, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->B.mass, mass, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
+    // mass0 = mass at the start of the run (Input_SW SPH_SW_2019.f90:1995)
+    if (h->rheo.nfric == 3) CK(cudaMemcpyAsync(h->mass0_u, mass, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(h->B.hsml, hsml, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
     if (out_flag) CK(cudaMemcpyAsync(h->B.flag, out_flag, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
     else CK(cudaMemsetAsync(h->B.flag, 0, (size_t)n * sizeof(int), st));

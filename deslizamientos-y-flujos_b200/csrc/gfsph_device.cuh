@@ -225,6 +225,12 @@ struct Rheo {
     // Mu2, r, I0 = const(3), (6), (7)), basal_friction_Ext_SW :9651-9668
     int muI;
     float mu_a, mu_r, mu_b;
+    // Herschel-Bulkley laws (nfric 23-25, :9538-9618) with m = const(8):
+    // hb_m selects nfric 23's quadratic (0: m = 1, 1: m = 2, 2: m ~ 1/3 or
+    // 1/2); hb_a0 = (1/Cm) (K/tauy0)**(1/m); hb_cm = nfric 25's
+    // ((2m+1)/m)**m (1 for nfric 24)
+    int hb_m;
+    float m_vexp, hb_a0, hb_cm;  // m_vexp = const(8) is also nfric 3's Manning n
     // soil and water particles (ic_ws_Interact = 1, ic_SWalg sw_alg): pairs of
     // one material only in the density, forces and av_vel; the soil-water
     // pairs push the soil by -dens_ws g m_j grad W (SPH_SW_2019.f90:8502-8521,
@@ -270,7 +276,7 @@ __device__ __forceinline__ float terrain_deng(float zpx, float zpy) { return sqr
 // number :9658-9665) is g/deng; the Voellmy term keeps cgra = g (:9749).
 template <bool COS = false>
 __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& d, float xx, float yy, float vx,
-                                                  float vy, float pwp, ExtLocal& L) {
+                                                  float vy, float pwp, float nsoil, ExtLocal& L) {
     const bool frictional = (c.nfric >= 5 && c.nfric <= 8) || c.nfric == 26 || c.nfric == 27;
     const bool v2byr = (c.nfric == 7 || c.nfric == 8 || c.nfric == 26 || c.nfric == 27);
     float zpx, zpy, top[6];
@@ -305,6 +311,77 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
             L.frictx = (cf4b * L.hu) * L.hvmodinv;
             L.fricty = (cf4b * L.hv) * L.hvmodinv;
         }
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+    } else if (c.nfric == 3) {  // Bingham of the eroded soil fraction nsoil, :9443-9489
+        const float fsoil = 1.f - (float)exp((double)(-(c.xi * nsoil)));  // C3 = const(3)
+        const float constKB = c.constK * fsoil, tauy0B = c.tauy0 * fsoil;
+        const float densB = 1000.f + (c.dens - 1000.f) * nsoil;
+        if (nsoil > 0.01f) {
+            const float a_hat = ((6.f * constKB) * L.hvmod) / (tauy0B * (hfrict * hfrict));
+            if (a_hat > 50.f) {
+                const float cf4b = (3.f * constKB) / densB;
+                L.frictx = (cf4b * L.hu) / (hfrict * hfrict);
+                L.fricty = (cf4b * L.hv) / (hfrict * hfrict);
+            } else if (a_hat < 0.01f) {
+                const float cf4b = tauy0B / densB;
+                L.frictx = (cf4b * L.hu) * L.hvmodinv;
+                L.fricty = (cf4b * L.hv) * L.hvmodinv;
+            } else {
+                const float a2 = 48.f, b2 = -(32.f * a_hat) - 114.f, c2 = 65.f;
+                const float xh = (-b2 - sqrtf(b2 * b2 - (4.f * a2) * c2)) / (2.f * a2);
+                const float cf4b = (tauy0B / xh) / densB;
+                L.frictx = (cf4b * L.hu) * L.hvmodinv;
+                L.fricty = (cf4b * L.hv) * L.hvmodinv;
+            }
+        }
+        // the Manning friction (n = const(8)) where it is larger, per component
+        const float cf1 = (c.g * c.m_vexp) * c.m_vexp;
+        const float p73 = powr(hfrict, 7.f / 3.f);
+        const float fxx = ((cf1 * L.hu) * L.hvmod) / p73, fyy = ((cf1 * L.hv) * L.hvmod) / p73;
+        if (fabsf(fxx) > fabsf(L.frictx)) L.frictx = fxx;
+        if (fabsf(fyy) > fabsf(L.fricty)) L.fricty = fyy;
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+    } else if (c.nfric == 1) {  // Newtonian turbulent (Manning n = const(3)), :9426-9430
+        const float cf1 = (c.g * c.xi) * c.xi;
+        const float p73 = powr(hfrict, 7.f / 3.f);
+        L.frictx = ((cf1 * L.hu) * L.hvmod) / p73;
+        L.fricty = ((cf1 * L.hv) * L.hvmod) / p73;
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+    } else if (c.nfric == 2) {  // Newtonian laminar, :9431-9437
+        const float cf2a = c.constK / (8.f * c.dens);
+        L.frictx = (cf2a * L.hu) / (hfrict * hfrict);
+        L.fricty = (cf2a * L.hv) / (hfrict * hfrict);
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+    } else if (c.nfric == 11) {  // Bagnold, K = const(3), :9791-9796
+        const float vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
+        L.frictx = ((c.xi * vxx) * L.vmod) / (hfrict * hfrict);
+        L.fricty = ((c.xi * vyy) * L.vmod) / (hfrict * hfrict);
+        L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+    } else if (c.nfric >= 23 && c.nfric <= 25) {  // Herschel-Bulkley, :9538-9618
+        float tau0;
+        if (c.nfric == 23) {  // exact solution, :9576-9603
+            float a_hat, a2 = 48.f, b2, c2 = 65.f;
+            if (c.hb_m == 2) {
+                a_hat = ((4.5f * c.constK) * L.hvmod) / (c.tauy0 * (hfrict * hfrict));
+            } else {
+                a_hat = c.hb_a0 * (L.hvmod / (hfrict * hfrict));
+            }
+            if (c.hb_m == 1) {
+                a2 = 10.f;
+                b2 = -a_hat - 19.2188f;
+                c2 = 9.1875f;
+            } else {
+                b2 = -(32.f * a_hat) - 114.f;
+            }
+            const float xh = (-b2 - sqrtf(b2 * b2 - (4.f * a2) * c2)) / (2.f * a2);
+            tau0 = c.tauy0 / xh;
+        } else {  // approximations, :9606-9613
+            tau0 = c.constK * powr(L.vmod / hfrict, c.m_vexp);
+            tau0 = c.tauy0 + tau0 * c.hb_cm;
+        }
+        const float cf4b = tau0 / c.dens;
+        L.frictx = (cf4b * L.hu) * L.hvmodinv;
+        L.fricty = (cf4b * L.hv) * L.hvmodinv;
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
     } else if (frictional) {  // :9660-9750
         float cv2byr = 0.f;
@@ -401,11 +478,11 @@ __device__ __forceinline__ void reversal_filter(const Rheo& c, float dt, float v
 // reversal filter, Hungr erosion momentum :8664-8697).
 template <bool COS = false>
 __device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float dt, float xx, float yy, float vx,
-                                          float vy, float hdepth, float pwp, float in0, float in1, float& ex0,
-                                          float& ex1) {
+                                          float vy, float hdepth, float pwp, float nsoil, float in0, float in1,
+                                          float& ex0, float& ex1) {
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
-    grav_and_friction<COS>(c, d, xx, yy, vx, vy, pwp, L);
+    grav_and_friction<COS>(c, d, xx, yy, vx, vy, pwp, nsoil, L);
     ex0 = 0.f + L.gravx;
     ex1 = 0.f + L.gravy;
     reversal_filter(c, dt, vx, vy, ex0 + in0, ex1 + in1, L);
@@ -450,7 +527,7 @@ __device__ __forceinline__ void ext_accel_wir(const Rheo& c, const DemView& d, f
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
         L.cf5 = 0.f;
     } else {
-        grav_and_friction<false>(c, d, xx, yy, vx, vy, 0.f, L);
+        grav_and_friction<false>(c, d, xx, yy, vx, vy, 0.f, 0.f, L);
     }
     if (water && c.swalg == 1) {
         const float hhsz = hdepth + zp;
@@ -468,10 +545,10 @@ __device__ __forceinline__ void ext_accel_wir(const Rheo& c, const DemView& d, f
 // Hungr erosion rate after the RK update (ExtForces_SW(1), :8717-8760):
 // E = C22 * h * vmod with the ExtForces locals after basal friction.
 __device__ __forceinline__ float erosion_rate_final(const Rheo& c, const DemView& d, float xx, float yy, float vx,
-                                                    float vy, float hdepth, float pwp) {
+                                                    float vy, float hdepth, float pwp, float nsoil) {
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
-    grav_and_friction(c, d, xx, yy, vx, vy, pwp, L);
+    grav_and_friction(c, d, xx, yy, vx, vy, pwp, nsoil, L);
     return (c.keros * L.h) * L.vmod;
 }
 

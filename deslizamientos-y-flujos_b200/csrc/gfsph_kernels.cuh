@@ -122,8 +122,17 @@ struct Search {
     float* zpw;
     float2* gzw;
     float2* bxy;
+    const float* mass0;  // caller index -> mass at upload (nfric 3), else null
     int kcap;
 };
+
+// nsoilB = (m - m0)/m of basal_friction_Ext_SW (SPH_SW_2019.f90:9449-9451),
+// the share of a particle's mass gained by erosion; 0 unless nfric = 3.
+__device__ __forceinline__ float soil_fraction(const Rheo& c, const Search& Q, const PState& A, int i) {
+    if (c.nfric != 3) return 0.f;
+    const float m = A.mass[i];
+    return (m - Q.mass0[A.id[i]]) / m;
+}
 constexpr int kCrossBit = (int)0x80000000;
 
 __device__ __forceinline__ bool step_skipped(const StepScalars* S) { return S->skip != 0; }
@@ -1219,7 +1228,7 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
         out = out_of_box(dem, xx, xy);
     }
     float er = 0.f;
-    if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h, pwp);
+    if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h, pwp, soil_fraction(c, Q, A, i));
     if (c.erosion) erosion_scatter(dem, xx, xy, dt * er, !out, auxv, box);
     if (!out) {
         if (c.erosion) m = m + ((dt * er) * m) / h;
@@ -1304,6 +1313,7 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
         const float hc = (h < c.h_inf) ? c.h_inf : h;  // IntForces_SW clamp, seen by ExtForces_SW(0)
         const float2 x0 = A.pos[i], v0 = A.vel[i];
         const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
+        const float nsoil = soil_fraction(c, Q, A, i);
         float xx = x0.x, xy = x0.y, vx = v0.x, vy = v0.y;
         float ex0 = 0.f, ex1 = 0.f;
         float Dx0 = 0.f, Dx1 = 0.f, Dv0 = 0.f, Dv1 = 0.f;
@@ -1322,7 +1332,7 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
                 if (out_of_box(dem, xx, xy)) {
                     out = true;
                 } else {
-                    ext_accel(c, dem, dt, xx, xy, vx, vy, hc, pwp, in0, in1, ex0, ex1);
+                    ext_accel(c, dem, dt, xx, xy, vx, vy, hc, pwp, nsoil, in0, in1, ex0, ex1);
                     Dv0 = Dv0 + f2 * (ex0 + in0);
                     Dv1 = Dv1 + f2 * (ex1 + in1);
                     Dx0 = Dx0 + f2 * vx;
@@ -1647,7 +1657,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
             ext_accel_wir(c, dem, dt, xx, xy, vx, vy, hc, fin.x, fin.y, Q.spec[i] == 2, Q.zpw[i], Q.gzw[i], Q.bxy[i],
                           ex0, ex1);
         else
-            ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
+            ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, soil_fraction(c, Q, A, i), fin.x, fin.y, ex0, ex1);
         const float a0 = ex0 + fin.x, a1 = ex1 + fin.y;
         dv.x = dv.x + f2 * a0;
         dv.y = dv.y + f2 * a1;
@@ -1719,7 +1729,8 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
                     ext_accel_wir(c, dem, dt, xx, xy, vx, vy, hc, fin.x, fin.y, Q.spec[i] == 2, Q.zpw[i], Q.gzw[i],
                                   Q.bxy[i], ex0, ex1);
                 else
-                    ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, fin.x, fin.y, ex0, ex1);
+                    ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, soil_fraction(c, Q, A, i), fin.x, fin.y,
+                                   ex0, ex1);
                 dv.x = dv.x + 1.f * (ex0 + fin.x);
                 dv.y = dv.y + 1.f * (ex1 + fin.y);
                 dx.x = dx.x + 1.f * vx;

@@ -358,7 +358,7 @@ def write_reference_inputs(w, directory, name, out_step=100, restart=False, wate
         for b in range(blocks):
             f.write("constants %d-%d\n  " % (15 * b + 1, 15 * b + 15) + " ".join("%.9g" % v for v in c[15 * b:15 * b + 15]) + "\n")
         nfric = int(c[4] + 0.01)
-        if 5 <= nfric <= 10:
+        if 5 <= nfric <= 10 or nfric in (26, 27):  # if_frictional, SPH_SW_2019.f90:1252-1253, 1374
             f.write("K0 activated?\n  0\n")
         icpwp = int(o.get("icpwp", 0))
         f.write("icpwp\n  %d\n" % icpwp)

@@ -55,8 +55,9 @@ extern "C" {
 /*
  * Control parameters.  cst[k-1] holds the reference's const(k)
  * (read in blocks of 15 by Input_SW, SPH_SW_2019.f90:1151-1204).  The ones the
- * step uses: const(1) g, const(2) density, const(3) Voellmy xi (or Manning),
- * const(5) nfric, const(6) Bingham yield stress, const(7) Bingham viscosity,
+ * step uses: const(1) g, const(2) density, const(3) Voellmy xi (or Manning n,
+ * or Bagnold K), const(5) nfric, const(6) yield stress, const(7) viscosity K,
+ * const(8) Herschel-Bulkley exponent m,
  * const(9) tan(phi), const(10) hfrict0, const(15) comp, const(16) ic_cosTheta
  * (0 g, 1 g/sqrt(1+|grad Z|^2) in the pressure and the friction, IntForces_SW
  * SPH_SW_2019.f90:6775-6783, Get_Grav_Ext_SW :9264-9270), const(20)
@@ -122,7 +123,15 @@ typedef struct gfsph_handle gfsph_handle;
 #define GFSPH_RASTER_AVAILABLE 8  /* remaining erodible depth topol(15,:) */
 
 /* Replaces Init_sph's SPH setup (SPH_MAIN_2019.f90:74) for the step: validates
- * the options, copies the DEM to the device, derives slopes if needed. */
+ * the options, copies the DEM to the device, derives slopes if needed.
+ * Basal laws (basal_friction_Ext_SW, SPH_SW_2019.f90:9355-9828): nfric 1
+ * Manning, 2 laminar, 3 Bingham scaled by the eroded soil fraction (m - m0)/m
+ * with m0 the mass at gfsph_upload (masses <= 1e-6 refused there with
+ * GFSPH_ERR_ARG), 4 Bingham, 5/6 frictional with Voellmy (xi > 0) or
+ * Coulomb-viscous (xi < 0), 7 with v^2/R, 8/26/27 mu(I), 11 Bagnold, 23
+ * Herschel-Bulkley (m = 1, 2, 1/3 or 1/2) and 24/25 its approximations
+ * (m > 0); yield stress const(6) >= 1e-32 for 4 and 23-25 (else
+ * GFSPH_ERR_ARG); other laws GFSPH_ERR_UNSUPPORTED. */
 int gfsph_create(const gfsph_params* params, const gfsph_dem* dem, gfsph_handle** out);
 
 /* Frees all device memory of the handle. */

@@ -277,6 +277,7 @@ struct Oracle {
     /* particles */
     int n;
     std::vector<R> x, v, rho, mass, hsml, x0, v0, p;
+    std::vector<R> mass0; /* mass at the start of the run (Input_SW SPH_SW_2019.f90:1995), nfric 3 */
     /* mode 3 (a precision experiment, not the reference): the RK45 position
      * updates carried in FP64 (xd), everything else as in mode 1; x holds
      * the single-precision positions that every other term reads */
@@ -784,7 +785,7 @@ struct Oracle {
         R hfrict = rmax<R>(L.h, cst[10]);
         L.frictx = 0; L.fricty = 0; L.totfrict = 0; L.cf5 = 0;
         R dens = cst[2];
-        if (nfric == 1) { /* Manning, :9426-9430 (the water of ic_ws_Interact 1) */
+        if (nfric == 1) { /* Manning, :9426-9430 (also the water of ic_ws_Interact 1) */
             R cmanning = cst[3];
             R cf1 = (cgra * cmanning) * cmanning;
             R p73 = (R)std::pow((double)hfrict, (double)lit<R>(7.0 / 3.0));
@@ -810,6 +811,77 @@ struct Oracle {
                 L.frictx = (cf4b * L.hu) * L.hvmodinv;
                 L.fricty = (cf4b * L.hv) * L.hvmodinv;
             }
+            L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+        } else if (nfric == 3) { /* Bingham of the eroded soil fraction, :9443-9489 */
+            /* nsoilB = (m - m0)/m, the share of the mass gained by erosion
+               (setup refuses masses <= 1e-6, where the reference stops) */
+            R nsoil = (mass[i] - mass0[i]) / mass[i];
+            R fsoil = (R)1 - rexp(-(cst[3] * nsoil));
+            R constKB = cst[7] * fsoil, tauy0B = cst[6] * fsoil;
+            R densB = (R)1000 + (dens - (R)1000) * nsoil;
+            if (nsoil > lit<R>(0.01)) {
+                R a_hat = (((R)6 * constKB) * L.hvmod) / (tauy0B * (hfrict * hfrict));
+                if (a_hat > (R)50) {
+                    R cf4b = ((R)3 * constKB) / densB;
+                    L.frictx = (cf4b * L.hu) / (hfrict * hfrict);
+                    L.fricty = (cf4b * L.hv) / (hfrict * hfrict);
+                } else if (a_hat < lit<R>(0.01)) {
+                    R cf4b = tauy0B / densB;
+                    L.frictx = (cf4b * L.hu) * L.hvmodinv;
+                    L.fricty = (cf4b * L.hv) * L.hvmodinv;
+                } else {
+                    R a2 = (R)48, b2 = -((R)32 * a_hat) - (R)114, c2 = (R)65;
+                    R xh = (-b2 - std::sqrt(b2 * b2 - ((R)4 * a2) * c2)) / ((R)2 * a2);
+                    R cf4b = (tauy0B / xh) / densB;
+                    L.frictx = (cf4b * L.hu) * L.hvmodinv;
+                    L.fricty = (cf4b * L.hv) * L.hvmodinv;
+                }
+            }
+            /* the Manning friction with n = const(8) where it is larger, per component */
+            R cf1 = (cgra * cst[8]) * cst[8];
+            R p73 = (R)std::pow((double)hfrict, (double)lit<R>(7.0 / 3.0));
+            R fxx = ((cf1 * L.hu) * L.hvmod) / p73;
+            R fyy = ((cf1 * L.hv) * L.hvmod) / p73;
+            if (std::fabs(fxx) > std::fabs(L.frictx)) L.frictx = fxx;
+            if (std::fabs(fyy) > std::fabs(L.fricty)) L.fricty = fyy;
+            L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+        } else if (nfric == 2) { /* Newtonian laminar, :9431-9437; hfrict**2. = hfrict*hfrict */
+            R cf2a = cst[7] / ((R)8 * dens);
+            L.frictx = (cf2a * L.hu) / (hfrict * hfrict);
+            L.fricty = (cf2a * L.hv) / (hfrict * hfrict);
+            L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+        } else if (nfric == 11) { /* Bagnold with K_Bagnold = const(3), :9791-9796 */
+            R vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
+            L.frictx = ((cst[3] * vxx) * L.vmod) / (hfrict * hfrict);
+            L.fricty = ((cst[3] * vyy) * L.vmod) / (hfrict * hfrict);
+            L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+        } else if (nfric >= 23 && nfric <= 25) { /* Herschel-Bulkley, :9538-9618 */
+            R tauy0 = cst[6], constK = cst[7], m = cst[8];
+            R tau0;
+            if (nfric == 23) { /* :9541-9545 then :9576-9603 */
+                R cm = m / ((m + (R)1) * ((R)2 * m + (R)1));
+                R a_hat = ((R)1 / cm) * (R)std::pow((double)(constK / tauy0), (double)((R)1 / m));
+                a_hat = a_hat * (L.hvmod / (hfrict * hfrict));
+                R a2, b2, c2;
+                if (m == (R)1) {
+                    a2 = (R)48; b2 = -((R)32 * a_hat) - (R)114; c2 = (R)65;
+                } else if (m == (R)2) {
+                    a2 = (R)10; b2 = -a_hat - lit<R>(19.2188); c2 = lit<R>(9.1875);
+                } else { /* m ~ 1/3 or m = 1/2 (setup refuses any other m) */
+                    a_hat = ((lit<R>(4.5) * constK) * L.hvmod) / (tauy0 * (hfrict * hfrict));
+                    a2 = (R)48; b2 = -((R)32 * a_hat) - (R)114; c2 = (R)65;
+                }
+                R xh = (-b2 - std::sqrt(b2 * b2 - ((R)4 * a2) * c2)) / ((R)2 * a2);
+                tau0 = tauy0 / xh;
+            } else { /* :9606-9613, constMu_CF = const(7) */
+                tau0 = constK * (R)std::pow((double)(L.vmod / hfrict), (double)m);
+                R cmf = (R)1;
+                if (nfric == 25) cmf = (R)std::pow((double)(((R)2 * m + (R)1) / m), (double)m);
+                tau0 = tauy0 + tau0 * cmf;
+            }
+            R cf4b = tau0 / dens; /* :9615-9618 */
+            L.frictx = (cf4b * L.hu) * L.hvmodinv;
+            L.fricty = (cf4b * L.hv) * L.hvmodinv;
             L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
         } else if (frictional) { /* :9660-9750 */
             R cv2byr = 0;
@@ -1183,7 +1255,18 @@ struct Oracle {
         ic_costheta = (int)(cst[16] + lit<R>(0.01)); /* SPH_SW_2019.f90:6734 */
         if (ic_costheta != 0 && ic_costheta != 1) return GFSPH_ERR_UNSUPPORTED;
         ic_erosion = (cst[21] > lit<R>(1.e-9)) ? 1 : 0;
-        if (!(nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
+        if (!(nfric == 1 || nfric == 2 || nfric == 3 || nfric == 4 || (nfric >= 5 && nfric <= 8) || nfric == 11 ||
+              (nfric >= 23 && nfric <= 27)))
+            return GFSPH_ERR_UNSUPPORTED;
+        if ((nfric == 4 || (nfric >= 23 && nfric <= 25)) && !(P->cst[5] >= 1.e-32f)) return GFSPH_ERR_ARG; /* :9547 */
+        if (nfric == 23) { /* m = 1, 2, ~1/3 or 1/2, :9578-9598 */
+            float m = P->cst[7];
+            if (!(m == 1.f || m == 2.f || std::fabs(m - 0.333333f) <= 1.e-3f || m == 0.5f)) return GFSPH_ERR_UNSUPPORTED;
+        }
+        if ((nfric == 24 || nfric == 25) && !(P->cst[7] > 0.f)) return GFSPH_ERR_ARG;
+        /* crushing (const(36)), the solid-end laws (const(43)), the late xi const(41) (:1312-1325, 8424-8434) */
+        if (P->cst[35] > 0.01f || P->cst[42] > 0.f || P->cst[40] > 1.e-6f) return GFSPH_ERR_UNSUPPORTED;
+        if (P->ws_interact == 1 && (P->cst[49] > 0.f || P->cst[54] > 0.f)) return GFSPH_ERR_UNSUPPORTED; /* :1328-1345 */
         if (ic_erosion && (int)(cst[21] + lit<R>(0.1)) != 1) return GFSPH_ERR_UNSUPPORTED;
         if (P->skf < 1 || P->skf > 4) return GFSPH_ERR_UNSUPPORTED;
         ws = P->ws_interact;
@@ -1314,6 +1397,10 @@ OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double 
     };
     cp(o.x, x, 2 * (size_t)n); cp(o.v, v, 2 * (size_t)n);
     cp(o.rho, rho, n); cp(o.mass, mass, n); cp(o.hsml, hsml, n);
+    cp(o.mass0, mass, n);
+    if (o.nfric == 3)
+        for (int k = 0; k < n; k++)
+            if (!(o.mass[k] > lit<R>(1.e-6))) { delete ob; *status = GFSPH_ERR_ARG; return nullptr; } /* :9450-9453 */
     o.set_flags(flag);
     o.p.assign(n, (R)0);
     o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
@@ -1326,8 +1413,9 @@ OracleBase* make_obj(const gfsph_params* p, int nx, int ny, double xmin, double 
 
 template <class R, class A>
 int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
-             double* topol, int n, double* x, double* v, double* rho, double* mass, double* hsml, int* flag,
-             double* pwp, int pwp_init, int nsteps, double* dt, double* t, double t_end, int* steps_done) {
+             double* topol, int n, double* x, double* v, double* rho, double* mass, const double* mass0,
+             double* hsml, int* flag, double* pwp, int pwp_init, int nsteps, double* dt, double* t, double t_end,
+             int* steps_done) {
     Oracle<R, A> o;
     int st = o.setup(p, nx, ny, xmin, ymin, dx, dy, topol);
     if (st) return st;
@@ -1338,6 +1426,10 @@ int run_mode(const gfsph_params* p, int nx, int ny, double xmin, double ymin, do
     };
     cp(o.x, x, 2 * (size_t)n); cp(o.v, v, 2 * (size_t)n);
     cp(o.rho, rho, n); cp(o.mass, mass, n); cp(o.hsml, hsml, n);
+    cp(o.mass0, mass0 ? mass0 : mass, n);
+    if (o.nfric == 3)
+        for (int k = 0; k < n; k++)
+            if (!(o.mass[k] > lit<R>(1.e-6))) return GFSPH_ERR_ARG; /* the reference stops, :9450-9453 */
     o.set_flags(flag);
     o.p.assign(n, (R)0);
     o.ex.assign(2 * (size_t)n, (R)0); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;
@@ -1785,15 +1877,16 @@ int oracle_solvegc2(int mode, int npoin, int nelem, int nnode, int ndofn, const 
  * pwp: Uaux(1,:) in/out when icpwp = 3 (may be NULL); pwp_init = 1 starts
  * it from pwp0rel*rho*const(14) as Input_SW does instead of reading it. */
 int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
-               double* topol, int n, double* x, double* v, double* rho, double* mass, double* hsml, int* flag,
-               double* pwp, int pwp_init, int nsteps, double* dt, double* t, double t_end, int* steps_done) {
+               double* topol, int n, double* x, double* v, double* rho, double* mass, const double* mass0,
+               double* hsml, int* flag, double* pwp, int pwp_init, int nsteps, double* dt, double* t, double t_end,
+               int* steps_done) {
     if (!p || !topol || !x || !v || !rho || !mass || !hsml || !flag || !dt || !t || n < 0 || nx < 2 || ny < 2)
         return GFSPH_ERR_ARG;
     if (p->summation_density != 1) return GFSPH_ERR_UNSUPPORTED;
     switch (mode) {
-    case 0: return run_mode<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
-    case 1: return run_mode<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
-    case 2: return run_mode<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
+    case 0: return run_mode<float, float>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, mass0, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
+    case 1: return run_mode<float, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, mass0, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
+    case 2: return run_mode<double, double>(p, nx, ny, xmin, ymin, dx, dy, topol, n, x, v, rho, mass, mass0, hsml, flag, pwp, pwp_init, nsteps, dt, t, t_end, steps_done);
     default: return GFSPH_ERR_ARG;
     }
 }
@@ -1832,6 +1925,7 @@ int tangent_run(const gfsph_params* p, int nx, int ny, double xmin, double ymin,
         o.mass[k] = R(mass[k], seed_m ? seed_m[k] : 0.0);
         o.hsml[k] = R(hsml[k]);
     }
+    o.mass0 = o.mass;
     o.set_flags(flag);
     o.p.assign(n, R(0.0));
     o.ex.assign(2 * (size_t)n, R(0.0)); o.in = o.ex; o.Dx = o.ex; o.Dv = o.ex; o.av = o.ex;

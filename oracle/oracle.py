@@ -92,8 +92,8 @@ def lib(omp=False):
         L = C.CDLL(path)
         L.oracle_run.restype = C.c_int
         L.oracle_run.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _IP, _DP, C.c_int, C.c_int, _DP,
-                                 _DP, C.c_double, _IP]
+                                 C.c_double, _DP, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _IP, _DP, C.c_int, C.c_int,
+                                 _DP, _DP, C.c_double, _IP]
         L.oracle_pairs.restype = C.c_int
         L.oracle_pairs.argtypes = [C.c_int, C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, _IP, C.c_int, _IP, _IP, _DP,
                                    _DP]
@@ -176,10 +176,12 @@ def initial_topol(z, dx, dy, const, deriv=1, mode=MODE_FP32):
 class State:
     """Particle state and DEM of an oracle run (float64 arrays)."""
 
-    def __init__(self, x, v, rho, mass, hsml, topol, flag=None, dt=0.01, t=0.0, pwp=None):
-        """pwp: Uaux(1,:) for icpwp = 3; None starts it as Input_SW does."""
+    def __init__(self, x, v, rho, mass, hsml, topol, flag=None, dt=0.01, t=0.0, pwp=None, mass0=None):
+        """pwp: Uaux(1,:) for icpwp = 3; None starts it as Input_SW does.
+        mass0: the masses at the start of the run (nfric 3); None takes mass."""
         self.x, self.v = _d(x).copy(), _d(v).copy()
         self.rho, self.mass, self.hsml = _d(rho).copy(), _d(mass).copy(), _d(hsml).copy()
+        self.mass0 = self.mass.copy() if mass0 is None else _d(mass0).copy()
         n = self.x.shape[0]
         self.flag = np.zeros(n, np.int32) if flag is None else np.ascontiguousarray(flag, np.int32).copy()
         self.topol = _d(topol).copy()
@@ -187,7 +189,8 @@ class State:
         self.pwp = None if pwp is None else _d(pwp).copy()
 
     def copy(self):
-        s = State(self.x, self.v, self.rho, self.mass, self.hsml, self.topol, self.flag, self.dt, self.t, self.pwp)
+        s = State(self.x, self.v, self.rho, self.mass, self.hsml, self.topol, self.flag, self.dt, self.t, self.pwp,
+                  self.mass0)
         return s
 
 
@@ -201,7 +204,7 @@ def run(mode, params, nx, ny, dx, dy, state, nsteps, xmin=0.0, ymin=0.0, t_end=1
     if params.icpwp == 3 and state.pwp is None:
         state.pwp, init = np.zeros(n), 1
     st = lib().oracle_run(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol),
-                          n, _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass),
+                          n, _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.mass0),
                           _dp(state.hsml), _ip(state.flag), _dp(state.pwp), init,
                           nsteps, C.byref(dt), C.byref(t), t_end, C.byref(done))
     if st:

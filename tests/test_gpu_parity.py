@@ -415,6 +415,15 @@ RHEOLOGIES = {
     "mu_I_8": {5: 8, 3: 1.0, 6: 0.5, 7: 2.0, 9: 0.25},
     "mu_I_26": {5: 26, 3: 0.5, 6: 0.5, 7: 1.0, 9: 0.25},
     "mu_I_27": {5: 27, 3: 0.6, 6: 0.5, 7: 0.3, 9: 0.2},
+    "manning_1": {5: 1, 3: 0.05},
+    "laminar_2": {5: 2, 7: 5000.0},
+    "bagnold_11": {5: 11, 3: 0.05},
+    "hb_23_m1": {5: 23, 6: 3000.0, 7: 1000.0, 8: 1.0},
+    "hb_23_m2": {5: 23, 6: 3000.0, 7: 1000.0, 8: 2.0},
+    "hb_23_m05": {5: 23, 6: 3000.0, 7: 1000.0, 8: 0.5},
+    "hb_23_m033": {5: 23, 6: 3000.0, 7: 1000.0, 8: 0.333333},
+    "hb_24": {5: 24, 6: 3000.0, 7: 1000.0, 8: 0.5},
+    "hb_25": {5: 25, 6: 3000.0, 7: 1000.0, 8: 0.5},
 }
 
 
@@ -435,6 +444,58 @@ def test_rheologies_match_oracle(gfsph_lib, oracle_mod, rheo):
         for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
             assert rel_l2(g[key], ref) <= tol, (key, nsteps)
     sim.close()
+
+
+def test_eroded_soil_bingham_matches_oracle(gfsph_lib, oracle_mod):
+    """nfric 3 (SPH_SW_2019.f90:9443-9489) with Hungr erosion: the mass a
+    particle gains by erosion, (m - m0)/m with m0 its mass at upload, turns
+    on and scales its Bingham friction; 1 and 40 steps against the oracle,
+    with the soil fraction past the 0.01 threshold for part of the flow.  A
+    massless particle is refused at upload (the reference stops there)."""
+    w = small_channel()
+    w.const = {**w.const, 5: 3, 3: 2.0, 6: 3000.0, 7: 1000.0, 8: 0.05}
+    sim, st, p = setup_pair(w, oracle_mod)
+    m0 = st.mass.copy()
+    ny, nx = w.z.shape
+    for nsteps in (1, 39):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        tol = 1e-6 if nsteps == 1 else 1e-5
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
+            assert rel_l2(g[key], ref) <= tol, (key, nsteps, rel_l2(g[key], ref))
+    soil = (g["mass"] - m0) / g["mass"]
+    assert soil.max() > 0.05 and (soil > 0.01).mean() > 0.1, (soil.max(), (soil > 0.01).mean())
+    mass = w.mass.copy()
+    mass[7] = 0.0
+    with pytest.raises(gfsph.GfsphError) as e:
+        sim.upload(w.x, w.v, w.rho, mass, w.hsml)
+    assert e.value.status == gfsph.ERR_ARG
+    sim.close()
+
+
+def test_basal_laws_outside_the_path_are_refused(gfsph_lib):
+    """basal_friction_Ext_SW stops for nfric 23 with m other than 1, 2, 1/3,
+    1/2 and for a yield stress below 1e-32 (SPH_SW_2019.f90:9547-9550,
+    :9596-9598); nfric 24/25 with m <= 0 would divide by zero at rest; nfric
+    9, 10, 22 and 201-203 are not on the path."""
+    w = small_channel(n=500, k=6)
+    cases = [({5: 23, 6: 3000.0, 7: 1000.0, 8: 0.7}, gfsph.ERR_UNSUPPORTED),
+             ({5: 23, 6: 0.0, 7: 1000.0, 8: 1.0}, gfsph.ERR_ARG),
+             ({5: 24, 6: 3000.0, 7: 1000.0, 8: 0.0}, gfsph.ERR_ARG),
+             ({5: 25, 6: 3000.0, 7: 1000.0, 8: -1.0}, gfsph.ERR_ARG)]
+    cases += [({5: nf}, gfsph.ERR_UNSUPPORTED) for nf in (9, 10, 22, 201)]
+    # grain crushing const(36), the solid-end laws const(43) and the late
+    # Voellmy xi const(41) (Input_SW :1312-1325, ExtForces_SW :8424-8434)
+    cases += [({36: 1.0}, gfsph.ERR_UNSUPPORTED), ({43: 1.0}, gfsph.ERR_UNSUPPORTED),
+              ({41: 300.0}, gfsph.ERR_UNSUPPORTED)]
+    for const, status in cases:
+        w.const = {**small_channel(n=500, k=6).const, **const}
+        p = workloads.make_params(w, gfsph)
+        with pytest.raises(gfsph.GfsphError) as e:
+            gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+        assert e.value.status == status, const
 
 
 @pytest.mark.parametrize("skf", [2, 3])

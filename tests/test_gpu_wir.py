@@ -83,7 +83,9 @@ def test_soil_and_water_refusals(gfsph_lib):
     assert e.value.status == gfsph.ERR_UNSUPPORTED
     sim.close()
     # options outside the scope of the two materials
-    for const, kw in (({21: 1, 22: 0.005}, {}), ({}, {"icpwp": 3}), ({}, {"nor_density": 1}), ({16: 1.0}, {})):
+    # (interface erosion const(50) and friction const(55), Input_SW :1328-1345, too)
+    for const, kw in (({21: 1, 22: 0.005}, {}), ({}, {"icpwp": 3}), ({}, {"nor_density": 1}), ({16: 1.0}, {}),
+                      ({50: 1.0, 51: 0.001}, {}), ({55: 1.0, 56: 0.1}, {})):
         p = gfsph.make_params({**CONST, **const}, sle=1, ic_adapt=0, dt=0.01, ws_interact=1, **kw)
         with pytest.raises(gfsph.GfsphError) as e:
             gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)

@@ -175,7 +175,7 @@ def test_still_layer_interior_force_is_zero(oracle_mod):
     assert edge > 1e-3  # the free edge is pushed outwards
 
 
-def single_particle_run(oracle_mod, const, tan_theta, steps, dt, sle=0, mode=2, rho=1.0, **kw):
+def single_particle_run(oracle_mod, const, tan_theta, steps, dt, sle=0, mode=2, rho=1.0, mass0=None, **kw):
     nx, ny, d = 20, 1200, 5.0
     yy = np.arange(ny)[:, None] * d * np.ones((1, nx))
     z = (ny * d - yy) * tan_theta
@@ -184,7 +184,7 @@ def single_particle_run(oracle_mod, const, tan_theta, steps, dt, sle=0, mode=2, 
     hs = 2.0
     m = 4.0
     st = oracle_mod.State(np.array([[50.0, 100.0]]), np.zeros((1, 2)), np.array([rho]), np.array([m]),
-                          np.array([hs]), topol, dt=dt)
+                          np.array([hs]), topol, dt=dt, mass0=None if mass0 is None else np.array([mass0]))
     oracle_mod.run(mode, p, nx, ny, d, d, st, steps)
     w0 = 15.0 / (7.0 * math.pi * hs * hs) * (2.0 / 3.0)
     return st, w0 * m
@@ -413,6 +413,90 @@ def test_mu_of_I_steady_velocity_on_infinite_slope(oracle_mod, nfric):
         inert = i0 * a / (1.0 - a)
     st, _ = single_particle_run(oracle_mod, const, tan_t, 1500, 0.02, rho=h)
     v_exact = inert * h / r * math.sqrt(9.8 * h)
+    v = np.hypot(*st.v[0])
+    assert abs(v - v_exact) < 2e-3 * v_exact, (v, v_exact)
+
+
+def _hb23_a_hat(xh, m):
+    """a_hat for which nfric 23's quadratic (SPH_SW_2019.f90:9578-9600) has
+    the root xh: 48 x^2 - (32 a + 114) x + 65 (m = 1, 1/3, 1/2) or
+    10 x^2 - (a + 19.2188) x + 9.1875 (m = 2)."""
+    if m == 2.0:
+        return (10.0 * xh * xh - 19.2188 * xh + 9.1875) / xh
+    return (48.0 * xh * xh - 114.0 * xh + 65.0) / (32.0 * xh)
+
+
+# steady velocity on the plane tan(theta) = 0.5 where each law's friction,
+# divided by h, equals g tan(theta); dens 2000, h the lone particle's depth
+def _steady_velocity(law, c, h, tan_t):
+    g, dens = 9.8, 2000.0
+    drive = dens * g * tan_t * h  # the basal shear Tau0 that balances gravity
+    if law == 1:  # g n^2 v^2 / h^(4/3) = g tan(theta)
+        return h ** (2.0 / 3.0) * math.sqrt(tan_t) / c[3]
+    if law == 2:  # K v / (8 dens h^2) = g tan(theta)
+        return 8.0 * dens * h * h * g * tan_t / c[7]
+    if law == 11:  # K v^2 / h^3 = g tan(theta)
+        return math.sqrt(g * tan_t * h ** 3 / c[3])
+    tau, k, m = c[6], c[7], c[8]
+    if law in (24, 25):  # tau_y + Cm K (v/h)^m = dens g tan(theta) h
+        cm = 1.0 if law == 24 else ((2 * m + 1) / m) ** m
+        return h * ((drive - tau) / (k * cm)) ** (1.0 / m)
+    xh = tau / drive  # nfric 23: Tau0 = tau_y / xh
+    a = _hb23_a_hat(xh, m)
+    if m == 1.0:  # a_hat = 6 K |hv| / (tau h^2)
+        return a * tau * h / (6.0 * k)
+    if m == 2.0:  # a_hat = (1/Cm) (K/tau)^(1/2) |hv| / h^2, Cm = m / ((m+1)(2m+1))
+        return a * h * (2.0 / 15.0) * math.sqrt(tau / k)
+    return a * tau * h / (4.5 * k)  # m = 1/3 or 1/2: a_hat = 4.5 K |hv| / (tau h^2)
+
+
+@pytest.mark.parametrize("law,const", [
+    (1, {5: 1, 3: 0.05}),
+    (2, {5: 2, 7: 1000.0}),
+    (11, {5: 11, 3: 0.01}),
+    (23, {5: 23, 6: 1000.0, 7: 100.0, 8: 1.0}),
+    (23, {5: 23, 6: 1000.0, 7: 100.0, 8: 2.0}),
+    (23, {5: 23, 6: 1000.0, 7: 100.0, 8: 0.5}),
+    (23, {5: 23, 6: 1000.0, 7: 100.0, 8: 0.333333}),
+    (24, {5: 24, 6: 1000.0, 7: 1000.0, 8: 0.5}),
+    (25, {5: 25, 6: 1000.0, 7: 1000.0, 8: 0.5}),
+])
+def test_viscous_laws_steady_velocity_on_infinite_slope(oracle_mod, law, const):
+    """Manning (nfric 1), laminar (2), Bagnold (11) and Herschel-Bulkley
+    (23 exact, 24/25 approximate) basal laws of basal_friction_Ext_SW
+    (SPH_SW_2019.f90:9426-9437, 9538-9618, 9791-9796): a lone particle on a
+    plane settles at the velocity where the friction balances gravity."""
+    tan_t = 0.5
+    h = lone_particle_depth(oracle_mod)
+    c = {3: 0.0, 9: 0.0, **const}
+    st, _ = single_particle_run(oracle_mod, c, tan_t, 1500, 0.02, rho=h)
+    v_exact = _steady_velocity(law, c, h, tan_t)
+    v = np.hypot(*st.v[0])
+    assert abs(v - v_exact) < 2e-3 * v_exact, (v, v_exact)
+    assert abs(st.v[0, 0]) < 1e-9
+
+
+@pytest.mark.parametrize("soil", [0.0, 0.5])
+def test_eroded_soil_bingham_steady_velocity(oracle_mod, soil):
+    """nfric 3 (SPH_SW_2019.f90:9443-9489): the soil fraction s = (m - m0)/m
+    scales the yield stress and viscosity by 1 - exp(-C3 s) and sets the
+    density to 1000 + (dens - 1000) s; below s = 0.01 only the Manning term
+    (n = const(8)) acts.  A lone particle that carries no eroded soil settles
+    at the Manning velocity, one whose mass is half soil at the Bingham
+    velocity of its scaled constants (intermediate regime)."""
+    tan_t, c3, tau, k, n8 = 0.5, 2.0, 2000.0, 100.0, 0.05
+    h = lone_particle_depth(oracle_mod)
+    const = {5: 3, 3: c3, 6: tau, 7: k, 8: n8, 9: 0.0}
+    st, _ = single_particle_run(oracle_mod, const, tan_t, 1500, 0.02, rho=h, mass0=4.0 * (1.0 - soil))
+    if soil == 0.0:
+        v_exact = h ** (2.0 / 3.0) * math.sqrt(tan_t) / n8
+    else:
+        f = 1.0 - math.exp(-c3 * soil)
+        dens_b = 1000.0 + (2000.0 - 1000.0) * soil
+        xh = tau * f / (dens_b * 9.8 * tan_t * h)
+        a = _hb23_a_hat(xh, 1.0)
+        assert 0.01 < a < 50.0
+        v_exact = a * tau * h / (6.0 * k)  # a_hat = 6 K f |hv| / (tau f h^2)
     v = np.hypot(*st.v[0])
     assert abs(v - v_exact) < 2e-3 * v_exact, (v, v_exact)
 
