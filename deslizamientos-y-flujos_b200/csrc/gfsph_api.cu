@@ -823,7 +823,12 @@ int validate(const gfsph_params* p) {
     if (nfric == 23 && hb_case(p->cst[7]) < 0) return GFSPH_ERR_UNSUPPORTED;
     // nfric 24/25 with m <= 0: (v/h)**m is infinite for a particle at rest
     if ((nfric == 24 || nfric == 25) && !(p->cst[7] > 0.f)) return GFSPH_ERR_ARG;
-    if (erosion && (int)(p->cst[20] + 0.1f) != 1) return GFSPH_ERR_UNSUPPORTED;
+    const int eros_law = erosion ? (int)(p->cst[20] + 0.1f) : 0;
+    if (erosion && eros_law != 1 && eros_law != 2) return GFSPH_ERR_UNSUPPORTED;
+    if (eros_law == 2) {  // tanfi is a local of the frictional laws; denss, densw (SPH_SW_2019.f90:10337-10340)
+        if (!((nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
+        if (p->cst[16] <= 1.e-3f || p->cst[17] <= 1.e-3f) return GFSPH_ERR_ARG;
+    }
     if (p->skf < 1 || p->skf > 4) return GFSPH_ERR_UNSUPPORTED;
     // skf 2, 3 (support 3 h): the pair set depends on the reference's own
     // grid, reproduced for nnps 2; nnps 4 grids the principal-axes rotation
@@ -972,6 +977,14 @@ int create_handle(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle* sha
     c.cgra05 = k[0] * 0.5f;
     c.nfric = (int)(k[4] + 0.01f);
     c.erosion = (k[20] > 1.e-9f) ? 1 : 0;
+    c.eros_law = c.erosion ? (int)(k[20] + 0.1f) : 0;
+    {  // erosion law 2, SPH_SW_2019.f90:10341-10350
+        const float denss = k[16], densw = k[17];
+        const float vol_conc = (k[1] - densw) / (denss - densw);
+        c.er_xnum = (denss - densw) * vol_conc;
+        c.er_xden = c.er_xnum + densw;
+        c.er_kc = k[21] * k[22];
+    }
     c.skf = p->skf; c.pa_sph = p->pa_sph; c.sle = p->sle; c.av_vel = p->average_velocity ? 1 : 0;
     c.ic_adapt = p->ic_adapt;
     c.nor_density = p->nor_density ? 1 : 0;

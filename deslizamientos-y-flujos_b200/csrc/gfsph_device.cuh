@@ -231,6 +231,9 @@ struct Rheo {
     // ((2m+1)/m)**m (1 for nfric 24)
     int hb_m;
     float m_vexp, hb_a0, hb_cm;  // m_vexp = const(8) is also nfric 3's Manning n
+    // erosion law const(21) (1 Hungr, 2 bed angle) and law 2's constants
+    int eros_law;
+    float er_kc, er_xnum, er_xden;
     // soil and water particles (ic_ws_Interact = 1, ic_SWalg sw_alg): pairs of
     // one material only in the density, forces and av_vel; the soil-water
     // pairs push the soil by -dens_ws g m_j grad W (SPH_SW_2019.f90:8502-8521,
@@ -246,11 +249,17 @@ __device__ __forceinline__ float powr(float x, float y) { return (float)pow((dou
 struct ExtLocal {
     float h, hu, hv, hinv, vmod, hvmod, hvmodinv, frictx, fricty, totfrict, cf5, gravx, gravy;
     float hrho;  // rho(ipoin) as ExtForces_SW reads it, before the comp clamp
+    // read by erosion law 2: vxx, vyy and tanfi as the friction leaves them,
+    // the slopes of Get_Z_Topo
+    float vxx, vyy, tanfi, zpx, zpy;
 };
 
 // Start of the ExtForces_SW particle loop, SPH_SW_2019.f90:8564-8596.
 __device__ __forceinline__ void ext_locals(const Rheo& c, float hdepth, float vx, float vy, ExtLocal& L) {
     L.hrho = hdepth;
+    L.vxx = vx;  // :8566-8569
+    L.vyy = vy;
+    L.tanfi = 0.f;
     L.h = hdepth;
     L.hu = L.h * vx;
     L.hv = L.h * vy;
@@ -281,6 +290,8 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
     const bool v2byr = (c.nfric == 7 || c.nfric == 8 || c.nfric == 26 || c.nfric == 27);
     float zpx, zpy, top[6];
     dem_lookup(d, xx, yy, zpx, zpy, v2byr, top);
+    L.zpx = zpx;
+    L.zpy = zpy;
     float gz = c.g;
     if (COS) {
         const float deng = terrain_deng(zpx, zpy);
@@ -353,9 +364,10 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
         L.fricty = (cf2a * L.hv) / (hfrict * hfrict);
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
     } else if (c.nfric == 11) {  // Bagnold, K = const(3), :9791-9796
-        const float vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
-        L.frictx = ((c.xi * vxx) * L.vmod) / (hfrict * hfrict);
-        L.fricty = ((c.xi * vyy) * L.vmod) / (hfrict * hfrict);
+        L.vxx = L.hu * L.hinv;
+        L.vyy = L.hv * L.hinv;
+        L.frictx = ((c.xi * L.vxx) * L.vmod) / (hfrict * hfrict);
+        L.fricty = ((c.xi * L.vyy) * L.vmod) / (hfrict * hfrict);
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
     } else if (c.nfric >= 23 && c.nfric <= 25) {  // Herschel-Bulkley, :9538-9618
         float tau0;
@@ -387,6 +399,8 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
         float cv2byr = 0.f;
         if (v2byr) {
             float vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
+            L.vxx = vxx;
+            L.vyy = vyy;
             L.vmod = sqrtf(vxx * vxx + vyy * vyy);
             if (L.vmod >= 1e-5f) {
                 float cosa = vxx / L.vmod, sina = vyy / L.vmod;
@@ -416,12 +430,15 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
             if (factpw > c.fact_pwp_max) factpw = c.fact_pwp_max;
             tanfi = tanfi * factpw;
         }
+        L.tanfi = tanfi;
         float gtanfi = ((gz + cv2byr) * tanfi) * c.fact_dens;  // :9706
         if (gtanfi < 0.f) gtanfi = 0.f;
         L.cf5 = gtanfi;
         L.frictx = ((L.cf5 * L.hu) * L.hvmodinv) * L.h;
         L.fricty = ((L.cf5 * L.hv) * L.hvmodinv) * L.h;
         if (c.xi != 0.f) {
+            L.vxx = vx;  // :9720-9723, 9752-9755
+            L.vyy = vy;
             float vm = vx * vx + vy * vy;
             vm = (vm > 0.f) ? sqrtf(vm) : 0.f;
             L.vmod = vm;
@@ -473,6 +490,34 @@ __device__ __forceinline__ void reversal_filter(const Rheo& c, float dt, float v
     }
 }
 
+// Get_Erosion_Rate_SW, SPH_SW_2019.f90:10329-10356, with the ExtForces_SW
+// locals after the basal friction: law 1 (Hungr) E = C22 h |v|; law 2
+// E = C22 C23 |v| tan(theta - theta_e) where the bed slope along the flow,
+// theta = atan2(-grad Z . v/|v|, 1), exceeds the equilibrium angle
+// tan(theta_e) = (denss - densw) c tanfi / ((denss - densw) c + densw),
+// c = (dens - densw)/(denss - densw) (er_xnum = (denss - densw) c, er_xden =
+// er_xnum + densw, er_kc = C22 C23); atan2, atan and tan in FP64, rounded once.
+// Law 2 is kept out of line: its FP64 atan2/atan/tan would otherwise raise the
+// register count of every kernel that inlines the friction.
+static __device__ __noinline__ float erosion_rate_bed_angle(float er_kc, float er_xnum, float er_xden, float vmod,
+                                                            float vxx, float vyy, float zpx, float zpy, float tanfi) {
+    float er = 0.f;
+    if (vmod > 1.e-5f) {
+        const float cosa = vxx / vmod, sina = vyy / vmod;
+        const float gradzv = zpx * cosa + zpy * sina;
+        const float theta = (float)atan2((double)(-gradzv), 1.0);
+        const float tanthetae = (er_xnum * tanfi) / er_xden;
+        const float thetae = (float)atan((double)tanthetae);
+        if (theta > thetae) er = (er_kc * vmod) * (float)tan((double)(theta - thetae));
+    }
+    return er;
+}
+
+__device__ __forceinline__ float erosion_rate(const Rheo& c, const ExtLocal& L) {
+    if (c.eros_law == 1) return (c.keros * L.h) * L.vmod;
+    return erosion_rate_bed_angle(c.er_kc, c.er_xnum, c.er_xden, L.vmod, L.vxx, L.vyy, L.zpx, L.zpy, L.tanfi);
+}
+
 // External acceleration of one particle in one RK stage: ExtForces_SW(0)
 // particle loop, SPH_SW_2019.f90:8532-8716 (gravity, basal friction with the
 // reversal filter, Hungr erosion momentum :8664-8697).
@@ -483,13 +528,15 @@ __device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
     grav_and_friction<COS>(c, d, xx, yy, vx, vy, pwp, nsoil, L);
+    // the erosion rate reads nothing that the reversal filter changes, so it
+    // is taken here and the locals it reads need not outlive the filter
+    const float er = c.erosion ? erosion_rate(c, L) : 0.f;
     ex0 = 0.f + L.gravx;
     ex1 = 0.f + L.gravy;
     reversal_filter(c, dt, vx, vy, ex0 + in0, ex1 + in1, L);
     ex0 = ex0 - L.frictx / L.h;
     ex1 = ex1 - L.fricty / L.h;
     if (c.erosion) {
-        float er = (c.keros * L.h) * L.vmod;
         ex0 = ex0 - ((er * vx) * L.hinv) * c.slip;
         ex1 = ex1 - ((er * vy) * L.hinv) * c.slip;
     }
@@ -549,7 +596,7 @@ __device__ __forceinline__ float erosion_rate_final(const Rheo& c, const DemView
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
     grav_and_friction(c, d, xx, yy, vx, vy, pwp, nsoil, L);
-    return (c.keros * L.h) * L.vmod;
+    return erosion_rate(c, L);
 }
 
 // Get_Pwp_SW with one pwp point (icpwp = 3), SPH_SW_2019.f90:11176-11371 (no

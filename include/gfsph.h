@@ -62,8 +62,10 @@ extern "C" {
  * (0 g, 1 g/sqrt(1+|grad Z|^2) in the pressure and the friction, IntForces_SW
  * SPH_SW_2019.f90:6775-6783, Get_Grav_Ext_SW :9264-9270), const(20)
  * density-factor switch (0 or 1), const(21)
- * erosion law (1 = Hungr), const(22) Hungr constant, const(47) slip factor
- * alpha, const(48) maximum erodible depth.
+ * erosion law (1 = Hungr, 2 = bed angle above the equilibrium angle, with a
+ * frictional law and const(17)/(18) solid and fluid densities), const(22)
+ * erosion constant, const(23) law 2's C*, const(47) slip factor alpha,
+ * const(48) maximum erodible depth.
  */
 typedef struct gfsph_params {
     float cst[GFSPH_NCONST];

@@ -269,7 +269,7 @@ struct Oracle {
     /* options */
     const gfsph_params* P;
     R cst[GFSPH_NCONST + 1]; /* 1-based like const(k) */
-    int nfric = 0, ic_erosion = 0, ic_costheta = 0;
+    int nfric = 0, ic_erosion = 0, eros_law = 0, ic_costheta = 0;
     /* DEM */
     int nx, ny, npoig;
     R xming, yming, dxg, dyg, xmaxg, ymaxg;
@@ -744,11 +744,17 @@ struct Oracle {
     struct Local { /* ExtForces_SW locals shared with its contained routines */
         R h, hu, hv, hinv, vmod, hvmod, hvmodinv, frictx, fricty, totfrict, cf5, gravx, gravy, gravz;
         R hrho; /* rho(ipoin) as ExtForces_SW reads it, before the comp clamp */
+        /* read by erosion law 2: vxx, vyy and tanfi as the friction leaves
+           them, the slopes of Get_Z_Topo */
+        R vxx, vyy, tanfi, zpx, zpy;
     };
 
     /* the start of the ExtForces_SW particle loop, SPH_SW_2019.f90:8564-8596 */
     void ext_locals(int i, R hdepth, Local& L) {
         L.hrho = hdepth;
+        L.vxx = v[2 * i]; /* :8566-8569 */
+        L.vyy = v[2 * i + 1];
+        L.tanfi = 0;
         L.h = hdepth;
         L.hu = L.h * v[2 * i];
         L.hv = L.h * v[2 * i + 1];
@@ -772,6 +778,8 @@ struct Oracle {
         bool v2byr = (nfric == 7 || nfric == 8 || nfric == 26 || nfric == 27);
         R zp, zpx, zpy;
         get_z_topo(x[2 * i], x[2 * i + 1], zp, zpx, zpy, top, v2byr);
+        L.zpx = zpx;
+        L.zpy = zpy;
         if (ic_costheta == 1) { /* :9264-9270 */
             R deng = terrain_deng(zpx, zpy);
             L.gravz = cgra / deng;
@@ -851,9 +859,10 @@ struct Oracle {
             L.fricty = (cf2a * L.hv) / (hfrict * hfrict);
             L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
         } else if (nfric == 11) { /* Bagnold with K_Bagnold = const(3), :9791-9796 */
-            R vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
-            L.frictx = ((cst[3] * vxx) * L.vmod) / (hfrict * hfrict);
-            L.fricty = ((cst[3] * vyy) * L.vmod) / (hfrict * hfrict);
+            L.vxx = L.hu * L.hinv;
+            L.vyy = L.hv * L.hinv;
+            L.frictx = ((cst[3] * L.vxx) * L.vmod) / (hfrict * hfrict);
+            L.fricty = ((cst[3] * L.vyy) * L.vmod) / (hfrict * hfrict);
             L.totfrict = std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
         } else if (nfric >= 23 && nfric <= 25) { /* Herschel-Bulkley, :9538-9618 */
             R tauy0 = cst[6], constK = cst[7], m = cst[8];
@@ -887,6 +896,8 @@ struct Oracle {
             R cv2byr = 0;
             if (v2byr) {
                 R vxx = L.hu * L.hinv, vyy = L.hv * L.hinv;
+                L.vxx = vxx;
+                L.vyy = vyy;
                 L.vmod = std::sqrt(vxx * vxx + vyy * vyy);
                 if (L.vmod >= lit<R>(1e-5)) {
                     R cosa = vxx / L.vmod, sina = vyy / L.vmod;
@@ -920,6 +931,7 @@ struct Oracle {
                 if (factpw > fact_pwp_max) factpw = fact_pwp_max;
                 tanfi = tanfi * factpw;
             }
+            L.tanfi = tanfi;
             R gtanfi = ((L.gravz + cv2byr) * tanfi) * fact_dens; /* :9706 */
             if (gtanfi < 0) gtanfi = 0;
             L.cf5 = gtanfi;
@@ -927,6 +939,8 @@ struct Oracle {
             L.fricty = ((L.cf5 * L.hv) * L.hvmodinv) * L.h;
             if (xi != 0) {
                 R vxx = v[2 * i], vyy = v[2 * i + 1];
+                L.vxx = vxx; /* :9720-9723, 9752-9755 */
+                L.vyy = vyy;
                 R vm = vxx * vxx + vyy * vyy;
                 vm = (vm > 0) ? std::sqrt(vm) : (R)0;
                 L.vmod = vm;
@@ -1024,13 +1038,38 @@ struct Oracle {
             reversal_filter(i, L, ex[2 * i] + in[2 * i], ex[2 * i + 1] + in[2 * i + 1], nf);
             ex[2 * i] = ex[2 * i] - L.frictx / L.h;
             ex[2 * i + 1] = ex[2 * i + 1] - L.fricty / L.h;
-            if (ic_erosion) { /* Hungr, Get_Erosion_Rate_SW :10329-10331; momentum :8664-8697 */
-                R er = (cst[22] * L.h) * L.vmod;
+            if (ic_erosion) { /* Get_Erosion_Rate_SW; momentum :8664-8697 */
+                R er = erosion_rate(L);
                 R sf = slip_fact();
                 ex[2 * i] = ex[2 * i] - ((er * v[2 * i]) * L.hinv) * sf;
                 ex[2 * i + 1] = ex[2 * i + 1] - ((er * v[2 * i + 1]) * L.hinv) * sf;
             }
         }
+    }
+
+    /* Get_Erosion_Rate_SW, SPH_SW_2019.f90:10329-10356: law 1 (Hungr) E =
+     * C22 h |v|; law 2 E = C22 C23 |v| tan(theta - theta_e) where the bed
+     * slope along the flow, theta = atan2(-grad Z . v/|v|, 1), exceeds the
+     * equilibrium angle tan(theta_e) = (denss - densw) c tanfi /
+     * ((denss - densw) c + densw), c = (dens - densw)/(denss - densw); atan2,
+     * atan and tan in FP64, rounded once */
+    R erosion_rate(const Local& L) {
+        if (eros_law == 1) return (cst[22] * L.h) * L.vmod;
+        R er = 0;
+        if (L.vmod > lit<R>(1.e-5)) {
+            R denss = cst[17], densw = cst[18], dens = cst[2];
+            R vol_conc = (dens - densw) / (denss - densw);
+            R cosa = L.vxx / L.vmod, sina = L.vyy / L.vmod;
+            R gradzv = L.zpx * cosa + L.zpy * sina;
+            R theta = (R)std::atan2((double)(-gradzv), 1.0);
+            R xnum = (denss - densw) * vol_conc;
+            R xden = xnum + densw;
+            xnum = xnum * L.tanfi;
+            R tanthetae = xnum / xden;
+            R thetae = (R)std::atan((double)tanthetae);
+            if (theta > thetae) er = ((cst[22] * cst[23]) * L.vmod) * (R)std::tan((double)(theta - thetae));
+        }
+        return er;
     }
 
     /* ExtForces_SW(1): erosion after the RK update, SPH_SW_2019.f90:8717-8807 */
@@ -1045,7 +1084,7 @@ struct Oracle {
             Local L;
             ext_locals(i, rho[i], L);
             grav_and_friction(i, L, top, nfric);
-            R er = (cst[22] * L.h) * L.vmod;
+            R er = erosion_rate(L);
             R base = dt * er;
             R xx = x[2 * i], yy = x[2 * i + 1];
             int ipx = (int)((xx - xming) / dxg + (R)1);
@@ -1267,7 +1306,12 @@ struct Oracle {
         /* crushing (const(36)), the solid-end laws (const(43)), the late xi const(41) (:1312-1325, 8424-8434) */
         if (P->cst[35] > 0.01f || P->cst[42] > 0.f || P->cst[40] > 1.e-6f) return GFSPH_ERR_UNSUPPORTED;
         if (P->ws_interact == 1 && (P->cst[49] > 0.f || P->cst[54] > 0.f)) return GFSPH_ERR_UNSUPPORTED; /* :1328-1345 */
-        if (ic_erosion && (int)(cst[21] + lit<R>(0.1)) != 1) return GFSPH_ERR_UNSUPPORTED;
+        eros_law = ic_erosion ? (int)(cst[21] + lit<R>(0.1)) : 0;
+        if (ic_erosion && eros_law != 1 && eros_law != 2) return GFSPH_ERR_UNSUPPORTED;
+        if (eros_law == 2) { /* tanfi is a friction-law local: frictional laws only; denss, densw (:10337-10340) */
+            if (!((nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
+            if (P->cst[16] <= 1.e-3f || P->cst[17] <= 1.e-3f) return GFSPH_ERR_ARG;
+        }
         if (P->skf < 1 || P->skf > 4) return GFSPH_ERR_UNSUPPORTED;
         ws = P->ws_interact;
         swalg = P->sw_alg;

@@ -145,6 +145,31 @@ def test_erosion_and_dem_rows_match_oracle(gfsph_lib, oracle_mod):
     sim.close()
 
 
+@pytest.mark.parametrize("rheo", ["frictional_voellmy", "curvature", "mu_I_8"])
+def test_erosion_law_2_matches_oracle(gfsph_lib, oracle_mod, rheo):
+    """Erosion law 2 (Get_Erosion_Rate_SW, SPH_SW_2019.f90:10332-10356): the
+    rate C22 C23 |v| tan(theta - theta_e) from the bed angle along the flow
+    and the equilibrium angle of the friction law's tanfi; 1 and 20 steps of
+    the channel release against the oracle, mass and DEM rows included."""
+    w = small_channel()
+    w.const = {**w.const, **RHEOLOGIES[rheo], 17: 2650.0, 18: 1000.0, 21: 2, 22: 0.05, 23: 0.6}
+    sim, st, p = setup_pair(w, oracle_mod)
+    ny, nx = w.z.shape
+    for nsteps in (1, 19):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        tol = 1e-6 if nsteps == 1 else 1e-5
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
+            assert rel_l2(g[key], ref) <= tol, (key, nsteps, rel_l2(g[key], ref))
+    assert g["mass"].sum() > w.mass.sum() * 1.001
+    t = st.topol.reshape(ny, nx, 16)
+    eroded = sim.raster(gfsph.RASTER_ERODED)
+    assert np.abs(eroded - t[..., 13]).max() <= 1e-6 + 1e-5 * t[..., 13].max()
+    sim.close()
+
+
 def test_rasters_match_oracle(gfsph_lib, oracle_mod):
     w = small_channel()
     sim, st, p = setup_pair(w, oracle_mod)
@@ -486,6 +511,9 @@ def test_basal_laws_outside_the_path_are_refused(gfsph_lib):
              ({5: 24, 6: 3000.0, 7: 1000.0, 8: 0.0}, gfsph.ERR_ARG),
              ({5: 25, 6: 3000.0, 7: 1000.0, 8: -1.0}, gfsph.ERR_ARG)]
     cases += [({5: nf}, gfsph.ERR_UNSUPPORTED) for nf in (9, 10, 22, 201)]
+    # erosion law 2 needs a frictional law's tanfi and the two densities; law 3 is not built
+    cases += [({5: 4, 6: 500.0, 7: 50.0, 17: 2650.0, 18: 1000.0, 21: 2, 22: 0.05}, gfsph.ERR_UNSUPPORTED),
+              ({21: 2, 22: 0.05, 17: 0.0, 18: 1000.0}, gfsph.ERR_ARG), ({21: 3, 22: 0.05}, gfsph.ERR_UNSUPPORTED)]
     # grain crushing const(36), the solid-end laws const(43) and the late
     # Voellmy xi const(41) (Input_SW :1312-1325, ExtForces_SW :8424-8434)
     cases += [({36: 1.0}, gfsph.ERR_UNSUPPORTED), ({43: 1.0}, gfsph.ERR_UNSUPPORTED),

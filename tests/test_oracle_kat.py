@@ -293,6 +293,36 @@ def test_erosion_moves_volume_from_dem_to_flow(oracle_mod):
     assert np.allclose(t[..., 0] + t[..., 13], w.z, atol=1e-3)  # Z lowered by exactly the eroded depth
 
 
+@pytest.mark.parametrize("vy0", [3.0, -3.0])
+def test_erosion_law_2_grows_the_mass_above_the_equilibrium_angle(oracle_mod, vy0):
+    """Get_Erosion_Rate_SW law 2 (SPH_SW_2019.f90:10332-10356): a lone
+    particle on a plane of slope tan(theta) = 0.5 moving down the fall line
+    erodes at E = C22 C23 |v| tan(theta - theta_e), tan(theta_e) =
+    (dens - densw) tanfi / dens here (c (denss - densw) = dens - densw), and
+    gains m dt E / h in the step; moving uphill the bed angle along the flow
+    is negative and nothing is eroded."""
+    tan_t, mu, keros, cstar, dt = 0.5, 0.2, 0.05, 0.6, 0.02
+    nx, ny, d = 20, 1200, 5.0
+    yy = np.arange(ny)[:, None] * d * np.ones((1, nx))
+    z = (ny * d - yy) * tan_t
+    const = {3: 0.0, 9: mu, 17: 2650.0, 18: 1000.0, 21: 2, 22: keros, 23: cstar, 48: 5.0}
+    p = params(const, sle=0, dt=dt, ic_adapt=0, average_velocity=0)
+    topol = oracle_mod.initial_topol(z, d, d, const, deriv=1, mode=2)
+    h = lone_particle_depth(oracle_mod)
+    st = oracle_mod.State(np.array([[50.0, 3000.0]]), np.array([[0.0, vy0]]), np.array([h]), np.array([4.0]),
+                          np.array([2.0]), topol, dt=dt)
+    oracle_mod.run(2, p, nx, ny, d, d, st, 1)
+    v1 = abs(st.v[0, 1])
+    if vy0 > 0:
+        theta = math.atan(tan_t)
+        thetae = math.atan((2000.0 - 1000.0) * mu / 2000.0)
+        e = keros * cstar * v1 * math.tan(theta - thetae)
+        assert abs(st.mass[0] / 4.0 - 1.0 - dt * e / h) < 1e-9, (st.mass[0], dt * e / h)
+    else:
+        assert st.mass[0] == 4.0
+    assert abs(st.v[0, 0]) < 1e-12
+
+
 def test_fp32_and_fp64_oracles_agree_closely(oracle_mod):
     w = workloads.inclined_plane()
     p = workloads.make_params(w, gfsph)
