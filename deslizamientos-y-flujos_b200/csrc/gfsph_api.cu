@@ -574,7 +574,12 @@ int enqueue_step(gfsph_handle* h) {
     nk++;
     join(h, 1);
     launch(h, K_FORCE_RK, [&] {
-        pdl_launch(k_force_rk, pb, kThreads, st, h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
+        if (h->rheo.icpwp == 1)
+            pdl_launch(k_force_rk<true>, pb, kThreads, st, h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0,
+                       nullptr);
+        else
+            pdl_launch(k_force_rk<false>, pb, kThreads, st, h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin,
+                       h->d_auxv, 0, nullptr);
     }); nk++;
     if (h->rheo.av_vel) {
         fork(h, 2);
@@ -845,7 +850,10 @@ int validate(const gfsph_params* p) {
     if (cos_theta != 0 && cos_theta != 1) return GFSPH_ERR_UNSUPPORTED;
     const int fct = (int)(p->cst[19] + 0.1f);                          // ic_fct_dens
     if (fct != 0 && fct != 1) return GFSPH_ERR_UNSUPPORTED;
-    if (p->icpwp != 0 && p->icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
+    if (p->icpwp != 0 && p->icpwp != 1 && p->icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
+    // icpwp 1 integrates u inside the fused RK45 only: not with the staged
+    // pressure (nor_density, ic_cosTheta = 1)
+    if (p->icpwp == 1 && (p->nor_density != 0 || cos_theta != 0)) return GFSPH_ERR_UNSUPPORTED;
     if ((fct != 0 || p->icpwp != 0) && (int)(p->cst[33] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;  // ic_hrelSat
     if (p->icpwp == 3 && p->cst[25] > 0.f) return GFSPH_ERR_UNSUPPORTED;  // drag laws rescale Bfact
     if (fct == 1 && (p->cst[16] < 1.e-3f || p->cst[17] < 1.e-3f)) return GFSPH_ERR_ARG;  // denss, densw
@@ -1211,7 +1219,7 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
         CK(cudaMemcpyAsync(h->spec_u, sp.data(), (size_t)n, cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));  // sp is a local
     }
-    if (h->rheo.icpwp == 3)
+    if (h->rheo.icpwp != 0)  // u (icpwp 1) or Uaux(1) (icpwp 3): the same start, :1724-1737, 1829-1852
         launch(h, K_UNSORT, [&] {
             k_pwp_init<<<blocks_for(n), kThreads, 0, st>>>(h->B.pwp, h->B.rho, n, h->P.pwp0rel, h->P.cst[13]);
         });
@@ -1447,8 +1455,8 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) try {
         with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });
     });
     launch(h, K_FORCE_RK, [&] {
-        k_force_rk<<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 1,
-                                                     h->velfin);
+        k_force_rk<false><<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin,
+                                                            h->d_auxv, 1, h->velfin);
     });
     launch(h, K_UNSORT, [&] { k_unsort_f2<<<blocks_for(n), kThreads, 0, s>>>(h->velfin, h->A.id, n, h->f2tmp); });
     launch(h, K_COPY, [&] { k_copy_state<<<blocks_for(n), kThreads, 0, s>>>(h->A, h->B, n); });

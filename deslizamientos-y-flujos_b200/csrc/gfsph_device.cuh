@@ -421,7 +421,7 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
             float inert = (froude * c.mu_r) / L.h;
             tanfi = tanfi + (c.mu_a - tanfi) / (1.f + c.mu_b / inert);
         }
-        if (c.icpwp == 3) {  // :9670-9688: pwp = Uaux(1,ipoin), filtered, then tanfi*factpw
+        if (c.icpwp != 0) {  // :9670-9688: pwp = u(ipoin) (icpwp 1) or Uaux(1,ipoin) (3), filtered, then tanfi*factpw
             float hhh = L.hrho;
             if (pwp > c.fpwp_max * hhh) pwp = c.fpwp_max * hhh;
             if (pwp < c.fpwp_min * hhh) pwp = c.fpwp_min * hhh;
@@ -621,6 +621,17 @@ __device__ __forceinline__ float pwp_update(const Rheo& c, float u, float hh, fl
     if (u > hh) u = hh;
     if (u < (hh * c.alphas) * c.fpwp_min_g) u = (hh * c.alphas) * c.fpwp_min_g;
     return u;
+}
+
+// The basal pore pressure of icpwp = 1, u(ipoin), integrated by the RK45
+// itself: ExtForces_SW(0) (SPH_SW_2019.f90:8648-8652) gives du = -(u/dt)
+// (1 - exp(-beta dt)), beta = Bfact hinv^2 / const(14)^2, with hinv of the
+// ExtForces locals (0 below comp); exp in FP64, rounded once.
+__device__ __forceinline__ float pwp1_rate(const Rheo& c, float hc, float u, float dt) {
+    const float hinv = (hc < c.comp) ? 0.f : 1.f / hc;
+    const float betaw = ((c.bfact * hinv) * hinv) / c.alphas2;
+    const float e = (float)exp((double)(-(betaw * dt)));
+    return -((u / dt) * (1.f - e));
 }
 
 __device__ __forceinline__ bool out_of_box(const DemView& d, float xx, float yy) {

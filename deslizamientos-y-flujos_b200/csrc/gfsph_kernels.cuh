@@ -709,8 +709,8 @@ __global__ void k_reorder(const PState B, int n, const int* perm, const int2* ke
         A.pos[s] = p;
         A.vel[s] = B.vel[o];
         A.rho[s] = r;
-        if (c.icpwp == 3) A.pwp[s] = B.pwp[o];
-        if (c.icpwp == 3 || c.nor_density)
+        if (c.icpwp != 0) A.pwp[s] = B.pwp[o];
+        if (c.icpwp != 0 || c.nor_density)
             rho0[s] = ((c.ic_adapt == 1 || c.ic_adapt == 2 || c.ic_adapt == 10) && r < c.h_inf) ? c.h_inf : r;
         A.mass[s] = m;
         A.hsml[s] = hs;
@@ -1203,6 +1203,7 @@ __device__ __forceinline__ void rk_carry(const PState& A, const Rheo& c, const P
     B.rho[i] = A.rho[i]; B.mass[i] = A.mass[i]; B.hsml[i] = A.hsml[i];
     B.flag[i] = A.flag[i]; B.id[i] = A.id[i];
     if (c.icpwp == 3) B.pwp[i] = 0.f;  // Get_Pwp_SW zeroes out-of-domain particles
+    if (c.icpwp == 1) B.pwp[i] = A.pwp[i];  // u of a frozen particle stays
 }
 
 // The end of the RK45 body of an active particle: the final update
@@ -1216,7 +1217,7 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
                                           const DemView& dem, const PState& B, float2* velfin, double2* auxv, int i,
                                           float dt, float2 x0, float2 v0, float Dx0, float Dx1, float Dv0, float Dv1,
                                           float xx, float xy, float vx, float vy, bool out, float h, float pwp,
-                                          NodeBox& box) {
+                                          float u0, float Du, NodeBox& box) {
     float m = A.mass[i];
     float hs = A.hsml[i];
     if (!out) {
@@ -1225,6 +1226,7 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
         xy = x0.y + dt6 * Dx1;
         vx = v0.x + dt6 * Dv0;
         vy = v0.y + dt6 * Dv1;
+        if (c.icpwp == 1) pwp = u0 + dt6 * Du;  // u of icpwp 1 (:921); else pwp is the stage's u
         out = out_of_box(dem, xx, xy);
     }
     float er = 0.f;
@@ -1244,6 +1246,13 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
     B.flag[i] = out ? 1 : 0;
     B.id[i] = A.id[i];
     if (c.icpwp == 3) B.pwp[i] = out ? 0.f : pwp_update(c, pwp, h, h - Q.rho0[i], dt);
+    if (c.icpwp == 1) {  // bounded by the depth after ExtForces_SW(1), RK45 :974-979
+        if (!out) {
+            if (pwp > h) pwp = h;
+            if (pwp < 0.f) pwp = 0.f;
+        }
+        B.pwp[i] = pwp;
+    }
 }
 
 // Internal acceleration of the regular particles, one thread each.  The
@@ -1281,6 +1290,9 @@ __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars*
 // stages.  (A particle that leaves the DEM box mid-step is frozen; the
 // reference then keeps scattering its stale pressure into its neighbours for
 // the remaining stages, which is not reproduced.)
+// PWP1 (icpwp = 1) carries u through the stages; the other runs are compiled
+// without it, so their stage loop keeps its registers.
+template <bool PWP1>
 __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
                                                    PState B, float2* velfin, double2* auxv, int forces_only,
                                                    float2* indv_out) {
@@ -1312,7 +1324,9 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
         const float h = A.rho[i];
         const float hc = (h < c.h_inf) ? c.h_inf : h;  // IntForces_SW clamp, seen by ExtForces_SW(0)
         const float2 x0 = A.pos[i], v0 = A.vel[i];
-        const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
+        // icpwp 3: Uaux(1) of the step start; icpwp 1: u0, then u of each stage
+        const float u0 = (c.icpwp != 0) ? A.pwp[i] : 0.f;
+        float pwp = u0, du = 0.f, Du = 0.f;
         const float nsoil = soil_fraction(c, Q, A, i);
         float xx = x0.x, xy = x0.y, vx = v0.x, vy = v0.y;
         float ex0 = 0.f, ex1 = 0.f;
@@ -1329,10 +1343,20 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
                 float nvx = v0.x + fdt * (ex0 + in0);
                 float nvy = v0.y + fdt * (ex1 + in1);
                 xx = nxx; xy = nxy; vx = nvx; vy = nvy;
+                if (PWP1) {  // RK45 :823-830, bounded by the depth as the stage finds it
+                    pwp = u0 + fdt * du;
+                    const float rc = (s == 0) ? Q.rho0[i] : hc;
+                    if (pwp > rc) pwp = rc;
+                    else if (pwp < 0.f) pwp = 0.f;
+                }
                 if (out_of_box(dem, xx, xy)) {
                     out = true;
                 } else {
                     ext_accel(c, dem, dt, xx, xy, vx, vy, hc, pwp, nsoil, in0, in1, ex0, ex1);
+                    if (PWP1) {
+                        du = pwp1_rate(c, hc, pwp, dt);
+                        Du = Du + f2 * du;
+                    }
                     Dv0 = Dv0 + f2 * (ex0 + in0);
                     Dv1 = Dv1 + f2 * (ex1 + in1);
                     Dx0 = Dx0 + f2 * vx;
@@ -1340,7 +1364,8 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
                 }
             }
         }
-        rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, Dx0, Dx1, Dv0, Dv1, xx, xy, vx, vy, out, h, pwp, box);
+        rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, Dx0, Dx1, Dv0, Dv1, xx, xy, vx, vy, out, h, pwp, u0,
+                  Du, box);
     }
     if (c.erosion) flush_node_box(S, box);
 }
@@ -1738,7 +1763,7 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
             }
         }
         rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, dx.x, dx.y, dv.x, dv.y, xx, xy, vx, vy, out,
-                  hfin[i], pwp, box);
+                  hfin[i], pwp, 0.f, 0.f, box);  // (icpwp 1 runs unstaged only)
     }
     if (c.erosion) flush_node_box(S, box);
 }

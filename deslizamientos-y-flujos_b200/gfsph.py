@@ -282,7 +282,7 @@ class Sim:
         return hs, g
 
     def pwp(self):
-        """Uaux(1,:), the basal pore-water pressure (icpwp = 3)."""
+        """The basal pore-water pressure: u (icpwp = 1) or Uaux(1,:) (icpwp = 3)."""
         out = np.empty(self.n, np.float32)
         _check(lib().gfsph_get_pwp(self.h, _fp(out)), "gfsph_get_pwp")
         return out

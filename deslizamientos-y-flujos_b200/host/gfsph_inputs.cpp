@@ -324,7 +324,7 @@ SwDat read_dat(const std::string& path) {
     }
     r.label();
     d.icpwp = r.read_int();
-    if (d.icpwp == 3) {  // Input_SW SPH_SW_2019.f90:1829-1835
+    if (d.icpwp == 1 || d.icpwp == 3) {  // Input_SW SPH_SW_2019.f90:1724-1729, 1829-1835
         r.label();
         d.pwp0rel = r.read_real();
     }

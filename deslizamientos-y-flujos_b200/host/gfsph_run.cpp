@@ -8,7 +8,8 @@
 //   - at every plot time (plot_step * dt): a summary line, the depth raster
 //     (ESRI ASCII grid) and the GiD results <problem>.post.res (height and
 //     velocity at the DEM nodes, displacement and velocity of the particles,
-//     OutputRes_Classic SPH_SW_2019.f90); the GiD mesh <problem>.post.msh
+//     the pore pressure at the nodes with icpwp = 1, OutputRes_Classic
+//     SPH_SW_2019.f90:13316-13471); the GiD mesh <problem>.post.msh
 //     (the DEM quadrilaterals and the particles, OutputMesh_Classic) at the
 //     start;
 //   - at every save time (save_step * dt): the restart files
@@ -114,12 +115,14 @@ void write_gid_mesh(const std::string& path, const TopoData& t, const std::vecto
 // OutputRes_Classic at one plot time: IDW averages (4x4 nodes around each
 // particle, weights 1/(dist/distg)) of h and v at the DEM nodes; the
 // particles' displacement from their first position (z from the current
-// terrain) and velocity.
+// terrain) and velocity; with icpwp = 1 (pwp given) the IDW average of the
+// pore pressure u as the "Pwp" result (SPH_SW_2019.f90:13363, 13436-13443).
 void write_gid_results(FILE* f, double time, const TopoData& t, const std::vector<float>& z, int n,
                        const std::vector<float>& x, const std::vector<float>& v, const std::vector<float>& h,
-                       const std::vector<int>& flag, const std::vector<float>& x00, const std::vector<float>& z00) {
+                       const std::vector<int>& flag, const std::vector<float>& x00, const std::vector<float>& z00,
+                       const std::vector<float>* pwp) {
     const int npoig = t.nx * t.ny;
-    std::vector<float> a1(npoig, 0.f), a2(npoig, 0.f), a3(npoig, 0.f), a5(npoig, 0.f);
+    std::vector<float> a1(npoig, 0.f), a2(npoig, 0.f), a3(npoig, 0.f), a4(npoig, 0.f), a5(npoig, 0.f);
     const float distg = std::sqrt(t.dx * t.dx + t.dy * t.dy);
     for (int i = 0; i < n; i++) {
         if (flag[i]) continue;
@@ -136,12 +139,15 @@ void write_gid_results(FILE* f, double time, const TopoData& t, const std::vecto
                 dist = dist / distg;
                 a1[ip] = a1[ip] + h[i] / dist;
                 a5[ip] = a5[ip] + 1.f / dist;
+                if (pwp) a4[ip] = a4[ip] + (*pwp)[i] / dist;
                 a2[ip] = a2[ip] + v[2 * i] / dist;
                 a3[ip] = a3[ip] + v[2 * i + 1] / dist;
             }
     }
     for (int ip = 0; ip < npoig; ip++)
-        if (a5[ip] >= 1.e-6f) { a1[ip] = a1[ip] / a5[ip]; a2[ip] = a2[ip] / a5[ip]; a3[ip] = a3[ip] / a5[ip]; }
+        if (a5[ip] >= 1.e-6f) {
+            a1[ip] = a1[ip] / a5[ip]; a2[ip] = a2[ip] / a5[ip]; a3[ip] = a3[ip] / a5[ip]; a4[ip] = a4[ip] / a5[ip];
+        }
     std::fprintf(f, " Result \"height\" \"Height\" %.9G Vector OnNodes \"where\" \n Values \n", time);
     for (int ip = 0; ip < npoig; ip++)
         if (a1[ip] > 1.e-6f) std::fprintf(f, " %d 0. 0. %.9G\n", ip + 1, (double)a1[ip]);
@@ -158,6 +164,12 @@ void write_gid_results(FILE* f, double time, const TopoData& t, const std::vecto
     for (int i = 0; i < n; i++)
         if (!flag[i]) std::fprintf(f, " %d %.9G %.9G 0.0\n", npoig + i + 1, (double)v[2 * i], (double)v[2 * i + 1]);
     std::fprintf(f, " End Values \n");
+    if (pwp) {
+        std::fprintf(f, " Result \"Pwp\" \"pwpress\" %.9G Vector OnNodes \"where\" \n Values \n", time);
+        for (int ip = 0; ip < npoig; ip++)
+            if (a1[ip] > 1.e-6f) std::fprintf(f, " %d 0.0 0.0 %.9G\n", ip + 1, (double)a4[ip]);
+        std::fprintf(f, " End Values \n");
+    }
     std::fflush(f);
 }
 
@@ -259,8 +271,8 @@ int main(int argc, char** argv) {
             std::printf("], \"z_mean\": %.6f}\n", zsum / (double)t.z.size());
             return 0;
         }
-        if (d.icpwp != 0 && d.icpwp != 3)
-            throw std::runtime_error("icpwp = " + std::to_string(d.icpwp) + " is not implemented (0 and 3 are)");
+        if (d.icpwp != 0 && d.icpwp != 1 && d.icpwp != 3)
+            throw std::runtime_error("icpwp = " + std::to_string(d.icpwp) + " is not implemented (0, 1 and 3 are)");
         gfsph_params p;
         std::memset(&p, 0, sizeof(p));
         for (int k = 0; k < GFSPH_NCONST; k++) p.cst[k] = d.cst[k];
@@ -319,7 +331,7 @@ int main(int argc, char** argv) {
         check(gfsph_upload(hd, n, x.data(), v0.data(), h.data(), mass.data(), hsml.data(), itype.data(), nullptr),
               "gfsph_upload");
         if (restart) {
-            if (d.icpwp == 3) check(gfsph_set_pwp(hd, pwp0.data()), "gfsph_set_pwp");
+            if (d.icpwp != 0) check(gfsph_set_pwp(hd, pwp0.data()), "gfsph_set_pwp");
             check(gfsph_set_time(hd, time0, m.dt_sph), "gfsph_set_time");
         }
         check(gfsph_hazard_reset(hd), "gfsph_hazard_reset");
@@ -334,7 +346,7 @@ int main(int argc, char** argv) {
         double tnow = time0;
         long long total = 0;
         int iplot = 0;
-        std::vector<float> rx(2 * (size_t)n), rv(2 * (size_t)n), rh(n), rm(n), rs(n);
+        std::vector<float> rx(2 * (size_t)n), rv(2 * (size_t)n), rh(n), rm(n), rs(n), rp(n);
         std::vector<int> rf(n);
         std::vector<float> raster(npoig), zcur(t.z);
         // the GiD mesh with the particles' first positions (OutputMesh_Classic)
@@ -355,7 +367,7 @@ int main(int argc, char** argv) {
             R.itype = itype;
             R.x = rx; R.v = rv; R.h = rh; R.mass = rm; R.hsml = rs;
             R.pwp.assign(n, 0.f);
-            if (d.icpwp == 3) check(gfsph_get_pwp(hd, R.pwp.data()), "gfsph_get_pwp");
+            if (d.icpwp != 0) check(gfsph_get_pwp(hd, R.pwp.data()), "gfsph_get_pwp");
             write_restart(join(out, problem + ".restart.dat"), R);
             if (erosion) {
                 TopoRestart T;
@@ -402,7 +414,8 @@ int main(int argc, char** argv) {
                 std::snprintf(name, sizeof(name), ".depth_%04d.asc", iplot);
                 write_asc(join(out, problem + name), t, raster);
                 if (erosion) check(gfsph_raster(hd, GFSPH_RASTER_Z, zcur.data()), "gfsph_raster");
-                write_gid_results(gid, tnow, t, zcur, n, rx, rv, rh, rf, x00, z00);
+                if (d.icpwp == 1) check(gfsph_get_pwp(hd, rp.data()), "gfsph_get_pwp");
+                write_gid_results(gid, tnow, t, zcur, n, rx, rv, rh, rf, x00, z00, d.icpwp == 1 ? &rp : nullptr);
                 iplot++;
                 next_plot = tnow + time_plot;
             }

@@ -308,7 +308,7 @@ def write_reference_inputs(w, directory, name, out_step=100, restart=False, wate
     Fortran program (or gfsph_run) can read it: <name>.MASTER.dat,
     <name>.dat, <name>.top (ictop = 100: a grid file with finite-difference
     slopes) and <name>.pts (the particles as source points on their
-    lattice).  w.options may carry icpwp (0 or 3) and pwp0rel.  out_step is
+    lattice).  w.options may carry icpwp (0, 1 or 3) and pwp0rel.  out_step is
     print_step = save_step = plot_step; restart=True writes icunk_s = 200,
     which reads the particles from restart.dat (Get_Restart_Info_SW).
     water: soil and water (ic_soil = ic_water = 1, ic_SWAlg = w.options'
@@ -362,7 +362,7 @@ def write_reference_inputs(w, directory, name, out_step=100, restart=False, wate
             f.write("K0 activated?\n  0\n")
         icpwp = int(o.get("icpwp", 0))
         f.write("icpwp\n  %d\n" % icpwp)
-        if icpwp == 3:
+        if icpwp in (1, 3):
             f.write(" pwp0rel\n  %.9g\n" % float(o.get("pwp0rel", 0.0)))
         f.write("coarse mesh saving utility?\n  0\ncontrol points?\n  0\n")
         f.write("GID filter\n  1 1 1 1 0 1 0 0 0 1 0 0\nT_change_to_W\n  1.e+12\n")

@@ -85,8 +85,11 @@ typedef struct gfsph_params {
     int dem_deriv;         /* slopes when not supplied: 0 FEM projection (Get_Topol), 1 finite differences */
     int max_neighbours;    /* initial neighbour-table capacity per particle, 0..65536;
                               0 = 96 (grows on demand) */
-    int icpwp;             /* 0 none, 3 basal pore-water pressure with one point (Get_Pwp_SW, nUaux = 1) */
-    float pwp0rel;         /* icpwp = 3: initial Uaux = pwp0rel * rho * const(14) (Input_SW SPH_SW_2019.f90:1829-1852) */
+    int icpwp;             /* 0 none; 1 basal pore-water pressure u integrated by the RK45 with the
+                              dissipation of ExtForces_SW (SPH_SW_2019.f90:8648-8652; not with nor_density
+                              or ic_cosTheta = 1); 3 with one point (Get_Pwp_SW, nUaux = 1) */
+    float pwp0rel;         /* icpwp = 1, 3: initial u, Uaux = pwp0rel * rho * const(14)
+                              (Input_SW SPH_SW_2019.f90:1724-1737, 1829-1852) */
     int ws_interact;       /* ic_ws_Interact: 0 one material; 1 soil and water particles (ic_soil = ic_water = 1,
                               Input_SW SPH_SW_2019.f90:947-951): species from gfsph_set_species */
     int sw_alg;            /* ic_SWalg with ws_interact 1: 0 both as landslides; 1 water over the soil surface
@@ -159,10 +162,11 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
 int gfsph_download(gfsph_handle* h, float* x, float* v, float* rho, float* mass, float* hsml,
                    int* out_flag);
 
-/* Basal pore-water pressure Uaux(1,:) (icpwp = 3), n values in the original
- * particle order: gfsph_upload starts it as Input_SW does
- * (pwp0rel * rho * const(14), SPH_SW_2019.f90:1829-1852); these replace or
- * read it (the reference's Uaux global, updated by Get_Pwp_SW
+/* Basal pore-water pressure, u(:) (icpwp = 1) or Uaux(1,:) (icpwp = 3), n
+ * values in the original particle order: gfsph_upload starts it as Input_SW
+ * does (pwp0rel * rho * const(14), SPH_SW_2019.f90:1724-1737, 1829-1852);
+ * these replace or read it (the reference's u or Uaux global, integrated by
+ * the RK45 with ExtForces_SW's du, or updated by Get_Pwp_SW
  * SPH_SW_2019.f90:11176-11371 at the end of every step). */
 int gfsph_set_pwp(gfsph_handle* h, const float* pwp);
 int gfsph_get_pwp(gfsph_handle* h, float* pwp);

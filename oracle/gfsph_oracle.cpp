@@ -12,9 +12,10 @@
  * density, IntForces_SW and ExtForces_SW(0) in each of its four stages,
  * recomputes the density after the final update, applies ExtForces_SW(1)
  * erosion, the basal pore-water pressure of Get_Pwp_SW (icpwp = 3),
- * h_upgrade and av_vel.  Every floating-point expression keeps the
- * Fortran left-to-right evaluation order, without FMA contraction
- * (build with -ffp-contract=off).
+ * h_upgrade and av_vel.  With icpwp = 1 the pore pressure u is a fifth
+ * RK45 variable whose rate ExtForces_SW(0) sets.  Every floating-point
+ * expression keeps the Fortran left-to-right evaluation order, without FMA
+ * contraction (build with -ffp-contract=off).
  *
  * Soil and water particles (ic_ws_Interact = 1, ic_SWalg 0 or 1): the
  * material of each particle travels in bit 1 of the flag array of this
@@ -283,7 +284,8 @@ struct Oracle {
      * the single-precision positions that every other term reads */
     bool pos64 = false;
     std::vector<double> xd, x0d;
-    std::vector<R> uaux, rho0; /* basal pore-water pressure Uaux(1,:) (icpwp = 3) and rho at the RK45 start */
+    std::vector<R> uaux, rho0; /* basal pore-water pressure u (icpwp 1) or Uaux(1,:) (3); rho at the RK45 start */
+    std::vector<R> u0, du1, Du; /* icpwp 1: u at the RK45 start, du of the last stage, Du_RK */
     /* pore-water-pressure and density factors: DFs_FSs_dens_and_pwp_factors
      * (ExtForces_SW, SPH_SW_2019.f90:8959-9109) for the friction, and
      * mini_DFs_dens_and_pwp_factors (Get_Pwp_SW, :11502-11632) for the update */
@@ -921,7 +923,7 @@ struct Oracle {
                     tanfi = tanfi * ff;
                 }
             }
-            if (icpwp == 3) { /* :9670-9688: pwp = Uaux(1,ipoin), filtered, then tanfi*factpw */
+            if (icpwp != 0) { /* :9670-9688: pwp = u(ipoin) (1) or Uaux(1,ipoin) (3), filtered, then tanfi*factpw */
                 R pwp = uaux[i];
                 R hhh = L.hrho;
                 if (pwp > fpwp_max * hhh) pwp = fpwp_max * hhh;
@@ -1038,6 +1040,11 @@ struct Oracle {
             reversal_filter(i, L, ex[2 * i] + in[2 * i], ex[2 * i + 1] + in[2 * i + 1], nf);
             ex[2 * i] = ex[2 * i] - L.frictx / L.h;
             ex[2 * i + 1] = ex[2 * i + 1] - L.fricty / L.h;
+            if (icpwp == 1) { /* du, :8648-8652 */
+                R betaw = ((cst[13] * L.hinv) * L.hinv) / (cst[14] * cst[14]);
+                R e = rexp(-(betaw * dt));
+                du1[i] = -((uaux[i] / dt) * ((R)1 - e));
+            }
             if (ic_erosion) { /* Get_Erosion_Rate_SW; momentum :8664-8697 */
                 R er = erosion_rate(L);
                 R sf = slip_fact();
@@ -1216,6 +1223,11 @@ struct Oracle {
         x0 = x; v0 = v;
         if (pos64) x0d = xd;
         rho0 = rho;
+        if (icpwp == 1) { /* u0 = u; du keeps the last step's values (times f1 = 0 in stage 1) */
+            u0 = uaux;
+            du1.resize(n, (R)0);
+            Du.assign(n, (R)0);
+        }
         const R f1[4] = {0, lit<R>(0.5), lit<R>(0.5), 1};
         const R f2[4] = {1, 2, 2, 1};
         for (int s = 0; s < 4; s++) {
@@ -1226,6 +1238,11 @@ struct Oracle {
                     const size_t k = 2 * i + d;
                     x[k] = pos64 ? (R)(x0d[k] + (double)fdt * (double)v[k]) : x0[k] + fdt * v[k];
                     v[k] = v0[k] + fdt * (ex[k] + in[k]);
+                }
+                if (icpwp == 1) { /* RK45 :823-830: bounded by the depth as this stage finds it */
+                    uaux[i] = u0[i] + fdt * du1[i];
+                    if (uaux[i] > rho[i]) uaux[i] = rho[i];
+                    else if (uaux[i] < 0) uaux[i] = 0;
                 }
             }
             check_out_domain();
@@ -1238,6 +1255,7 @@ struct Oracle {
                     Dv[2 * i + d] = Dv[2 * i + d] + f2[s] * (ex[2 * i + d] + in[2 * i + d]);
                     Dx[2 * i + d] = Dx[2 * i + d] + f2[s] * v[2 * i + d];
                 }
+                if (icpwp == 1) Du[i] = Du[i] + f2[s] * du1[i];
             }
         }
         R dt6 = dt / (R)6;
@@ -1256,11 +1274,18 @@ struct Oracle {
                 }
                 v[k] = v0[k] + dt6 * Dv[k];
             }
+            if (icpwp == 1) uaux[i] = u0[i] + dt6 * Du[i]; /* :921 */
         }
         sum_density();
         check_out_domain();
         ext_forces1();
         get_pwp();
+        if (icpwp == 1) /* :974-979 */
+            for (int i = 0; i < n; i++) {
+                if (flag[i]) continue;
+                if (uaux[i] > rho[i]) uaux[i] = rho[i];
+                if (uaux[i] < 0) uaux[i] = 0;
+            }
         h_upgrade();
         if (P->average_velocity) av_vel();
     }
@@ -1360,7 +1385,8 @@ struct Oracle {
         } else if (ic_fct_dens != 0) {
             return GFSPH_ERR_UNSUPPORTED;
         }
-        if (icpwp != 0 && icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
+        if (icpwp != 0 && icpwp != 1 && icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
+        if (icpwp == 1 && (P->nor_density != 0 || ic_costheta != 0)) return GFSPH_ERR_UNSUPPORTED; /* as the device */
         if ((ic_fct_dens != 0 || icpwp != 0) && (int)(cst[34] + lit<R>(0.01)) != 0) return GFSPH_ERR_UNSUPPORTED;
         if (icpwp == 3 && cst[26] > 0) return GFSPH_ERR_UNSUPPORTED; /* drag laws rescale Bfact */
         if (ic_fct_dens == 1 && icpwp != 0 && !(alphas > lit<R>(0.01))) return GFSPH_ERR_UNSUPPORTED;
@@ -1372,7 +1398,7 @@ struct Oracle {
     /* Uaux(1,:) = pwp0rel * rho * alphas at input (Input_SW, SPH_SW_2019.f90:1829-1852) */
     void init_pwp(const double* pwp_in) {
         uaux.assign(n, (R)0);
-        if (icpwp != 3) return;
+        if (icpwp != 3 && icpwp != 1) return;
         for (int i = 0; i < n; i++)
             uaux[i] = pwp_in ? (R)pwp_in[i] : (R)P->pwp0rel * (rho[i] * cst[14]);
     }
@@ -1918,7 +1944,7 @@ int oracle_solvegc2(int mode, int npoin, int nelem, int nnode, int ndofn, const 
 
 /* Runs nsteps steps of the reference path on the given state (in/out).
  * topol: (16, nx*ny) in/out (erosion lowers Z).  mode: 0, 1, 2 as above.
- * pwp: Uaux(1,:) in/out when icpwp = 3 (may be NULL); pwp_init = 1 starts
+ * pwp: u (icpwp = 1) or Uaux(1,:) (icpwp = 3) in/out (may be NULL); pwp_init = 1 starts
  * it from pwp0rel*rho*const(14) as Input_SW does instead of reading it. */
 int oracle_run(int mode, const gfsph_params* p, int nx, int ny, double xmin, double ymin, double dx, double dy,
                double* topol, int n, double* x, double* v, double* rho, double* mass, const double* mass0,

@@ -177,7 +177,7 @@ class State:
     """Particle state and DEM of an oracle run (float64 arrays)."""
 
     def __init__(self, x, v, rho, mass, hsml, topol, flag=None, dt=0.01, t=0.0, pwp=None, mass0=None):
-        """pwp: Uaux(1,:) for icpwp = 3; None starts it as Input_SW does.
+        """pwp: u (icpwp = 1) or Uaux(1,:) (icpwp = 3); None starts it as Input_SW does.
         mass0: the masses at the start of the run (nfric 3); None takes mass."""
         self.x, self.v = _d(x).copy(), _d(v).copy()
         self.rho, self.mass, self.hsml = _d(rho).copy(), _d(mass).copy(), _d(hsml).copy()
@@ -201,7 +201,7 @@ def run(mode, params, nx, ny, dx, dy, state, nsteps, xmin=0.0, ymin=0.0, t_end=1
     done = C.c_int(0)
     n = state.x.shape[0]
     init = 0
-    if params.icpwp == 3 and state.pwp is None:
+    if params.icpwp in (1, 3) and state.pwp is None:
         state.pwp, init = np.zeros(n), 1
     st = lib().oracle_run(mode, C.addressof(params), nx, ny, xmin, ymin, dx, dy, _dp(state.topol),
                           n, _dp(state.x), _dp(state.v), _dp(state.rho), _dp(state.mass), _dp(state.mass0),
@@ -299,7 +299,7 @@ class Run:
         self.L.oracle_get(self.h, _dp(x), _dp(v), _dp(rho), _dp(mass), _dp(hsml), _ip(flag), C.byref(dt), C.byref(t),
                          _dp(topol))
         pwp = None
-        if self.params.icpwp == 3:
+        if self.params.icpwp in (1, 3):
             pwp = np.zeros(n)
             self.L.oracle_get_pwp(self.h, _dp(pwp))
         return State(x, v, rho, mass, hsml, topol if with_topol else np.zeros(1), flag, dt.value, t.value, pwp)

@@ -42,11 +42,11 @@ def test_gfsph_run_on_written_inputs(gfsph_lib, tmp_path):
 
 
 def test_gfsph_run_with_basal_pore_pressure(gfsph_lib, tmp_path):
-    """icpwp = 3 read from the .dat (with its pwp0rel line) reaches the step:
-    a liquefied release (pwp0rel = 1, slow dissipation) runs out faster than
-    the same release without pore pressure."""
+    """icpwp = 1 and 3 read from the .dat (with their pwp0rel line) reach the
+    step: a liquefied release (pwp0rel = 1, slow dissipation) runs out faster
+    than the same release without pore pressure."""
     speeds = {}
-    for icpwp in (0, 3):
+    for icpwp in (0, 1, 3):
         w = workloads.inclined_plane()
         w.const = {**w.const, 9: 0.55, 13: 0.001, 14: 1.0}
         w.options = {**w.options, "icpwp": icpwp, "pwp0rel": 1.0}
@@ -59,7 +59,10 @@ def test_gfsph_run_with_basal_pore_pressure(gfsph_lib, tmp_path):
                              text=True)
         assert out.returncode == 0, out.stderr
         speeds[icpwp] = np.loadtxt(os.path.join(d, "plane.gfsph.log"))[-1, 5]
-    assert speeds[3] > 1.2 * speeds[0]
+        # OutputRes_Classic writes the pore pressure at the nodes for icpwp 1 only
+        res = open(os.path.join(d, "plane.post.res")).read()
+        assert ('Result "Pwp"' in res) == (icpwp == 1)
+    assert speeds[3] > 1.2 * speeds[0] and speeds[1] > 1.2 * speeds[0]
 
 
 def test_kernels_report_sm100(gfsph_lib):

@@ -400,18 +400,20 @@ def test_far_apart_releases_on_a_large_dem(gfsph_lib, oracle_mod):
     sim.close()
 
 
-@pytest.mark.parametrize("fct", [0, 1])
-def test_pore_water_pressure_matches_oracle(gfsph_lib, oracle_mod, fct):
+@pytest.mark.parametrize("icpwp,fct", [(3, 0), (3, 1), (1, 0), (1, 1)])
+def test_pore_water_pressure_matches_oracle(gfsph_lib, oracle_mod, icpwp, fct):
     """icpwp = 3 (Get_Pwp_SW with one point): Uaux starts at pwp0rel * h,
     lowers the basal friction by 1 - pwp/h, and relaxes towards the depth
-    change of every step.  ic_fct_dens = 1 adds the buoyancy factor of tanfi
-    and the negative pwp bounds."""
+    change of every step.  icpwp = 1: u starts the same way and the RK45
+    integrates its dissipation stage by stage (ExtForces_SW :8648-8652).
+    ic_fct_dens = 1 adds the buoyancy factor of tanfi and the negative pwp
+    bounds."""
     w = small_channel()
     extra = {13: 0.02, 14: 1.0}
     if fct:
         extra.update({17: 2650.0, 18: 1000.0, 19: 0.5, 20: 1})
     w.const = {**w.const, **extra}
-    sim, st, p = setup_pair(w, oracle_mod, icpwp=3, pwp0rel=0.8)
+    sim, st, p = setup_pair(w, oracle_mod, icpwp=icpwp, pwp0rel=0.8)
     assert np.array_equal(sim.pwp(), (np.float32(0.8) * (w.rho * np.float32(1.0))).astype(np.float32))
     ny, nx = w.z.shape
     for nsteps in (1, 29):
@@ -518,6 +520,12 @@ def test_basal_laws_outside_the_path_are_refused(gfsph_lib):
     # Voellmy xi const(41) (Input_SW :1312-1325, ExtForces_SW :8424-8434)
     cases += [({36: 1.0}, gfsph.ERR_UNSUPPORTED), ({43: 1.0}, gfsph.ERR_UNSUPPORTED),
               ({41: 300.0}, gfsph.ERR_UNSUPPORTED)]
+    # icpwp 1 integrates u inside the unstaged RK45 only; icpwp 2 is not built
+    for kw in ({"icpwp": 1, "nor_density": 1}, {"icpwp": 2}):
+        p = workloads.make_params(w, gfsph, pwp0rel=0.5, **kw)
+        with pytest.raises(gfsph.GfsphError) as e:
+            gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
+        assert e.value.status == gfsph.ERR_UNSUPPORTED, kw
     for const, status in cases:
         w.const = {**small_channel(n=500, k=6).const, **const}
         p = workloads.make_params(w, gfsph)

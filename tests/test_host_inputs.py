@@ -64,12 +64,14 @@ def test_reader_reports_unsupported_options(gfsph_lib, tmp_path):
     assert out.returncode == 2 and "ictop 3" in out.stderr
 
 
-def test_written_inputs_with_pore_pressure_parse(gfsph_lib, tmp_path):
+@pytest.mark.parametrize("icpwp", [1, 3])
+def test_written_inputs_with_pore_pressure_parse(gfsph_lib, tmp_path, icpwp):
+    """icpwp 1 and 3 each read a pwp0rel line (Input_SW SPH_SW_2019.f90:1724-1729, 1829-1835)."""
     w = workloads.inclined_plane()
-    w.options = {**w.options, "icpwp": 3, "pwp0rel": 0.75}
+    w.options = {**w.options, "icpwp": icpwp, "pwp0rel": 0.75}
     workloads.write_reference_inputs(w, str(tmp_path), "pw")
     meta = parse("pw", str(tmp_path))
-    assert meta["icpwp"] == 3 and abs(meta["pwp0rel"] - 0.75) < 1e-7
+    assert meta["icpwp"] == icpwp and abs(meta["pwp0rel"] - 0.75) < 1e-7
 
 
 def _damage(ext, how):

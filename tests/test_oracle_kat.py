@@ -424,6 +424,34 @@ def test_pwp_dissipates_exponentially(oracle_mod):
     assert abs(v - v_exact) < 1e-5 * v_exact, (v, v_exact)
 
 
+def test_rk_integrated_pwp_of_icpwp_1(oracle_mod):
+    """icpwp = 1: u is a fifth RK45 variable (SPH_MAIN_2019.f90:823, 903,
+    921) with the rate du = -(u/dt)(1 - exp(-beta dt)) of ExtForces_SW(0)
+    (SPH_SW_2019.f90:8648-8652), beta = Bfact / (h alphas)^2, and the
+    friction of each stage uses that stage's u.  For a lone particle (fixed
+    depth) the RK45 stages are linear in u: u1 = u0 + dt/6 sum_s f2_s du_s
+    with u_s = u0 + f1_s dt du_(s-1), and v gains dt g (tan(theta) - mu) +
+    g mu dt/6 sum_s f2_s u_s / h."""
+    tan_t, mu, dt, steps, bfact = 0.5, 0.6, 0.02, 100, 0.05
+    h = lone_particle_depth(oracle_mod)
+    st, _ = single_particle_run(oracle_mod, {3: 0.0, 9: mu, 13: bfact, 14: 1.0}, tan_t, steps, dt, rho=h,
+                                icpwp=1, pwp0rel=1.0)
+    # the constants as the FP32 parameter block carries them
+    b32, mu32, g32 = (float(np.float32(c)) for c in (bfact, mu, 9.8))
+    k = (1.0 - math.exp(-b32 / (h * h) * dt)) / dt
+    u, v = h, 0.0
+    for _ in range(steps):
+        us, du, acc = [], 0.0, 0.0
+        for f1, f2 in ((0.0, 1.0), (0.5, 2.0), (0.5, 2.0), (1.0, 1.0)):
+            ui = u + f1 * dt * du
+            du = -k * ui
+            us.append((f2, ui))
+        v += dt * g32 * (tan_t - mu32) + g32 * mu32 * dt / 6.0 * sum(f2 * ui for f2, ui in us) / h
+        u = u - k * dt / 6.0 * sum(f2 * ui for f2, ui in us)
+    assert abs(st.pwp[0] - u) < 1e-9 * h, (st.pwp[0], u)
+    assert abs(np.hypot(*st.v[0]) - v) < 1e-9 * v, (np.hypot(*st.v[0]), v)
+
+
 @pytest.mark.parametrize("nfric", [8, 27])
 def test_mu_of_I_steady_velocity_on_infinite_slope(oracle_mod, nfric):
     """mu(I) basal friction (nfric 8: tanfi (1 + b I^n); nfric 27: tanfi +
