@@ -574,12 +574,12 @@ int enqueue_step(gfsph_handle* h) {
     nk++;
     join(h, 1);
     launch(h, K_FORCE_RK, [&] {
-        if (h->rheo.icpwp == 1)
-            pdl_launch(k_force_rk<true>, pb, kThreads, st, h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0,
-                       nullptr);
-        else
-            pdl_launch(k_force_rk<false>, pb, kThreads, st, h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin,
-                       h->d_auxv, 0, nullptr);
+        const Rheo& c = h->rheo;
+        const bool gen = !(c.nfric == 4 || (c.nfric >= 5 && c.nfric <= 8) || c.nfric == 26 || c.nfric == 27) ||
+                         (c.erosion && c.eros_law != 1);
+        auto kf = (c.icpwp == 1) ? (gen ? k_force_rk<true, true> : k_force_rk<true, false>)
+                                 : (gen ? k_force_rk<false, true> : k_force_rk<false, false>);
+        pdl_launch(kf, pb, kThreads, st, h->A, q, S, h->rheo, h->dem, n, h->B, h->velfin, h->d_auxv, 0, nullptr);
     }); nk++;
     if (h->rheo.av_vel) {
         fork(h, 2);
@@ -773,6 +773,8 @@ void pwp_factors(const gfsph_params* p, Rheo& c) {
     c.icpwp = p->icpwp;
     c.fact_dens = 1.f; c.fact_pwp_max = 1.f; c.fact_pwp_min = 0.f; c.fpwp_max = 1.f; c.fpwp_min = 0.f;
     c.fpwp_min_g = 0.f;
+    c.dens_bar = dens;  // ic_fct_dens = 0 (:8999-9008)
+    c.dens_bar_eff = dens - ((densw < 1.e-3f) ? 1000.f : densw);
     if (fct == 1) {
         float porosity = (denss - dens) / (denss - densw);
         float dens2 = (1.f - porosity) * denss;
@@ -780,6 +782,8 @@ void pwp_factors(const gfsph_params* p, Rheo& c) {
         float dens_bar = (1.f - alphas) * dens2 + alphas * dens1;
         float dens_bar_eff = dens_bar - densw * alphas;
         c.fact_dens = dens_bar_eff / dens_bar;
+        c.dens_bar = dens_bar;
+        c.dens_bar_eff = dens_bar_eff;
         if (p->icpwp > 0) {
             c.fact_pwp_max = 1.f + (alphas * densw) / dens_bar_eff;
             c.fpwp_min = -(alphas * densw) / dens_bar_eff;
@@ -829,7 +833,11 @@ int validate(const gfsph_params* p) {
     // nfric 24/25 with m <= 0: (v/h)**m is infinite for a particle at rest
     if ((nfric == 24 || nfric == 25) && !(p->cst[7] > 0.f)) return GFSPH_ERR_ARG;
     const int eros_law = erosion ? (int)(p->cst[20] + 0.1f) : 0;
-    if (erosion && eros_law != 1 && eros_law != 2) return GFSPH_ERR_UNSUPPORTED;
+    if (erosion && (eros_law < 1 || eros_law > 3)) return GFSPH_ERR_UNSUPPORTED;
+    if (eros_law == 3) {  // denss, densw (SPH_SW_2019.f90:10363-10367); constant dens_bar (ic_hrelSat 0)
+        if (p->cst[16] <= 1.e-3f || p->cst[17] <= 1.e-3f) return GFSPH_ERR_ARG;
+        if ((int)(p->cst[33] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;
+    }
     if (eros_law == 2) {  // tanfi is a local of the frictional laws; denss, densw (SPH_SW_2019.f90:10337-10340)
         if (!((nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
         if (p->cst[16] <= 1.e-3f || p->cst[17] <= 1.e-3f) return GFSPH_ERR_ARG;
@@ -998,6 +1006,11 @@ int create_handle(const gfsph_params* p, const gfsph_dem* dem, gfsph_handle* sha
     c.nor_density = p->nor_density ? 1 : 0;
     c.cos_theta = ((int)(k[15] + 0.01f) == 1) ? 1 : 0;
     pwp_factors(p, c);
+    // erosion law 3 with pwp_factors' dens_bar_eff, SPH_SW_2019.f90:10357-10376
+    c.er_cb = k[22];
+    c.er_c1 = c.dens_bar_eff * k[0];
+    c.er_c2 = 1.f - k[24];
+    c.er_tb = k[23];
     c.muI = (c.nfric == 8 || c.nfric == 26) ? 1 : (c.nfric == 27 ? 2 : 0);
     c.mu_a = k[2]; c.mu_r = k[5]; c.mu_b = k[6];
     if (c.muI) c.xi = 0.f;  // const(3) is a mu(I) parameter, not xi (:9653)
@@ -1455,8 +1468,8 @@ int gfsph_internal_forces(gfsph_handle* h, float* indvxdt) try {
         with_skf(h, [&](auto sk) { k_force_big<decltype(sk)::value><<<big_blocks(h), 128, 0, s>>>(As[0], q, h->S, h->rheo); });
     });
     launch(h, K_FORCE_RK, [&] {
-        k_force_rk<false><<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B, h->velfin,
-                                                            h->d_auxv, 1, h->velfin);
+        k_force_rk<false, true><<<blocks_for(n), kThreads, 0, s>>>(h->A, q, h->S, h->rheo, h->dem, n, h->B,
+                                                                  h->velfin, h->d_auxv, 1, h->velfin);
     });
     launch(h, K_UNSORT, [&] { k_unsort_f2<<<blocks_for(n), kThreads, 0, s>>>(h->velfin, h->A.id, n, h->f2tmp); });
     launch(h, K_COPY, [&] { k_copy_state<<<blocks_for(n), kThreads, 0, s>>>(h->A, h->B, n); });

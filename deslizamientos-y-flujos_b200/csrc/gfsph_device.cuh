@@ -231,9 +231,12 @@ struct Rheo {
     // ((2m+1)/m)**m (1 for nfric 24)
     int hb_m;
     float m_vexp, hb_a0, hb_cm;  // m_vexp = const(8) is also nfric 3's Manning n
-    // erosion law const(21) (1 Hungr, 2 bed angle) and law 2's constants
+    // erosion law const(21) (1 Hungr, 2 bed angle, 3 basal shear) and the
+    // constants of laws 2 and 3; dens_bar, dens_bar_eff of
+    // DFs_FSs_dens_and_pwp_factors (SPH_SW_2019.f90:8959-9060)
     int eros_law;
     float er_kc, er_xnum, er_xden;
+    float dens_bar, dens_bar_eff, er_cb, er_c1, er_c2, er_tb;
     // soil and water particles (ic_ws_Interact = 1, ic_SWalg sw_alg): pairs of
     // one material only in the density, forces and av_vel; the soil-water
     // pairs push the soil by -dens_ws g m_j grad W (SPH_SW_2019.f90:8502-8521,
@@ -283,7 +286,10 @@ __device__ __forceinline__ float terrain_deng(float zpx, float zpy) { return sqr
 // COS) and basal_friction_Ext_SW (:9355-9828) before its reversal filter.
 // With ic_cosTheta = 1 the friction's gravz (gtanfi :9706, the mu(I) Froude
 // number :9658-9665) is g/deng; the Voellmy term keeps cgra = g (:9749).
-template <bool COS = false>
+// GEN = false compiles only the Bingham, frictional and mu(I) laws (nfric 4-8,
+// 26, 27), the common ones, so the kernels that inline them for those runs
+// stay small; GEN = true has every law.
+template <bool COS = false, bool GEN = true>
 __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& d, float xx, float yy, float vx,
                                                   float vy, float pwp, float nsoil, ExtLocal& L) {
     const bool frictional = (c.nfric >= 5 && c.nfric <= 8) || c.nfric == 26 || c.nfric == 27;
@@ -323,7 +329,7 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
             L.fricty = (cf4b * L.hv) * L.hvmodinv;
         }
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
-    } else if (c.nfric == 3) {  // Bingham of the eroded soil fraction nsoil, :9443-9489
+    } else if (GEN && c.nfric == 3) {  // Bingham of the eroded soil fraction nsoil, :9443-9489
         const float fsoil = 1.f - (float)exp((double)(-(c.xi * nsoil)));  // C3 = const(3)
         const float constKB = c.constK * fsoil, tauy0B = c.tauy0 * fsoil;
         const float densB = 1000.f + (c.dens - 1000.f) * nsoil;
@@ -352,24 +358,24 @@ __device__ __forceinline__ void grav_and_friction(const Rheo& c, const DemView& 
         if (fabsf(fxx) > fabsf(L.frictx)) L.frictx = fxx;
         if (fabsf(fyy) > fabsf(L.fricty)) L.fricty = fyy;
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
-    } else if (c.nfric == 1) {  // Newtonian turbulent (Manning n = const(3)), :9426-9430
+    } else if (GEN && c.nfric == 1) {  // Newtonian turbulent (Manning n = const(3)), :9426-9430
         const float cf1 = (c.g * c.xi) * c.xi;
         const float p73 = powr(hfrict, 7.f / 3.f);
         L.frictx = ((cf1 * L.hu) * L.hvmod) / p73;
         L.fricty = ((cf1 * L.hv) * L.hvmod) / p73;
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
-    } else if (c.nfric == 2) {  // Newtonian laminar, :9431-9437
+    } else if (GEN && c.nfric == 2) {  // Newtonian laminar, :9431-9437
         const float cf2a = c.constK / (8.f * c.dens);
         L.frictx = (cf2a * L.hu) / (hfrict * hfrict);
         L.fricty = (cf2a * L.hv) / (hfrict * hfrict);
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
-    } else if (c.nfric == 11) {  // Bagnold, K = const(3), :9791-9796
+    } else if (GEN && c.nfric == 11) {  // Bagnold, K = const(3), :9791-9796
         L.vxx = L.hu * L.hinv;
         L.vyy = L.hv * L.hinv;
         L.frictx = ((c.xi * L.vxx) * L.vmod) / (hfrict * hfrict);
         L.fricty = ((c.xi * L.vyy) * L.vmod) / (hfrict * hfrict);
         L.totfrict = sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
-    } else if (c.nfric >= 23 && c.nfric <= 25) {  // Herschel-Bulkley, :9538-9618
+    } else if (GEN && c.nfric >= 23 && c.nfric <= 25) {  // Herschel-Bulkley, :9538-9618
         float tau0;
         if (c.nfric == 23) {  // exact solution, :9576-9603
             float a_hat, a2 = 48.f, b2, c2 = 65.f;
@@ -513,30 +519,47 @@ static __device__ __noinline__ float erosion_rate_bed_angle(float er_kc, float e
     return er;
 }
 
+template <bool GEN = true>
 __device__ __forceinline__ float erosion_rate(const Rheo& c, const ExtLocal& L) {
-    if (c.eros_law == 1) return (c.keros * L.h) * L.vmod;
+    if (!GEN || c.eros_law == 1) return (c.keros * L.h) * L.vmod;
     return erosion_rate_bed_angle(c.er_kc, c.er_xnum, c.er_xden, L.vmod, L.vxx, L.vyy, L.zpx, L.zpy, L.tanfi);
+}
+
+// Erosion law 3 (SPH_SW_2019.f90:10357-10376) with the friction after the
+// reversal filter: E = C22 (Taub - Tauf) / dens_bar_eff where the basal
+// shear Taub = dens_bar |frict| exceeds the bed strength Tauf = C23 +
+// dens_bar_eff g h (1 - C25) C24 (er_c1 = dens_bar_eff g, er_c2 = 1 - C25).
+__device__ __forceinline__ float erosion_rate_shear(const Rheo& c, const ExtLocal& L) {
+    float er = 0.f;
+    if (L.vmod > 1.e-5f) {
+        const float taub = c.dens_bar * sqrtf(L.frictx * L.frictx + L.fricty * L.fricty);
+        const float tauf = c.er_cb + ((c.er_c1 * L.h) * c.er_c2) * c.er_tb;
+        if (taub > tauf && L.vmod > 1.e-3f) er = (c.keros * (taub - tauf)) / c.dens_bar_eff;
+    }
+    return er;
 }
 
 // External acceleration of one particle in one RK stage: ExtForces_SW(0)
 // particle loop, SPH_SW_2019.f90:8532-8716 (gravity, basal friction with the
 // reversal filter, Hungr erosion momentum :8664-8697).
-template <bool COS = false>
+template <bool COS = false, bool GEN = true>
 __device__ __forceinline__ void ext_accel(const Rheo& c, const DemView& d, float dt, float xx, float yy, float vx,
                                           float vy, float hdepth, float pwp, float nsoil, float in0, float in1,
                                           float& ex0, float& ex1) {
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
-    grav_and_friction<COS>(c, d, xx, yy, vx, vy, pwp, nsoil, L);
-    // the erosion rate reads nothing that the reversal filter changes, so it
-    // is taken here and the locals it reads need not outlive the filter
-    const float er = c.erosion ? erosion_rate(c, L) : 0.f;
+    grav_and_friction<COS, GEN>(c, d, xx, yy, vx, vy, pwp, nsoil, L);
+    // erosion laws 1 and 2 read nothing that the reversal filter changes, so
+    // their rate is taken here and the locals it reads need not outlive the
+    // filter; law 3 reads the filtered friction
+    float er = (c.erosion && !(GEN && c.eros_law == 3)) ? erosion_rate<GEN>(c, L) : 0.f;
     ex0 = 0.f + L.gravx;
     ex1 = 0.f + L.gravy;
     reversal_filter(c, dt, vx, vy, ex0 + in0, ex1 + in1, L);
     ex0 = ex0 - L.frictx / L.h;
     ex1 = ex1 - L.fricty / L.h;
     if (c.erosion) {
+        if (GEN && c.eros_law == 3) er = erosion_rate_shear(c, L);
         ex0 = ex0 - ((er * vx) * L.hinv) * c.slip;
         ex1 = ex1 - ((er * vy) * L.hinv) * c.slip;
     }
@@ -589,14 +612,20 @@ __device__ __forceinline__ void ext_accel_wir(const Rheo& c, const DemView& d, f
     ex1 = ex1 - L.fricty / L.h;
 }
 
-// Hungr erosion rate after the RK update (ExtForces_SW(1), :8717-8760):
-// E = C22 * h * vmod with the ExtForces locals after basal friction.
+// The erosion rate after the RK update (ExtForces_SW(1), :8717-8760) with
+// the ExtForces locals after basal friction.  Law 3 applies the reversal
+// filter first, with the last stage's total acceleration (exdvxdt + indvxdt
+// as ExtForces_SW(1) finds them).
+template <bool GEN = true>
 __device__ __forceinline__ float erosion_rate_final(const Rheo& c, const DemView& d, float xx, float yy, float vx,
-                                                    float vy, float hdepth, float pwp, float nsoil) {
+                                                    float vy, float hdepth, float pwp, float nsoil, float acc0,
+                                                    float acc1, float dt) {
     ExtLocal L;
     ext_locals(c, hdepth, vx, vy, L);
-    grav_and_friction(c, d, xx, yy, vx, vy, pwp, nsoil, L);
-    return erosion_rate(c, L);
+    grav_and_friction<false, GEN>(c, d, xx, yy, vx, vy, pwp, nsoil, L);
+    if (!GEN || c.eros_law != 3) return erosion_rate<GEN>(c, L);
+    reversal_filter(c, dt, vx, vy, acc0, acc1, L);
+    return erosion_rate_shear(c, L);
 }
 
 // Get_Pwp_SW with one pwp point (icpwp = 3), SPH_SW_2019.f90:11176-11371 (no

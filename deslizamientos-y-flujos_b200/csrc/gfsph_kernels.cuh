@@ -1213,11 +1213,12 @@ __device__ __forceinline__ void rk_carry(const PState& A, const Rheo& c, const P
 // the step's final depth; (xx, xy, vx, vy) the last stage's state, kept as
 // the result when the particle left the domain in a stage (out).  Every lane
 // of the warp must call it (erosion_scatter).
+template <bool GEN = true>
 __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, StepScalars* S, const Rheo& c,
                                           const DemView& dem, const PState& B, float2* velfin, double2* auxv, int i,
                                           float dt, float2 x0, float2 v0, float Dx0, float Dx1, float Dv0, float Dv1,
                                           float xx, float xy, float vx, float vy, bool out, float h, float pwp,
-                                          float u0, float Du, NodeBox& box) {
+                                          float u0, float Du, float acc0, float acc1, NodeBox& box) {
     float m = A.mass[i];
     float hs = A.hsml[i];
     if (!out) {
@@ -1230,7 +1231,8 @@ __device__ __forceinline__ void rk_finish(const PState& A, const Search& Q, Step
         out = out_of_box(dem, xx, xy);
     }
     float er = 0.f;
-    if (!out && c.erosion) er = erosion_rate_final(c, dem, xx, xy, vx, vy, h, pwp, soil_fraction(c, Q, A, i));
+    if (!out && c.erosion)
+        er = erosion_rate_final<GEN>(c, dem, xx, xy, vx, vy, h, pwp, soil_fraction(c, Q, A, i), acc0, acc1, dt);
     if (c.erosion) erosion_scatter(dem, xx, xy, dt * er, !out, auxv, box);
     if (!out) {
         if (c.erosion) m = m + ((dt * er) * m) / h;
@@ -1290,9 +1292,11 @@ __global__ void __launch_bounds__(128) k_iforce(PState A, Search Q, StepScalars*
 // stages.  (A particle that leaves the DEM box mid-step is frozen; the
 // reference then keeps scattering its stale pressure into its neighbours for
 // the remaining stages, which is not reproduced.)
-// PWP1 (icpwp = 1) carries u through the stages; the other runs are compiled
-// without it, so their stage loop keeps its registers.
-template <bool PWP1>
+// PWP1 (icpwp = 1) carries u through the stages; GEN compiles every basal
+// law and erosion law (else only nfric 4-8, 26, 27 and erosion law 1).  The
+// other runs are compiled without them, so their stage loop keeps its
+// registers and its code small.
+template <bool PWP1, bool GEN>
 __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
                                                    PState B, float2* velfin, double2* auxv, int forces_only,
                                                    float2* indv_out) {
@@ -1352,7 +1356,7 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
                 if (out_of_box(dem, xx, xy)) {
                     out = true;
                 } else {
-                    ext_accel(c, dem, dt, xx, xy, vx, vy, hc, pwp, nsoil, in0, in1, ex0, ex1);
+                    ext_accel<false, GEN>(c, dem, dt, xx, xy, vx, vy, hc, pwp, nsoil, in0, in1, ex0, ex1);
                     if (PWP1) {
                         du = pwp1_rate(c, hc, pwp, dt);
                         Du = Du + f2 * du;
@@ -1364,8 +1368,8 @@ __global__ void __launch_bounds__(128, 6) k_force_rk(PState A, Search Q, StepSca
                 }
             }
         }
-        rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, Dx0, Dx1, Dv0, Dv1, xx, xy, vx, vy, out, h, pwp, u0,
-                  Du, box);
+        rk_finish<GEN>(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, Dx0, Dx1, Dv0, Dv1, xx, xy, vx, vy, out, h, pwp,
+                       u0, Du, GEN ? ex0 + in0 : 0.f, GEN ? ex1 + in1 : 0.f, box);
     }
     if (c.erosion) flush_node_box(S, box);
 }
@@ -1733,6 +1737,7 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
         bool out = C.out[i] != 0;
         float xx, xy, vx, vy;
         float2 dx = make_float2(0.f, 0.f), dv = make_float2(0.f, 0.f);
+        float2 acc = make_float2(0.f, 0.f);  // ex + in of the last stage
         if (out) {
             const float2 xo = C.xo[i], vo = C.v[i];
             xx = xo.x; xy = xo.y; vx = vo.x; vy = vo.y;
@@ -1756,14 +1761,15 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
                 else
                     ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, soil_fraction(c, Q, A, i), fin.x, fin.y,
                                    ex0, ex1);
-                dv.x = dv.x + 1.f * (ex0 + fin.x);
-                dv.y = dv.y + 1.f * (ex1 + fin.y);
+                acc = make_float2(ex0 + fin.x, ex1 + fin.y);
+                dv.x = dv.x + 1.f * acc.x;
+                dv.y = dv.y + 1.f * acc.y;
                 dx.x = dx.x + 1.f * vx;
                 dx.y = dx.y + 1.f * vy;
             }
         }
         rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, dx.x, dx.y, dv.x, dv.y, xx, xy, vx, vy, out,
-                  hfin[i], pwp, 0.f, 0.f, box);  // (icpwp 1 runs unstaged only)
+                  hfin[i], pwp, 0.f, 0.f, acc.x, acc.y, box);  // (icpwp 1 runs unstaged only)
     }
     if (c.erosion) flush_node_box(S, box);
 }

@@ -63,9 +63,11 @@ extern "C" {
  * SPH_SW_2019.f90:6775-6783, Get_Grav_Ext_SW :9264-9270), const(20)
  * density-factor switch (0 or 1), const(21)
  * erosion law (1 = Hungr, 2 = bed angle above the equilibrium angle, with a
- * frictional law and const(17)/(18) solid and fluid densities), const(22)
- * erosion constant, const(23) law 2's C*, const(47) slip factor alpha,
- * const(48) maximum erodible depth.
+ * frictional law, 3 = basal shear above the bed strength; 2 and 3 with
+ * const(17)/(18) solid and fluid densities), const(22) erosion constant,
+ * const(23) law 2's C* or law 3's bed cohesion, const(24)/(25) law 3's
+ * tan(phi) and pore-pressure factor, const(47) slip factor alpha, const(48)
+ * maximum erodible depth.
  */
 typedef struct gfsph_params {
     float cst[GFSPH_NCONST];

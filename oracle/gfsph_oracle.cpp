@@ -291,6 +291,7 @@ struct Oracle {
      * mini_DFs_dens_and_pwp_factors (Get_Pwp_SW, :11502-11632) for the update */
     int icpwp;
     R fact_dens, fact_pwp_max, fact_pwp_min, fpwp_max, fpwp_min, fpwp_min_g, bfact, alphas, alphas2;
+    R dens_bar, dens_bar_eff; /* of DFs_FSs_dens_and_pwp_factors, read by erosion law 3 */
     std::vector<R> ex, in, Dx, Dv, av;
     std::vector<int> flag;
     /* pairs */
@@ -1062,6 +1063,15 @@ struct Oracle {
      * atan and tan in FP64, rounded once */
     R erosion_rate(const Local& L) {
         if (eros_law == 1) return (cst[22] * L.h) * L.vmod;
+        if (eros_law == 3) { /* :10357-10376, with the friction after the reversal filter */
+            R er = 0;
+            if (L.vmod > lit<R>(1.e-5)) {
+                R taub = dens_bar * std::sqrt(L.frictx * L.frictx + L.fricty * L.fricty);
+                R tauf = cst[23] + (((dens_bar_eff * cst[1]) * L.h) * ((R)1 - cst[25])) * cst[24];
+                if (taub > tauf && L.vmod > lit<R>(1.e-3)) er = (cst[22] * (taub - tauf)) / dens_bar_eff;
+            }
+            return er;
+        }
         R er = 0;
         if (L.vmod > lit<R>(1.e-5)) {
             R denss = cst[17], densw = cst[18], dens = cst[2];
@@ -1091,6 +1101,9 @@ struct Oracle {
             Local L;
             ext_locals(i, rho[i], L);
             grav_and_friction(i, L, top, nfric);
+            /* law 3 reads the friction after the reversal filter, with the
+               last stage's exdvxdt + indvxdt (ExtForces_SW(1) keeps them) */
+            if (eros_law == 3) reversal_filter(i, L, ex[2 * i] + in[2 * i], ex[2 * i + 1] + in[2 * i + 1], nfric);
             R er = erosion_rate(L);
             R base = dt * er;
             R xx = x[2 * i], yy = x[2 * i + 1];
@@ -1332,7 +1345,11 @@ struct Oracle {
         if (P->cst[35] > 0.01f || P->cst[42] > 0.f || P->cst[40] > 1.e-6f) return GFSPH_ERR_UNSUPPORTED;
         if (P->ws_interact == 1 && (P->cst[49] > 0.f || P->cst[54] > 0.f)) return GFSPH_ERR_UNSUPPORTED; /* :1328-1345 */
         eros_law = ic_erosion ? (int)(cst[21] + lit<R>(0.1)) : 0;
-        if (ic_erosion && eros_law != 1 && eros_law != 2) return GFSPH_ERR_UNSUPPORTED;
+        if (ic_erosion && (eros_law < 1 || eros_law > 3)) return GFSPH_ERR_UNSUPPORTED;
+        if (eros_law == 3) { /* denss, densw (:10363-10367); constant dens_bar (ic_hrelSat 0) */
+            if (P->cst[16] <= 1.e-3f || P->cst[17] <= 1.e-3f) return GFSPH_ERR_ARG;
+            if ((int)(P->cst[33] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;
+        }
         if (eros_law == 2) { /* tanfi is a friction-law local: frictional laws only; denss, densw (:10337-10340) */
             if (!((nfric >= 5 && nfric <= 8) || nfric == 26 || nfric == 27)) return GFSPH_ERR_UNSUPPORTED;
             if (P->cst[16] <= 1.e-3f || P->cst[17] <= 1.e-3f) return GFSPH_ERR_ARG;
@@ -1363,13 +1380,15 @@ struct Oracle {
         alphas = cst[14];
         fact_pwp_max = 1; fact_pwp_min = 0; fpwp_max = 1; fpwp_min = 0; fpwp_min_g = 0;
         fact_dens = 1;
+        dens_bar = dens; /* ic_fct_dens = 0, :8999-9008 */
+        dens_bar_eff = dens - ((densw < lit<R>(1.e-3)) ? (R)1000 : densw);
         if (ic_fct_dens == 1) {
             if (denss < lit<R>(1.e-3) || densw < lit<R>(1.e-3)) return GFSPH_ERR_ARG;
             R porosity = (denss - dens) / (denss - densw);
             R dens2 = ((R)1 - porosity) * denss;
             R dens1 = ((R)1 - porosity) * denss + porosity * densw;
-            R dens_bar = ((R)1 - alphas) * dens2 + alphas * dens1;
-            R dens_bar_eff = dens_bar - densw * alphas;
+            dens_bar = ((R)1 - alphas) * dens2 + alphas * dens1;
+            dens_bar_eff = dens_bar - densw * alphas;
             fact_dens = dens_bar_eff / dens_bar;
             if (icpwp > 0) {
                 fact_pwp_max = (R)1 + (alphas * densw) / dens_bar_eff;

@@ -145,14 +145,23 @@ def test_erosion_and_dem_rows_match_oracle(gfsph_lib, oracle_mod):
     sim.close()
 
 
-@pytest.mark.parametrize("rheo", ["frictional_voellmy", "curvature", "mu_I_8"])
-def test_erosion_law_2_matches_oracle(gfsph_lib, oracle_mod, rheo):
+EROSION_LAWS = {
+    2: {17: 2650.0, 18: 1000.0, 21: 2, 22: 0.05, 23: 0.6},
+    3: {17: 2650.0, 18: 1000.0, 21: 3, 22: 2e-3, 23: 500.0, 24: 0.1, 25: 0.5},
+}
+
+
+@pytest.mark.parametrize("law,rheo", [(2, "frictional_voellmy"), (2, "curvature"), (2, "mu_I_8"),
+                                      (3, "frictional_voellmy"), (3, "hb_23_m1")])
+def test_erosion_laws_2_and_3_match_oracle(gfsph_lib, oracle_mod, law, rheo):
     """Erosion law 2 (Get_Erosion_Rate_SW, SPH_SW_2019.f90:10332-10356): the
     rate C22 C23 |v| tan(theta - theta_e) from the bed angle along the flow
-    and the equilibrium angle of the friction law's tanfi; 1 and 20 steps of
-    the channel release against the oracle, mass and DEM rows included."""
+    and the equilibrium angle of the friction law's tanfi; law 3 (:10357-10376):
+    C22 (Taub - Tauf) / dens_bar_eff from the basal shear of the friction
+    after the reversal filter.  1 and 20 steps of the channel release against
+    the oracle, mass and DEM rows included."""
     w = small_channel()
-    w.const = {**w.const, **RHEOLOGIES[rheo], 17: 2650.0, 18: 1000.0, 21: 2, 22: 0.05, 23: 0.6}
+    w.const = {**w.const, **RHEOLOGIES[rheo], **EROSION_LAWS[law]}
     sim, st, p = setup_pair(w, oracle_mod)
     ny, nx = w.z.shape
     for nsteps in (1, 19):
@@ -513,9 +522,10 @@ def test_basal_laws_outside_the_path_are_refused(gfsph_lib):
              ({5: 24, 6: 3000.0, 7: 1000.0, 8: 0.0}, gfsph.ERR_ARG),
              ({5: 25, 6: 3000.0, 7: 1000.0, 8: -1.0}, gfsph.ERR_ARG)]
     cases += [({5: nf}, gfsph.ERR_UNSUPPORTED) for nf in (9, 10, 22, 201)]
-    # erosion law 2 needs a frictional law's tanfi and the two densities; law 3 is not built
+    # erosion law 2 needs a frictional law's tanfi, laws 2 and 3 the two densities; law 4 does not exist
     cases += [({5: 4, 6: 500.0, 7: 50.0, 17: 2650.0, 18: 1000.0, 21: 2, 22: 0.05}, gfsph.ERR_UNSUPPORTED),
-              ({21: 2, 22: 0.05, 17: 0.0, 18: 1000.0}, gfsph.ERR_ARG), ({21: 3, 22: 0.05}, gfsph.ERR_UNSUPPORTED)]
+              ({21: 2, 22: 0.05, 17: 0.0, 18: 1000.0}, gfsph.ERR_ARG), ({21: 3, 22: 0.05}, gfsph.ERR_ARG),
+              ({21: 4, 22: 0.05}, gfsph.ERR_UNSUPPORTED)]
     # grain crushing const(36), the solid-end laws const(43) and the late
     # Voellmy xi const(41) (Input_SW :1312-1325, ExtForces_SW :8424-8434)
     cases += [({36: 1.0}, gfsph.ERR_UNSUPPORTED), ({43: 1.0}, gfsph.ERR_UNSUPPORTED),

@@ -323,6 +323,34 @@ def test_erosion_law_2_grows_the_mass_above_the_equilibrium_angle(oracle_mod, vy
     assert abs(st.v[0, 0]) < 1e-12
 
 
+@pytest.mark.parametrize("c_basal", [100.0, 5000.0])
+def test_erosion_law_3_erodes_where_the_basal_shear_exceeds_the_strength(oracle_mod, c_basal):
+    """Get_Erosion_Rate_SW law 3 (SPH_SW_2019.f90:10357-10376): a lone
+    frictional particle sliding down a plane carries the basal shear Taub =
+    dens |frict| = dens g tan(phi) h (ic_fct_dens 0: dens_bar = dens,
+    dens_bar_eff = dens - densw) and erodes at C22 (Taub - Tauf) /
+    dens_bar_eff where it exceeds Tauf = C23 + dens_bar_eff g h (1 - C25)
+    C24; with a strong bed (C23 = 5000) nothing is eroded."""
+    tan_t, mu, keros, beta, tanb, dt = 0.5, 0.2, 1e-3, 0.5, 0.1, 0.02
+    nx, ny, d = 20, 1200, 5.0
+    yy = np.arange(ny)[:, None] * d * np.ones((1, nx))
+    z = (ny * d - yy) * tan_t
+    const = {3: 0.0, 9: mu, 17: 2650.0, 18: 1000.0, 21: 3, 22: keros, 23: c_basal, 24: tanb, 25: beta, 48: 5.0}
+    p = params(const, sle=0, dt=dt, ic_adapt=0, average_velocity=0)
+    topol = oracle_mod.initial_topol(z, d, d, const, deriv=1, mode=2)
+    h = lone_particle_depth(oracle_mod)
+    st = oracle_mod.State(np.array([[50.0, 3000.0]]), np.array([[0.0, 3.0]]), np.array([h]), np.array([4.0]),
+                          np.array([2.0]), topol, dt=dt)
+    oracle_mod.run(2, p, nx, ny, d, d, st, 1)
+    f = lambda c: float(np.float32(c))  # the constants as the FP32 parameter block carries them
+    g, dens, densw = f(9.8), 2000.0, 1000.0
+    taub = dens * g * f(mu) * h
+    tauf = f(c_basal) + (dens - densw) * g * h * (1.0 - f(beta)) * f(tanb)
+    e = max(0.0, f(keros) * (taub - tauf) / (dens - densw))
+    assert abs(st.mass[0] / 4.0 - 1.0 - dt * e / h) < 1e-10, (st.mass[0], dt * e / h)
+    assert (e > 0) == (c_basal < 1000.0)
+
+
 def test_fp32_and_fp64_oracles_agree_closely(oracle_mod):
     w = workloads.inclined_plane()
     p = workloads.make_params(w, gfsph)
