@@ -500,18 +500,21 @@ int enqueue_stages(gfsph_handle* h, PState As[5]) {
         });
         nk++;
         launch(h, K_STAGE, [&] {
+            // hprev: the depth the previous stage left (icpwp 1's bound)
+            const float* hprev = (s > 0) ? As[s - 1].rho : As[0].rho;
             if (s < 3) {
                 if (c.cos_theta)
-                    pdl_launch(k_stage<true>, pb, kThreads, st, h->A, q, S, c, h->dem, h->carry, s, As[s].rho, As[s + 1].rho);
+                    pdl_launch(k_stage<true>, pb, kThreads, st, h->A, q, S, c, h->dem, h->carry, s, As[s].rho,
+                               As[s + 1].rho, hprev);
                 else
                     pdl_launch(k_stage<false>, pb, kThreads, st, h->A, q, S, c, h->dem, h->carry, s, As[s].rho,
-                                                            As[s + 1].rho);
+                               As[s + 1].rho, hprev);
             } else if (c.cos_theta) {
                 pdl_launch(k_stage_final<true>, pb, kThreads, st, h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
-                                                             h->carry, As[3].rho, As[4].rho);
+                           h->carry, As[3].rho, As[4].rho, hprev);
             } else {
                 pdl_launch(k_stage_final<false>, pb, kThreads, st, h->A, q, S, c, h->dem, n, h->B, h->velfin, h->d_auxv,
-                                                              h->carry, As[3].rho, As[4].rho);
+                           h->carry, As[3].rho, As[4].rho, hprev);
             }
         });
         nk++;
@@ -687,7 +690,7 @@ void free_particles(gfsph_handle* h) {
     dfree(h->cellA); dfree(h->velfin); dfree(h->pterm); dfree(h->keyrank); dfree(h->perm); dfree(h->ncount);
     dfree(h->nbr); dfree(h->f2tmp); dfree(h->xhm); dfree(h->indv); dfree(h->rho0);
     dfree(h->carry.v); dfree(h->carry.acc); dfree(h->carry.dx); dfree(h->carry.dv); dfree(h->carry.xo);
-    dfree(h->carry.out); dfree(h->rhoS); dfree(h->rcell); dfree(h->xsv); dfree(h->pr);
+    dfree(h->carry.out); dfree(h->carry.u); dfree(h->carry.du); dfree(h->carry.Du); dfree(h->rhoS); dfree(h->rcell); dfree(h->xsv); dfree(h->pr);
     dfree(h->spec_u); dfree(h->spec_a); dfree(h->zpw); dfree(h->gzw); dfree(h->bxy);
     dfree(h->mass0_u);
     h->kcap = 0;
@@ -859,9 +862,6 @@ int validate(const gfsph_params* p) {
     const int fct = (int)(p->cst[19] + 0.1f);                          // ic_fct_dens
     if (fct != 0 && fct != 1) return GFSPH_ERR_UNSUPPORTED;
     if (p->icpwp != 0 && p->icpwp != 1 && p->icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
-    // icpwp 1 integrates u inside the fused RK45 only: not with the staged
-    // pressure (nor_density, ic_cosTheta = 1)
-    if (p->icpwp == 1 && (p->nor_density != 0 || cos_theta != 0)) return GFSPH_ERR_UNSUPPORTED;
     if ((fct != 0 || p->icpwp != 0) && (int)(p->cst[33] + 0.01f) != 0) return GFSPH_ERR_UNSUPPORTED;  // ic_hrelSat
     if (p->icpwp == 3 && p->cst[25] > 0.f) return GFSPH_ERR_UNSUPPORTED;  // drag laws rescale Bfact
     if (fct == 1 && (p->cst[16] < 1.e-3f || p->cst[17] < 1.e-3f)) return GFSPH_ERR_ARG;  // denss, densw
@@ -1193,6 +1193,7 @@ int gfsph_upload(gfsph_handle* h, int n, const float* x, const float* v, const f
             StageCarry& C = h->carry;
             st |= dalloc(&C.v, n); st |= dalloc(&C.acc, n); st |= dalloc(&C.dx, n); st |= dalloc(&C.dv, n);
             st |= dalloc(&C.xo, n); st |= dalloc(&C.out, n);
+            if (h->rheo.icpwp == 1) { st |= dalloc(&C.u, n); st |= dalloc(&C.du, n); st |= dalloc(&C.Du, n); }
             if (h->rheo.nor_density) st |= dalloc(&h->rhoS, 5 * (size_t)n);
         }
         if (h->rheo.skf == 2 || h->rheo.skf == 3) st |= dalloc(&h->rcell, n);

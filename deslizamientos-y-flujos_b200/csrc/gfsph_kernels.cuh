@@ -1397,7 +1397,37 @@ struct StageCarry {
     float2* dv;   // Dvx_RK
     float2* xo;   // stage position of a particle that left the DEM box
     int* out;     // 1 once it has (it is frozen for the rest of the step)
+    // icpwp = 1: u of the last stage (kept by a particle that left), its
+    // rate du and Du_RK
+    float* u;
+    float* du;
+    float* Du;
 };
+
+// The stage value of icpwp 1's u (RK45 :823-830): u0 + f1 dt du of the
+// previous stage, bounded by the depth that stage left (the step start's,
+// after Adaptive_dt's clamp, in stage 0; else IntForces_SW's clamp to h_inf).
+__device__ __forceinline__ float pwp1_stage(const Rheo& c, const PState& A, const Search& Q, const StageCarry& C,
+                                            int s, int i, float fdt, const float* hprev) {
+    float u = A.pwp[i] + fdt * ((s > 0) ? C.du[i] : 0.f);
+    float rc = Q.rho0[i];
+    if (s > 0) {
+        rc = hprev[i];
+        if (rc < c.h_inf) rc = c.h_inf;
+    }
+    if (u > rc) u = rc;
+    else if (u < 0.f) u = 0.f;
+    C.u[i] = u;
+    return u;
+}
+
+// Its rate of this stage and the running Du_RK.
+__device__ __forceinline__ void pwp1_accumulate(const Rheo& c, const StageCarry& C, int s, int i, float hc, float u,
+                                                float dt, float f2) {
+    const float du = pwp1_rate(c, hc, u, dt);
+    C.du[i] = du;
+    C.Du[i] = ((s > 0) ? C.Du[i] : 0.f) + f2 * du;
+}
 
 // Depth of the previous sum_density_Tools call as the next one reads it:
 // clamped to h_inf when IntForces_SW (:6769) has run in between.
@@ -1651,7 +1681,8 @@ __global__ void __launch_bounds__(128) k_wir_pairs_big(PState A, Search Q, StepS
 // skips it.
 template <bool COS>
 __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* S, Rheo c, DemView dem,
-                                               StageCarry C, int s, const float* hs_, const float* hnext) {
+                                               StageCarry C, int s, const float* hs_, const float* hnext,
+                                               const float* hprev) {
     PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive;
@@ -1669,6 +1700,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
         const float fdt = f1 * dt;
         const float xx = x0.x + fdt * vp.x, xy = x0.y + fdt * vp.y;
         const float vx = v0.x + fdt * ap.x, vy = v0.y + fdt * ap.y;
+        const float u1 = (c.icpwp == 1) ? pwp1_stage(c, A, Q, C, s, i, fdt, hprev) : 0.f;
         if (out_of_box(dem, xx, xy)) {
             C.out[i] = 1;
             C.xo[i] = make_float2(xx, xy);
@@ -1680,13 +1712,14 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
         const float h = hs_[i];
         const float hc = (h < c.h_inf) ? c.h_inf : h;
         const float2 fin = Q.indv[i];
-        const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
+        const float pwp = (c.icpwp == 3) ? A.pwp[i] : u1;
         float ex0, ex1;
         if (c.ws)
             ext_accel_wir(c, dem, dt, xx, xy, vx, vy, hc, fin.x, fin.y, Q.spec[i] == 2, Q.zpw[i], Q.gzw[i], Q.bxy[i],
                           ex0, ex1);
         else
             ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, soil_fraction(c, Q, A, i), fin.x, fin.y, ex0, ex1);
+        if (c.icpwp == 1) pwp1_accumulate(c, C, s, i, hc, u1, dt, f2);
         const float a0 = ex0 + fin.x, a1 = ex1 + fin.y;
         dv.x = dv.x + f2 * a0;
         dv.y = dv.y + f2 * a1;
@@ -1713,7 +1746,7 @@ __global__ void __launch_bounds__(128) k_stage(PState A, Search Q, StepScalars* 
 template <bool COS>
 __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepScalars* S, Rheo c, DemView dem, int n,
                                                      PState B, float2* velfin, double2* auxv, StageCarry C,
-                                                     const float* h4, const float* hfin) {
+                                                     const float* h4, const float* hfin, const float* h3) {
     PDL_ENTRY();
     if (S->skip) return;
     const int nact = S->nactive;
@@ -1733,7 +1766,7 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
             continue;
         }
         const float2 x0 = A.pos[i], v0 = A.vel[i];
-        const float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
+        float pwp = (c.icpwp == 3) ? A.pwp[i] : 0.f;
         bool out = C.out[i] != 0;
         float xx, xy, vx, vy;
         float2 dx = make_float2(0.f, 0.f), dv = make_float2(0.f, 0.f);
@@ -1741,6 +1774,7 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
         if (out) {
             const float2 xo = C.xo[i], vo = C.v[i];
             xx = xo.x; xy = xo.y; vx = vo.x; vy = vo.y;
+            if (c.icpwp == 1) pwp = C.u[i];  // u of the stage it left in
         } else {
             const float2 vp = C.v[i], ap = C.acc[i];
             dx = C.dx[i];
@@ -1748,6 +1782,7 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
             const float fdt = 1.f * dt;
             xx = x0.x + fdt * vp.x; xy = x0.y + fdt * vp.y;
             vx = v0.x + fdt * ap.x; vy = v0.y + fdt * ap.y;
+            if (c.icpwp == 1) pwp = pwp1_stage(c, A, Q, C, 3, i, fdt, h3);
             if (out_of_box(dem, xx, xy)) {
                 out = true;
             } else {
@@ -1761,6 +1796,7 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
                 else
                     ext_accel<COS>(c, dem, dt, xx, xy, vx, vy, hc, pwp, soil_fraction(c, Q, A, i), fin.x, fin.y,
                                    ex0, ex1);
+                if (c.icpwp == 1) pwp1_accumulate(c, C, 3, i, hc, pwp, dt, 1.f);
                 acc = make_float2(ex0 + fin.x, ex1 + fin.y);
                 dv.x = dv.x + 1.f * acc.x;
                 dv.y = dv.y + 1.f * acc.y;
@@ -1768,8 +1804,10 @@ __global__ void __launch_bounds__(128) k_stage_final(PState A, Search Q, StepSca
                 dx.y = dx.y + 1.f * vy;
             }
         }
+        const float u0 = (c.icpwp == 1) ? A.pwp[i] : 0.f;
+        const float Du = (c.icpwp == 1 && !out) ? C.Du[i] : 0.f;
         rk_finish(A, Q, S, c, dem, B, velfin, auxv, i, dt, x0, v0, dx.x, dx.y, dv.x, dv.y, xx, xy, vx, vy, out,
-                  hfin[i], pwp, 0.f, 0.f, acc.x, acc.y, box);  // (icpwp 1 runs unstaged only)
+                  hfin[i], pwp, u0, Du, acc.x, acc.y, box);
     }
     if (c.erosion) flush_node_box(S, box);
 }

@@ -88,8 +88,8 @@ typedef struct gfsph_params {
     int max_neighbours;    /* initial neighbour-table capacity per particle, 0..65536;
                               0 = 96 (grows on demand) */
     int icpwp;             /* 0 none; 1 basal pore-water pressure u integrated by the RK45 with the
-                              dissipation of ExtForces_SW (SPH_SW_2019.f90:8648-8652; not with nor_density
-                              or ic_cosTheta = 1); 3 with one point (Get_Pwp_SW, nUaux = 1) */
+                              dissipation of ExtForces_SW (SPH_SW_2019.f90:8648-8652); 3 with one point
+                              (Get_Pwp_SW, nUaux = 1) */
     float pwp0rel;         /* icpwp = 1, 3: initial u, Uaux = pwp0rel * rho * const(14)
                               (Input_SW SPH_SW_2019.f90:1724-1737, 1829-1852) */
     int ws_interact;       /* ic_ws_Interact: 0 one material; 1 soil and water particles (ic_soil = ic_water = 1,

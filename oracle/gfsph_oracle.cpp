@@ -1405,7 +1405,6 @@ struct Oracle {
             return GFSPH_ERR_UNSUPPORTED;
         }
         if (icpwp != 0 && icpwp != 1 && icpwp != 3) return GFSPH_ERR_UNSUPPORTED;
-        if (icpwp == 1 && (P->nor_density != 0 || ic_costheta != 0)) return GFSPH_ERR_UNSUPPORTED; /* as the device */
         if ((ic_fct_dens != 0 || icpwp != 0) && (int)(cst[34] + lit<R>(0.01)) != 0) return GFSPH_ERR_UNSUPPORTED;
         if (icpwp == 3 && cst[26] > 0) return GFSPH_ERR_UNSUPPORTED; /* drag laws rescale Bfact */
         if (ic_fct_dens == 1 && icpwp != 0 && !(alphas > lit<R>(0.01))) return GFSPH_ERR_UNSUPPORTED;

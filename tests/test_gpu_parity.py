@@ -409,20 +409,25 @@ def test_far_apart_releases_on_a_large_dem(gfsph_lib, oracle_mod):
     sim.close()
 
 
-@pytest.mark.parametrize("icpwp,fct", [(3, 0), (3, 1), (1, 0), (1, 1)])
-def test_pore_water_pressure_matches_oracle(gfsph_lib, oracle_mod, icpwp, fct):
+@pytest.mark.parametrize("icpwp,fct,staged", [(3, 0, ""), (3, 1, ""), (1, 0, ""), (1, 1, ""), (1, 0, "nor"),
+                                              (1, 1, "cos")])
+def test_pore_water_pressure_matches_oracle(gfsph_lib, oracle_mod, icpwp, fct, staged):
     """icpwp = 3 (Get_Pwp_SW with one point): Uaux starts at pwp0rel * h,
     lowers the basal friction by 1 - pwp/h, and relaxes towards the depth
     change of every step.  icpwp = 1: u starts the same way and the RK45
     integrates its dissipation stage by stage (ExtForces_SW :8648-8652).
     ic_fct_dens = 1 adds the buoyancy factor of tanfi and the negative pwp
-    bounds."""
+    bounds.  With the staged RK45 (nor_density, ic_cosTheta = 1) u's bound
+    in each stage is the depth the previous stage left."""
     w = small_channel()
     extra = {13: 0.02, 14: 1.0}
     if fct:
         extra.update({17: 2650.0, 18: 1000.0, 19: 0.5, 20: 1})
+    if staged == "cos":
+        extra[16] = 1.0
     w.const = {**w.const, **extra}
-    sim, st, p = setup_pair(w, oracle_mod, icpwp=icpwp, pwp0rel=0.8)
+    kw = {"nor_density": 1} if staged == "nor" else {}
+    sim, st, p = setup_pair(w, oracle_mod, icpwp=icpwp, pwp0rel=0.8, **kw)
     assert np.array_equal(sim.pwp(), (np.float32(0.8) * (w.rho * np.float32(1.0))).astype(np.float32))
     ny, nx = w.z.shape
     for nsteps in (1, 29):
@@ -435,7 +440,7 @@ def test_pore_water_pressure_matches_oracle(gfsph_lib, oracle_mod, icpwp, fct):
             assert rel_l2(g[key], ref) <= tol, (key, nsteps)
         assert rel_l2(sim.pwp(), st.pwp) <= tol
     # the friction really is lowered: without pore pressure the flow is slower
-    sim0, st0, _ = setup_pair(w, oracle_mod)
+    sim0, st0, _ = setup_pair(w, oracle_mod, **kw)
     sim0.step(30)
     v0 = np.hypot(*sim0.download()["v"].T).mean()
     assert np.hypot(*g["v"].T).mean() > v0
@@ -530,8 +535,8 @@ def test_basal_laws_outside_the_path_are_refused(gfsph_lib):
     # Voellmy xi const(41) (Input_SW :1312-1325, ExtForces_SW :8424-8434)
     cases += [({36: 1.0}, gfsph.ERR_UNSUPPORTED), ({43: 1.0}, gfsph.ERR_UNSUPPORTED),
               ({41: 300.0}, gfsph.ERR_UNSUPPORTED)]
-    # icpwp 1 integrates u inside the unstaged RK45 only; icpwp 2 is not built
-    for kw in ({"icpwp": 1, "nor_density": 1}, {"icpwp": 2}):
+    # icpwp 2 (a finite-difference column per particle) is not built
+    for kw in ({"icpwp": 2}, {"icpwp": 4}):
         p = workloads.make_params(w, gfsph, pwp0rel=0.5, **kw)
         with pytest.raises(gfsph.GfsphError) as e:
             gfsph.Sim(p, w.z, dx=w.dx, dy=w.dy)
