@@ -1909,7 +1909,7 @@ int adj_capture(gfsph_adjoint* a, float2* x, float2* v, bool fields, float* hs =
 }
 
 int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v, const float* rho = nullptr,
-                const float* hs = nullptr) {
+                const float* hs = nullptr, bool clear_err = true) {
     gfsph_handle* h = a->h;
     if (h->n != a->n) return GFSPH_ERR_STATE;  // the handle's buffers were dropped or resized
     launch(h, K_ADJOINT, [&] {
@@ -1918,8 +1918,22 @@ int adj_restore(gfsph_adjoint* a, const float2* x, const float2* v, const float*
     });
     CK(cudaGetLastError());
     set_field<float>(h, offsetof(StepScalars, dt), a->dt0);
-    set_field<int>(h, offsetof(StepScalars, err), 0);
+    if (clear_err) set_field<int>(h, offsetof(StepScalars, err), 0);
     h->has_state = true;
+    return 0;
+}
+
+// The backward sweep replays steps that the recording run has taken from
+// the same states with the same deterministic kernels, so their capacity and
+// their particle counts (every particle active and regular) were checked
+// then: within a segment the steps are enqueued without waiting, the error
+// word left set by any failed step (which also makes every later step skip),
+// and checked once at the segment's end.
+int adj_segment_check(gfsph_handle* h) {
+    int st = read_scalars(h);
+    if (st) return st;
+    if (h->hS->err) return GFSPH_ERR_CAPACITY;
+    if (h->hS->nactive != h->n || h->hS->nreg != h->hS->nactive) return GFSPH_ERR_UNSUPPORTED;
     return 0;
 }
 
@@ -2129,16 +2143,21 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
         CK(cudaMemcpyAsync(a->segv, a->ckv + un * sg, un * sizeof(float2), cudaMemcpyDeviceToDevice, st));
         if (a->sle) CK(cudaMemcpyAsync(a->segh, a->ckh + un * sg, un * sizeof(float), cudaMemcpyDeviceToDevice, st));
         auto seg_h = [&](int q) -> float* { return a->sle ? a->segh + un * q : nullptr; };
+        set_field<int>(h, offsetof(StepScalars, err), 0);
         for (int q = 1; q < len; q++) {
-            int r = adj_restore(a, a->segx + un * (q - 1), a->segv + un * (q - 1), nullptr, seg_h(q - 1));
-            if (!r) r = adj_one_step(h);
+            int r = adj_restore(a, a->segx + un * (q - 1), a->segv + un * (q - 1), nullptr, seg_h(q - 1), false);
+            if (!r) r = enqueue_chunk(h, 1, 1e300);
             if (!r) r = adj_capture(a, a->segx + un * q, a->segv + un * q, false, seg_h(q));
+            if (r) return r;
+        }
+        if (len > 1) {
+            int r = adj_segment_check(h);
             if (r) return r;
         }
         for (int q = len - 1; q >= 0; q--) {
             const bool last = (t0 + q == a->nsteps - 1);
-            int r = adj_restore(a, a->segx + un * q, a->segv + un * q, nullptr, seg_h(q));
-            if (!r) r = adj_one_step(h);  // neighbour table, density, forces of this step
+            int r = adj_restore(a, a->segx + un * q, a->segv + un * q, nullptr, seg_h(q), false);
+            if (!r) r = enqueue_chunk(h, 1, 1e300);  // neighbour table, density, forces of this step
             if (r) return r;
             Search Q = make_search(h);
             const int pb = blocks_for(n);
@@ -2168,6 +2187,8 @@ int gfsph_adjoint_backward(gfsph_adjoint* a, const float* gx, const float* gv, c
             });
             CK(cudaGetLastError());
         }
+        int r = adj_segment_check(h);
+        if (r) return r;
     }
     if (gx0) CK(cudaMemcpyAsync(gx0, a->lx, un * sizeof(float2), cudaMemcpyDeviceToHost, st));
     if (gv0) CK(cudaMemcpyAsync(gv0, a->lv, un * sizeof(float2), cudaMemcpyDeviceToHost, st));
