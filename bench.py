@@ -637,6 +637,8 @@ def run_leg(args):
         out = wir_bench(args, gfsph, workloads, torch)
     elif args.leg == "plane":
         out = plane_bench(args, gfsph, workloads, torch)
+    elif args.leg == "adjoint":  # --steps recorded steps, a checkpoint every --steps // 10
+        out = adjoint_bench(gfsph, workloads, torch, nsteps=args.steps, every=max(1, args.steps // 10))
     else:
         out = cg_bench(args, gfsph, workloads, peak)
     print(json.dumps({"leg": args.leg, **out}))
@@ -656,7 +658,7 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=8)
     ap.add_argument("--ensemble-wave", type=int, default=64, help="members held on the device at once")
     ap.add_argument("--no-extras", action="store_true", help="only the step: no ensemble, CG, coupling, adjoint")
-    ap.add_argument("--leg", choices=["gfl", "wir", "plane", "cg"],
+    ap.add_argument("--leg", choices=["gfl", "wir", "plane", "cg", "adjoint"],
                     help="run one secondary leg alone and print its line (for profiling it)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)

@@ -272,29 +272,31 @@ __global__ void __launch_bounds__(128) k_adj_xsph(PState A, Search Q, Rheo c, in
         const int cnt = Q.ncount[k];
         double s = 0.0, a0 = 0.0, a1 = 0.0, dm = 0.0, dh = 0.0, dx0 = 0.0, dx1 = 0.0, dhs = 0.0;
         for (int q = 0; q < cnt; q++) {
-            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride].x;
+            // the pair's W and grad W as the replayed step's search stored them
+            const int4 e = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride];
+            const int j = e.x & ~kCrossBit;
+            const float w = __int_as_float(e.y), d0 = __int_as_float(e.z), d1 = __int_as_float(e.w);
             const float4 o = Q.xhm[j];
-            PairGeom g;
-            pair_test(xk, make_float2(o.x, o.y), me.z, o.z, g);
-            float w, d0, d1;
-            sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
             // the pair terms in FP64: their sums over the neighbours cancel
             // strongly (antisymmetric in k, j)
             const float2 vj = velfin[j], lj = lv2[j];
             const double den = (double)hk + (double)A.rho[j], mj = o.w, wd = w;
-            const double ckj = (2.0 * mj * wd) / den, cjk = (2.0 * (double)mk * wd) / den;
+            const double rden = 1.0 / den;
+            const double ckj = (2.0 * mj * wd) * rden, cjk = (2.0 * (double)mk * wd) * rden;
             const double D0 = (double)vj.x - vk.x, D1 = (double)vj.y - vk.y;
             const double pk = lk.x * D0 + lk.y * D1;     // lambda_k . (v_j - v_k)
             const double pj = -(lj.x * D0 + lj.y * D1);  // lambda_j . (v_k - v_j)
             s += ckj;
             a0 += cjk * lj.x;
             a1 += cjk * lj.y;
-            dm += (2.0 * wd / den) * pj;
-            dh -= (ckj * pk + cjk * pj) / den;
-            const double lw = (2.0 * mj / den) * pk + (2.0 * (double)mk / den) * pj;
+            dm += (2.0 * wd * rden) * pj;
+            dh -= (ckj * pk + cjk * pj) * rden;
+            const double lw = (2.0 * mj * rden) * pk + (2.0 * (double)mk * rden) * pj;
             dx0 += lw * d0;
             dx1 += lw * d1;
             if (lhsacc) {  // W_kj through mh = (hs_k + hs_j)/2
+                PairGeom g;
+                pair_test(xk, make_float2(o.x, o.y), me.z, o.z, g);
                 double dwdh, dgdh;
                 sph_kernel_dh(c.skf, g.r, g.mh, dwdh, dgdh);
                 dhs += 0.5 * lw * dwdh;
@@ -402,12 +404,14 @@ __global__ void __launch_bounds__(128) k_adj_gather(PState A, Search Q, Rheo c, 
         // the self term W(0, hs_k) m_k: dW/dh = -2 W/h
         double dhs = lhsacc ? (double)lhk * (double)mk * (-2.0 * (double)w0 / (double)me.z) : 0.0;
         for (int q = 0; q < cnt; q++) {
-            const int j = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride].x;
+            // the pair's W and grad W as the replayed step's search stored them
+            const int4 e = Q.nbr[tab_base(k, Q.kcap) + (size_t)q * kTabStride];
+            const int j = e.x & ~kCrossBit;
+            const float w = __int_as_float(e.y), d0 = __int_as_float(e.z), d1 = __int_as_float(e.w);
             const float4 o = Q.xhm[j];
             PairGeom g;
             pair_test(xk, make_float2(o.x, o.y), me.z, o.z, g);
-            float w, d0, d1, ca, cb;
-            sph_kernel(c.skf, g.r, g.dx0, g.dx1, g.mh, w, d0, d1);
+            float ca, cb;
             sph_kernel_hess(c.skf, g.r, g.mh, ca, cb);
             // the pair terms in FP64: their sums over the neighbours cancel
             // strongly (the kernel gradient is antisymmetric in k, j)
@@ -420,7 +424,8 @@ __global__ void __launch_bounds__(128) k_adj_gather(PState A, Search Q, Rheo c, 
             dx1 += fd * d1;
             // (P_k + P_j) H(d_kj) (m_k lambda_j - m_j lambda_k), H = ca dhat dhat^T + cb I
             const double u0 = (double)mk * laj.x - mj * lak.x, u1 = (double)mk * laj.y - mj * lak.y;
-            const double dh0 = (double)g.dx0 / g.r, dh1 = (double)g.dx1 / g.r;
+            const double ir = 1.0 / (double)g.r;
+            const double dh0 = (double)g.dx0 * ir, dh1 = (double)g.dx1 * ir;
             const double du = dh0 * u0 + dh1 * u1;
             dx0 += cp * ((double)ca * dh0 * du + (double)cb * u0);
             dx1 += cp * ((double)ca * dh1 * du + (double)cb * u1);
