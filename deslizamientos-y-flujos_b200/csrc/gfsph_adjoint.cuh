@@ -162,7 +162,7 @@ __device__ __forceinline__ void ext_vjp(const Rheo& c, const DemView& dem, float
                                         ExtGrad& g) {
     ExtLocal L;
     ext_locals(c, hc, vx, vy, L);
-    grav_and_friction(c, dem, xx, yy, vx, vy, 0.f, 0.f, L);
+    grav_and_friction<false, false>(c, dem, xx, yy, vx, vy, 0.f, 0.f, L);  // nfric 4-6 only here
     const float acc0 = L.gravx + in0, acc1 = L.gravy + in1;
     // branch of reversal_filter
     float dc0 = -(L.frictx * L.hinv), dc1 = -(L.fricty * L.hinv);
@@ -335,7 +335,8 @@ __global__ void __launch_bounds__(128) k_adj_rk(PState A, Search Q, const StepSc
             float nvx = v0.x + fdt * (ex0 + in0), nvy = v0.y + fdt * (ex1 + in1);
             xs[s] = nxx; ys[s] = nxy; us[s] = nvx; ws[s] = nvy;
             vx = nvx; vy = nvy;
-            ext_accel(c, dem, dt, nxx, nxy, nvx, nvy, hc, 0.f, 0.f, in0, in1, ex0, ex1);
+            // the adjoint's scope (nfric 4-6, no erosion) needs only the common laws
+            ext_accel<false, false>(c, dem, dt, nxx, nxy, nvx, nvy, hc, 0.f, 0.f, in0, in1, ex0, ex1);
         }
         const float2 lx = lx1[i], lv = lvp[i];
         const float dt6 = dt / 6.f;
