@@ -516,6 +516,28 @@ def test_eroded_soil_bingham_matches_oracle(gfsph_lib, oracle_mod):
     sim.close()
 
 
+@pytest.mark.parametrize("rheo,staged", [("manning_1", "cos"), ("laminar_2", "nor"), ("bagnold_11", "cos"),
+                                         ("hb_23_m2", "nor"), ("hb_25", "cos")])
+def test_basal_laws_on_the_staged_path_match_oracle(gfsph_lib, oracle_mod, rheo, staged):
+    """The same laws through the staged RK45 (ic_cosTheta = 1: g/sqrt(1 + |grad
+    Z|^2) in the pressure and the friction; nor_density): 1 and 20 steps
+    against the oracle."""
+    w = small_channel()
+    w.const = {**w.const, **RHEOLOGIES[rheo], **({16: 1.0} if staged == "cos" else {})}
+    kw = {"nor_density": 1} if staged == "nor" else {}
+    sim, st, p = setup_pair(w, oracle_mod, **kw)
+    ny, nx = w.z.shape
+    for nsteps in (1, 19):
+        sim.step(nsteps)
+        oracle_mod.run(oracle_mod.MODE_FP32_DACC, p, nx, ny, w.dx, w.dy, st, nsteps)
+        g = sim.download()
+        assert np.array_equal(g["flag"], st.flag)
+        tol = 1e-6 if nsteps == 1 else 1e-5
+        for key, ref in (("x", st.x), ("v", st.v), ("rho", st.rho), ("mass", st.mass)):
+            assert rel_l2(g[key], ref) <= tol, (key, nsteps, rel_l2(g[key], ref))
+    sim.close()
+
+
 def test_basal_laws_outside_the_path_are_refused(gfsph_lib):
     """basal_friction_Ext_SW stops for nfric 23 with m other than 1, 2, 1/3,
     1/2 and for a yield stress below 1e-32 (SPH_SW_2019.f90:9547-9550,
