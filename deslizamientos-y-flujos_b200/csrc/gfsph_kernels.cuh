@@ -1542,25 +1542,20 @@ __global__ void __launch_bounds__(128) k_wir_scatter(PState A, Search Q, StepSca
     if (S->skip) return;
     const int nact = S->nactive;
     const float dt = S->dt_step;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nact; i += gridDim.x * blockDim.x) {
-        if (Q.spec[i] != 1) continue;
-        float2 p;
-        if (!wir_stage_pos(A, C, s, dt, i, p) || out_of_box(dem, p.x, p.y)) continue;
-        const float h = hdep[i];
-        const int ipx = (int)((p.x - dem.xmin) / dem.dx + 1.f), ipy = (int)((p.y - dem.ymin) / dem.dy + 1.f);
-        const int x0 = max(1, ipx - 1), y0 = max(1, ipy - 1), x1 = min(dem.nx, ipx + 2), y1 = min(dem.ny, ipy + 2);
-        for (int inx = x0; inx <= x1; inx++)
-            for (int iny = y0; iny <= y1; iny++) {
-                const int ip = (iny - 1) * dem.nx + (inx - 1);
-                float dx2 = p.x - (dem.xmin + (float)(inx - 1) * dem.dx);
-                dx2 = dx2 * dx2;
-                float dy2 = p.y - (dem.ymin + (float)(iny - 1) * dem.dy);
-                dy2 = dy2 * dy2;
-                float dist = sqrtf(dx2 + dy2);
-                dist = (1.e-6f > dist) ? 1.e-6f : dist;
-                atomicAdd(&acc[ip].x, (double)(h / dist));
-                atomicAdd(&acc[ip].y, (double)(1.f / dist));
-            }
+    // the same terms h/dist and 1/dist as the erosion scatter, combined over
+    // runs of lanes with equal DEM cells before one FP64 atomic per run;
+    // block-uniform trip count: every lane of a warp reaches the scatter
+    NodeBox box = empty_node_box();
+    for (int i0 = blockIdx.x * blockDim.x; i0 < nact; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        float2 p = make_float2(0.f, 0.f);
+        float h = 0.f;
+        bool part = false;
+        if (i < nact && Q.spec[i] == 1 && wir_stage_pos(A, C, s, dt, i, p) && !out_of_box(dem, p.x, p.y)) {
+            h = hdep[i];
+            part = true;
+        }
+        erosion_scatter(dem, p.x, p.y, h, part, acc, box);
     }
 }
 
