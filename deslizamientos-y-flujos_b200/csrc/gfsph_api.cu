@@ -536,6 +536,9 @@ int enqueue_step_end(gfsph_handle* h) {
     return 1;
 }
 
+// Enqueues one step; returns the number of kernels it enqueued (not a
+// status: a failed launch surfaces through cudaGetLastError, which every
+// caller checks after the enqueue or the capture).
 int enqueue_step(gfsph_handle* h) {
     const int n = h->n;
     cudaStream_t st = h->stream;
